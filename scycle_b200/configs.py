@@ -1,0 +1,122 @@
+"""Seeded synthetic workloads in the reference's ``.in`` format.
+
+Each builder writes an ``.in`` file plus the PETSc-binary per-node fields it
+names under ``inputDir`` (big-endian int32 class id 1211214, int32 length,
+big-endian float64 values), exactly what ``Domain``/``Fault`` read with
+``loadVecFromInputFile`` (source/genFuncs.cpp:380-410).
+
+Workloads (no public dataset is involved; all inputs are seeded synthetic):
+
+* ``aging_const_101``: order-4 constant grid 101x101 on Ly=Lz=30 km, mu 32.04
+  GPa, rho 2.67 g/cm^3, sN 50 MPa, f0 0.6, v0 1e-6 m/s, a 0.010, b 0.015
+  above 12 km falling to 0.005 at 17 km, Dc 8 mm, vL 1e-9 m/s, free
+  surface / remote loading / symmetric fault, psi = f0 + N(0, 1e-4), RK32
+  with absolute tolerance 1e-7 over 200 simulated years.
+* ``slip_var_401``: the same friction profile on a 401x401 grid stretched
+  toward the fault and the surface (y/z coordinate files), slip law, Dc
+  lognormal per node (mean 8 mm, sigma_ln 0.2) supplied as ``inputDir/Dc``.
+"""
+import os
+import struct
+
+import numpy as np
+
+YEAR = 31557600.0
+VEC_FILE_CLASSID = 1211214
+
+
+def write_petsc_vec(path, vec):
+    vec = np.asarray(vec, dtype=np.float64)
+    with open(path, "wb") as f:
+        f.write(struct.pack(">ii", VEC_FILE_CLASSID, vec.size))
+        f.write(vec.astype(">f8").tobytes())
+
+
+_COMMON = """\
+# seeded synthetic quasi-dynamic strike-slip problem
+order = {order}
+Ny = {Ny}
+Nz = {Nz}
+Ly = {Ly}
+Lz = {Lz}
+vL = 1e-9
+gridSpacingType = {grid}
+inputDir = {inputDir}
+outputDir = {outputDir}
+bulkDeformationType = linearElastic
+momentumBalanceType = quasidynamic
+stateLaw = {stateLaw}
+f0 = 0.6
+v0 = 1e-6
+DcVals = [0.008 0.008]
+DcDepths = [0 {Lz}]
+aVals = [0.010 0.010]
+aDepths = [0 {Lz}]
+bVals = [0.015 0.015 0.005 0.005]
+bDepths = [0 12 17 {Lz}]
+sNVals = [50 50]
+sNDepths = [0 {Lz}]
+muVals = [32.04 32.04]
+muDepths = [0 {Lz}]
+rhoVals = [2.67 2.67]
+rhoDepths = [0 {Lz}]
+timeIntegrator = {integrator}
+timeControlType = PID
+stride1D = 0
+stride2D = 0
+maxStepCount = {maxStepCount}
+initTime = 0
+maxTime = {maxTime}
+initDeltaT = {initDeltaT}
+timeStepTol = {tol}
+timeIntInds = [psi slip]
+"""
+
+
+def tanh_stretch(n, L, beta):
+    """Coordinates 0..L clustered at 0: L*(1 - tanh(beta*(1-q))/tanh(beta))."""
+    q = np.arange(n) / (n - 1.0)
+    return L * (1.0 - np.tanh(beta * (1.0 - q)) / np.tanh(beta))
+
+
+def make_qd_problem(workdir, Ny=101, Nz=101, Ly=30.0, Lz=30.0, order=4, seed=0,
+                    grid="constantGridSpacing", state_law="agingLaw", integrator="RK32",
+                    tol=1e-7, years=200.0, max_steps=100000000, init_dt=1e-3,
+                    stretch_beta=None, dc_lognormal=False, name="qd"):
+    """Write ``<workdir>/<name>.in`` and its inputDir fields; return the .in path."""
+    os.makedirs(workdir, exist_ok=True)
+    rng = np.random.default_rng(seed)
+    input_dir = os.path.join(workdir, name + "_in_")
+    out_dir = os.path.join(workdir, name + "_out_")
+    text = _COMMON.format(order=order, Ny=Ny, Nz=Nz, Ly=repr(float(Ly)), Lz=repr(float(Lz)), grid=grid,
+                          inputDir=input_dir, outputDir=out_dir, stateLaw=state_law,
+                          integrator=integrator, maxStepCount=int(max_steps),
+                          maxTime=repr(float(years * YEAR)), initDeltaT=repr(float(init_dt)), tol=repr(float(tol)))
+    psi = 0.6 + rng.normal(0.0, 1e-4, size=Nz)
+    write_petsc_vec(input_dir + "psi", psi)
+    if stretch_beta is not None:
+        yv = tanh_stretch(Ny, Ly, stretch_beta)
+        zv = tanh_stretch(Nz, Lz, stretch_beta)
+        write_petsc_vec(input_dir + "y", np.repeat(yv, Nz))
+        write_petsc_vec(input_dir + "z", np.tile(zv, Ny))
+    if dc_lognormal:
+        sig = 0.2
+        mu_ln = np.log(0.008) - 0.5 * sig * sig
+        write_petsc_vec(input_dir + "Dc", np.exp(rng.normal(mu_ln, sig, size=Nz)))
+    path = os.path.join(workdir, name + ".in")
+    with open(path, "w") as f:
+        f.write(text)
+    return path
+
+
+def aging_const_101(workdir, seed=0, **kw):
+    args = dict(Ny=101, Nz=101, seed=seed, name="aging_const_101")
+    args.update(kw)
+    return make_qd_problem(workdir, **args)
+
+
+def slip_var_401(workdir, seed=0, **kw):
+    args = dict(Ny=401, Nz=401, seed=seed, grid="variableGridSpacing", state_law="slipLaw",
+                stretch_beta=2.0, dc_lognormal=True, name="slip_var_401")
+    args.update(kw)
+    return make_qd_problem(workdir, **args)

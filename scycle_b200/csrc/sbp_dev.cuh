@@ -1,0 +1,283 @@
+// Matrix-free SBP-SAT operator on the device.
+//
+// A = H*(Dyy^mu + Dzz^mu) + SAT_L + SAT_R + SAT_T + SAT_B, applied as two
+// banded stages per direction:
+//   stage 1 (at row k):  g1 = c_k (D x)_k,  g3 = w3_k m3_k (R3 x)_k,  g4 = w4_k c_k (R4 x)_k
+//   stage 2 (at row i):  (A x)_i = w_i [ (Q g1)_i - (R3^T g3)_i - (R4^T g4)_i ] + SAT_i
+// with Q = H_d*D, (R3, R4) = (D3, D4) for order 4 or (D2, 0) for order 2,
+// c = mu (constant grid) or mu*qy / mu*rz (curvilinear grid), m3 the
+// flattened-index average of c, w = Hz*zr (y part) or Hy*yq (z part).  This is
+// the product the reference assembles as a sparse matrix in
+// SbpOps_m_constGrid::constructA / SbpOps_m_varGrid::constructA.
+#pragma once
+#include "common.cuh"
+
+namespace scy {
+
+constexpr int BAND = 9;  // coefficients per row, column offsets -4..+4
+constexpr int HALF = 4;
+constexpr int TY = 8;    // tile rows (y, slow index)
+constexpr int TZ = 32;   // tile columns (z, fast index: one warp per row)
+constexpr int HX = 8;    // x halo: stage-2 reach + stage-1 reach
+constexpr int HG = 4;    // stage-1 result halo: stage-2 reach
+
+template <typename T>
+struct DirDev {
+  int n;
+  const T *D, *R3, *R4, *Q, *R3T, *R4T;  // banded n*9
+  const T *w3, *w4, *Hd, *Hinvd;         // n
+  T bs0[BAND], bsN[BAND];
+  T alphaD;
+  int bc_lo, bc_hi;  // 0 Dirichlet, 1 Neumann (y: lo=L, hi=R; z: lo=T, hi=B)
+};
+
+template <typename T>
+struct LevelDev {
+  int Ny, Nz, var;
+  DirDev<T> y, z;
+  const T *cy, *cz, *m3y, *m3z, *wy, *wz, *mu, *qy, *rz, *dinv;
+};
+
+// -------------------------------------------------------------------------
+// Loaders: the value of the operand at an in-domain node.
+template <typename T>
+struct LoadPlain {
+  const T* x;
+  __device__ __forceinline__ T operator()(long node, int, int) const { return x[node]; }
+};
+
+// p = z + beta*p_old (beta = rz_new/rz_old read from device scalars, or p = z
+// on the first iteration).
+template <typename Tz>
+struct LoadPUpdate {
+  const Tz* z;
+  const double* pold;
+  const double* rz_new;
+  const double* rz_old;
+  int first;
+  __device__ __forceinline__ double operator()(long node, int, int) const {
+    double zv = (double)z[node];
+    if (first) return zv;
+    double beta = *rz_new / *rz_old;
+    return zv + beta * pold[node];
+  }
+};
+
+// x + P*xc: coarse-grid correction folded into the load.
+template <typename T>
+struct LoadProlong {
+  const T* x;
+  const T* xc;
+  int Ncz;
+  const int *jy, *jz;
+  const T *wy0, *wy1, *wz0, *wz1;
+  __device__ __forceinline__ T operator()(long node, int iy, int iz) const {
+    int a = jy[iy], b = jz[iz];
+    const T* c0 = xc + (long)a * Ncz + b;
+    const T* c1 = c0 + Ncz;
+    T v = wy0[iy] * (wz0[iz] * c0[0] + wz1[iz] * c0[1]) + wy1[iy] * (wz0[iz] * c1[0] + wz1[iz] * c1[1]);
+    return (x ? x[node] : T(0)) + v;
+  }
+};
+
+// -------------------------------------------------------------------------
+// Epilogues: consume (A x)_node and the operand value x_node; return a
+// contribution to the optional block/grid sum.
+template <typename T>
+struct EpiStore {
+  T* out;
+  T scale;
+  static constexpr bool kReduce = false;
+  __device__ __forceinline__ double operator()(long node, T Ax, T) const {
+    out[node] = scale * Ax;
+    return 0.0;
+  }
+};
+
+// r = f - K x with K = -A and f = sign_f * b  ->  r = sign_f*b + A x; returns r.r
+template <typename T, typename Tb>
+struct EpiResidual {
+  const Tb* b;
+  T* r;
+  T sign_b;
+  static constexpr bool kReduce = true;
+  __device__ __forceinline__ double operator()(long node, T Ax, T) const {
+    T v = sign_b * (T)b[node] + Ax;
+    r[node] = v;
+    return (double)v * (double)v;
+  }
+};
+
+// CG: q = K p = -A p, store p; returns p.q
+struct EpiCGMatvec {
+  double* pnew;
+  double* q;
+  static constexpr bool kReduce = true;
+  __device__ __forceinline__ double operator()(long node, double Ax, double p) const {
+    double qv = -Ax;
+    pnew[node] = p;
+    q[node] = qv;
+    return p * qv;
+  }
+};
+
+// Chebyshev-Jacobi step: res = b - K x = b + A x; d = c1*d + c2*dinv*res; xout = x + d
+template <typename T>
+struct EpiCheb {
+  const T* b;
+  const T* dinv;
+  T* d;
+  T* xout;
+  T c1, c2;
+  static constexpr bool kReduce = false;
+  __device__ __forceinline__ double operator()(long node, T Ax, T xv) const {
+    T res = b[node] + Ax;
+    T dv = c2 * dinv[node] * res;
+    if (c1 != T(0)) dv += c1 * d[node];
+    d[node] = dv;
+    xout[node] = xv + dv;
+    return 0.0;
+  }
+};
+
+// -------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T band_dot(const T* __restrict__ row, const T* s, int stride) {
+  T acc = T(0);
+#pragma unroll
+  for (int j = 0; j < BAND; ++j) acc += row[j] * s[j * stride];
+  return acc;
+}
+
+// One 8x32 tile of outputs per block; 256 threads.
+template <typename T, class Loader, class Epi>
+__global__ void __launch_bounds__(256) stencil_kernel(LevelDev<T> L, Loader ld, Epi ep, double* partials,
+                                                      unsigned int* counter, double* red_out) {
+  __shared__ T xs_y[(TY + 2 * HX) * TZ];
+  __shared__ T xs_z[TY * (TZ + 2 * HX)];
+  __shared__ T gy[3][(TY + 2 * HG) * TZ];
+  __shared__ T gz[3][TY * (TZ + 2 * HG)];
+  __shared__ double red[32];
+  const int Ny = L.Ny, Nz = L.Nz;
+  const int y0 = blockIdx.y * TY, z0 = blockIdx.x * TZ;
+  const int tid = threadIdx.x;
+
+  for (int i = tid; i < (TY + 2 * HX) * TZ; i += blockDim.x) {
+    int r = i / TZ, c = i % TZ;
+    int iy = y0 - HX + r, iz = z0 + c;
+    T v = T(0);
+    if (iy >= 0 && iy < Ny && iz < Nz) v = ld((long)iy * Nz + iz, iy, iz);
+    xs_y[i] = v;
+  }
+  for (int i = tid; i < TY * (TZ + 2 * HX); i += blockDim.x) {
+    int r = i / (TZ + 2 * HX), c = i % (TZ + 2 * HX);
+    int iy = y0 + r, iz = z0 - HX + c;
+    T v = T(0);
+    if (iy < Ny && iz >= 0 && iz < Nz) v = ld((long)iy * Nz + iz, iy, iz);
+    xs_z[i] = v;
+  }
+  __syncthreads();
+  // stage 1, y direction: rows y0-HG .. y0+TY+HG
+  for (int i = tid; i < (TY + 2 * HG) * TZ; i += blockDim.x) {
+    int r = i / TZ, c = i % TZ;
+    int k = y0 - HG + r, iz = z0 + c;
+    T g1 = T(0), g3 = T(0), g4 = T(0);
+    if (k >= 0 && k < Ny && iz < Nz) {
+      const T* xcol = xs_y + r * TZ + c;  // row k-4 of xs_y sits at (r + HX - HG - HALF) = r
+      long node = (long)k * Nz + iz;
+      T cyv = L.cy[node];
+      g1 = cyv * band_dot(L.y.D + (long)k * BAND, xcol, TZ);
+      g3 = L.y.w3[k] * L.m3y[node] * band_dot(L.y.R3 + (long)k * BAND, xcol, TZ);
+      if (L.y.R4) g4 = L.y.w4[k] * cyv * band_dot(L.y.R4 + (long)k * BAND, xcol, TZ);
+    }
+    gy[0][i] = g1;
+    gy[1][i] = g3;
+    gy[2][i] = g4;
+  }
+  // stage 1, z direction: columns z0-HG .. z0+TZ+HG
+  for (int i = tid; i < TY * (TZ + 2 * HG); i += blockDim.x) {
+    int r = i / (TZ + 2 * HG), c = i % (TZ + 2 * HG);
+    int iy = y0 + r, k = z0 - HG + c;
+    T g1 = T(0), g3 = T(0), g4 = T(0);
+    if (iy < Ny && k >= 0 && k < Nz) {
+      const T* xrow = xs_z + r * (TZ + 2 * HX) + c;  // column k-4 sits at c
+      long node = (long)iy * Nz + k;
+      T czv = L.cz[node];
+      g1 = czv * band_dot(L.z.D + (long)k * BAND, xrow, 1);
+      g3 = L.z.w3[k] * L.m3z[node] * band_dot(L.z.R3 + (long)k * BAND, xrow, 1);
+      if (L.z.R4) g4 = L.z.w4[k] * czv * band_dot(L.z.R4 + (long)k * BAND, xrow, 1);
+    }
+    gz[0][i] = g1;
+    gz[1][i] = g3;
+    gz[2][i] = g4;
+  }
+  __syncthreads();
+  const int ty = tid / TZ, tz = tid % TZ;
+  const int iy = y0 + ty, iz = z0 + tz;
+  double contrib = 0.0;
+  if (iy < Ny && iz < Nz) {
+    const long node = (long)iy * Nz + iz;
+    // y part: g rows iy-4..iy+4 sit at gy rows ty..ty+8
+    const T* qrow = L.y.Q + (long)iy * BAND;
+    const T* r3 = L.y.R3T + (long)iy * BAND;
+    const T* r4 = L.y.R4T + (long)iy * BAND;
+    T sy = T(0);
+#pragma unroll
+    for (int j = 0; j < BAND; ++j) {
+      int gi = (ty + j) * TZ + tz;
+      sy += qrow[j] * gy[0][gi] - r3[j] * gy[1][gi];
+      if (L.y.R4T) sy -= r4[j] * gy[2][gi];
+    }
+    const int gcen_y = (ty + HG) * TZ + tz;
+    // SAT on the y = 0 (L) and y = Ly (R) boundaries
+    if (L.y.bc_lo == 0) {
+      if (iy < BAND) sy += (L.y.bs0[iy] + (iy == 0 ? L.y.alphaD : T(0))) * L.cy[iz] * xs_y[(0 - y0 + HX) * TZ + tz];
+    } else if (iy == 0) {
+      sy += gy[0][gcen_y];
+    }
+    if (L.y.bc_hi == 0) {
+      if (iy >= Ny - BAND) {
+        long bn = (long)(Ny - 1) * Nz + iz;
+        int rr = Ny - 1 - y0 + HX;  // row of xs_y holding iy = Ny-1 (inside the tile halo)
+        sy += (L.y.bsN[iy - (Ny - BAND)] + (iy == Ny - 1 ? L.y.alphaD : T(0))) * L.cy[bn] * xs_y[rr * TZ + tz];
+      }
+    } else if (iy == Ny - 1) {
+      sy -= gy[0][gcen_y];
+    }
+    // z part: g columns iz-4..iz+4 sit at gz columns tz..tz+8
+    const T* qz = L.z.Q + (long)iz * BAND;
+    const T* z3 = L.z.R3T + (long)iz * BAND;
+    const T* z4 = L.z.R4T + (long)iz * BAND;
+    T sz = T(0);
+#pragma unroll
+    for (int j = 0; j < BAND; ++j) {
+      int gi = ty * (TZ + 2 * HG) + tz + j;
+      sz += qz[j] * gz[0][gi] - z3[j] * gz[1][gi];
+      if (L.z.R4T) sz -= z4[j] * gz[2][gi];
+    }
+    const int gcen_z = ty * (TZ + 2 * HG) + tz + HG;
+    if (L.z.bc_lo == 0) {
+      if (iz < BAND) sz += (L.z.bs0[iz] + (iz == 0 ? L.z.alphaD : T(0))) * L.cz[(long)iy * Nz] * xs_z[ty * (TZ + 2 * HX) + (0 - z0 + HX)];
+    } else if (iz == 0) {
+      sz += gz[0][gcen_z];
+    }
+    if (L.z.bc_hi == 0) {
+      if (iz >= Nz - BAND) {
+        long bn = (long)iy * Nz + Nz - 1;
+        int cc = Nz - 1 - z0 + HX;
+        sz += (L.z.bsN[iz - (Nz - BAND)] + (iz == Nz - 1 ? L.z.alphaD : T(0))) * L.cz[bn] * xs_z[ty * (TZ + 2 * HX) + cc];
+      }
+    } else if (iz == Nz - 1) {
+      sz -= gz[0][gcen_z];
+    }
+    T Ax = L.wy[node] * sy + L.wz[node] * sz;
+    T xv = xs_y[(ty + HX) * TZ + tz];
+    contrib = ep(node, Ax, xv);
+  }
+  if constexpr (Epi::kReduce) {
+    double tot = block_sum(contrib, red);
+    grid_reduce_finish(tot, partials, counter, red_out, red);
+  }
+}
+
+}  // namespace scy

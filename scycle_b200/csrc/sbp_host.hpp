@@ -1,0 +1,84 @@
+// Host-side construction of the 1D SBP operators and the per-level
+// coefficient fields used by the matrix-free device stencil.
+#pragma once
+#include <map>
+#include <string>
+#include <vector>
+
+namespace scy {
+
+// Sparse 1D matrix (row -> col -> value), the same shape of container the
+// reference builds its 1D operators in (source/spmat.hpp:18-75).
+struct Sparse1D {
+  int n = 0;
+  std::vector<std::map<int, double>> rows;
+  explicit Sparse1D(int n_ = 0) : n(n_), rows(n_) {}
+  void set(int r, int c, double v) { rows[r][c] = v; }
+  double get(int r, int c) const {
+    auto it = rows[r].find(c);
+    return it == rows[r].end() ? 0.0 : it->second;
+  }
+  Sparse1D transpose() const;
+};
+
+// All 1D operators of one direction (spmat.cpp:310-627).
+struct Ops1D {
+  int order = 4, n = 0;
+  double scale = 1.0;            // 1/h
+  std::vector<double> H, Hinv;   // diagonals
+  Sparse1D D1, BS;               // first derivative and boundary derivative
+  Sparse1D D3, D4, D2;           // R-term difference operators (unscaled D3/D4; D2 scaled)
+  std::vector<double> C3, C4, C2;
+};
+
+// Builds the operators; throws std::invalid_argument on an unsupported size/order.
+Ops1D build_ops1d(int order, int n, double scale, int compat /*0 fully,1 compatible*/);
+
+// Centred band: 9 coefficients per row at column offsets -4..+4.
+constexpr int kBand = 9;
+constexpr int kHalf = 4;
+std::vector<double> to_band(const Sparse1D& m);  // throws if a row reaches beyond +-4
+
+// Per-direction tables in the order the device kernel consumes them.
+struct DirTables {
+  int n = 0;
+  int nterms = 3;                // 3 (order 4: D, D3, D4) or 2 (order 2: D, D2)
+  std::vector<double> D, R3, R4; // stage 1 (applied to x), banded n*9
+  std::vector<double> Q, R3T, R4T; // stage 2 (applied to the stage-1 results), banded
+  std::vector<double> w3, w4;    // per-row weights of the R terms
+  std::vector<double> Hd, Hinvd; // H diagonal and its inverse
+  double bs0[kBand];             // BS row 0, columns 0..8
+  double bsN[kBand];             // BS row n-1, columns n-9..n-1
+  double alphaD = 0.0;           // Dirichlet penalty
+};
+DirTables build_dir_tables(int order, int n, double h, int compat);
+
+// One grid of the hierarchy: sizes, tables and per-node coefficient fields.
+struct LevelHost {
+  int order = 4, Ny = 0, Nz = 0, grid_type = 0, compat = 0;
+  double Ly = 1, Lz = 1, dy = 1, dz = 1;
+  int bc[4] = {0, 1, 0, 1};      // R, T, L, B
+  DirTables ty, tz;
+  // fields, length Ny*Nz
+  std::vector<double> mu, cy, cz, m3y, m3z, wy, wz, yq, zr, qy, rz;
+  std::vector<double> diagK;     // diagonal of K = -A
+  double lambda_max = 0.0;       // spectral bound of diag(K)^-1 K (power iteration)
+  void apply_A(const double* x, double* out) const;  // host reference of the device stencil
+  void compute_diag();
+};
+
+// Builds a level from grid data; y/z may be empty (-> q*Ly, r*Lz).
+LevelHost build_level(int order, int Ny, int Nz, double Ly, double Lz, int grid_type, int compat,
+                      const std::vector<double>& y, const std::vector<double>& z,
+                      const std::vector<double>& mu, const int bc[4]);
+
+// 1D linear interpolation from a coarse logical grid of nc points onto a fine
+// one of nf points: fine i = w0*coarse[j0] + w1*coarse[j0+1].
+struct Interp1D {
+  int nf = 0, nc = 0;
+  std::vector<int> j0;
+  std::vector<double> w0, w1;
+};
+Interp1D make_interp(int nf, int nc);
+
+}  // namespace scy

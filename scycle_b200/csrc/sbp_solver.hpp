@@ -1,0 +1,121 @@
+// Device-side SbpOps context and the multigrid-preconditioned CG solver.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <type_traits>
+#include <vector>
+
+#include "sbp_dev.cuh"
+#include "sbp_host.hpp"
+
+namespace scy {
+
+const char* last_error();
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept : p(o.p), bytes(o.bytes) {
+    o.p = nullptr;
+    o.bytes = 0;
+  }
+  DevBuf& operator=(DevBuf&& o) noexcept {
+    if (this != &o) {
+      release();
+      p = o.p;
+      bytes = o.bytes;
+      o.p = nullptr;
+      o.bytes = 0;
+    }
+    return *this;
+  }
+  ~DevBuf();
+  int alloc(size_t b);
+  void release();
+  template <typename T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+};
+
+// Partial sums for the deterministic grid reductions.
+struct Reducer {
+  DevBuf partials, counter;
+  int init(int max_blocks);
+};
+
+template <typename T>
+struct LevelStore {
+  int Ny = 0, Nz = 0;
+  DevBuf tab[2][10];  // per direction: D, R3, R4, Q, R3T, R4T, w3, w4, Hd, Hinvd
+  DevBuf fld[10];     // cy, cz, m3y, m3z, wy, wz, mu, qy, rz, dinv
+  LevelDev<T> dev{};
+  int init(const LevelHost& h, cudaStream_t s);
+};
+
+struct Transfer {
+  Interp1D iy, iz;
+  std::vector<int> ylo, yhi, zlo, zhi;  // fine index range feeding each coarse index
+};
+
+struct TransferDev {
+  DevBuf jy, wy0, wy1, jz, wz0, wz1, ylo, yhi, zlo, zhi;
+};
+
+struct ChebCoef {
+  double c1, c2;
+};
+
+template <typename T>
+struct Multigrid {
+  struct Work {
+    DevBuf v[5];  // x ping, x pong, d, b, r
+  };
+  int nlev = 0, nu = 2, ncoarse = 0;
+  std::vector<std::unique_ptr<LevelStore<T>>> lev;
+  std::vector<Work> work;
+  std::vector<TransferDev> tr;
+  std::vector<std::vector<ChebCoef>> cheb;
+  std::vector<double> lambda;
+  DevBuf coarse_inv;
+  int init(const std::vector<LevelHost>& hosts, const std::vector<Transfer>& xfer, cudaStream_t s);
+  int setup_smoothers(const std::vector<LevelHost>& hosts, Reducer& red, double* dscal, cudaStream_t s);
+  template <typename Tin>
+  int vcycle(int l, const Tin* b_in, T** x_out, cudaStream_t s);
+};
+
+int build_hierarchy(const scy_grid_desc& g, const std::vector<double>& y, const std::vector<double>& z,
+                    const std::vector<double>& mu, const int bc[4], std::vector<LevelHost>& hosts,
+                    std::vector<Transfer>& xfer);
+
+struct SbpContext {
+  scy_grid_desc desc{};
+  std::vector<double> y, z, mu;
+  int bc[4] = {0, 1, 0, 1};  // R, T, L, B
+  cudaStream_t stream = nullptr;
+  std::vector<LevelHost> hosts;
+  std::vector<Transfer> xfer;
+  std::unique_ptr<LevelStore<double>> fine;
+  std::unique_ptr<Multigrid<double>> mg64;
+  std::unique_ptr<Multigrid<float>> mg32;
+  Reducer red;
+  DevBuf scal;
+  DevBuf cg_r, cg_p[2], cg_q, cg_z;
+
+  int create(const scy_grid_desc& g);
+  int rebuild();
+  int apply(int op, const double* in, double* out);
+  int set_rhs(const double* bcL, const double* bcR, const double* bcT, const double* bcB, double* rhs);
+  int solve(const double* rhs, double* u, const scy_solve_opts& o, scy_solve_stats& st);
+  int change_bc(int R, int T, int L, int B);
+  template <typename T>
+  int ensure_mg(std::unique_ptr<Multigrid<T>>& mg);
+  template <typename T>
+  int pcg(Multigrid<T>& mg, const double* rhs, double* u, const scy_solve_opts& o, scy_solve_stats& st);
+};
+
+}  // namespace scy
