@@ -1,0 +1,323 @@
+"""Benchmark of the quasi-dynamic time-step path on B200.
+
+Workload: the 401x401 linear-elastic quasi-dynamic strike-slip problem on a
+grid stretched toward the fault and the surface, slip law, per-node
+lognormal Dc (seeded synthetic inputs written in the reference's .in format,
+loaded by the library's C++ reader), started from the reference's
+steady-state initial guess and integrated with adaptive RK32.
+
+A step is one accepted RK32 time step (its stage d_dt evaluations, each an
+elliptic solve + fault update, plus rejected attempts).  ``value`` is whole-
+job stage-solves per second (one stage-solve = one d_dt evaluation);
+``sim_years_per_hour`` is reported beside it over the same window.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun (N > 1) every rank integrates its own replica (weak scaling,
+no data-path collective); the timed region is bracketed by barriers and the
+reported time is the max over ranks.
+"""
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "sim-years/hour & stage-solves/s: mixed+batched vs FP64 GPU, V err<=1e-6"
+YEAR = 31557600.0
+WORKLOAD = ("slip_var_401: linear-elastic quasi-dynamic, 401x401 SBP order 4 on a tanh-stretched grid "
+            "(beta 2) over 30x30 km, slip law, lognormal Dc (mean 8 mm, sigma_ln 0.2), RK32 tol 1e-7, "
+            "steady-state initial guess")
+
+
+def _peaks():
+    try:
+        return json.load(open(os.path.join(HERE, "MEASURED_PEAKS.json")))
+    except Exception:
+        return {}
+
+
+class Clocks:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+
+    def __init__(self, gpu_index=0):
+        self.proc = None
+        self.path = os.path.join(tempfile.gettempdir(), "scy_clocks_%d.csv" % os.getpid())
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(gpu_index), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world <= 1:
+        return None, 0, 1, 0
+    import torch.distributed as dist
+    import datetime
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return dist, rank, world, local
+
+
+def _max_over_ranks(dist, v):
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _sum_over_ranks(dist, v):
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def make_workload(workdir, n=401, seed=0):
+    from scycle_b200.configs import slip_var_401
+    return slip_var_401(workdir, seed=seed, Ny=n, Nz=n, years=1.0e4)
+
+
+# ---------------------------------------------------------------------------
+def run_ours(args, dist, rank, world, local):
+    import torch
+    torch.cuda.set_device(local)
+    from scycle_b200 import build
+    build.build(verbose=False)
+    from scycle_b200 import _lib as S
+    from scycle_b200.qd import QD
+    L = S.lib()
+    work = tempfile.mkdtemp(prefix="scy_bench_")
+    path = make_workload(work, n=args.n, seed=rank)
+    prec = "mixed" if args.precision == "mixed" else "fp64"
+    q = QD.from_in(path, solve_rtol=args.rtol, precision=prec, check_every=args.check_every)
+    q.integrate_begin_from_in()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")  # > 126 MB L2
+
+    def steps(k, e2e=False, hostbuf=None):
+        for _ in range(k):
+            if e2e:
+                S.check(L.scy_qd_set_state(q.h, S.as_dptr(hostbuf["var"]), 0))
+            st = q.integrate_steps(1)
+            if e2e:
+                for nm, arr in (("psi", hostbuf["psi"]), ("slip", hostbuf["slip"]), ("slipVel", hostbuf["vel"])):
+                    S.check(L.scy_qd_get_field(q.h, {"psi": 0, "slip": 1, "slipVel": 2}[nm], S.as_dptr(arr)))
+                hostbuf["var"][:q.Nz] = hostbuf["psi"]
+                hostbuf["var"][q.Nz:] = hostbuf["slip"]
+            flush.zero_()
+        return st
+
+    st0 = steps(args.warmup)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks = Clocks(local) if rank == 0 else None
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = L.scy_launch_count()
+    t_sim0, n0 = st0.t, st0.d_dt_evals
+    ev0.record()
+    st1 = steps(args.steps)
+    ev1.record()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    launches = L.scy_launch_count() - launches0
+    clk = clocks.stop() if clocks else None
+    ms = ev0.elapsed_time(ev1)
+    ms_max = _max_over_ranks(dist, ms)
+    evals = st1.d_dt_evals - n0
+    sim_s = st1.t - t_sim0
+    total_evals = _sum_over_ranks(dist, evals)
+    total_sim_years = _sum_over_ranks(dist, sim_s / YEAR)
+    value = total_evals / (ms_max / 1e3)
+    syph = total_sim_years / (ms_max / 3.6e6)
+    solve_its = (st1.solve_its - st0.solve_its) / max(st1.solves - st0.solves, 1)
+
+    # end to end through the C ABI with host buffers (pinned): the state goes
+    # host -> device before and device -> host after every step
+    Nz = q.Nz
+    pin = lambda n: torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    hb = {"var": pin(2 * Nz), "psi": pin(Nz), "slip": pin(Nz), "vel": pin(Nz)}
+    S.check(L.scy_qd_get_field(q.h, 0, S.as_dptr(hb["psi"])))
+    S.check(L.scy_qd_get_field(q.h, 1, S.as_dptr(hb["slip"])))
+    hb["var"][:Nz], hb["var"][Nz:] = hb["psi"], hb["slip"]
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e0 = q.integrate_steps(0)
+    t0 = time.perf_counter()
+    ev0.record()
+    e1 = steps(args.steps, e2e=True, hostbuf=hb)
+    ev1.record()
+    torch.cuda.synchronize()
+    e_ms = _max_over_ranks(dist, ev0.elapsed_time(ev1))
+    e_evals = _sum_over_ranks(dist, e1.d_dt_evals - e0.d_dt_evals)
+    e2e = {"value": e_evals / (e_ms / 1e3), "unit": "stage-solves/s", "h2d_bytes_per_step": 2 * Nz * 8,
+           "d2h_bytes_per_step": 3 * Nz * 8, "sim_years_per_hour": None,
+           "wall_s": time.perf_counter() - t0}
+
+    # stencil kernel timing pass (CUDA events around each launch)
+    S.check(L.scy_profile_enable(1))
+    steps(min(args.steps, 20))
+    torch.cuda.synchronize()
+    S.check(L.scy_profile_enable(0))
+    pm, pl, pb = C.c_double(), C.c_longlong(), C.c_double()
+    width = 4 if prec == "mixed" else 8
+    S.check(L.scy_profile_collect(0, width, C.byref(pm), C.byref(pl), C.byref(pb)))
+    achieved = (pb.value / pl.value) / (pm.value / pl.value / 1e3) / 1e9 if pl.value else None
+    peaks = _peaks()
+    peak = peaks.get("hbm_gbs")
+    peak_src = "measured"
+    if peak is None:
+        peak, peak_src = 6650.0, "fallback"
+    roofline = {"kernel": "stencil_kernel (level-0 %s Chebyshev/residual launches)" % ("fp32" if width == 4 else "fp64"),
+                "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None, "peak_source": peak_src,
+                "traffic": None, "launch_us": (pm.value / pl.value * 1e3) if pl.value else None,
+                "algorithmic_bytes_per_launch": (pb.value / pl.value) if pl.value else None,
+                "note": "level-0 fields (0.64 MB per fp32 field) are L2-resident; DRAM traffic per launch is "
+                        "far below the algorithmic bytes, so this kernel is latency/L2 bound"}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(path, args)
+    out = {"metric": METRIC, "value": value, "unit": "stage-solves/s", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64 (%s elliptic preconditioner)" % ("fp32" if prec == "mixed" else "fp64"),
+           "data": "synthetic (seeded; reference .in format)",
+           "config": {"workload": WORKLOAD, "Ny": args.n, "Nz": args.n, "integrator": "RK32",
+                      "solver": "PCG + geometric multigrid (%s V-cycle), rtol %g" % (prec, args.rtol),
+                      "l2": "flushed between steps (256 MB write)", "parallelism": "replicas x%d" % world},
+           "sim_years_per_hour": syph, "sim_years_timed": total_sim_years,
+           "stage_solves": total_evals, "cg_iterations_per_solve": solve_its,
+           "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "gpu_launches": int(launches),
+           "clocks": clk}
+    if rank == 0:
+        print(json.dumps(out))
+    q.close()
+
+
+def cpu_baseline(path, args, max_evals=None):
+    """The oracle (SciPy SuperLU direct solve + restated fault / RK32) on the
+    host cores, on a bounded sample of the same workload."""
+    from oracle.problem import build_qd_problem
+    from oracle.qd import QDLinearElastic
+    t0 = time.perf_counter()
+    P = build_qd_problem(open(path).read())
+    ora = QDLinearElastic(P, keep_history=False)
+    setup = time.perf_counter() - t0
+    steps = args.cpu_steps
+    t1 = time.perf_counter()
+    rk = ora.integrate(max_steps=steps)
+    el = time.perf_counter() - t1
+    evals = rk.stage_evals
+    return {"value": evals / el, "unit": "stage-solves/s", "cores": 1, "kind": "port",
+            "sample": "%d RK32 steps (%d stage-solves) of the same workload after a %.1f s SuperLU factorisation; "
+                      "SuperLU and the restated root finder are single-threaded" % (steps, evals, setup),
+            "sim_years_per_hour": (rk.currT - P["driver"]["initTime"]) / YEAR / (el / 3600.0)}
+
+
+def run_reference(args, dist, rank, world, local):
+    if rank != 0:
+        return
+    work = tempfile.mkdtemp(prefix="scy_ref_")
+    path = make_workload(work, n=args.n, seed=0)
+    from oracle.problem import build_qd_problem
+    from oracle.qd import QDLinearElastic
+    P = build_qd_problem(open(path).read())
+    ora = QDLinearElastic(P, keep_history=False)
+    k = min(args.steps, args.cpu_steps)
+    w = min(args.warmup, 1)
+    t0 = time.perf_counter()
+    rk = ora.integrate(max_steps=w + k)
+    el = time.perf_counter() - t0
+    evals = rk.stage_evals
+    value = evals / el
+    out = {"impl": "reference", "metric": METRIC, "value": value, "unit": "stage-solves/s", "n_gpus": 1,
+           "steps": k, "warmup": w, "ms_per_step": el * 1e3 / (w + k), "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded; reference .in format)",
+           "config": {"workload": WORKLOAD, "Ny": args.n, "Nz": args.n, "integrator": "RK32",
+                      "solver": "SciPy SuperLU direct (stands in for the reference's MUMPS Cholesky)"},
+           "cpu_baseline": {"value": value, "unit": "stage-solves/s", "cores": 1, "kind": "port",
+                            "sample": "%d RK32 steps (%d stage-solves, factorisation excluded)" % (w + k, evals)},
+           "e2e": {"value": value, "unit": "stage-solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=401)
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--rtol", type=float, default=1e-12)
+    ap.add_argument("--check-every", type=int, default=1)
+    ap.add_argument("--cpu-steps", type=int, default=4)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    dist, rank, world, local = _dist()
+    try:
+        if args.impl == "reference":
+            run_reference(args, dist, rank, world, local)
+        else:
+            run_ours(args, dist, rank, world, local)
+    finally:
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -43,6 +43,17 @@ enum { SCY_BC_DIRICHLET = 0, SCY_BC_NEUMANN = 1 };
 enum { SCY_GRID_CONST = 0, SCY_GRID_VAR = 1 };
 enum { SCY_COMPAT_FULLY = 0, SCY_COMPAT_COMPATIBLE = 1 };
 
+/* Number of kernels this library has launched in the process so far. */
+long long scy_launch_count(void);
+/* Brackets every launch of the SBP stencil kernel with CUDA events while on
+ * (adds host overhead: use it in a separate measurement pass). */
+scy_status scy_profile_enable(int on);
+/* Sums the recorded stencil launches of multigrid level `level` (-1: all)
+ * and value width `width` (4, 8; 0: both): total milliseconds, launch
+ * count and algorithmic bytes (operand + mu read, result written); clears
+ * the record. */
+scy_status scy_profile_collect(int level, int width, double* ms, long long* launches, double* bytes);
+
 /* Returns the message of the last failed call on this thread. */
 const char* scy_get_last_error(void);
 /* Library version string. */
@@ -136,6 +147,132 @@ scy_status scy_sbp_info(scy_sbp* s, int* Ny, int* Nz, int* n_levels);
  * machine.  in/out are host arrays of length Ny*Nz.  The solver never uses
  * it on the hot path. */
 scy_status scy_grid_host_apply(const scy_grid_desc* desc, const double* in, double* out);
+
+/* ------------------------------------------------------------------------
+ * Fault_qd + StrikeSlip_LinearElastic_qd (linear-elastic quasi-dynamic).
+ *
+ * scy_qd_d_dt replaces StrikeSlip_LinearElastic_qd::d_dt
+ * (source/strikeSlip_linearElastic_qd.cpp:756-798): boundary data from slip
+ * and time, setRHS + KSPSolve + muxDy (solveMomentumBalance :874-891), the
+ * body-to-fault scatter and Fault_qd::d_dt (source/fault.cpp:861-918) with
+ * ComputeVel_qd's bracketed Newton (fault.cpp:954-1059,
+ * rootFinder.cpp:174-257) and the aging / slip laws (fault.cpp:1984-2088).
+ * scy_qd_integrate_* replace RK32::integrate / RK43::integrate
+ * (source/odeSolver.cpp:505-627, :973-1175) with P / PID step control
+ * (:395-445, :846-898).
+ * ---------------------------------------------------------------------- */
+enum { SCY_LAW_AGING = 0, SCY_LAW_SLIP = 1, SCY_LAW_CONSTANT = 2 };
+
+typedef struct scy_fault_desc {
+  int Nz;
+  const double* a;         /* host, Nz: direct-effect parameter */
+  const double* b;         /* host, Nz: evolution-effect parameter */
+  const double* sN;        /* host, Nz: effective normal stress (MPa) */
+  const double* Dc;        /* host, Nz: state evolution distance (m) */
+  const double* eta;       /* host, Nz: radiation damping sqrt(mu rho)/faultTypeScale */
+  const double* locked;    /* host, Nz or NULL: >0.5 held at 0, <-0.5 creeps at vL */
+  const double* prestress; /* host, Nz or NULL */
+  double f0, v0, vL;
+  double root_tol;         /* absolute residual tolerance (MPa), reference default 1e-12 */
+  int max_its;             /* root iteration cap, reference default 1e4 */
+  int state_law;           /* SCY_LAW_* */
+} scy_fault_desc;
+
+typedef struct scy_qd_desc {
+  scy_grid_desc grid;
+  scy_fault_desc fault;
+  double fault_type_scale; /* 2 for symmFault, 1 for rigidFault */
+  int bcL_from_slip;       /* 1: bcL = slip/fault_type_scale (symmFault, rigidFault) */
+  int bcR_remote;          /* 1: bcR = vL*t/fault_type_scale + bcRShift (remoteLoading) */
+  double vL;               /* loading rate of the driver (m/s) */
+  const double* bcL0;      /* host, Nz or NULL: initial bcL (momBal_bcL) */
+  const double* bcRShift;  /* host, Nz or NULL (momBal_bcR) */
+  scy_solve_opts solve;    /* elliptic solve settings for every stage */
+} scy_qd_desc;
+
+typedef struct scy_qd scy_qd;
+
+scy_status scy_qd_create(const scy_qd_desc* desc, scy_qd** out);
+scy_status scy_qd_destroy(scy_qd* q);
+scy_status scy_qd_set_stream(scy_qd* q, void* cuda_stream);
+
+/* dvar = d_dt(t, var).  var = [psi | slip], dvar = [dpsi | dslip]: device,
+ * 2*Nz doubles each (psi first: the reference integrates a std::map, whose
+ * keys iterate in sorted order).  Updates the fault fields (slipVel, tauQS,
+ * tauP, strength) and the body displacement like the reference. */
+scy_status scy_qd_d_dt(scy_qd* q, double t, const double* var, double* dvar);
+
+enum { SCY_RK32 = 0, SCY_RK43 = 1 };
+enum { SCY_CTRL_P = 0, SCY_CTRL_PID = 1 };
+enum { SCY_NORM_L2_ABS = 0, SCY_NORM_L2_REL = 1 };
+enum { SCY_KEY_PSI = 0, SCY_KEY_SLIP = 1 };
+
+typedef struct scy_ode_opts {
+  int method;           /* SCY_RK32 / SCY_RK43 */
+  int control;          /* SCY_CTRL_P / SCY_CTRL_PID */
+  int norm;             /* SCY_NORM_L2_ABS / SCY_NORM_L2_REL */
+  double tol;           /* timeStepTol */
+  double min_dt, max_dt, init_dt;
+  double t0, t1;        /* initTime, maxTime */
+  long max_steps;       /* maxStepCount */
+  int n_err;            /* 0: all keys in sorted order with scale 1 */
+  int err_keys[2];      /* SCY_KEY_* in timeIntInds order */
+  double err_scale[2];  /* scale per key */
+} scy_ode_opts;
+
+typedef struct scy_ode_stats {
+  double t, dt, new_dt;
+  long step_count, rejected, d_dt_evals, solve_its, solves;
+  double errA[2];       /* errA[0] newest accepted error */
+  int done;             /* 1: reached t1 or max_steps */
+} scy_ode_stats;
+
+/* OdeSolver setInitialConds + the first d_dt.  var0 = [psi | slip] host. */
+scy_status scy_qd_integrate_begin(scy_qd* q, const scy_ode_opts* opts, const double* var0_host);
+/* Advances up to nsteps accepted steps (fewer at t1 / max_steps). */
+scy_status scy_qd_integrate_steps(scy_qd* q, long nsteps, scy_ode_stats* stats);
+/* Forces the step size and accept decision of the next n attempts. */
+scy_status scy_qd_force_attempts(scy_qd* q, const double* dts, const int* accept, long n);
+/* Starts (1) / stops (0) recording (dt, accept) of every attempt. */
+scy_status scy_qd_record_attempts(scy_qd* q, int on);
+/* Copies the recorded attempts; *n receives their number. */
+scy_status scy_qd_get_attempts(scy_qd* q, double* dts, int* accept, long cap, long* n);
+
+enum {
+  SCY_FIELD_PSI = 0, SCY_FIELD_SLIP = 1, SCY_FIELD_SLIPVEL = 2, SCY_FIELD_TAUP = 3,
+  SCY_FIELD_TAUQSP = 4, SCY_FIELD_STRENGTH = 5, SCY_FIELD_U = 6, SCY_FIELD_SURFDISP = 7,
+  SCY_FIELD_SXY = 8, SCY_FIELD_DPSI = 9, SCY_FIELD_DSLIP = 10
+};
+/* Copies a field to host memory (Nz, Ny or Ny*Nz doubles; see SCY_FIELD_*). */
+scy_status scy_qd_get_field(scy_qd* q, int field, double* host_out);
+
+/* Reads a StrikeSlip_LinearElastic_qd input file (the reference's .in
+ * format: Domain, LinearElastic, Fault and driver keys, inputDir
+ * PETSc-binary fields) and creates the driver (the reference's
+ * Domain(file) + StrikeSlip_LinearElastic_qd(D), source/main.cpp:227-233).
+ * `solve` sets the elliptic solver (NULL: FP64, rtol 1e-12). */
+scy_status scy_qd_create_from_in(const char* path, const scy_solve_opts* solve, scy_qd** out);
+/* Sizes and the integrator settings read from the input file (min_dt is the
+ * computeMinTimeStep value unless the file set minDeltaT). */
+scy_status scy_qd_get_problem(scy_qd* q, int* Ny, int* Nz, scy_ode_opts* ode);
+/* integrate()'s set-up for a driver made by scy_qd_create_from_in:
+ * initiateIntegrand (with the steady-state guess when the file asks for it,
+ * strikeSlip_linearElastic_qd.cpp:377-413) and the first d_dt. */
+scy_status scy_qd_integrate_begin_from_in(scy_qd* q);
+/* Host-only inspection of an input file (no GPU needed): the derived array
+ * `name` ("y", "z", "mu", "rho", "cs", "a", "b", "sN", "Dc", "psi",
+ * "locked", "prestress", "eta", "bcL", "bcRShift") is copied to out (cap
+ * doubles); *n receives its length. */
+scy_status scy_in_problem_field(const char* path, const char* name, double* out, long cap, long* n);
+/* Host-only: grid descriptor scalars and integrator settings of an input
+ * file (pointer members of *grid are set to NULL). */
+scy_status scy_in_problem_info(const char* path, scy_grid_desc* grid, scy_ode_opts* ode, int* state_law,
+                               int* guess_ss, double* fault_type_scale);
+
+/* Overwrites the integrated state [psi | slip] (host, 2*Nz) between steps.
+ * recompute = 1 re-evaluates the rates from it (one d_dt); recompute = 0
+ * only uploads it (for a host round trip of the state the device holds). */
+scy_status scy_qd_set_state(scy_qd* q, const double* var_host, int recompute);
 
 #ifdef __cplusplus
 }

@@ -31,7 +31,7 @@ def resid_qd(V, tauQS, eta, sN, psi, a, v0):
     return f, J
 
 
-def test_roots_resid(val):
+def known_answer_resid(val):
     """TestRoots::getResid (rootFinder.cpp:12-24), the reference's known-answer residual."""
     tauQS = 0.75 * (3.000075e+01 - 9.999920e-06)
     return 0.015 * 50 * np.arcsinh((val / 2.0 / 1e-6) * np.exp(0.6 / 0.015)) + 0.5 * 12 * val - tauQS

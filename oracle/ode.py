@@ -140,7 +140,7 @@ class AdaptiveRK:
                 attempt += 1
                 if self.currT + self.deltaT > self.finalT:
                     self.deltaT = self.finalT - self.currT
-                forced = next(rp) if rp is not None else None
+                forced = next(rp, None) if rp is not None else None
                 if forced is not None:
                     self.deltaT = forced[0]
                 lo, hi = self._attempt(ev, keys, dvar)

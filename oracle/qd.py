@@ -89,8 +89,36 @@ class QDLinearElastic:
         return False
 
     def initiate_integrand(self):
-        """initiateIntegrand (strikeSlip_linearElastic_qd.cpp:377-413) without the steady-state guess."""
-        return {"slip": self.bcL * self.fts, "psi": self.fault.psi.copy()}
+        """initiateIntegrand (strikeSlip_linearElastic_qd.cpp:377-413)."""
+        var = {"slip": self.bcL * self.fts, "psi": self.fault.psi.copy()}
+        if self.P["driver"]["guessSteadyStateICs"] == 1:
+            var["slip"] = self.solve_ss()
+            var["psi"] = self.fault.psi.copy()
+        return var
+
+    def solve_ss(self):
+        """solveSS + solveSSb (strikeSlip_linearElastic_qd.cpp:895-1006) with
+        Fault::guessSS / computePsiSS (fault.cpp:619-672).  Returns the slip."""
+        f = self.fault
+        f.slipVel = np.full(self.Nz, self.vL)
+        if not self.P["fault"]["stateVals"]:
+            f.psi = f.f0 - f.b * np.log(abs(self.vL) / f.v0)
+        tau = f.sN * f.a * np.arcsinh(0.5 * self.vL * np.exp(f.psi / f.a) / f.v0)
+        bc = self.P["bc"]
+        self.sbp.change_bc_types(bc["R"], bc["T"], "Neumann", bc["B"])
+        lu = spla.splu(self.sbp.A.tocsc())
+        rhs = self.sbp.set_rhs(tau, np.zeros(self.Nz), self.bcT, self.bcB)
+        u = lu.solve(rhs)
+        mn = u.min()
+        if mn < 0:
+            u = u + abs(mn)
+        self.bcRShift = u[-self.Nz:].copy()
+        self.bcR = self.bcRShift.copy()
+        uL = u[:self.Nz].copy()
+        self.bcL = uL.copy()
+        self.u = u
+        self.sbp.change_bc_types(bc["R"], bc["T"], bc["L"], bc["B"])
+        return uL * self.fts
 
     def integrate(self, max_steps=None, replay=None, record=None):
         s = self.P["driver"]

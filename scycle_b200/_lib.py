@@ -68,6 +68,9 @@ def lib():
         L.scy_sbp_solve.argtypes = [vp, vp, vp, C.POINTER(SolveOpts), C.POINTER(SolveStats)]
         L.scy_sbp_info.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.scy_grid_host_apply.argtypes = [C.POINTER(GridDesc), dptr, dptr]
+        L.scy_launch_count.restype = C.c_longlong
+        L.scy_profile_enable.argtypes = [C.c_int]
+        L.scy_profile_collect.argtypes = [C.c_int, C.c_int, dptr, C.POINTER(C.c_longlong), dptr]
         _declare_extra(L)
         _lib = L
     return _lib

@@ -1,5 +1,58 @@
-"""Argument types of the fault / driver entry points (filled in as they are added)."""
+"""ctypes declarations of the fault / quasi-dynamic driver entry points."""
+import ctypes as C
+
+from . import _lib as S
+
+dptr = C.POINTER(C.c_double)
+
+
+class FaultDesc(C.Structure):
+    _fields_ = [("Nz", C.c_int), ("a", dptr), ("b", dptr), ("sN", dptr), ("Dc", dptr), ("eta", dptr),
+                ("locked", dptr), ("prestress", dptr), ("f0", C.c_double), ("v0", C.c_double), ("vL", C.c_double),
+                ("root_tol", C.c_double), ("max_its", C.c_int), ("state_law", C.c_int)]
+
+
+class QDDesc(C.Structure):
+    _fields_ = [("grid", S.GridDesc), ("fault", FaultDesc), ("fault_type_scale", C.c_double),
+                ("bcL_from_slip", C.c_int), ("bcR_remote", C.c_int), ("vL", C.c_double), ("bcL0", dptr),
+                ("bcRShift", dptr), ("solve", S.SolveOpts)]
+
+
+class OdeOpts(C.Structure):
+    _fields_ = [("method", C.c_int), ("control", C.c_int), ("norm", C.c_int), ("tol", C.c_double),
+                ("min_dt", C.c_double), ("max_dt", C.c_double), ("init_dt", C.c_double), ("t0", C.c_double),
+                ("t1", C.c_double), ("max_steps", C.c_long), ("n_err", C.c_int), ("err_keys", C.c_int * 2),
+                ("err_scale", C.c_double * 2)]
+
+
+class OdeStats(C.Structure):
+    _fields_ = [("t", C.c_double), ("dt", C.c_double), ("new_dt", C.c_double), ("step_count", C.c_long),
+                ("rejected", C.c_long), ("d_dt_evals", C.c_long), ("solve_its", C.c_long), ("solves", C.c_long),
+                ("errA", C.c_double * 2), ("done", C.c_int)]
+
+
+FIELDS = {"psi": 0, "slip": 1, "slipVel": 2, "tauP": 3, "tauQSP": 4, "strength": 5, "u": 6, "surfDisp": 7,
+          "sxy": 8, "dpsi": 9, "dslip": 10}
+LAWS = {"agingLaw": 0, "slipLaw": 1, "constantState": 2}
 
 
 def declare(L):
+    vp = C.c_void_p
+    L.scy_qd_create.argtypes = [C.POINTER(QDDesc), C.POINTER(vp)]
+    L.scy_qd_destroy.argtypes = [vp]
+    L.scy_qd_set_stream.argtypes = [vp, vp]
+    L.scy_qd_d_dt.argtypes = [vp, C.c_double, vp, vp]
+    L.scy_qd_integrate_begin.argtypes = [vp, C.POINTER(OdeOpts), dptr]
+    L.scy_qd_integrate_steps.argtypes = [vp, C.c_long, C.POINTER(OdeStats)]
+    L.scy_qd_force_attempts.argtypes = [vp, dptr, C.POINTER(C.c_int), C.c_long]
+    L.scy_qd_record_attempts.argtypes = [vp, C.c_int]
+    L.scy_qd_get_attempts.argtypes = [vp, dptr, C.POINTER(C.c_int), C.c_long, C.POINTER(C.c_long)]
+    L.scy_qd_get_field.argtypes = [vp, C.c_int, dptr]
+    L.scy_qd_create_from_in.argtypes = [C.c_char_p, C.POINTER(S.SolveOpts), C.POINTER(vp)]
+    L.scy_qd_get_problem.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(OdeOpts)]
+    L.scy_qd_integrate_begin_from_in.argtypes = [vp]
+    L.scy_qd_set_state.argtypes = [vp, dptr, C.c_int]
+    L.scy_in_problem_field.argtypes = [C.c_char_p, C.c_char_p, dptr, C.c_long, C.POINTER(C.c_long)]
+    L.scy_in_problem_info.argtypes = [C.c_char_p, C.POINTER(S.GridDesc), C.POINTER(OdeOpts), C.POINTER(C.c_int),
+                                      C.POINTER(C.c_int), C.POINTER(C.c_double)]
     return L

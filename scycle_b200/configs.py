@@ -46,6 +46,7 @@ outputDir = {outputDir}
 bulkDeformationType = linearElastic
 momentumBalanceType = quasidynamic
 stateLaw = {stateLaw}
+guessSteadyStateICs = {guess}
 f0 = 0.6
 v0 = 1e-6
 DcVals = [0.008 0.008]
@@ -82,7 +83,7 @@ def tanh_stretch(n, L, beta):
 def make_qd_problem(workdir, Ny=101, Nz=101, Ly=30.0, Lz=30.0, order=4, seed=0,
                     grid="constantGridSpacing", state_law="agingLaw", integrator="RK32",
                     tol=1e-7, years=200.0, max_steps=100000000, init_dt=1e-3,
-                    stretch_beta=None, dc_lognormal=False, name="qd"):
+                    stretch_beta=None, dc_lognormal=False, name="qd", guess_ss=0):
     """Write ``<workdir>/<name>.in`` and its inputDir fields; return the .in path."""
     os.makedirs(workdir, exist_ok=True)
     rng = np.random.default_rng(seed)
@@ -91,7 +92,8 @@ def make_qd_problem(workdir, Ny=101, Nz=101, Ly=30.0, Lz=30.0, order=4, seed=0,
     text = _COMMON.format(order=order, Ny=Ny, Nz=Nz, Ly=repr(float(Ly)), Lz=repr(float(Lz)), grid=grid,
                           inputDir=input_dir, outputDir=out_dir, stateLaw=state_law,
                           integrator=integrator, maxStepCount=int(max_steps),
-                          maxTime=repr(float(years * YEAR)), initDeltaT=repr(float(init_dt)), tol=repr(float(tol)))
+                          maxTime=repr(float(years * YEAR)), initDeltaT=repr(float(init_dt)), tol=repr(float(tol)),
+                          guess=int(guess_ss))
     psi = 0.6 + rng.normal(0.0, 1e-4, size=Nz)
     write_petsc_vec(input_dir + "psi", psi)
     if stretch_beta is not None:
@@ -116,7 +118,9 @@ def aging_const_101(workdir, seed=0, **kw):
 
 
 def slip_var_401(workdir, seed=0, **kw):
+    """401x401 stretched grid, slip law, per-node lognormal Dc; starts from the
+    steady-state guess (guessSteadyStateICs = 1) so the run is inside the cycle."""
     args = dict(Ny=401, Nz=401, seed=seed, grid="variableGridSpacing", state_law="slipLaw",
-                stretch_beta=2.0, dc_lognormal=True, name="slip_var_401")
+                stretch_beta=2.0, dc_lognormal=True, name="slip_var_401", guess_ss=1)
     args.update(kw)
     return make_qd_problem(workdir, **args)

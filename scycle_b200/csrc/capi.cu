@@ -4,10 +4,18 @@
 #include <vector>
 
 #include "common.cuh"
+#include "infile.hpp"
+#include "qd.hpp"
+#include <memory>
 #include "sbp_solver.hpp"
 
 struct scy_sbp {
   scy::SbpContext ctx;
+};
+
+struct scy_qd {
+  scy::QDContext ctx;
+  std::unique_ptr<scy::QDProblem> prob;  // set by scy_qd_create_from_in
 };
 
 extern "C" {
@@ -15,6 +23,18 @@ extern "C" {
 const char* scy_get_last_error(void) { return scy::last_error(); }
 
 const char* scy_version(void) { return "scycle_b200 0.1 (sm_100a)"; }
+
+long long scy_launch_count(void) { return scy::launch_count(); }
+
+scy_status scy_profile_enable(int on) {
+  scy::profile_enable(on);
+  return SCY_OK;
+}
+
+scy_status scy_profile_collect(int level, int width, double* ms, long long* launches, double* bytes) {
+  if (!ms || !launches || !bytes) return SCY_ERR_ARG;
+  return scy::profile_collect(level, width, ms, launches, bytes);
+}
 
 scy_status scy_sbp_create(const scy_grid_desc* desc, scy_sbp** out) {
   if (!desc || !out) {
@@ -124,6 +144,274 @@ scy_status scy_grid_host_apply(const scy_grid_desc* g, const double* in, double*
     scy::set_error("scy_grid_host_apply: %s", e.what());
     return SCY_ERR_ARG;
   }
+  return SCY_OK;
+}
+
+scy_status scy_qd_create(const scy_qd_desc* d, scy_qd** out) {
+  if (!d || !out) {
+    scy::set_error("scy_qd_create: NULL argument");
+    return SCY_ERR_ARG;
+  }
+  *out = nullptr;
+  scy_qd* q = new (std::nothrow) scy_qd();
+  if (!q) return SCY_ERR_NOMEM;
+  int st = q->ctx.create(*d);
+  if (st != SCY_OK) {
+    delete q;
+    return st;
+  }
+  *out = q;
+  return SCY_OK;
+}
+
+scy_status scy_qd_destroy(scy_qd* q) {
+  delete q;
+  return SCY_OK;
+}
+
+scy_status scy_qd_set_stream(scy_qd* q, void* stream) {
+  if (!q) return SCY_ERR_ARG;
+  q->ctx.sbp.stream = (cudaStream_t)stream;
+  return SCY_OK;
+}
+
+scy_status scy_qd_d_dt(scy_qd* q, double t, const double* var, double* dvar) {
+  if (!q || !var || !dvar) {
+    scy::set_error("scy_qd_d_dt: NULL argument");
+    return SCY_ERR_ARG;
+  }
+  SCY_TRY(q->ctx.d_dt(t, var, dvar));
+  return q->ctx.read_flags();
+}
+
+scy_status scy_qd_integrate_begin(scy_qd* q, const scy_ode_opts* o, const double* var0) {
+  if (!q || !o || !var0) {
+    scy::set_error("scy_qd_integrate_begin: NULL argument");
+    return SCY_ERR_ARG;
+  }
+  if (!(o->tol > 0) || !(o->max_dt >= o->min_dt) || !(o->t1 >= o->t0) || o->max_steps < 0 || o->n_err > 2) {
+    scy::set_error("scy_qd_integrate_begin: invalid options");
+    return SCY_ERR_ARG;
+  }
+  scy::QDContext& c = q->ctx;
+  SCY_CUDA_TRY(cudaMemcpyAsync(c.rk[0].p, var0, 2 * (size_t)c.Nz * sizeof(double), cudaMemcpyHostToDevice,
+                               c.sbp.stream));
+  return c.integrate_begin(*o);
+}
+
+scy_status scy_qd_integrate_steps(scy_qd* q, long nsteps, scy_ode_stats* st) {
+  if (!q || nsteps < 0) {
+    scy::set_error("scy_qd_integrate_steps: invalid argument");
+    return SCY_ERR_ARG;
+  }
+  return q->ctx.integrate_steps(nsteps, st);
+}
+
+scy_status scy_qd_force_attempts(scy_qd* q, const double* dts, const int* acc, long n) {
+  if (!q || n < 0 || (n > 0 && (!dts || !acc))) return SCY_ERR_ARG;
+  q->ctx.forced_dt.assign(dts, dts + n);
+  q->ctx.forced_acc.assign(acc, acc + n);
+  q->ctx.forced_pos = 0;
+  return SCY_OK;
+}
+
+scy_status scy_qd_record_attempts(scy_qd* q, int on) {
+  if (!q) return SCY_ERR_ARG;
+  q->ctx.record = on ? 1 : 0;
+  if (on) {
+    q->ctx.log_dt.clear();
+    q->ctx.log_acc.clear();
+  }
+  return SCY_OK;
+}
+
+scy_status scy_qd_get_attempts(scy_qd* q, double* dts, int* acc, long cap, long* n) {
+  if (!q || !n) return SCY_ERR_ARG;
+  long m = (long)q->ctx.log_dt.size();
+  *n = m;
+  for (long i = 0; i < m && i < cap; ++i) {
+    if (dts) dts[i] = q->ctx.log_dt[i];
+    if (acc) acc[i] = q->ctx.log_acc[i];
+  }
+  return SCY_OK;
+}
+
+scy_status scy_qd_get_field(scy_qd* q, int field, double* out) {
+  if (!q || !out) return SCY_ERR_ARG;
+  scy::QDContext& c = q->ctx;
+  cudaStream_t s = c.sbp.stream;
+  const double* src = nullptr;
+  size_t n = c.Nz;
+  long stride = 1;
+  switch (field) {
+    case SCY_FIELD_PSI: src = c.rk[0].as<double>(); break;
+    case SCY_FIELD_SLIP: src = c.rk[0].as<double>() + c.Nz; break;
+    case SCY_FIELD_DPSI: src = c.rk[1].as<double>(); break;
+    case SCY_FIELD_DSLIP: src = c.rk[1].as<double>() + c.Nz; break;
+    case SCY_FIELD_SLIPVEL: src = c.slipVel.as<double>(); break;
+    case SCY_FIELD_TAUP: src = c.tauP.as<double>(); break;
+    case SCY_FIELD_TAUQSP: src = c.tauQSP.as<double>(); break;
+    case SCY_FIELD_STRENGTH: src = c.strength.as<double>(); break;
+    case SCY_FIELD_U: src = c.u.as<double>(); n = c.N; break;
+    case SCY_FIELD_SURFDISP: src = c.u.as<double>(); n = c.Ny; stride = c.Nz; break;
+    case SCY_FIELD_SXY:
+      SCY_TRY(c.sbp.apply(SCY_OP_MUXDY, c.u.as<double>(), c.sxy.as<double>()));
+      src = c.sxy.as<double>();
+      n = c.N;
+      break;
+    default:
+      scy::set_error("unknown field %d", field);
+      return SCY_ERR_ARG;
+  }
+  if (stride == 1) {
+    SCY_CUDA_TRY(cudaMemcpyAsync(out, src, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+  } else {
+    SCY_CUDA_TRY(cudaMemcpy2DAsync(out, sizeof(double), src, stride * sizeof(double), sizeof(double), n,
+                                   cudaMemcpyDeviceToHost, s));
+  }
+  SCY_CUDA_TRY(cudaStreamSynchronize(s));
+  return SCY_OK;
+}
+
+scy_status scy_qd_create_from_in(const char* path, const scy_solve_opts* solve, scy_qd** out) {
+  if (!path || !out) {
+    scy::set_error("scy_qd_create_from_in: NULL argument");
+    return SCY_ERR_ARG;
+  }
+  *out = nullptr;
+  std::unique_ptr<scy::QDProblem> P(new (std::nothrow) scy::QDProblem());
+  if (!P) return SCY_ERR_NOMEM;
+  try {
+    scy::load_qd_problem(path, *P);
+  } catch (const std::exception& e) {
+    scy::set_error("%s", e.what());
+    return SCY_ERR_IO;
+  }
+  if (solve) {
+    P->desc.solve = *solve;
+  } else {
+    P->desc.solve.rtol = 1e-12;
+    P->desc.solve.atol = 0.0;
+    P->desc.solve.max_its = 300;
+    P->desc.solve.precision = SCY_PREC_FP64;
+    P->desc.solve.nonzero_guess = 1;
+    P->desc.solve.check_every = 1;
+  }
+  scy_qd* q = new (std::nothrow) scy_qd();
+  if (!q) return SCY_ERR_NOMEM;
+  int st = q->ctx.create(P->desc);
+  if (st != SCY_OK) {
+    delete q;
+    return st;
+  }
+  if (P->min_dt_user == -1.0) P->ode.min_dt = q->ctx.compute_min_dt(P->cs, P->desc.grid.Ly, P->desc.grid.Lz);
+  q->prob = std::move(P);
+  *out = q;
+  return SCY_OK;
+}
+
+scy_status scy_qd_get_problem(scy_qd* q, int* Ny, int* Nz, scy_ode_opts* ode) {
+  if (!q) return SCY_ERR_ARG;
+  if (Ny) *Ny = q->ctx.Ny;
+  if (Nz) *Nz = q->ctx.Nz;
+  if (ode) {
+    if (!q->prob) {
+      scy::set_error("driver was not created from an input file");
+      return SCY_ERR_STATE;
+    }
+    *ode = q->prob->ode;
+  }
+  return SCY_OK;
+}
+
+scy_status scy_qd_integrate_begin_from_in(scy_qd* q) {
+  if (!q || !q->prob) {
+    scy::set_error("scy_qd_integrate_begin_from_in: driver was not created from an input file");
+    return SCY_ERR_STATE;
+  }
+  scy::QDProblem& P = *q->prob;
+  scy::QDContext& c = q->ctx;
+  const int Nz = c.Nz;
+  std::vector<double> psi = P.psi, slip(Nz);
+  for (int i = 0; i < Nz; ++i) slip[i] = P.bcL0[i] * P.desc.fault_type_scale;
+  if (P.guess_ss) SCY_TRY(c.steady_state_guess(psi, P.stateVals_given, slip));
+  std::vector<double> var0(2 * (size_t)Nz);
+  std::copy(psi.begin(), psi.end(), var0.begin());
+  std::copy(slip.begin(), slip.end(), var0.begin() + Nz);
+  SCY_CUDA_TRY(cudaMemcpyAsync(c.rk[0].p, var0.data(), var0.size() * sizeof(double), cudaMemcpyHostToDevice,
+                               c.sbp.stream));
+  SCY_CUDA_TRY(cudaStreamSynchronize(c.sbp.stream));
+  return c.integrate_begin(P.ode);
+}
+
+scy_status scy_qd_set_state(scy_qd* q, const double* var, int recompute) {
+  if (!q || !var) return SCY_ERR_ARG;
+  scy::QDContext& c = q->ctx;
+  if (!c.ode_ready) {
+    scy::set_error("scy_qd_set_state: integration not started");
+    return SCY_ERR_STATE;
+  }
+  SCY_CUDA_TRY(cudaMemcpyAsync(c.rk[0].p, var, 2 * (size_t)c.Nz * sizeof(double), cudaMemcpyHostToDevice,
+                               c.sbp.stream));
+  if (!recompute) return SCY_OK;
+  SCY_TRY(c.d_dt(c.currT, c.rk[0].as<double>(), c.rk[1].as<double>()));
+  return c.read_flags();
+}
+
+scy_status scy_in_problem_field(const char* path, const char* name, double* out, long cap, long* n) {
+  if (!path || !name || !n) return SCY_ERR_ARG;
+  scy::QDProblem P;
+  try {
+    scy::load_qd_problem(path, P);
+  } catch (const std::exception& e) {
+    scy::set_error("%s", e.what());
+    return SCY_ERR_IO;
+  }
+  const std::string nm(name);
+  const std::vector<double>* v = nullptr;
+  if (nm == "y") v = &P.y;
+  else if (nm == "z") v = &P.z;
+  else if (nm == "mu") v = &P.mu;
+  else if (nm == "rho") v = &P.rho;
+  else if (nm == "cs") v = &P.cs;
+  else if (nm == "a") v = &P.a;
+  else if (nm == "b") v = &P.b;
+  else if (nm == "sN") v = &P.sN;
+  else if (nm == "Dc") v = &P.Dc;
+  else if (nm == "psi") v = &P.psi;
+  else if (nm == "locked") v = &P.locked;
+  else if (nm == "prestress") v = &P.prestress;
+  else if (nm == "eta") v = &P.eta;
+  else if (nm == "bcL") v = &P.bcL0;
+  else if (nm == "bcRShift") v = &P.bcRShift;
+  if (!v) {
+    scy::set_error("unknown problem field '%s'", name);
+    return SCY_ERR_ARG;
+  }
+  *n = (long)v->size();
+  if (out)
+    for (long i = 0; i < *n && i < cap; ++i) out[i] = (*v)[i];
+  return SCY_OK;
+}
+
+scy_status scy_in_problem_info(const char* path, scy_grid_desc* grid, scy_ode_opts* ode, int* state_law,
+                               int* guess_ss, double* fault_type_scale) {
+  if (!path) return SCY_ERR_ARG;
+  scy::QDProblem P;
+  try {
+    scy::load_qd_problem(path, P);
+  } catch (const std::exception& e) {
+    scy::set_error("%s", e.what());
+    return SCY_ERR_IO;
+  }
+  if (grid) {
+    *grid = P.desc.grid;
+    grid->y = grid->z = grid->mu = nullptr;
+  }
+  if (ode) *ode = P.ode;
+  if (state_law) *state_law = P.desc.fault.state_law;
+  if (guess_ss) *guess_ss = P.guess_ss;
+  if (fault_type_scale) *fault_type_scale = P.desc.fault_type_scale;
   return SCY_OK;
 }
 

@@ -12,6 +12,8 @@ namespace scy {
 
 // Last error message of this thread, returned through scy_get_last_error().
 void set_error(const char* fmt, ...);
+// Counts kernel launches of this library (read by scy_launch_count()).
+void count_launch();
 
 #define SCY_CUDA_TRY(call)                                                     \
   do {                                                                         \
@@ -25,6 +27,7 @@ void set_error(const char* fmt, ...);
 
 #define SCY_LAUNCH_CHECK()                                                     \
   do {                                                                         \
+    ::scy::count_launch();                                                     \
     cudaError_t e_ = cudaGetLastError();                                       \
     if (e_ != cudaSuccess) {                                                   \
       ::scy::set_error("%s:%d: kernel launch failed: %s", __FILE__, __LINE__,  \
@@ -86,23 +89,25 @@ __device__ __forceinline__ T block_sum(T v, T* sh /* >= 32 entries */) {
 }
 
 // Grid-wide deterministic reduction: each block stores its partial sum in
-// partials[blockIdx.x]; the last block to finish adds them in index order and
+// partials[linear block id]; the last block to finish adds them in index order and
 // writes *out.  `counter` must be zero on entry and is reset to zero.
 __device__ __forceinline__ void grid_reduce_finish(double block_total, double* partials,
                                                    unsigned int* counter, double* out,
                                                    double* sh) {
   __shared__ bool am_last;
+  const unsigned int nblocks = gridDim.x * gridDim.y * gridDim.z;
+  const unsigned int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
   if (threadIdx.x == 0) {
-    partials[blockIdx.x] = block_total;
+    partials[bid] = block_total;
     __threadfence();
     unsigned int prev = atomicAdd(counter, 1u);
-    am_last = (prev == gridDim.x - 1);
+    am_last = (prev == nblocks - 1);
   }
   __syncthreads();
   if (am_last) {
     __threadfence();
     double s = 0.0;
-    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) s += ((volatile double*)partials)[i];
+    for (int i = threadIdx.x; i < (int)nblocks; i += blockDim.x) s += ((volatile double*)partials)[i];
     s = block_sum(s, sh);
     if (threadIdx.x == 0) {
       *out = s;

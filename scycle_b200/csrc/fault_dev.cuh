@@ -1,0 +1,106 @@
+// Rate-and-state fault on the device: one thread per fault node.
+//
+// Follows Fault_qd::d_dt / ComputeVel_qd::computeVel (reference
+// source/fault.cpp:861-1059), BracketedNewton::findRoot
+// (source/rootFinder.cpp:174-257) and the state laws (fault.cpp:1984-2088,
+// strength :2247-2251).
+#pragma once
+#include <cuda_runtime.h>
+
+namespace scy {
+
+enum FaultFlags : unsigned {
+  FAULT_ROOT_NOCONV = 1u,
+  FAULT_NONFINITE = 2u,
+};
+
+struct FaultParams {
+  int Nz;
+  const double *a, *b, *sN, *Dc, *eta, *locked, *prestress;
+  double f0, v0, vL, root_tol;
+  int max_its;
+  int state_law;  // 0 aging, 1 slip, 2 constant state
+};
+
+__device__ __forceinline__ double strength_psi(double sN, double psi, double V, double a, double v0) {
+  return a * sN * asinh((0.5 * V / v0) * exp(psi / a));
+}
+
+// Residual of tau_qs - eta V = strength(V) and the reference's derivative
+// expression a*sN*V/sqrt(B^2 V^2 + 1) + eta with B = exp(psi/a)/(2 v0)
+// (fault.cpp:1051).  The exact derivative has B in place of V in the
+// numerator; the expression only steers the Newton/bisection choice.
+__device__ __forceinline__ void resid_qd(double V, double tauQS, double eta, double sN, double psi, double a,
+                                         double v0, double& f, double& J) {
+  f = strength_psi(sN, psi, V, a, v0) - (tauQS - eta * V);
+  double A = a * sN;
+  double B = exp(psi / a) / (2.0 * v0);
+  J = A * V / sqrt(B * B * V * V + 1.0) + eta;
+}
+
+// Safeguarded Newton on [left, right] starting from x0.  Returns the root;
+// sets *its and *ok.  Every loop is bounded by max_its.
+__device__ __forceinline__ double bracketed_newton(double left, double right, double x0, double atol, int max_its,
+                                                   double tauQS, double eta, double sN, double psi, double a,
+                                                   double v0, int* its, bool* ok) {
+  double f, fp, fl, fr, dum;
+  *its = 0;
+  *ok = true;
+  resid_qd(x0, tauQS, eta, sN, psi, a, v0, f, fp);
+  if (fabs(f) <= atol) return x0;
+  resid_qd(left, tauQS, eta, sN, psi, a, v0, fl, dum);
+  resid_qd(right, tauQS, eta, sN, psi, a, v0, fr, dum);
+  if (!isfinite(fl) || !isfinite(fr)) {
+    *ok = false;
+    return x0;
+  }
+  if (sqrt(fl * fl) <= atol) return left;
+  if (sqrt(fr * fr) <= atol) return right;
+  if (fl > 0) {
+    double t = left;
+    left = right;
+    right = t;
+  }
+  double x = x0;
+  double dxold = fabs(right - left), dx = dxold;
+  resid_qd(x, tauQS, eta, sN, psi, a, v0, f, fp);
+  int n = 0;
+  while (n <= max_its && fabs(f) >= atol) {
+    if (((x - right) * fp - f) * ((x - left) * fp - f) > 0.0 || fabs(2.0 * f) > fabs(dxold * fp)) {
+      dxold = dx;
+      dx = 0.5 * (right - left);
+      x = left + dx;
+    } else {
+      dxold = dx;
+      dx = f / fp;
+      x -= dx;
+    }
+    resid_qd(x, tauQS, eta, sN, psi, a, v0, f, fp);
+    if (f < 0.0)
+      left = x;
+    else
+      right = x;
+    ++n;
+  }
+  *its = n;
+  if (!(fabs(f) <= atol)) *ok = false;
+  if (!isfinite(f)) *ok = false;
+  return x;
+}
+
+__device__ __forceinline__ double aging_law_psi(double psi, double V, double b, double f0, double v0, double Dc) {
+  double A = exp((f0 - psi) / b);
+  if (!isinf(A) && b > 1e-3) return (b * v0 / Dc) * (A - V / v0);
+  return 0.0;
+}
+
+__device__ __forceinline__ double slip_law_psi(double psi, double V, double a, double b, double f0, double v0,
+                                               double Dc) {
+  if (V == 0.0) return 0.0;
+  double absV = fabs(V);
+  double fss = f0 + (a - b) * log(absV / v0);
+  double f = a * asinh((absV / 2.0 / v0) * exp(psi / a));
+  return -absV / Dc * (f - fss);
+}
+
+}  // namespace scy

@@ -1,0 +1,55 @@
+// The reference's ``.in`` input format and PETSc-binary vectors, on the host.
+#pragma once
+#include <string>
+#include <vector>
+
+#include "../../include/scycle_b200.h"
+
+namespace scy {
+
+struct InEntry {
+  std::string var, rhs, full;  // key, value up to the first space, everything after " = "
+};
+
+// Splits every line at the first " = " (source/domain.cpp:153-166 and the
+// same loop in every class's loadSettings).  Throws std::runtime_error if
+// the file cannot be read.
+std::vector<InEntry> parse_in_file(const std::string& path);
+std::vector<InEntry> parse_in_text(const std::string& text);
+
+double c_atof(const std::string& s);
+int c_atoi(const std::string& s);
+// ``[v1 v2 ...]`` lists (source/genFuncs.cpp:413-440, :476-505)
+std::vector<double> load_vector_double(const std::string& s);
+std::vector<std::string> load_vector_string(const std::string& s);
+// Piecewise-linear depth profile with extrapolation (source/genFuncs.cpp:574-617).
+std::vector<double> set_vec(const std::vector<double>& coord, const std::vector<double>& vals,
+                            const std::vector<double>& depths);
+// Reads the first Vec record of a PETSc binary file into out.  Returns false
+// if the file does not exist; throws std::runtime_error if it is malformed
+// or holds a different length than n.
+bool read_petsc_vec(const std::string& path, size_t n, std::vector<double>& out);
+// Writes (append = 0) or appends (append = 1) one Vec record.
+void write_petsc_vec(const std::string& path, const double* v, size_t n, int append);
+
+// Everything StrikeSlip_LinearElastic_qd reads from an input file, with the
+// host arrays the descriptor points into.
+struct QDProblem {
+  scy_qd_desc desc{};
+  scy_ode_opts ode{};
+  int guess_ss = 0;
+  int stride1D = 1, stride2D = 1;
+  std::string inputDir, outputDir, stateLaw, integrator;
+  double vL = 1e-9, min_dt_user = -1.0;
+  std::vector<double> y, z, mu, rho, cs;
+  std::vector<double> a, b, sN, Dc, locked, prestress, psi, eta, mu_f, rho_f;
+  std::vector<double> bcL0, bcRShift;
+  int stateVals_given = 0;
+};
+
+// Builds the problem like Domain + LinearElastic + Fault_qd +
+// StrikeSlip_LinearElastic_qd constructors do.  Throws std::runtime_error
+// with a message on invalid input.
+void load_qd_problem(const std::string& path, QDProblem& P);
+
+}  // namespace scy

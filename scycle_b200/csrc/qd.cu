@@ -1,0 +1,566 @@
+// Linear-elastic quasi-dynamic driver on the device.
+//
+// d_dt follows StrikeSlip_LinearElastic_qd::d_dt
+// (source/strikeSlip_linearElastic_qd.cpp:756-798) and Fault_qd::d_dt
+// (source/fault.cpp:861-918); the integrators follow RK32::integrate and
+// RK43::integrate (source/odeSolver.cpp:505-627, :973-1175) with their step
+// control (:395-445, :846-898), including the reference's handling of the
+// 100-attempt cap and of a step that falls to the minimum size.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "common.cuh"
+#include "qd.hpp"
+
+namespace scy {
+
+// ---------------------------------------------------------------------------
+// bcL = slip/faultTypeScale, bcR = vL t/faultTypeScale + bcRShift
+__global__ void qd_bc_kernel(const double* __restrict__ var, int Nz, double t, double vL, double inv_fts,
+                             int bcL_from_slip, int bcR_remote, const double* __restrict__ shift,
+                             double* __restrict__ bcL, double* __restrict__ bcR) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= Nz) return;
+  if (bcL_from_slip) bcL[i] = var[Nz + i] * inv_fts;
+  if (bcR_remote) bcR[i] = vL * t * inv_fts + shift[i];
+}
+
+// Fault column: sxy = mu*Dy*u at iy = 0 (body2L scatter of muxDy), then
+// Fault_qd::d_dt for each node.
+__global__ void qd_fault_kernel(LevelDev<double> L, const double* __restrict__ u, FaultParams fp,
+                                const double* __restrict__ var, double* __restrict__ f,
+                                double* __restrict__ slipVel, double* __restrict__ tauQSP,
+                                double* __restrict__ tauP, double* __restrict__ strength, unsigned* flags,
+                                unsigned long long* its_total) {
+  const int Nz = fp.Nz;
+  int iz = blockIdx.x * blockDim.x + threadIdx.x;
+  if (iz >= Nz) return;
+  // Dy row 0 (band offsets -4..4 around row 0; only columns >= 0 exist)
+  double d = 0.0;
+#pragma unroll
+  for (int j = HALF; j < BAND; ++j) {
+    int k = j - HALF;
+    if (k < L.Ny) d += L.y.D[j] * u[(long)k * Nz + iz];
+  }
+  if (L.var) d *= L.qy[iz];
+  const double sxy = L.mu[iz] * d;
+  const double tq = sxy + fp.prestress[iz];
+  tauQSP[iz] = tq;
+  const double psi = var[iz];
+  const double a = fp.a[iz], sN = fp.sN[iz], eta = fp.eta[iz];
+  double V;
+  const double lk = fp.locked[iz];
+  if (lk > 0.5) {
+    V = 0.0;
+  } else if (lk < -0.5) {
+    V = fp.vL;
+  } else {
+    double left = 0.0, right = tq / eta;
+    if (isnan(right)) {
+      atomicOr(flags, (unsigned)FAULT_NONFINITE);
+      V = slipVel[iz];
+    } else if (fabs(left - right) < 1e-14) {
+      V = left;
+    } else {
+      int its = 0;
+      bool ok = true;
+      V = bracketed_newton(left, right, slipVel[iz], fp.root_tol, fp.max_its, tq, eta, sN, psi, a, fp.v0, &its, &ok);
+      atomicAdd(its_total, (unsigned long long)its);
+      if (!ok) atomicOr(flags, (unsigned)FAULT_ROOT_NOCONV);
+    }
+  }
+  slipVel[iz] = V;
+  double dpsi;
+  if (fp.state_law == 0)
+    dpsi = aging_law_psi(psi, V, fp.b[iz], fp.f0, fp.v0, fp.Dc[iz]);
+  else if (fp.state_law == 1)
+    dpsi = slip_law_psi(psi, V, a, fp.b[iz], fp.f0, fp.v0, fp.Dc[iz]);
+  else
+    dpsi = 0.0;
+  if (!isfinite(dpsi) || !isfinite(V)) atomicOr(flags, (unsigned)FAULT_NONFINITE);
+  f[iz] = dpsi;
+  f[Nz + iz] = V;
+  tauP[iz] = tq - eta * V;
+  strength[iz] = strength_psi(sN, psi, V, a, fp.v0);
+}
+
+// out = ((var + c0 f0) + c1 f1) + ... in the reference's WAXPY/AXPY order
+struct Combo {
+  const double* f[5];
+  double c[5];
+  int nf;
+};
+
+__global__ void rk_combine_kernel(double* __restrict__ out, const double* __restrict__ var, Combo cb, int n) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double v = cb.c[0] * cb.f[0][i] + var[i];
+  for (int j = 1; j < cb.nf; ++j) v = v + cb.c[j] * cb.f[j][i];
+  out[i] = v;
+}
+
+// Per key (psi: [0,Nz), slip: [Nz,2Nz)): sum (lo-hi)^2, sum hi^2, max(|lo-hi|/hi).
+__global__ void rk_error_kernel(const double* __restrict__ lo, const double* __restrict__ hi, int Nz,
+                                double* __restrict__ out) {
+  __shared__ double sh[32];
+  for (int key = 0; key < 2; ++key) {
+    double ss = 0.0, sh2 = 0.0, mx = -INFINITY;
+    for (int i = threadIdx.x; i < Nz; i += blockDim.x) {
+      double h = hi[key * Nz + i];
+      double d = lo[key * Nz + i] - h;
+      ss += d * d;
+      sh2 += h * h;
+      double r = fabs(d) / h;
+      mx = fmax(mx, r);
+    }
+    ss = block_sum(ss, sh);
+    sh2 = block_sum(sh2, sh);
+    // max reduction
+    double m = warp_max(mx);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      double t = threadIdx.x < (blockDim.x + 31) / 32 ? sh[threadIdx.x] : -INFINITY;
+      t = warp_max(t);
+      if (threadIdx.x == 0) {
+        out[key * 3 + 0] = ss;
+        out[key * 3 + 1] = sh2;
+        out[key * 3 + 2] = t;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+template <typename T>
+static int upload_vec(DevBuf& b, const T* src, size_t n, cudaStream_t s) {
+  SCY_TRY(b.alloc(n * sizeof(T)));
+  SCY_CUDA_TRY(cudaMemcpyAsync(b.p, src, n * sizeof(T), cudaMemcpyHostToDevice, s));
+  return SCY_OK;
+}
+
+static int upload_or_fill(DevBuf& b, const double* src, size_t n, double fill, cudaStream_t s) {
+  std::vector<double> v(n, fill);
+  if (src) std::copy(src, src + n, v.begin());
+  SCY_TRY(upload_vec(b, v.data(), n, s));
+  SCY_CUDA_TRY(cudaStreamSynchronize(s));
+  return SCY_OK;
+}
+
+int QDContext::create(const scy_qd_desc& d) {
+  SCY_TRY(sbp.create(d.grid));
+  Ny = d.grid.Ny;
+  Nz = d.grid.Nz;
+  N = (long)Ny * Nz;
+  const scy_fault_desc& f = d.fault;
+  if (f.Nz != Nz) {
+    set_error("fault Nz (%d) differs from grid Nz (%d)", f.Nz, Nz);
+    return SCY_ERR_ARG;
+  }
+  if (!f.a || !f.b || !f.sN || !f.Dc || !f.eta) {
+    set_error("fault arrays a, b, sN, Dc, eta are required");
+    return SCY_ERR_ARG;
+  }
+  if (f.state_law < 0 || f.state_law > 2) {
+    set_error("unknown state law %d", f.state_law);
+    return SCY_ERR_ARG;
+  }
+  if (!(f.v0 > 0) || !(f.root_tol > 0) || f.max_its < 1) {
+    set_error("fault needs v0 > 0, root_tol > 0, max_its >= 1");
+    return SCY_ERR_ARG;
+  }
+  cudaStream_t s = sbp.stream;
+  SCY_TRY(upload_or_fill(fa, f.a, Nz, 0, s));
+  SCY_TRY(upload_or_fill(fb, f.b, Nz, 0, s));
+  SCY_TRY(upload_or_fill(fsN, f.sN, Nz, 0, s));
+  SCY_TRY(upload_or_fill(fDc, f.Dc, Nz, 0, s));
+  SCY_TRY(upload_or_fill(feta, f.eta, Nz, 0, s));
+  SCY_TRY(upload_or_fill(flocked, f.locked, Nz, 0, s));
+  SCY_TRY(upload_or_fill(fprestress, f.prestress, Nz, 0, s));
+  for (DevBuf* b : {&slipVel, &tauQSP, &tauP, &strength}) SCY_TRY(upload_or_fill(*b, nullptr, Nz, 0, s));
+  SCY_TRY(upload_or_fill(bcL, d.bcL0, Nz, 0, s));
+  SCY_TRY(upload_or_fill(bcR, nullptr, Nz, 0, s));
+  SCY_TRY(upload_or_fill(bcRShift, d.bcRShift, Nz, 0, s));
+  SCY_TRY(upload_or_fill(bcT, nullptr, Ny, 0, s));
+  SCY_TRY(upload_or_fill(bcB, nullptr, Ny, 0, s));
+  SCY_TRY(rhs.alloc(N * 8));
+  SCY_TRY(u.alloc(N * 8));
+  SCY_TRY(sxy.alloc(N * 8));
+  SCY_CUDA_TRY(cudaMemset(u.p, 0, N * 8));
+  SCY_TRY(flags.alloc(16));
+  SCY_CUDA_TRY(cudaMemset(flags.p, 0, 16));
+  SCY_TRY(fault_its.alloc(16));
+  SCY_CUDA_TRY(cudaMemset(fault_its.p, 0, 16));
+  h_a.assign(f.a, f.a + Nz);
+  h_b.assign(f.b, f.b + Nz);
+  h_sN.assign(f.sN, f.sN + Nz);
+  f0 = f.f0;
+  v0 = f.v0;
+  fp.Nz = Nz;
+  fp.a = fa.as<double>();
+  fp.b = fb.as<double>();
+  fp.sN = fsN.as<double>();
+  fp.Dc = fDc.as<double>();
+  fp.eta = feta.as<double>();
+  fp.locked = flocked.as<double>();
+  fp.prestress = fprestress.as<double>();
+  fp.f0 = f.f0;
+  fp.v0 = f.v0;
+  fp.vL = f.vL;
+  fp.root_tol = f.root_tol;
+  fp.max_its = f.max_its;
+  fp.state_law = f.state_law;
+  vL = d.vL;
+  fts = d.fault_type_scale;
+  if (!(fts > 0)) {
+    set_error("fault_type_scale must be positive");
+    return SCY_ERR_ARG;
+  }
+  bcL_from_slip = d.bcL_from_slip;
+  bcR_remote = d.bcR_remote;
+  solve_opts = d.solve;
+  if (solve_opts.max_its < 1) solve_opts.max_its = 200;
+  if (solve_opts.check_every < 1) solve_opts.check_every = 1;
+  for (auto& b : rk) {
+    SCY_TRY(b.alloc(2 * (size_t)Nz * 8));
+    SCY_CUDA_TRY(cudaMemset(b.p, 0, 2 * (size_t)Nz * 8));
+  }
+  SCY_TRY(errbuf.alloc(16 * 8));
+  return SCY_OK;
+}
+
+int QDContext::read_flags() {
+  unsigned h = 0;
+  SCY_CUDA_TRY(cudaMemcpyAsync(&h, flags.p, sizeof(unsigned), cudaMemcpyDeviceToHost, sbp.stream));
+  SCY_CUDA_TRY(cudaStreamSynchronize(sbp.stream));
+  if (h) {
+    SCY_CUDA_TRY(cudaMemsetAsync(flags.p, 0, sizeof(unsigned), sbp.stream));
+    if (h & FAULT_NONFINITE) {
+      set_error("non-finite value in the fault root bracket or state rate");
+      return SCY_ERR_NONFINITE;
+    }
+    set_error("rootFinder BracketedNewton did not converge within %d iterations", fp.max_its);
+    return SCY_ERR_ROOT_NOCONV;
+  }
+  return SCY_OK;
+}
+
+int QDContext::d_dt(double t, const double* var, double* f) {
+  cudaStream_t s = sbp.stream;
+  const int tb = 256, gb = (Nz + tb - 1) / tb;
+  qd_bc_kernel<<<gb, tb, 0, s>>>(var, Nz, t, vL, 1.0 / fts, bcL_from_slip, bcR_remote, bcRShift.as<double>(),
+                                 bcL.as<double>(), bcR.as<double>());
+  SCY_LAUNCH_CHECK();
+  SCY_TRY(sbp.set_rhs(bcL.as<double>(), bcR.as<double>(), bcT.as<double>(), bcB.as<double>(), rhs.as<double>()));
+  scy_solve_opts o = solve_opts;
+  o.nonzero_guess = 1;  // the previous stage's displacement is the initial guess
+  scy_solve_stats st{};
+  SCY_TRY(sbp.solve(rhs.as<double>(), u.as<double>(), o, st));
+  n_solve_its += st.iterations;
+  n_solves += 1;
+  last_rnorm = st.rnorm;
+  qd_fault_kernel<<<gb, tb, 0, s>>>(sbp.fine->dev, u.as<double>(), fp, var, f, slipVel.as<double>(),
+                                    tauQSP.as<double>(), tauP.as<double>(), strength.as<double>(),
+                                    flags.as<unsigned>(), fault_its.as<unsigned long long>());
+  SCY_LAUNCH_CHECK();
+  ++n_d_dt;
+  return SCY_OK;
+}
+
+// ---------------------------------------------------------------------------
+int QDContext::steady_state_guess(std::vector<double>& psi, int keep_psi, std::vector<double>& slip) {
+  cudaStream_t s = sbp.stream;
+  // Fault::guessSS / computePsiSS (fault.cpp:619-672)
+  std::vector<double> tau(Nz), vel(Nz, vL);
+  for (int i = 0; i < Nz; ++i) {
+    if (!keep_psi) psi[i] = f0 - h_b[i] * std::log(std::fabs(vL) / v0);
+    tau[i] = h_sN[i] * h_a[i] * std::asinh(0.5 * vL * std::exp(psi[i] / h_a[i]) / v0);
+  }
+  SCY_CUDA_TRY(cudaMemcpyAsync(slipVel.p, vel.data(), Nz * 8, cudaMemcpyHostToDevice, s));
+  // solve with a traction (Neumann) condition at the fault, bcL = tau
+  // (strikeSlip_linearElastic_qd.cpp:60-62, :895-930)
+  const int saved[4] = {sbp.bc[0], sbp.bc[1], sbp.bc[2], sbp.bc[3]};
+  SCY_TRY(sbp.change_bc(saved[0], saved[1], SCY_BC_NEUMANN, saved[3]));
+  std::vector<double> zeros((size_t)std::max(Ny, Nz), 0.0);
+  SCY_CUDA_TRY(cudaMemcpyAsync(bcL.p, tau.data(), Nz * 8, cudaMemcpyHostToDevice, s));
+  SCY_CUDA_TRY(cudaMemcpyAsync(bcR.p, zeros.data(), Nz * 8, cudaMemcpyHostToDevice, s));
+  SCY_TRY(sbp.set_rhs(bcL.as<double>(), bcR.as<double>(), bcT.as<double>(), bcB.as<double>(), rhs.as<double>()));
+  scy_solve_opts o = solve_opts;
+  o.nonzero_guess = 0;
+  o.max_its = std::max(o.max_its, 500);
+  scy_solve_stats st{};
+  int rc = sbp.solve(rhs.as<double>(), u.as<double>(), o, st);
+  if (rc != SCY_OK) {
+    sbp.change_bc(saved[0], saved[1], saved[2], saved[3]);
+    return rc;
+  }
+  std::vector<double> hu((size_t)N);
+  SCY_CUDA_TRY(cudaMemcpyAsync(hu.data(), u.p, N * 8, cudaMemcpyDeviceToHost, s));
+  SCY_CUDA_TRY(cudaStreamSynchronize(s));
+  // solveSSb (strikeSlip_linearElastic_qd.cpp:934-1006): shift u to be
+  // non-negative, take bcRShift from y = Ly and slip from y = 0
+  double mn = *std::min_element(hu.begin(), hu.end());
+  if (mn < 0) {
+    double add = std::fabs(mn);
+    for (auto& v : hu) v += add;
+  }
+  std::vector<double> shift(hu.end() - Nz, hu.end()), uL(hu.begin(), hu.begin() + Nz);
+  slip.resize(Nz);
+  for (int i = 0; i < Nz; ++i) slip[i] = uL[i] * fts;
+  SCY_CUDA_TRY(cudaMemcpyAsync(u.p, hu.data(), N * 8, cudaMemcpyHostToDevice, s));
+  SCY_CUDA_TRY(cudaMemcpyAsync(bcRShift.p, shift.data(), Nz * 8, cudaMemcpyHostToDevice, s));
+  SCY_CUDA_TRY(cudaMemcpyAsync(bcR.p, shift.data(), Nz * 8, cudaMemcpyHostToDevice, s));
+  SCY_CUDA_TRY(cudaMemcpyAsync(bcL.p, uL.data(), Nz * 8, cudaMemcpyHostToDevice, s));
+  SCY_CUDA_TRY(cudaStreamSynchronize(s));
+  SCY_TRY(sbp.change_bc(saved[0], saved[1], saved[2], saved[3]));
+  return SCY_OK;
+}
+
+double QDContext::compute_min_dt(const std::vector<double>& cs, double Ly, double Lz) const {
+  const LevelHost& h = sbp.hosts[0];
+  double m = INFINITY;
+  const double ry = 1.0 / (Ny - 1), rz_ = 1.0 / (Nz - 1);
+  for (long i = 0; i < N; ++i) {
+    double dy = h.grid_type == 1 ? h.yq[i] * ry : Ly / (Ny - 1.0);
+    double dz = h.grid_type == 1 ? h.zr[i] * rz_ : Lz / (Nz - 1.0);
+    m = std::min(m, std::min(dy / cs[i], dz / cs[i]));
+  }
+  return m;
+}
+
+double QDContext::compute_step_size(double totErr) {
+  const double ord = ode.method == SCY_RK32 ? 3.0 : 4.0;
+  const double kappa = 0.9;
+  double ratio;
+  if (ode.control == SCY_CTRL_P) {
+    ratio = kappa * std::pow(totTol / totErr, 1.0 / (1.0 + ord));
+  } else {
+    const double alpha = 0.49 / ord, beta = 0.34 / ord, gamma = 0.1 / ord;
+    if (stepCount < 4)
+      ratio = kappa * std::pow(totTol / totErr, 1.0 / (1.0 + ord));
+    else
+      ratio = kappa * std::pow(totTol / totErr, alpha) * std::pow(errA[0] / totTol, beta) *
+              std::pow(totTol / errA[1], gamma);
+  }
+  double dt = ratio * deltaT;
+  dt = std::min(deltaT * 5.0, dt);
+  dt = std::min(ode.max_dt, dt);
+  dt = std::max(ode.min_dt, dt);
+  if (ode.min_dt == dt)
+    ++numMin;
+  else if (ode.max_dt == dt)
+    ++numMax;
+  return dt;
+}
+
+int QDContext::compute_error(const double* lo, const double* hi, double* err) {
+  cudaStream_t s = sbp.stream;
+  rk_error_kernel<<<1, 1024, 0, s>>>(lo, hi, Nz, errbuf.as<double>());
+  SCY_LAUNCH_CHECK();
+  double h[6];
+  SCY_CUDA_TRY(cudaMemcpyAsync(h, errbuf.p, sizeof(h), cudaMemcpyDeviceToHost, s));
+  SCY_CUDA_TRY(cudaStreamSynchronize(s));
+  double tot = 0.0;
+  for (int i = 0; i < ode.n_err; ++i) {
+    int key = ode.err_keys[i];
+    double scale = ode.err_scale[i];
+    double ss = h[key * 3 + 0], sh = h[key * 3 + 1], mx = h[key * 3 + 2];
+    if (ode.norm == SCY_NORM_L2_ABS) {
+      tot += std::sqrt(ss) / (std::sqrt((double)Nz) * scale);
+    } else if (ode.method == SCY_RK32) {
+      tot += std::sqrt(ss) / (std::sqrt(sh) * scale);
+    } else {
+      tot += mx / scale;
+    }
+  }
+  *err = tot;
+  return SCY_OK;
+}
+
+static Combo combo(std::initializer_list<std::pair<const double*, double>> terms) {
+  Combo c{};
+  int i = 0;
+  for (auto& t : terms) {
+    c.f[i] = t.first;
+    c.c[i] = t.second;
+    ++i;
+  }
+  c.nf = i;
+  return c;
+}
+
+// RK vector slots
+enum { V_VAR = 0, V_DVAR, V_K, V_F1, V_F2, V_F3, V_F4, V_F5, V_F6, V_LO, V_HI };
+
+int QDContext::attempt(double dt, double** lo, double** hi) {
+  cudaStream_t s = sbp.stream;
+  const int n = 2 * Nz, tb = 256, gb = (n + tb - 1) / tb;
+  double* var = rk[V_VAR].as<double>();
+  double* f0 = rk[V_DVAR].as<double>();
+  double* k = rk[V_K].as<double>();
+  double* L = rk[V_LO].as<double>();
+  double* H = rk[V_HI].as<double>();
+  const double t = currT;
+  if (ode.method == SCY_RK32) {
+    double* fa = rk[V_F1].as<double>();
+    double* fb = rk[V_F2].as<double>();
+    rk_combine_kernel<<<gb, tb, 0, s>>>(k, var, combo({{f0, 0.5 * dt}}), n);
+    SCY_LAUNCH_CHECK();
+    SCY_TRY(d_dt(t + 0.5 * dt, k, fa));
+    rk_combine_kernel<<<gb, tb, 0, s>>>(k, var, combo({{f0, -dt}, {fa, 2 * dt}}), n);
+    SCY_LAUNCH_CHECK();
+    SCY_TRY(d_dt(t + dt, k, fb));
+    rk_combine_kernel<<<gb, tb, 0, s>>>(L, var, combo({{f0, 0.5 * dt}, {fb, 0.5 * dt}}), n);
+    SCY_LAUNCH_CHECK();
+    rk_combine_kernel<<<gb, tb, 0, s>>>(H, var, combo({{f0, dt / 6.0}, {fa, 2 * dt / 3.0}, {fb, dt / 6.0}}), n);
+    SCY_LAUNCH_CHECK();
+  } else {
+    const double c2 = 1. / 2., c3 = 83. / 250., c4 = 31. / 50., c5 = 17. / 20., c6 = 1.;
+    const double b1 = 82889. / 524892., b3 = 15625. / 83664., b4 = 69875. / 102672., b5 = -2260. / 8211.,
+                 b6 = 1. / 4.;
+    const double hb1 = 4586570599. / 29645900160., hb3 = 178811875. / 945068544.,
+                 hb4 = 814220225. / 1159782912., hb5 = -3700637. / 11593932., hb6 = 61727. / 225920.;
+    const double a21 = 1. / 2., a31 = 13861. / 62500., a32 = 6889. / 62500.;
+    const double a41 = -116923316275. / 2393684061468., a42 = -2731218467317. / 15368042101831.,
+                 a43 = 9408046702089. / 11113171139209.;
+    const double a51 = -451086348788. / 2902428689909., a52 = -2682348792572. / 7519795681897.,
+                 a53 = 12662868775082. / 11960479115383., a54 = 3355817975965. / 11060851509271.;
+    const double a61 = 647845179188. / 3216320057751., a62 = 73281519250. / 8382639484533.,
+                 a63 = 552539513391. / 3454668386233., a64 = 3354512671639. / 8306763924573., a65 = 4040. / 17871.;
+    double* f2 = rk[V_F2].as<double>();
+    double* f3 = rk[V_F3].as<double>();
+    double* f4 = rk[V_F4].as<double>();
+    double* f5 = rk[V_F5].as<double>();
+    double* f6 = rk[V_F6].as<double>();
+    rk_combine_kernel<<<gb, tb, 0, s>>>(k, var, combo({{f0, a21 * dt}}), n);
+    SCY_LAUNCH_CHECK();
+    SCY_TRY(d_dt(t + c2 * dt, k, f2));
+    rk_combine_kernel<<<gb, tb, 0, s>>>(k, var, combo({{f0, a31 * dt}, {f2, a32 * dt}}), n);
+    SCY_LAUNCH_CHECK();
+    SCY_TRY(d_dt(t + c3 * dt, k, f3));
+    rk_combine_kernel<<<gb, tb, 0, s>>>(k, var, combo({{f0, a41 * dt}, {f2, a42 * dt}, {f3, a43 * dt}}), n);
+    SCY_LAUNCH_CHECK();
+    SCY_TRY(d_dt(t + c4 * dt, k, f4));
+    rk_combine_kernel<<<gb, tb, 0, s>>>(k, var,
+                                        combo({{f0, a51 * dt}, {f2, a52 * dt}, {f3, a53 * dt}, {f4, a54 * dt}}), n);
+    SCY_LAUNCH_CHECK();
+    SCY_TRY(d_dt(t + c5 * dt, k, f5));
+    rk_combine_kernel<<<gb, tb, 0, s>>>(
+        k, var, combo({{f0, a61 * dt}, {f2, a62 * dt}, {f3, a63 * dt}, {f4, a64 * dt}, {f5, a65 * dt}}), n);
+    SCY_LAUNCH_CHECK();
+    SCY_TRY(d_dt(t + c6 * dt, k, f6));
+    rk_combine_kernel<<<gb, tb, 0, s>>>(
+        L, var, combo({{f0, hb1 * dt}, {f3, hb3 * dt}, {f4, hb4 * dt}, {f5, hb5 * dt}, {f6, hb6 * dt}}), n);
+    SCY_LAUNCH_CHECK();
+    rk_combine_kernel<<<gb, tb, 0, s>>>(
+        H, var, combo({{f0, b1 * dt}, {f3, b3 * dt}, {f4, b4 * dt}, {f5, b5 * dt}, {f6, b6 * dt}}), n);
+    SCY_LAUNCH_CHECK();
+  }
+  *lo = L;
+  *hi = H;
+  return SCY_OK;
+}
+
+int QDContext::integrate_begin(const scy_ode_opts& o) {
+  ode = o;
+  if (ode.method != SCY_RK32 && ode.method != SCY_RK43) {
+    set_error("unsupported integrator %d", ode.method);
+    return SCY_ERR_ARG;
+  }
+  if (ode.n_err <= 0) {
+    ode.n_err = 2;
+    ode.err_keys[0] = SCY_KEY_PSI;
+    ode.err_keys[1] = SCY_KEY_SLIP;
+    ode.err_scale[0] = ode.err_scale[1] = 1.0;
+  }
+  for (int i = 0; i < ode.n_err; ++i)
+    if (ode.err_keys[i] != SCY_KEY_PSI && ode.err_keys[i] != SCY_KEY_SLIP) {
+      set_error("error index %d names no integrated variable", ode.err_keys[i]);
+      return SCY_ERR_ARG;
+    }
+  totTol = o.tol;
+  currT = o.t0;
+  deltaT = o.init_dt;
+  newDeltaT = o.init_dt;
+  stepCount = 0;
+  numRejected = numMin = numMax = 0;
+  errA[0] = errA[1] = 0.0;
+  if (deltaT == 0) deltaT = (o.t1 - o.t0) / (double)o.max_steps;
+  ode_ready = 1;
+  // first evaluation of the rates (odeSolver.cpp:545)
+  SCY_TRY(d_dt(currT, rk[V_VAR].as<double>(), rk[V_DVAR].as<double>()));
+  return read_flags();
+}
+
+int QDContext::integrate_steps(long nsteps, scy_ode_stats* st) {
+  if (!ode_ready) {
+    set_error("integrate_steps called before integrate_begin");
+    return SCY_ERR_STATE;
+  }
+  cudaStream_t s = sbp.stream;
+  double* var = rk[V_VAR].as<double>();
+  double* dvar = rk[V_DVAR].as<double>();
+  const int n = 2 * Nz;
+  long done_steps = 0;
+  double totErr = 0.0;
+  while (done_steps < nsteps && stepCount < ode.max_steps && currT < ode.t1) {
+    ++stepCount;
+    int attemptCount = 0;
+    double *lo = nullptr, *hi = nullptr;
+    while (attemptCount < 100) {
+      ++attemptCount;
+      if (currT + deltaT > ode.t1) deltaT = ode.t1 - currT;
+      bool forced = forced_pos < forced_dt.size();
+      int forced_accept = 0;
+      if (forced) {
+        deltaT = forced_dt[forced_pos];
+        forced_accept = forced_acc[forced_pos];
+        ++forced_pos;
+      }
+      SCY_TRY(attempt(deltaT, &lo, &hi));
+      SCY_TRY(compute_error(lo, hi, &totErr));
+      SCY_TRY(read_flags());
+      bool acc = ode.method == SCY_RK32 ? (totErr <= totTol) : (totErr < totTol);
+      if (forced) acc = forced_accept != 0;
+      if (record) {
+        log_dt.push_back(deltaT);
+        log_acc.push_back(acc ? 1 : 0);
+      }
+      if (acc) break;
+      double nd = compute_step_size(totErr);
+      if (!forced) deltaT = nd;
+      if (ode.min_dt == deltaT) break;
+      ++numRejected;
+    }
+    // accept the higher-order solution (odeSolver.cpp:599-603, :1148-1152)
+    currT = currT + deltaT;
+    SCY_CUDA_TRY(cudaMemcpyAsync(var, hi, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    SCY_TRY(d_dt(currT, var, dvar));
+    SCY_TRY(read_flags());
+    if (totErr != 0.0) newDeltaT = compute_step_size(totErr);
+    errA[1] = errA[0];
+    errA[0] = totErr;
+    last_dt = deltaT;
+    deltaT = newDeltaT;
+    ++done_steps;
+  }
+  if (st) {
+    st->t = currT;
+    st->dt = last_dt;
+    st->new_dt = newDeltaT;
+    st->step_count = stepCount;
+    st->rejected = numRejected;
+    st->d_dt_evals = n_d_dt;
+    st->solve_its = n_solve_its;
+    st->solves = n_solves;
+    st->errA[0] = errA[0];
+    st->errA[1] = errA[1];
+    st->done = (stepCount >= ode.max_steps || currT >= ode.t1) ? 1 : 0;
+  }
+  return SCY_OK;
+}
+
+}  // namespace scy

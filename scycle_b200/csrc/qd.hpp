@@ -1,0 +1,62 @@
+// Linear-elastic quasi-dynamic strike-slip driver on the device: the d_dt of
+// StrikeSlip_LinearElastic_qd and the adaptive RK32 / RK43 integrators.
+#pragma once
+#include <vector>
+
+#include "fault_dev.cuh"
+#include "sbp_solver.hpp"
+
+namespace scy {
+
+struct QDContext {
+  SbpContext sbp;
+  int Ny = 0, Nz = 0;
+  long N = 0;
+  FaultParams fp{};
+  DevBuf fa, fb, fsN, fDc, feta, flocked, fprestress;
+  DevBuf slipVel, tauQSP, tauP, strength;  // Nz
+  DevBuf bcL, bcR, bcT, bcB, bcRShift;     // boundary data
+  DevBuf rhs, u, sxy;                       // N
+  DevBuf flags;                             // unsigned, fault status bits
+  DevBuf fault_its;                         // unsigned long long, root iterations
+  double vL = 1e-9, fts = 2.0;
+  int bcL_from_slip = 1, bcR_remote = 1;
+  scy_solve_opts solve_opts{};
+  long n_d_dt = 0, n_solve_its = 0, n_solves = 0;
+  double last_rnorm = 0.0;
+
+  // RK integrator state
+  scy_ode_opts ode{};
+  int ode_ready = 0;
+  DevBuf rk[16];  // var, dvar, k/f stage vectors, lo/hi
+  DevBuf errbuf;  // 8 doubles
+  double currT = 0, deltaT = 0, newDeltaT = 0, totTol = 1e-9, last_dt = 0;
+  long stepCount = 0, numRejected = 0, numMin = 0, numMax = 0;
+  double errA[2] = {0, 0};
+  std::vector<double> forced_dt;
+  std::vector<int> forced_acc;
+  size_t forced_pos = 0;
+  std::vector<double> log_dt;
+  std::vector<int> log_acc;
+  int record = 0;
+
+  std::vector<double> h_a, h_b, h_sN;  // host copies for the steady-state guess
+  double f0 = 0.6, v0 = 1e-6;
+
+  int create(const scy_qd_desc& d);
+  // StrikeSlip_LinearElastic_qd::solveSS + solveSSb + Fault::guessSS: fills
+  // psi (unless keep_psi) and slip, updates bcL, bcRShift, slipVel, u.
+  int steady_state_guess(std::vector<double>& psi, int keep_psi, std::vector<double>& slip);
+  // computeMinTimeStep (strikeSlip_linearElastic_qd.cpp:262-322)
+  double compute_min_dt(const std::vector<double>& cs, double Ly, double Lz) const;
+  // f = d_dt(t, var) with var = [psi | slip] and f = [dpsi | dslip] (device, 2*Nz each)
+  int d_dt(double t, const double* var, double* f);
+  int integrate_begin(const scy_ode_opts& o);
+  int integrate_steps(long nsteps, scy_ode_stats* st);
+  double compute_step_size(double totErr);
+  int compute_error(const double* lo, const double* hi, double* err);
+  int attempt(double dt, double** lo, double** hi);
+  int read_flags();
+};
+
+}  // namespace scy

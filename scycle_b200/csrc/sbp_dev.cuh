@@ -275,8 +275,10 @@ __global__ void __launch_bounds__(256) stencil_kernel(LevelDev<T> L, Loader ld, 
     contrib = ep(node, Ax, xv);
   }
   if constexpr (Epi::kReduce) {
-    double tot = block_sum(contrib, red);
-    grid_reduce_finish(tot, partials, counter, red_out, red);
+    if (partials != nullptr) {  // uniform across the grid
+      double tot = block_sum(contrib, red);
+      grid_reduce_finish(tot, partials, counter, red_out, red);
+    }
   }
 }
 

@@ -7,6 +7,7 @@
 // geometric-multigrid V-cycle (rediscretised SBP-SAT operators on coarsened
 // grids, Chebyshev-Jacobi smoothing, bilinear transfer, dense coarsest solve)
 // run in FP64 or FP32.
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstring>
@@ -30,6 +31,46 @@ void set_error(const char* fmt, ...) {
   va_end(ap);
 }
 const char* last_error() { return g_err; }
+
+static std::atomic<long long> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+long long launch_count() { return g_launches.load(); }
+
+// Optional per-launch timing of the stencil kernel (CUDA events around each
+// launch); off unless scy_profile_enable(1) was called.
+struct ProfRec {
+  cudaEvent_t a, b;
+  long long bytes;  // algorithmic bytes: read the operand and mu, write the result
+  int level;
+  int width;        // bytes per value (4 or 8)
+};
+static bool g_prof = false;
+static std::vector<ProfRec> g_recs;
+void profile_enable(int on) { g_prof = on != 0; }
+int profile_collect(int level, int width, double* ms, long long* launches, double* bytes) {
+  double tms = 0, tb = 0;
+  long long nl = 0;
+  for (auto& r : g_recs) {
+    if (cudaEventSynchronize(r.b) != cudaSuccess) {
+      set_error("profile event failed");
+      return SCY_ERR_CUDA;
+    }
+    float m = 0;
+    cudaEventElapsedTime(&m, r.a, r.b);
+    if ((level < 0 || r.level == level) && (width == 0 || r.width == width)) {
+      tms += m;
+      tb += (double)r.bytes;
+      ++nl;
+    }
+    cudaEventDestroy(r.a);
+    cudaEventDestroy(r.b);
+  }
+  g_recs.clear();
+  *ms = tms;
+  *launches = nl;
+  *bytes = tb;
+  return SCY_OK;
+}
 
 // ------------------------------------------------------------------------
 // device buffers
@@ -137,12 +178,26 @@ template struct LevelStore<float>;
 static dim3 tile_grid(int Ny, int Nz) { return dim3((Nz + TZ - 1) / TZ, (Ny + TY - 1) / TY); }
 
 template <typename T, class Ld, class Ep>
-static int launch_stencil(const LevelDev<T>& L, Ld ld, Ep ep, Reducer* red, double* out, cudaStream_t s) {
+static int launch_stencil(const LevelDev<T>& L, Ld ld, Ep ep, Reducer* red, double* out, cudaStream_t s,
+                          int level = 0) {
   dim3 g = tile_grid(L.Ny, L.Nz);
   double* parts = red ? red->partials.template as<double>() : nullptr;
   unsigned* cnt = red ? red->counter.template as<unsigned>() : nullptr;
+  ProfRec rec{};
+  if (g_prof) {
+    cudaEventCreate(&rec.a);
+    cudaEventCreate(&rec.b);
+    cudaEventRecord(rec.a, s);
+  }
   stencil_kernel<T, Ld, Ep><<<g, 256, 0, s>>>(L, ld, ep, parts, cnt, out);
   SCY_LAUNCH_CHECK();
+  if (g_prof) {
+    cudaEventRecord(rec.b, s);
+    rec.bytes = 3LL * (long long)sizeof(T) * (long long)L.Ny * L.Nz;
+    rec.level = level;
+    rec.width = (int)sizeof(T);
+    g_recs.push_back(rec);
+  }
   return SCY_OK;
 }
 
@@ -518,11 +573,11 @@ int Multigrid<T>::vcycle(int l, const Tin* b_in, T** x_out, cudaStream_t s) {
   T* xo = xb;
   for (int k = 1; k < nu; ++k) {
     SCY_TRY(launch_stencil<T>(L, LoadPlain<T>{x}, EpiCheb<T>{bl, L.dinv, d, xo, (T)cheb[l][k].c1, (T)cheb[l][k].c2},
-                              nullptr, nullptr, s));
+                              nullptr, nullptr, s, l));
     std::swap(x, xo);
   }
   // residual and restriction
-  SCY_TRY(launch_stencil<T>(L, LoadPlain<T>{x}, EpiResidual<T, T>{bl, r, T(1)}, nullptr, nullptr, s));
+  SCY_TRY(launch_stencil<T>(L, LoadPlain<T>{x}, EpiResidual<T, T>{bl, r, T(1)}, nullptr, nullptr, s, l));
   const LevelDev<T>& C = lev[l + 1]->dev;
   long nc = (long)C.Ny * C.Nz;
   T* bcoarse = work[l + 1].v[3].template as<T>();
@@ -539,11 +594,11 @@ int Multigrid<T>::vcycle(int l, const Tin* b_in, T** x_out, cudaStream_t s) {
   // post-smoothing: the first step folds in the coarse-grid correction
   LoadProlong<T> lp{x, xc, C.Nz, t.jy.template as<int>(), t.jz.template as<int>(), t.wy0.template as<T>(),
                     t.wy1.template as<T>(), t.wz0.template as<T>(), t.wz1.template as<T>()};
-  SCY_TRY(launch_stencil<T>(L, lp, EpiCheb<T>{bl, L.dinv, d, xo, T(0), (T)cheb[l][0].c2}, nullptr, nullptr, s));
+  SCY_TRY(launch_stencil<T>(L, lp, EpiCheb<T>{bl, L.dinv, d, xo, T(0), (T)cheb[l][0].c2}, nullptr, nullptr, s, l));
   std::swap(x, xo);
   for (int k = 1; k < nu; ++k) {
     SCY_TRY(launch_stencil<T>(L, LoadPlain<T>{x}, EpiCheb<T>{bl, L.dinv, d, xo, (T)cheb[l][k].c1, (T)cheb[l][k].c2},
-                              nullptr, nullptr, s));
+                              nullptr, nullptr, s, l));
     std::swap(x, xo);
   }
   *x_out = x;

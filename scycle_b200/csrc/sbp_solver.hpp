@@ -12,6 +12,9 @@
 namespace scy {
 
 const char* last_error();
+long long launch_count();
+void profile_enable(int on);
+int profile_collect(int level, int width, double* ms, long long* launches, double* bytes);
 
 struct DevBuf {
   void* p = nullptr;

@@ -1,0 +1,90 @@
+"""Device SBP-SAT operators and elliptic solve vs the oracle (GPU)."""
+import itertools
+
+import numpy as np
+import pytest
+
+from oracle.sbp2d import SbpOps as OracleSbp
+
+pytestmark = pytest.mark.gpu
+
+BCS = [("Dirichlet", "Neumann", "Dirichlet", "Neumann"), ("Neumann", "Dirichlet", "Neumann", "Dirichlet"),
+       ("Dirichlet", "Dirichlet", "Dirichlet", "Dirichlet")]
+
+
+def _case(order, grid, Ny, Nz, seed=0, compat="fullyCompatible", bcs=BCS[0]):
+    rng = np.random.default_rng(seed)
+    Ly, Lz = 30.0, 24.0
+    q = np.repeat(np.arange(Ny) / (Ny - 1), Nz)
+    r = np.tile(np.arange(Nz) / (Nz - 1), Ny)
+    var = grid == "variableGridSpacing"
+    y = Ly * np.sinh(2 * q) / np.sinh(2) if var else None
+    z = Lz * (r + 0.2 * r * r) / 1.2 if var else None
+    mu = 32.04 + 2 * rng.random(Ny * Nz)
+    from scycle_b200.sbp import SbpOps
+    dev = SbpOps(order, Ny, Nz, Ly, Lz, mu, grid=grid, y=y, z=z, compat=compat, bcs=bcs)
+    ora = OracleSbp(order, Ny, Nz, Ly, Lz, mu, grid=grid, y=y, z=z, compat=compat, bcs=bcs)
+    return dev, ora, rng
+
+
+def _rel(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+@pytest.mark.parametrize("order,grid,bcs,shape", list(itertools.product(
+    (2, 4), ("constantGridSpacing", "variableGridSpacing"), BCS, [(37, 45), (101, 67)])))
+def test_apply_A_matches_oracle(order, grid, bcs, shape):
+    dev, ora, rng = _case(order, grid, *shape, bcs=bcs)
+    x = rng.standard_normal(dev.N)
+    out = dev.apply("A", x).cpu().numpy()
+    assert _rel(out, ora.A @ x) <= 1e-13
+
+
+@pytest.mark.parametrize("order,grid", list(itertools.product((2, 4), ("constantGridSpacing", "variableGridSpacing"))))
+def test_first_derivative_ops(order, grid):
+    dev, ora, rng = _case(order, grid, 41, 29)
+    x = rng.standard_normal(dev.N)
+    checks = {"Dy": ora.Dy_Iz @ x, "Dz": ora.Iy_Dz @ x, "muxDy": ora.muxDy(x), "muxDz": ora.muxDz(x),
+              "Dyxmu": ora.Dy_Iz @ (ora.mu_vec * x), "Dzxmu": ora.Iy_Dz @ (ora.mu_vec * x),
+              "H": ora.H @ x, "Hinv": ora.Hinv @ x}
+    for op, ref in checks.items():
+        assert _rel(dev.apply(op, x).cpu().numpy(), ref) <= 1e-13, op
+
+
+@pytest.mark.parametrize("order,grid,bcs", list(itertools.product((2, 4), ("constantGridSpacing", "variableGridSpacing"), BCS)))
+def test_set_rhs_matches_oracle(order, grid, bcs):
+    dev, ora, rng = _case(order, grid, 33, 41, bcs=bcs)
+    bcL, bcR = rng.standard_normal(41), rng.standard_normal(41)
+    bcT, bcB = rng.standard_normal(33), rng.standard_normal(33)
+    out = dev.set_rhs(bcL, bcR, bcT, bcB).cpu().numpy()
+    assert _rel(out, ora.set_rhs(bcL, bcR, bcT, bcB)) <= 1e-13
+
+
+@pytest.mark.parametrize("order,grid,precision", list(itertools.product(
+    (2, 4), ("constantGridSpacing", "variableGridSpacing"), ("fp64", "mixed"))))
+def test_solve_matches_direct_solve(order, grid, precision):
+    import scipy.sparse.linalg as spla
+    dev, ora, rng = _case(order, grid, 101, 81)
+    bcL = np.linspace(0, 1, 81) ** 2
+    bcR = np.full(81, 0.3)
+    rhs = ora.set_rhs(bcL, bcR, np.zeros(101), np.zeros(101))
+    ref = spla.spsolve(ora.A.tocsc(), rhs)
+    u, st = dev.solve(rhs, rtol=1e-12, max_its=300, precision=precision)
+    assert st.converged
+    assert _rel(u.cpu().numpy(), ref) <= 1e-9
+
+
+def test_change_bc_types_rebuilds_operator():
+    dev, ora, rng = _case(4, "constantGridSpacing", 45, 37)
+    dev.change_bc_types("Neumann", "Neumann", "Neumann", "Neumann")
+    ora.change_bc_types("Neumann", "Neumann", "Neumann", "Neumann")
+    x = rng.standard_normal(dev.N)
+    assert _rel(dev.apply("A", x).cpu().numpy(), ora.A @ x) <= 1e-13
+
+
+def test_solve_warm_start_converges_immediately():
+    dev, ora, rng = _case(4, "constantGridSpacing", 65, 65)
+    rhs = ora.set_rhs(np.ones(65), np.zeros(65), np.zeros(65), np.zeros(65))
+    u, st = dev.solve(rhs, rtol=1e-11)
+    u2, st2 = dev.solve(rhs, u0=u, rtol=1e-11)
+    assert st2.iterations == 0 and st2.converged
