@@ -138,6 +138,24 @@ typedef struct scy_solve_stats {
 scy_status scy_sbp_solve(scy_sbp* s, const double* rhs, double* u,
                          const scy_solve_opts* opts, scy_solve_stats* stats);
 
+/* The same solve for callers that cannot allocate device memory.  No
+ * counterpart in the reference.  cudaMalloc/cudaFree can synchronise the
+ * device and fail when another allocator (a framework's caching pool, a
+ * memory manager that reserved the device up front) holds the free memory;
+ * callers in that position, or that cannot afford an implicit device
+ * synchronisation between stages, use this entry point: it allocates
+ * nothing.  Its work vectors live in one fixed device array inside the
+ * library (about 2.6 MB, held by every GPU that loads the library until the
+ * process exits), so it accepts grids of at most 65,536 nodes (e.g.
+ * 256 x 256) and returns SCY_ERR_ARG beyond that.  It preconditions CG with
+ * point Jacobi instead of multigrid, so it needs more iterations; opts and
+ * stats mean what they mean for scy_sbp_solve (opts->precision is ignored:
+ * FP64).  All calls share the array: calls that overlap on the GPU race.
+ * The first call on each device looks up the array's address with that
+ * device current. */
+scy_status scy_sbp_solve_noalloc(scy_sbp* s, const double* rhs, double* u,
+                                 const scy_solve_opts* opts, scy_solve_stats* stats);
+
 /* Grid facts for callers (levels of the multigrid hierarchy, sizes). */
 scy_status scy_sbp_info(scy_sbp* s, int* Ny, int* Nz, int* n_levels);
 

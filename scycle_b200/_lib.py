@@ -66,6 +66,7 @@ def lib():
         L.scy_sbp_apply.argtypes = [vp, C.c_int, vp, vp]
         L.scy_sbp_set_rhs.argtypes = [vp, vp, vp, vp, vp, vp]
         L.scy_sbp_solve.argtypes = [vp, vp, vp, C.POINTER(SolveOpts), C.POINTER(SolveStats)]
+        L.scy_sbp_solve_noalloc.argtypes = [vp, vp, vp, C.POINTER(SolveOpts), C.POINTER(SolveStats)]
         L.scy_sbp_info.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.scy_grid_host_apply.argtypes = [C.POINTER(GridDesc), dptr, dptr]
         L.scy_launch_count.restype = C.c_longlong

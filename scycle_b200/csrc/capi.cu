@@ -117,6 +117,22 @@ scy_status scy_sbp_solve(scy_sbp* s, const double* rhs, double* u, const scy_sol
   return st;
 }
 
+scy_status scy_sbp_solve_noalloc(scy_sbp* s, const double* rhs, double* u, const scy_solve_opts* opts,
+                                 scy_solve_stats* stats) {
+  if (!s || !rhs || !u || !opts) {
+    scy::set_error("scy_sbp_solve_noalloc: NULL argument");
+    return SCY_ERR_ARG;
+  }
+  if (opts->max_its < 1 || !(opts->rtol >= 0.0) || !(opts->atol >= 0.0)) {
+    scy::set_error("scy_sbp_solve_noalloc: invalid options");
+    return SCY_ERR_ARG;
+  }
+  scy_solve_stats tmp{};
+  int st = s->ctx.solve_noalloc(rhs, u, *opts, tmp);
+  if (stats) *stats = tmp;
+  return st;
+}
+
 scy_status scy_sbp_info(scy_sbp* s, int* Ny, int* Nz, int* n_levels) {
   if (!s) return SCY_ERR_ARG;
   if (Ny) *Ny = s->ctx.desc.Ny;

@@ -114,6 +114,7 @@ struct SbpContext {
   int apply(int op, const double* in, double* out);
   int set_rhs(const double* bcL, const double* bcR, const double* bcT, const double* bcB, double* rhs);
   int solve(const double* rhs, double* u, const scy_solve_opts& o, scy_solve_stats& st);
+  int solve_noalloc(const double* rhs, double* u, const scy_solve_opts& o, scy_solve_stats& st);
   int change_bc(int R, int T, int L, int B);
   template <typename T>
   int ensure_mg(std::unique_ptr<Multigrid<T>>& mg);
