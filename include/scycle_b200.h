@@ -114,23 +114,35 @@ scy_status scy_sbp_set_rhs(scy_sbp* s, const double* bcL, const double* bcR,
                            const double* bcT, const double* bcB, double* rhs);
 
 enum { SCY_PREC_FP64 = 0, SCY_PREC_MIXED = 1 };
+enum {
+  SCY_PC_AUTO = 0, /* fast diagonalisation when the grid metrics and mu are
+                      separable (y depends only on iy, z only on iz, mu
+                      constant), multigrid otherwise */
+  SCY_PC_MG = 1,   /* geometric-multigrid V-cycle */
+  SCY_PC_FD = 2    /* fast diagonalisation of the separable part: four dense
+                      GEMMs per application (tensor cores) */
+};
 
 typedef struct scy_solve_opts {
   double rtol;       /* stop when ||A u - rhs||_2 <= max(rtol*||rhs||_2, atol) */
   double atol;
   int max_its;       /* PCG iteration cap */
-  int precision;     /* SCY_PREC_FP64: FP64 multigrid; SCY_PREC_MIXED: FP32
-                        multigrid preconditioner inside FP64 CG with FP64
-                        true-residual refinement */
+  int precision;     /* SCY_PREC_FP64: FP64 preconditioner; SCY_PREC_MIXED:
+                        FP32 preconditioner inside FP64 CG with an FP64
+                        true-residual check */
   int nonzero_guess; /* 1: start from the incoming u (KSPSetInitialGuessNonzero) */
   int check_every;   /* residual read-back interval in iterations (>= 1) */
+  int precond;       /* SCY_PC_* */
+  int verify;        /* 1: recompute the true residual A u - rhs after the
+                        last iteration (one more operator application);
+                        0: trust the CG recurrence residual */
 } scy_solve_opts;
 
 typedef struct scy_solve_stats {
   int iterations;
   int converged;
   double rnorm0;     /* ||rhs - A u0|| */
-  double rnorm;      /* final true residual norm */
+  double rnorm;      /* final residual norm (true residual when verify = 1) */
   double bnorm;      /* ||rhs|| */
 } scy_solve_stats;
 
@@ -194,6 +206,10 @@ typedef struct scy_fault_desc {
   double root_tol;         /* absolute residual tolerance (MPa), reference default 1e-12 */
   int max_its;             /* root iteration cap, reference default 1e4 */
   int state_law;           /* SCY_LAW_* */
+  int exact_jacobian;      /* 0: Newton steps use the reference's derivative
+                              expression (fault.cpp:1051), reproducing its
+                              iteration path; 1: the exact derivative (same
+                              root within root_tol, far fewer iterations) */
 } scy_fault_desc;
 
 typedef struct scy_qd_desc {
@@ -286,6 +302,11 @@ scy_status scy_in_problem_field(const char* path, const char* name, double* out,
  * file (pointer members of *grid are set to NULL). */
 scy_status scy_in_problem_info(const char* path, scy_grid_desc* grid, scy_ode_opts* ode, int* state_law,
                                int* guess_ss, double* fault_type_scale);
+
+/* Selects the root finder's derivative: 0 the reference's expression, 1 the
+ * exact derivative (see scy_fault_desc.exact_jacobian).  Drivers made by
+ * scy_qd_create_from_in start with the exact derivative. */
+scy_status scy_qd_set_jacobian(scy_qd* q, int exact);
 
 /* Overwrites the integrated state [psi | slip] (host, 2*Nz) between steps.
  * recompute = 1 re-evaluates the rates from it (one d_dt); recompute = 0

@@ -20,6 +20,7 @@ GRID = {"constantGridSpacing": 0, "variableGridSpacing": 1}
 COMPAT = {"fullyCompatible": 0, "compatible": 1}
 OPS = {"A": 0, "Dy": 1, "Dz": 2, "muxDy": 3, "muxDz": 4, "H": 5, "Hinv": 6, "Dyxmu": 7, "Dzxmu": 8}
 PREC = {"fp64": 0, "mixed": 1}
+PRECOND = {"auto": 0, "mg": 1, "fd": 2}
 
 dptr = C.POINTER(C.c_double)
 
@@ -32,7 +33,7 @@ class GridDesc(C.Structure):
 
 class SolveOpts(C.Structure):
     _fields_ = [("rtol", C.c_double), ("atol", C.c_double), ("max_its", C.c_int), ("precision", C.c_int),
-                ("nonzero_guess", C.c_int), ("check_every", C.c_int)]
+                ("nonzero_guess", C.c_int), ("check_every", C.c_int), ("precond", C.c_int), ("verify", C.c_int)]
 
 
 class SolveStats(C.Structure):

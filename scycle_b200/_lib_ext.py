@@ -9,7 +9,7 @@ dptr = C.POINTER(C.c_double)
 class FaultDesc(C.Structure):
     _fields_ = [("Nz", C.c_int), ("a", dptr), ("b", dptr), ("sN", dptr), ("Dc", dptr), ("eta", dptr),
                 ("locked", dptr), ("prestress", dptr), ("f0", C.c_double), ("v0", C.c_double), ("vL", C.c_double),
-                ("root_tol", C.c_double), ("max_its", C.c_int), ("state_law", C.c_int)]
+                ("root_tol", C.c_double), ("max_its", C.c_int), ("state_law", C.c_int), ("exact_jacobian", C.c_int)]
 
 
 class QDDesc(C.Structure):
@@ -52,6 +52,7 @@ def declare(L):
     L.scy_qd_get_problem.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(OdeOpts)]
     L.scy_qd_integrate_begin_from_in.argtypes = [vp]
     L.scy_qd_set_state.argtypes = [vp, dptr, C.c_int]
+    L.scy_qd_set_jacobian.argtypes = [vp, C.c_int]
     L.scy_in_problem_field.argtypes = [C.c_char_p, C.c_char_p, dptr, C.c_long, C.POINTER(C.c_long)]
     L.scy_in_problem_info.argtypes = [C.c_char_p, C.POINTER(S.GridDesc), C.POINTER(OdeOpts), C.POINTER(C.c_int),
                                       C.POINTER(C.c_int), C.POINTER(C.c_double)]

@@ -6,7 +6,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libscycle_b200.so")
-SOURCES = ["capi.cu", "sbp_solver.cu", "sbp_host.cpp", "qd.cu", "infile.cpp", "noalloc.cu"]
+SOURCES = ["capi.cu", "sbp_solver.cu", "sbp_host.cpp", "qd.cu", "infile.cpp", "noalloc.cu", "fdiag.cu"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC", "-Xcompiler", "-O3", "--expt-relaxed-constexpr"]
 
@@ -31,7 +31,7 @@ def build(force=False, verbose=True):
     if not force and not needs_build():
         return LIB
     srcs = [os.path.join(CSRC, s) for s in SOURCES]
-    cmd = [nvcc(), *NVCC_FLAGS, "-shared", "-o", LIB + ".tmp", *srcs, "-lcudart"]
+    cmd = [nvcc(), *NVCC_FLAGS, "-shared", "-o", LIB + ".tmp", *srcs, "-lcudart", "-lcublas", "-lcusolver"]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)

@@ -360,6 +360,12 @@ scy_status scy_qd_integrate_begin_from_in(scy_qd* q) {
   return c.integrate_begin(P.ode);
 }
 
+scy_status scy_qd_set_jacobian(scy_qd* q, int exact) {
+  if (!q) return SCY_ERR_ARG;
+  q->ctx.fp.jacobian = exact ? 1 : 0;
+  return SCY_OK;
+}
+
 scy_status scy_qd_set_state(scy_qd* q, const double* var, int recompute) {
   if (!q || !var) return SCY_ERR_ARG;
   scy::QDContext& c = q->ctx;

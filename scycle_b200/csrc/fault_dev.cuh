@@ -20,36 +20,42 @@ struct FaultParams {
   double f0, v0, vL, root_tol;
   int max_its;
   int state_law;  // 0 aging, 1 slip, 2 constant state
+  int jacobian;   // 0 the reference's derivative expression, 1 the exact derivative
 };
 
 __device__ __forceinline__ double strength_psi(double sN, double psi, double V, double a, double v0) {
   return a * sN * asinh((0.5 * V / v0) * exp(psi / a));
 }
 
-// Residual of tau_qs - eta V = strength(V) and the reference's derivative
-// expression a*sN*V/sqrt(B^2 V^2 + 1) + eta with B = exp(psi/a)/(2 v0)
-// (fault.cpp:1051).  The exact derivative has B in place of V in the
-// numerator; the expression only steers the Newton/bisection choice.
-__device__ __forceinline__ void resid_qd(double V, double tauQS, double eta, double sN, double psi, double a,
-                                         double v0, double& f, double& J) {
-  f = strength_psi(sN, psi, V, a, v0) - (tauQS - eta * V);
+// Residual of tau_qs - eta V = strength(V) and its derivative.  E =
+// exp(psi/a) is computed once per node by the caller.  With exact == 0 the
+// derivative is the reference's expression a*sN*V/sqrt(B^2 V^2 + 1) + eta
+// with B = E/(2 v0) (fault.cpp:1051); the exact derivative has B in place of
+// V in the numerator.  The derivative only steers the Newton / bisection
+// choice: both converge to the same root within the residual tolerance, the
+// reference's expression through many more (mostly bisection) steps.
+__device__ __forceinline__ void resid_qd(double V, double tauQS, double eta, double sN, double E, double a,
+                                         double v0, int exact, double& f, double& J) {
+  f = a * sN * asinh((0.5 * V / v0) * E) - (tauQS - eta * V);
   double A = a * sN;
-  double B = exp(psi / a) / (2.0 * v0);
-  J = A * V / sqrt(B * B * V * V + 1.0) + eta;
+  double B = E / (2.0 * v0);
+  double s = sqrt(B * B * V * V + 1.0);
+  J = (exact ? A * B / s : A * V / s) + eta;
 }
 
 // Safeguarded Newton on [left, right] starting from x0.  Returns the root;
 // sets *its and *ok.  Every loop is bounded by max_its.
 __device__ __forceinline__ double bracketed_newton(double left, double right, double x0, double atol, int max_its,
                                                    double tauQS, double eta, double sN, double psi, double a,
-                                                   double v0, int* its, bool* ok) {
+                                                   double v0, int exact, int* its, bool* ok) {
   double f, fp, fl, fr, dum;
+  const double E = exp(psi / a);
   *its = 0;
   *ok = true;
-  resid_qd(x0, tauQS, eta, sN, psi, a, v0, f, fp);
+  resid_qd(x0, tauQS, eta, sN, E, a, v0, exact, f, fp);
   if (fabs(f) <= atol) return x0;
-  resid_qd(left, tauQS, eta, sN, psi, a, v0, fl, dum);
-  resid_qd(right, tauQS, eta, sN, psi, a, v0, fr, dum);
+  resid_qd(left, tauQS, eta, sN, E, a, v0, exact, fl, dum);
+  resid_qd(right, tauQS, eta, sN, E, a, v0, exact, fr, dum);
   if (!isfinite(fl) || !isfinite(fr)) {
     *ok = false;
     return x0;
@@ -63,7 +69,7 @@ __device__ __forceinline__ double bracketed_newton(double left, double right, do
   }
   double x = x0;
   double dxold = fabs(right - left), dx = dxold;
-  resid_qd(x, tauQS, eta, sN, psi, a, v0, f, fp);
+  resid_qd(x, tauQS, eta, sN, E, a, v0, exact, f, fp);
   int n = 0;
   while (n <= max_its && fabs(f) >= atol) {
     if (((x - right) * fp - f) * ((x - left) * fp - f) > 0.0 || fabs(2.0 * f) > fabs(dxold * fp)) {
@@ -75,7 +81,7 @@ __device__ __forceinline__ double bracketed_newton(double left, double right, do
       dx = f / fp;
       x -= dx;
     }
-    resid_qd(x, tauQS, eta, sN, psi, a, v0, f, fp);
+    resid_qd(x, tauQS, eta, sN, E, a, v0, exact, f, fp);
     if (f < 0.0)
       left = x;
     else

@@ -1,0 +1,254 @@
+// Fast-diagonalisation preconditioner (see fdiag.hpp).
+#include <cusolverDn.h>
+
+#include <cmath>
+#include <vector>
+
+#include "common.cuh"
+#include "fdiag.hpp"
+
+namespace scy {
+
+#define SCY_BLAS_TRY(call)                                                   \
+  do {                                                                       \
+    cublasStatus_t b_ = (call);                                              \
+    if (b_ != CUBLAS_STATUS_SUCCESS) {                                       \
+      ::scy::set_error("%s:%d: %s failed (%d)", __FILE__, __LINE__, #call,   \
+                       (int)b_);                                             \
+      return SCY_ERR_CUDA;                                                   \
+    }                                                                        \
+  } while (0)
+
+namespace {
+
+// Dense 1D operator of one direction with averaged coefficients c1, m31
+// (column-major n x n, symmetric): the y or z part of A restricted to a line,
+// SAT terms included.  Entry (i, l) of L = sum_k Q[i,k] c1_k D[k,l]
+//   - R3T[i,k] w3_k m31_k R3[k,l] - R4T[i,k] w4_k c1_k R4[k,l] + SAT.
+std::vector<double> dense_line_operator(const DirTables& t, const std::vector<double>& c1,
+                                        const std::vector<double>& m31, int bc_lo, int bc_hi) {
+  const int n = t.n;
+  std::vector<double> Lm((size_t)n * n, 0.0);
+  auto at = [&](int i, int l) -> double& { return Lm[(size_t)l * n + i]; };
+  auto band = [&](const std::vector<double>& b, int row, int col) {
+    int off = col - row;
+    if (off < -kHalf || off > kHalf || b.empty()) return 0.0;
+    return b[(size_t)row * kBand + off + kHalf];
+  };
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < kBand; ++j) {
+      int k = i + j - kHalf;
+      if (k < 0 || k >= n) continue;
+      const double q = t.Q[(size_t)i * kBand + j], r3 = t.R3T[(size_t)i * kBand + j],
+                   r4 = t.R4T[(size_t)i * kBand + j];
+      for (int jj = 0; jj < kBand; ++jj) {
+        int l = k + jj - kHalf;
+        if (l < 0 || l >= n) continue;
+        double v = q * c1[k] * band(t.D, k, l) - r3 * t.w3[k] * m31[k] * band(t.R3, k, l) -
+                   r4 * t.w4[k] * c1[k] * band(t.R4, k, l);
+        at(i, l) += v;
+      }
+    }
+  if (bc_lo == 0) {
+    for (int i = 0; i < kBand && i < n; ++i) at(i, 0) += (t.bs0[i] + (i == 0 ? t.alphaD : 0.0)) * c1[0];
+  } else {
+    for (int l = 0; l < n; ++l) at(0, l) += c1[0] * band(t.D, 0, l);
+  }
+  if (bc_hi == 0) {
+    for (int i = std::max(0, n - kBand); i < n; ++i)
+      at(i, n - 1) += (t.bsN[i - (n - kBand)] + (i == n - 1 ? t.alphaD : 0.0)) * c1[n - 1];
+  } else {
+    for (int l = 0; l < n; ++l) at(n - 1, l) -= c1[n - 1] * band(t.D, n - 1, l);
+  }
+  return Lm;
+}
+
+// Generalised eigendecomposition of (-L, M): returns V (column-major,
+// V^T M V = I) and the eigenvalues.
+int gen_eig(std::vector<double>& negL, const std::vector<double>& M, int n, std::vector<double>& V,
+            std::vector<double>& lam, cudaStream_t s) {
+  std::vector<double> S((size_t)n * n);
+  for (int l = 0; l < n; ++l)
+    for (int i = 0; i < n; ++i) {
+      double a = negL[(size_t)l * n + i], b = negL[(size_t)i * n + l];
+      S[(size_t)l * n + i] = 0.5 * (a + b) / std::sqrt(M[i] * M[l]);
+    }
+  cusolverDnHandle_t h = nullptr;
+  if (cusolverDnCreate(&h) != CUSOLVER_STATUS_SUCCESS) {
+    set_error("cusolverDnCreate failed");
+    return SCY_ERR_CUDA;
+  }
+  cusolverDnSetStream(h, s);
+  DevBuf dS, dW, dinfo, dwork;
+  int rc = SCY_OK;
+  do {
+    if ((rc = dS.alloc(S.size() * 8)) != SCY_OK) break;
+    if ((rc = dW.alloc((size_t)n * 8)) != SCY_OK) break;
+    if ((rc = dinfo.alloc(16)) != SCY_OK) break;
+    if (cudaMemcpyAsync(dS.p, S.data(), S.size() * 8, cudaMemcpyHostToDevice, s) != cudaSuccess) {
+      rc = SCY_ERR_CUDA;
+      set_error("copy to the eigensolver failed");
+      break;
+    }
+    int lwork = 0;
+    if (cusolverDnDsyevd_bufferSize(h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, dS.as<double>(), n,
+                                    dW.as<double>(), &lwork) != CUSOLVER_STATUS_SUCCESS) {
+      rc = SCY_ERR_CUDA;
+      set_error("cusolverDnDsyevd_bufferSize failed");
+      break;
+    }
+    if ((rc = dwork.alloc((size_t)std::max(lwork, 1) * 8)) != SCY_OK) break;
+    if (cusolverDnDsyevd(h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, dS.as<double>(), n,
+                         dW.as<double>(), dwork.as<double>(), lwork, dinfo.as<int>()) != CUSOLVER_STATUS_SUCCESS) {
+      rc = SCY_ERR_CUDA;
+      set_error("cusolverDnDsyevd failed");
+      break;
+    }
+    int info = 0;
+    lam.resize(n);
+    cudaMemcpyAsync(&info, dinfo.p, sizeof(int), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(lam.data(), dW.p, (size_t)n * 8, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(S.data(), dS.p, S.size() * 8, cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) {
+      rc = SCY_ERR_CUDA;
+      set_error("eigensolver synchronisation failed");
+      break;
+    }
+    if (info != 0) {
+      rc = SCY_ERR_ARG;
+      set_error("eigensolver reported info = %d", info);
+      break;
+    }
+  } while (0);
+  cusolverDnDestroy(h);
+  if (rc != SCY_OK) return rc;
+  V.resize((size_t)n * n);
+  for (int c = 0; c < n; ++c)
+    for (int i = 0; i < n; ++i) V[(size_t)c * n + i] = S[(size_t)c * n + i] / std::sqrt(M[i]);
+  return SCY_OK;
+}
+
+template <typename T>
+__global__ void scale_by_kernel(T* __restrict__ x, const T* __restrict__ s, long n) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) x[i] *= s[i];
+}
+
+__global__ void to_f32_kernel(const double* __restrict__ a, float* __restrict__ b, long n) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    b[i] = (float)a[i];
+}
+
+template <typename T>
+int upload_as(DevBuf& b, const std::vector<double>& v, cudaStream_t s) {
+  std::vector<T> t(v.begin(), v.end());
+  SCY_TRY(b.alloc(t.size() * sizeof(T)));
+  SCY_CUDA_TRY(cudaMemcpyAsync(b.p, t.data(), t.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+  SCY_CUDA_TRY(cudaStreamSynchronize(s));
+  return SCY_OK;
+}
+}  // namespace
+
+FDPrecond::~FDPrecond() {
+  if (blas) cublasDestroy(blas);
+}
+
+int FDPrecond::build(const LevelHost& L, cudaStream_t s) {
+  Ny = L.Ny;
+  Nz = L.Nz;
+  const size_t N = (size_t)Ny * Nz;
+  // averaged 1D coefficients and weights
+  std::vector<double> cy1(Ny, 0), m3y1(Ny, 0), My(Ny, 0), cz1(Nz, 0), m3z1(Nz, 0), Mz(Nz, 0);
+  for (int iy = 0; iy < Ny; ++iy)
+    for (int iz = 0; iz < Nz; ++iz) {
+      size_t i = (size_t)iy * Nz + iz;
+      cy1[iy] += L.cy[i] / Nz;
+      m3y1[iy] += L.m3y[i] / Nz;
+      My[iy] += L.wz[i] / Nz;
+      cz1[iz] += L.cz[i] / Ny;
+      m3z1[iz] += L.m3z[i] / Ny;
+      Mz[iz] += L.wy[i] / Ny;
+    }
+  std::vector<double> Ly = dense_line_operator(L.ty, cy1, m3y1, L.bc[2], L.bc[0]);
+  std::vector<double> Lz = dense_line_operator(L.tz, cz1, m3z1, L.bc[1], L.bc[3]);
+  for (auto& v : Ly) v = -v;
+  for (auto& v : Lz) v = -v;
+  std::vector<double> Vyh, Vzh, ly, lz;
+  SCY_TRY(gen_eig(Ly, My, Ny, Vyh, ly, s));
+  SCY_TRY(gen_eig(Lz, Mz, Nz, Vzh, lz, s));
+  std::vector<double> il(N);
+  for (int iy = 0; iy < Ny; ++iy)
+    for (int iz = 0; iz < Nz; ++iz) {
+      double d = ly[iy] + lz[iz];
+      if (!(d > 0)) {
+        set_error("separable operator is singular (eigenvalue sum %g): no Dirichlet boundary?", d);
+        return SCY_ERR_ARG;
+      }
+      il[(size_t)iy * Nz + iz] = 1.0 / d;
+    }
+  SCY_TRY(upload_as<double>(Vy, Vyh, s));
+  SCY_TRY(upload_as<double>(Vz, Vzh, s));
+  SCY_TRY(upload_as<double>(inv_lam, il, s));
+  SCY_TRY(upload_as<float>(Vy32, Vyh, s));
+  SCY_TRY(upload_as<float>(Vz32, Vzh, s));
+  SCY_TRY(upload_as<float>(inv_lam32, il, s));
+  SCY_TRY(t1.alloc(N * 8));
+  SCY_TRY(t2.alloc(N * 8));
+  SCY_TRY(t1f.alloc(N * 4));
+  SCY_TRY(t2f.alloc(N * 4));
+  SCY_TRY(r32.alloc(N * 4));
+  if (!blas) SCY_BLAS_TRY(cublasCreate(&blas));
+  ready = 1;
+  return SCY_OK;
+}
+
+int FDPrecond::apply(const double* r, double* z, cudaStream_t s) {
+  SCY_BLAS_TRY(cublasSetStream(blas, s));
+  SCY_BLAS_TRY(cublasSetMathMode(blas, CUBLAS_DEFAULT_MATH));
+  const double one = 1.0, zero = 0.0;
+  double* a = t1.as<double>();
+  double* b = t2.as<double>();
+  const double* vy = Vy.as<double>();
+  const double* vz = Vz.as<double>();
+  // column-major views: body vector = Nz x Ny matrix (z fastest)
+  SCY_BLAS_TRY(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, Nz, Ny, Nz, &one, vz, Nz, r, Nz, &zero, a, Nz));
+  SCY_BLAS_TRY(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, Nz, Ny, Ny, &one, a, Nz, vy, Ny, &zero, b, Nz));
+  count_launch();
+  count_launch();
+  long n = (long)Ny * Nz;
+  scale_by_kernel<double><<<grid_for(n), 256, 0, s>>>(b, inv_lam.as<double>(), n);
+  SCY_LAUNCH_CHECK();
+  SCY_BLAS_TRY(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_T, Nz, Ny, Ny, &one, b, Nz, vy, Ny, &zero, a, Nz));
+  SCY_BLAS_TRY(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, Nz, Ny, Nz, &one, vz, Nz, a, Nz, &zero, z, Nz));
+  count_launch();
+  count_launch();
+  return SCY_OK;
+}
+
+int FDPrecond::apply32(const double* r, float* z, cudaStream_t s) {
+  SCY_BLAS_TRY(cublasSetStream(blas, s));
+  // full FP32 GEMMs: TF32 inputs (10-bit mantissa) cost CG two to three
+  // times the iterations on these operators
+  SCY_BLAS_TRY(cublasSetMathMode(blas, CUBLAS_DEFAULT_MATH));
+  const float one = 1.0f, zero = 0.0f;
+  long n = (long)Ny * Nz;
+  float* rf = r32.as<float>();
+  to_f32_kernel<<<grid_for(n), 256, 0, s>>>(r, rf, n);
+  SCY_LAUNCH_CHECK();
+  float* a = t1f.as<float>();
+  float* b = t2f.as<float>();
+  const float* vy = Vy32.as<float>();
+  const float* vz = Vz32.as<float>();
+  SCY_BLAS_TRY(cublasSgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, Nz, Ny, Nz, &one, vz, Nz, rf, Nz, &zero, a, Nz));
+  SCY_BLAS_TRY(cublasSgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, Nz, Ny, Ny, &one, a, Nz, vy, Ny, &zero, b, Nz));
+  count_launch();
+  count_launch();
+  scale_by_kernel<float><<<grid_for(n), 256, 0, s>>>(b, inv_lam32.as<float>(), n);
+  SCY_LAUNCH_CHECK();
+  SCY_BLAS_TRY(cublasSgemm(blas, CUBLAS_OP_N, CUBLAS_OP_T, Nz, Ny, Ny, &one, b, Nz, vy, Ny, &zero, a, Nz));
+  SCY_BLAS_TRY(cublasSgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, Nz, Ny, Nz, &one, vz, Nz, a, Nz, &zero, z, Nz));
+  count_launch();
+  count_launch();
+  return SCY_OK;
+}
+
+}  // namespace scy

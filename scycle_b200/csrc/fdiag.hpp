@@ -1,0 +1,35 @@
+// Fast-diagonalisation preconditioner for K = -A.
+//
+// K is approximated by its separable part K_sep = (-Ly) (x) Mz + My (x) (-Lz)
+// with 1D SBP-SAT operators Ly, Lz (coefficients averaged across the other
+// direction) and diagonal weights My = Hy*yq, Mz = Hz*zr.  For constant mu
+// on a grid whose y depends only on iy and z only on iz, K_sep differs from
+// K only in the flattened-index mu3 average of the last z column.  With the
+// generalised eigendecompositions (-Ly) Vy = My Vy Ly_lambda (Vy^T My Vy = I)
+// and likewise for z,
+//     K_sep^-1 = (Vy (x) Vz) diag(1/(ly_i + lz_j)) (Vy^T (x) Vz^T),
+// applied to a body vector R (Ny x Nz, z fastest) as four dense GEMMs on
+// the tensor cores: Z = Vy [ (Vy^T R Vz) ./ (ly_i + lz_j) ] Vz^T.
+#pragma once
+#include <cublas_v2.h>
+
+#include "sbp_solver.hpp"
+
+namespace scy {
+
+struct FDPrecond {
+  int Ny = 0, Nz = 0;
+  int ready = 0;
+  cublasHandle_t blas = nullptr;
+  DevBuf Vy, Vz, inv_lam, t1, t2;          // FP64
+  DevBuf Vy32, Vz32, inv_lam32, t1f, t2f;  // FP32 copies for the mixed path
+  DevBuf r32;                              // FP32 copy of the residual
+  ~FDPrecond();
+  int build(const LevelHost& L, cudaStream_t s);
+  // z = K_sep^-1 r (FP64)
+  int apply(const double* r, double* z, cudaStream_t s);
+  // z = K_sep^-1 r with FP32 GEMMs (z in FP32)
+  int apply32(const double* r, float* z, cudaStream_t s);
+};
+
+}  // namespace scy

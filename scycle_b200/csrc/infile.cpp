@@ -375,6 +375,7 @@ void load_qd_problem(const std::string& path, QDProblem& P) {
   d.fault.root_tol = rootTol;
   d.fault.max_its = 10000;
   d.fault.state_law = stateLaw == "agingLaw" ? SCY_LAW_AGING : stateLaw == "slipLaw" ? SCY_LAW_SLIP : SCY_LAW_CONSTANT;
+  d.fault.exact_jacobian = 1;
   d.fault_type_scale = fts;
   d.bcL_from_slip = 1;
   d.bcR_remote = bcRType == "remoteLoading" ? 1 : 0;

@@ -91,7 +91,8 @@ __global__ void na_update_kernel(double* __restrict__ x, double* __restrict__ r,
                                  const double* __restrict__ pq, long n, double* partials, unsigned* counter,
                                  double* out) {
   __shared__ double sh[32];
-  const double alpha = *rz / *pq;
+  const double pqv = *pq;
+  const double alpha = pqv != 0.0 ? *rz / pqv : 0.0;
   double acc = 0.0;
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
     x[i] += alpha * p[i];

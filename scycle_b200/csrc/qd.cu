@@ -65,7 +65,8 @@ __global__ void qd_fault_kernel(LevelDev<double> L, const double* __restrict__ u
     } else {
       int its = 0;
       bool ok = true;
-      V = bracketed_newton(left, right, slipVel[iz], fp.root_tol, fp.max_its, tq, eta, sN, psi, a, fp.v0, &its, &ok);
+      V = bracketed_newton(left, right, slipVel[iz], fp.root_tol, fp.max_its, tq, eta, sN, psi, a, fp.v0,
+                           fp.jacobian, &its, &ok);
       atomicAdd(its_total, (unsigned long long)its);
       if (!ok) atomicOr(flags, (unsigned)FAULT_ROOT_NOCONV);
     }
@@ -213,6 +214,7 @@ int QDContext::create(const scy_qd_desc& d) {
   fp.root_tol = f.root_tol;
   fp.max_its = f.max_its;
   fp.state_law = f.state_law;
+  fp.jacobian = f.exact_jacobian ? 1 : 0;
   vL = d.vL;
   fts = d.fault_type_scale;
   if (!(fts > 0)) {
@@ -250,7 +252,7 @@ int QDContext::read_flags() {
 
 int QDContext::d_dt(double t, const double* var, double* f) {
   cudaStream_t s = sbp.stream;
-  const int tb = 256, gb = (Nz + tb - 1) / tb;
+  const int tb = 64, gb = (Nz + tb - 1) / tb;
   qd_bc_kernel<<<gb, tb, 0, s>>>(var, Nz, t, vL, 1.0 / fts, bcL_from_slip, bcR_remote, bcRShift.as<double>(),
                                  bcL.as<double>(), bcR.as<double>());
   SCY_LAUNCH_CHECK();

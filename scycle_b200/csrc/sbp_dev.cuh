@@ -29,6 +29,12 @@ struct DirDev {
   T bs0[BAND], bsN[BAND];
   T alphaD;
   int bc_lo, bc_hi;  // 0 Dirichlet, 1 Neumann (y: lo=L, hi=R; z: lo=T, hi=B)
+  // Interior stencil of the order-4 operators (rows 4 .. n-6 of the stage-1
+  // operators, 6 .. n-8 of the stage-2 operators), copied from an interior
+  // row of the tables: D at offsets -2,-1,1,2; D3 at -1..2; D4 at -2..2; Q at
+  // -2,-1,1,2; D3^T at -2..1; D4^T at -2..2; and the interior R weights.
+  int fast;  // 1 when these are valid (order 4, n >= 17)
+  T cD[4], cR3[4], cR4[5], cQ[4], cR3T[4], cR4T[5], cw3, cw4;
 };
 
 template <typename T>
@@ -58,7 +64,8 @@ struct LoadPUpdate {
   __device__ __forceinline__ double operator()(long node, int, int) const {
     double zv = (double)z[node];
     if (first) return zv;
-    double beta = *rz_new / *rz_old;
+    const double ro = *rz_old;
+    const double beta = ro != 0.0 ? *rz_new / ro : 0.0;  // a converged residual gives rz = 0
     return zv + beta * pold[node];
   }
 };
@@ -177,6 +184,69 @@ __global__ void __launch_bounds__(256) stencil_kernel(LevelDev<T> L, Loader ld, 
     xs_z[i] = v;
   }
   __syncthreads();
+  // Interior tiles (every stage-1 row in the interior band of both
+  // directions) use the constant interior stencil from the kernel parameters.
+  const bool fast = L.y.fast && L.z.fast && y0 - HG >= 4 && y0 + TY + HG - 1 <= Ny - 6 && z0 - HG >= 4 &&
+                    z0 + TZ + HG - 1 <= Nz - 6;
+  if (fast) {
+    for (int i = tid; i < (TY + 2 * HG) * TZ; i += blockDim.x) {
+      int r = i / TZ, c = i % TZ;
+      int k = y0 - HG + r, iz = z0 + c;
+      const T* x = xs_y + (r + HALF) * TZ + c;  // row k
+      long node = (long)k * Nz + iz;
+      T cyv = L.cy[node];
+      T d1 = L.y.cD[0] * x[-2 * TZ] + L.y.cD[1] * x[-TZ] + L.y.cD[2] * x[TZ] + L.y.cD[3] * x[2 * TZ];
+      T d3 = L.y.cR3[0] * x[-TZ] + L.y.cR3[1] * x[0] + L.y.cR3[2] * x[TZ] + L.y.cR3[3] * x[2 * TZ];
+      T d4 = L.y.cR4[0] * x[-2 * TZ] + L.y.cR4[1] * x[-TZ] + L.y.cR4[2] * x[0] + L.y.cR4[3] * x[TZ] +
+             L.y.cR4[4] * x[2 * TZ];
+      gy[0][i] = cyv * d1;
+      gy[1][i] = L.y.cw3 * L.m3y[node] * d3;
+      gy[2][i] = L.y.cw4 * cyv * d4;
+    }
+    for (int i = tid; i < TY * (TZ + 2 * HG); i += blockDim.x) {
+      int r = i / (TZ + 2 * HG), c = i % (TZ + 2 * HG);
+      int iy = y0 + r, k = z0 - HG + c;
+      const T* x = xs_z + r * (TZ + 2 * HX) + c + HALF;  // column k
+      long node = (long)iy * Nz + k;
+      T czv = L.cz[node];
+      T d1 = L.z.cD[0] * x[-2] + L.z.cD[1] * x[-1] + L.z.cD[2] * x[1] + L.z.cD[3] * x[2];
+      T d3 = L.z.cR3[0] * x[-1] + L.z.cR3[1] * x[0] + L.z.cR3[2] * x[1] + L.z.cR3[3] * x[2];
+      T d4 = L.z.cR4[0] * x[-2] + L.z.cR4[1] * x[-1] + L.z.cR4[2] * x[0] + L.z.cR4[3] * x[1] + L.z.cR4[4] * x[2];
+      gz[0][i] = czv * d1;
+      gz[1][i] = L.z.cw3 * L.m3z[node] * d3;
+      gz[2][i] = L.z.cw4 * czv * d4;
+    }
+    __syncthreads();
+    const int ty = tid / TZ, tz = tid % TZ;
+    const int iy = y0 + ty, iz = z0 + tz;
+    const long node = (long)iy * Nz + iz;
+    const int gc = (ty + HG) * TZ + tz;  // g row of iy
+    const T* g0 = gy[0] + gc;
+    const T* g1 = gy[1] + gc;
+    const T* g2 = gy[2] + gc;
+    T sy = L.y.cQ[0] * g0[-2 * TZ] + L.y.cQ[1] * g0[-TZ] + L.y.cQ[2] * g0[TZ] + L.y.cQ[3] * g0[2 * TZ];
+    sy -= L.y.cR3T[0] * g1[-2 * TZ] + L.y.cR3T[1] * g1[-TZ] + L.y.cR3T[2] * g1[0] + L.y.cR3T[3] * g1[TZ];
+    sy -= L.y.cR4T[0] * g2[-2 * TZ] + L.y.cR4T[1] * g2[-TZ] + L.y.cR4T[2] * g2[0] + L.y.cR4T[3] * g2[TZ] +
+          L.y.cR4T[4] * g2[2 * TZ];
+    const int zc = ty * (TZ + 2 * HG) + tz + HG;  // g column of iz
+    const T* h0 = gz[0] + zc;
+    const T* h1 = gz[1] + zc;
+    const T* h2 = gz[2] + zc;
+    T sz = L.z.cQ[0] * h0[-2] + L.z.cQ[1] * h0[-1] + L.z.cQ[2] * h0[1] + L.z.cQ[3] * h0[2];
+    sz -= L.z.cR3T[0] * h1[-2] + L.z.cR3T[1] * h1[-1] + L.z.cR3T[2] * h1[0] + L.z.cR3T[3] * h1[1];
+    sz -= L.z.cR4T[0] * h2[-2] + L.z.cR4T[1] * h2[-1] + L.z.cR4T[2] * h2[0] + L.z.cR4T[3] * h2[1] +
+          L.z.cR4T[4] * h2[2];
+    T Ax = L.wy[node] * sy + L.wz[node] * sz;
+    T xv = xs_y[(ty + HX) * TZ + tz];
+    double contrib = ep(node, Ax, xv);
+    if constexpr (Epi::kReduce) {
+      if (partials != nullptr) {
+        double tot = block_sum(contrib, red);
+        grid_reduce_finish(tot, partials, counter, red_out, red);
+      }
+    }
+    return;
+  }
   // stage 1, y direction: rows y0-HG .. y0+TY+HG
   for (int i = tid; i < (TY + 2 * HG) * TZ; i += blockDim.x) {
     int r = i / TZ, c = i % TZ;

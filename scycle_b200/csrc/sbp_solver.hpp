@@ -95,7 +95,11 @@ int build_hierarchy(const scy_grid_desc& g, const std::vector<double>& y, const 
                     const std::vector<double>& mu, const int bc[4], std::vector<LevelHost>& hosts,
                     std::vector<Transfer>& xfer);
 
+struct FDPrecond;
+
 struct SbpContext {
+  SbpContext();
+  ~SbpContext();
   scy_grid_desc desc{};
   std::vector<double> y, z, mu;
   int bc[4] = {0, 1, 0, 1};  // R, T, L, B
@@ -105,9 +109,11 @@ struct SbpContext {
   std::unique_ptr<LevelStore<double>> fine;
   std::unique_ptr<Multigrid<double>> mg64;
   std::unique_ptr<Multigrid<float>> mg32;
+  std::unique_ptr<FDPrecond> fd;
+  int separable = 0;  // metrics and mu separable: fast diagonalisation is exact up to the mu3 column
   Reducer red;
   DevBuf scal;
-  DevBuf cg_r, cg_p[2], cg_q, cg_z;
+  DevBuf cg_r, cg_p[2], cg_q, cg_z, cg_z32;
 
   int create(const scy_grid_desc& g);
   int rebuild();
@@ -118,8 +124,9 @@ struct SbpContext {
   int change_bc(int R, int T, int L, int B);
   template <typename T>
   int ensure_mg(std::unique_ptr<Multigrid<T>>& mg);
-  template <typename T>
-  int pcg(Multigrid<T>& mg, const double* rhs, double* u, const scy_solve_opts& o, scy_solve_stats& st);
+  int ensure_fd();
+  template <typename Tz, class PC>
+  int pcg(PC&& pc, const double* rhs, double* u, const scy_solve_opts& o, scy_solve_stats& st);
 };
 
 }  // namespace scy

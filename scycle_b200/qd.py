@@ -14,17 +14,19 @@ from . import _lib_ext as X
 
 class QD:
     @classmethod
-    def from_in(cls, path, solve_rtol=1e-12, precision="fp64", solve_max_its=300, check_every=1):
+    def from_in(cls, path, solve_rtol=1e-12, precision="fp64", solve_max_its=300, check_every=1, precond="auto",
+                exact_jacobian=True):
         """Driver created by the C++ reader of the reference's .in format."""
         self = cls.__new__(cls)
         self._keep = []
-        o = S.SolveOpts(solve_rtol, 0.0, solve_max_its, S.PREC[precision], 1, check_every)
+        o = S.SolveOpts(solve_rtol, 0.0, solve_max_its, S.PREC[precision], 1, check_every, S.PRECOND[precond])
         h = C.c_void_p()
         S.check(S.lib().scy_qd_create_from_in(path.encode(), C.byref(o), C.byref(h)))
         self.h = h
         ny, nz = C.c_int(), C.c_int()
         self.ode = X.OdeOpts()
         S.check(S.lib().scy_qd_get_problem(h, C.byref(ny), C.byref(nz), C.byref(self.ode)))
+        S.check(S.lib().scy_qd_set_jacobian(h, 1 if exact_jacobian else 0))
         self.Ny, self.Nz, self.N = ny.value, nz.value, ny.value * nz.value
         self.P = None
         return self
@@ -36,7 +38,8 @@ class QD:
         var = np.ascontiguousarray(np.concatenate([psi, slip]), dtype=np.float64)
         S.check(S.lib().scy_qd_set_state(self.h, S.as_dptr(var), 1 if recompute else 0))
 
-    def __init__(self, P, solve_rtol=1e-12, precision="fp64", solve_max_its=300, check_every=1):
+    def __init__(self, P, solve_rtol=1e-12, precision="fp64", solve_max_its=300, check_every=1, precond="auto",
+                 exact_jacobian=True):
         self.P = P
         d = P["domain"]
         Ny, Nz = P["Ny"], P["Nz"]
@@ -59,6 +62,7 @@ class QD:
         f.f0, f.v0, f.vL = P["fault"]["f0"], P["fault"]["v0"], d["vL"]
         f.root_tol, f.max_its = P["fault"]["rootTol"], int(P["fault"]["maxNumIts"])
         f.state_law = X.LAWS[P["driver"]["stateLaw"]]
+        f.exact_jacobian = 1 if exact_jacobian else 0
         q = X.QDDesc()
         q.grid = gdesc
         q.fault = f
@@ -69,7 +73,7 @@ class QD:
         q.vL = s["vL"]
         q.bcL0 = arr(P["bcL0"])
         q.bcRShift = arr(P["bcRShift"])
-        q.solve = S.SolveOpts(solve_rtol, 0.0, solve_max_its, S.PREC[precision], 1, check_every)
+        q.solve = S.SolveOpts(solve_rtol, 0.0, solve_max_its, S.PREC[precision], 1, check_every, S.PRECOND[precond])
         h = C.c_void_p()
         S.check(S.lib().scy_qd_create(C.byref(q), C.byref(h)))
         self.h = h

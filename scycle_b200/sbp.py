@@ -69,11 +69,13 @@ class SbpOps:
         self.sync()
         return out
 
-    def solve(self, rhs, u0=None, rtol=1e-12, atol=0.0, max_its=200, precision="fp64", check_every=1):
+    def solve(self, rhs, u0=None, rtol=1e-12, atol=0.0, max_its=200, precision="fp64", check_every=1,
+              precond="auto"):
         t = self.torch
         b = self._dev(rhs)
         u = t.zeros(self.N, dtype=t.float64, device="cuda") if u0 is None else self._dev(u0).clone()
-        o = S.SolveOpts(rtol, atol, max_its, S.PREC[precision], 0 if u0 is None else 1, check_every)
+        o = S.SolveOpts(rtol, atol, max_its, S.PREC[precision], 0 if u0 is None else 1, check_every,
+                        S.PRECOND[precond], 1)
         st = S.SolveStats()
         t.cuda.synchronize()
         S.check(S.lib().scy_sbp_solve(self.h, C.c_void_p(b.data_ptr()), C.c_void_p(u.data_ptr()), C.byref(o),
