@@ -303,6 +303,21 @@ scy_status scy_in_problem_field(const char* path, const char* name, double* out,
 scy_status scy_in_problem_info(const char* path, scy_grid_desc* grid, scy_ode_opts* ode, int* state_law,
                                int* guess_ss, double* fault_type_scale);
 
+enum {
+  SCY_QD_MODE_SOLVE = 0,    /* every d_dt solves the momentum balance (default) */
+  SCY_QD_MODE_RESPONSE = 1  /* every d_dt evaluates the fault stress from the
+                               discrete response of the fault to its boundary
+                               data: tau = GL*(slip/faultTypeScale) + c(t)*g1 + gs,
+                               GL (Nz x Nz) and g1, gs built once from Nz + 2
+                               solves with the same solver; exact to the solve
+                               tolerance because the momentum balance is linear
+                               and its right-hand side depends only on bcL, bcR */
+};
+/* Selects how d_dt gets the fault stress (SCY_QD_MODE_*).  The response
+ * matrices are built at the first d_dt after the switch (after the
+ * steady-state guess, which changes bcRShift). */
+scy_status scy_qd_set_mode(scy_qd* q, int mode);
+
 /* Selects the root finder's derivative: 0 the reference's expression, 1 the
  * exact derivative (see scy_fault_desc.exact_jacobian).  Drivers made by
  * scy_qd_create_from_in start with the exact derivative. */

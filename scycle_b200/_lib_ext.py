@@ -53,6 +53,7 @@ def declare(L):
     L.scy_qd_integrate_begin_from_in.argtypes = [vp]
     L.scy_qd_set_state.argtypes = [vp, dptr, C.c_int]
     L.scy_qd_set_jacobian.argtypes = [vp, C.c_int]
+    L.scy_qd_set_mode.argtypes = [vp, C.c_int]
     L.scy_in_problem_field.argtypes = [C.c_char_p, C.c_char_p, dptr, C.c_long, C.POINTER(C.c_long)]
     L.scy_in_problem_info.argtypes = [C.c_char_p, C.POINTER(S.GridDesc), C.POINTER(OdeOpts), C.POINTER(C.c_int),
                                       C.POINTER(C.c_int), C.POINTER(C.c_double)]

@@ -259,6 +259,12 @@ scy_status scy_qd_get_field(scy_qd* q, int field, double* out) {
   const double* src = nullptr;
   size_t n = c.Nz;
   long stride = 1;
+  if (c.mode == SCY_QD_MODE_RESPONSE && c.green_ready &&
+      (field == SCY_FIELD_U || field == SCY_FIELD_SXY || field == SCY_FIELD_SURFDISP)) {
+    const double cc = c.bcR_remote ? c.vL * c.last_t * (1.0 / c.fts) : 0.0;
+    if (field == SCY_FIELD_SURFDISP) return scy::qd_green_surf_launch(c, cc, out);
+    SCY_TRY(c.full_solve_for_output());
+  }
   switch (field) {
     case SCY_FIELD_PSI: src = c.rk[0].as<double>(); break;
     case SCY_FIELD_SLIP: src = c.rk[0].as<double>() + c.Nz; break;
@@ -358,6 +364,16 @@ scy_status scy_qd_integrate_begin_from_in(scy_qd* q) {
                                c.sbp.stream));
   SCY_CUDA_TRY(cudaStreamSynchronize(c.sbp.stream));
   return c.integrate_begin(P.ode);
+}
+
+scy_status scy_qd_set_mode(scy_qd* q, int mode) {
+  if (!q || (mode != SCY_QD_MODE_SOLVE && mode != SCY_QD_MODE_RESPONSE)) {
+    scy::set_error("scy_qd_set_mode: unknown mode");
+    return SCY_ERR_ARG;
+  }
+  q->ctx.mode = mode;
+  q->ctx.green_ready = 0;
+  return SCY_OK;
 }
 
 scy_status scy_qd_set_jacobian(scy_qd* q, int exact) {

@@ -26,26 +26,16 @@ __global__ void qd_bc_kernel(const double* __restrict__ var, int Nz, double t, d
   if (bcR_remote) bcR[i] = vL * t * inv_fts + shift[i];
 }
 
-// Fault column: sxy = mu*Dy*u at iy = 0 (body2L scatter of muxDy), then
-// Fault_qd::d_dt for each node.
-__global__ void qd_fault_kernel(LevelDev<double> L, const double* __restrict__ u, FaultParams fp,
-                                const double* __restrict__ var, double* __restrict__ f,
-                                double* __restrict__ slipVel, double* __restrict__ tauQSP,
-                                double* __restrict__ tauP, double* __restrict__ strength, unsigned* flags,
-                                unsigned long long* its_total) {
+// Fault_qd::d_dt for one node given its quasi-static shear stress from the
+// body (fault.cpp:861-918): prestress, bracketed Newton, state law, tauP,
+// strength.
+__device__ __forceinline__ void fault_node_update(int iz, double tau_body, const FaultParams& fp,
+                                                  const double* __restrict__ var, double* __restrict__ f,
+                                                  double* __restrict__ slipVel, double* __restrict__ tauQSP,
+                                                  double* __restrict__ tauP, double* __restrict__ strength,
+                                                  unsigned* flags, unsigned long long* its_total) {
   const int Nz = fp.Nz;
-  int iz = blockIdx.x * blockDim.x + threadIdx.x;
-  if (iz >= Nz) return;
-  // Dy row 0 (band offsets -4..4 around row 0; only columns >= 0 exist)
-  double d = 0.0;
-#pragma unroll
-  for (int j = HALF; j < BAND; ++j) {
-    int k = j - HALF;
-    if (k < L.Ny) d += L.y.D[j] * u[(long)k * Nz + iz];
-  }
-  if (L.var) d *= L.qy[iz];
-  const double sxy = L.mu[iz] * d;
-  const double tq = sxy + fp.prestress[iz];
+  const double tq = tau_body + fp.prestress[iz];
   tauQSP[iz] = tq;
   const double psi = var[iz];
   const double a = fp.a[iz], sN = fp.sN[iz], eta = fp.eta[iz];
@@ -84,6 +74,110 @@ __global__ void qd_fault_kernel(LevelDev<double> L, const double* __restrict__ u
   f[Nz + iz] = V;
   tauP[iz] = tq - eta * V;
   strength[iz] = strength_psi(sN, psi, V, a, fp.v0);
+}
+
+// Fault column: sxy = mu*Dy*u at iy = 0 (body2L scatter of muxDy), then the
+// fault update.
+__global__ void qd_fault_kernel(LevelDev<double> L, const double* __restrict__ u, FaultParams fp,
+                                const double* __restrict__ var, double* __restrict__ f,
+                                double* __restrict__ slipVel, double* __restrict__ tauQSP,
+                                double* __restrict__ tauP, double* __restrict__ strength, unsigned* flags,
+                                unsigned long long* its_total) {
+  const int Nz = fp.Nz;
+  int iz = blockIdx.x * blockDim.x + threadIdx.x;
+  if (iz >= Nz) return;
+  // Dy row 0 (band offsets -4..4 around row 0; only columns >= 0 exist)
+  double d = 0.0;
+#pragma unroll
+  for (int j = HALF; j < BAND; ++j) {
+    int k = j - HALF;
+    if (k < L.Ny) d += L.y.D[j] * u[(long)k * Nz + iz];
+  }
+  if (L.var) d *= L.qy[iz];
+  const double sxy = L.mu[iz] * d;
+  fault_node_update(iz, sxy, fp, var, f, slipVel, tauQSP, tauP, strength, flags, its_total);
+}
+
+// Fault column stress of a body displacement, for building the response
+// matrices: out[iz * ld + col] = mu * Dy u at (0, iz); surf[iy * ld + col] = u(iy, 0).
+__global__ void qd_response_column_kernel(LevelDev<double> L, const double* __restrict__ u, double* __restrict__ out,
+                                          double* __restrict__ surf, int ld, int col) {
+  const int Ny = L.Ny, Nz = L.Nz;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < Nz) {
+    double d = 0.0;
+#pragma unroll
+    for (int j = HALF; j < BAND; ++j) {
+      int k = j - HALF;
+      if (k < Ny) d += L.y.D[j] * u[(long)k * Nz + i];
+    }
+    if (L.var) d *= L.qy[i];
+    out[(long)i * ld + col] = L.mu[i] * d;
+  }
+  if (i < Ny && surf) surf[(long)i * ld + col] = u[(long)i * Nz];
+}
+
+// Fault-response d_dt: one warp per fault node forms
+// tau = GL[iz,:] . (slip/faultTypeScale) + c g1[iz] + gs[iz], lane 0 then
+// runs the fault update.
+__global__ void qd_green_kernel(const double* __restrict__ GL, const double* __restrict__ g1,
+                                const double* __restrict__ gs, double c, double inv_fts, FaultParams fp,
+                                const double* __restrict__ var, double* __restrict__ f, double* __restrict__ slipVel,
+                                double* __restrict__ tauQSP, double* __restrict__ tauP, double* __restrict__ strength,
+                                double* __restrict__ bcL, unsigned* flags, unsigned long long* its_total) {
+  const int Nz = fp.Nz;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (warp >= Nz) return;
+  const double* row = GL + (long)warp * Nz;
+  const double* slip = var + Nz;
+  double acc = 0.0;
+  for (int j = lane; j < Nz; j += 32) acc += row[j] * (slip[j] * inv_fts);
+  acc = warp_sum(acc);
+  if (lane == 0) {
+    bcL[warp] = slip[warp] * inv_fts;  // kept for output fields
+    const double tau = acc + (c * g1[warp] + gs[warp]);
+    fault_node_update(warp, tau, fp, var, f, slipVel, tauQSP, tauP, strength, flags, its_total);
+  }
+}
+
+// surface displacement from the response matrices and the last bcL
+__global__ void qd_green_surf_kernel(const double* __restrict__ SL, const double* __restrict__ s1,
+                                     const double* __restrict__ ss, double c, int Ny, int Nz,
+                                     const double* __restrict__ bcL, double* __restrict__ out) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (warp >= Ny) return;
+  const double* row = SL + (long)warp * Nz;
+  double acc = 0.0;
+  for (int j = lane; j < Nz; j += 32) acc += row[j] * bcL[j];
+  acc = warp_sum(acc);
+  if (lane == 0) out[warp] = acc + (c * s1[warp] + ss[warp]);
+}
+
+int qd_green_surf_launch(QDContext& q, double c, double* host_out) {
+  cudaStream_t s = q.sbp.stream;
+  const int wpb = 4;
+  qd_green_surf_kernel<<<(q.Ny + wpb - 1) / wpb, 32 * wpb, 0, s>>>(q.SL.as<double>(), q.s1.as<double>(),
+                                                                   q.ss.as<double>(), c, q.Ny, q.Nz,
+                                                                   q.bcL.as<double>(), q.sxy.as<double>());
+  SCY_LAUNCH_CHECK();
+  SCY_CUDA_TRY(cudaMemcpyAsync(host_out, q.sxy.p, (size_t)q.Ny * 8, cudaMemcpyDeviceToHost, s));
+  SCY_CUDA_TRY(cudaStreamSynchronize(s));
+  return SCY_OK;
+}
+
+// Body displacement for output in response mode: one full solve with the
+// boundary data of the last d_dt.
+int QDContext::full_solve_for_output() {
+  cudaStream_t s = sbp.stream;
+  const int tb = 64, gb = (Nz + tb - 1) / tb;
+  qd_bc_kernel<<<gb, tb, 0, s>>>(rk[0].as<double>(), Nz, last_t, vL, 1.0 / fts, 0, bcR_remote,
+                                 bcRShift.as<double>(), bcL.as<double>(), bcR.as<double>());
+  SCY_LAUNCH_CHECK();
+  SCY_TRY(sbp.set_rhs(bcL.as<double>(), bcR.as<double>(), bcT.as<double>(), bcB.as<double>(), rhs.as<double>()));
+  scy_solve_opts o = solve_opts;
+  o.nonzero_guess = 1;
+  scy_solve_stats st{};
+  return sbp.solve(rhs.as<double>(), u.as<double>(), o, st);
 }
 
 // out = ((var + c0 f0) + c1 f1) + ... in the reference's WAXPY/AXPY order
@@ -252,6 +346,19 @@ int QDContext::read_flags() {
 
 int QDContext::d_dt(double t, const double* var, double* f) {
   cudaStream_t s = sbp.stream;
+  if (mode == SCY_QD_MODE_RESPONSE) {
+    if (!green_ready) SCY_TRY(build_green());
+    const double c = bcR_remote ? vL * t * (1.0 / fts) : 0.0;
+    const int wpb = 4;
+    qd_green_kernel<<<(Nz + wpb - 1) / wpb, 32 * wpb, 0, s>>>(
+        GL.as<double>(), g1.as<double>(), gs.as<double>(), c, 1.0 / fts, fp, var, f, slipVel.as<double>(),
+        tauQSP.as<double>(), tauP.as<double>(), strength.as<double>(), bcL.as<double>(), flags.as<unsigned>(),
+        fault_its.as<unsigned long long>());
+    SCY_LAUNCH_CHECK();
+    last_t = t;
+    ++n_d_dt;
+    return SCY_OK;
+  }
   const int tb = 64, gb = (Nz + tb - 1) / tb;
   qd_bc_kernel<<<gb, tb, 0, s>>>(var, Nz, t, vL, 1.0 / fts, bcL_from_slip, bcR_remote, bcRShift.as<double>(),
                                  bcL.as<double>(), bcR.as<double>());
@@ -268,7 +375,93 @@ int QDContext::d_dt(double t, const double* var, double* f) {
                                     tauQSP.as<double>(), tauP.as<double>(), strength.as<double>(),
                                     flags.as<unsigned>(), fault_its.as<unsigned long long>());
   SCY_LAUNCH_CHECK();
+  last_t = t;
   ++n_d_dt;
+  return SCY_OK;
+}
+
+// Response of the fault stress and the surface displacement to unit boundary
+// data: Nz solves with bcL = e_j, one with bcR = 1 and one with the current
+// fixed part of bcR (bcRShift when the right boundary is loaded, else bcR).
+int QDContext::build_green() {
+  cudaStream_t s = sbp.stream;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, s);
+  SCY_TRY(GL.alloc((size_t)Nz * Nz * 8));
+  SCY_TRY(SL.alloc((size_t)Ny * Nz * 8));
+  DevBuf cols, scol;
+  SCY_TRY(cols.alloc((size_t)Nz * 2 * 8));
+  SCY_TRY(scol.alloc((size_t)Ny * 2 * 8));
+  SCY_TRY(g1.alloc((size_t)Nz * 8));
+  SCY_TRY(gs.alloc((size_t)Nz * 8));
+  SCY_TRY(s1.alloc((size_t)Ny * 8));
+  SCY_TRY(ss.alloc((size_t)Ny * 8));
+  DevBuf bL, bR, uu;
+  SCY_TRY(bL.alloc((size_t)Nz * 8));
+  SCY_TRY(bR.alloc((size_t)Nz * 8));
+  SCY_TRY(uu.alloc((size_t)N * 8));
+  scy_solve_opts o = solve_opts;
+  o.rtol = std::min(o.rtol, 1e-13);
+  o.nonzero_guess = 0;
+  o.max_its = std::max(o.max_its, 500);
+  const LevelDev<double>& L = sbp.fine->dev;
+  const int tb = 128, gb = (std::max(Ny, Nz) + tb - 1) / tb;
+  std::vector<double> e(Nz, 0.0);
+  SCY_CUDA_TRY(cudaMemsetAsync(bR.p, 0, (size_t)Nz * 8, s));
+  for (int j = 0; j < Nz; ++j) {
+    e[j] = 1.0;
+    SCY_CUDA_TRY(cudaMemcpyAsync(bL.p, e.data(), (size_t)Nz * 8, cudaMemcpyHostToDevice, s));
+    e[j] = 0.0;
+    SCY_TRY(sbp.set_rhs(bL.as<double>(), bR.as<double>(), bcT.as<double>(), bcB.as<double>(), rhs.as<double>()));
+    scy_solve_stats st{};
+    SCY_TRY(sbp.solve(rhs.as<double>(), uu.as<double>(), o, st));
+    qd_response_column_kernel<<<gb, tb, 0, s>>>(L, uu.as<double>(), GL.as<double>(), SL.as<double>(), Nz, j);
+    SCY_LAUNCH_CHECK();
+  }
+  // bcR = 1 and the fixed part of bcR
+  SCY_CUDA_TRY(cudaMemsetAsync(bL.p, 0, (size_t)Nz * 8, s));
+  for (int k = 0; k < 2; ++k) {
+    if (k == 0) {
+      std::vector<double> ones(Nz, 1.0);
+      SCY_CUDA_TRY(cudaMemcpyAsync(bR.p, ones.data(), (size_t)Nz * 8, cudaMemcpyHostToDevice, s));
+      SCY_CUDA_TRY(cudaStreamSynchronize(s));
+    } else {
+      const DevBuf& fixed = bcR_remote ? bcRShift : bcR;
+      SCY_CUDA_TRY(cudaMemcpyAsync(bR.p, fixed.p, (size_t)Nz * 8, cudaMemcpyDeviceToDevice, s));
+    }
+    SCY_TRY(sbp.set_rhs(bL.as<double>(), bR.as<double>(), bcT.as<double>(), bcB.as<double>(), rhs.as<double>()));
+    scy_solve_stats st{};
+    SCY_TRY(sbp.solve(rhs.as<double>(), uu.as<double>(), o, st));
+    qd_response_column_kernel<<<gb, tb, 0, s>>>(L, uu.as<double>(), cols.as<double>(), scol.as<double>(), 2, k);
+    SCY_LAUNCH_CHECK();
+  }
+  // split the two columns into g1/gs and s1/ss
+  std::vector<double> hc((size_t)Nz * 2), hs((size_t)Ny * 2), a(Nz), b(Nz), c(Ny), d(Ny);
+  SCY_CUDA_TRY(cudaMemcpyAsync(hc.data(), cols.p, hc.size() * 8, cudaMemcpyDeviceToHost, s));
+  SCY_CUDA_TRY(cudaMemcpyAsync(hs.data(), scol.p, hs.size() * 8, cudaMemcpyDeviceToHost, s));
+  SCY_CUDA_TRY(cudaStreamSynchronize(s));
+  for (int i = 0; i < Nz; ++i) {
+    a[i] = hc[(size_t)i * 2];
+    b[i] = hc[(size_t)i * 2 + 1];
+  }
+  for (int i = 0; i < Ny; ++i) {
+    c[i] = hs[(size_t)i * 2];
+    d[i] = hs[(size_t)i * 2 + 1];
+  }
+  SCY_CUDA_TRY(cudaMemcpyAsync(g1.p, a.data(), (size_t)Nz * 8, cudaMemcpyHostToDevice, s));
+  SCY_CUDA_TRY(cudaMemcpyAsync(gs.p, b.data(), (size_t)Nz * 8, cudaMemcpyHostToDevice, s));
+  SCY_CUDA_TRY(cudaMemcpyAsync(s1.p, c.data(), (size_t)Ny * 8, cudaMemcpyHostToDevice, s));
+  SCY_CUDA_TRY(cudaMemcpyAsync(ss.p, d.data(), (size_t)Ny * 8, cudaMemcpyHostToDevice, s));
+  cudaEventRecord(e1, s);
+  SCY_CUDA_TRY(cudaStreamSynchronize(s));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  green_build_ms = ms;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  green_ready = 1;
   return SCY_OK;
 }
 

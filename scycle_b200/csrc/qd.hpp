@@ -41,6 +41,15 @@ struct QDContext {
   int record = 0;
 
   std::vector<double> h_a, h_b, h_sN;  // host copies for the steady-state guess
+  // fault-response mode: tau_qs(body) = GL bcL + c(t) g1 + gs, surface
+  // displacement = SL bcL + c(t) s1 + ss (c(t) = vL t / faultTypeScale)
+  int mode = 0;        // SCY_QD_MODE_*
+  int green_ready = 0;
+  DevBuf GL, SL, g1, gs, s1, ss;
+  double green_build_ms = 0.0;
+  int build_green();
+  int full_solve_for_output();
+  double last_t = 0.0;  // time of the last d_dt (for output fields in response mode)
   double f0 = 0.6, v0 = 1e-6;
 
   int create(const scy_qd_desc& d);
@@ -58,5 +67,7 @@ struct QDContext {
   int attempt(double dt, double** lo, double** hi);
   int read_flags();
 };
+
+int qd_green_surf_launch(QDContext& q, double c, double* host_out);
 
 }  // namespace scy

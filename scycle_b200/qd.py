@@ -31,6 +31,11 @@ class QD:
         self.P = None
         return self
 
+    def set_mode(self, mode):
+        """"solve" (every d_dt solves the momentum balance) or "response"
+        (fault stress from the precomputed discrete fault response)."""
+        S.check(S.lib().scy_qd_set_mode(self.h, {"solve": 0, "response": 1}[mode]))
+
     def integrate_begin_from_in(self):
         S.check(S.lib().scy_qd_integrate_begin_from_in(self.h))
 

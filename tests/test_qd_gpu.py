@@ -132,3 +132,44 @@ def test_reference_example_from_input_file(tmp_path, integrator):
     assert _rel(dev.field("slipVel"), f.slipVel, 1e-30) <= REL
     assert _rel(dev.field("tauP"), f.tauP, 1e-9) <= REL
     assert _nrel(dev.field("surfDisp"), ora.u[::P["Nz"]]) <= REL
+
+
+@pytest.mark.parametrize("integrator", ["RK32", "RK43"])
+def test_response_mode_matches_oracle(tmp_path, integrator):
+    """Fault stress from the precomputed discrete fault response (Nz + 2
+    solves) instead of a solve per stage: same states as the oracle's direct
+    solves to the parity tolerance."""
+    from scycle_b200.qd import QD
+    path = _ex2_like(tmp_path, n=33, integrator=integrator)
+    P = build_qd_problem(open(path).read())
+    ora = QDLinearElastic(P, keep_history=False)
+    dev = QD.from_in(path, solve_rtol=SOLVE_RTOL)
+    dev.set_mode("response")
+    dev.record_attempts(True)
+    dev.integrate_begin_from_in()
+    st = dev.integrate_steps(30)
+    rk = ora.integrate(max_steps=30, replay=dev.attempts())
+    assert st.step_count == rk.stepCount == 30
+    f = ora.fault
+    assert _rel(dev.field("slip"), f.slip, 1e-12) <= REL
+    assert _rel(dev.field("psi"), f.psi) <= REL
+    assert _rel(dev.field("slipVel"), f.slipVel, 1e-30) <= REL
+    assert _rel(dev.field("tauP"), f.tauP, 1e-9) <= REL
+    assert _nrel(dev.field("surfDisp"), ora.u[::P["Nz"]]) <= REL
+    assert _nrel(dev.field("u"), ora.u) <= REL
+
+
+def test_response_mode_d_dt_matches_solve_mode(tmp_path):
+    from scycle_b200.qd import QD
+    P = _problem(tmp_path, n=45, law="slipLaw", grid="variableGridSpacing", prestress=27.0)
+    a = QD(P, solve_rtol=SOLVE_RTOL)
+    b = QD(P, solve_rtol=SOLVE_RTOL)
+    b.set_mode("response")
+    rng = np.random.default_rng(11)
+    for t in (0.0, 5.0e8):
+        psi = P["psi"] + 1e-3 * rng.standard_normal(P["Nz"])
+        slip = 0.05 * rng.random(P["Nz"])
+        fa, fb = a.d_dt(t, psi, slip), b.d_dt(t, psi, slip)
+        assert _rel(fb["slip"], fa["slip"], 1e-30) <= REL
+        assert _rel(fb["psi"], fa["psi"], 1e-12) <= REL
+        assert _rel(b.field("tauQSP"), a.field("tauQSP"), 1e-9) <= REL
