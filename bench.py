@@ -265,6 +265,36 @@ def run_ours(args, dist, rank, world, local):
     q.close()
 
 
+def run_stencil_only(args):
+    """A x on an n x n grid (FP64, constant grid, Dirichlet/Neumann SATs): the
+    operator kernel alone, sized past L2 when n >= 4097, for profiling."""
+    import torch
+    from scycle_b200 import build
+    build.build(verbose=False)
+    from scycle_b200.sbp import SbpOps
+    from scycle_b200 import _lib as S
+    n = args.profile_stencil
+    sbp = SbpOps(4, n, n, 30.0, 30.0, np.full(n * n, 32.04))
+    x = torch.randn(n * n, dtype=torch.float64, device="cuda")
+    out = torch.empty_like(x)
+    L = S.lib()
+    for _ in range(3):
+        S.check(L.scy_sbp_apply(sbp.h, 0, C.c_void_p(x.data_ptr()), C.c_void_p(out.data_ptr())))
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 20
+    ev0.record()
+    for _ in range(reps):
+        S.check(L.scy_sbp_apply(sbp.h, 0, C.c_void_p(x.data_ptr()), C.c_void_p(out.data_ptr())))
+    ev1.record()
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / reps
+    algo = 3 * 8 * n * n
+    peak = _peaks().get("hbm_gbs", 6650.0)
+    print(json.dumps({"stencil_only": True, "n": n, "us_per_apply": ms * 1e3,
+                      "algorithmic_GBps": algo / (ms / 1e3) / 1e9, "frac_of_measured_hbm": algo / (ms / 1e3) / 1e9 / peak}))
+
+
 def cpu_baseline(path, args, max_evals=None):
     """The oracle (SciPy SuperLU direct solve + restated fault / RK32) on the
     host cores, on a bounded sample of the same workload."""
@@ -326,9 +356,14 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-response", action="store_true")
+    ap.add_argument("--profile-stencil", type=int, default=0,
+                    help="time only the FP64 operator kernel on an n x n grid and exit")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
+    if args.profile_stencil:
+        run_stencil_only(args)
+        return
     dist, rank, world, local = _dist()
     try:
         if args.impl == "reference":
