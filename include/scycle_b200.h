@@ -328,6 +328,114 @@ scy_status scy_qd_set_jacobian(scy_qd* q, int exact);
  * only uploads it (for a host round trip of the state the device holds). */
 scy_status scy_qd_set_state(scy_qd* q, const double* var_host, int recompute);
 
+/* ---------------------------------------------------------------------------
+ * Quasi-dynamic / fully dynamic earthquake cycles: the
+ * strikeSlip_linearElastic_qd_fd driver (source/strikeSlip_linearElastic_qd_fd.cpp,
+ * selected by momentumBalanceType = quasidynamic_and_dynamic, main.cpp:266-274).
+ * Quasi-dynamic phases run the scy_qd integrator, restarted per phase
+ * (integrate_qd :1436-1508); fully dynamic phases step the wave equation with
+ * a fixed CFL-limited step (computeTimeStep :356-442, propagateWaves
+ * :1170-1239, Fault_fd::d_dt fault.cpp:1436-1523, OdeSolver_WaveEq::integrate
+ * odeSolver_WaveEq.cpp:147-186).  The phases switch on R = max(eta V / tauQS)
+ * (checkSwitchRegime :586-662).
+ * ------------------------------------------------------------------------- */
+enum { SCY_FD_FREE_SURFACE = 0, SCY_FD_OUTGOING = 1 };
+
+typedef struct scy_cycle_desc {
+  const double* rho;        /* host, Ny*Nz: body density (LinearElastic::_rho) */
+  const double* cs;         /* host, Ny*Nz or NULL (sqrt(mu/rho)): shear-wave speed (LinearElastic::_cs) */
+  const double* rho_fault;  /* host, Nz: fault density (Fault::_rho) */
+  int fd_bcR, fd_bcT, fd_bcB; /* SCY_FD_*: momBal_bcR_fd, momBal_bcT_fd, momBal_bcB_fd; the
+                                 left boundary is the fault (symmFault / rigidFault) */
+  double deltaT_fd;         /* requested wave-equation step (s), <= 0: not given */
+  double CFL;               /* requested CFL number, <= 0: not given */
+  double trigger_qd2fd, trigger_fd2qd, limit_qd, limit_fd; /* after checkInput (:292-303) */
+  int max_num_cycles;       /* maxNumCycles */
+  int ay_index_quirk;       /* 1: the outgoing-characteristics damping ay indexed as
+                               computePenaltyVectors does (its index advances only in
+                               the last test, :493-495, so the damping lands on body
+                               entries 0..Nz); 0: on the boundary nodes it names */
+} scy_cycle_desc;
+
+typedef struct scy_cycle scy_cycle;
+
+enum { SCY_PHASE_QD = 0, SCY_PHASE_FD = 1, SCY_PHASE_DONE = 2 };
+
+typedef struct scy_cycle_stats {
+  double t;                 /* _currTime */
+  double dt;                /* last quasi-dynamic step size */
+  double new_dt;            /* the quasi-dynamic integrator's next step size (_newDeltaT) */
+  double dt_fd;             /* wave-equation step (_deltaT_fd) */
+  long step_count;          /* _stepCount: quasi-dynamic and wave-equation steps */
+  int phase;                /* SCY_PHASE_* */
+  int cycle_count;          /* _cycleCount */
+  int allowed;              /* _allowed */
+  int done;                 /* 1: integrate() has returned */
+  long qd_steps, fd_steps;  /* quasi-dynamic steps (with the single step at each switch), wave steps */
+  long switches;            /* phase switches so far */
+  double last_ratio;        /* max(eta V / tauQS) at the last switch test */
+  long d_dt_evals, solve_its, solves;
+  double qd_ms, fd_ms;      /* host time spent in quasi-dynamic phases (with the single
+                               steps) and in wave-equation batches */
+} scy_cycle_stats;
+
+scy_status scy_cycle_create(const scy_qd_desc* qd, const scy_cycle_desc* cd, scy_cycle** out);
+/* Reads a strikeSlip_linearElastic_qd_fd input file (.in format; the
+ * quasi-dynamic keys of scy_qd_create_from_in plus trigger_qd2fd,
+ * trigger_fd2qd, limit_qd, limit_fd, deltaT_fd, CFL, maxNumCycles and
+ * momBal_bc*_fd, loadSettings :135-230, with the defaults of :8-33). */
+scy_status scy_cycle_create_from_in(const char* path, const scy_solve_opts* solve, scy_cycle** out);
+scy_status scy_cycle_destroy(scy_cycle* c);
+/* Sizes, the wave-equation step and the quasi-dynamic integrator settings
+ * (a driver made from an input file). */
+scy_status scy_cycle_get_problem(scy_cycle* c, int* Ny, int* Nz, double* dt_fd, scy_ode_opts* ode);
+/* initiateIntegrands (:668-744) from var0 = [psi | slip] (host, 2*Nz). */
+scy_status scy_cycle_begin(scy_cycle* c, const scy_ode_opts* ode, const double* var0_host);
+/* initiateIntegrands for a driver made from an input file, with the
+ * steady-state guess when the file asks for it (solveSS :1243-1340). */
+scy_status scy_cycle_begin_from_in(scy_cycle* c);
+/* integrate() (:511-581), advanced by at most max_steps steps; call again to
+ * continue.  Returns with stats->done = 1 once the reference would return. */
+scy_status scy_cycle_run(scy_cycle* c, long max_steps, scy_cycle_stats* stats);
+/* Fields of the current phase (SCY_FIELD_*; U and SURFDISP are the material
+ * displacement, u + u0 in a fully dynamic phase). */
+scy_status scy_cycle_get_field(scy_cycle* c, int field, double* host_out);
+/* Phase switches so far: the step and time of each, and to_fd = 1 for a
+ * quasi-dynamic to fully dynamic switch. */
+scy_status scy_cycle_get_switches(scy_cycle* c, long* steps, double* times, int* to_fd, long cap, long* n);
+/* Forced / recorded attempts of the quasi-dynamic integrator, across all
+ * quasi-dynamic phases and single steps (see scy_qd_force_attempts). */
+scy_status scy_cycle_force_attempts(scy_cycle* c, const double* dts, const int* accept, long n);
+scy_status scy_cycle_record_attempts(scy_cycle* c, int on);
+scy_status scy_cycle_get_attempts(scy_cycle* c, double* dts, int* accept, long cap, long* n);
+/* Quasi-dynamic phase mode (SCY_QD_MODE_*) and root-finder derivative. */
+scy_status scy_cycle_set_mode(scy_cycle* c, int mode);
+scy_status scy_cycle_set_jacobian(scy_cycle* c, int exact);
+/* Wave-equation steps per graph launch (default 64; 1..4096). */
+scy_status scy_cycle_set_fd_batch(scy_cycle* c, int steps);
+/* Restart hook: puts the driver at the start of a fully dynamic step at time
+ * t after global step `step`, with the wave-equation state of steps n
+ * (psi, slip, u) and n-1 (psiPrev, slipPrev, uPrev), the displacement offset
+ * u0 (material u = u + u0), the fault's slip0 and tau0 (strength + prestress
+ * at the switch), its slip velocity and the switch test's _allowed (host
+ * arrays: Nz for fault fields, Ny*Nz for u, uPrev, u0).  A driver made by
+ * scy_cycle_create_from_in must have been begun first. */
+scy_status scy_cycle_set_fd_state(scy_cycle* c, double t, long step, int allowed, const double* psi,
+                                  const double* slip, const double* u, const double* psiPrev,
+                                  const double* slipPrev, const double* uPrev, const double* u0,
+                                  const double* slip0, const double* tau0, const double* slipVel);
+/* Profiling hook: average device time (CUDA events, `reps` back-to-back
+ * launches each) of the wave-equation stencil launch and of the fault launch
+ * of one fully dynamic step, on the driver's current wave state.  Both
+ * launches rewrite the step-n+1 buffers and the fault's slip velocity, so
+ * call it only when the run is over or about to be restarted. */
+scy_status scy_cycle_time_kernels(scy_cycle* c, int reps, double* wave_us, double* fault_us);
+/* Host-only (no GPU needed): the cycle settings of an input file after
+ * checkInput (pointer members set to NULL), the wave-equation step of
+ * computeTimeStep and the penalty vector ay of computePenaltyVectors (Ny*Nz
+ * doubles into ay when cap allows; *n receives the length). */
+scy_status scy_in_cycle_info(const char* path, scy_cycle_desc* cd, double* dt_fd, double* ay, long cap, long* n);
+
 #ifdef __cplusplus
 }
 #endif

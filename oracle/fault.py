@@ -3,9 +3,10 @@
 Restates source/fault.cpp (Fault_qd::computeVel :812-857, Fault_qd::d_dt
 :861-918, ComputeVel_qd :954-1059, agingLaw_psi :1984-1994, slipLaw_psi
 :2072-2088, strength_psi :2247-2251) and BracketedNewton::findRoot
-(source/rootFinder.cpp:168-266).  The per-node Newton iteration is
-vectorised across nodes with masks; each node follows exactly the scalar
-control flow of the reference.
+(source/rootFinder.cpp:168-266), and the fully dynamic fault (Fault_fd
+:1065-1575, ComputeVel_fd :1588-1685, ComputeAging_fd / ComputeSlipLaw_fd
+:1690-1879).  The per-node Newton iteration is vectorised across nodes with
+masks; each node follows exactly the scalar control flow of the reference.
 """
 import numpy as np
 
@@ -193,3 +194,142 @@ class FaultQD:
         self.tauP = self.tauQSP - self.eta * V
         self.strength = strength_psi(self.sN, self.psi, V, self.a, self.v0)
         return V.copy(), dpsi
+
+
+# ---------------------------------------------------------------------------
+# Fully dynamic fault (Fault_fd, fault.cpp:1065-1575; ComputeVel_fd
+# :1588-1685; ComputeAging_fd / ComputeSlipLaw_fd :1690-1879)
+
+def resid_vel_fd(V, Phi, fricPen, sN, psi, a, v0):
+    """ComputeVel_fd::getResid with Jacobian (fault.cpp:1649-1685):
+    fricPen*strength(V) - (|Phi| - V) and its exact derivative."""
+    constraints = fricPen * strength_psi(sN, psi, V, a, v0)
+    stress = np.abs(Phi) - V
+    f = constraints - stress
+    A = a * sN
+    B = np.exp(psi / a) / (2.0 * v0)
+    J = 1 + fricPen * A * B / np.sqrt(1. + B * B * V * V)
+    return f, J
+
+
+def compute_vel_fd(Vprev, Phi, fricPen, sN, psi, a, locked, v0, vL, root_tol=1e-12, max_its=10000):
+    """ComputeVel_fd::computeVel (fault.cpp:1594-1644): |V| from a bracketed
+    Newton on [0, |Phi|] started at |V_prev|; locked nodes are held at 0 or vL."""
+    V = np.abs(np.array(Vprev, dtype=np.float64, copy=True))
+    locked = np.asarray(locked, dtype=np.float64)
+    lk = locked > 0.5
+    ck = locked < -0.5
+    out = V.copy()
+    out[lk] = 0.0
+    out[ck] = vL
+    free = np.nonzero(~(lk | ck))[0]
+    its_total, conv = 0, True
+    if free.size == 0:
+        return out, its_total, conv
+    left = np.zeros(free.size)
+    right = np.abs(Phi[free])
+    deg = np.abs(left - right) < 1e-14
+    out[free[deg]] = left[deg]
+    nd = np.nonzero(~deg)[0]
+    if nd.size:
+        sel = free[nd]
+
+        def resid(x, idx):
+            j = sel[idx]
+            return resid_vel_fd(x, Phi[j], fricPen[j], sN[j], psi[j], a[j], v0)
+
+        x, its, c = bracketed_newton(resid, left[nd], right[nd], V[sel], root_tol, max_its)
+        out[sel] = x
+        its_total = int(its.sum())
+        conv = bool(c.all())
+    return out, its_total, conv
+
+
+def resid_state_fd(law, state, psiPrev, V, a, b, f0, v0, Dc, dt):
+    """ComputeAging_fd / ComputeSlipLaw_fd ::getResid with Jacobian
+    (fault.cpp:1750-1763, :1851-1865): implicit midpoint about psiPrev,
+    -2 dt G((psiPrev + state)/2, V) + (state - psiPrev)."""
+    mid = (psiPrev + state) / 2.0
+    temp = state - psiPrev
+    if law == "agingLaw":
+        G = aging_law_psi(mid, V, b, f0, v0, Dc)
+        J = 1 + dt * v0 / Dc * np.exp((f0 - (psiPrev + state) / 2.) / b)
+    elif law == "slipLaw":
+        G = slip_law_psi(mid, V, a, b, f0, v0, Dc)
+        A = np.abs(V) / 2. / v0 * np.exp((psiPrev + state) / 2.0 / a)
+        J = 1 + dt * np.abs(V) / Dc * A / np.sqrt(1 + A * A)
+    else:
+        raise ValueError(law)
+    return -2 * dt * G + temp, J
+
+
+def compute_state_fd(law, psi, psiPrev, V, a, b, f0, v0, Dc, dt, root_tol=1e-12, max_its=10000):
+    """ComputeAging_fd / ComputeSlipLaw_fd ::computeLaw (fault.cpp:1702-1745,
+    :1802-1846): root on [-2, 2] started at psi."""
+    n = psi.size
+    left = np.full(n, -2.0)
+    right = np.full(n, 2.0)
+
+    def resid(x, idx):
+        return resid_state_fd(law, x, psiPrev[idx], V[idx], a[idx], b[idx], f0, v0, Dc[idx], dt)
+
+    x, its, c = bracketed_newton(resid, left, right, psi, root_tol, max_its)
+    return x, int(its.sum()), bool(c.all())
+
+
+class FaultFD:
+    """Fault_fd::d_dt and setPhi (fault.cpp:1436-1575) on the fields the
+    cycle driver keeps.  ``fq`` is the quasi-dynamic fault whose friction
+    parameters and eta_rad the fully dynamic fault shares."""
+
+    def __init__(self, fq, rho, alphay, fault_type_scale):
+        self.fq = fq
+        n = fq.a.size
+        self.rho = np.asarray(rho, float)
+        self.alphay = np.asarray(alphay, float)
+        self.fts = fault_type_scale
+        self.psi = fq.psi.copy(); self.slip = np.zeros(n); self.slip0 = np.zeros(n)
+        self.slipVel = np.zeros(n); self.tau0 = np.zeros(n)
+        self.tauQSP = np.zeros(n); self.tauP = np.zeros(n); self.strength = np.zeros(n)
+        self.u = np.zeros(n); self.uPrev = np.zeros(n); self.d2u = np.zeros(n)
+        self.an = np.zeros(n); self.Phi = np.zeros(n); self.fricPen = np.zeros(n)
+        self.root_its = 0
+
+    def set_phi(self, dt):
+        """fault.cpp:1527-1575."""
+        self.an = self.d2u + self.tau0 / self.alphay
+        self.Phi = 2.0 / dt * (self.u - self.uPrev) + dt * self.an / self.rho
+        self.fricPen = dt / self.alphay / self.rho
+
+    def d_dt(self, dt, var, varPrev):
+        """fault.cpp:1436-1523.  Returns (psiNext, slipNext); self.u holds the
+        fault displacement at the next step."""
+        fq = self.fq
+        self.psi = var["psi"].copy()
+        self.slip = var["slip"].copy()
+        self.uPrev = (varPrev["slip"] - self.slip0) * (1.0 / self.fts)
+        self.u = (var["slip"] - self.slip0) * (1.0 / self.fts)
+        self.set_phi(dt)
+        V, its, conv = compute_vel_fd(self.slipVel, self.Phi, self.fricPen, fq.sN, self.psi, fq.a, fq.locked,
+                                      fq.v0, fq.vL, fq.root_tol, fq.max_its)
+        if not conv:
+            raise FloatingPointError("rootFinder BracketedNewton did not converge")
+        self.root_its += its
+        mv = ~(V < 1e-14)
+        fric = strength_psi(fq.sN, self.psi, V, fq.a, fq.v0)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            alpha = 1.0 / (self.rho * self.alphay) * fric / V
+        A = 1.0 + alpha * dt
+        Vn = np.where(mv, self.Phi / (1. + dt * alpha), V)
+        un = np.where(mv, (2. * self.u + (self.an * dt * dt / self.rho) + (dt * alpha - 1.) * self.uPrev) / A,
+                      self.u)
+        self.slipVel = Vn
+        self.u = un
+        psiNext, its, conv = compute_state_fd(fq.state_law, var["psi"], varPrev["psi"], self.slipVel, fq.a, fq.b,
+                                              fq.f0, fq.v0, fq.Dc, dt, fq.root_tol, fq.max_its)
+        if not conv:
+            raise FloatingPointError("rootFinder BracketedNewton did not converge (state)")
+        self.psi = psiNext.copy()
+        self.slip = self.fts * self.u + self.slip0
+        self.strength = strength_psi(fq.sN, self.psi, self.slipVel, fq.a, fq.v0)
+        return psiNext, self.slip.copy()

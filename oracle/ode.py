@@ -28,6 +28,12 @@ RK43_TABLEAU = dict(
 )
 
 
+def _ieee_div(a, b):
+    if b == 0.0:
+        return math.copysign(math.inf, a) if a != 0.0 else math.nan
+    return a / b
+
+
 class AdaptiveRK:
     """RK32 (method="RK32") or RK43 (method="RK43") with P / PID control."""
 
@@ -58,6 +64,12 @@ class AdaptiveRK:
     def set_time_range(self, t0, t1):
         self.initT = t0; self.currT = t0; self.finalT = t1
 
+    def set_initial_step_count(self, step_count):
+        """OdeSolver::setInitialStepCount (odeSolver.cpp:25-29): the step
+        budget is counted on from the given step."""
+        self.stepCount = step_count
+        self.maxNumSteps = step_count + self.maxNumSteps
+
     def set_tolerance_type(self, t):
         assert t in ("L2_relative", "L2_absolute")
         self.normType = t
@@ -77,9 +89,11 @@ class AdaptiveRK:
             if self.stepCount < 4:
                 ratio = self.kappa * math.pow(self.totTol / totErr, 1. / (1. + self.ord))
             else:
+                # IEEE semantics as in C++: a fresh solver's errA = [0, 0]
+                # gives 0 * inf = NaN, and the growth cap below then wins
                 ratio = (self.kappa * math.pow(self.totTol / totErr, alpha)
                          * math.pow(self.errA[0] / self.totTol, beta)
-                         * math.pow(self.totTol / self.errA[1], gamma))
+                         * math.pow(_ieee_div(self.totTol, self.errA[1]), gamma))
         else:
             raise ValueError(self.controlType)
         dt = ratio * self.deltaT

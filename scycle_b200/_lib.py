@@ -82,6 +82,7 @@ def _declare_extra(L):
     """Hook for entry points declared by other modules of the package."""
     from . import _lib_ext  # noqa: F401  (adds argtypes for the fault / driver API)
     _lib_ext.declare(L)
+    _lib_ext.declare_cycle(L)
 
 
 def check(status):

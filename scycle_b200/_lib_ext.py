@@ -58,3 +58,48 @@ def declare(L):
     L.scy_in_problem_info.argtypes = [C.c_char_p, C.POINTER(S.GridDesc), C.POINTER(OdeOpts), C.POINTER(C.c_int),
                                       C.POINTER(C.c_int), C.POINTER(C.c_double)]
     return L
+
+
+class CycleDesc(C.Structure):
+    _fields_ = [("rho", dptr), ("cs", dptr), ("rho_fault", dptr), ("fd_bcR", C.c_int), ("fd_bcT", C.c_int),
+                ("fd_bcB", C.c_int), ("deltaT_fd", C.c_double), ("CFL", C.c_double),
+                ("trigger_qd2fd", C.c_double), ("trigger_fd2qd", C.c_double), ("limit_qd", C.c_double),
+                ("limit_fd", C.c_double), ("max_num_cycles", C.c_int), ("ay_index_quirk", C.c_int)]
+
+
+class CycleStats(C.Structure):
+    _fields_ = [("t", C.c_double), ("dt", C.c_double), ("new_dt", C.c_double), ("dt_fd", C.c_double),
+                ("step_count", C.c_long),
+                ("phase", C.c_int), ("cycle_count", C.c_int), ("allowed", C.c_int), ("done", C.c_int),
+                ("qd_steps", C.c_long), ("fd_steps", C.c_long), ("switches", C.c_long),
+                ("last_ratio", C.c_double), ("d_dt_evals", C.c_long), ("solve_its", C.c_long),
+                ("solves", C.c_long), ("qd_ms", C.c_double), ("fd_ms", C.c_double)]
+
+
+PHASES = {0: "qd", 1: "fd", 2: "done"}
+
+
+def declare_cycle(L):
+    vp = C.c_void_p
+    L.scy_cycle_create.argtypes = [C.POINTER(QDDesc), C.POINTER(CycleDesc), C.POINTER(vp)]
+    L.scy_cycle_create_from_in.argtypes = [C.c_char_p, C.POINTER(S.SolveOpts), C.POINTER(vp)]
+    L.scy_cycle_destroy.argtypes = [vp]
+    L.scy_cycle_get_problem.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double),
+                                        C.POINTER(OdeOpts)]
+    L.scy_cycle_begin.argtypes = [vp, C.POINTER(OdeOpts), dptr]
+    L.scy_cycle_begin_from_in.argtypes = [vp]
+    L.scy_cycle_run.argtypes = [vp, C.c_long, C.POINTER(CycleStats)]
+    L.scy_cycle_get_field.argtypes = [vp, C.c_int, dptr]
+    L.scy_cycle_get_switches.argtypes = [vp, C.POINTER(C.c_long), dptr, C.POINTER(C.c_int), C.c_long,
+                                         C.POINTER(C.c_long)]
+    L.scy_cycle_force_attempts.argtypes = [vp, dptr, C.POINTER(C.c_int), C.c_long]
+    L.scy_cycle_record_attempts.argtypes = [vp, C.c_int]
+    L.scy_cycle_get_attempts.argtypes = [vp, dptr, C.POINTER(C.c_int), C.c_long, C.POINTER(C.c_long)]
+    L.scy_cycle_set_mode.argtypes = [vp, C.c_int]
+    L.scy_cycle_set_jacobian.argtypes = [vp, C.c_int]
+    L.scy_cycle_set_fd_batch.argtypes = [vp, C.c_int]
+    L.scy_cycle_time_kernels.argtypes = [vp, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    L.scy_cycle_set_fd_state.argtypes = [vp, C.c_double, C.c_long, C.c_int] + [dptr] * 10
+    L.scy_in_cycle_info.argtypes = [C.c_char_p, C.POINTER(CycleDesc), C.POINTER(C.c_double), dptr, C.c_long,
+                                    C.POINTER(C.c_long)]
+    return L

@@ -6,7 +6,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libscycle_b200.so")
-SOURCES = ["capi.cu", "sbp_solver.cu", "sbp_host.cpp", "qd.cu", "infile.cpp", "noalloc.cu", "fdiag.cu"]
+SOURCES = ["capi.cu", "sbp_solver.cu", "sbp_host.cpp", "qd.cu", "infile.cpp", "noalloc.cu", "fdiag.cu", "cycle.cu",
+           "cycle_host.cpp"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC", "-Xcompiler", "-O3", "--expt-relaxed-constexpr"]
 
@@ -28,14 +29,44 @@ def needs_build():
 
 
 def build(force=False, verbose=True):
+    """Compiles the sources in parallel (one nvcc per file) and links."""
     if not force and not needs_build():
         return LIB
+    from concurrent.futures import ThreadPoolExecutor
+    import tempfile
+    objdir = tempfile.mkdtemp(prefix="scy_build_")
     srcs = [os.path.join(CSRC, s) for s in SOURCES]
-    cmd = [nvcc(), *NVCC_FLAGS, "-shared", "-o", LIB + ".tmp", *srcs, "-lcudart", "-lcublas", "-lcusolver"]
+    objs = [os.path.join(objdir, os.path.basename(s) + ".o") for s in srcs]
+
+    def compile_one(pair):
+        src, obj = pair
+        cmd = [nvcc(), *NVCC_FLAGS, "-c", src, "-o", obj]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        return subprocess.run(cmd, capture_output=True, text=True)
+
+    with ThreadPoolExecutor(max_workers=min(len(srcs), os.cpu_count() or 4)) as ex:
+        results = list(ex.map(compile_one, zip(srcs, objs)))
+    for r in results:
+        if r.stderr:
+            sys.stderr.write(r.stderr)
+    bad = [s for s, r in zip(srcs, results) if r.returncode != 0]
+    if bad:
+        raise subprocess.CalledProcessError(1, "nvcc", "failed: %s" % ", ".join(bad))
+    cmd = [nvcc(), *NVCC_FLAGS, "-shared", "-o", LIB + ".tmp", *objs, "-lcudart", "-lcublas", "-lcusolver"]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)
     os.replace(LIB + ".tmp", LIB)
+    for o in objs:
+        try:
+            os.remove(o)
+        except OSError:
+            pass
+    try:
+        os.rmdir(objdir)
+    except OSError:
+        pass
     return LIB
 
 

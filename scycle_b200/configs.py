@@ -44,7 +44,7 @@ gridSpacingType = {grid}
 inputDir = {inputDir}
 outputDir = {outputDir}
 bulkDeformationType = linearElastic
-momentumBalanceType = quasidynamic
+momentumBalanceType = {mbt}
 stateLaw = {stateLaw}
 guessSteadyStateICs = {guess}
 f0 = 0.6
@@ -83,7 +83,8 @@ def tanh_stretch(n, L, beta):
 def make_qd_problem(workdir, Ny=101, Nz=101, Ly=30.0, Lz=30.0, order=4, seed=0,
                     grid="constantGridSpacing", state_law="agingLaw", integrator="RK32",
                     tol=1e-7, years=200.0, max_steps=100000000, init_dt=1e-3,
-                    stretch_beta=None, dc_lognormal=False, name="qd", guess_ss=0):
+                    stretch_beta=None, dc_lognormal=False, name="qd", guess_ss=0,
+                    mbt="quasidynamic", extra=None):
     """Write ``<workdir>/<name>.in`` and its inputDir fields; return the .in path."""
     os.makedirs(workdir, exist_ok=True)
     rng = np.random.default_rng(seed)
@@ -93,9 +94,15 @@ def make_qd_problem(workdir, Ny=101, Nz=101, Ly=30.0, Lz=30.0, order=4, seed=0,
                           inputDir=input_dir, outputDir=out_dir, stateLaw=state_law,
                           integrator=integrator, maxStepCount=int(max_steps),
                           maxTime=repr(float(years * YEAR)), initDeltaT=repr(float(init_dt)), tol=repr(float(tol)),
-                          guess=int(guess_ss))
+                          guess=int(guess_ss), mbt=mbt)
+    if extra:
+        text += "".join("%s = %s\n" % (k, v) for k, v in extra.items())
     psi = 0.6 + rng.normal(0.0, 1e-4, size=Nz)
     write_petsc_vec(input_dir + "psi", psi)
+    # fields a previous problem of the same name may have left behind
+    for nm, keep in (("y", stretch_beta is not None), ("z", stretch_beta is not None), ("Dc", dc_lognormal)):
+        if not keep and os.path.exists(input_dir + nm):
+            os.remove(input_dir + nm)
     if stretch_beta is not None:
         yv = tanh_stretch(Ny, Ly, stretch_beta)
         zv = tanh_stretch(Nz, Lz, stretch_beta)
@@ -109,6 +116,26 @@ def make_qd_problem(workdir, Ny=101, Nz=101, Ly=30.0, Lz=30.0, order=4, seed=0,
     with open(path, "w") as f:
         f.write(text)
     return path
+
+
+def make_qdfd_problem(workdir, Ny=801, Nz=801, Ly=30.0, Lz=30.0, seed=0, cycles=3, trigger=1e-3,
+                      name="qdfd", integrator="RK43", tol=1e-7, years=1000.0, min_dt=1e-3, **kw):
+    """Quasi-dynamic / fully dynamic switching (momentumBalanceType
+    quasidynamic_and_dynamic): order-4 constant grid, cs = sqrt(32.04/2.67)
+    = 3.464 km/s, switch to the wave equation when max(eta V / tau) exceeds
+    ``trigger``, CFL-limited fully dynamic step, ``cycles`` full cycles."""
+    extra = {"maxNumCycles": int(cycles), "trigger_qd2fd": repr(float(trigger)),
+             "trigger_fd2qd": repr(float(trigger)), "minDeltaT": repr(float(min_dt))}
+    extra.update(kw.pop("extra", {}) or {})
+    args = dict(Ny=Ny, Nz=Nz, Ly=Ly, Lz=Lz, seed=seed, name=name, integrator=integrator, tol=tol,
+                years=years, guess_ss=1, mbt="quasidynamic_and_dynamic", extra=extra)
+    args.update(kw)
+    return make_qd_problem(workdir, **args)
+
+
+def qdfd_const_801(workdir, seed=0, **kw):
+    """801x801 order-4 constant grid on 30 km, three full cycles."""
+    return make_qdfd_problem(workdir, Ny=801, Nz=801, seed=seed, name="qdfd_const_801", **kw)
 
 
 def aging_const_101(workdir, seed=0, **kw):

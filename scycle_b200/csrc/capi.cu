@@ -3,10 +3,13 @@
 #include <stdexcept>
 #include <vector>
 
+#include <memory>
+
 #include "common.cuh"
+#include "cycle.hpp"
+#include "cycle_host.hpp"
 #include "infile.hpp"
 #include "qd.hpp"
-#include <memory>
 #include "sbp_solver.hpp"
 
 struct scy_sbp {
@@ -17,6 +20,22 @@ struct scy_qd {
   scy::QDContext ctx;
   std::unique_ptr<scy::QDProblem> prob;  // set by scy_qd_create_from_in
 };
+
+struct scy_cycle {
+  scy::CycleContext ctx;
+  std::unique_ptr<scy::QDProblem> prob;  // set by scy_cycle_create_from_in
+};
+
+namespace {
+void default_solve(scy_solve_opts& o) {
+  o.rtol = 1e-12;
+  o.atol = 0.0;
+  o.max_its = 300;
+  o.precision = SCY_PREC_FP64;
+  o.nonzero_guess = 1;
+  o.check_every = 1;
+}
+}  // namespace
 
 extern "C" {
 
@@ -450,6 +469,238 @@ scy_status scy_in_problem_info(const char* path, scy_grid_desc* grid, scy_ode_op
   if (state_law) *state_law = P.desc.fault.state_law;
   if (guess_ss) *guess_ss = P.guess_ss;
   if (fault_type_scale) *fault_type_scale = P.desc.fault_type_scale;
+  return SCY_OK;
+}
+
+// ---------------------------------------------------------------------------
+// quasi-dynamic / fully dynamic cycles
+
+scy_status scy_in_cycle_info(const char* path, scy_cycle_desc* cd, double* dt_fd, double* ay, long cap, long* n) {
+  if (!path) return SCY_ERR_ARG;
+  scy::QDProblem P;
+  try {
+    scy::load_qd_problem(path, P, 1);
+    const scy_grid_desc& g = P.desc.grid;
+    const int nm[4] = {SCY_BC_NEUMANN, SCY_BC_NEUMANN, SCY_BC_NEUMANN, SCY_BC_NEUMANN};
+    scy::LevelHost h = scy::build_level(g.order, g.Ny, g.Nz, g.Ly, g.Lz, g.grid_type, g.compat, P.y, P.z, P.mu, nm);
+    if (cd) {
+      *cd = P.cdesc;
+      cd->rho = cd->cs = cd->rho_fault = nullptr;
+    }
+    if (dt_fd) *dt_fd = scy::cycle_time_step(h, P.cs, P.cdesc.deltaT_fd, P.cdesc.CFL);
+    if (n) {
+      const double h11 = g.order == 2 ? 0.5 : 17.0 / 48.0;
+      std::vector<double> a = scy::penalty_ay(g.Ny, g.Nz, h11 * h.dy, h11 * h.dz, P.cdesc.fd_bcR == SCY_FD_OUTGOING,
+                                              P.cdesc.fd_bcT == SCY_FD_OUTGOING, P.cdesc.fd_bcB == SCY_FD_OUTGOING,
+                                              P.cdesc.ay_index_quirk, P.cs);
+      *n = (long)a.size();
+      if (ay)
+        for (long i = 0; i < *n && i < cap; ++i) ay[i] = a[i];
+    }
+  } catch (const std::exception& e) {
+    scy::set_error("%s", e.what());
+    return SCY_ERR_IO;
+  }
+  return SCY_OK;
+}
+
+scy_status scy_cycle_create(const scy_qd_desc* qd, const scy_cycle_desc* cd, scy_cycle** out) {
+  if (!qd || !cd || !out) {
+    scy::set_error("scy_cycle_create: NULL argument");
+    return SCY_ERR_ARG;
+  }
+  *out = nullptr;
+  scy_cycle* c = new (std::nothrow) scy_cycle();
+  if (!c) return SCY_ERR_NOMEM;
+  int st = c->ctx.create(*qd, *cd);
+  if (st != SCY_OK) {
+    delete c;
+    return st;
+  }
+  *out = c;
+  return SCY_OK;
+}
+
+scy_status scy_cycle_create_from_in(const char* path, const scy_solve_opts* solve, scy_cycle** out) {
+  if (!path || !out) {
+    scy::set_error("scy_cycle_create_from_in: NULL argument");
+    return SCY_ERR_ARG;
+  }
+  *out = nullptr;
+  std::unique_ptr<scy::QDProblem> P(new (std::nothrow) scy::QDProblem());
+  if (!P) return SCY_ERR_NOMEM;
+  try {
+    scy::load_qd_problem(path, *P, 1);
+  } catch (const std::exception& e) {
+    scy::set_error("%s", e.what());
+    return SCY_ERR_IO;
+  }
+  if (solve)
+    P->desc.solve = *solve;
+  else
+    default_solve(P->desc.solve);
+  scy_cycle* c = new (std::nothrow) scy_cycle();
+  if (!c) return SCY_ERR_NOMEM;
+  int st = c->ctx.create(P->desc, P->cdesc);
+  if (st != SCY_OK) {
+    delete c;
+    return st;
+  }
+  c->prob = std::move(P);
+  *out = c;
+  return SCY_OK;
+}
+
+scy_status scy_cycle_destroy(scy_cycle* c) {
+  delete c;
+  return SCY_OK;
+}
+
+scy_status scy_cycle_get_problem(scy_cycle* c, int* Ny, int* Nz, double* dt_fd, scy_ode_opts* ode) {
+  if (!c) return SCY_ERR_ARG;
+  if (Ny) *Ny = c->ctx.Ny;
+  if (Nz) *Nz = c->ctx.Nz;
+  if (dt_fd) *dt_fd = c->ctx.dt_fd;
+  if (ode) {
+    if (!c->prob) {
+      scy::set_error("driver was not created from an input file");
+      return SCY_ERR_STATE;
+    }
+    *ode = c->prob->ode;
+  }
+  return SCY_OK;
+}
+
+scy_status scy_cycle_begin(scy_cycle* c, const scy_ode_opts* o, const double* var0) {
+  if (!c || !o || !var0) {
+    scy::set_error("scy_cycle_begin: NULL argument");
+    return SCY_ERR_ARG;
+  }
+  if (!(o->tol > 0) || !(o->max_dt >= o->min_dt) || !(o->t1 >= o->t0) || o->max_steps < 0 || o->n_err > 2 ||
+      (o->method != SCY_RK32 && o->method != SCY_RK43)) {
+    scy::set_error("scy_cycle_begin: invalid options");
+    return SCY_ERR_ARG;
+  }
+  return c->ctx.begin(*o, var0);
+}
+
+scy_status scy_cycle_begin_from_in(scy_cycle* c) {
+  if (!c || !c->prob) {
+    scy::set_error("scy_cycle_begin_from_in: driver was not created from an input file");
+    return SCY_ERR_STATE;
+  }
+  scy::QDProblem& P = *c->prob;
+  scy::QDContext& q = c->ctx.q;
+  const int Nz = q.Nz;
+  std::vector<double> psi = P.psi, slip(Nz);
+  for (int i = 0; i < Nz; ++i) slip[i] = P.bcL0[i] * P.desc.fault_type_scale;
+  if (!P.slip_file.empty()) slip = P.slip_file;
+  if (P.guess_ss) SCY_TRY(q.steady_state_guess(psi, P.stateVals_given, slip));
+  std::vector<double> var0(2 * (size_t)Nz);
+  std::copy(psi.begin(), psi.end(), var0.begin());
+  std::copy(slip.begin(), slip.end(), var0.begin() + Nz);
+  return c->ctx.begin(P.ode, var0.data());
+}
+
+scy_status scy_cycle_run(scy_cycle* c, long max_steps, scy_cycle_stats* st) {
+  if (!c || max_steps < 0) {
+    scy::set_error("scy_cycle_run: invalid argument");
+    return SCY_ERR_ARG;
+  }
+  int rc = c->ctx.run(max_steps, st);
+  if (rc != SCY_OK && st) c->ctx.fill_stats(st);
+  return rc;
+}
+
+scy_status scy_cycle_get_field(scy_cycle* c, int field, double* out) {
+  if (!c || !out) return SCY_ERR_ARG;
+  return c->ctx.get_field(field, out);
+}
+
+scy_status scy_cycle_get_switches(scy_cycle* c, long* steps, double* times, int* to_fd, long cap, long* n) {
+  if (!c || !n) return SCY_ERR_ARG;
+  const auto& sw = c->ctx.switches;
+  *n = (long)sw.size();
+  for (long i = 0; i < (long)sw.size() && i < cap; ++i) {
+    if (steps) steps[i] = sw[i].step;
+    if (times) times[i] = sw[i].t;
+    if (to_fd) to_fd[i] = sw[i].to_fd;
+  }
+  return SCY_OK;
+}
+
+scy_status scy_cycle_set_fd_state(scy_cycle* c, double t, long step, int allowed, const double* psi,
+                                  const double* slip, const double* u, const double* psiPrev,
+                                  const double* slipPrev, const double* uPrev, const double* u0,
+                                  const double* slip0, const double* tau0, const double* slipVel) {
+  if (!c || !psi || !slip || !u || !psiPrev || !slipPrev || !uPrev || !u0 || !slip0 || !tau0 || !slipVel) {
+    scy::set_error("scy_cycle_set_fd_state: NULL argument");
+    return SCY_ERR_ARG;
+  }
+  const double* now[2] = {psi, slip};
+  const double* prev[2] = {psiPrev, slipPrev};
+  return c->ctx.set_fd_state(t, step, allowed, now, u, prev, uPrev, u0, slip0, tau0, slipVel);
+}
+
+scy_status scy_cycle_time_kernels(scy_cycle* c, int reps, double* wave_us, double* fault_us) {
+  if (!c) return SCY_ERR_ARG;
+  return c->ctx.time_kernels(reps, wave_us, fault_us);
+}
+
+scy_status scy_cycle_force_attempts(scy_cycle* c, const double* dts, const int* acc, long n) {
+  if (!c || n < 0 || (n > 0 && (!dts || !acc))) return SCY_ERR_ARG;
+  scy::QDContext& q = c->ctx.q;
+  q.forced_dt.assign(dts, dts + n);
+  q.forced_acc.assign(acc, acc + n);
+  q.forced_pos = 0;
+  return SCY_OK;
+}
+
+scy_status scy_cycle_record_attempts(scy_cycle* c, int on) {
+  if (!c) return SCY_ERR_ARG;
+  scy::QDContext& q = c->ctx.q;
+  q.record = on ? 1 : 0;
+  if (on) {
+    q.log_dt.clear();
+    q.log_acc.clear();
+  }
+  return SCY_OK;
+}
+
+scy_status scy_cycle_get_attempts(scy_cycle* c, double* dts, int* acc, long cap, long* n) {
+  if (!c || !n) return SCY_ERR_ARG;
+  const scy::QDContext& q = c->ctx.q;
+  long m = (long)q.log_dt.size();
+  *n = m;
+  for (long i = 0; i < m && i < cap; ++i) {
+    if (dts) dts[i] = q.log_dt[i];
+    if (acc) acc[i] = q.log_acc[i];
+  }
+  return SCY_OK;
+}
+
+scy_status scy_cycle_set_mode(scy_cycle* c, int mode) {
+  if (!c || (mode != SCY_QD_MODE_SOLVE && mode != SCY_QD_MODE_RESPONSE)) {
+    scy::set_error("scy_cycle_set_mode: unknown mode");
+    return SCY_ERR_ARG;
+  }
+  c->ctx.q.mode = mode;
+  c->ctx.q.green_ready = 0;
+  return SCY_OK;
+}
+
+scy_status scy_cycle_set_jacobian(scy_cycle* c, int exact) {
+  if (!c) return SCY_ERR_ARG;
+  c->ctx.q.fp.jacobian = exact ? 1 : 0;
+  return SCY_OK;
+}
+
+scy_status scy_cycle_set_fd_batch(scy_cycle* c, int steps) {
+  if (!c || steps < 1 || steps > 4096) {
+    scy::set_error("scy_cycle_set_fd_batch: steps must be in 1..4096");
+    return SCY_ERR_ARG;
+  }
+  c->ctx.fd_batch = steps;
   return SCY_OK;
 }
 

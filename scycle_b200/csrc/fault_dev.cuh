@@ -43,19 +43,19 @@ __device__ __forceinline__ void resid_qd(double V, double tauQS, double eta, dou
   J = (exact ? A * B / s : A * V / s) + eta;
 }
 
-// Safeguarded Newton on [left, right] starting from x0.  Returns the root;
-// sets *its and *ok.  Every loop is bounded by max_its.
-__device__ __forceinline__ double bracketed_newton(double left, double right, double x0, double atol, int max_its,
-                                                   double tauQS, double eta, double sN, double psi, double a,
-                                                   double v0, int exact, int* its, bool* ok) {
+// Safeguarded Newton on [left, right] starting from x0 for the residual
+// R(x, f, f'), following BracketedNewton::findRoot (rootFinder.cpp:174-257).
+// Returns the root; sets *its and *ok.  Every loop is bounded by max_its.
+template <class Resid>
+__device__ __forceinline__ double bracketed_newton_f(const Resid& R, double left, double right, double x0,
+                                                     double atol, int max_its, int* its, bool* ok) {
   double f, fp, fl, fr, dum;
-  const double E = exp(psi / a);
   *its = 0;
   *ok = true;
-  resid_qd(x0, tauQS, eta, sN, E, a, v0, exact, f, fp);
+  R(x0, f, fp);
   if (fabs(f) <= atol) return x0;
-  resid_qd(left, tauQS, eta, sN, E, a, v0, exact, fl, dum);
-  resid_qd(right, tauQS, eta, sN, E, a, v0, exact, fr, dum);
+  R(left, fl, dum);
+  R(right, fr, dum);
   if (!isfinite(fl) || !isfinite(fr)) {
     *ok = false;
     return x0;
@@ -69,7 +69,7 @@ __device__ __forceinline__ double bracketed_newton(double left, double right, do
   }
   double x = x0;
   double dxold = fabs(right - left), dx = dxold;
-  resid_qd(x, tauQS, eta, sN, E, a, v0, exact, f, fp);
+  R(x, f, fp);
   int n = 0;
   while (n <= max_its && fabs(f) >= atol) {
     if (((x - right) * fp - f) * ((x - left) * fp - f) > 0.0 || fabs(2.0 * f) > fabs(dxold * fp)) {
@@ -81,7 +81,7 @@ __device__ __forceinline__ double bracketed_newton(double left, double right, do
       dx = f / fp;
       x -= dx;
     }
-    resid_qd(x, tauQS, eta, sN, E, a, v0, exact, f, fp);
+    R(x, f, fp);
     if (f < 0.0)
       left = x;
     else
@@ -92,6 +92,22 @@ __device__ __forceinline__ double bracketed_newton(double left, double right, do
   if (!(fabs(f) <= atol)) *ok = false;
   if (!isfinite(f)) *ok = false;
   return x;
+}
+
+// Quasi-dynamic slip-velocity residual (ComputeVel_qd::getResid).
+struct ResidQD {
+  double tauQS, eta, sN, E, a, v0;
+  int exact;
+  __device__ __forceinline__ void operator()(double V, double& f, double& J) const {
+    resid_qd(V, tauQS, eta, sN, E, a, v0, exact, f, J);
+  }
+};
+
+__device__ __forceinline__ double bracketed_newton(double left, double right, double x0, double atol, int max_its,
+                                                   double tauQS, double eta, double sN, double psi, double a,
+                                                   double v0, int exact, int* its, bool* ok) {
+  const ResidQD R{tauQS, eta, sN, exp(psi / a), a, v0, exact};
+  return bracketed_newton_f(R, left, right, x0, atol, max_its, its, ok);
 }
 
 __device__ __forceinline__ double aging_law_psi(double psi, double V, double b, double f0, double v0, double Dc) {
@@ -108,5 +124,45 @@ __device__ __forceinline__ double slip_law_psi(double psi, double V, double a, d
   double f = a * asinh((absV / 2.0 / v0) * exp(psi / a));
   return -absV / Dc * (f - fss);
 }
+
+}  // namespace scy
+
+namespace scy {
+
+// Fully dynamic slip-velocity residual (ComputeVel_fd::getResid,
+// fault.cpp:1649-1685): fricPen*strength(V) - (|Phi| - V), exact derivative.
+struct ResidVelFD {
+  double absPhi, fricPen, sN, psi, a, v0, E;
+  __device__ __forceinline__ void operator()(double V, double& f, double& J) const {
+    const double constraints = fricPen * (a * sN * asinh((0.5 * V / v0) * E));
+    const double stress = absPhi - V;
+    f = constraints - stress;
+    const double A = a * sN;
+    const double B = E / (2. * v0);
+    J = 1 + fricPen * A * B / sqrt(1. + B * B * V * V);
+  }
+};
+
+// Implicit-midpoint state residuals of the fully dynamic phase
+// (ComputeAging_fd / ComputeSlipLaw_fd ::getResid, fault.cpp:1750-1763,
+// :1851-1865): -2 dt G((psiPrev + state)/2, V) + (state - psiPrev).
+struct ResidAgingFD {
+  double psiPrev, V, b, f0, v0, Dc, dt;
+  __device__ __forceinline__ void operator()(double state, double& f, double& J) const {
+    const double G = aging_law_psi((psiPrev + state) / 2.0, V, b, f0, v0, Dc);
+    f = -2 * dt * G + (state - psiPrev);
+    J = 1 + dt * v0 / Dc * exp((f0 - (psiPrev + state) / 2.) / b);
+  }
+};
+
+struct ResidSlipFD {
+  double psiPrev, V, a, b, f0, v0, Dc, dt;
+  __device__ __forceinline__ void operator()(double state, double& f, double& J) const {
+    const double G = slip_law_psi((psiPrev + state) / 2.0, V, a, b, f0, v0, Dc);
+    f = -2 * dt * G + (state - psiPrev);
+    const double A = fabs(V) / 2. / v0 * exp((psiPrev + state) / 2.0 / a);
+    J = 1 + dt * fabs(V) / Dc * A / sqrt(1 + A * A);
+  }
+};
 
 }  // namespace scy

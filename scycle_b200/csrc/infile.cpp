@@ -162,7 +162,7 @@ static int parse_bc(const std::string& t) {
   throw std::runtime_error("unknown boundary condition type '" + t + "'");
 }
 
-void load_qd_problem(const std::string& path, QDProblem& P) {
+void load_qd_problem(const std::string& path, QDProblem& P, int cycle) {
   const std::vector<InEntry> E = parse_in_file(path);
   // ---- Domain (domain.cpp:8-16, :133-196, :233-262)
   int order = 4, Ny = -1, Nz = -1;
@@ -188,7 +188,11 @@ void load_qd_problem(const std::string& path, QDProblem& P) {
   }
   if (bCoordTrans > 0.0) gridType = "variableGridSpacing";
   if (bulk != "linearElastic") throw std::runtime_error("bulkDeformationType '" + bulk + "' is not the linear-elastic path");
-  if (momBal != "quasidynamic") throw std::runtime_error("momentumBalanceType '" + momBal + "' is not the quasi-dynamic path");
+  if (!cycle && momBal != "quasidynamic")
+    throw std::runtime_error("momentumBalanceType '" + momBal + "' is not the quasi-dynamic path");
+  if (cycle && momBal != "quasidynamic_and_dynamic")
+    throw std::runtime_error("momentumBalanceType '" + momBal + "' is not the quasi-dynamic / fully dynamic path");
+  P.cycle = cycle;
   if (order != 2 && order != 4) throw std::runtime_error("order must be 2 or 4");
   if (Ny < 2 || Nz < 2) throw std::runtime_error("Ny and Nz must both exceed 1");
   if (!(Ly > 0) || !(Lz > 0)) throw std::runtime_error("Ly and Lz must be positive");
@@ -285,7 +289,16 @@ void load_qd_problem(const std::string& path, QDProblem& P) {
   std::string timeIntegrator = "RK43", timeControlType = "PID", normType = "L2_absolute";
   std::string bcRType = "remoteLoading", bcTType = "freeSurface", bcLType = "symmFault", bcBType = "freeSurface";
   long maxStepCount = 100000000;
-  double initTime = 0, maxTime = 1e15, minDeltaT = -1, maxDeltaT = 1e10, initDeltaT = 1e-3, timeStepTol = 1e-8;
+  // the cycle driver's constructor sets minDeltaT = 1e-3 where the
+  // quasi-dynamic driver leaves -1 for computeMinTimeStep
+  // (strikeSlip_linearElastic_qd_fd.cpp:25)
+  double initTime = 0, maxTime = 1e15, minDeltaT = cycle ? 1e-3 : -1, maxDeltaT = 1e10, initDeltaT = 1e-3,
+         timeStepTol = 1e-8;
+  // strikeSlip_linearElastic_qd_fd keys and defaults (:8-33, :135-230)
+  double trig_qd2fd = 1e-3, trig_fd2qd = 1e-3, limit_qd = 10 * 1e-9, limit_fd = 1e-1, limit_stride_fd = -1;
+  double deltaT_fd = -1, CFL = -1;
+  int maxNumCycles = 1000;
+  std::string fdR = "outGoingCharacteristics", fdT = "freeSurface", fdL = "symmFault", fdB = "outGoingCharacteristics";
   double vL = 1e-9;
   std::vector<std::string> timeIntInds;
   std::vector<double> scale;
@@ -316,6 +329,18 @@ void load_qd_problem(const std::string& path, QDProblem& P) {
     else if (e.var == "momBal_bcT_qd") bcTType = e.rhs;
     else if (e.var == "momBal_bcL_qd") bcLType = e.rhs;
     else if (e.var == "momBal_bcB_qd") bcBType = e.rhs;
+    else if (cycle && e.var == "trigger_qd2fd") trig_qd2fd = c_atof(e.rhs);
+    else if (cycle && e.var == "trigger_fd2qd") trig_fd2qd = c_atof(e.rhs);
+    else if (cycle && e.var == "limit_qd") limit_qd = c_atof(e.rhs);
+    else if (cycle && e.var == "limit_fd") limit_fd = c_atof(e.rhs);
+    else if (cycle && e.var == "limit_stride_fd") limit_stride_fd = c_atof(e.rhs);
+    else if (cycle && e.var == "deltaT_fd") deltaT_fd = c_atof(e.rhs);
+    else if (cycle && e.var == "CFL") CFL = c_atof(e.rhs);
+    else if (cycle && e.var == "maxNumCycles") maxNumCycles = c_atoi(e.rhs);
+    else if (cycle && e.var == "momBal_bcR_fd") fdR = e.rhs;
+    else if (cycle && e.var == "momBal_bcT_fd") fdT = e.rhs;
+    else if (cycle && e.var == "momBal_bcL_fd") fdL = e.rhs;
+    else if (cycle && e.var == "momBal_bcB_fd") fdB = e.rhs;
   }
   if (thermal != "no" || hydraulic != "no") throw std::runtime_error("thermal / hydraulic coupling is outside this path");
   if (forcing != "no") throw std::runtime_error("forcingType '" + forcing + "' is outside this path");
@@ -402,6 +427,36 @@ void load_qd_problem(const std::string& path, QDProblem& P) {
     o.err_scale[i] = scale.empty() ? 1.0 : (i < scale.size() ? scale[i] : 1.0);
   }
   if (!scale.empty() && scale.size() != timeIntInds.size()) throw std::runtime_error("scale and timeIntInds differ in length");
+  if (!cycle) return;
+  // ---- strikeSlip_linearElastic_qd_fd::checkInput (:232-305)
+  auto fd_side = [](const std::string& t, const char* key) {
+    if (t == "outGoingCharacteristics") return (int)SCY_FD_OUTGOING;
+    if (t == "freeSurface") return (int)SCY_FD_FREE_SURFACE;
+    throw std::runtime_error(std::string(key) + " must be freeSurface or outGoingCharacteristics");
+  };
+  if (fdL != "symmFault" && fdL != "rigidFault") throw std::runtime_error("momBal_bcL_fd must be symmFault or rigidFault");
+  if (stateLaw != "agingLaw" && stateLaw != "slipLaw")
+    throw std::runtime_error("the fully dynamic phase needs stateLaw agingLaw or slipLaw");
+  if (limit_fd < trig_qd2fd) limit_fd = 10 * trig_qd2fd;
+  if (limit_qd > trig_fd2qd) limit_qd = trig_qd2fd / 10.0;
+  if (limit_stride_fd == -1) limit_stride_fd = limit_fd / 10.0;
+  scy_cycle_desc& c = P.cdesc;
+  c.rho = P.rho.data();
+  c.cs = P.cs.data();
+  c.rho_fault = P.rho_f.data();
+  c.fd_bcR = fd_side(fdR, "momBal_bcR_fd");
+  c.fd_bcT = fd_side(fdT, "momBal_bcT_fd");
+  c.fd_bcB = fd_side(fdB, "momBal_bcB_fd");
+  c.deltaT_fd = deltaT_fd;
+  c.CFL = CFL;
+  c.trigger_qd2fd = trig_qd2fd;
+  c.trigger_fd2qd = trig_fd2qd;
+  c.limit_qd = limit_qd;
+  c.limit_fd = limit_fd;
+  c.max_num_cycles = maxNumCycles;
+  c.ay_index_quirk = 1;
+  // initiateIntegrands reads inputDir/slip when present (:678)
+  if (!read_petsc_vec(P.inputDir + "slip", Nz, P.slip_file)) P.slip_file.clear();
 }
 
 }  // namespace scy

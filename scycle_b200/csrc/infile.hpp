@@ -45,11 +45,16 @@ struct QDProblem {
   std::vector<double> a, b, sN, Dc, locked, prestress, psi, eta, mu_f, rho_f;
   std::vector<double> bcL0, bcRShift;
   int stateVals_given = 0;
+  // strikeSlip_linearElastic_qd_fd only (cycle = 1)
+  int cycle = 0;
+  scy_cycle_desc cdesc{};
+  std::vector<double> slip_file;  // inputDir/slip, empty if absent
 };
 
 // Builds the problem like Domain + LinearElastic + Fault_qd +
-// StrikeSlip_LinearElastic_qd constructors do.  Throws std::runtime_error
-// with a message on invalid input.
-void load_qd_problem(const std::string& path, QDProblem& P);
+// StrikeSlip_LinearElastic_qd constructors do, or (cycle = 1) like
+// strikeSlip_linearElastic_qd_fd's.  Throws std::runtime_error with a
+// message on invalid input.
+void load_qd_problem(const std::string& path, QDProblem& P, int cycle = 0);
 
 }  // namespace scy

@@ -690,6 +690,33 @@ int QDContext::integrate_begin(const scy_ode_opts& o) {
   return read_flags();
 }
 
+int QDContext::phase_begin(double t0, double t1, double init_dt, double min_dt, double max_dt, long step0,
+                           long max_rel) {
+  if (ode.method != SCY_RK32 && ode.method != SCY_RK43) {
+    set_error("phase_begin: integrator settings missing");
+    return SCY_ERR_STATE;
+  }
+  ode.t0 = t0;
+  ode.t1 = t1;
+  ode.init_dt = init_dt;
+  ode.min_dt = min_dt;
+  ode.max_dt = max_dt;
+  ode.max_steps = step0 + max_rel;
+  totTol = ode.tol;
+  currT = t0;
+  deltaT = init_dt;
+  newDeltaT = init_dt;
+  stepCount = step0;
+  numRejected = numMin = numMax = 0;
+  errA[0] = errA[1] = 0.0;
+  phase_stopped = 0;
+  if (deltaT == 0) deltaT = (t1 - t0) / (double)ode.max_steps;
+  ode_ready = 1;
+  if (ode.max_steps == 0) return SCY_OK;
+  SCY_TRY(d_dt(currT, rk[V_VAR].as<double>(), rk[V_DVAR].as<double>()));
+  return read_flags();
+}
+
 int QDContext::integrate_steps(long nsteps, scy_ode_stats* st) {
   if (!ode_ready) {
     set_error("integrate_steps called before integrate_begin");
@@ -739,8 +766,16 @@ int QDContext::integrate_steps(long nsteps, scy_ode_stats* st) {
     errA[1] = errA[0];
     errA[0] = totErr;
     last_dt = deltaT;
-    deltaT = newDeltaT;
     ++done_steps;
+    if (monitor) {
+      int stop = 0;
+      SCY_TRY(monitor(&stop));
+      if (stop) {
+        phase_stopped = 1;
+        break;
+      }
+    }
+    deltaT = newDeltaT;
   }
   if (st) {
     st->t = currT;

@@ -1,6 +1,7 @@
 // Linear-elastic quasi-dynamic strike-slip driver on the device: the d_dt of
 // StrikeSlip_LinearElastic_qd and the adaptive RK32 / RK43 integrators.
 #pragma once
+#include <functional>
 #include <vector>
 
 #include "fault_dev.cuh"
@@ -61,7 +62,17 @@ struct QDContext {
   // f = d_dt(t, var) with var = [psi | slip] and f = [dpsi | dslip] (device, 2*Nz each)
   int d_dt(double t, const double* var, double* f);
   int integrate_begin(const scy_ode_opts& o);
+  // A fresh integrator object of a driver that restarts the RK per phase
+  // (strikeSlip_linearElastic_qd_fd.cpp:1436-1508, :891-956): time range
+  // [t0, t1], first step init_dt, bounds [min_dt, max_dt], step count
+  // continuing from step0 with max_rel more steps allowed, empty error
+  // history; evaluates the rates at t0.
+  int phase_begin(double t0, double t1, double init_dt, double min_dt, double max_dt, long step0, long max_rel);
   int integrate_steps(long nsteps, scy_ode_stats* st);
+  // Called after every accepted step (timeMonitor); a nonzero *stop ends
+  // the phase (integrate_steps returns with phase_stopped = 1).
+  std::function<int(int* stop)> monitor;
+  int phase_stopped = 0;
   double compute_step_size(double totErr);
   int compute_error(const double* lo, const double* hi, double* err);
   int attempt(double dt, double** lo, double** hi);

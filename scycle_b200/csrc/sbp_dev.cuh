@@ -42,6 +42,13 @@ struct LevelDev {
   int Ny, Nz, var;
   DirDev<T> y, z;
   const T *cy, *cz, *m3y, *m3z, *wy, *wz, *mu, *qy, *rz, *dinv;
+  // Separable interior: when sep = 1 every node of the interior box
+  // [4, Ny-6] x [4, Nz-6] has cy, m3y, wz depending on iy only and cz, m3z,
+  // wy on iz only (checked bitwise on the host), so interior tiles read these
+  // 1D arrays (L1-resident) instead of six per-node fields.
+  int sep;
+  const T *cy1, *m3y1, *wz1;  // Ny
+  const T *cz1, *m3z1, *wy1;  // Nz
 };
 
 // -------------------------------------------------------------------------
@@ -88,14 +95,14 @@ struct LoadProlong {
 };
 
 // -------------------------------------------------------------------------
-// Epilogues: consume (A x)_node and the operand value x_node; return a
-// contribution to the optional block/grid sum.
+// Epilogues: consume (A x) and the operand value x at the node (index and
+// coordinates); return a contribution to the optional block/grid sum.
 template <typename T>
 struct EpiStore {
   T* out;
   T scale;
   static constexpr bool kReduce = false;
-  __device__ __forceinline__ double operator()(long node, T Ax, T) const {
+  __device__ __forceinline__ double operator()(long node, int, int, T Ax, T) const {
     out[node] = scale * Ax;
     return 0.0;
   }
@@ -108,7 +115,7 @@ struct EpiResidual {
   T* r;
   T sign_b;
   static constexpr bool kReduce = true;
-  __device__ __forceinline__ double operator()(long node, T Ax, T) const {
+  __device__ __forceinline__ double operator()(long node, int, int, T Ax, T) const {
     T v = sign_b * (T)b[node] + Ax;
     r[node] = v;
     return (double)v * (double)v;
@@ -120,7 +127,7 @@ struct EpiCGMatvec {
   double* pnew;
   double* q;
   static constexpr bool kReduce = true;
-  __device__ __forceinline__ double operator()(long node, double Ax, double p) const {
+  __device__ __forceinline__ double operator()(long node, int, int, double Ax, double p) const {
     double qv = -Ax;
     pnew[node] = p;
     q[node] = qv;
@@ -137,7 +144,7 @@ struct EpiCheb {
   T* xout;
   T c1, c2;
   static constexpr bool kReduce = false;
-  __device__ __forceinline__ double operator()(long node, T Ax, T xv) const {
+  __device__ __forceinline__ double operator()(long node, int, int, T Ax, T xv) const {
     T res = b[node] + Ax;
     T dv = c2 * dinv[node] * res;
     if (c1 != T(0)) dv += c1 * d[node];
@@ -158,8 +165,8 @@ __device__ __forceinline__ T band_dot(const T* __restrict__ row, const T* s, int
 
 // One 8x32 tile of outputs per block; 256 threads.
 template <typename T, class Loader, class Epi>
-__global__ void __launch_bounds__(256) stencil_kernel(LevelDev<T> L, Loader ld, Epi ep, double* partials,
-                                                      unsigned int* counter, double* red_out) {
+__device__ __forceinline__ void stencil_tile(const LevelDev<T>& L, const Loader& ld, const Epi& ep, double* partials,
+                                             unsigned int* counter, double* red_out) {
   __shared__ T xs_y[(TY + 2 * HX) * TZ];
   __shared__ T xs_z[TY * (TZ + 2 * HX)];
   __shared__ T gy[3][(TY + 2 * HG) * TZ];
@@ -194,13 +201,14 @@ __global__ void __launch_bounds__(256) stencil_kernel(LevelDev<T> L, Loader ld, 
       int k = y0 - HG + r, iz = z0 + c;
       const T* x = xs_y + (r + HALF) * TZ + c;  // row k
       long node = (long)k * Nz + iz;
-      T cyv = L.cy[node];
+      const T cyv = L.sep ? L.cy1[k] : L.cy[node];
+      const T m3v = L.sep ? L.m3y1[k] : L.m3y[node];
       T d1 = L.y.cD[0] * x[-2 * TZ] + L.y.cD[1] * x[-TZ] + L.y.cD[2] * x[TZ] + L.y.cD[3] * x[2 * TZ];
       T d3 = L.y.cR3[0] * x[-TZ] + L.y.cR3[1] * x[0] + L.y.cR3[2] * x[TZ] + L.y.cR3[3] * x[2 * TZ];
       T d4 = L.y.cR4[0] * x[-2 * TZ] + L.y.cR4[1] * x[-TZ] + L.y.cR4[2] * x[0] + L.y.cR4[3] * x[TZ] +
              L.y.cR4[4] * x[2 * TZ];
       gy[0][i] = cyv * d1;
-      gy[1][i] = L.y.cw3 * L.m3y[node] * d3;
+      gy[1][i] = L.y.cw3 * m3v * d3;
       gy[2][i] = L.y.cw4 * cyv * d4;
     }
     for (int i = tid; i < TY * (TZ + 2 * HG); i += blockDim.x) {
@@ -208,12 +216,13 @@ __global__ void __launch_bounds__(256) stencil_kernel(LevelDev<T> L, Loader ld, 
       int iy = y0 + r, k = z0 - HG + c;
       const T* x = xs_z + r * (TZ + 2 * HX) + c + HALF;  // column k
       long node = (long)iy * Nz + k;
-      T czv = L.cz[node];
+      const T czv = L.sep ? L.cz1[k] : L.cz[node];
+      const T m3v = L.sep ? L.m3z1[k] : L.m3z[node];
       T d1 = L.z.cD[0] * x[-2] + L.z.cD[1] * x[-1] + L.z.cD[2] * x[1] + L.z.cD[3] * x[2];
       T d3 = L.z.cR3[0] * x[-1] + L.z.cR3[1] * x[0] + L.z.cR3[2] * x[1] + L.z.cR3[3] * x[2];
       T d4 = L.z.cR4[0] * x[-2] + L.z.cR4[1] * x[-1] + L.z.cR4[2] * x[0] + L.z.cR4[3] * x[1] + L.z.cR4[4] * x[2];
       gz[0][i] = czv * d1;
-      gz[1][i] = L.z.cw3 * L.m3z[node] * d3;
+      gz[1][i] = L.z.cw3 * m3v * d3;
       gz[2][i] = L.z.cw4 * czv * d4;
     }
     __syncthreads();
@@ -236,9 +245,11 @@ __global__ void __launch_bounds__(256) stencil_kernel(LevelDev<T> L, Loader ld, 
     sz -= L.z.cR3T[0] * h1[-2] + L.z.cR3T[1] * h1[-1] + L.z.cR3T[2] * h1[0] + L.z.cR3T[3] * h1[1];
     sz -= L.z.cR4T[0] * h2[-2] + L.z.cR4T[1] * h2[-1] + L.z.cR4T[2] * h2[0] + L.z.cR4T[3] * h2[1] +
           L.z.cR4T[4] * h2[2];
-    T Ax = L.wy[node] * sy + L.wz[node] * sz;
+    const T wyv = L.sep ? L.wy1[iz] : L.wy[node];
+    const T wzv = L.sep ? L.wz1[iy] : L.wz[node];
+    T Ax = wyv * sy + wzv * sz;
     T xv = xs_y[(ty + HX) * TZ + tz];
-    double contrib = ep(node, Ax, xv);
+    double contrib = ep(node, iy, iz, Ax, xv);
     if constexpr (Epi::kReduce) {
       if (partials != nullptr) {
         double tot = block_sum(contrib, red);
@@ -342,7 +353,7 @@ __global__ void __launch_bounds__(256) stencil_kernel(LevelDev<T> L, Loader ld, 
     }
     T Ax = L.wy[node] * sy + L.wz[node] * sz;
     T xv = xs_y[(ty + HX) * TZ + tz];
-    contrib = ep(node, Ax, xv);
+    contrib = ep(node, iy, iz, Ax, xv);
   }
   if constexpr (Epi::kReduce) {
     if (partials != nullptr) {  // uniform across the grid
@@ -350,6 +361,12 @@ __global__ void __launch_bounds__(256) stencil_kernel(LevelDev<T> L, Loader ld, 
       grid_reduce_finish(tot, partials, counter, red_out, red);
     }
   }
+}
+
+template <typename T, class Loader, class Epi>
+__global__ void __launch_bounds__(256) stencil_kernel(LevelDev<T> L, Loader ld, Epi ep, double* partials,
+                                                      unsigned int* counter, double* red_out) {
+  stencil_tile<T, Loader, Epi>(L, ld, ep, partials, counter, red_out);
 }
 
 }  // namespace scy

@@ -188,6 +188,46 @@ int LevelStore<T>::init(const LevelHost& h, cudaStream_t s) {
   dev.qy = fld[7].template as<T>();
   dev.rz = fld[8].template as<T>();
   dev.dinv = fld[9].template as<T>();
+  // separable interior (see LevelDev::sep): verified bitwise over the box
+  // of nodes the interior fast path can read
+  dev.sep = 0;
+  if (dev.y.fast && dev.z.fast) {
+    const int iy_ref = Ny / 2, iz_ref = Nz / 2;
+    std::vector<double> cy1(Ny), m3y1(Ny), wz1(Ny), cz1(Nz), m3z1(Nz), wy1(Nz);
+    for (int iy = 0; iy < Ny; ++iy) {
+      const size_t i = (size_t)iy * Nz + iz_ref;
+      cy1[iy] = h.cy[i];
+      m3y1[iy] = h.m3y[i];
+      wz1[iy] = h.wz[i];
+    }
+    for (int iz = 0; iz < Nz; ++iz) {
+      const size_t i = (size_t)iy_ref * Nz + iz;
+      cz1[iz] = h.cz[i];
+      m3z1[iz] = h.m3z[i];
+      wy1[iz] = h.wy[i];
+    }
+    bool ok = true;
+    for (int iy = 4; ok && iy <= Ny - 6; ++iy)
+      for (int iz = 4; iz <= Nz - 6; ++iz) {
+        const size_t i = (size_t)iy * Nz + iz;
+        if (h.cy[i] != cy1[iy] || h.m3y[i] != m3y1[iy] || h.wz[i] != wz1[iy] || h.cz[i] != cz1[iz] ||
+            h.m3z[i] != m3z1[iz] || h.wy[i] != wy1[iz]) {
+          ok = false;
+          break;
+        }
+      }
+    if (ok) {
+      const std::vector<double>* v[6] = {&cy1, &m3y1, &wz1, &cz1, &m3z1, &wy1};
+      for (int k = 0; k < 6; ++k) SCY_TRY(upload<T>(sep1[k], *v[k], s));
+      dev.cy1 = sep1[0].template as<T>();
+      dev.m3y1 = sep1[1].template as<T>();
+      dev.wz1 = sep1[2].template as<T>();
+      dev.cz1 = sep1[3].template as<T>();
+      dev.m3z1 = sep1[4].template as<T>();
+      dev.wy1 = sep1[5].template as<T>();
+      dev.sep = 1;
+    }
+  }
   return SCY_OK;
 }
 

@@ -56,6 +56,7 @@ struct LevelStore {
   int Ny = 0, Nz = 0;
   DevBuf tab[2][10];  // per direction: D, R3, R4, Q, R3T, R4T, w3, w4, Hd, Hinvd
   DevBuf fld[10];     // cy, cz, m3y, m3z, wy, wz, mu, qy, rz, dinv
+  DevBuf sep1[6];     // cy1, m3y1, wz1 (Ny), cz1, m3z1, wy1 (Nz) when separable
   LevelDev<T> dev{};
   int init(const LevelHost& h, cudaStream_t s);
 };
