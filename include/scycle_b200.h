@@ -239,7 +239,10 @@ scy_status scy_qd_d_dt(scy_qd* q, double t, const double* var, double* dvar);
 enum { SCY_RK32 = 0, SCY_RK43 = 1 };
 enum { SCY_CTRL_P = 0, SCY_CTRL_PID = 1 };
 enum { SCY_NORM_L2_ABS = 0, SCY_NORM_L2_REL = 1 };
-enum { SCY_KEY_PSI = 0, SCY_KEY_SLIP = 1 };
+/* Integrated fields.  The state vector holds them in the std::map's key
+ * order: [psi | slip] (Nz each) for the linear-elastic drivers, [gVxy |
+ * gVxz | psi | slip] (Ny*Nz, Ny*Nz, Nz, Nz) for the power-law driver. */
+enum { SCY_KEY_PSI = 0, SCY_KEY_SLIP = 1, SCY_KEY_GVXY = 2, SCY_KEY_GVXZ = 3 };
 
 typedef struct scy_ode_opts {
   int method;           /* SCY_RK32 / SCY_RK43 */
@@ -250,8 +253,8 @@ typedef struct scy_ode_opts {
   double t0, t1;        /* initTime, maxTime */
   long max_steps;       /* maxStepCount */
   int n_err;            /* 0: all keys in sorted order with scale 1 */
-  int err_keys[2];      /* SCY_KEY_* in timeIntInds order */
-  double err_scale[2];  /* scale per key */
+  int err_keys[4];      /* SCY_KEY_* in timeIntInds order */
+  double err_scale[4];  /* scale per key */
 } scy_ode_opts;
 
 typedef struct scy_ode_stats {
@@ -327,6 +330,37 @@ scy_status scy_qd_set_jacobian(scy_qd* q, int exact);
  * recompute = 1 re-evaluates the rates from it (one d_dt); recompute = 0
  * only uploads it (for a host round trip of the state the device holds). */
 scy_status scy_qd_set_state(scy_qd* q, const double* var_host, int recompute);
+
+/* ---------------------------------------------------------------------------
+ * Power-law viscoelastic quasi-dynamic driver: StrikeSlip_PowerLaw_qd
+ * (source/strikeSlip_powerLaw_qd.cpp) with PowerLaw's dislocation creep
+ * (source/powerLaw.cpp).  The driver is an scy_qd whose integrated state is
+ * [gVxy | gVxz | psi | slip]; every scy_qd_* entry point applies to it.
+ * d_dt adds the viscous source B*gVxy + C*gVxz to the momentum balance
+ * (computeViscStrainSourceTerms :1651-1671), forms the total strains and
+ * the stresses sxy = mu (Dy u - gVxy), sxz = mu (Dz u - gVxz), the effective
+ * viscosity 1/eta = 1/maxEffVisc + 1e3 A sdev^(n-1) exp(-B/T)
+ * (DislocationCreep::computeInvEffVisc :438-474) and the viscous strain
+ * rates with their boundary SAT term (computeViscStrainRates :1707-1743),
+ * and feeds sxy on the fault to the rate-and-state fault.
+ * ------------------------------------------------------------------------- */
+typedef struct scy_pl_desc {
+  const double* A;         /* host, Ny*Nz: dislocation-creep prefactor (disl_AVals) */
+  const double* B;         /* host, Ny*Nz: activation temperature Q/R in K (disl_BVals) */
+  const double* n;         /* host, Ny*Nz: stress exponent (disl_nVals) */
+  const double* T;         /* host, Ny*Nz: temperature in K (TVals) */
+  double visc_cap;         /* maxEffVisc (reference default 1e30) */
+} scy_pl_desc;
+
+/* A power-law driver; desc->grid.mu is PowerLaw's mu (interpolated against
+ * z, powerLaw.cpp:1016). */
+scy_status scy_pl_create(const scy_qd_desc* desc, const scy_pl_desc* pl, scy_qd** out);
+/* Length of the integrated state of a driver (2*Nz, or 2*Ny*Nz + 2*Nz). */
+scy_status scy_qd_state_size(scy_qd* q, long* n);
+
+enum {
+  SCY_FIELD_GVXY = 11, SCY_FIELD_GVXZ = 12, SCY_FIELD_SXZ = 13, SCY_FIELD_SDEV = 14, SCY_FIELD_EFFVISC = 15
+};
 
 /* ---------------------------------------------------------------------------
  * Quasi-dynamic / fully dynamic earthquake cycles: the

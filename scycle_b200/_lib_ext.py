@@ -21,8 +21,8 @@ class QDDesc(C.Structure):
 class OdeOpts(C.Structure):
     _fields_ = [("method", C.c_int), ("control", C.c_int), ("norm", C.c_int), ("tol", C.c_double),
                 ("min_dt", C.c_double), ("max_dt", C.c_double), ("init_dt", C.c_double), ("t0", C.c_double),
-                ("t1", C.c_double), ("max_steps", C.c_long), ("n_err", C.c_int), ("err_keys", C.c_int * 2),
-                ("err_scale", C.c_double * 2)]
+                ("t1", C.c_double), ("max_steps", C.c_long), ("n_err", C.c_int), ("err_keys", C.c_int * 4),
+                ("err_scale", C.c_double * 4)]
 
 
 class OdeStats(C.Structure):
@@ -32,7 +32,8 @@ class OdeStats(C.Structure):
 
 
 FIELDS = {"psi": 0, "slip": 1, "slipVel": 2, "tauP": 3, "tauQSP": 4, "strength": 5, "u": 6, "surfDisp": 7,
-          "sxy": 8, "dpsi": 9, "dslip": 10}
+          "sxy": 8, "dpsi": 9, "dslip": 10, "gVxy": 11, "gVxz": 12, "sxz": 13, "sdev": 14, "effVisc": 15}
+BODY_FIELDS = ("u", "sxy", "gVxy", "gVxz", "sxz", "sdev", "effVisc")
 LAWS = {"agingLaw": 0, "slipLaw": 1, "constantState": 2}
 
 
@@ -54,6 +55,8 @@ def declare(L):
     L.scy_qd_set_state.argtypes = [vp, dptr, C.c_int]
     L.scy_qd_set_jacobian.argtypes = [vp, C.c_int]
     L.scy_qd_set_mode.argtypes = [vp, C.c_int]
+    L.scy_pl_create.argtypes = [C.POINTER(QDDesc), vp, C.POINTER(vp)]
+    L.scy_qd_state_size.argtypes = [vp, C.POINTER(C.c_long)]
     L.scy_in_problem_field.argtypes = [C.c_char_p, C.c_char_p, dptr, C.c_long, C.POINTER(C.c_long)]
     L.scy_in_problem_info.argtypes = [C.c_char_p, C.POINTER(S.GridDesc), C.POINTER(OdeOpts), C.POINTER(C.c_int),
                                       C.POINTER(C.c_int), C.POINTER(C.c_double)]

@@ -138,6 +138,30 @@ def qdfd_const_801(workdir, seed=0, **kw):
     return make_qdfd_problem(workdir, Ny=801, Nz=801, seed=seed, name="qdfd_const_801", **kw)
 
 
+def make_pl_problem(workdir, Ny=101, Nz=101, Ly=30.0, Lz=30.0, seed=0, A=1e-4, n=3.0, Q=135e3,
+                    T0=283.0, grad=25.0, name="pl", integrator="RK43", tol=1e-7, years=1000.0,
+                    min_dt=1e-3, max_effvisc=1e30, **kw):
+    """Power-law viscoelastic quasi-dynamic problem (bulkDeformationType
+    powerLaw): dislocation creep with prefactor A (MPa^-n/s), exponent n,
+    activation energy Q (J/mol, B = Q/R in kelvin) and a linear geotherm
+    T = T0 + grad*z (grad in K/km)."""
+    R = 8.314462618
+    extra = {"wDislCreep": "yes", "disl_AVals": "[%r %r]" % (A, A), "disl_ADepths": "[0 %r]" % Lz,
+             "disl_BVals": "[%r %r]" % (Q / R, Q / R), "disl_BDepths": "[0 %r]" % Lz,
+             "disl_nVals": "[%r %r]" % (n, n), "disl_nDepths": "[0 %r]" % Lz,
+             "TVals": "[%r %r]" % (T0, T0 + grad * Lz), "TDepths": "[0 %r]" % Lz,
+             "maxEffVisc": repr(float(max_effvisc)), "minDeltaT": repr(float(min_dt))}
+    extra.update(kw.pop("extra", {}) or {})
+    args = dict(Ny=Ny, Nz=Nz, Ly=Ly, Lz=Lz, seed=seed, name=name, integrator=integrator, tol=tol,
+                years=years, mbt="quasidynamic", extra=extra)
+    args.update(kw)
+    path = make_qd_problem(workdir, **args)
+    text = open(path).read().replace("bulkDeformationType = linearElastic", "bulkDeformationType = powerLaw")
+    with open(path, "w") as f:
+        f.write(text)
+    return path
+
+
 def aging_const_101(workdir, seed=0, **kw):
     args = dict(Ny=101, Nz=101, seed=seed, name="aging_const_101")
     args.update(kw)

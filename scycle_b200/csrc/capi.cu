@@ -199,6 +199,29 @@ scy_status scy_qd_create(const scy_qd_desc* d, scy_qd** out) {
   return SCY_OK;
 }
 
+scy_status scy_pl_create(const scy_qd_desc* d, const scy_pl_desc* pl, scy_qd** out) {
+  if (!d || !pl || !out) {
+    scy::set_error("scy_pl_create: NULL argument");
+    return SCY_ERR_ARG;
+  }
+  *out = nullptr;
+  scy_qd* q = new (std::nothrow) scy_qd();
+  if (!q) return SCY_ERR_NOMEM;
+  int st = q->ctx.create(*d, pl);
+  if (st != SCY_OK) {
+    delete q;
+    return st;
+  }
+  *out = q;
+  return SCY_OK;
+}
+
+scy_status scy_qd_state_size(scy_qd* q, long* n) {
+  if (!q || !n) return SCY_ERR_ARG;
+  *n = q->ctx.nvar;
+  return SCY_OK;
+}
+
 scy_status scy_qd_destroy(scy_qd* q) {
   delete q;
   return SCY_OK;
@@ -224,12 +247,12 @@ scy_status scy_qd_integrate_begin(scy_qd* q, const scy_ode_opts* o, const double
     scy::set_error("scy_qd_integrate_begin: NULL argument");
     return SCY_ERR_ARG;
   }
-  if (!(o->tol > 0) || !(o->max_dt >= o->min_dt) || !(o->t1 >= o->t0) || o->max_steps < 0 || o->n_err > 2) {
+  if (!(o->tol > 0) || !(o->max_dt >= o->min_dt) || !(o->t1 >= o->t0) || o->max_steps < 0 || o->n_err > 4) {
     scy::set_error("scy_qd_integrate_begin: invalid options");
     return SCY_ERR_ARG;
   }
   scy::QDContext& c = q->ctx;
-  SCY_CUDA_TRY(cudaMemcpyAsync(c.rk[0].p, var0, 2 * (size_t)c.Nz * sizeof(double), cudaMemcpyHostToDevice,
+  SCY_CUDA_TRY(cudaMemcpyAsync(c.rk[0].p, var0, (size_t)c.nvar * sizeof(double), cudaMemcpyHostToDevice,
                                c.sbp.stream));
   return c.integrate_begin(*o);
 }
@@ -284,11 +307,28 @@ scy_status scy_qd_get_field(scy_qd* q, int field, double* out) {
     if (field == SCY_FIELD_SURFDISP) return scy::qd_green_surf_launch(c, cc, out);
     SCY_TRY(c.full_solve_for_output());
   }
+  const long op = c.key_off[SCY_KEY_PSI], os = c.key_off[SCY_KEY_SLIP];
   switch (field) {
-    case SCY_FIELD_PSI: src = c.rk[0].as<double>(); break;
-    case SCY_FIELD_SLIP: src = c.rk[0].as<double>() + c.Nz; break;
-    case SCY_FIELD_DPSI: src = c.rk[1].as<double>(); break;
-    case SCY_FIELD_DSLIP: src = c.rk[1].as<double>() + c.Nz; break;
+    case SCY_FIELD_PSI: src = c.rk[0].as<double>() + op; break;
+    case SCY_FIELD_SLIP: src = c.rk[0].as<double>() + os; break;
+    case SCY_FIELD_DPSI: src = c.rk[1].as<double>() + op; break;
+    case SCY_FIELD_DSLIP: src = c.rk[1].as<double>() + os; break;
+    case SCY_FIELD_GVXY:
+    case SCY_FIELD_GVXZ:
+    case SCY_FIELD_SXZ:
+    case SCY_FIELD_SDEV:
+    case SCY_FIELD_EFFVISC:
+      if (!c.pl) {
+        scy::set_error("field %d exists for the power-law driver only", field);
+        return SCY_ERR_ARG;
+      }
+      n = c.N;
+      src = field == SCY_FIELD_GVXY   ? c.rk[0].as<double>() + c.key_off[SCY_KEY_GVXY]
+            : field == SCY_FIELD_GVXZ ? c.rk[0].as<double>() + c.key_off[SCY_KEY_GVXZ]
+            : field == SCY_FIELD_SXZ  ? c.sxz.as<double>()
+            : field == SCY_FIELD_SDEV ? c.sdev.as<double>()
+                                      : c.effVisc.as<double>();
+      break;
     case SCY_FIELD_SLIPVEL: src = c.slipVel.as<double>(); break;
     case SCY_FIELD_TAUP: src = c.tauP.as<double>(); break;
     case SCY_FIELD_TAUQSP: src = c.tauQSP.as<double>(); break;
@@ -296,7 +336,8 @@ scy_status scy_qd_get_field(scy_qd* q, int field, double* out) {
     case SCY_FIELD_U: src = c.u.as<double>(); n = c.N; break;
     case SCY_FIELD_SURFDISP: src = c.u.as<double>(); n = c.Ny; stride = c.Nz; break;
     case SCY_FIELD_SXY:
-      SCY_TRY(c.sbp.apply(SCY_OP_MUXDY, c.u.as<double>(), c.sxy.as<double>()));
+      // the power-law material keeps sxy = mu (Dy u - gVxy) from its last d_dt
+      if (!c.pl) SCY_TRY(c.sbp.apply(SCY_OP_MUXDY, c.u.as<double>(), c.sxy.as<double>()));
       src = c.sxy.as<double>();
       n = c.N;
       break;
@@ -340,7 +381,7 @@ scy_status scy_qd_create_from_in(const char* path, const scy_solve_opts* solve, 
   }
   scy_qd* q = new (std::nothrow) scy_qd();
   if (!q) return SCY_ERR_NOMEM;
-  int st = q->ctx.create(P->desc);
+  int st = q->ctx.create(P->desc, P->pl ? &P->pdesc : nullptr);
   if (st != SCY_OK) {
     delete q;
     return st;
@@ -374,11 +415,20 @@ scy_status scy_qd_integrate_begin_from_in(scy_qd* q) {
   scy::QDContext& c = q->ctx;
   const int Nz = c.Nz;
   std::vector<double> psi = P.psi, slip(Nz);
-  for (int i = 0; i < Nz; ++i) slip[i] = P.bcL0[i] * P.desc.fault_type_scale;
-  if (P.guess_ss) SCY_TRY(c.steady_state_guess(psi, P.stateVals_given, slip));
-  std::vector<double> var0(2 * (size_t)Nz);
-  std::copy(psi.begin(), psi.end(), var0.begin());
-  std::copy(slip.begin(), slip.end(), var0.begin() + Nz);
+  std::vector<double> var0((size_t)c.nvar);
+  if (P.pl) {
+    // StrikeSlip_PowerLaw_qd::initiateIntegrand (:305-350): slip = 2 bcL or
+    // inputDir/slip; the viscous strains of the material
+    for (int i = 0; i < Nz; ++i) slip[i] = P.bcL0[i] * 2.0;
+    if (!P.slip_file.empty()) slip = P.slip_file;
+    std::copy(P.gVxy0.begin(), P.gVxy0.end(), var0.begin() + c.key_off[SCY_KEY_GVXY]);
+    std::copy(P.gVxz0.begin(), P.gVxz0.end(), var0.begin() + c.key_off[SCY_KEY_GVXZ]);
+  } else {
+    for (int i = 0; i < Nz; ++i) slip[i] = P.bcL0[i] * P.desc.fault_type_scale;
+    if (P.guess_ss) SCY_TRY(c.steady_state_guess(psi, P.stateVals_given, slip));
+  }
+  std::copy(psi.begin(), psi.end(), var0.begin() + c.key_off[SCY_KEY_PSI]);
+  std::copy(slip.begin(), slip.end(), var0.begin() + c.key_off[SCY_KEY_SLIP]);
   SCY_CUDA_TRY(cudaMemcpyAsync(c.rk[0].p, var0.data(), var0.size() * sizeof(double), cudaMemcpyHostToDevice,
                                c.sbp.stream));
   SCY_CUDA_TRY(cudaStreamSynchronize(c.sbp.stream));
@@ -408,7 +458,7 @@ scy_status scy_qd_set_state(scy_qd* q, const double* var, int recompute) {
     scy::set_error("scy_qd_set_state: integration not started");
     return SCY_ERR_STATE;
   }
-  SCY_CUDA_TRY(cudaMemcpyAsync(c.rk[0].p, var, 2 * (size_t)c.Nz * sizeof(double), cudaMemcpyHostToDevice,
+  SCY_CUDA_TRY(cudaMemcpyAsync(c.rk[0].p, var, (size_t)c.nvar * sizeof(double), cudaMemcpyHostToDevice,
                                c.sbp.stream));
   if (!recompute) return SCY_OK;
   SCY_TRY(c.d_dt(c.currT, c.rk[0].as<double>(), c.rk[1].as<double>()));

@@ -16,6 +16,7 @@ enum FaultFlags : unsigned {
 
 struct FaultParams {
   int Nz;
+  long psi_off, slip_off;  // offsets of psi and slip in the integrated state
   const double *a, *b, *sN, *Dc, *eta, *locked, *prestress;
   double f0, v0, vL, root_tol;
   int max_its;

@@ -187,7 +187,9 @@ void load_qd_problem(const std::string& path, QDProblem& P, int cycle) {
     else if (e.var == "vL") vL_dom = c_atof(e.rhs);
   }
   if (bCoordTrans > 0.0) gridType = "variableGridSpacing";
-  if (bulk != "linearElastic") throw std::runtime_error("bulkDeformationType '" + bulk + "' is not the linear-elastic path");
+  P.pl = (!cycle && bulk == "powerLaw") ? 1 : 0;
+  if (bulk != "linearElastic" && !P.pl)
+    throw std::runtime_error("bulkDeformationType '" + bulk + "' is not on this path");
   if (!cycle && momBal != "quasidynamic")
     throw std::runtime_error("momentumBalanceType '" + momBal + "' is not the quasi-dynamic path");
   if (cycle && momBal != "quasidynamic_and_dynamic")
@@ -226,10 +228,19 @@ void load_qd_problem(const std::string& path, QDProblem& P, int cycle) {
   }
   if (muVals.empty() || muVals.size() != muDepths.size()) throw std::runtime_error("muVals/muDepths missing or of different lengths");
   if (rhoVals.empty() || rhoVals.size() != rhoDepths.size()) throw std::runtime_error("rhoVals/rhoDepths missing or of different lengths");
-  P.mu = set_vec(P.y, muVals, muDepths);
-  P.rho = set_vec(P.z, rhoVals, rhoDepths);
-  read_petsc_vec(P.inputDir + "momBal_mu", N, P.mu);
-  read_petsc_vec(P.inputDir + "momBal_rho", N, P.rho);
+  if (P.pl) {
+    // PowerLaw::setMaterialParameters interpolates mu and rho against z and
+    // loadFieldsFromFiles reads inputDir/mu, rho (powerLaw.cpp:1016-1017, :1070-1071)
+    P.mu = set_vec(P.z, muVals, muDepths);
+    P.rho = set_vec(P.z, rhoVals, rhoDepths);
+    read_petsc_vec(P.inputDir + "mu", N, P.mu);
+    read_petsc_vec(P.inputDir + "rho", N, P.rho);
+  } else {
+    P.mu = set_vec(P.y, muVals, muDepths);
+    P.rho = set_vec(P.z, rhoVals, rhoDepths);
+    read_petsc_vec(P.inputDir + "momBal_mu", N, P.mu);
+    read_petsc_vec(P.inputDir + "momBal_rho", N, P.rho);
+  }
   P.cs.resize(N);
   for (size_t i = 0; i < N; ++i) P.cs[i] = std::sqrt(std::fabs(P.mu[i] / P.rho[i]));
   read_petsc_vec(P.inputDir + "momBal_cs", N, P.cs);
@@ -292,12 +303,16 @@ void load_qd_problem(const std::string& path, QDProblem& P, int cycle) {
   // the cycle driver's constructor sets minDeltaT = 1e-3 where the
   // quasi-dynamic driver leaves -1 for computeMinTimeStep
   // (strikeSlip_linearElastic_qd_fd.cpp:25)
-  double initTime = 0, maxTime = 1e15, minDeltaT = cycle ? 1e-3 : -1, maxDeltaT = 1e10, initDeltaT = 1e-3,
-         timeStepTol = 1e-8;
+  double initTime = 0, maxTime = 1e15, minDeltaT = (cycle || P.pl) ? 1e-3 : -1, maxDeltaT = 1e10,
+         initDeltaT = 1e-3, timeStepTol = 1e-8;
   // strikeSlip_linearElastic_qd_fd keys and defaults (:8-33, :135-230)
   double trig_qd2fd = 1e-3, trig_fd2qd = 1e-3, limit_qd = 10 * 1e-9, limit_fd = 1e-1, limit_stride_fd = -1;
   double deltaT_fd = -1, CFL = -1;
   int maxNumCycles = 1000;
+  // extension key (not read by the reference): 0 puts the outgoing-
+  // characteristics damping on the boundary nodes it names instead of the
+  // reference's indexing of computePenaltyVectors
+  int ay_quirk = 1;
   std::string fdR = "outGoingCharacteristics", fdT = "freeSurface", fdL = "symmFault", fdB = "outGoingCharacteristics";
   double vL = 1e-9;
   std::vector<std::string> timeIntInds;
@@ -341,6 +356,7 @@ void load_qd_problem(const std::string& path, QDProblem& P, int cycle) {
     else if (cycle && e.var == "momBal_bcT_fd") fdT = e.rhs;
     else if (cycle && e.var == "momBal_bcL_fd") fdL = e.rhs;
     else if (cycle && e.var == "momBal_bcB_fd") fdB = e.rhs;
+    else if (cycle && e.var == "fd_ayIndexQuirk") ay_quirk = c_atoi(e.rhs);
   }
   if (thermal != "no" || hydraulic != "no") throw std::runtime_error("thermal / hydraulic coupling is outside this path");
   if (forcing != "no") throw std::runtime_error("forcingType '" + forcing + "' is outside this path");
@@ -418,15 +434,62 @@ void load_qd_problem(const std::string& path, QDProblem& P, int cycle) {
   o.t0 = initTime;
   o.t1 = maxTime;
   o.max_steps = maxStepCount;
-  if (timeIntInds.size() > 2) throw std::runtime_error("timeIntInds names more than the two integrated fields");
+  if (timeIntInds.size() > (P.pl ? 4u : 2u)) throw std::runtime_error("timeIntInds names more fields than are integrated");
   o.n_err = (int)timeIntInds.size();
   for (size_t i = 0; i < timeIntInds.size(); ++i) {
     if (timeIntInds[i] == "psi") o.err_keys[i] = SCY_KEY_PSI;
     else if (timeIntInds[i] == "slip") o.err_keys[i] = SCY_KEY_SLIP;
+    else if (P.pl && timeIntInds[i] == "gVxy") o.err_keys[i] = SCY_KEY_GVXY;
+    else if (P.pl && timeIntInds[i] == "gVxz") o.err_keys[i] = SCY_KEY_GVXZ;
     else throw std::runtime_error("timeIntInds entry '" + timeIntInds[i] + "' is not an integrated field");
     o.err_scale[i] = scale.empty() ? 1.0 : (i < scale.size() ? scale[i] : 1.0);
   }
   if (!scale.empty() && scale.size() != timeIntInds.size()) throw std::runtime_error("scale and timeIntInds differ in length");
+  if (P.pl) {
+    // ---- PowerLaw + DislocationCreep settings (powerLaw.cpp:260-305, :851-915)
+    std::string wDisl = "yes", wDiff = "no", wPlast = "no", wLM = "no";
+    double cap = 1e30;
+    std::vector<double> AV, AD, BV, BD, nV, nD, TV, TD;
+    for (const auto& e : E) {
+      auto app = [&](std::vector<double>& dst) { auto v = load_vector_double(e.full); dst.insert(dst.end(), v.begin(), v.end()); };
+      if (e.var == "wDislCreep") wDisl = e.rhs;
+      else if (e.var == "wDiffCreep") wDiff = e.rhs;
+      else if (e.var == "wPlasticity") wPlast = e.rhs;
+      else if (e.var == "wLinearMaxwell") wLM = e.rhs;
+      else if (e.var == "maxEffVisc") cap = c_atof(e.rhs);
+      else if (e.var == "disl_AVals") app(AV);
+      else if (e.var == "disl_ADepths") app(AD);
+      else if (e.var == "disl_BVals") app(BV);
+      else if (e.var == "disl_BDepths") app(BD);
+      else if (e.var == "disl_nVals") app(nV);
+      else if (e.var == "disl_nDepths") app(nD);
+      else if (e.var == "TVals") app(TV);
+      else if (e.var == "TDepths") app(TD);
+    }
+    if (wDisl != "yes" || wDiff != "no" || wPlast != "no" || wLM != "no")
+      throw std::runtime_error("the power-law path covers dislocation creep only (wDislCreep = yes, the others no)");
+    if (guess) throw std::runtime_error("the power-law steady-state iteration (guessSteadyStateICs = 1) is outside this path");
+    if (AV.size() < 2 || BV.size() < 2 || nV.size() < 2 || AV.size() != AD.size() || BV.size() != BD.size() ||
+        nV.size() != nD.size())
+      throw std::runtime_error("disl_A/B/n values and depths need at least two matching entries");
+    if (TV.empty() || TV.size() != TD.size()) throw std::runtime_error("TVals/TDepths missing or of different lengths");
+    P.plA = set_vec(P.z, AV, AD);
+    P.plB = set_vec(P.z, BV, BD);
+    P.pln = set_vec(P.z, nV, nD);
+    P.plT = set_vec(P.z, TV, TD);
+    read_petsc_vec(P.inputDir + "T", N, P.plT);
+    P.gVxy0.assign(N, 0.0);
+    P.gVxz0.assign(N, 0.0);
+    read_petsc_vec(P.inputDir + "GVxy", N, P.gVxy0);
+    read_petsc_vec(P.inputDir + "GVxz", N, P.gVxz0);
+    if (!read_petsc_vec(P.inputDir + "slip", Nz, P.slip_file)) P.slip_file.clear();
+    P.pdesc.A = P.plA.data();
+    P.pdesc.B = P.plB.data();
+    P.pdesc.n = P.pln.data();
+    P.pdesc.T = P.plT.data();
+    P.pdesc.visc_cap = cap;
+    return;
+  }
   if (!cycle) return;
   // ---- strikeSlip_linearElastic_qd_fd::checkInput (:232-305)
   auto fd_side = [](const std::string& t, const char* key) {
@@ -454,7 +517,7 @@ void load_qd_problem(const std::string& path, QDProblem& P, int cycle) {
   c.limit_qd = limit_qd;
   c.limit_fd = limit_fd;
   c.max_num_cycles = maxNumCycles;
-  c.ay_index_quirk = 1;
+  c.ay_index_quirk = ay_quirk ? 1 : 0;
   // initiateIntegrands reads inputDir/slip when present (:678)
   if (!read_petsc_vec(P.inputDir + "slip", Nz, P.slip_file)) P.slip_file.clear();
 }

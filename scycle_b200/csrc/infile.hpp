@@ -45,6 +45,10 @@ struct QDProblem {
   std::vector<double> a, b, sN, Dc, locked, prestress, psi, eta, mu_f, rho_f;
   std::vector<double> bcL0, bcRShift;
   int stateVals_given = 0;
+  // StrikeSlip_PowerLaw_qd (bulkDeformationType powerLaw)
+  int pl = 0;
+  scy_pl_desc pdesc{};
+  std::vector<double> plA, plB, pln, plT, gVxy0, gVxz0;
   // strikeSlip_linearElastic_qd_fd only (cycle = 1)
   int cycle = 0;
   scy_cycle_desc cdesc{};

@@ -11,69 +11,20 @@
 #include <cstring>
 
 #include "common.cuh"
+#include "fault_node.cuh"
 #include "qd.hpp"
 
 namespace scy {
 
 // ---------------------------------------------------------------------------
 // bcL = slip/faultTypeScale, bcR = vL t/faultTypeScale + bcRShift
-__global__ void qd_bc_kernel(const double* __restrict__ var, int Nz, double t, double vL, double inv_fts,
+__global__ void qd_bc_kernel(const double* __restrict__ slip, int Nz, double t, double vL, double inv_fts,
                              int bcL_from_slip, int bcR_remote, const double* __restrict__ shift,
                              double* __restrict__ bcL, double* __restrict__ bcR) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= Nz) return;
-  if (bcL_from_slip) bcL[i] = var[Nz + i] * inv_fts;
+  if (bcL_from_slip) bcL[i] = slip[i] * inv_fts;
   if (bcR_remote) bcR[i] = vL * t * inv_fts + shift[i];
-}
-
-// Fault_qd::d_dt for one node given its quasi-static shear stress from the
-// body (fault.cpp:861-918): prestress, bracketed Newton, state law, tauP,
-// strength.
-__device__ __forceinline__ void fault_node_update(int iz, double tau_body, const FaultParams& fp,
-                                                  const double* __restrict__ var, double* __restrict__ f,
-                                                  double* __restrict__ slipVel, double* __restrict__ tauQSP,
-                                                  double* __restrict__ tauP, double* __restrict__ strength,
-                                                  unsigned* flags, unsigned long long* its_total) {
-  const int Nz = fp.Nz;
-  const double tq = tau_body + fp.prestress[iz];
-  tauQSP[iz] = tq;
-  const double psi = var[iz];
-  const double a = fp.a[iz], sN = fp.sN[iz], eta = fp.eta[iz];
-  double V;
-  const double lk = fp.locked[iz];
-  if (lk > 0.5) {
-    V = 0.0;
-  } else if (lk < -0.5) {
-    V = fp.vL;
-  } else {
-    double left = 0.0, right = tq / eta;
-    if (isnan(right)) {
-      atomicOr(flags, (unsigned)FAULT_NONFINITE);
-      V = slipVel[iz];
-    } else if (fabs(left - right) < 1e-14) {
-      V = left;
-    } else {
-      int its = 0;
-      bool ok = true;
-      V = bracketed_newton(left, right, slipVel[iz], fp.root_tol, fp.max_its, tq, eta, sN, psi, a, fp.v0,
-                           fp.jacobian, &its, &ok);
-      atomicAdd(its_total, (unsigned long long)its);
-      if (!ok) atomicOr(flags, (unsigned)FAULT_ROOT_NOCONV);
-    }
-  }
-  slipVel[iz] = V;
-  double dpsi;
-  if (fp.state_law == 0)
-    dpsi = aging_law_psi(psi, V, fp.b[iz], fp.f0, fp.v0, fp.Dc[iz]);
-  else if (fp.state_law == 1)
-    dpsi = slip_law_psi(psi, V, a, fp.b[iz], fp.f0, fp.v0, fp.Dc[iz]);
-  else
-    dpsi = 0.0;
-  if (!isfinite(dpsi) || !isfinite(V)) atomicOr(flags, (unsigned)FAULT_NONFINITE);
-  f[iz] = dpsi;
-  f[Nz + iz] = V;
-  tauP[iz] = tq - eta * V;
-  strength[iz] = strength_psi(sN, psi, V, a, fp.v0);
 }
 
 // Fault column: sxy = mu*Dy*u at iy = 0 (body2L scatter of muxDy), then the
@@ -129,7 +80,7 @@ __global__ void qd_green_kernel(const double* __restrict__ GL, const double* __r
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (warp >= Nz) return;
   const double* row = GL + (long)warp * Nz;
-  const double* slip = var + Nz;
+  const double* slip = var + fp.slip_off;
   double acc = 0.0;
   for (int j = lane; j < Nz; j += 32) acc += row[j] * (slip[j] * inv_fts);
   acc = warp_sum(acc);
@@ -170,7 +121,7 @@ int qd_green_surf_launch(QDContext& q, double c, double* host_out) {
 int QDContext::full_solve_for_output() {
   cudaStream_t s = sbp.stream;
   const int tb = 64, gb = (Nz + tb - 1) / tb;
-  qd_bc_kernel<<<gb, tb, 0, s>>>(rk[0].as<double>(), Nz, last_t, vL, 1.0 / fts, 0, bcR_remote,
+  qd_bc_kernel<<<gb, tb, 0, s>>>(rk[0].as<double>() + fp.slip_off, Nz, last_t, vL, 1.0 / fts, 0, bcR_remote,
                                  bcRShift.as<double>(), bcL.as<double>(), bcR.as<double>());
   SCY_LAUNCH_CHECK();
   SCY_TRY(sbp.set_rhs(bcL.as<double>(), bcR.as<double>(), bcT.as<double>(), bcB.as<double>(), rhs.as<double>()));
@@ -187,45 +138,48 @@ struct Combo {
   int nf;
 };
 
-__global__ void rk_combine_kernel(double* __restrict__ out, const double* __restrict__ var, Combo cb, int n) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void rk_combine_kernel(double* __restrict__ out, const double* __restrict__ var, Combo cb, long n) {
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (i >= n) return;
   double v = cb.c[0] * cb.f[0][i] + var[i];
   for (int j = 1; j < cb.nf; ++j) v = v + cb.c[j] * cb.f[j][i];
   out[i] = v;
 }
 
-// Per key (psi: [0,Nz), slip: [Nz,2Nz)): sum (lo-hi)^2, sum hi^2, max(|lo-hi|/hi).
-__global__ void rk_error_kernel(const double* __restrict__ lo, const double* __restrict__ hi, int Nz,
+// Per integrated field (block b handles SCY_KEY b at [off[b], off[b]+len[b])):
+// sum (lo-hi)^2, sum hi^2, max(|lo-hi|/hi) into out[3b .. 3b+2].
+struct KeyTable {
+  long off[4], len[4];
+};
+
+__global__ void rk_error_kernel(const double* __restrict__ lo, const double* __restrict__ hi, KeyTable kt,
                                 double* __restrict__ out) {
   __shared__ double sh[32];
-  for (int key = 0; key < 2; ++key) {
-    double ss = 0.0, sh2 = 0.0, mx = -INFINITY;
-    for (int i = threadIdx.x; i < Nz; i += blockDim.x) {
-      double h = hi[key * Nz + i];
-      double d = lo[key * Nz + i] - h;
-      ss += d * d;
-      sh2 += h * h;
-      double r = fabs(d) / h;
-      mx = fmax(mx, r);
+  const int key = blockIdx.x;
+  const long off = kt.off[key], len = kt.len[key];
+  double ss = 0.0, sh2 = 0.0, mx = -INFINITY;
+  for (long i = threadIdx.x; i < len; i += blockDim.x) {
+    double h = hi[off + i];
+    double d = lo[off + i] - h;
+    ss += d * d;
+    sh2 += h * h;
+    double r = fabs(d) / h;
+    mx = fmax(mx, r);
+  }
+  ss = block_sum(ss, sh);
+  sh2 = block_sum(sh2, sh);
+  double m = warp_max(mx);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double t = threadIdx.x < (blockDim.x + 31) / 32 ? sh[threadIdx.x] : -INFINITY;
+    t = warp_max(t);
+    if (threadIdx.x == 0) {
+      out[key * 3 + 0] = ss;
+      out[key * 3 + 1] = sh2;
+      out[key * 3 + 2] = t;
     }
-    ss = block_sum(ss, sh);
-    sh2 = block_sum(sh2, sh);
-    // max reduction
-    double m = warp_max(mx);
-    __syncthreads();
-    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = m;
-    __syncthreads();
-    if (threadIdx.x < 32) {
-      double t = threadIdx.x < (blockDim.x + 31) / 32 ? sh[threadIdx.x] : -INFINITY;
-      t = warp_max(t);
-      if (threadIdx.x == 0) {
-        out[key * 3 + 0] = ss;
-        out[key * 3 + 1] = sh2;
-        out[key * 3 + 2] = t;
-      }
-    }
-    __syncthreads();
   }
 }
 
@@ -245,7 +199,12 @@ static int upload_or_fill(DevBuf& b, const double* src, size_t n, double fill, c
   return SCY_OK;
 }
 
-int QDContext::create(const scy_qd_desc& d) {
+int QDContext::create(const scy_qd_desc& d, const scy_pl_desc* pld) {
+  pl = pld ? 1 : 0;
+  if (pl && (!pld->A || !pld->B || !pld->n || !pld->T || !(pld->visc_cap > 0))) {
+    set_error("power-law descriptor needs A, B, n, T and visc_cap > 0");
+    return SCY_ERR_ARG;
+  }
   SCY_TRY(sbp.create(d.grid));
   Ny = d.grid.Ny;
   Nz = d.grid.Nz;
@@ -320,9 +279,47 @@ int QDContext::create(const scy_qd_desc& d) {
   solve_opts = d.solve;
   if (solve_opts.max_its < 1) solve_opts.max_its = 200;
   if (solve_opts.check_every < 1) solve_opts.check_every = 1;
+  // integrated state layout (the std::map's key order)
+  for (int k = 0; k < 4; ++k) key_off[k] = key_len[k] = 0;
+  if (pl) {
+    key_off[SCY_KEY_GVXY] = 0;
+    key_len[SCY_KEY_GVXY] = N;
+    key_off[SCY_KEY_GVXZ] = N;
+    key_len[SCY_KEY_GVXZ] = N;
+    key_off[SCY_KEY_PSI] = 2 * N;
+    key_off[SCY_KEY_SLIP] = 2 * N + Nz;
+    nvar = 2 * N + 2 * (long)Nz;
+  } else {
+    key_off[SCY_KEY_PSI] = 0;
+    key_off[SCY_KEY_SLIP] = Nz;
+    nvar = 2 * (long)Nz;
+  }
+  key_len[SCY_KEY_PSI] = key_len[SCY_KEY_SLIP] = Nz;
+  fp.psi_off = key_off[SCY_KEY_PSI];
+  fp.slip_off = key_off[SCY_KEY_SLIP];
+  if (pl) {
+    // DislocationCreep::computeInvEffVisc evaluates 1e3*A*pow(s, n-1)*exp(-B/T)
+    // left to right; 1e3*A and exp(-B/T) are fixed without thermal coupling
+    std::vector<double> c1(N), e1(N);
+    for (long i = 0; i < N; ++i) {
+      c1[i] = 1e3 * pld->A[i];
+      e1[i] = std::exp(-pld->B[i] / pld->T[i]);
+    }
+    SCY_TRY(upload_vec(pl_c1, c1.data(), N, s));
+    SCY_TRY(upload_vec(pl_e1, e1.data(), N, s));
+    SCY_TRY(upload_vec(pl_n, pld->n, N, s));
+    inv_visc_cap = 1.0 / pld->visc_cap;
+    SCY_TRY(sxz.alloc(N * 8));
+    SCY_TRY(sdev.alloc(N * 8));
+    SCY_TRY(effVisc.alloc(N * 8));
+    SCY_CUDA_TRY(cudaMemsetAsync(sxz.p, 0, N * 8, s));
+    SCY_CUDA_TRY(cudaMemsetAsync(sdev.p, 0, N * 8, s));
+    SCY_CUDA_TRY(cudaMemsetAsync(effVisc.p, 0, N * 8, s));
+    SCY_CUDA_TRY(cudaStreamSynchronize(s));
+  }
   for (auto& b : rk) {
-    SCY_TRY(b.alloc(2 * (size_t)Nz * 8));
-    SCY_CUDA_TRY(cudaMemset(b.p, 0, 2 * (size_t)Nz * 8));
+    SCY_TRY(b.alloc((size_t)nvar * 8));
+    SCY_CUDA_TRY(cudaMemset(b.p, 0, (size_t)nvar * 8));
   }
   SCY_TRY(errbuf.alloc(16 * 8));
   return SCY_OK;
@@ -344,8 +341,27 @@ int QDContext::read_flags() {
   return SCY_OK;
 }
 
+int qd_bc_launch(QDContext& q, double t, const double* var) {
+  const int tb = 64, gb = (q.Nz + tb - 1) / tb;
+  qd_bc_kernel<<<gb, tb, 0, q.sbp.stream>>>(var + q.fp.slip_off, q.Nz, t, q.vL, 1.0 / q.fts, q.bcL_from_slip,
+                                            q.bcR_remote, q.bcRShift.as<double>(), q.bcL.as<double>(),
+                                            q.bcR.as<double>());
+  SCY_LAUNCH_CHECK();
+  return SCY_OK;
+}
+
 int QDContext::d_dt(double t, const double* var, double* f) {
   cudaStream_t s = sbp.stream;
+  if (pl) {
+    if (mode == SCY_QD_MODE_RESPONSE) {
+      set_error("the fault-response mode does not apply to the power-law material");
+      return SCY_ERR_STATE;
+    }
+    SCY_TRY(pl_d_dt(*this, t, var, f));
+    last_t = t;
+    ++n_d_dt;
+    return SCY_OK;
+  }
   if (mode == SCY_QD_MODE_RESPONSE) {
     if (!green_ready) SCY_TRY(build_green());
     const double c = bcR_remote ? vL * t * (1.0 / fts) : 0.0;
@@ -360,8 +376,8 @@ int QDContext::d_dt(double t, const double* var, double* f) {
     return SCY_OK;
   }
   const int tb = 64, gb = (Nz + tb - 1) / tb;
-  qd_bc_kernel<<<gb, tb, 0, s>>>(var, Nz, t, vL, 1.0 / fts, bcL_from_slip, bcR_remote, bcRShift.as<double>(),
-                                 bcL.as<double>(), bcR.as<double>());
+  qd_bc_kernel<<<gb, tb, 0, s>>>(var + fp.slip_off, Nz, t, vL, 1.0 / fts, bcL_from_slip, bcR_remote,
+                                 bcRShift.as<double>(), bcL.as<double>(), bcR.as<double>());
   SCY_LAUNCH_CHECK();
   SCY_TRY(sbp.set_rhs(bcL.as<double>(), bcR.as<double>(), bcT.as<double>(), bcB.as<double>(), rhs.as<double>()));
   scy_solve_opts o = solve_opts;
@@ -553,10 +569,15 @@ double QDContext::compute_step_size(double totErr) {
 
 int QDContext::compute_error(const double* lo, const double* hi, double* err) {
   cudaStream_t s = sbp.stream;
-  rk_error_kernel<<<1, 1024, 0, s>>>(lo, hi, Nz, errbuf.as<double>());
+  KeyTable kt;
+  for (int k = 0; k < 4; ++k) {
+    kt.off[k] = key_off[k];
+    kt.len[k] = key_len[k];
+  }
+  rk_error_kernel<<<pl ? 4 : 2, 1024, 0, s>>>(lo, hi, kt, errbuf.as<double>());
   SCY_LAUNCH_CHECK();
-  double h[6];
-  SCY_CUDA_TRY(cudaMemcpyAsync(h, errbuf.p, sizeof(h), cudaMemcpyDeviceToHost, s));
+  double h[12];
+  SCY_CUDA_TRY(cudaMemcpyAsync(h, errbuf.p, (pl ? 12 : 6) * sizeof(double), cudaMemcpyDeviceToHost, s));
   SCY_CUDA_TRY(cudaStreamSynchronize(s));
   double tot = 0.0;
   for (int i = 0; i < ode.n_err; ++i) {
@@ -564,7 +585,7 @@ int QDContext::compute_error(const double* lo, const double* hi, double* err) {
     double scale = ode.err_scale[i];
     double ss = h[key * 3 + 0], sh = h[key * 3 + 1], mx = h[key * 3 + 2];
     if (ode.norm == SCY_NORM_L2_ABS) {
-      tot += std::sqrt(ss) / (std::sqrt((double)Nz) * scale);
+      tot += std::sqrt(ss) / (std::sqrt((double)key_len[key]) * scale);
     } else if (ode.method == SCY_RK32) {
       tot += std::sqrt(ss) / (std::sqrt(sh) * scale);
     } else {
@@ -592,7 +613,8 @@ enum { V_VAR = 0, V_DVAR, V_K, V_F1, V_F2, V_F3, V_F4, V_F5, V_F6, V_LO, V_HI };
 
 int QDContext::attempt(double dt, double** lo, double** hi) {
   cudaStream_t s = sbp.stream;
-  const int n = 2 * Nz, tb = 256, gb = (n + tb - 1) / tb;
+  const long n = nvar;
+  const int tb = 256, gb = (int)((n + tb - 1) / tb);
   double* var = rk[V_VAR].as<double>();
   double* f0 = rk[V_DVAR].as<double>();
   double* k = rk[V_K].as<double>();
@@ -659,23 +681,37 @@ int QDContext::attempt(double dt, double** lo, double** hi) {
   return SCY_OK;
 }
 
+// setErrInds: an empty list means every integrated field in the map's
+// sorted key order (odeSolver.cpp:77-95)
+int QDContext::check_err_keys(scy_ode_opts& o) const {
+  if (o.n_err <= 0) {
+    const int le[2] = {SCY_KEY_PSI, SCY_KEY_SLIP};
+    const int pk[4] = {SCY_KEY_GVXY, SCY_KEY_GVXZ, SCY_KEY_PSI, SCY_KEY_SLIP};
+    o.n_err = pl ? 4 : 2;
+    for (int i = 0; i < o.n_err; ++i) {
+      o.err_keys[i] = pl ? pk[i] : le[i];
+      o.err_scale[i] = 1.0;
+    }
+  }
+  if (o.n_err > 4) {
+    set_error("at most four error indices");
+    return SCY_ERR_ARG;
+  }
+  for (int i = 0; i < o.n_err; ++i)
+    if (o.err_keys[i] < 0 || o.err_keys[i] > 3 || key_len[o.err_keys[i]] == 0) {
+      set_error("error index %d names no integrated variable", o.err_keys[i]);
+      return SCY_ERR_ARG;
+    }
+  return SCY_OK;
+}
+
 int QDContext::integrate_begin(const scy_ode_opts& o) {
   ode = o;
   if (ode.method != SCY_RK32 && ode.method != SCY_RK43) {
     set_error("unsupported integrator %d", ode.method);
     return SCY_ERR_ARG;
   }
-  if (ode.n_err <= 0) {
-    ode.n_err = 2;
-    ode.err_keys[0] = SCY_KEY_PSI;
-    ode.err_keys[1] = SCY_KEY_SLIP;
-    ode.err_scale[0] = ode.err_scale[1] = 1.0;
-  }
-  for (int i = 0; i < ode.n_err; ++i)
-    if (ode.err_keys[i] != SCY_KEY_PSI && ode.err_keys[i] != SCY_KEY_SLIP) {
-      set_error("error index %d names no integrated variable", ode.err_keys[i]);
-      return SCY_ERR_ARG;
-    }
+  SCY_TRY(check_err_keys(ode));
   totTol = o.tol;
   currT = o.t0;
   deltaT = o.init_dt;
@@ -725,7 +761,7 @@ int QDContext::integrate_steps(long nsteps, scy_ode_stats* st) {
   cudaStream_t s = sbp.stream;
   double* var = rk[V_VAR].as<double>();
   double* dvar = rk[V_DVAR].as<double>();
-  const int n = 2 * Nz;
+  const long n = nvar;
   long done_steps = 0;
   double totErr = 0.0;
   while (done_steps < nsteps && stepCount < ode.max_steps && currT < ode.t1) {

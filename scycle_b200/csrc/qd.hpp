@@ -53,7 +53,16 @@ struct QDContext {
   double last_t = 0.0;  // time of the last d_dt (for output fields in response mode)
   double f0 = 0.6, v0 = 1e-6;
 
-  int create(const scy_qd_desc& d);
+  // integrated state: length and per-field offsets / lengths by SCY_KEY_*
+  long nvar = 0;
+  long key_off[4] = {0, 0, 0, 0}, key_len[4] = {0, 0, 0, 0};
+  int check_err_keys(scy_ode_opts& o) const;
+  // power-law viscoelastic material (StrikeSlip_PowerLaw_qd); pl = 0: linear elastic
+  int pl = 0;
+  double inv_visc_cap = 0.0;
+  DevBuf pl_c1, pl_e1, pl_n;   // 1e3*A, exp(-B/T), n per node
+  DevBuf sxz, sdev, effVisc;   // N
+  int create(const scy_qd_desc& d, const scy_pl_desc* pl_desc = nullptr);
   // StrikeSlip_LinearElastic_qd::solveSS + solveSSb + Fault::guessSS: fills
   // psi (unless keep_psi) and slip, updates bcL, bcRShift, slipVel, u.
   int steady_state_guess(std::vector<double>& psi, int keep_psi, std::vector<double>& slip);
@@ -80,5 +89,9 @@ struct QDContext {
 };
 
 int qd_green_surf_launch(QDContext& q, double c, double* host_out);
+// bcL = slip/faultTypeScale, bcR = vL t/faultTypeScale + bcRShift from the state var
+int qd_bc_launch(QDContext& q, double t, const double* var);
+// StrikeSlip_PowerLaw_qd::d_dt (powerlaw.cu)
+int pl_d_dt(QDContext& q, double t, const double* var, double* f);
 
 }  // namespace scy

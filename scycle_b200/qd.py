@@ -39,6 +39,17 @@ class QD:
     def integrate_begin_from_in(self):
         S.check(S.lib().scy_qd_integrate_begin_from_in(self.h))
 
+    def state_size(self):
+        n = C.c_long()
+        S.check(S.lib().scy_qd_state_size(self.h, C.byref(n)))
+        return n.value
+
+    def set_state_vector(self, var, recompute=True):
+        """The whole integrated state ([gVxy | gVxz |] psi | slip)."""
+        var = np.ascontiguousarray(var, dtype=np.float64)
+        assert var.size == self.state_size()
+        S.check(S.lib().scy_qd_set_state(self.h, S.as_dptr(var), 1 if recompute else 0))
+
     def set_state(self, psi, slip, recompute=True):
         var = np.ascontiguousarray(np.concatenate([psi, slip]), dtype=np.float64)
         S.check(S.lib().scy_qd_set_state(self.h, S.as_dptr(var), 1 if recompute else 0))
@@ -108,7 +119,7 @@ class QD:
         return {"psi": o[:self.Nz], "slip": o[self.Nz:]}
 
     def field(self, name):
-        n = {"u": self.N, "sxy": self.N, "surfDisp": self.Ny}.get(name, self.Nz)
+        n = self.N if name in X.BODY_FIELDS else (self.Ny if name == "surfDisp" else self.Nz)
         out = np.empty(n)
         S.check(S.lib().scy_qd_get_field(self.h, X.FIELDS[name], S.as_dptr(out)))
         return out
