@@ -13,6 +13,11 @@ job stage-solves per second (one stage-solve = one d_dt evaluation);
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
+The line also carries ``cycle``: three quasi-dynamic / fully dynamic cycles
+of the 801x801 constant-grid workload (wall time, simulated years per hour,
+event times, wave-equation steps per second), and ``response_mode``: the same
+steps as ``value`` with the fault stress from the precomputed fault response.
+
 Under torchrun (N > 1) every rank integrates its own replica (weak scaling,
 no data-path collective); the timed region is bracketed by barriers and the
 reported time is the max over ranks.
@@ -321,6 +326,31 @@ def run_cycle(args):
     return out
 
 
+def run_wave_only(args):
+    """The cycle workload on an n x n grid run into its first fully dynamic
+    phase, then the wave-equation and fault launches timed alone (for
+    profiling)."""
+    import torch
+    from scycle_b200 import build
+    build.build(verbose=False)
+    from scycle_b200.configs import make_qdfd_problem
+    from scycle_b200.cycle import Cycle
+    n = args.profile_wave
+    work = tempfile.mkdtemp(prefix="scy_wave_")
+    path = make_qdfd_problem(work, Ny=n, Nz=n, cycles=3, years=1000.0, extra={"fd_ayIndexQuirk": "0"})
+    c = Cycle.from_in(path, solve_rtol=args.rtol)
+    c.set_mode("response")
+    c.begin_from_in()
+    st = c.run(50)
+    while st.phase != 1 and not st.done:
+        st = c.run(50)
+    st = c.run(20)
+    w, f = c.time_kernels(args.profile_reps)
+    print(json.dumps({"wave_only": True, "n": n, "step": st.step_count, "phase": st.phase, "wave_us": w,
+                      "fault_us": f, "wave_algorithmic_GBps": 24.0 * n * n / (w * 1e-6) / 1e9}))
+    c.close()
+
+
 def run_stencil_only(args):
     """A x on an n x n grid (FP64, constant grid, Dirichlet/Neumann SATs): the
     operator kernel alone, sized past L2 when n >= 4097, for profiling."""
@@ -417,11 +447,17 @@ def main():
     ap.add_argument("--cycle-mode", default="response", choices=["response", "solve"])
     ap.add_argument("--profile-stencil", type=int, default=0,
                     help="time only the FP64 operator kernel on an n x n grid and exit")
+    ap.add_argument("--profile-wave", type=int, default=0,
+                    help="run the cycle workload on an n x n grid into a wave phase, time its two launches, exit")
+    ap.add_argument("--profile-reps", type=int, default=20)
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
     if args.profile_stencil:
         run_stencil_only(args)
+        return
+    if args.profile_wave:
+        run_wave_only(args)
         return
     dist, rank, world, local = _dist()
     try:
