@@ -459,11 +459,14 @@ scy_status scy_cycle_set_fd_state(scy_cycle* c, double t, long step, int allowed
                                   const double* slipPrev, const double* uPrev, const double* u0,
                                   const double* slip0, const double* tau0, const double* slipVel);
 /* Profiling hook: average device time (CUDA events, `reps` back-to-back
- * launches each) of the wave-equation stencil launch and of the fault launch
- * of one fully dynamic step, on the driver's current wave state.  Both
- * launches rewrite the step-n+1 buffers and the fault's slip velocity, so
- * call it only when the run is over or about to be restarted. */
-scy_status scy_cycle_time_kernels(scy_cycle* c, int reps, double* wave_us, double* fault_us);
+ * launches each) of one fully dynamic step as the fused launch (step_us) and
+ * of the two-launch form's wave stencil and fault update, on the driver's
+ * current wave state.  The launches rewrite the step-n+1 buffers and the
+ * fault's slip velocity, so call it only when the run is over or about to be
+ * restarted. */
+scy_status scy_cycle_time_kernels(scy_cycle* c, int reps, double* wave_us, double* fault_us, double* step_us);
+/* 1: one fused launch per wave step (default); 0: the two-launch form. */
+scy_status scy_cycle_set_fd_fused(scy_cycle* c, int fused);
 /* Host-only (no GPU needed): the cycle settings of an input file after
  * checkInput (pointer members set to NULL), the wave-equation step of
  * computeTimeStep and the penalty vector ay of computePenaltyVectors (Ny*Nz

@@ -101,7 +101,9 @@ def declare_cycle(L):
     L.scy_cycle_set_mode.argtypes = [vp, C.c_int]
     L.scy_cycle_set_jacobian.argtypes = [vp, C.c_int]
     L.scy_cycle_set_fd_batch.argtypes = [vp, C.c_int]
-    L.scy_cycle_time_kernels.argtypes = [vp, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    L.scy_cycle_time_kernels.argtypes = [vp, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                         C.POINTER(C.c_double)]
+    L.scy_cycle_set_fd_fused.argtypes = [vp, C.c_int]
     L.scy_cycle_set_fd_state.argtypes = [vp, C.c_double, C.c_long, C.c_int] + [dptr] * 10
     L.scy_in_cycle_info.argtypes = [C.c_char_p, C.POINTER(CycleDesc), C.POINTER(C.c_double), dptr, C.c_long,
                                     C.POINTER(C.c_long)]

@@ -692,9 +692,20 @@ scy_status scy_cycle_set_fd_state(scy_cycle* c, double t, long step, int allowed
   return c->ctx.set_fd_state(t, step, allowed, now, u, prev, uPrev, u0, slip0, tau0, slipVel);
 }
 
-scy_status scy_cycle_time_kernels(scy_cycle* c, int reps, double* wave_us, double* fault_us) {
+scy_status scy_cycle_time_kernels(scy_cycle* c, int reps, double* wave_us, double* fault_us, double* step_us) {
   if (!c) return SCY_ERR_ARG;
-  return c->ctx.time_kernels(reps, wave_us, fault_us);
+  return c->ctx.time_kernels(reps, wave_us, fault_us, step_us);
+}
+
+scy_status scy_cycle_set_fd_fused(scy_cycle* c, int fused) {
+  if (!c) return SCY_ERR_ARG;
+  const int parts = fused ? scy::FD_FUSED : (scy::FD_WAVE | scy::FD_FAULT);
+  if (parts != c->ctx.fd_parts) {
+    for (auto& g : c->ctx.graphs) cudaGraphExecDestroy(g.second);
+    c->ctx.graphs.clear();
+    c->ctx.fd_parts = parts;
+  }
+  return SCY_OK;
 }
 
 scy_status scy_cycle_force_attempts(scy_cycle* c, const double* dts, const int* acc, long n) {

@@ -41,6 +41,10 @@ struct EpiWave {
   double* __restrict__ d2u;
   double dt;
   int Ny, Nz;
+  // fused step: the fault tile keeps uNext rows 0..4 and the fault row's d2u
+  // of its 32 columns in shared memory (null elsewhere)
+  double* s_rows;
+  double* s_d2u;
   static constexpr bool kReduce = false;
   __device__ __forceinline__ double operator()(long node, int iy, int iz, double Ax, double u) const {
     const bool edge = iy == 0 || iy == Ny - 1 || iz == 0 || iz == Nz - 1;
@@ -53,7 +57,12 @@ struct EpiWave {
     else
       un = (acc + (dt * a - 1.0) * uPrev[node]) / (dt * a + 1.0);
     uNext[node] = un;
-    if (iy == 0) d2u[iz] = (Ax * hinvf[iz]) * jinvf[iz];
+    if (s_rows) {
+      if (iy < 5) s_rows[iy * TZ + (iz & (TZ - 1))] = un;
+      if (iy == 0) s_d2u[iz & (TZ - 1)] = (Ax * hinvf[iz]) * jinvf[iz];
+    } else if (iy == 0) {
+      d2u[iz] = (Ax * hinvf[iz]) * jinvf[iz];
+    }
     return 0.0;
   }
 };
@@ -82,110 +91,105 @@ struct FDFaultArgs {
 
 constexpr int kFaultBlock = 128;
 
-// Fault_fd::d_dt for every fault node, the fault-row stress, tauQS / tauP,
-// then checkSwitchRegime on max(eta V / tauQS) in the last block.
-__global__ void __launch_bounds__(kFaultBlock) fd_fault_kernel(FDFaultArgs A) {
-  CycleDevState* st = A.st;
-  if (st->stop) return;
+// Fault_fd::d_dt for fault node iz (fault.cpp:1436-1575), the fault-row
+// stress of uNext + u0, tauQS and tauP; returns eta V / tauQS.  d2u is the
+// node's Hinv Jinv A u; un(k) returns uNext at body row k (k = 1..4).
+template <class Rows>
+__device__ __forceinline__ double fd_fault_node(const FDFaultArgs& A, int iz, double d2u, const Rows& un_row,
+                                                unsigned* bad_out) {
   const FaultParams& fp = A.fp;
   const int Nz = fp.Nz;
-  const int iz = blockIdx.x * blockDim.x + threadIdx.x;
-  double R = -INFINITY;
-  if (iz < Nz) {
-    const double dt = A.dt;
-    const double rho = A.rho_f[iz], alphay = A.alphay[iz];
-    const double a = fp.a[iz], sN = fp.sN[iz], eta = fp.eta[iz];
-    const double slip0 = A.slip0[iz];
-    const double uPrev = (A.slipPrev[iz] - slip0) * A.inv_fts;
-    double u = (A.slip[iz] - slip0) * A.inv_fts;
-    // setPhi (fault.cpp:1527-1575)
-    const double an = A.d2u[iz] + A.tau0[iz] / alphay;
-    const double Phi = 2.0 / dt * (u - uPrev) + dt * an / rho;
-    const double fricPen = dt / alphay / rho;
-    const double psi = A.psi[iz];
-    // ComputeVel_fd::computeVel (fault.cpp:1594-1644)
-    double V;
-    const double lk = fp.locked[iz];
-    unsigned bad = 0;
-    if (lk > 0.5) {
+  CycleDevState* st = A.st;
+  const double dt = A.dt;
+  const double rho = A.rho_f[iz], alphay = A.alphay[iz];
+  const double a = fp.a[iz], sN = fp.sN[iz], eta = fp.eta[iz];
+  const double slip0 = A.slip0[iz];
+  const double uPrev = (A.slipPrev[iz] - slip0) * A.inv_fts;
+  double u = (A.slip[iz] - slip0) * A.inv_fts;
+  // setPhi (fault.cpp:1527-1575)
+  const double an = d2u + A.tau0[iz] / alphay;
+  const double Phi = 2.0 / dt * (u - uPrev) + dt * an / rho;
+  const double fricPen = dt / alphay / rho;
+  const double psi = A.psi[iz];
+  // ComputeVel_fd::computeVel (fault.cpp:1594-1644)
+  double V;
+  const double lk = fp.locked[iz];
+  unsigned bad = 0;
+  if (lk > 0.5) {
+    V = 0.0;
+  } else if (lk < -0.5) {
+    V = fp.vL;
+  } else {
+    const double right = fabs(Phi);
+    if (isnan(right)) {
+      bad |= FAULT_NONFINITE;
       V = 0.0;
-    } else if (lk < -0.5) {
-      V = fp.vL;
+    } else if (fabs(0.0 - right) < 1e-14) {
+      V = 0.0;
     } else {
-      const double right = fabs(Phi);
-      if (isnan(right)) {
-        bad |= FAULT_NONFINITE;
-        V = 0.0;
-      } else if (fabs(0.0 - right) < 1e-14) {
-        V = 0.0;
-      } else {
-        const ResidVelFD R1{right, fricPen, sN, psi, a, fp.v0, exp(psi / a)};
-        int its = 0;
-        bool ok = true;
-        V = bracketed_newton_f(R1, 0.0, right, fabs(A.slipVel[iz]), fp.root_tol, fp.max_its, &its, &ok);
-        atomicAdd(&st->its, (unsigned long long)its);
-        if (!ok) bad |= FAULT_ROOT_NOCONV;
-      }
-    }
-    // velocity and displacement update (fault.cpp:1481-1496)
-    if (!(V < 1e-14)) {
-      const double fric = strength_psi(sN, psi, V, a, fp.v0);
-      const double alpha = 1.0 / (rho * alphay) * fric / V;
-      const double Ad = 1.0 + alpha * dt;
-      V = Phi / (1. + dt * alpha);
-      u = (2. * u + (an * dt * dt / rho) + (dt * alpha - 1.) * uPrev) / Ad;
-    }
-    A.slipVel[iz] = V;
-    // ComputeAging_fd / ComputeSlipLaw_fd (fault.cpp:1702-1745, :1802-1846)
-    const double psiPrev = A.psiPrev[iz];
-    double psiN;
-    {
+      const ResidVelFD R1{right, fricPen, sN, psi, a, fp.v0, exp(psi / a)};
       int its = 0;
       bool ok = true;
-      if (fp.state_law == 0) {
-        const ResidAgingFD R2{psiPrev, V, fp.b[iz], fp.f0, fp.v0, fp.Dc[iz], dt};
-        psiN = bracketed_newton_f(R2, -2.0, 2.0, psi, fp.root_tol, fp.max_its, &its, &ok);
-      } else {
-        const ResidSlipFD R2{psiPrev, V, a, fp.b[iz], fp.f0, fp.v0, fp.Dc[iz], dt};
-        psiN = bracketed_newton_f(R2, -2.0, 2.0, psi, fp.root_tol, fp.max_its, &its, &ok);
-      }
+      V = bracketed_newton_f(R1, 0.0, right, fabs(A.slipVel[iz]), fp.root_tol, fp.max_its, &its, &ok);
       atomicAdd(&st->its, (unsigned long long)its);
       if (!ok) bad |= FAULT_ROOT_NOCONV;
     }
-    A.psiNext[iz] = psiN;
-    A.slipNext[iz] = A.fts * u + slip0;
-    A.strength[iz] = strength_psi(sN, psiN, V, a, fp.v0);
-    A.uNext[iz] = u;  // body row 0 takes the fault displacement
-    // sxy = mu * Dy (uNext + u0) at the fault (LinearElastic::computeStresses)
-    double d = 0.0;
-#pragma unroll
-    for (int j = HALF; j < BAND; ++j) {
-      const int k = j - HALF;
-      if (k < A.Ny) {
-        const long node = (long)k * Nz + iz;
-        const double un = k == 0 ? u : A.uNext[node];
-        d += A.D0[j] * (un + 1.0 * A.u0[node]);
-      }
-    }
-    if (A.var_grid) d *= A.qy0[iz];
-    const double tq = A.mu0[iz] * d + 1.0 * fp.prestress[iz];
-    A.tauQSP[iz] = tq;
-    A.tauP[iz] = -1.0 * (eta * V) + tq;
-    R = eta * V / tq;
-    if (!isfinite(V) || !isfinite(psiN)) bad |= FAULT_NONFINITE;
-    if (bad) atomicOr(&st->flags, bad);
   }
-  // block max, then the last block finishes the grid max and the switch test
-  __shared__ double sh[32];
+  // velocity and displacement update (fault.cpp:1481-1496)
+  if (!(V < 1e-14)) {
+    const double fric = strength_psi(sN, psi, V, a, fp.v0);
+    const double alpha = 1.0 / (rho * alphay) * fric / V;
+    const double Ad = 1.0 + alpha * dt;
+    V = Phi / (1. + dt * alpha);
+    u = (2. * u + (an * dt * dt / rho) + (dt * alpha - 1.) * uPrev) / Ad;
+  }
+  A.slipVel[iz] = V;
+  // ComputeAging_fd / ComputeSlipLaw_fd (fault.cpp:1702-1745, :1802-1846)
+  const double psiPrev = A.psiPrev[iz];
+  double psiN;
+  {
+    int its = 0;
+    bool ok = true;
+    if (fp.state_law == 0) {
+      const ResidAgingFD R2{psiPrev, V, fp.b[iz], fp.f0, fp.v0, fp.Dc[iz], dt};
+      psiN = bracketed_newton_f(R2, -2.0, 2.0, psi, fp.root_tol, fp.max_its, &its, &ok);
+    } else {
+      const ResidSlipFD R2{psiPrev, V, a, fp.b[iz], fp.f0, fp.v0, fp.Dc[iz], dt};
+      psiN = bracketed_newton_f(R2, -2.0, 2.0, psi, fp.root_tol, fp.max_its, &its, &ok);
+    }
+    atomicAdd(&st->its, (unsigned long long)its);
+    if (!ok) bad |= FAULT_ROOT_NOCONV;
+  }
+  A.psiNext[iz] = psiN;
+  A.slipNext[iz] = A.fts * u + slip0;
+  A.strength[iz] = strength_psi(sN, psiN, V, a, fp.v0);
+  A.uNext[iz] = u;  // body row 0 takes the fault displacement
+  // sxy = mu * Dy (uNext + u0) at the fault (LinearElastic::computeStresses)
+  double d = 0.0;
+#pragma unroll
+  for (int j = HALF; j < BAND; ++j) {
+    const int k = j - HALF;
+    if (k < A.Ny) {
+      const double un = k == 0 ? u : un_row(k);
+      d += A.D0[j] * (un + 1.0 * A.u0[(long)k * Nz + iz]);
+    }
+  }
+  if (A.var_grid) d *= A.qy0[iz];
+  const double tq = A.mu0[iz] * d + 1.0 * fp.prestress[iz];
+  A.tauQSP[iz] = tq;
+  A.tauP[iz] = -1.0 * (eta * V) + tq;
+  if (!isfinite(V) || !isfinite(psiN)) bad |= FAULT_NONFINITE;
+  *bad_out = bad;
+  return eta * V / tq;
+}
+
+// The last of the gridDim.x participating blocks finishes max(eta V / tauQS)
+// and runs checkSwitchRegime for the fully dynamic phase.
+__device__ __forceinline__ void fd_switch_test(const FDFaultArgs& A, double block_max) {
+  CycleDevState* st = A.st;
   __shared__ bool am_last;
-  double m = warp_max(R);
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  if (lane == 0) sh[wid] = m;
-  __syncthreads();
   if (threadIdx.x == 0) {
-    double b = sh[0];
-    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) b = sh[w] > b ? sh[w] : b;
-    A.partials[blockIdx.x] = b;
+    A.partials[blockIdx.x] = block_max;
     __threadfence();
     const unsigned prev = atomicAdd(&st->counter, 1u);
     am_last = prev == gridDim.x - 1;
@@ -199,12 +203,66 @@ __global__ void __launch_bounds__(kFaultBlock) fd_fault_kernel(FDFaultArgs A) {
       mx = v > mx ? v : mx;
     }
     st->maxR = mx;
-    // checkSwitchRegime in the fully dynamic phase
     if (!st->allowed && mx > A.limit_fd) st->allowed = 1;
     if (st->allowed && mx < A.trigger_fd2qd) st->stop = 1;
     st->steps_done += 1;
     st->counter = 0u;
   }
+}
+
+// Fault launch of the two-launch step (used for profiling and as the
+// reference the fused step is tested against).
+__global__ void __launch_bounds__(kFaultBlock) fd_fault_kernel(FDFaultArgs A) {
+  CycleDevState* st = A.st;
+  if (st->stop) return;
+  const int Nz = A.fp.Nz;
+  const int iz = blockIdx.x * blockDim.x + threadIdx.x;
+  double R = -INFINITY;
+  if (iz < Nz) {
+    unsigned bad = 0;
+    auto rows = [&](int k) { return A.uNext[(long)k * Nz + iz]; };
+    R = fd_fault_node(A, iz, A.d2u[iz], rows, &bad);
+    if (bad) atomicOr(&st->flags, bad);
+  }
+  __shared__ double sh[32];
+  double m = warp_max(R);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = m;
+  __syncthreads();
+  double b = sh[0];
+  for (int w = 1; w < (int)(blockDim.x >> 5); ++w) b = sh[w] > b ? sh[w] : b;
+  fd_switch_test(A, b);
+}
+
+// One fully dynamic step in one launch: every tile applies the wave update;
+// the tiles of the fault row (blockIdx.y == 0, rows 0..7) then run the fault
+// update of their 32 columns from the rows they just computed, while the
+// rest of the grid is still stepping the body.
+__global__ void __launch_bounds__(256) fd_step_kernel(LevelDev<double> L, LoadPlain<double> ld, EpiWave ep,
+                                                      FDFaultArgs A) {
+  CycleDevState* st = A.st;
+  if (st->stop) return;
+  __shared__ double s_rows[5 * TZ];
+  __shared__ double s_d2u[TZ];
+  const bool fault_tile = blockIdx.y == 0;
+  EpiWave e = ep;
+  e.s_rows = fault_tile ? s_rows : nullptr;
+  e.s_d2u = fault_tile ? s_d2u : nullptr;
+  stencil_tile<double, LoadPlain<double>, EpiWave>(L, ld, e, nullptr, nullptr, nullptr);
+  if (!fault_tile) return;
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  double R = -INFINITY;
+  if (threadIdx.x < 32) {
+    const int iz = blockIdx.x * TZ + lane;
+    if (iz < A.fp.Nz) {
+      unsigned bad = 0;
+      auto rows = [&](int k) { return s_rows[k * TZ + lane]; };
+      R = fd_fault_node(A, iz, s_d2u[lane], rows, &bad);
+      if (bad) atomicOr(&st->flags, bad);
+    }
+    R = warp_max(R);
+  }
+  fd_switch_test(A, R);
 }
 
 // max over the fault of eta V / tauQS (the quasi-dynamic phase's test)
@@ -367,7 +425,9 @@ int CycleContext::create(const scy_qd_desc& qd, const scy_cycle_desc& cd) {
   SCY_TRY(d2u.alloc(Nz * 8));
   SCY_TRY(slip0.alloc(Nz * 8));
   SCY_TRY(tau0.alloc(Nz * 8));
-  SCY_TRY(dstate.alloc(sizeof(CycleDevState) + 8 * (size_t)((Nz + kFaultBlock - 1) / kFaultBlock + 1)));
+  // block maxima of the switch test: one per fault-row tile (fused step) or
+  // per fault block (two-launch step)
+  SCY_TRY(dstate.alloc(sizeof(CycleDevState) + 8 * (size_t)((Nz + TZ - 1) / TZ + (Nz + kFaultBlock - 1) / kFaultBlock + 2)));
   SCY_CUDA_TRY(cudaMemsetAsync(dstate.p, 0, dstate.bytes, s));
   SCY_CUDA_TRY(cudaMallocHost((void**)&h_state, sizeof(CycleDevState)));
   std::memset(h_state, 0, sizeof(CycleDevState));
@@ -535,13 +595,9 @@ int CycleContext::fd_launch_step(int r, cudaStream_t s, int part) {
              d2u.as<double>(),
              dt_fd,
              Ny,
-             Nz};
-  dim3 g((Nz + TZ - 1) / TZ, (Ny + TY - 1) / TY);
-  if (part & 1) {
-    fd_wave_kernel<<<g, 256, 0, s>>>(L, LoadPlain<double>{u3[cur].as<double>()}, ep, st);
-    SCY_LAUNCH_CHECK();
-  }
-  if (!(part & 2)) return SCY_OK;
+             Nz,
+             nullptr,
+             nullptr};
   FDFaultArgs A{};
   A.fp = q.fp;
   A.D0 = L.y.D;  // row 0 of the band table
@@ -573,12 +629,24 @@ int CycleContext::fd_launch_step(int r, cudaStream_t s, int part) {
   A.trigger_fd2qd = trigger_fd2qd;
   A.partials = reinterpret_cast<double*>(dstate.as<char>() + sizeof(CycleDevState));
   A.st = st;
-  fd_fault_kernel<<<(Nz + kFaultBlock - 1) / kFaultBlock, kFaultBlock, 0, s>>>(A);
-  SCY_LAUNCH_CHECK();
+  const LoadPlain<double> ld{u3[cur].as<double>()};
+  dim3 g((Nz + TZ - 1) / TZ, (Ny + TY - 1) / TY);
+  if (part & FD_FUSED) {
+    fd_step_kernel<<<g, 256, 0, s>>>(L, ld, ep, A);
+    SCY_LAUNCH_CHECK();
+  }
+  if (part & FD_WAVE) {
+    fd_wave_kernel<<<g, 256, 0, s>>>(L, ld, ep, st);
+    SCY_LAUNCH_CHECK();
+  }
+  if (part & FD_FAULT) {
+    fd_fault_kernel<<<(Nz + kFaultBlock - 1) / kFaultBlock, kFaultBlock, 0, s>>>(A);
+    SCY_LAUNCH_CHECK();
+  }
   return SCY_OK;
 }
 
-int CycleContext::time_kernels(int reps, double* wave_us, double* fault_us) {
+int CycleContext::time_kernels(int reps, double* wave_us, double* fault_us, double* step_us) {
   if (reps < 1) reps = 1;
   cudaStream_t s = q.sbp.stream;
   CycleDevState* st = dstate.as<CycleDevState>();
@@ -586,20 +654,21 @@ int CycleContext::time_kernels(int reps, double* wave_us, double* fault_us) {
   cudaEvent_t e0, e1;
   SCY_CUDA_TRY(cudaEventCreate(&e0));
   SCY_CUDA_TRY(cudaEventCreate(&e1));
-  float ms[2] = {0, 0};
+  const int parts[3] = {FD_WAVE, FD_FAULT, FD_FUSED};
+  float ms[3] = {0, 0, 0};
   int rc = SCY_OK;
-  for (int part = 1; part <= 2 && rc == SCY_OK; ++part) {
-    rc = fd_launch_step(rot, s, part);  // warm-up
+  for (int p = 0; p < 3 && rc == SCY_OK; ++p) {
+    rc = fd_launch_step(rot, s, parts[p]);  // warm-up
     if (rc != SCY_OK) break;
     cudaEventRecord(e0, s);
     for (int i = 0; i < reps && rc == SCY_OK; ++i) {
       // keep the stop flag clear: a firing switch test would make later launches no-ops
       cudaMemsetAsync(&st->stop, 0, sizeof(int), s);
-      rc = fd_launch_step(rot, s, part);
+      rc = fd_launch_step(rot, s, parts[p]);
     }
     cudaEventRecord(e1, s);
     cudaEventSynchronize(e1);
-    cudaEventElapsedTime(&ms[part - 1], e0, e1);
+    cudaEventElapsedTime(&ms[p], e0, e1);
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -607,6 +676,7 @@ int CycleContext::time_kernels(int reps, double* wave_us, double* fault_us) {
   SCY_CUDA_TRY(cudaStreamSynchronize(s));
   if (wave_us) *wave_us = ms[0] * 1e3 / reps;
   if (fault_us) *fault_us = ms[1] * 1e3 / reps;
+  if (step_us) *step_us = ms[2] * 1e3 / reps;
   return SCY_OK;
 }
 
@@ -623,7 +693,7 @@ int CycleContext::fd_batch_run(int K, int* n_done, int* stopped) {
     cudaGraph_t graph = nullptr;
     SCY_CUDA_TRY(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
     int rc = SCY_OK;
-    for (int j = 0; j < K && rc == SCY_OK; ++j) rc = fd_launch_step(r0 + j, cs);
+    for (int j = 0; j < K && rc == SCY_OK; ++j) rc = fd_launch_step(r0 + j, cs, fd_parts);
     cudaError_t ce = cudaStreamEndCapture(cs, &graph);
     cudaStreamDestroy(cs);
     if (rc != SCY_OK) {

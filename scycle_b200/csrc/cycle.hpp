@@ -41,6 +41,10 @@ struct CycleSwitch {
 
 enum CyclePhase { CP_QD_BEGIN = 0, CP_QD, CP_FD_BEGIN, CP_FD_SINGLE, CP_FD, CP_DONE };
 
+// launches of one fully dynamic step: the wave stencil and the fault update
+// as two launches, or one fused launch
+enum { FD_WAVE = 1, FD_FAULT = 2, FD_FUSED = 4 };
+
 struct CycleContext {
   QDContext q;
   int Ny = 0, Nz = 0;
@@ -93,8 +97,9 @@ struct CycleContext {
   int enter_fd();                               // the rest of prepare_qd2fd
   int leave_fd();                               // prepare_fd2qd's data movement
   int fd_batch_run(int K, int* n_done, int* stopped);
-  int fd_launch_step(int r, cudaStream_t s, int part = 3);  // part: 1 wave, 2 fault, 3 both
-  int time_kernels(int reps, double* wave_us, double* fault_us);
+  int fd_launch_step(int r, cudaStream_t s, int part);  // FD_* bits
+  int time_kernels(int reps, double* wave_us, double* fault_us, double* step_us);
+  int fd_parts = FD_FUSED;  // what one graph step launches
   int current_u(double* dst);                   // material u of the phase (device)
 };
 

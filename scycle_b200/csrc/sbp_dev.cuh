@@ -49,6 +49,17 @@ struct LevelDev {
   int sep;
   const T *cy1, *m3y1, *wz1;  // Ny
   const T *cz1, *m3z1, *wy1;  // Nz
+  // With sep = 1 the two stages compose, for an interior output row i, into
+  // one 9-point stencil per direction: sy(i) = sum_o Cy[i*9 + o+4] x(i+o, iz)
+  // and sz at column iz = sum_o CzT[(o+4)*Nz + iz] x(iy, iz+o) (host-built).
+  const T *Cy, *CzT;
+  // full = 1: the coefficient fields are separable over every node, so the
+  // whole operator (closures and SAT terms included) composes into one
+  // 17-point stencil per row and per column (offsets -8..8):
+  // (A x)(iy,iz) = wy1[iz] sum_o Cy17[iy*17 + o+8] x(iy+o, iz)
+  //              + wz1[iy] sum_o CzT17[(o+8)*Nz + iz] x(iy, iz+o)
+  int full;
+  const T *Cy17, *CzT17;
 };
 
 // -------------------------------------------------------------------------
@@ -193,8 +204,59 @@ __device__ __forceinline__ void stencil_tile(const LevelDev<T>& L, const Loader&
   __syncthreads();
   // Interior tiles (every stage-1 row in the interior band of both
   // directions) use the constant interior stencil from the kernel parameters.
+  if (L.full) {
+    const int ty = tid / TZ, tz = tid % TZ;
+    const int iy = y0 + ty, iz = z0 + tz;
+    double contrib = 0.0;
+    if (iy < Ny && iz < Nz) {
+      const long node = (long)iy * Nz + iz;
+      const T* cy = L.Cy17 + (long)iy * 17;
+      const T* xy = xs_y + (ty + HX) * TZ + tz;
+      const T* xz = xs_z + ty * (TZ + 2 * HX) + tz + HX;
+      T sy = T(0), sz = T(0);
+#pragma unroll
+      for (int o = 0; o < 17; ++o) {
+        sy += cy[o] * xy[(o - 8) * TZ];
+        sz += L.CzT17[(long)o * Nz + iz] * xz[o - 8];
+      }
+      T Ax = L.wy1[iz] * sy + L.wz1[iy] * sz;
+      contrib = ep(node, iy, iz, Ax, xy[0]);
+    }
+    if constexpr (Epi::kReduce) {
+      if (partials != nullptr) {
+        double tot = block_sum(contrib, red);
+        grid_reduce_finish(tot, partials, counter, red_out, red);
+      }
+    }
+    return;
+  }
   const bool fast = L.y.fast && L.z.fast && y0 - HG >= 4 && y0 + TY + HG - 1 <= Ny - 6 && z0 - HG >= 4 &&
                     z0 + TZ + HG - 1 <= Nz - 6;
+  if (fast && L.sep) {
+    // separable interior: the composed 9-point stencils, straight from the
+    // two staged tiles of x (a warp is one output row, so Cy is a broadcast)
+    const int ty = tid / TZ, tz = tid % TZ;
+    const int iy = y0 + ty, iz = z0 + tz;
+    const long node = (long)iy * Nz + iz;
+    const T* cy = L.Cy + (long)iy * BAND;
+    const T* xy = xs_y + (ty + HX) * TZ + tz;
+    const T* xz = xs_z + ty * (TZ + 2 * HX) + tz + HX;
+    T sy = T(0), sz = T(0);
+#pragma unroll
+    for (int o = 0; o < BAND; ++o) {
+      sy += cy[o] * xy[(o - HALF) * TZ];
+      sz += L.CzT[(long)o * Nz + iz] * xz[o - HALF];
+    }
+    T Ax = L.wy1[iz] * sy + L.wz1[iy] * sz;
+    double contrib = ep(node, iy, iz, Ax, xy[0]);
+    if constexpr (Epi::kReduce) {
+      if (partials != nullptr) {
+        double tot = block_sum(contrib, red);
+        grid_reduce_finish(tot, partials, counter, red_out, red);
+      }
+    }
+    return;
+  }
   if (fast) {
     for (int i = tid; i < (TY + 2 * HG) * TZ; i += blockDim.x) {
       int r = i / TZ, c = i % TZ;

@@ -112,6 +112,45 @@ static int upload_ints(DevBuf& buf, const std::vector<int>& v, cudaStream_t s) {
 }
 
 // ------------------------------------------------------------------------
+// One direction of A composed into 17-point rows: stage 2 (Q, R3^T, R4^T)
+// applied to stage 1 (c D, w3 m3 R3, w4 c R4) over the band tables, plus the
+// SAT terms the stencil adds at the ends (Dirichlet: (BS row + alphaD) * c *
+// x(end); Neumann: +/- c D x at the end row).  C[i*17 + o+8] multiplies
+// x(i+o); bc_lo / bc_hi: 0 Dirichlet, 1 Neumann.
+static void compose_full(const DirTables& t, int bc_lo, int bc_hi, const std::vector<double>& c1,
+                         const std::vector<double>& m31, std::vector<double>& C) {
+  const int n = t.n;
+  C.assign((size_t)n * 17, 0.0);
+  const bool r4 = t.nterms == 3;
+  for (int i = 0; i < n; ++i) {
+    double* row = &C[(size_t)i * 17];
+    for (int a = 0; a < BAND; ++a) {
+      const int k = i + a - HALF;
+      if (k < 0 || k >= n) continue;
+      const double q = t.Q[(size_t)i * BAND + a], q3 = t.R3T[(size_t)i * BAND + a];
+      const double q4 = r4 ? t.R4T[(size_t)i * BAND + a] : 0.0;
+      for (int b = 0; b < BAND; ++b) {
+        const int j = k + b - HALF;
+        if (j < 0 || j >= n) continue;
+        double v = q * (c1[k] * t.D[(size_t)k * BAND + b]);
+        v -= q3 * (t.w3[k] * m31[k] * t.R3[(size_t)k * BAND + b]);
+        if (r4) v -= q4 * (t.w4[k] * c1[k] * t.R4[(size_t)k * BAND + b]);
+        row[j - i + 8] += v;
+      }
+    }
+    if (bc_lo == 0) {
+      if (i < BAND) row[0 - i + 8] += (t.bs0[i] + (i == 0 ? t.alphaD : 0.0)) * c1[0];
+    } else if (i == 0) {
+      for (int b = HALF; b < BAND; ++b) row[b - HALF + 8] += c1[0] * t.D[b];
+    }
+    if (bc_hi == 0) {
+      if (i >= n - BAND) row[(n - 1) - i + 8] += (t.bsN[i - (n - BAND)] + (i == n - 1 ? t.alphaD : 0.0)) * c1[n - 1];
+    } else if (i == n - 1) {
+      for (int b = 0; b <= HALF; ++b) row[b - HALF + 8] -= c1[n - 1] * t.D[(size_t)(n - 1) * BAND + b];
+    }
+  }
+}
+
 template <typename T>
 int LevelStore<T>::init(const LevelHost& h, cudaStream_t s) {
   Ny = h.Ny;
@@ -219,6 +258,65 @@ int LevelStore<T>::init(const LevelHost& h, cudaStream_t s) {
     if (ok) {
       const std::vector<double>* v[6] = {&cy1, &m3y1, &wz1, &cz1, &m3z1, &wy1};
       for (int k = 0; k < 6; ++k) SCY_TRY(upload<T>(sep1[k], *v[k], s));
+      // compose stage 2 (Q, D3^T, D4^T at offsets -2..2) with stage 1 (D, D3,
+      // D4 at offsets -2..2, scaled per row by c, w3*m3, w4*c) into one
+      // 9-point stencil per interior row; rows whose stage-1 rows leave the
+      // interior band stay zero (the fast path never reaches them)
+      auto compose = [](const DirDev<T>& d, int n, const std::vector<double>& c1, const std::vector<double>& m31,
+                        std::vector<double>& C) {
+        C.assign((size_t)n * BAND, 0.0);
+        const int oQ[4] = {-2, -1, 1, 2}, oD[4] = {-2, -1, 1, 2};
+        for (int i = 6; i <= n - 8; ++i) {
+          double row[17] = {0};  // offsets -8..8
+          for (int a = 0; a < 4; ++a) {  // Q * c * D
+            const int k = i + oQ[a];
+            for (int b = 0; b < 4; ++b) row[oQ[a] + oD[b] + 8] += (double)d.cQ[a] * c1[k] * (double)d.cD[b];
+          }
+          for (int a = 0; a < 4; ++a) {  // - D3^T * (w3 m3) * D3: D3^T at -2..1, D3 at -1..2
+            const int k = i + a - 2;
+            for (int b = 0; b < 4; ++b)
+              row[(a - 2) + (b - 1) + 8] -= (double)d.cR3T[a] * (double)d.cw3 * m31[k] * (double)d.cR3[b];
+          }
+          for (int a = 0; a < 5; ++a) {  // - D4^T * (w4 c) * D4: both at -2..2
+            const int k = i + a - 2;
+            for (int b = 0; b < 5; ++b)
+              row[(a - 2) + (b - 2) + 8] -= (double)d.cR4T[a] * (double)d.cw4 * c1[k] * (double)d.cR4[b];
+          }
+          for (int o = -4; o <= 4; ++o) C[(size_t)i * BAND + o + HALF] = row[o + 8];
+        }
+      };
+      std::vector<double> Cy, Cz, CzT((size_t)BAND * Nz);
+      compose(dev.y, Ny, cy1, m3y1, Cy);
+      compose(dev.z, Nz, cz1, m3z1, Cz);
+      for (int iz = 0; iz < Nz; ++iz)
+        for (int o = 0; o < BAND; ++o) CzT[(size_t)o * Nz + iz] = Cz[(size_t)iz * BAND + o];
+      SCY_TRY(upload<T>(comp[0], Cy, s));
+      SCY_TRY(upload<T>(comp[1], CzT, s));
+      dev.Cy = comp[0].template as<T>();
+      dev.CzT = comp[1].template as<T>();
+      // separable over every node too?  then compose the whole operator
+      bool all = true;
+      for (int iy = 0; all && iy < Ny; ++iy)
+        for (int iz = 0; iz < Nz; ++iz) {
+          const size_t i = (size_t)iy * Nz + iz;
+          if (h.cy[i] != cy1[iy] || h.m3y[i] != m3y1[iy] || h.wz[i] != wz1[iy] || h.cz[i] != cz1[iz] ||
+              h.m3z[i] != m3z1[iz] || h.wy[i] != wy1[iz]) {
+            all = false;
+            break;
+          }
+        }
+      if (all) {
+        std::vector<double> Cy17, Cz17, CzT17((size_t)17 * Nz);
+        compose_full(h.ty, h.bc[2], h.bc[0], cy1, m3y1, Cy17);
+        compose_full(h.tz, h.bc[1], h.bc[3], cz1, m3z1, Cz17);
+        for (int iz = 0; iz < Nz; ++iz)
+          for (int o = 0; o < 17; ++o) CzT17[(size_t)o * Nz + iz] = Cz17[(size_t)iz * 17 + o];
+        SCY_TRY(upload<T>(comp17[0], Cy17, s));
+        SCY_TRY(upload<T>(comp17[1], CzT17, s));
+        dev.Cy17 = comp17[0].template as<T>();
+        dev.CzT17 = comp17[1].template as<T>();
+        dev.full = 1;
+      }
       dev.cy1 = sep1[0].template as<T>();
       dev.m3y1 = sep1[1].template as<T>();
       dev.wz1 = sep1[2].template as<T>();

@@ -112,10 +112,13 @@ class Cycle:
                                                *[S.as_dptr(x) for x in arrs]))
 
     def time_kernels(self, reps=50):
-        """(wave launch us, fault launch us) on the current wave state."""
-        w, f = C.c_double(), C.c_double()
-        S.check(S.lib().scy_cycle_time_kernels(self.h, int(reps), C.byref(w), C.byref(f)))
-        return w.value, f.value
+        """(wave launch us, fault launch us, fused step us) on the current wave state."""
+        w, f, t = C.c_double(), C.c_double(), C.c_double()
+        S.check(S.lib().scy_cycle_time_kernels(self.h, int(reps), C.byref(w), C.byref(f), C.byref(t)))
+        return w.value, f.value, t.value
+
+    def set_fd_fused(self, fused=True):
+        S.check(S.lib().scy_cycle_set_fd_fused(self.h, 1 if fused else 0))
 
     def set_mode(self, mode):
         S.check(S.lib().scy_cycle_set_mode(self.h, {"solve": 0, "response": 1}[mode]))

@@ -205,6 +205,25 @@ def test_cycle_graph_batch_invariance(three_cycles):
         assert np.array_equal(out[1][f], out[64][f]), f
 
 
+def test_cycle_fused_step_matches_two_launches(three_cycles):
+    """The fused wave + fault launch gives bitwise the results of the
+    two-launch form, through the switch back to the quasi-dynamic phase."""
+    path, m, rec, hist, snaps = three_cycles
+    snap = snaps[0]
+    out = {}
+    for fused in (True, False):
+        c = _gpu(path)
+        c.set_fd_fused(fused)
+        c.set_fd_state(snap["t"], snap["step"], snap["allowed"], snap["var"], snap["prev"], snap["u0"],
+                       snap["slip0"], snap["tau0"], snap["slipVel"])
+        end = [s["step"] for s in m.switches if s["to"] == "qd" and s["step"] > snap["step"]][0]
+        st = c.run(end - snap["step"])
+        assert st.step_count == end and c.switches()[-1]["step"] == end
+        out[fused] = {f: c.field(f) for f in FIELDS + ("u",)}
+    for f in out[True]:
+        assert np.array_equal(out[True][f], out[False][f]), f
+
+
 def test_cycle_pid_restart_rule(tmp_path):
     """PID control: each phase starts a fresh integrator with no error
     history, so past step 4 its first step-size update is 0 * inf = NaN and
