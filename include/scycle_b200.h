@@ -287,7 +287,8 @@ scy_status scy_qd_get_field(scy_qd* q, int field, double* host_out);
  * format: Domain, LinearElastic, Fault and driver keys, inputDir
  * PETSc-binary fields) and creates the driver (the reference's
  * Domain(file) + StrikeSlip_LinearElastic_qd(D), source/main.cpp:227-233).
- * `solve` sets the elliptic solver (NULL: FP64, rtol 1e-12). */
+ * `solve` sets the elliptic solver (NULL: FP64, rtol 1e-12 and atol 0, or rtol = atol =
+ * kspTol when the file sets it, as LinearElastic passes it to KSPSetTolerances). */
 scy_status scy_qd_create_from_in(const char* path, const scy_solve_opts* solve, scy_qd** out);
 /* Sizes and the integrator settings read from the input file (min_dt is the
  * computeMinTimeStep value unless the file set minDeltaT). */

@@ -378,6 +378,8 @@ scy_status scy_qd_create_from_in(const char* path, const scy_solve_opts* solve, 
     P->desc.solve.precision = SCY_PREC_FP64;
     P->desc.solve.nonzero_guess = 1;
     P->desc.solve.check_every = 1;
+    // LinearElastic / PowerLaw: KSPSetTolerances(ksp, kspTol, kspTol, ...)
+    if (P->ksp_tol > 0) P->desc.solve.rtol = P->desc.solve.atol = P->ksp_tol;
   }
   scy_qd* q = new (std::nothrow) scy_qd();
   if (!q) return SCY_ERR_NOMEM;
@@ -585,10 +587,12 @@ scy_status scy_cycle_create_from_in(const char* path, const scy_solve_opts* solv
     scy::set_error("%s", e.what());
     return SCY_ERR_IO;
   }
-  if (solve)
+  if (solve) {
     P->desc.solve = *solve;
-  else
+  } else {
     default_solve(P->desc.solve);
+    if (P->ksp_tol > 0) P->desc.solve.rtol = P->desc.solve.atol = P->ksp_tol;
+  }
   scy_cycle* c = new (std::nothrow) scy_cycle();
   if (!c) return SCY_ERR_NOMEM;
   int st = c->ctx.create(P->desc, P->cdesc);

@@ -340,6 +340,7 @@ void load_qd_problem(const std::string& path, QDProblem& P, int cycle) {
     else if (e.var == "scale") { auto v = load_vector_double(e.full); scale.insert(scale.end(), v.begin(), v.end()); }
     else if (e.var == "normType") normType = e.rhs;
     else if (e.var == "vL") vL = c_atof(e.rhs);
+    else if (e.var == "kspTol") P.ksp_tol = c_atof(e.rhs);
     else if (e.var == "momBal_bcR_qd") bcRType = e.rhs;
     else if (e.var == "momBal_bcT_qd") bcTType = e.rhs;
     else if (e.var == "momBal_bcL_qd") bcLType = e.rhs;

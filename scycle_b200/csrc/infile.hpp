@@ -41,6 +41,7 @@ struct QDProblem {
   int stride1D = 1, stride2D = 1;
   std::string inputDir, outputDir, stateLaw, integrator;
   double vL = 1e-9, min_dt_user = -1.0;
+  double ksp_tol = -1.0;  // kspTol (LinearElastic: KSP rtol = atol = kspTol), -1 if absent
   std::vector<double> y, z, mu, rho, cs;
   std::vector<double> a, b, sN, Dc, locked, prestress, psi, eta, mu_f, rho_f;
   std::vector<double> bcL0, bcRShift;

@@ -1018,6 +1018,14 @@ int SbpContext::pcg(PC&& pc, const double* rhs, double* u, const scy_solve_opts&
         st.bnorm = std::sqrt(h[0]);
         st.rnorm0 = std::sqrt(h[5]);
         tol = std::max(o.rtol * st.bnorm, o.atol);
+        if (h[0] == 0.0 && tol == 0.0) {
+          // zero right-hand side: the solution is zero (a warm start from
+          // an earlier solve would otherwise never reach ||r|| <= 0)
+          SCY_CUDA_TRY(cudaMemsetAsync(u, 0, n * sizeof(double), stream));
+          st.rnorm = 0.0;
+          st.converged = 1;
+          return SCY_OK;
+        }
       }
       st.rnorm = std::sqrt(h[1]);
       if (!std::isfinite(h[1])) {
