@@ -132,6 +132,115 @@ def make_workload(workdir, n=401, seed=0):
 
 
 # ---------------------------------------------------------------------------
+BATCH_WORKLOAD = ("slip_var_401 ensemble: %d instances per GPU of the 401x401 stretched-grid slip-law workload "
+                  "(seeds differ: lognormal Dc and initial state), every instance with its own RK32 step control")
+
+
+def run_batched(args, dist, rank, world, local):
+    """The batched ensemble: args.batch instances of the workload per GPU
+    advanced together (one CUDA graph launch per round of attempts).  A step
+    is one scy_batch_run(1): every instance advances one accepted step."""
+    import torch
+    from scycle_b200 import _lib as S
+    from scycle_b200.batch import Batch
+    from scycle_b200.qd import QD
+    L = S.lib()
+    K = args.batch
+    work = tempfile.mkdtemp(prefix="scy_batch_")
+    paths = [make_workload(os.path.join(work, "i%d" % s), n=args.n, seed=rank * K + s) for s in range(K)]
+    t0 = time.perf_counter()
+    b = Batch(paths, solve_rtol=args.rtol, precision=args.batch_precision)
+    setup_s = time.perf_counter() - t0
+    for i in range(K):
+        b.instance(i).record_attempts(True)
+    b.run(args.warmup)
+    torch.cuda.synchronize()
+
+    def totals():
+        st = [b.instance(i).integrate_steps(0) for i in range(K)]
+        return sum(x.d_dt_evals for x in st), sum(x.t for x in st)
+
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks = Clocks(local) if rank == 0 else None
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, s0 = totals()
+    st0 = b.run(0)
+    l0 = L.scy_launch_count()
+    torch.cuda.nvtx.range_push("batched_timed")
+    ev0.record()
+    for _ in range(args.steps):
+        st1 = b.run(1)
+    ev1.record()
+    torch.cuda.nvtx.range_pop()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    launches = L.scy_launch_count() - l0
+    clk = clocks.stop() if clocks else None
+    ms = _max_over_ranks(dist, ev0.elapsed_time(ev1))
+    e1, s1 = totals()
+    evals = _sum_over_ranks(dist, e1 - e0)
+    sim_years = _sum_over_ranks(dist, (s1 - s0) / YEAR)
+    out = {"value": evals / (ms / 1e3), "ms_per_step": ms / args.steps, "sim_years_per_hour": sim_years / (ms / 3.6e6),
+           "sim_years_timed": sim_years, "stage_solves": evals, "instances": K * world, "setup_s": setup_s,
+           "rounds": st1.rounds - st0.rounds, "redo_rounds": st1.redo_rounds - st0.redo_rounds,
+           "cg_its": st1.cg_its, "groups": st1.groups, "gpu_launches": int(launches), "clocks": clk,
+           "precision": args.batch_precision}
+    # slip velocity against the plain FP64 single-instance path on instance 0's
+    # own attempt sequence (the reported error of the batched form)
+    if rank == 0:
+        q = QD.from_in(paths[0], solve_rtol=args.rtol, precision="fp64")
+        q.force_attempts(b.instance(0).attempts())
+        q.integrate_begin_from_in()
+        q.integrate_steps(args.warmup + args.steps)
+        v_ref, v_b = q.field("slipVel"), b.instance(0).field("slipVel")
+        out["v_rel_err_vs_fp64_single"] = float(np.max(np.abs(v_b - v_ref) / np.abs(v_ref)))
+        q.close()
+    # end to end through the C ABI: every step the states go host -> device and
+    # psi, slip and slip velocity device -> host (pinned buffers)
+    pin = lambda n: torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    nst = b.state_size()
+    nz_tot = sum(b.instance(i).Nz for i in range(K))
+    hs = {"state": pin(nst), "psi": pin(nz_tot), "slip": pin(nz_tot), "vel": pin(nz_tot)}
+    offs = np.cumsum([0] + [b.instance(i).Nz for i in range(K)])
+    b.fault_field("psi", hs["psi"])
+    b.fault_field("slip", hs["slip"])
+
+    def pack():
+        o = 0
+        for i in range(K):
+            nz = offs[i + 1] - offs[i]
+            hs["state"][o:o + nz] = hs["psi"][offs[i]:offs[i + 1]]
+            hs["state"][o + nz:o + 2 * nz] = hs["slip"][offs[i]:offs[i + 1]]
+            o += 2 * nz
+
+    pack()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e0, _ = totals()
+    t_w = time.perf_counter()
+    ev0.record()
+    for _ in range(args.steps):
+        b.set_states(hs["state"])
+        b.run(1)
+        b.fault_field("psi", hs["psi"])
+        b.fault_field("slip", hs["slip"])
+        b.fault_field("slipVel", hs["vel"])
+        pack()
+    ev1.record()
+    torch.cuda.synchronize()
+    e_ms = _max_over_ranks(dist, ev0.elapsed_time(ev1))
+    e1, _ = totals()
+    out["e2e"] = {"value": _sum_over_ranks(dist, e1 - e0) / (e_ms / 1e3), "unit": "stage-solves/s",
+                  "h2d_bytes_per_step": nst * 8, "d2h_bytes_per_step": 3 * nz_tot * 8,
+                  "wall_s": time.perf_counter() - t_w}
+    b.close()
+    return out
+
+
 def run_ours(args, dist, rank, world, local):
     import torch
     torch.cuda.set_device(local)
@@ -140,6 +249,12 @@ def run_ours(args, dist, rank, world, local):
     from scycle_b200 import _lib as S
     from scycle_b200.qd import QD
     L = S.lib()
+    if args.batch_only:
+        if rank == 0:
+            print(json.dumps(run_batched(args, dist, rank, world, local)))
+        else:
+            run_batched(args, dist, rank, world, local)
+        return
     work = tempfile.mkdtemp(prefix="scy_bench_")
     path = make_workload(work, n=args.n, seed=rank)
     prec = "mixed" if args.precision == "mixed" else "fp64"
@@ -255,22 +370,38 @@ def run_ours(args, dist, rank, world, local):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(path, args)
-    out = {"metric": METRIC, "value": value, "unit": "stage-solves/s", "n_gpus": world, "steps": args.steps,
-           "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
-           "vs_baseline": None, "dtype": "f64 (%s elliptic preconditioner)" % ("fp32" if prec == "mixed" else "fp64"),
-           "data": "synthetic (seeded; reference .in format)",
-           "config": {"workload": WORKLOAD, "Ny": args.n, "Nz": args.n, "integrator": "RK32",
-                      "solver": "FP64 PCG, %s preconditioner (%s), rtol %g" % (
-                          args.precond, "fp32" if prec == "mixed" else "fp64", args.rtol),
-                      "l2": "flushed between steps (256 MB write)", "parallelism": "replicas x%d" % world},
-           "sim_years_per_hour": syph, "sim_years_timed": total_sim_years,
-           "stage_solves": total_evals, "cg_iterations_per_solve": solve_its,
-           "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "gpu_launches": int(launches),
-           "response_mode": resp, "cycle": cycle,
-           "clocks": clk}
+    single = {"value": value, "unit": "stage-solves/s", "ms_per_step": ms_max / args.steps,
+              "sim_years_per_hour": syph, "sim_years_timed": total_sim_years, "stage_solves": total_evals,
+              "cg_iterations_per_solve": solve_its, "gpu_launches": int(launches), "e2e": e2e,
+              "solver": "FP64 PCG, %s preconditioner (%s), rtol %g, residual read back every %d iterations" % (
+                  args.precond, "fp32" if prec == "mixed" else "fp64", args.rtol, args.check_every),
+              "l2": "flushed between steps (256 MB write)", "clocks": clk}
+    q.close()
+    batched = run_batched(args, dist, rank, world, local) if args.batch > 0 else None
+    head = batched if batched else single
+    config = {"workload": (BATCH_WORKLOAD % args.batch) if batched else WORKLOAD, "Ny": args.n, "Nz": args.n,
+              "integrator": "RK32", "parallelism": "replicas x%d" % world}
+    if batched:
+        config.update({"instances_per_gpu": args.batch,
+                       "solver": "FP64 CG preconditioned by fast diagonalisation (%s GEMMs over the ensemble), "
+                                 "device-verified rtol %g" % (args.batch_precision, args.rtol),
+                       "l2": "not flushed: the ensemble's working set (about 20 MB per instance) exceeds the "
+                             "126 MB L2"})
+    else:
+        config.update({"solver": single["solver"], "l2": single["l2"]})
+    out = {"metric": METRIC, "value": head["value"], "unit": "stage-solves/s", "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": head["ms_per_step"],
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f64 (%s preconditioner)" % ((args.batch_precision if batched else prec)),
+           "data": "synthetic (seeded; reference .in format)", "config": config,
+           "sim_years_per_hour": head["sim_years_per_hour"], "sim_years_timed": head["sim_years_timed"],
+           "stage_solves": head["stage_solves"], "e2e": head["e2e"], "roofline": roofline, "cpu_baseline": cpu,
+           "gpu_launches": head["gpu_launches"], "clocks": head["clocks"],
+           "batched": batched, "fp64_single": single,
+           "batched_vs_fp64_single_sim_years": (batched["sim_years_per_hour"] / syph) if batched else None,
+           "response_mode": resp, "cycle": cycle}
     if rank == 0:
         print(json.dumps(out))
-    q.close()
 
 
 CYCLE_WORKLOAD = ("qdfd_const_801: linear-elastic quasi-dynamic / fully dynamic cycles, 801x801 SBP order 4, "
@@ -447,6 +578,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-response", action="store_true")
     ap.add_argument("--no-cycle", action="store_true", help="skip the 801x801 quasi-dynamic / fully dynamic cycles")
+    ap.add_argument("--batch", type=int, default=32, help="instances per GPU of the batched ensemble (0: none)")
+    ap.add_argument("--batch-precision", default="fp64", choices=["fp64", "mixed", "tf32"])
+    ap.add_argument("--batch-only", action="store_true", help="measure the batched ensemble alone")
     ap.add_argument("--cycle-n", type=int, default=801)
     ap.add_argument("--cycle-mode", default="response", choices=["response", "solve"])
     ap.add_argument("--profile-stencil", type=int, default=0,

@@ -113,7 +113,7 @@ scy_status scy_sbp_apply(scy_sbp* s, int op, const double* in, double* out);
 scy_status scy_sbp_set_rhs(scy_sbp* s, const double* bcL, const double* bcR,
                            const double* bcT, const double* bcB, double* rhs);
 
-enum { SCY_PREC_FP64 = 0, SCY_PREC_MIXED = 1 };
+enum { SCY_PREC_FP64 = 0, SCY_PREC_MIXED = 1, SCY_PREC_TF32 = 2 };
 enum {
   SCY_PC_AUTO = 0, /* fast diagonalisation when the grid metrics and mu are
                       separable (y depends only on iy, z only on iz, mu
@@ -473,6 +473,77 @@ scy_status scy_cycle_set_fd_fused(scy_cycle* c, int fused);
  * computeTimeStep and the penalty vector ay of computePenaltyVectors (Ny*Nz
  * doubles into ay when cap allows; *n receives the length). */
 scy_status scy_in_cycle_info(const char* path, scy_cycle_desc* cd, double* dt_fd, double* ay, long cap, long* n);
+
+/* ---------------------------------------------------------------------------
+ * Batched ensemble of quasi-dynamic instances (linear elastic or power law).
+ *
+ * The reference runs one StrikeSlip_*_qd per process
+ * (strikeSlip_linearElastic_qd.cpp:475-505 integrate(), power law
+ * strikeSlip_powerLaw_qd.cpp:521-560); an ensemble is many such runs.  Here
+ * the instances of one batch share every launch: instances whose operators
+ * are identical (grid size, coordinates, mu, boundary types) form a group,
+ * and each RK attempt of every instance is one round of batched launches
+ * per group, captured once as a CUDA graph with the groups on concurrent
+ * streams.  Every instance keeps its own adaptive RK32/RK43 step control
+ * (odeSolver.cpp:505-627, :973-1175), decided on the host from one read-back
+ * per round, and so takes the same steps as the same instance run alone.
+ * The stage solves run a fixed number of preconditioned CG iterations
+ * (fast diagonalisation of the group's operator, FP64 or FP32) with the
+ * convergence test on the device; a round in which an instance misses the
+ * tolerance is repeated for that instance with more iterations, and later
+ * rounds use one more.  Instances must all use the same driver (linear
+ * elastic or power law) and integrator. */
+typedef struct scy_batch scy_batch;
+typedef struct scy_batch_opts {
+  int precision;  /* preconditioner of the FP64 CG: SCY_PREC_FP64 (FP64 GEMMs), SCY_PREC_MIXED (FP32
+                     GEMMs), SCY_PREC_TF32 (FP32 data, GEMMs on the TF32 tensor cores) */
+  int cg_its;     /* CG iterations per stage solve at the start (0: 1 for FP64, 2 otherwise); the
+                     batch raises it after a missed tolerance and tries one fewer after a run of
+                     rounds without one */
+  int graphs;     /* 1: one CUDA graph launch per round (default); 0: the same launches issued directly */
+  int concurrent; /* 1: groups on concurrent streams (default); 0: one stream */
+  int exact_jacobian; /* root-finder derivative of every instance (see scy_qd_set_jacobian) */
+} scy_batch_opts;
+typedef struct scy_batch_stats {
+  long rounds;          /* rounds of batched attempts so far */
+  long redo_rounds;     /* rounds repeated after a missed solve tolerance */
+  long graph_launches;  /* CUDA graph launches so far */
+  long instance_steps;  /* accepted steps summed over the instances */
+  long stage_solves;    /* d_dt evaluations summed over the instances */
+  int cg_its;           /* CG iterations per stage solve now */
+  int groups;           /* groups of instances with one operator */
+  int done;             /* 1: every instance reached its t1 or max_steps */
+} scy_batch_stats;
+/* Creates every instance from its input file (as scy_qd_create_from_in)
+ * and begins it (as scy_qd_integrate_begin_from_in); `solve` as there
+ * (its rtol / atol are the batched solves' tolerance).  opts may be NULL. */
+scy_status scy_batch_create_from_in(int n, const char* const* paths, const scy_solve_opts* solve,
+                                    const scy_batch_opts* opts, scy_batch** out);
+/* Destroys the batch and its instances. */
+scy_status scy_batch_destroy(scy_batch* b);
+/* Number of instances and of groups; group_of (n ints, may be NULL) gets
+ * each instance's group. */
+scy_status scy_batch_info(scy_batch* b, int* n, int* groups, int* group_of);
+/* The driver handle of instance i, owned by the batch: for scy_qd_get_field,
+ * scy_qd_force_attempts, scy_qd_record_attempts, scy_qd_get_attempts and
+ * scy_qd_integrate_steps(q, 0, stats) (its counters).  Advancing it on its
+ * own between batched runs is allowed. */
+scy_status scy_batch_instance(scy_batch* b, int i, scy_qd** q);
+/* Advances every instance by up to nsteps accepted steps (fewer at its t1 /
+ * max_steps); returns once all are done and their rates are evaluated at
+ * the accepted states. */
+scy_status scy_batch_run(scy_batch* b, long nsteps, scy_batch_stats* stats);
+/* Total length of the instances' integrated states (scy_qd_state_size
+ * each), concatenated in the caller's instance order. */
+scy_status scy_batch_state_size(scy_batch* b, long* total);
+/* Replaces every instance's integrated state from one host array of that
+ * length (the rates are not recomputed: give states the instances hold,
+ * e.g. read back after a run, or restart the instances on their own). */
+scy_status scy_batch_set_states(scy_batch* b, const double* host);
+/* A fault field (SCY_FIELD_PSI, SLIP, DPSI, DSLIP, SLIPVEL, TAUP, TAUQSP,
+ * STRENGTH) of every instance into one host array, Nz values per instance
+ * in the caller's instance order. */
+scy_status scy_batch_get_fault_field(scy_batch* b, int field, double* host);
 
 #ifdef __cplusplus
 }

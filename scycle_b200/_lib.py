@@ -19,7 +19,7 @@ BC = {"Dirichlet": 0, "Neumann": 1}
 GRID = {"constantGridSpacing": 0, "variableGridSpacing": 1}
 COMPAT = {"fullyCompatible": 0, "compatible": 1}
 OPS = {"A": 0, "Dy": 1, "Dz": 2, "muxDy": 3, "muxDz": 4, "H": 5, "Hinv": 6, "Dyxmu": 7, "Dzxmu": 8}
-PREC = {"fp64": 0, "mixed": 1}
+PREC = {"fp64": 0, "mixed": 1, "tf32": 2}
 PRECOND = {"auto": 0, "mg": 1, "fd": 2}
 
 dptr = C.POINTER(C.c_double)
@@ -83,6 +83,7 @@ def _declare_extra(L):
     from . import _lib_ext  # noqa: F401  (adds argtypes for the fault / driver API)
     _lib_ext.declare(L)
     _lib_ext.declare_cycle(L)
+    _lib_ext.declare_batch(L)
 
 
 def check(status):

@@ -108,3 +108,27 @@ def declare_cycle(L):
     L.scy_in_cycle_info.argtypes = [C.c_char_p, C.POINTER(CycleDesc), C.POINTER(C.c_double), dptr, C.c_long,
                                     C.POINTER(C.c_long)]
     return L
+
+
+class BatchOpts(C.Structure):
+    _fields_ = [("precision", C.c_int), ("cg_its", C.c_int), ("graphs", C.c_int), ("concurrent", C.c_int),
+                ("exact_jacobian", C.c_int)]
+
+
+class BatchStats(C.Structure):
+    _fields_ = [("rounds", C.c_long), ("redo_rounds", C.c_long), ("graph_launches", C.c_long),
+                ("instance_steps", C.c_long), ("stage_solves", C.c_long), ("cg_its", C.c_int), ("groups", C.c_int),
+                ("done", C.c_int)]
+
+
+def declare_batch(L):
+    vp = C.c_void_p
+    L.scy_batch_create_from_in.argtypes = [C.c_int, C.POINTER(C.c_char_p), C.POINTER(S.SolveOpts),
+                                           C.POINTER(BatchOpts), C.POINTER(vp)]
+    L.scy_batch_destroy.argtypes = [vp]
+    L.scy_batch_info.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.scy_batch_instance.argtypes = [vp, C.c_int, C.POINTER(vp)]
+    L.scy_batch_run.argtypes = [vp, C.c_long, C.POINTER(BatchStats)]
+    L.scy_batch_state_size.argtypes = [vp, C.POINTER(C.c_long)]
+    L.scy_batch_set_states.argtypes = [vp, dptr]
+    L.scy_batch_get_fault_field.argtypes = [vp, C.c_int, dptr]

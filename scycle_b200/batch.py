@@ -1,0 +1,89 @@
+"""Python view of the batched ensemble C ABI (scy_batch_*).
+
+``Batch(paths)`` creates one quasi-dynamic driver per input file (the
+reference's .in format) and runs them together: every RK attempt of every
+instance is one round of shared launches (one CUDA graph launch per round),
+while each instance keeps its own step control.  ``instance(i)`` is a
+``QD`` view of instance i (fields, attempt logs, counters).
+"""
+import ctypes as C
+
+from . import _lib as S
+from . import _lib_ext as X
+from .qd import QD
+
+
+class _InstanceView(QD):
+    """A QD over a handle that the batch owns (never destroyed here)."""
+
+    def close(self):
+        self.h = None
+
+    __del__ = close
+
+
+class Batch:
+    def __init__(self, paths, solve_rtol=1e-12, solve_atol=0.0, precision="fp64", cg_its=0, graphs=True,
+                 concurrent=True, solve_max_its=300, exact_jacobian=True):
+        self.paths = [str(p) for p in paths]
+        arr = (C.c_char_p * len(self.paths))(*[p.encode() for p in self.paths])
+        o = S.SolveOpts(solve_rtol, solve_atol, solve_max_its, 0, 1, 1, S.PRECOND["auto"])
+        bo = X.BatchOpts(S.PREC[precision], int(cg_its), 1 if graphs else 0, 1 if concurrent else 0,
+                         1 if exact_jacobian else 0)
+        h = C.c_void_p()
+        S.check(S.lib().scy_batch_create_from_in(len(self.paths), arr, C.byref(o), C.byref(bo), C.byref(h)))
+        self.h = h
+        n, g = C.c_int(), C.c_int()
+        gof = (C.c_int * len(self.paths))()
+        S.check(S.lib().scy_batch_info(h, C.byref(n), C.byref(g), gof))
+        self.n, self.n_groups, self.group_of = n.value, g.value, list(gof)
+        self._views = []
+        for i in range(self.n):
+            qh = C.c_void_p()
+            S.check(S.lib().scy_batch_instance(h, i, C.byref(qh)))
+            v = _InstanceView.__new__(_InstanceView)
+            v._keep, v.h, v.P = [], qh, None
+            ny, nz = C.c_int(), C.c_int()
+            v.ode = X.OdeOpts()
+            S.check(S.lib().scy_qd_get_problem(qh, C.byref(ny), C.byref(nz), C.byref(v.ode)))
+            v.Ny, v.Nz, v.N = ny.value, nz.value, ny.value * nz.value
+            self._views.append(v)
+
+    def instance(self, i):
+        return self._views[i]
+
+    def run(self, nsteps):
+        st = X.BatchStats()
+        S.check(S.lib().scy_batch_run(self.h, int(nsteps), C.byref(st)))
+        return st
+
+    def state_size(self):
+        n = C.c_long()
+        S.check(S.lib().scy_batch_state_size(self.h, C.byref(n)))
+        return n.value
+
+    def set_states(self, host):
+        """Every instance's integrated state from one float64 array (pinned
+        or pageable), concatenated in instance order."""
+        S.check(S.lib().scy_batch_set_states(self.h, S.as_dptr(host)))
+
+    def fault_field(self, name, out=None):
+        """A fault field of every instance, concatenated (Nz each)."""
+        if out is None:
+            import numpy as np
+            out = np.empty(sum(v.Nz for v in self._views))
+        S.check(S.lib().scy_batch_get_fault_field(self.h, X.FIELDS[name], S.as_dptr(out)))
+        return out
+
+    def close(self):
+        h = getattr(self, "h", None)
+        if h:
+            self.h = None
+            for v in getattr(self, "_views", []):
+                v.h = None
+            try:
+                S.lib().scy_batch_destroy(h)
+            except Exception:
+                pass
+
+    __del__ = close

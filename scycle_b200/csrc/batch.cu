@@ -1,0 +1,1094 @@
+// Batched ensemble of quasi-dynamic instances (see batch.hpp).
+//
+// One round = for every instance: (copy) var = the accepted solution and
+// (acc) the rates at the accepted state, as RK32/RK43::integrate do after an
+// accepted attempt (odeSolver.cpp:599-603, :1148-1152); then (run) one RK
+// attempt (:567-592, :1080-1140) and its error sums (:449-501, :902-969).
+// The host reads the sums of all instances once per round and takes each
+// instance's accept / step-size decision with the single-instance
+// QDContext's own step control, so an instance takes the steps it would
+// take alone.
+//
+// A stage d_dt of a group: boundary data and rhs (with its norm), the
+// residual of the warm start, `its` preconditioned CG iterations, the
+// device convergence test, and the fault update (linear elastic) or the
+// viscous rates and fault update (power law), following
+// StrikeSlip_LinearElastic_qd::d_dt (strikeSlip_linearElastic_qd.cpp:756-798)
+// and StrikeSlip_PowerLaw_qd::d_dt (strikeSlip_powerLaw_qd.cpp:633-690).
+#include <cmath>
+#include <cstring>
+#include <string>
+
+#include "batch.hpp"
+#include "capi_types.hpp"
+#include "common.cuh"
+#include "fault_node.cuh"
+#include "powerlaw_dev.cuh"
+
+namespace scy {
+
+#define SCY_BLAS_TRY(call)                                                 \
+  do {                                                                     \
+    cublasStatus_t b_ = (call);                                            \
+    if (b_ != CUBLAS_STATUS_SUCCESS) {                                     \
+      ::scy::set_error("%s:%d: %s failed (%d)", __FILE__, __LINE__, #call, \
+                       (int)b_);                                           \
+      return SCY_ERR_CUDA;                                                 \
+    }                                                                      \
+  } while (0)
+
+namespace {
+
+constexpr int TB = 256;
+
+// blocks per instance for the node loops: about four nodes per thread
+int node_blocks(long N) {
+  long b = (N + 4L * TB - 1) / (4L * TB);
+  return (int)std::max(1L, std::min(b, 1024L));
+}
+
+__device__ __forceinline__ double stage_time(const double* t, const double* dt, int g, double c) {
+  return __dadd_rn(t[g], __dmul_rn(c, dt[g]));
+}
+
+// bcL = slip / faultTypeScale, bcR = vL t / faultTypeScale + bcRShift
+__global__ void b_bc_kernel(const BatchInst* __restrict__ tab, const int* __restrict__ mask,
+                            const double* __restrict__ t, const double* __restrict__ dt, int base, double c,
+                            int in_slot) {
+  const int k = blockIdx.z;
+  if (!mask[k]) return;
+  const BatchInst& I = tab[k];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= I.fp.Nz) return;
+  const double te = stage_time(t, dt, base + k, c);
+  if (I.bcL_from_slip) I.bcL[i] = I.rk[in_slot][I.fp.slip_off + i] * I.inv_fts;
+  if (I.bcR_remote) I.bcR[i] = I.vL * te * I.inv_fts + I.bcRShift[i];
+}
+
+// rhs = setRhs(bc) (+ B gVxy + C gVxz for the power law); |rhs|^2 -> sc[0]
+__global__ void b_rhs_kernel(LevelDev<double> L, const BatchInst* __restrict__ tab, const int* __restrict__ mask,
+                             int in_slot, BatchWork w) {
+  __shared__ double sh[32];
+  const int k = blockIdx.z;
+  if (!mask[k]) return;
+  const BatchInst& I = tab[k];
+  const double* gxy = I.c1 ? I.rk[in_slot] + I.key_off[SCY_KEY_GVXY] : nullptr;
+  const double* gxz = I.c1 ? I.rk[in_slot] + I.key_off[SCY_KEY_GVXZ] : nullptr;
+  double acc = 0.0;
+  for (long node = blockIdx.x * (long)blockDim.x + threadIdx.x; node < w.N; node += (long)gridDim.x * blockDim.x) {
+    double v = set_rhs_node(L, I.bcL, I.bcR, I.bcT, I.bcB, node);
+    if (gxy) v = v + 1.0 * pl_source_node(L, gxy, gxz, node);
+    I.rhs[node] = v;
+    acc += v * v;
+  }
+  double s = block_sum(acc, sh);
+  grid_reduce_finish(s, w.partials + (long)k * w.PB, w.counters + 4 * k, w.sc + 16 * k + 0, sh);
+}
+
+// r = -rhs + A u (0 when rhs = 0, whose solution is u = 0); r.r -> sc[5]
+struct EpiBatchResidual {
+  const double* b;
+  double* r;
+  float* r32;
+  bool zero;
+  static constexpr bool kReduce = true;
+  __device__ __forceinline__ double operator()(long node, int, int, double Ax, double) const {
+    double v = zero ? 0.0 : -1.0 * b[node] + Ax;
+    r[node] = v;
+    if (r32) r32[node] = (float)v;
+    return v * v;
+  }
+};
+
+__global__ void __launch_bounds__(256) b_residual_kernel(LevelDev<double> L, const BatchInst* __restrict__ tab,
+                                                         const int* __restrict__ mask, BatchWork w, int mixed) {
+  const int k = blockIdx.z;
+  if (!mask[k]) return;
+  const long off = (long)k * w.N;
+  double* sc = w.sc + 16 * k;
+  EpiBatchResidual ep{tab[k].rhs, w.r + off, mixed ? w.r32 + off : nullptr, sc[0] == 0.0};
+  stencil_tile<double>(L, LoadPlain<double>{tab[k].u}, ep, w.partials + (long)k * w.PB, w.counters + 4 * k, sc + 5);
+}
+
+// rz = r.z -> sc[2] (the previous value moves to sc[3])
+template <typename Tz>
+__global__ void b_dot_rz_kernel(const int* __restrict__ mask, BatchWork w, const Tz* __restrict__ z) {
+  __shared__ double sh[32];
+  const int k = blockIdx.z;
+  if (!mask[k]) return;
+  const long off = (long)k * w.N;
+  double acc = 0.0;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < w.N; i += (long)gridDim.x * blockDim.x)
+    acc += w.r[off + i] * (double)z[off + i];
+  double t = block_sum(acc, sh);
+  __shared__ bool am_last;
+  const unsigned nb = gridDim.x;
+  double* partials = w.partials + (long)k * w.PB;
+  unsigned* counter = w.counters + 4 * k;
+  if (threadIdx.x == 0) {
+    partials[blockIdx.x] = t;
+    __threadfence();
+    am_last = atomicAdd(counter, 1u) == nb - 1;
+  }
+  __syncthreads();
+  if (am_last) {
+    __threadfence();
+    double s = 0.0;
+    for (int i = threadIdx.x; i < (int)nb; i += blockDim.x) s += ((volatile double*)partials)[i];
+    s = block_sum(s, sh);
+    if (threadIdx.x == 0) {
+      double* sc = w.sc + 16 * k;
+      sc[3] = sc[2];
+      sc[2] = s;
+      *counter = 0u;
+    }
+  }
+}
+
+// p_new = z + beta p_old ; q = -A p_new ; p.q -> sc[4]
+template <typename Tz>
+__global__ void __launch_bounds__(256) b_matvec_kernel(LevelDev<double> L, const int* __restrict__ mask, BatchWork w,
+                                                       const Tz* __restrict__ z, int first, int pi) {
+  const int k = blockIdx.z;
+  if (!mask[k]) return;
+  const long off = (long)k * w.N;
+  double* sc = w.sc + 16 * k;
+  double* pold = (pi ? w.p1 : w.p0) + off;
+  double* pnew = (pi ? w.p0 : w.p1) + off;
+  LoadPUpdate<Tz> lp{z + off, pold, sc + 2, sc + 3, first};
+  stencil_tile<double>(L, lp, EpiCGMatvec{pnew, w.q + off}, w.partials + (long)k * w.PB, w.counters + 4 * k, sc + 4);
+}
+
+// u += alpha p ; r -= alpha q ; r.r -> sc[1]   (alpha = rz / pq)
+__global__ void b_update_kernel(const BatchInst* __restrict__ tab, const int* __restrict__ mask, BatchWork w, int pi,
+                                int mixed) {
+  __shared__ double sh[32];
+  const int k = blockIdx.z;
+  if (!mask[k]) return;
+  const long off = (long)k * w.N;
+  double* sc = w.sc + 16 * k;
+  const double pqv = sc[4];
+  const double alpha = pqv != 0.0 ? sc[2] / pqv : 0.0;
+  const bool zero = sc[0] == 0.0;
+  const double* p = (pi ? w.p0 : w.p1) + off;  // the p_new of b_matvec_kernel
+  double* x = tab[k].u;
+  double acc = 0.0;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < w.N; i += (long)gridDim.x * blockDim.x) {
+    if (zero) {
+      x[i] = 0.0;
+    } else {
+      x[i] += alpha * p[i];
+    }
+    double rv = w.r[off + i] - alpha * w.q[off + i];
+    w.r[off + i] = rv;
+    if (mixed) w.r32[off + i] = (float)rv;
+    acc += rv * rv;
+  }
+  double t = block_sum(acc, sh);
+  grid_reduce_finish(t, w.partials + (long)k * w.PB, w.counters + 4 * k, sc + 1, sh);
+}
+
+// status bit 1: residual above max(rtol |rhs|, atol); bit 2: non-finite
+__global__ void b_verify_kernel(const int* __restrict__ mask, BatchWork w, double rtol, double atol) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= w.K || !mask[k]) return;
+  const double* sc = w.sc + 16 * k;
+  const double tol = fmax(rtol * sqrt(sc[0]), atol);
+  const double rr = sc[1];
+  if (!isfinite(rr)) atomicOr(w.status + k, 2u);
+  else if (!(sqrt(rr) <= tol) && !(sqrt(sc[5]) <= tol)) atomicOr(w.status + k, 1u);
+}
+
+template <typename T>
+__global__ void b_scale_kernel(T* __restrict__ x, const T* __restrict__ s, long N) {
+  const long off = (long)blockIdx.z * N;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x)
+    x[off + i] *= s[i];
+}
+
+// Fault_qd::d_dt with tauQS = mu Dy u on the fault row (linear elastic) or
+// the material's sxy there (power law)
+__global__ void b_fault_kernel(LevelDev<double> L, const BatchInst* __restrict__ tab, const int* __restrict__ mask,
+                               int in_slot, int out_slot) {
+  const int k = blockIdx.z;
+  if (!mask[k]) return;
+  const BatchInst& I = tab[k];
+  const int iz = blockIdx.x * blockDim.x + threadIdx.x;
+  if (iz >= I.fp.Nz) return;
+  const double sxy = I.c1 ? I.sxy[iz] : fault_row_sxy(L, I.u, iz);
+  fault_node_update(iz, sxy, I.fp, I.rk[in_slot], I.rk[out_slot], I.slipVel, I.tauQSP, I.tauP, I.strength, I.flags,
+                    I.fault_its);
+}
+
+// power law: strains, stresses, viscosity and viscous strain rates per node
+__global__ void b_pl_rates_kernel(LevelDev<double> L, const BatchInst* __restrict__ tab, const int* __restrict__ mask,
+                                  int in_slot, int out_slot, long N) {
+  const int k = blockIdx.z;
+  if (!mask[k]) return;
+  const BatchInst& I = tab[k];
+  PLRatesArgs a;
+  a.u = I.u;
+  a.gxy = I.rk[in_slot] + I.key_off[SCY_KEY_GVXY];
+  a.gxz = I.rk[in_slot] + I.key_off[SCY_KEY_GVXZ];
+  a.bcL = I.bcL;
+  a.bcR = I.bcR;
+  a.c1 = I.c1;
+  a.e1 = I.e1;
+  a.n = I.n;
+  a.inv_cap = I.inv_cap;
+  a.dgxy = I.rk[out_slot] + I.key_off[SCY_KEY_GVXY];
+  a.dgxz = I.rk[out_slot] + I.key_off[SCY_KEY_GVXZ];
+  a.sxy = I.sxy;
+  a.sxz = I.sxz;
+  a.sdev = I.sdev;
+  a.effVisc = I.effVisc;
+  for (long node = blockIdx.x * (long)blockDim.x + threadIdx.x; node < N; node += (long)gridDim.x * blockDim.x)
+    pl_rates_node(L, a, node);
+}
+
+// out = var + sum_j c_j f_j with c_j = (num_j dt) / den_j, in the order of
+// the single-instance combine (first term, then var, then the others)
+struct BCombo {
+  int slot[5];
+  double num[5], den[5];
+  int nf;
+};
+
+__global__ void b_combine_kernel(const BatchInst* __restrict__ tab, const int* __restrict__ mask,
+                                 const double* __restrict__ dt, int base, int out_slot, BCombo cb) {
+  const int k = blockIdx.z;
+  if (!mask[k]) return;
+  const BatchInst& I = tab[k];
+  const double h = dt[base + k];
+  double c[5];
+  const double* f[5];
+#pragma unroll
+  for (int j = 0; j < 5; ++j) {
+    if (j < cb.nf) {
+      const double nd = __dmul_rn(cb.num[j], h);
+      c[j] = cb.den[j] == 1.0 ? nd : __ddiv_rn(nd, cb.den[j]);
+      f[j] = I.rk[cb.slot[j]];
+    }
+  }
+  const double* var = I.rk[V_VAR];
+  double* out = I.rk[out_slot];
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < I.nvar; i += (long)gridDim.x * blockDim.x) {
+    double v = c[0] * f[0][i] + var[i];
+    for (int j = 1; j < cb.nf; ++j) v = v + c[j] * f[j][i];
+    out[i] = v;
+  }
+}
+
+__global__ void b_copy_kernel(const BatchInst* __restrict__ tab, const int* __restrict__ mask) {
+  const int k = blockIdx.z;
+  if (!mask[k]) return;
+  const BatchInst& I = tab[k];
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < I.nvar; i += (long)gridDim.x * blockDim.x)
+    I.rk[V_VAR][i] = I.rk[V_HI][i];
+}
+
+// per (key, instance): sum (lo-hi)^2, sum hi^2, max |lo-hi|/hi -> err[16 g + 3 key ..]
+__global__ void b_error_kernel(const BatchInst* __restrict__ tab, const int* __restrict__ mask, int base,
+                               double* __restrict__ err) {
+  __shared__ double sh[32];
+  const int k = blockIdx.z, key = blockIdx.x;
+  if (!mask[k]) return;
+  const BatchInst& I = tab[k];
+  const long off = I.key_off[key], len = I.key_len[key];
+  if (len == 0) return;
+  const double* lo = I.rk[V_LO];
+  const double* hi = I.rk[V_HI];
+  double ss = 0.0, sh2 = 0.0, mx = -INFINITY;
+  for (long i = threadIdx.x; i < len; i += blockDim.x) {
+    double h = hi[off + i];
+    double d = lo[off + i] - h;
+    ss += d * d;
+    sh2 += h * h;
+    double r = fabs(d) / h;
+    mx = fmax(mx, r);
+  }
+  ss = block_sum(ss, sh);
+  sh2 = block_sum(sh2, sh);
+  double m = warp_max(mx);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double t = threadIdx.x < (blockDim.x + 31) / 32 ? sh[threadIdx.x] : -INFINITY;
+    t = warp_max(t);
+    if (threadIdx.x == 0) {
+      double* o = err + 16L * (base + k) + 3 * key;
+      o[0] = ss;
+      o[1] = sh2;
+      o[2] = t;
+    }
+  }
+}
+
+// fault flags and solve status of every instance of the group -> err[16 g + 14, 15], cleared
+__global__ void b_status_kernel(const BatchInst* __restrict__ tab, BatchWork w, int base, double* __restrict__ err) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= w.K) return;
+  err[16L * (base + k) + 14] = (double)atomicExch(tab[k].flags, 0u);
+  err[16L * (base + k) + 15] = (double)atomicExch(w.status + k, 0u);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+BatchGroup::~BatchGroup() {
+  if (blas) cublasDestroy(blas);
+  if (join) cudaEventDestroy(join);
+  if (stream) cudaStreamDestroy(stream);
+}
+
+BatchContext::~BatchContext() {
+  for (auto& kv : graph_of_its) cudaGraphExecDestroy(kv.second);
+  graph_of_its.clear();
+  groups.clear();
+  if (ctl_host) cudaFreeHost(ctl_host);
+  if (err_host) cudaFreeHost(err_host);
+  if (fork) cudaEventDestroy(fork);
+  if (stream) cudaStreamDestroy(stream);
+  for (scy_qd* p : inst) delete p;
+}
+
+QDContext& BatchContext::q(int i) const { return inst[i]->ctx; }
+
+const double* BatchContext::d_t() const { return ctl.as<double>(); }
+const double* BatchContext::d_dt_() const { return ctl.as<double>() + n; }
+const int* BatchContext::d_copy(const BatchGroup& g) const {
+  return reinterpret_cast<const int*>(ctl.as<double>() + 2 * n) + g.base;
+}
+const int* BatchContext::d_acc(const BatchGroup& g) const { return d_copy(g) + n; }
+const int* BatchContext::d_run(const BatchGroup& g) const { return d_copy(g) + 2 * n; }
+
+static bool same_operator(const SbpContext& a, const SbpContext& b) {
+  const scy_grid_desc &x = a.desc, &y = b.desc;
+  if (x.order != y.order || x.Ny != y.Ny || x.Nz != y.Nz || x.grid_type != y.grid_type || x.compat != y.compat)
+    return false;
+  if (x.Ly != y.Ly || x.Lz != y.Lz) return false;
+  for (int i = 0; i < 4; ++i)
+    if (a.bc[i] != b.bc[i]) return false;
+  return a.y == b.y && a.z == b.z && a.mu == b.mu;
+}
+
+int BatchContext::create(int n_inst, const char* const* paths, const scy_solve_opts* solve,
+                         const scy_batch_opts* o) {
+  n = n_inst;
+  if (o) {
+    precision = o->precision;
+    its = o->cg_its;
+    graphs = o->graphs;
+    concurrent = o->concurrent;
+  }
+  if (precision != SCY_PREC_FP64 && precision != SCY_PREC_MIXED && precision != SCY_PREC_TF32) {
+    set_error("unknown batch precision %d", precision);
+    return SCY_ERR_ARG;
+  }
+  if (its <= 0) its = precision == SCY_PREC_FP64 ? 1 : 2;
+  std::vector<scy_qd*> made(n, nullptr);
+  for (int i = 0; i < n; ++i) {
+    int rc = scy_qd_create_from_in(paths[i], solve, &made[i]);
+    if (rc != SCY_OK) {
+      std::string e = last_error();
+      for (scy_qd* h : made) delete h;
+      set_error("instance %d (%s): %s", i, paths[i], e.c_str());
+      return rc;
+    }
+  }
+  if (o)
+    for (scy_qd* h : made) h->ctx.fp.jacobian = o->exact_jacobian ? 1 : 0;
+  // groups of instances with one operator; the batch addresses instances
+  // group by group (slots), the caller by its own numbering
+  std::vector<std::vector<int>> members;
+  std::vector<int> gof(n);
+  for (int i = 0; i < n; ++i) {
+    int gi = -1;
+    for (size_t g = 0; g < members.size() && gi < 0; ++g)
+      if (same_operator(made[members[g][0]]->ctx.sbp, made[i]->ctx.sbp)) gi = (int)g;
+    if (gi < 0) {
+      gi = (int)members.size();
+      members.emplace_back();
+    }
+    members[gi].push_back(i);
+    gof[i] = gi;
+  }
+  slot_of.assign(n, 0);
+  user_of.clear();
+  inst.clear();
+  group_of = gof;
+  for (auto& m : members)
+    for (int i : m) {
+      slot_of[i] = (int)inst.size();
+      user_of.push_back(i);
+      inst.push_back(made[i]);
+    }
+  const QDContext& q0 = q(0);
+  pl = q0.pl;
+  rtol = q0.solve_opts.rtol;
+  atol = q0.solve_opts.atol;
+  max_its = q0.solve_opts.max_its;
+  method = inst[0]->prob->ode.method;
+  for (int s = 1; s < n; ++s) {
+    if (q(s).pl != pl || inst[s]->prob->ode.method != method) {
+      set_error("instance %d: every instance of a batch needs the same driver and integrator", user_of[s]);
+      return SCY_ERR_ARG;
+    }
+  }
+  // one fast-diagonalisation preconditioner per operator, shared by the
+  // members' own solves as well
+  int base = 0;
+  for (auto& m : members) {
+    SCY_TRY(q(base).sbp.ensure_fd());
+    for (size_t k = 1; k < m.size(); ++k) q(base + (int)k).sbp.fd = q(base).sbp.fd;
+    base += (int)m.size();
+  }
+  // begin every instance (initial state and first rates on its own solver)
+  for (int s = 0; s < n; ++s) {
+    int rc = scy_qd_integrate_begin_from_in(inst[s]);
+    if (rc != SCY_OK) {
+      std::string e = last_error();
+      set_error("instance %d: %s", user_of[s], e.c_str());
+      return rc;
+    }
+  }
+  SCY_CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  SCY_CUDA_TRY(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+  base = 0;
+  for (auto& m : members) {
+    SCY_TRY(setup_group(base, (int)m.size()));
+    base += (int)m.size();
+  }
+  ctl_bytes = (size_t)n * (2 * sizeof(double) + 3 * sizeof(int));
+  SCY_TRY(ctl.alloc(ctl_bytes));
+  SCY_CUDA_TRY(cudaMallocHost(&ctl_host, ctl_bytes));
+  std::memset(ctl_host, 0, ctl_bytes);
+  SCY_TRY(err.alloc((size_t)n * 16 * sizeof(double)));
+  SCY_CUDA_TRY(cudaMemset(err.p, 0, (size_t)n * 16 * sizeof(double)));
+  SCY_CUDA_TRY(cudaMallocHost((void**)&err_host, (size_t)n * 16 * sizeof(double)));
+  hc.assign(n, Ctl());
+  return SCY_OK;
+}
+
+int BatchContext::setup_group(int base, int K) {
+  std::unique_ptr<BatchGroup> G(new BatchGroup());
+  BatchGroup& g = *G;
+  g.K = K;
+  g.base = base;
+  QDContext& q0 = q(base);
+  g.Ny = q0.Ny;
+  g.Nz = q0.Nz;
+  g.N = q0.N;
+  // a steady-state guess changes the boundary types and back, which rebuilds
+  // the members' operators: take the representative's current ones
+  SCY_TRY(q0.sbp.ensure_fd());
+  g.fd = q0.sbp.fd;
+  g.L = q0.sbp.fine->dev;
+  const long KN = (long)g.K * g.N;
+  for (auto& v : g.vec) {
+    SCY_TRY(v.alloc((size_t)KN * 8));
+    SCY_CUDA_TRY(cudaMemset(v.p, 0, (size_t)KN * 8));
+  }
+  for (auto& v : g.vecf) {
+    SCY_TRY(v.alloc((size_t)KN * 4));
+    SCY_CUDA_TRY(cudaMemset(v.p, 0, (size_t)KN * 4));
+  }
+  const int tiles = ((g.Nz + TZ - 1) / TZ) * ((g.Ny + TY - 1) / TY);
+  g.w.PB = std::max(tiles, node_blocks(g.N));
+  SCY_TRY(g.sc.alloc((size_t)g.K * 16 * 8));
+  SCY_CUDA_TRY(cudaMemset(g.sc.p, 0, (size_t)g.K * 16 * 8));
+  SCY_TRY(g.partials.alloc((size_t)g.K * g.w.PB * 8));
+  SCY_TRY(g.counters.alloc((size_t)g.K * 4 * 4));
+  SCY_CUDA_TRY(cudaMemset(g.counters.p, 0, (size_t)g.K * 16));
+  SCY_TRY(g.status.alloc((size_t)g.K * 4));
+  SCY_CUDA_TRY(cudaMemset(g.status.p, 0, (size_t)g.K * 4));
+  g.w.K = g.K;
+  g.w.N = g.N;
+  g.w.r = g.vec[0].as<double>();
+  g.w.p0 = g.vec[1].as<double>();
+  g.w.p1 = g.vec[2].as<double>();
+  g.w.q = g.vec[3].as<double>();
+  g.w.z = g.vec[4].as<double>();
+  g.w.t1 = g.vec[5].as<double>();
+  g.w.t2 = g.vec[6].as<double>();
+  g.w.r32 = g.vecf[0].as<float>();
+  g.w.z32 = g.vecf[1].as<float>();
+  g.w.t1f = g.vecf[2].as<float>();
+  g.w.t2f = g.vecf[3].as<float>();
+  g.w.sc = g.sc.as<double>();
+  g.w.partials = g.partials.as<double>();
+  g.w.counters = g.counters.as<unsigned>();
+  g.w.status = g.status.as<unsigned>();
+  std::vector<BatchInst> tab(g.K);
+  for (int k = 0; k < g.K; ++k) {
+    QDContext& c = q(g.base + k);
+    BatchInst& I = tab[k];
+    std::memset(&I, 0, sizeof(I));
+    for (int j = 0; j < 11; ++j) I.rk[j] = c.rk[j].as<double>();
+    I.u = c.u.as<double>();
+    I.rhs = c.rhs.as<double>();
+    I.bcL = c.bcL.as<double>();
+    I.bcR = c.bcR.as<double>();
+    I.bcT = c.bcT.as<double>();
+    I.bcB = c.bcB.as<double>();
+    I.bcRShift = c.bcRShift.as<double>();
+    I.sxy = c.sxy.as<double>();
+    I.slipVel = c.slipVel.as<double>();
+    I.tauQSP = c.tauQSP.as<double>();
+    I.tauP = c.tauP.as<double>();
+    I.strength = c.strength.as<double>();
+    I.flags = c.flags.as<unsigned>();
+    I.fault_its = c.fault_its.as<unsigned long long>();
+    I.fp = c.fp;
+    I.vL = c.vL;
+    I.inv_fts = 1.0 / c.fts;
+    I.bcL_from_slip = c.bcL_from_slip;
+    I.bcR_remote = c.bcR_remote;
+    I.nvar = c.nvar;
+    for (int j = 0; j < 4; ++j) {
+      I.key_off[j] = c.key_off[j];
+      I.key_len[j] = c.key_len[j];
+    }
+    if (c.pl) {
+      I.c1 = c.pl_c1.as<double>();
+      I.e1 = c.pl_e1.as<double>();
+      I.n = c.pl_n.as<double>();
+      I.sxz = c.sxz.as<double>();
+      I.sdev = c.sdev.as<double>();
+      I.effVisc = c.effVisc.as<double>();
+      I.inv_cap = c.inv_visc_cap;
+    }
+  }
+  SCY_TRY(g.tab.alloc(sizeof(BatchInst) * g.K));
+  SCY_CUDA_TRY(cudaMemcpy(g.tab.p, tab.data(), sizeof(BatchInst) * g.K, cudaMemcpyHostToDevice));
+  SCY_CUDA_TRY(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
+  SCY_CUDA_TRY(cudaEventCreateWithFlags(&g.join, cudaEventDisableTiming));
+  SCY_BLAS_TRY(cublasCreate(&g.blas));
+  const size_t ws = 32u << 20;
+  SCY_TRY(g.blas_ws.alloc(ws));
+  SCY_BLAS_TRY(cublasSetWorkspace(g.blas, g.blas_ws.p, ws));
+  SCY_BLAS_TRY(cublasSetMathMode(g.blas, CUBLAS_DEFAULT_MATH));
+  groups.push_back(std::move(G));
+  return SCY_OK;
+}
+
+// z = K_sep^-1 r for every instance of the group (instance k's r at k*N):
+// Z = Vz [ (Vz^T R Vy) ./ (lz + ly) ] Vy^T with R the Nz x Ny column-major
+// view of an instance; the outer products act on all instances at once
+// (Nz x Ny*K), the inner ones as strided batches.
+int BatchContext::fd_apply(BatchGroup& g) {
+  FDPrecond& F = *g.fd;
+  const int Ny = g.Ny, Nz = g.Nz, K = g.K;
+  const long N = g.N;
+  SCY_BLAS_TRY(cublasSetStream(g.blas, g.stream));
+  dim3 sg(node_blocks(N), 1, K);
+  if (precision != SCY_PREC_FP64) {
+    SCY_BLAS_TRY(cublasSetMathMode(g.blas, precision == SCY_PREC_TF32 ? CUBLAS_TF32_TENSOR_OP_MATH
+                                                                     : CUBLAS_DEFAULT_MATH));
+    const float one = 1.0f, zero = 0.0f;
+    const float* vy = F.Vy32.as<float>();
+    const float* vz = F.Vz32.as<float>();
+    SCY_BLAS_TRY(cublasSgemm(g.blas, CUBLAS_OP_T, CUBLAS_OP_N, Nz, Ny * K, Nz, &one, vz, Nz, g.w.r32, Nz, &zero,
+                             g.w.t1f, Nz));
+    SCY_BLAS_TRY(cublasSgemmStridedBatched(g.blas, CUBLAS_OP_N, CUBLAS_OP_N, Nz, Ny, Ny, &one, g.w.t1f, Nz, N, vy,
+                                           Ny, 0, &zero, g.w.t2f, Nz, N, K));
+    b_scale_kernel<float><<<sg, TB, 0, g.stream>>>(g.w.t2f, F.inv_lam32.as<float>(), N);
+    SCY_LAUNCH_CHECK();
+    SCY_BLAS_TRY(cublasSgemmStridedBatched(g.blas, CUBLAS_OP_N, CUBLAS_OP_T, Nz, Ny, Ny, &one, g.w.t2f, Nz, N, vy,
+                                           Ny, 0, &zero, g.w.t1f, Nz, N, K));
+    SCY_BLAS_TRY(cublasSgemm(g.blas, CUBLAS_OP_N, CUBLAS_OP_N, Nz, Ny * K, Nz, &one, vz, Nz, g.w.t1f, Nz, &zero,
+                             g.w.z32, Nz));
+  } else {
+    SCY_BLAS_TRY(cublasSetMathMode(g.blas, CUBLAS_DEFAULT_MATH));
+    const double one = 1.0, zero = 0.0;
+    const double* vy = F.Vy.as<double>();
+    const double* vz = F.Vz.as<double>();
+    SCY_BLAS_TRY(cublasDgemm(g.blas, CUBLAS_OP_T, CUBLAS_OP_N, Nz, Ny * K, Nz, &one, vz, Nz, g.w.r, Nz, &zero,
+                             g.w.t1, Nz));
+    SCY_BLAS_TRY(cublasDgemmStridedBatched(g.blas, CUBLAS_OP_N, CUBLAS_OP_N, Nz, Ny, Ny, &one, g.w.t1, Nz, N, vy, Ny,
+                                           0, &zero, g.w.t2, Nz, N, K));
+    b_scale_kernel<double><<<sg, TB, 0, g.stream>>>(g.w.t2, F.inv_lam.as<double>(), N);
+    SCY_LAUNCH_CHECK();
+    SCY_BLAS_TRY(cublasDgemmStridedBatched(g.blas, CUBLAS_OP_N, CUBLAS_OP_T, Nz, Ny, Ny, &one, g.w.t2, Nz, N, vy, Ny,
+                                           0, &zero, g.w.t1, Nz, N, K));
+    SCY_BLAS_TRY(cublasDgemm(g.blas, CUBLAS_OP_N, CUBLAS_OP_N, Nz, Ny * K, Nz, &one, vz, Nz, g.w.t1, Nz, &zero,
+                             g.w.z, Nz));
+  }
+  for (int i = 0; i < 4; ++i) count_launch();
+  return SCY_OK;
+}
+
+int BatchContext::solve(BatchGroup& g, const int* mask, int its_now) {
+  const int mixed = precision != SCY_PREC_FP64 ? 1 : 0;
+  const dim3 tg((g.Nz + TZ - 1) / TZ, (g.Ny + TY - 1) / TY, g.K);
+  const dim3 ng(node_blocks(g.N), 1, g.K);
+  const BatchInst* tab = g.tab.as<BatchInst>();
+  b_residual_kernel<<<tg, 256, 0, g.stream>>>(g.L, tab, mask, g.w, mixed);
+  SCY_LAUNCH_CHECK();
+  int pi = 0;
+  for (int it = 1; it <= its_now; ++it) {
+    SCY_TRY(fd_apply(g));
+    if (mixed) {
+      b_dot_rz_kernel<float><<<ng, TB, 0, g.stream>>>(mask, g.w, g.w.z32);
+      SCY_LAUNCH_CHECK();
+      b_matvec_kernel<float><<<tg, 256, 0, g.stream>>>(g.L, mask, g.w, g.w.z32, it == 1 ? 1 : 0, pi);
+    } else {
+      b_dot_rz_kernel<double><<<ng, TB, 0, g.stream>>>(mask, g.w, g.w.z);
+      SCY_LAUNCH_CHECK();
+      b_matvec_kernel<double><<<tg, 256, 0, g.stream>>>(g.L, mask, g.w, g.w.z, it == 1 ? 1 : 0, pi);
+    }
+    SCY_LAUNCH_CHECK();
+    b_update_kernel<<<ng, TB, 0, g.stream>>>(tab, mask, g.w, pi, mixed);
+    SCY_LAUNCH_CHECK();
+    pi ^= 1;
+  }
+  b_verify_kernel<<<(g.K + 127) / 128, 128, 0, g.stream>>>(mask, g.w, rtol, atol);
+  SCY_LAUNCH_CHECK();
+  return SCY_OK;
+}
+
+int BatchContext::d_dt(BatchGroup& g, const int* mask, double c, int in_slot, int out_slot, int its_now) {
+  const BatchInst* tab = g.tab.as<BatchInst>();
+  const dim3 fg((g.Nz + 63) / 64, 1, g.K);
+  const dim3 ng(node_blocks(g.N), 1, g.K);
+  b_bc_kernel<<<fg, 64, 0, g.stream>>>(tab, mask, d_t(), d_dt_(), g.base, c, in_slot);
+  SCY_LAUNCH_CHECK();
+  b_rhs_kernel<<<ng, TB, 0, g.stream>>>(g.L, tab, mask, in_slot, g.w);
+  SCY_LAUNCH_CHECK();
+  SCY_TRY(solve(g, mask, its_now));
+  if (pl) {
+    b_pl_rates_kernel<<<ng, TB, 0, g.stream>>>(g.L, tab, mask, in_slot, out_slot, g.N);
+    SCY_LAUNCH_CHECK();
+  }
+  b_fault_kernel<<<fg, 64, 0, g.stream>>>(g.L, tab, mask, in_slot, out_slot);
+  SCY_LAUNCH_CHECK();
+  return SCY_OK;
+}
+
+int BatchContext::combine(BatchGroup& g, const int* mask, int out_slot, std::initializer_list<int> slots,
+                          std::initializer_list<double> num, std::initializer_list<double> den) {
+  BCombo cb{};
+  int j = 0;
+  for (int s : slots) cb.slot[j++] = s;
+  cb.nf = j;
+  j = 0;
+  for (double v : num) cb.num[j++] = v;
+  j = 0;
+  for (double v : den) cb.den[j++] = v;
+  long nv = q(g.base).nvar;
+  const dim3 gr(node_blocks(nv), 1, g.K);
+  b_combine_kernel<<<gr, TB, 0, g.stream>>>(g.tab.as<BatchInst>(), mask, d_dt_(), g.base, out_slot, cb);
+  SCY_LAUNCH_CHECK();
+  return SCY_OK;
+}
+
+// One round of one group: copy + rates at accepted states, one attempt,
+// its error sums and the status words.
+int BatchContext::enqueue_group(BatchGroup& g, int its_now, int phases) {
+  const BatchInst* tab = g.tab.as<BatchInst>();
+  const int* mc = d_copy(g);
+  const int* ma = d_acc(g);
+  const int* mr = d_run(g);
+  const long nv = q(g.base).nvar;
+  if (phases & 1) {
+    b_copy_kernel<<<dim3(node_blocks(nv), 1, g.K), TB, 0, g.stream>>>(tab, mc);
+    SCY_LAUNCH_CHECK();
+    SCY_TRY(d_dt(g, ma, 0.0, V_VAR, V_DVAR, its_now));
+  }
+  if (!(phases & 2)) {
+    // no attempt this round: only the status words
+  } else if (method == SCY_RK32) {
+    SCY_TRY(combine(g, mr, V_K, {V_DVAR}, {0.5}, {1.0}));
+    SCY_TRY(d_dt(g, mr, 0.5, V_K, V_F1, its_now));
+    SCY_TRY(combine(g, mr, V_K, {V_DVAR, V_F1}, {-1.0, 2.0}, {1.0, 1.0}));
+    SCY_TRY(d_dt(g, mr, 1.0, V_K, V_F2, its_now));
+    SCY_TRY(combine(g, mr, V_LO, {V_DVAR, V_F2}, {0.5, 0.5}, {1.0, 1.0}));
+    SCY_TRY(combine(g, mr, V_HI, {V_DVAR, V_F1, V_F2}, {1.0, 2.0, 1.0}, {6.0, 3.0, 6.0}));
+  } else {
+    using namespace rk43;
+    SCY_TRY(combine(g, mr, V_K, {V_DVAR}, {a21}, {1.0}));
+    SCY_TRY(d_dt(g, mr, c2, V_K, V_F2, its_now));
+    SCY_TRY(combine(g, mr, V_K, {V_DVAR, V_F2}, {a31, a32}, {1.0, 1.0}));
+    SCY_TRY(d_dt(g, mr, c3, V_K, V_F3, its_now));
+    SCY_TRY(combine(g, mr, V_K, {V_DVAR, V_F2, V_F3}, {a41, a42, a43}, {1.0, 1.0, 1.0}));
+    SCY_TRY(d_dt(g, mr, c4, V_K, V_F4, its_now));
+    SCY_TRY(combine(g, mr, V_K, {V_DVAR, V_F2, V_F3, V_F4}, {a51, a52, a53, a54}, {1.0, 1.0, 1.0, 1.0}));
+    SCY_TRY(d_dt(g, mr, c5, V_K, V_F5, its_now));
+    SCY_TRY(combine(g, mr, V_K, {V_DVAR, V_F2, V_F3, V_F4, V_F5}, {a61, a62, a63, a64, a65},
+                    {1.0, 1.0, 1.0, 1.0, 1.0}));
+    SCY_TRY(d_dt(g, mr, c6, V_K, V_F6, its_now));
+    SCY_TRY(combine(g, mr, V_LO, {V_DVAR, V_F3, V_F4, V_F5, V_F6}, {hb1, hb3, hb4, hb5, hb6},
+                    {1.0, 1.0, 1.0, 1.0, 1.0}));
+    SCY_TRY(combine(g, mr, V_HI, {V_DVAR, V_F3, V_F4, V_F5, V_F6}, {b1, b3, b4, b5, b6}, {1.0, 1.0, 1.0, 1.0, 1.0}));
+  }
+  if (phases & 2) {
+    b_error_kernel<<<dim3(4, 1, g.K), 1024, 0, g.stream>>>(tab, mr, g.base, err.as<double>());
+    SCY_LAUNCH_CHECK();
+  }
+  b_status_kernel<<<(g.K + 127) / 128, 128, 0, g.stream>>>(tab, g.w, g.base, err.as<double>());
+  SCY_LAUNCH_CHECK();
+  return SCY_OK;
+}
+
+int BatchContext::enqueue_round(int its_now, int phases) {
+  SCY_CUDA_TRY(cudaEventRecord(fork, stream));
+  for (auto& G : groups) {
+    BatchGroup& g = *G;
+    // concurrent: every group waits for the fork only; otherwise each waits
+    // for the group before it (the fork event is re-recorded behind it)
+    SCY_CUDA_TRY(cudaStreamWaitEvent(g.stream, fork, 0));
+    SCY_TRY(enqueue_group(g, its_now, phases));
+    SCY_CUDA_TRY(cudaEventRecord(g.join, g.stream));
+    if (!concurrent) SCY_CUDA_TRY(cudaEventRecord(fork, g.stream));
+  }
+  for (auto& G : groups) SCY_CUDA_TRY(cudaStreamWaitEvent(stream, G->join, 0));
+  return SCY_OK;
+}
+
+int BatchContext::launch_round(int its_now, int phases) {
+  const int key = its_now * 4 + phases;
+  SCY_CUDA_TRY(cudaMemcpyAsync(ctl.p, ctl_host, ctl_bytes, cudaMemcpyHostToDevice, stream));
+  if (graphs) {
+    auto it = graph_of_its.find(key);
+    if (it == graph_of_its.end()) {
+      cudaGraph_t graph = nullptr;
+      SCY_CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+      const long long l0 = launch_count();
+      int rc = enqueue_round(its_now, phases);
+      cudaError_t ce = cudaStreamEndCapture(stream, &graph);
+      if (rc != SCY_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+      }
+      if (ce != cudaSuccess) {
+        set_error("capturing a batched round failed: %s", cudaGetErrorString(ce));
+        return SCY_ERR_CUDA;
+      }
+      cudaGraphExec_t exec = nullptr;
+      ce = cudaGraphInstantiate(&exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (ce != cudaSuccess) {
+        set_error("instantiating a batched round failed: %s", cudaGetErrorString(ce));
+        return SCY_ERR_CUDA;
+      }
+      // the kernels recorded while capturing run again at every replay
+      kernels_of_its[key] = launch_count() - l0;
+      count_launches(-kernels_of_its[key]);  // recorded, not run
+      it = graph_of_its.emplace(key, exec).first;
+    }
+    SCY_CUDA_TRY(cudaGraphLaunch(it->second, stream));
+    count_launches(kernels_of_its[key]);
+    ++graph_launches;
+  } else {
+    SCY_TRY(enqueue_round(its_now, phases));
+  }
+  SCY_CUDA_TRY(cudaMemcpyAsync(err_host, err.p, (size_t)n * 16 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+  SCY_CUDA_TRY(cudaStreamSynchronize(stream));
+  return SCY_OK;
+}
+
+// --- host step control (QDContext::integrate_steps, one attempt at a time)
+void BatchContext::begin_step(int i) {
+  Ctl& h = hc[i];
+  QDContext& c = q(i);
+  h.running = 0;
+  if (h.done_steps >= h.target || c.stepCount >= c.ode.max_steps || c.currT >= c.ode.t1) return;
+  ++c.stepCount;
+  h.attemptCount = 0;
+  h.running = 1;
+  begin_attempt(i);
+}
+
+void BatchContext::begin_attempt(int i) {
+  Ctl& h = hc[i];
+  QDContext& c = q(i);
+  ++h.attemptCount;
+  if (c.currT + c.deltaT > c.ode.t1) c.deltaT = c.ode.t1 - c.currT;
+  h.forced = c.forced_pos < c.forced_dt.size() ? 1 : 0;
+  h.forced_accept = 0;
+  if (h.forced) {
+    c.deltaT = c.forced_dt[c.forced_pos];
+    h.forced_accept = c.forced_acc[c.forced_pos];
+    ++c.forced_pos;
+  }
+}
+
+void BatchContext::consume(int i, double totErr) {
+  Ctl& h = hc[i];
+  QDContext& c = q(i);
+  bool acc = c.ode.method == SCY_RK32 ? (totErr <= c.totTol) : (totErr < c.totTol);
+  if (h.forced) acc = h.forced_accept != 0;
+  if (c.record) {
+    c.log_dt.push_back(c.deltaT);
+    c.log_acc.push_back(acc ? 1 : 0);
+  }
+  if (acc) return finish_step(i, totErr);
+  double nd = c.compute_step_size(totErr);
+  if (!h.forced) c.deltaT = nd;
+  if (c.ode.min_dt == c.deltaT) return finish_step(i, totErr);
+  ++c.numRejected;
+  if (h.attemptCount >= 100) return finish_step(i, totErr);
+  begin_attempt(i);
+}
+
+void BatchContext::finish_step(int i, double totErr) {
+  Ctl& h = hc[i];
+  QDContext& c = q(i);
+  c.currT = c.currT + c.deltaT;
+  h.copy = h.acc = 1;  // var = hi and the rates there, at the start of the next round
+  if (totErr != 0.0) c.newDeltaT = c.compute_step_size(totErr);
+  c.errA[1] = c.errA[0];
+  c.errA[0] = totErr;
+  c.last_dt = c.deltaT;
+  ++h.done_steps;
+  ++inst_steps;
+  c.deltaT = c.newDeltaT;
+  begin_step(i);
+}
+
+int BatchContext::check_fault_flags() const {
+  for (int i = 0; i < n; ++i) {
+    const unsigned fb = (unsigned)err_host[16 * i + 14];
+    if (fb) {
+      set_error("instance %d: %s", user_of[i],
+                (fb & FAULT_NONFINITE) ? "non-finite value in the fault root bracket or state rate"
+                                       : "rootFinder BracketedNewton did not converge");
+      return (fb & FAULT_NONFINITE) ? SCY_ERR_NONFINITE : SCY_ERR_ROOT_NOCONV;
+    }
+  }
+  return SCY_OK;
+}
+
+int BatchContext::run(long nsteps, scy_batch_stats* st) {
+  // work the caller queued on an instance's own stream comes first
+  for (int i = 0; i < n; ++i) SCY_CUDA_TRY(cudaStreamSynchronize(q(i).sbp.stream));
+  for (int i = 0; i < n; ++i) {
+    if (!q(i).ode_ready) {
+      set_error("instance %d has not been begun", i);
+      return SCY_ERR_STATE;
+    }
+    hc[i].done_steps = 0;
+    hc[i].target = nsteps;
+    hc[i].copy = hc[i].acc = 0;
+    begin_step(i);
+  }
+  const int stages = method == SCY_RK32 ? 2 : 5;
+  double* t = static_cast<double*>(ctl_host);
+  double* dt = t + n;
+  int* mcopy = reinterpret_cast<int*>(dt + n);
+  int* macc = mcopy + n;
+  int* mrun = macc + n;
+  auto phases_of = [&]() {
+    int ph = 0;
+    for (int i = 0; i < n; ++i) {
+      if (macc[i]) ph |= 1;
+      if (mrun[i]) ph |= 2;
+    }
+    return ph;
+  };
+  while (true) {
+    for (int i = 0; i < n; ++i) {
+      const QDContext& c = q(i);
+      t[i] = c.currT;
+      dt[i] = c.deltaT;
+      mcopy[i] = hc[i].copy;
+      macc[i] = hc[i].acc;
+      mrun[i] = hc[i].running;
+    }
+    const int phases = phases_of();
+    if (!phases) break;
+    const int its_round = its;
+    SCY_TRY(launch_round(its_round, phases));
+    ++rounds;
+    // a missed solve tolerance: repeat the round's work for those instances
+    // (the copy is done) with more iterations; later rounds use one more
+    bool missed = false;
+    for (int attempt = 0; attempt < 3; ++attempt) {
+      bool miss = false;
+      for (int i = 0; i < n; ++i) {
+        const unsigned sv = (unsigned)err_host[16 * i + 15];
+        if (sv && (macc[i] || mrun[i])) {
+          miss = true;
+        } else {
+          macc[i] = mrun[i] = 0;
+        }
+        mcopy[i] = 0;
+      }
+      if (!miss) break;
+      missed = true;
+      SCY_TRY(check_fault_flags());
+      const int redo_its = std::min(max_its, (attempt == 0 ? 2 : 8) * its_round);
+      if (attempt == 2 || redo_its <= its_round) {
+        set_error("batched stage solve missed its tolerance after %d CG iterations", redo_its);
+        return SCY_ERR_CG_NOCONV;
+      }
+      SCY_TRY(launch_round(redo_its, phases_of()));
+      ++redo_rounds;
+      for (int i = 0; i < n; ++i) {
+        QDContext& c = q(i);
+        const long e = macc[i] + (mrun[i] ? stages : 0);
+        c.n_d_dt += e;
+        c.n_solves += e;
+        c.n_solve_its += e * redo_its;
+        stage_solves += e;
+      }
+    }
+    // iteration-count tuning: one more after a miss; after a run of rounds
+    // without one, try one fewer (a miss costs one repeated round)
+    if (missed) {
+      its = std::min(max_its, its_round + 1);
+      probe_period = std::min(probe_period * 2, 1L << 14);
+      calm_rounds = 0;
+    } else if (++calm_rounds >= probe_period && its > 1) {
+      --its;
+      calm_rounds = 0;
+    }
+    SCY_TRY(check_fault_flags());
+    for (int i = 0; i < n; ++i) {
+      QDContext& c = q(i);
+      Ctl& h = hc[i];
+      const long e = h.acc + (h.running ? stages : 0);
+      c.n_d_dt += e;
+      c.n_solves += e;
+      c.n_solve_its += e * its_round;
+      stage_solves += e;
+      if (h.acc) c.last_t = c.currT;
+      h.copy = h.acc = 0;
+      if (h.running) consume(i, c.error_from(err_host + 16 * i));
+    }
+  }
+  stats(st);
+  return SCY_OK;
+}
+
+void BatchContext::stats(scy_batch_stats* st) const {
+  if (!st) return;
+  st->rounds = rounds;
+  st->redo_rounds = redo_rounds;
+  st->graph_launches = graph_launches;
+  st->instance_steps = inst_steps;
+  st->stage_solves = stage_solves;
+  st->cg_its = its;
+  st->groups = (int)groups.size();
+  int done = 1;
+  for (int i = 0; i < n; ++i) {
+    const QDContext& c = q(i);
+    if (!(c.stepCount >= c.ode.max_steps || c.currT >= c.ode.t1)) done = 0;
+  }
+  st->done = done;
+}
+
+}  // namespace scy
+
+// ---------------------------------------------------------------------------
+struct scy_batch {
+  scy::BatchContext ctx;
+};
+
+extern "C" {
+
+scy_status scy_batch_create_from_in(int n, const char* const* paths, const scy_solve_opts* solve,
+                                    const scy_batch_opts* opts, scy_batch** out) {
+  if (!out || n < 1 || !paths) {
+    scy::set_error("scy_batch_create_from_in: invalid argument");
+    return SCY_ERR_ARG;
+  }
+  *out = nullptr;
+  for (int i = 0; i < n; ++i)
+    if (!paths[i]) {
+      scy::set_error("scy_batch_create_from_in: path %d is NULL", i);
+      return SCY_ERR_ARG;
+    }
+  scy_batch* b = new (std::nothrow) scy_batch();
+  if (!b) return SCY_ERR_NOMEM;
+  int rc = b->ctx.create(n, paths, solve, opts);
+  if (rc != SCY_OK) {
+    delete b;
+    return rc;
+  }
+  *out = b;
+  return SCY_OK;
+}
+
+scy_status scy_batch_destroy(scy_batch* b) {
+  delete b;
+  return SCY_OK;
+}
+
+scy_status scy_batch_info(scy_batch* b, int* n, int* groups, int* group_of) {
+  if (!b) return SCY_ERR_ARG;
+  if (n) *n = b->ctx.n;
+  if (groups) *groups = (int)b->ctx.groups.size();
+  if (group_of)
+    for (int i = 0; i < b->ctx.n; ++i) group_of[i] = b->ctx.group_of[i];
+  return SCY_OK;
+}
+
+scy_status scy_batch_instance(scy_batch* b, int i, scy_qd** q) {
+  if (!b || !q || i < 0 || i >= b->ctx.n) {
+    scy::set_error("scy_batch_instance: invalid argument");
+    return SCY_ERR_ARG;
+  }
+  *q = b->ctx.inst[b->ctx.slot_of[i]];
+  return SCY_OK;
+}
+
+scy_status scy_batch_state_size(scy_batch* b, long* total) {
+  if (!b || !total) return SCY_ERR_ARG;
+  long t = 0;
+  for (int i = 0; i < b->ctx.n; ++i) t += b->ctx.inst[b->ctx.slot_of[i]]->ctx.nvar;
+  *total = t;
+  return SCY_OK;
+}
+
+scy_status scy_batch_set_states(scy_batch* b, const double* host) {
+  if (!b || !host) return SCY_ERR_ARG;
+  scy::BatchContext& B = b->ctx;
+  long off = 0;
+  for (int i = 0; i < B.n; ++i) {
+    scy::QDContext& c = B.inst[B.slot_of[i]]->ctx;
+    SCY_CUDA_TRY(cudaMemcpyAsync(c.rk[scy::V_VAR].p, host + off, (size_t)c.nvar * sizeof(double),
+                                 cudaMemcpyHostToDevice, B.stream));
+    off += c.nvar;
+  }
+  SCY_CUDA_TRY(cudaStreamSynchronize(B.stream));
+  return SCY_OK;
+}
+
+scy_status scy_batch_get_fault_field(scy_batch* b, int field, double* host) {
+  if (!b || !host) return SCY_ERR_ARG;
+  scy::BatchContext& B = b->ctx;
+  long off = 0;
+  for (int i = 0; i < B.n; ++i) {
+    scy::QDContext& c = B.inst[B.slot_of[i]]->ctx;
+    const double* src = nullptr;
+    switch (field) {
+      case SCY_FIELD_PSI: src = c.rk[scy::V_VAR].as<double>() + c.key_off[SCY_KEY_PSI]; break;
+      case SCY_FIELD_SLIP: src = c.rk[scy::V_VAR].as<double>() + c.key_off[SCY_KEY_SLIP]; break;
+      case SCY_FIELD_DPSI: src = c.rk[scy::V_DVAR].as<double>() + c.key_off[SCY_KEY_PSI]; break;
+      case SCY_FIELD_DSLIP: src = c.rk[scy::V_DVAR].as<double>() + c.key_off[SCY_KEY_SLIP]; break;
+      case SCY_FIELD_SLIPVEL: src = c.slipVel.as<double>(); break;
+      case SCY_FIELD_TAUP: src = c.tauP.as<double>(); break;
+      case SCY_FIELD_TAUQSP: src = c.tauQSP.as<double>(); break;
+      case SCY_FIELD_STRENGTH: src = c.strength.as<double>(); break;
+      default:
+        scy::set_error("scy_batch_get_fault_field: field %d is not a fault field", field);
+        return SCY_ERR_ARG;
+    }
+    SCY_CUDA_TRY(cudaMemcpyAsync(host + off, src, (size_t)c.Nz * sizeof(double), cudaMemcpyDeviceToHost, B.stream));
+    off += c.Nz;
+  }
+  SCY_CUDA_TRY(cudaStreamSynchronize(B.stream));
+  return SCY_OK;
+}
+
+scy_status scy_batch_run(scy_batch* b, long nsteps, scy_batch_stats* st) {
+  if (!b || nsteps < 0) {
+    scy::set_error("scy_batch_run: invalid argument");
+    return SCY_ERR_ARG;
+  }
+  return b->ctx.run(nsteps, st);
+}
+
+}  // extern "C"

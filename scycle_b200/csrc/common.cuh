@@ -14,6 +14,7 @@ namespace scy {
 void set_error(const char* fmt, ...);
 // Counts kernel launches of this library (read by scy_launch_count()).
 void count_launch();
+void count_launches(long long n);  // n kernels launched at once (a CUDA graph replay)
 
 #define SCY_CUDA_TRY(call)                                                     \
   do {                                                                         \
@@ -88,15 +89,18 @@ __device__ __forceinline__ T block_sum(T v, T* sh /* >= 32 entries */) {
   return t;
 }
 
-// Grid-wide deterministic reduction: each block stores its partial sum in
-// partials[linear block id]; the last block to finish adds them in index order and
-// writes *out.  `counter` must be zero on entry and is reset to zero.
+// Grid-wide deterministic reduction over the blocks of one z-slice of the
+// grid (the whole grid when gridDim.z == 1; batched launches give each
+// instance its own slice and pass that slice's partials, counter and out):
+// each block stores its partial sum in partials[block id within the slice];
+// the last block of the slice to finish adds them in index order and writes
+// *out.  `counter` must be zero on entry and is reset to zero.
 __device__ __forceinline__ void grid_reduce_finish(double block_total, double* partials,
                                                    unsigned int* counter, double* out,
                                                    double* sh) {
   __shared__ bool am_last;
-  const unsigned int nblocks = gridDim.x * gridDim.y * gridDim.z;
-  const unsigned int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+  const unsigned int nblocks = gridDim.x * gridDim.y;
+  const unsigned int bid = blockIdx.x + gridDim.x * blockIdx.y;
   if (threadIdx.x == 0) {
     partials[bid] = block_total;
     __threadfence();

@@ -17,116 +17,25 @@
 #include "common.cuh"
 #include "fault_node.cuh"
 #include "qd.hpp"
+#include "powerlaw_dev.cuh"
 #include "sbp_dev.cuh"
 
 namespace scy {
 
-__device__ __forceinline__ double band_row_y(const LevelDev<double>& L, const double* __restrict__ x,
-                                             const double* __restrict__ w, int iy, int iz) {
-  // sum_k D[iy][k] * (w ? w[k,iz] : 1) * x[k,iz]
-  const double* row = L.y.D + (long)iy * BAND;
-  const int Nz = L.Nz;
-  double acc = 0.0;
-#pragma unroll
-  for (int j = 0; j < BAND; ++j) {
-    const int k = iy + j - HALF;
-    if (k >= 0 && k < L.Ny) {
-      const long n = (long)k * Nz + iz;
-      acc += row[j] * (w ? w[n] * x[n] : x[n]);
-    }
-  }
-  return acc;
-}
-
-__device__ __forceinline__ double band_row_z(const LevelDev<double>& L, const double* __restrict__ x,
-                                             const double* __restrict__ w, int iy, int iz) {
-  const double* row = L.z.D + (long)iz * BAND;
-  const int Nz = L.Nz;
-  double acc = 0.0;
-#pragma unroll
-  for (int j = 0; j < BAND; ++j) {
-    const int k = iz + j - HALF;
-    if (k >= 0 && k < Nz) {
-      const long n = (long)iy * Nz + k;
-      acc += row[j] * (w ? w[n] * x[n] : x[n]);
-    }
-  }
-  return acc;
-}
-
 // rhs += B gVxy + C gVxz (computeViscStrainSourceTerms, initializeMomBalMats)
 __global__ void pl_source_kernel(LevelDev<double> L, const double* __restrict__ gxy, const double* __restrict__ gxz,
                                  double* __restrict__ rhs) {
-  const int Ny = L.Ny, Nz = L.Nz;
-  const long N = (long)Ny * Nz;
-  for (long node = blockIdx.x * (long)blockDim.x + threadIdx.x; node < N; node += (long)gridDim.x * blockDim.x) {
-    const int iy = (int)(node / Nz), iz = (int)(node - (long)iy * Nz);
-    const double wyz = L.wy[node] * L.wz[node];  // yq zr H
-    double dy = band_row_y(L, gxy, L.mu, iy, iz);
-    double dz = band_row_z(L, gxz, L.mu, iy, iz);
-    if (L.var) {
-      dy *= L.qy[node];
-      dz *= L.rz[node];
-    }
-    double b = wyz * dy;
-    // Neumann SATs: + zr Hz mu E0y, - zr Hz mu ENy; + yq Hy mu E0z, - yq Hy mu ENz
-    if (L.y.bc_lo == 1 && iy == 0) b += L.wy[node] * L.mu[node] * gxy[node];
-    if (L.y.bc_hi == 1 && iy == Ny - 1) b -= L.wy[node] * L.mu[node] * gxy[node];
-    double c = wyz * dz;
-    if (L.z.bc_lo == 1 && iz == 0) c += L.wz[node] * L.mu[node] * gxz[node];
-    if (L.z.bc_hi == 1 && iz == Nz - 1) c -= L.wz[node] * L.mu[node] * gxz[node];
-    rhs[node] = rhs[node] + 1.0 * (b + c);
-  }
+  const long N = (long)L.Ny * L.Nz;
+  for (long node = blockIdx.x * (long)blockDim.x + threadIdx.x; node < N; node += (long)gridDim.x * blockDim.x)
+    rhs[node] = rhs[node] + 1.0 * pl_source_node(L, gxy, gxz, node);
 }
-
-struct PLRatesArgs {
-  LevelDev<double> L;
-  const double *u, *gxy, *gxz, *bcL, *bcR;
-  const double *c1, *e1, *n;
-  double inv_cap;
-  double *dgxy, *dgxz, *sxy, *sxz, *sdev, *effVisc;
-};
 
 // computeTotalStrains, computeStresses / computeSDev, computeViscosity and
 // computeViscStrainRates (with computeViscousStrainRateSAT) per node
 __global__ void pl_rates_kernel(PLRatesArgs a) {
-  const LevelDev<double>& L = a.L;
-  const int Ny = L.Ny, Nz = L.Nz;
-  const long N = (long)Ny * Nz;
-  for (long node = blockIdx.x * (long)blockDim.x + threadIdx.x; node < N; node += (long)gridDim.x * blockDim.x) {
-    const int iy = (int)(node / Nz), iz = (int)(node - (long)iy * Nz);
-    double gTxy = band_row_y(L, a.u, nullptr, iy, iz);
-    double gTxz = band_row_z(L, a.u, nullptr, iy, iz);
-    if (L.var) {
-      gTxy *= L.qy[node];
-      gTxz *= L.rz[node];
-    }
-    const double mu = L.mu[node];
-    const double sxy = (gTxy + (-1.0) * a.gxy[node]) * mu;
-    const double sxz = (gTxz + (-1.0) * a.gxz[node]) * mu;
-    const double sdev = sqrt(fabs(sxy * sxy + 1.0 * (sxz * sxz)));
-    const double inv = a.c1[node] * pow(sdev, a.n[node] - 1.0) * a.e1[node];
-    const double visc = 1.0 / (a.inv_cap + 1.0 * inv);
-    // SAT of the viscous strain rate at Dirichlet y boundaries
-    double sat = 0.0;
-    if (L.y.bc_lo == 0 && iy == 0) {
-      const double hinv = L.y.Hinvd[0];
-      sat = sat + 1.0 * (hinv * a.u[node]);
-      sat = sat + (-1.0) * (hinv * a.bcL[iz]);
-    }
-    if (L.y.bc_hi == 0 && iy == Ny - 1) {
-      const double hinv = L.y.Hinvd[Ny - 1];
-      sat = sat + (-1.0) * (hinv * a.u[node]);
-      sat = sat + 1.0 * (hinv * a.bcR[iz]);
-    }
-    if (L.var) sat = L.qy[node] * sat;
-    a.dgxy[node] = (mu * sat + 1.0 * sxy) / visc;
-    a.dgxz[node] = sxz / visc;
-    a.sxy[node] = sxy;
-    a.sxz[node] = sxz;
-    a.sdev[node] = sdev;
-    a.effVisc[node] = visc;
-  }
+  const long N = (long)a.L.Ny * a.L.Nz;
+  for (long node = blockIdx.x * (long)blockDim.x + threadIdx.x; node < N; node += (long)gridDim.x * blockDim.x)
+    pl_rates_node(a.L, a, node);
 }
 
 // Fault_qd::d_dt with tauQS from the material's sxy on the fault row

@@ -34,18 +34,9 @@ __global__ void qd_fault_kernel(LevelDev<double> L, const double* __restrict__ u
                                 double* __restrict__ slipVel, double* __restrict__ tauQSP,
                                 double* __restrict__ tauP, double* __restrict__ strength, unsigned* flags,
                                 unsigned long long* its_total) {
-  const int Nz = fp.Nz;
   int iz = blockIdx.x * blockDim.x + threadIdx.x;
-  if (iz >= Nz) return;
-  // Dy row 0 (band offsets -4..4 around row 0; only columns >= 0 exist)
-  double d = 0.0;
-#pragma unroll
-  for (int j = HALF; j < BAND; ++j) {
-    int k = j - HALF;
-    if (k < L.Ny) d += L.y.D[j] * u[(long)k * Nz + iz];
-  }
-  if (L.var) d *= L.qy[iz];
-  const double sxy = L.mu[iz] * d;
+  if (iz >= fp.Nz) return;
+  const double sxy = fault_row_sxy(L, u, iz);
   fault_node_update(iz, sxy, fp, var, f, slipVel, tauQSP, tauP, strength, flags, its_total);
 }
 
@@ -579,6 +570,11 @@ int QDContext::compute_error(const double* lo, const double* hi, double* err) {
   double h[12];
   SCY_CUDA_TRY(cudaMemcpyAsync(h, errbuf.p, (pl ? 12 : 6) * sizeof(double), cudaMemcpyDeviceToHost, s));
   SCY_CUDA_TRY(cudaStreamSynchronize(s));
+  *err = error_from(h);
+  return SCY_OK;
+}
+
+double QDContext::error_from(const double* h) const {
   double tot = 0.0;
   for (int i = 0; i < ode.n_err; ++i) {
     int key = ode.err_keys[i];
@@ -592,8 +588,7 @@ int QDContext::compute_error(const double* lo, const double* hi, double* err) {
       tot += mx / scale;
     }
   }
-  *err = tot;
-  return SCY_OK;
+  return tot;
 }
 
 static Combo combo(std::initializer_list<std::pair<const double*, double>> terms) {
@@ -608,8 +603,6 @@ static Combo combo(std::initializer_list<std::pair<const double*, double>> terms
   return c;
 }
 
-// RK vector slots
-enum { V_VAR = 0, V_DVAR, V_K, V_F1, V_F2, V_F3, V_F4, V_F5, V_F6, V_LO, V_HI };
 
 int QDContext::attempt(double dt, double** lo, double** hi) {
   cudaStream_t s = sbp.stream;
@@ -635,18 +628,7 @@ int QDContext::attempt(double dt, double** lo, double** hi) {
     rk_combine_kernel<<<gb, tb, 0, s>>>(H, var, combo({{f0, dt / 6.0}, {fa, 2 * dt / 3.0}, {fb, dt / 6.0}}), n);
     SCY_LAUNCH_CHECK();
   } else {
-    const double c2 = 1. / 2., c3 = 83. / 250., c4 = 31. / 50., c5 = 17. / 20., c6 = 1.;
-    const double b1 = 82889. / 524892., b3 = 15625. / 83664., b4 = 69875. / 102672., b5 = -2260. / 8211.,
-                 b6 = 1. / 4.;
-    const double hb1 = 4586570599. / 29645900160., hb3 = 178811875. / 945068544.,
-                 hb4 = 814220225. / 1159782912., hb5 = -3700637. / 11593932., hb6 = 61727. / 225920.;
-    const double a21 = 1. / 2., a31 = 13861. / 62500., a32 = 6889. / 62500.;
-    const double a41 = -116923316275. / 2393684061468., a42 = -2731218467317. / 15368042101831.,
-                 a43 = 9408046702089. / 11113171139209.;
-    const double a51 = -451086348788. / 2902428689909., a52 = -2682348792572. / 7519795681897.,
-                 a53 = 12662868775082. / 11960479115383., a54 = 3355817975965. / 11060851509271.;
-    const double a61 = 647845179188. / 3216320057751., a62 = 73281519250. / 8382639484533.,
-                 a63 = 552539513391. / 3454668386233., a64 = 3354512671639. / 8306763924573., a65 = 4040. / 17871.;
+    using namespace rk43;
     double* f2 = rk[V_F2].as<double>();
     double* f3 = rk[V_F3].as<double>();
     double* f4 = rk[V_F4].as<double>();

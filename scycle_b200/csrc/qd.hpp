@@ -9,6 +9,26 @@
 
 namespace scy {
 
+// RK vector slots of QDContext::rk
+enum { V_VAR = 0, V_DVAR, V_K, V_F1, V_F2, V_F3, V_F4, V_F5, V_F6, V_LO, V_HI };
+
+// RK43 tableau (odeSolver.cpp:985-1023): stage times c, stage weights a,
+// solution weights b (order 4) and hb (order 3)
+namespace rk43 {
+constexpr double c2 = 1. / 2., c3 = 83. / 250., c4 = 31. / 50., c5 = 17. / 20., c6 = 1.;
+constexpr double b1 = 82889. / 524892., b3 = 15625. / 83664., b4 = 69875. / 102672., b5 = -2260. / 8211.,
+                 b6 = 1. / 4.;
+constexpr double hb1 = 4586570599. / 29645900160., hb3 = 178811875. / 945068544.,
+                 hb4 = 814220225. / 1159782912., hb5 = -3700637. / 11593932., hb6 = 61727. / 225920.;
+constexpr double a21 = 1. / 2., a31 = 13861. / 62500., a32 = 6889. / 62500.;
+constexpr double a41 = -116923316275. / 2393684061468., a42 = -2731218467317. / 15368042101831.,
+                 a43 = 9408046702089. / 11113171139209.;
+constexpr double a51 = -451086348788. / 2902428689909., a52 = -2682348792572. / 7519795681897.,
+                 a53 = 12662868775082. / 11960479115383., a54 = 3355817975965. / 11060851509271.;
+constexpr double a61 = 647845179188. / 3216320057751., a62 = 73281519250. / 8382639484533.,
+                 a63 = 552539513391. / 3454668386233., a64 = 3354512671639. / 8306763924573., a65 = 4040. / 17871.;
+}  // namespace rk43
+
 struct QDContext {
   SbpContext sbp;
   int Ny = 0, Nz = 0;
@@ -84,6 +104,8 @@ struct QDContext {
   int phase_stopped = 0;
   double compute_step_size(double totErr);
   int compute_error(const double* lo, const double* hi, double* err);
+  // computeError from the per-key sums (sum d^2, sum hi^2, max |d/hi|) at h[3*key]
+  double error_from(const double* h) const;
   int attempt(double dt, double** lo, double** hi);
   int read_flags();
 };

@@ -425,6 +425,55 @@ __device__ __forceinline__ void stencil_tile(const LevelDev<T>& L, const Loader&
   }
 }
 
+// rhs at one node from the boundary data (SbpOps::setRhs,
+// sbpOps_m_constGrid.cpp:877-914): the SAT columns of the Dirichlet
+// boundaries and the Neumann boundary values, times the outer weights.
+__device__ __forceinline__ double set_rhs_node(const LevelDev<double>& L, const double* __restrict__ bcL,
+                                               const double* __restrict__ bcR, const double* __restrict__ bcT,
+                                               const double* __restrict__ bcB, long node) {
+  const int Ny = L.Ny, Nz = L.Nz;
+  const int iy = (int)(node / Nz), iz = (int)(node % Nz);
+  double sy = 0.0, sz = 0.0;
+  if (L.y.bc_lo == 0) {
+    if (iy < BAND) sy += (L.y.bs0[iy] + (iy == 0 ? L.y.alphaD : 0.0)) * L.cy[iz] * bcL[iz];
+  } else if (iy == 0) {
+    sy += bcL[iz];
+  }
+  if (L.y.bc_hi == 0) {
+    if (iy >= Ny - BAND)
+      sy += (L.y.bsN[iy - (Ny - BAND)] + (iy == Ny - 1 ? L.y.alphaD : 0.0)) * L.cy[(long)(Ny - 1) * Nz + iz] * bcR[iz];
+  } else if (iy == Ny - 1) {
+    sy -= bcR[iz];
+  }
+  if (L.z.bc_lo == 0) {
+    if (iz < BAND) sz += (L.z.bs0[iz] + (iz == 0 ? L.z.alphaD : 0.0)) * L.cz[(long)iy * Nz] * bcT[iy];
+  } else if (iz == 0) {
+    sz += bcT[iy];
+  }
+  if (L.z.bc_hi == 0) {
+    if (iz >= Nz - BAND)
+      sz += (L.z.bsN[iz - (Nz - BAND)] + (iz == Nz - 1 ? L.z.alphaD : 0.0)) * L.cz[(long)iy * Nz + Nz - 1] * bcB[iy];
+  } else if (iz == Nz - 1) {
+    sz -= bcB[iy];
+  }
+  return L.wy[node] * sy + L.wz[node] * sz;
+}
+
+// Shear stress mu * Dy u on the fault row iy = 0 at column iz (muxDy of
+// sbpOps_m_constGrid.cpp:1481-1500 scattered to the fault,
+// strikeSlip_linearElastic_qd.cpp:785-788): Dy row 0 reaches columns 0..4.
+__device__ __forceinline__ double fault_row_sxy(const LevelDev<double>& L, const double* __restrict__ u, int iz) {
+  const int Nz = L.Nz;
+  double d = 0.0;
+#pragma unroll
+  for (int j = HALF; j < BAND; ++j) {
+    int k = j - HALF;
+    if (k < L.Ny) d += L.y.D[j] * u[(long)k * Nz + iz];
+  }
+  if (L.var) d *= L.qy[iz];
+  return L.mu[iz] * d;
+}
+
 template <typename T, class Loader, class Epi>
 __global__ void __launch_bounds__(256) stencil_kernel(LevelDev<T> L, Loader ld, Epi ep, double* partials,
                                                       unsigned int* counter, double* red_out) {

@@ -35,6 +35,7 @@ const char* last_error() { return g_err; }
 
 static std::atomic<long long> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void count_launches(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 long long launch_count() { return g_launches.load(); }
 
 // Optional per-launch timing of the stencil kernel (CUDA events around each
@@ -823,35 +824,9 @@ __global__ void hmul_kernel(LevelDev<double> L, const double* __restrict__ in, d
 __global__ void set_rhs_kernel(LevelDev<double> L, const double* __restrict__ bcL, const double* __restrict__ bcR,
                                const double* __restrict__ bcT, const double* __restrict__ bcB,
                                double* __restrict__ rhs) {
-  const int Ny = L.Ny, Nz = L.Nz;
-  long n = (long)Ny * Nz;
-  for (long node = blockIdx.x * (long)blockDim.x + threadIdx.x; node < n; node += (long)gridDim.x * blockDim.x) {
-    int iy = (int)(node / Nz), iz = (int)(node % Nz);
-    double sy = 0.0, sz = 0.0;
-    if (L.y.bc_lo == 0) {
-      if (iy < BAND) sy += (L.y.bs0[iy] + (iy == 0 ? L.y.alphaD : 0.0)) * L.cy[iz] * bcL[iz];
-    } else if (iy == 0) {
-      sy += bcL[iz];
-    }
-    if (L.y.bc_hi == 0) {
-      if (iy >= Ny - BAND)
-        sy += (L.y.bsN[iy - (Ny - BAND)] + (iy == Ny - 1 ? L.y.alphaD : 0.0)) * L.cy[(long)(Ny - 1) * Nz + iz] * bcR[iz];
-    } else if (iy == Ny - 1) {
-      sy -= bcR[iz];
-    }
-    if (L.z.bc_lo == 0) {
-      if (iz < BAND) sz += (L.z.bs0[iz] + (iz == 0 ? L.z.alphaD : 0.0)) * L.cz[(long)iy * Nz] * bcT[iy];
-    } else if (iz == 0) {
-      sz += bcT[iy];
-    }
-    if (L.z.bc_hi == 0) {
-      if (iz >= Nz - BAND)
-        sz += (L.z.bsN[iz - (Nz - BAND)] + (iz == Nz - 1 ? L.z.alphaD : 0.0)) * L.cz[(long)iy * Nz + Nz - 1] * bcB[iy];
-    } else if (iz == Nz - 1) {
-      sz -= bcB[iy];
-    }
-    rhs[node] = L.wy[node] * sy + L.wz[node] * sz;
-  }
+  long n = (long)L.Ny * L.Nz;
+  for (long node = blockIdx.x * (long)blockDim.x + threadIdx.x; node < n; node += (long)gridDim.x * blockDim.x)
+    rhs[node] = set_rhs_node(L, bcL, bcR, bcT, bcB, node);
 }
 
 // ------------------------------------------------------------------------

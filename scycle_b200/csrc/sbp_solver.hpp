@@ -112,7 +112,7 @@ struct SbpContext {
   std::unique_ptr<LevelStore<double>> fine;
   std::unique_ptr<Multigrid<double>> mg64;
   std::unique_ptr<Multigrid<float>> mg32;
-  std::unique_ptr<FDPrecond> fd;
+  std::shared_ptr<FDPrecond> fd;  // shared by the instances of a batch with one operator
   int separable = 0;  // metrics and mu separable: fast diagonalisation is exact up to the mu3 column
   Reducer red;
   DevBuf scal;
