@@ -177,6 +177,11 @@ scy_status scy_sbp_info(scy_sbp* s, int* Ny, int* Nz, int* n_levels);
  * machine.  in/out are host arrays of length Ny*Nz.  The solver never uses
  * it on the hot path. */
 scy_status scy_grid_host_apply(const scy_grid_desc* desc, const double* in, double* out);
+/* Host reference of the operator in the per-node form the batched ensemble
+ * applies (A as a 33-point cross stencil per node: every column's y
+ * operator and every row's z operator composed with that line's
+ * coefficients and SAT terms).  Same arguments as scy_grid_host_apply. */
+scy_status scy_grid_host_apply_cross(const scy_grid_desc* desc, const double* in, double* out);
 
 /* ------------------------------------------------------------------------
  * Fault_qd + StrikeSlip_LinearElastic_qd (linear-elastic quasi-dynamic).
@@ -503,6 +508,8 @@ typedef struct scy_batch_opts {
   int graphs;     /* 1: one CUDA graph launch per round (default); 0: the same launches issued directly */
   int concurrent; /* 1: groups on concurrent streams (default); 0: one stream */
   int exact_jacobian; /* root-finder derivative of every instance (see scy_qd_set_jacobian) */
+  int fd_dense;   /* 1: the preconditioner as four GEMMs (y and z transforms) even where the y part
+                     is banded; 0 (default): z transform GEMMs and banded Cholesky solves along y */
 } scy_batch_opts;
 typedef struct scy_batch_stats {
   long rounds;          /* rounds of batched attempts so far */

@@ -70,6 +70,7 @@ def lib():
         L.scy_sbp_solve_noalloc.argtypes = [vp, vp, vp, C.POINTER(SolveOpts), C.POINTER(SolveStats)]
         L.scy_sbp_info.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.scy_grid_host_apply.argtypes = [C.POINTER(GridDesc), dptr, dptr]
+        L.scy_grid_host_apply_cross.argtypes = [C.POINTER(GridDesc), dptr, dptr]
         L.scy_launch_count.restype = C.c_longlong
         L.scy_profile_enable.argtypes = [C.c_int]
         L.scy_profile_collect.argtypes = [C.c_int, C.c_int, dptr, C.POINTER(C.c_longlong), dptr]
@@ -118,8 +119,11 @@ def grid_desc(order, Ny, Nz, Ly, Lz, mu, grid="constantGridSpacing", y=None, z=N
     return d, keep
 
 
-def host_apply(desc, x):
+def host_apply(desc, x, form="stages"):
+    """A x on the host: the two-stage form of the device stencil ("stages")
+    or the per-node cross-stencil form of the batched ensemble ("cross")."""
     x = np.ascontiguousarray(x, dtype=np.float64)
     out = np.zeros_like(x)
-    check(lib().scy_grid_host_apply(C.byref(desc), as_dptr(x), as_dptr(out)))
+    f = lib().scy_grid_host_apply if form == "stages" else lib().scy_grid_host_apply_cross
+    check(f(C.byref(desc), as_dptr(x), as_dptr(out)))
     return out

@@ -85,31 +85,6 @@ __global__ void b_rhs_kernel(LevelDev<double> L, const BatchInst* __restrict__ t
   grid_reduce_finish(s, w.partials + (long)k * w.PB, w.counters + 4 * k, w.sc + 16 * k + 0, sh);
 }
 
-// r = -rhs + A u (0 when rhs = 0, whose solution is u = 0); r.r -> sc[5]
-struct EpiBatchResidual {
-  const double* b;
-  double* r;
-  float* r32;
-  bool zero;
-  static constexpr bool kReduce = true;
-  __device__ __forceinline__ double operator()(long node, int, int, double Ax, double) const {
-    double v = zero ? 0.0 : -1.0 * b[node] + Ax;
-    r[node] = v;
-    if (r32) r32[node] = (float)v;
-    return v * v;
-  }
-};
-
-__global__ void __launch_bounds__(256) b_residual_kernel(LevelDev<double> L, const BatchInst* __restrict__ tab,
-                                                         const int* __restrict__ mask, BatchWork w, int mixed) {
-  const int k = blockIdx.z;
-  if (!mask[k]) return;
-  const long off = (long)k * w.N;
-  double* sc = w.sc + 16 * k;
-  EpiBatchResidual ep{tab[k].rhs, w.r + off, mixed ? w.r32 + off : nullptr, sc[0] == 0.0};
-  stencil_tile<double>(L, LoadPlain<double>{tab[k].u}, ep, w.partials + (long)k * w.PB, w.counters + 4 * k, sc + 5);
-}
-
 // rz = r.z -> sc[2] (the previous value moves to sc[3])
 template <typename Tz>
 __global__ void b_dot_rz_kernel(const int* __restrict__ mask, BatchWork w, const Tz* __restrict__ z) {
@@ -145,18 +120,127 @@ __global__ void b_dot_rz_kernel(const int* __restrict__ mask, BatchWork w, const
   }
 }
 
-// p_new = z + beta p_old ; q = -A p_new ; p.q -> sc[4]
-template <typename Tz>
-__global__ void __launch_bounds__(256) b_matvec_kernel(LevelDev<double> L, const int* __restrict__ mask, BatchWork w,
-                                                       const Tz* __restrict__ z, int first, int pi) {
-  const int k = blockIdx.z;
+// A applied in its per-node cross form (33 coefficient planes shared by
+// the group, see build_cross_planes): a block owns one 8 x 32 tile of
+// nodes, keeps its nodes' coefficients in registers and applies them to
+// kpb instances in turn, staging each instance's operand (tile plus an
+// 8-node halo in y and in z) in shared memory.
+//   MODE 0: r = -rhs + A u (0 where rhs = 0), r.r -> sc[5]
+//   MODE 1: p = z + beta p_old (beta = rz / rz_old; p = z on the first
+//           iteration), q = -A p, p stored, p.q -> sc[4]
+constexpr int XTY = 8, XTZ = 32, XH = 8;
+
+template <int MODE, typename Tz>
+__global__ void __launch_bounds__(256) b_cross_kernel(const double* __restrict__ C, int Ny, int Nz,
+                                                      const BatchInst* __restrict__ tab, const int* __restrict__ mask,
+                                                      BatchWork w, const Tz* __restrict__ zv, int first, int pi,
+                                                      int mixed, int kpb) {
+  constexpr int NY = (XTY + 2 * XH) * XTZ, NZ = XTY * (XTZ + 2 * XH);
+  constexpr int PY = (NY + 255) / 256, PZ = (NZ + 255) / 256;  // staged values per thread
+  __shared__ double xy[NY];
+  __shared__ double xz[NZ];
+  __shared__ double red[32];
+  const long N = (long)Ny * Nz;
+  const int tid = threadIdx.x, ty = tid / XTZ, tz = tid % XTZ;
+  const int y0 = blockIdx.y * XTY, z0 = blockIdx.x * XTZ;
+  const int iy = y0 + ty, iz = z0 + tz;
+  const bool valid = iy < Ny && iz < Nz;
+  const long node = (long)iy * Nz + iz;
+  const int tile = blockIdx.x + gridDim.x * blockIdx.y;
+  double c[33];
+#pragma unroll
+  for (int o = 0; o < 33; ++o) c[o] = valid ? C[(long)o * N + node] : 0.0;
+  const int kb = blockIdx.z * kpb, ke = min(w.K, kb + kpb);
+  // the operand of instance k at the staged positions, into registers
+  double vy[PY], vz[PZ];
+  auto fetch = [&](int k) {
+    const long off = (long)k * N;
+    const double* xsrc = tab[k].u;
+    const Tz* zsrc = zv + off;
+    const double* pold = (pi ? w.p1 : w.p0) + off;
+    double beta = 0.0;
+    if (MODE == 1 && !first) {
+      const double ro = w.sc[16 * k + 3];
+      beta = ro != 0.0 ? w.sc[16 * k + 2] / ro : 0.0;
+    }
+    auto ld = [&](long n) -> double {
+      if (MODE == 0) return xsrc[n];
+      const double zz = (double)zsrc[n];
+      return first ? zz : zz + beta * pold[n];
+    };
+#pragma unroll
+    for (int a = 0; a < PY; ++a) {
+      const int i = tid + 256 * a;
+      const int r = i / XTZ, cc = i % XTZ;
+      const int jy = y0 - XH + r, jz = z0 + cc;
+      vy[a] = (i < NY && jy >= 0 && jy < Ny && jz < Nz) ? ld((long)jy * Nz + jz) : 0.0;
+    }
+#pragma unroll
+    for (int a = 0; a < PZ; ++a) {
+      const int i = tid + 256 * a;
+      const int r = i / (XTZ + 2 * XH), cc = i % (XTZ + 2 * XH);
+      const int jy = y0 + r, jz = z0 - XH + cc;
+      vz[a] = (i < NZ && jy < Ny && jz >= 0 && jz < Nz) ? ld((long)jy * Nz + jz) : 0.0;
+    }
+  };
+  auto next_active = [&](int k) {
+    while (k < ke && !mask[k]) ++k;
+    return k;
+  };
+  int k = next_active(kb);
+  if (k < ke) fetch(k);
+  while (k < ke) {
+#pragma unroll
+    for (int a = 0; a < PY; ++a)
+      if (tid + 256 * a < NY) xy[tid + 256 * a] = vy[a];
+#pragma unroll
+    for (int a = 0; a < PZ; ++a)
+      if (tid + 256 * a < NZ) xz[tid + 256 * a] = vz[a];
+    __syncthreads();
+    const int kn = next_active(k + 1);
+    if (kn < ke) fetch(kn);  // in flight while this instance is computed
+    const long off = (long)k * N;
+    double contrib = 0.0;
+    if (valid) {
+      const double* ay = xy + ty * XTZ + tz;             // row iy - 8
+      const double* az = xz + ty * (XTZ + 2 * XH) + tz;  // column iz - 8
+      double Ax = 0.0;
+#pragma unroll
+      for (int o = 0; o < 17; ++o) Ax += c[o] * ay[o * XTZ];
+#pragma unroll
+      for (int o = 0; o < 8; ++o) Ax += c[17 + o] * az[o];
+#pragma unroll
+      for (int o = 9; o < 17; ++o) Ax += c[16 + o] * az[o];
+      if (MODE == 0) {
+        const double v = w.sc[16 * k] == 0.0 ? 0.0 : -1.0 * tab[k].rhs[node] + Ax;
+        w.r[off + node] = v;
+        if (mixed) w.r32[off + node] = (float)v;
+        contrib = v * v;
+      } else {
+        const double p = ay[XH * XTZ];
+        const double qv = -Ax;
+        (pi ? w.p0 : w.p1)[off + node] = p;
+        w.q[off + node] = qv;
+        contrib = p * qv;
+      }
+    }
+    // block partial of this instance; b_partials_kernel adds the tiles up
+    const double tot = block_sum(contrib, red);
+    if (tid == 0) w.partials[(long)k * w.PB + tile] = tot;
+    k = kn;
+  }
+}
+
+// sc[16 k + slot] = sum of the instance's first n partials, in tile order
+__global__ void b_partials_kernel(const int* __restrict__ mask, BatchWork w, int n, int slot) {
+  __shared__ double sh[32];
+  const int k = blockIdx.x;
   if (!mask[k]) return;
-  const long off = (long)k * w.N;
-  double* sc = w.sc + 16 * k;
-  double* pold = (pi ? w.p1 : w.p0) + off;
-  double* pnew = (pi ? w.p0 : w.p1) + off;
-  LoadPUpdate<Tz> lp{z + off, pold, sc + 2, sc + 3, first};
-  stencil_tile<double>(L, lp, EpiCGMatvec{pnew, w.q + off}, w.partials + (long)k * w.PB, w.counters + 4 * k, sc + 4);
+  const double* p = w.partials + (long)k * w.PB;
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) acc += p[i];
+  acc = block_sum(acc, sh);
+  if (threadIdx.x == 0) w.sc[16 * k + slot] = acc;
 }
 
 // u += alpha p ; r -= alpha q ; r.r -> sc[1]   (alpha = rz / pq)
@@ -204,6 +288,99 @@ __global__ void b_scale_kernel(T* __restrict__ x, const T* __restrict__ s, long 
   const long off = (long)blockIdx.z * N;
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x)
     x[off + i] *= s[i];
+}
+
+// After the z transform: for every z mode j and instance k, the banded
+// solve (Ky + lz_j My) x = t along y with the Cholesky factor (forward and
+// back substitution), in place.  t is the Nz x Ny*K column-major matrix of
+// the transform, so consecutive threads (consecutive j) touch consecutive
+// addresses; the last eight values of the sweep stay in registers.
+template <typename T, int R>
+__global__ void __launch_bounds__(128) b_ysolve_kernel(const T* __restrict__ Lb, T* __restrict__ t, int Ny, int Nz,
+                                                       int K) {
+  // A thread sweeps the systems of one z mode j for R instances at once:
+  // every factor coefficient is loaded once for the R sweeps, and the rows
+  // are taken RB at a time (their loads issued together, so one memory
+  // latency covers RB steps of the R sweeps).
+  constexpr int RB = 4;
+  const int KR = (K + R - 1) / R;
+  const long g = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (g >= (long)Nz * KR) return;
+  const int j = (int)(g % Nz), k0 = (int)(g / Nz) * R;
+  const long NN = (long)Ny * Nz;
+  T* col = t + (long)k0 * NN + j;
+  const int nr = min(R, K - k0);
+  const T* L = Lb + j;
+  T w[R][8];
+#pragma unroll
+  for (int q = 0; q < R; ++q)
+#pragma unroll
+    for (int m = 0; m < 8; ++m) w[q][m] = T(0);
+  // forward: y(i) = (b(i) - sum_m L(i, i-m) y(i-m)) / L(i, i); w[q][m-1] = y(i-m)
+  for (int i0 = 0; i0 < Ny; i0 += RB) {
+    T cf[RB][9], bv[RB][R];
+#pragma unroll
+    for (int r = 0; r < RB; ++r) {
+      const int i = i0 + r;
+      const T* row = L + (long)i * 9 * Nz;  // rows up to Ny + 7 exist (zero padded)
+#pragma unroll
+      for (int m = 0; m < 9; ++m) cf[r][m] = row[(long)m * Nz];
+#pragma unroll
+      for (int q = 0; q < R; ++q) bv[r][q] = (i < Ny && q < nr) ? col[q * NN + (long)i * Nz] : T(0);
+    }
+#pragma unroll
+    for (int r = 0; r < RB; ++r) {
+      const int i = i0 + r;
+      if (i < Ny) {
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+          T s = bv[r][q];
+#pragma unroll
+          for (int m = 8; m >= 1; --m) s -= cf[r][m] * w[q][m - 1];
+          const T y = s * cf[r][0];
+          if (q < nr) col[q * NN + (long)i * Nz] = y;
+#pragma unroll
+          for (int m = 7; m >= 1; --m) w[q][m] = w[q][m - 1];
+          w[q][0] = y;
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < R; ++q)
+#pragma unroll
+    for (int m = 0; m < 8; ++m) w[q][m] = T(0);
+  // back: x(i) = (y(i) - sum_m L(i+m, i) x(i+m)) / L(i, i); w[q][m-1] = x(i+m)
+  for (int i0 = Ny - 1; i0 >= 0; i0 -= RB) {
+    T cf[RB][9], bv[RB][R];
+#pragma unroll
+    for (int r = 0; r < RB; ++r) {
+      const int i = i0 - r;
+      const bool in = i >= 0;
+      cf[r][0] = in ? L[(long)i * 9 * Nz] : T(0);
+#pragma unroll
+      for (int m = 1; m <= 8; ++m) cf[r][m] = in ? L[((long)(i + m) * 9 + m) * Nz] : T(0);
+#pragma unroll
+      for (int q = 0; q < R; ++q) bv[r][q] = (in && q < nr) ? col[q * NN + (long)i * Nz] : T(0);
+    }
+#pragma unroll
+    for (int r = 0; r < RB; ++r) {
+      const int i = i0 - r;
+      if (i >= 0) {
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+          T s = bv[r][q];
+#pragma unroll
+          for (int m = 8; m >= 1; --m) s -= cf[r][m] * w[q][m - 1];
+          const T x = s * cf[r][0];
+          if (q < nr) col[q * NN + (long)i * Nz] = x;
+#pragma unroll
+          for (int m = 7; m >= 1; --m) w[q][m] = w[q][m - 1];
+          w[q][0] = x;
+        }
+      }
+    }
+  }
 }
 
 // Fault_qd::d_dt with tauQS = mu Dy u on the fault row (linear elastic) or
@@ -381,6 +558,7 @@ int BatchContext::create(int n_inst, const char* const* paths, const scy_solve_o
     its = o->cg_its;
     graphs = o->graphs;
     concurrent = o->concurrent;
+    fd_dense = o->fd_dense;
   }
   if (precision != SCY_PREC_FP64 && precision != SCY_PREC_MIXED && precision != SCY_PREC_TF32) {
     set_error("unknown batch precision %d", precision);
@@ -494,8 +672,17 @@ int BatchContext::setup_group(int base, int K) {
     SCY_TRY(v.alloc((size_t)KN * 4));
     SCY_CUDA_TRY(cudaMemset(v.p, 0, (size_t)KN * 4));
   }
-  const int tiles = ((g.Nz + TZ - 1) / TZ) * ((g.Ny + TY - 1) / TY);
+  const int tiles = ((g.Nz + XTZ - 1) / XTZ) * ((g.Ny + XTY - 1) / XTY);
   g.w.PB = std::max(tiles, node_blocks(g.N));
+  // instances per block of the operator kernels: enough blocks for about
+  // four per SM, at most eight instances each
+  g.kpb = (int)std::max(1L, std::min(8L, (long)g.K * tiles / (148L * 4)));
+  {
+    std::vector<double> planes;
+    build_cross_planes(q0.sbp.hosts[0], planes);
+    SCY_TRY(g.planes.alloc(planes.size() * sizeof(double)));
+    SCY_CUDA_TRY(cudaMemcpy(g.planes.p, planes.data(), planes.size() * sizeof(double), cudaMemcpyHostToDevice));
+  }
   SCY_TRY(g.sc.alloc((size_t)g.K * 16 * 8));
   SCY_CUDA_TRY(cudaMemset(g.sc.p, 0, (size_t)g.K * 16 * 8));
   SCY_TRY(g.partials.alloc((size_t)g.K * g.w.PB * 8));
@@ -583,6 +770,37 @@ int BatchContext::fd_apply(BatchGroup& g) {
   const long N = g.N;
   SCY_BLAS_TRY(cublasSetStream(g.blas, g.stream));
   dim3 sg(node_blocks(N), 1, K);
+  if (F.ybanded && !fd_dense) {
+    // Z = Vz [ per z mode: (Ky + lz_j My)^-1 along y ] (Vz^T R)
+    // instances per thread in the banded sweeps (register budget: 4 in FP32, 2 in FP64)
+    const int R = precision != SCY_PREC_FP64 ? 4 : 2;
+    const int nb = (int)(((long)Nz * ((K + R - 1) / R) + 127) / 128);
+    if (precision != SCY_PREC_FP64) {
+      SCY_BLAS_TRY(cublasSetMathMode(g.blas, precision == SCY_PREC_TF32 ? CUBLAS_TF32_TENSOR_OP_MATH
+                                                                       : CUBLAS_DEFAULT_MATH));
+      const float one = 1.0f, zero = 0.0f;
+      const float* vz = F.Vz32.as<float>();
+      SCY_BLAS_TRY(cublasSgemm(g.blas, CUBLAS_OP_T, CUBLAS_OP_N, Nz, Ny * K, Nz, &one, vz, Nz, g.w.r32, Nz, &zero,
+                               g.w.t1f, Nz));
+      b_ysolve_kernel<float, 4><<<nb, 128, 0, g.stream>>>(F.Lb32.as<float>(), g.w.t1f, Ny, Nz, K);
+      SCY_LAUNCH_CHECK();
+      SCY_BLAS_TRY(cublasSgemm(g.blas, CUBLAS_OP_N, CUBLAS_OP_N, Nz, Ny * K, Nz, &one, vz, Nz, g.w.t1f, Nz, &zero,
+                               g.w.z32, Nz));
+    } else {
+      SCY_BLAS_TRY(cublasSetMathMode(g.blas, CUBLAS_DEFAULT_MATH));
+      const double one = 1.0, zero = 0.0;
+      const double* vz = F.Vz.as<double>();
+      SCY_BLAS_TRY(cublasDgemm(g.blas, CUBLAS_OP_T, CUBLAS_OP_N, Nz, Ny * K, Nz, &one, vz, Nz, g.w.r, Nz, &zero,
+                               g.w.t1, Nz));
+      b_ysolve_kernel<double, 2><<<nb, 128, 0, g.stream>>>(F.Lb.as<double>(), g.w.t1, Ny, Nz, K);
+      SCY_LAUNCH_CHECK();
+      SCY_BLAS_TRY(cublasDgemm(g.blas, CUBLAS_OP_N, CUBLAS_OP_N, Nz, Ny * K, Nz, &one, vz, Nz, g.w.t1, Nz, &zero,
+                               g.w.z, Nz));
+    }
+    count_launch();
+    count_launch();
+    return SCY_OK;
+  }
   if (precision != SCY_PREC_FP64) {
     SCY_BLAS_TRY(cublasSetMathMode(g.blas, precision == SCY_PREC_TF32 ? CUBLAS_TF32_TENSOR_OP_MATH
                                                                      : CUBLAS_DEFAULT_MATH));
@@ -621,10 +839,14 @@ int BatchContext::fd_apply(BatchGroup& g) {
 
 int BatchContext::solve(BatchGroup& g, const int* mask, int its_now) {
   const int mixed = precision != SCY_PREC_FP64 ? 1 : 0;
-  const dim3 tg((g.Nz + TZ - 1) / TZ, (g.Ny + TY - 1) / TY, g.K);
+  const dim3 tg((g.Nz + XTZ - 1) / XTZ, (g.Ny + XTY - 1) / XTY, (g.K + g.kpb - 1) / g.kpb);
   const dim3 ng(node_blocks(g.N), 1, g.K);
   const BatchInst* tab = g.tab.as<BatchInst>();
-  b_residual_kernel<<<tg, 256, 0, g.stream>>>(g.L, tab, mask, g.w, mixed);
+  const double* C = g.planes.as<double>();
+  const int ntiles = (int)(tg.x * tg.y);
+  b_cross_kernel<0, double><<<tg, 256, 0, g.stream>>>(C, g.Ny, g.Nz, tab, mask, g.w, nullptr, 0, 0, mixed, g.kpb);
+  SCY_LAUNCH_CHECK();
+  b_partials_kernel<<<g.K, 256, 0, g.stream>>>(mask, g.w, ntiles, 5);
   SCY_LAUNCH_CHECK();
   int pi = 0;
   for (int it = 1; it <= its_now; ++it) {
@@ -632,12 +854,16 @@ int BatchContext::solve(BatchGroup& g, const int* mask, int its_now) {
     if (mixed) {
       b_dot_rz_kernel<float><<<ng, TB, 0, g.stream>>>(mask, g.w, g.w.z32);
       SCY_LAUNCH_CHECK();
-      b_matvec_kernel<float><<<tg, 256, 0, g.stream>>>(g.L, mask, g.w, g.w.z32, it == 1 ? 1 : 0, pi);
+      b_cross_kernel<1, float><<<tg, 256, 0, g.stream>>>(C, g.Ny, g.Nz, tab, mask, g.w, g.w.z32, it == 1 ? 1 : 0,
+                                                          pi, mixed, g.kpb);
     } else {
       b_dot_rz_kernel<double><<<ng, TB, 0, g.stream>>>(mask, g.w, g.w.z);
       SCY_LAUNCH_CHECK();
-      b_matvec_kernel<double><<<tg, 256, 0, g.stream>>>(g.L, mask, g.w, g.w.z, it == 1 ? 1 : 0, pi);
+      b_cross_kernel<1, double><<<tg, 256, 0, g.stream>>>(C, g.Ny, g.Nz, tab, mask, g.w, g.w.z, it == 1 ? 1 : 0,
+                                                           pi, mixed, g.kpb);
     }
+    SCY_LAUNCH_CHECK();
+    b_partials_kernel<<<g.K, 256, 0, g.stream>>>(mask, g.w, ntiles, 4);
     SCY_LAUNCH_CHECK();
     b_update_kernel<<<ng, TB, 0, g.stream>>>(tab, mask, g.w, pi, mixed);
     SCY_LAUNCH_CHECK();

@@ -59,7 +59,9 @@ struct BatchGroup {
   long N = 0;
   LevelDev<double> L{};
   std::shared_ptr<FDPrecond> fd;
-  DevBuf tab;  // BatchInst[K]
+  DevBuf tab;     // BatchInst[K]
+  DevBuf planes;  // the operator's 33 cross-stencil coefficient planes (build_cross_planes)
+  int kpb = 1;    // instances per block of the operator kernels
   DevBuf vec[7], vecf[4], sc, partials, counters, status;
   BatchWork w{};
   cudaStream_t stream = nullptr;
@@ -74,7 +76,7 @@ struct BatchContext {
   std::vector<int> group_of;  // by the caller's numbering
   std::vector<int> slot_of, user_of;
   std::vector<std::unique_ptr<BatchGroup>> groups;
-  int n = 0, pl = 0, method = 0, precision = 0, its = 1, graphs = 1, concurrent = 1;
+  int n = 0, pl = 0, method = 0, precision = 0, its = 1, graphs = 1, concurrent = 1, fd_dense = 0;
   double rtol = 1e-12, atol = 0.0;
   int max_its = 300;
   cudaStream_t stream = nullptr;

@@ -170,6 +170,30 @@ scy_status scy_grid_host_apply(const scy_grid_desc* g, const double* in, double*
   return SCY_OK;
 }
 
+scy_status scy_grid_host_apply_cross(const scy_grid_desc* g, const double* in, double* out) {
+  if (!g || !in || !out || !g->mu) {
+    scy::set_error("scy_grid_host_apply_cross: NULL argument");
+    return SCY_ERR_ARG;
+  }
+  try {
+    const size_t N = (size_t)g->Ny * g->Nz;
+    std::vector<double> y, z, mu(g->mu, g->mu + N);
+    if (g->grid_type == SCY_GRID_VAR) {
+      if (g->y) y.assign(g->y, g->y + N);
+      if (g->z) z.assign(g->z, g->z + N);
+    }
+    int bc[4] = {g->bcR, g->bcT, g->bcL, g->bcB};
+    scy::LevelHost L = scy::build_level(g->order, g->Ny, g->Nz, g->Ly, g->Lz, g->grid_type, g->compat, y, z, mu, bc);
+    std::vector<double> C;
+    scy::build_cross_planes(L, C);
+    scy::apply_cross_planes(C, g->Ny, g->Nz, in, out);
+  } catch (const std::exception& e) {
+    scy::set_error("scy_grid_host_apply_cross: %s", e.what());
+    return SCY_ERR_ARG;
+  }
+  return SCY_OK;
+}
+
 scy_status scy_qd_create(const scy_qd_desc* d, scy_qd** out) {
   if (!d || !out) {
     scy::set_error("scy_qd_create: NULL argument");

@@ -1,7 +1,9 @@
 // Fast-diagonalisation preconditioner (see fdiag.hpp).
 #include <cusolverDn.h>
 
+#include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <vector>
 
 #include "common.cuh"
@@ -185,6 +187,54 @@ int FDPrecond::build(const LevelHost& L, cudaStream_t s) {
       }
       il[(size_t)iy * Nz + iz] = 1.0 / d;
     }
+  // banded Cholesky factors of Ky + lz_j My, Ky = (Ly + Ly^T) / 2
+  {
+    const int bw = 8;
+    bool banded = true;
+    auto ks = [&](int i, int l) { return 0.5 * (Ly[(size_t)l * Ny + i] + Ly[(size_t)i * Ny + l]); };
+    for (int l = 0; l < Ny && banded; ++l)
+      for (int i = 0; i < Ny; ++i)
+        if (std::abs(i - l) > bw && ks(i, l) != 0.0) {
+          banded = false;
+          break;
+        }
+    if (banded) {
+      std::vector<double> Lbh((size_t)(Ny + bw) * 9 * Nz, 0.0);
+      std::vector<double> c((size_t)Ny * (bw + 1));  // c[i*(bw+1) + k] = L(i, i-k)
+      bool spd = true;
+      for (int j = 0; j < Nz && spd; ++j) {
+        for (int i = 0; i < Ny && spd; ++i)
+          for (int col = std::max(0, i - bw); col <= i; ++col) {
+            double sum = ks(i, col) + (i == col ? lz[j] * My[i] : 0.0);
+            for (int p = std::max(0, i - bw); p < col; ++p) {
+              if (col - p > bw) continue;
+              sum -= c[(size_t)i * (bw + 1) + (i - p)] * c[(size_t)col * (bw + 1) + (col - p)];
+            }
+            if (col == i) {
+              if (!(sum > 0)) {
+                spd = false;
+                break;
+              }
+              c[(size_t)i * (bw + 1)] = std::sqrt(sum);
+            } else {
+              c[(size_t)i * (bw + 1) + (i - col)] = sum / c[(size_t)col * (bw + 1)];
+            }
+          }
+        for (int i = 0; i < Ny && spd; ++i)
+          for (int k = 0; k <= bw; ++k) {
+            double v = c[(size_t)i * (bw + 1) + k];
+            if (k == 0) v = 1.0 / v;
+            if (i - k < 0 && k > 0) v = 0.0;
+            Lbh[((size_t)i * 9 + k) * Nz + j] = v;
+          }
+      }
+      if (spd) {
+        SCY_TRY(upload_as<double>(Lb, Lbh, s));
+        SCY_TRY(upload_as<float>(Lb32, Lbh, s));
+        ybanded = 1;
+      }
+    }
+  }
   SCY_TRY(upload_as<double>(Vy, Vyh, s));
   SCY_TRY(upload_as<double>(Vz, Vzh, s));
   SCY_TRY(upload_as<double>(inv_lam, il, s));

@@ -24,6 +24,14 @@ struct FDPrecond {
   DevBuf Vy, Vz, inv_lam, t1, t2;          // FP64
   DevBuf Vy32, Vz32, inv_lam32, t1f, t2f;  // FP32 copies for the mixed path
   DevBuf r32;                              // FP32 copy of the residual
+  // Banded form of the y part (ybanded = 1 when the symmetric part of the y
+  // line operator has half-bandwidth <= 8): after the z transform the
+  // operator splits into one banded SPD system per z mode j,
+  // Ky + lz_j My, solved with its Cholesky factor L_j.  Layout
+  // [(iy * 9 + k) * Nz + j] = L_j(iy, iy - k) for k = 1..8 and 1 / L_j(iy, iy)
+  // for k = 0, with 8 zero rows after the last (Ny + 8 rows in all).
+  int ybanded = 0;
+  DevBuf Lb, Lb32;
   ~FDPrecond();
   int build(const LevelHost& L, cudaStream_t s);
   // z = K_sep^-1 r (FP64)

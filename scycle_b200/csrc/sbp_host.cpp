@@ -479,4 +479,102 @@ Interp1D make_interp(int nf, int nc) {
   return I;
 }
 
+// One direction of A composed into 17-point rows: stage 2 (Q, R3^T, R4^T)
+// applied to stage 1 (c D, w3 m3 R3, w4 c R4) over the band tables, plus the
+// SAT terms the stencil adds at the ends (Dirichlet: (BS row + alphaD) * c *
+// x(end); Neumann: +/- c D x at the end row).  C[i*17 + o+8] multiplies
+// x(i+o); bc_lo / bc_hi: 0 Dirichlet, 1 Neumann.
+void compose_line(const DirTables& t, int bc_lo, int bc_hi, const std::vector<double>& c1,
+                         const std::vector<double>& m31, std::vector<double>& C) {
+  const int n = t.n;
+  C.assign((size_t)n * 17, 0.0);
+  const bool r4 = t.nterms == 3;
+  for (int i = 0; i < n; ++i) {
+    double* row = &C[(size_t)i * 17];
+    for (int a = 0; a < kBand; ++a) {
+      const int k = i + a - kHalf;
+      if (k < 0 || k >= n) continue;
+      const double q = t.Q[(size_t)i * kBand + a], q3 = t.R3T[(size_t)i * kBand + a];
+      const double q4 = r4 ? t.R4T[(size_t)i * kBand + a] : 0.0;
+      for (int b = 0; b < kBand; ++b) {
+        const int j = k + b - kHalf;
+        if (j < 0 || j >= n) continue;
+        double v = q * (c1[k] * t.D[(size_t)k * kBand + b]);
+        v -= q3 * (t.w3[k] * m31[k] * t.R3[(size_t)k * kBand + b]);
+        if (r4) v -= q4 * (t.w4[k] * c1[k] * t.R4[(size_t)k * kBand + b]);
+        row[j - i + 8] += v;
+      }
+    }
+    if (bc_lo == 0) {
+      if (i < kBand) row[0 - i + 8] += (t.bs0[i] + (i == 0 ? t.alphaD : 0.0)) * c1[0];
+    } else if (i == 0) {
+      for (int b = kHalf; b < kBand; ++b) row[b - kHalf + 8] += c1[0] * t.D[b];
+    }
+    if (bc_hi == 0) {
+      if (i >= n - kBand) row[(n - 1) - i + 8] += (t.bsN[i - (n - kBand)] + (i == n - 1 ? t.alphaD : 0.0)) * c1[n - 1];
+    } else if (i == n - 1) {
+      for (int b = 0; b <= kHalf; ++b) row[b - kHalf + 8] -= c1[n - 1] * t.D[(size_t)(n - 1) * kBand + b];
+    }
+  }
+}
+
+
+void build_cross_planes(const LevelHost& h, std::vector<double>& C) {
+  const int Ny = h.Ny, Nz = h.Nz;
+  const size_t N = (size_t)Ny * Nz;
+  C.assign(33 * N, 0.0);
+  std::vector<double> c1, m31, L;
+  c1.resize(Ny);
+  m31.resize(Ny);
+  for (int iz = 0; iz < Nz; ++iz) {
+    for (int iy = 0; iy < Ny; ++iy) {
+      c1[iy] = h.cy[(size_t)iy * Nz + iz];
+      m31[iy] = h.m3y[(size_t)iy * Nz + iz];
+    }
+    compose_line(h.ty, h.bc[2], h.bc[0], c1, m31, L);
+    for (int iy = 0; iy < Ny; ++iy) {
+      const size_t node = (size_t)iy * Nz + iz;
+      for (int o = 0; o < 17; ++o) C[(size_t)o * N + node] = h.wy[node] * L[(size_t)iy * 17 + o];
+    }
+  }
+  c1.resize(Nz);
+  m31.resize(Nz);
+  for (int iy = 0; iy < Ny; ++iy) {
+    for (int iz = 0; iz < Nz; ++iz) {
+      c1[iz] = h.cz[(size_t)iy * Nz + iz];
+      m31[iz] = h.m3z[(size_t)iy * Nz + iz];
+    }
+    compose_line(h.tz, h.bc[1], h.bc[3], c1, m31, L);
+    for (int iz = 0; iz < Nz; ++iz) {
+      const size_t node = (size_t)iy * Nz + iz;
+      for (int o = 0; o < 17; ++o) {
+        const double v = h.wz[node] * L[(size_t)iz * 17 + o];
+        if (o == 8)
+          C[(size_t)8 * N + node] += v;
+        else
+          C[(size_t)(o < 8 ? 17 + o : 16 + o) * N + node] = v;
+      }
+    }
+  }
+}
+
+void apply_cross_planes(const std::vector<double>& C, int Ny, int Nz, const double* x, double* out) {
+  const size_t N = (size_t)Ny * Nz;
+  for (int iy = 0; iy < Ny; ++iy)
+    for (int iz = 0; iz < Nz; ++iz) {
+      const size_t node = (size_t)iy * Nz + iz;
+      double s = 0.0;
+      for (int o = -8; o <= 8; ++o) {
+        const int jy = iy + o;
+        if (jy >= 0 && jy < Ny) s += C[(size_t)(o + 8) * N + node] * x[(size_t)jy * Nz + iz];
+      }
+      for (int o = -8; o <= 8; ++o) {
+        const int jz = iz + o;
+        if (o == 0 || jz < 0 || jz >= Nz) continue;
+        s += C[(size_t)(o < 0 ? 25 + o : 24 + o) * N + node] * x[(size_t)iy * Nz + jz];
+      }
+      out[node] = s;
+    }
+}
+
 }  // namespace scy

@@ -81,4 +81,20 @@ struct Interp1D {
 };
 Interp1D make_interp(int nf, int nc);
 
+// One direction of A composed into 17-point rows (offsets -8..8): stage 2
+// (Q, R3^T, R4^T) applied to stage 1 (c D, w3 m3 R3, w4 c R4) over the band
+// tables, plus the SAT terms of the boundary rows (Dirichlet: (BS row +
+// alphaD) * c * x(end); Neumann: +/- c D x at the end row).  C[i*17 + o+8]
+// multiplies x(i+o); bc_lo / bc_hi: 0 Dirichlet, 1 Neumann.
+void compose_line(const DirTables& t, int bc_lo, int bc_hi, const std::vector<double>& c1,
+                  const std::vector<double>& m31, std::vector<double>& C);
+// A as a 33-point cross stencil per node, exact for any coefficient fields:
+// (A x)(iy, iz) = sum_{o=-8..8} C[(o+8) N + node] x(iy+o, iz)
+//               + sum_{o=-8..-1} C[(25+o) N + node] x(iy, iz+o) + sum_{o=1..8} C[(24+o) N + node] x(iy, iz+o)
+// (each column's y operator and each row's z operator composed with that
+// line's coefficients, times the outer weights wy and wz).
+void build_cross_planes(const LevelHost& h, std::vector<double>& C);
+// Host reference of the cross-plane form (for checking it against apply_A).
+void apply_cross_planes(const std::vector<double>& C, int Ny, int Nz, const double* x, double* out);
+
 }  // namespace scy

@@ -112,46 +112,6 @@ static int upload_ints(DevBuf& buf, const std::vector<int>& v, cudaStream_t s) {
   return SCY_OK;
 }
 
-// ------------------------------------------------------------------------
-// One direction of A composed into 17-point rows: stage 2 (Q, R3^T, R4^T)
-// applied to stage 1 (c D, w3 m3 R3, w4 c R4) over the band tables, plus the
-// SAT terms the stencil adds at the ends (Dirichlet: (BS row + alphaD) * c *
-// x(end); Neumann: +/- c D x at the end row).  C[i*17 + o+8] multiplies
-// x(i+o); bc_lo / bc_hi: 0 Dirichlet, 1 Neumann.
-static void compose_full(const DirTables& t, int bc_lo, int bc_hi, const std::vector<double>& c1,
-                         const std::vector<double>& m31, std::vector<double>& C) {
-  const int n = t.n;
-  C.assign((size_t)n * 17, 0.0);
-  const bool r4 = t.nterms == 3;
-  for (int i = 0; i < n; ++i) {
-    double* row = &C[(size_t)i * 17];
-    for (int a = 0; a < BAND; ++a) {
-      const int k = i + a - HALF;
-      if (k < 0 || k >= n) continue;
-      const double q = t.Q[(size_t)i * BAND + a], q3 = t.R3T[(size_t)i * BAND + a];
-      const double q4 = r4 ? t.R4T[(size_t)i * BAND + a] : 0.0;
-      for (int b = 0; b < BAND; ++b) {
-        const int j = k + b - HALF;
-        if (j < 0 || j >= n) continue;
-        double v = q * (c1[k] * t.D[(size_t)k * BAND + b]);
-        v -= q3 * (t.w3[k] * m31[k] * t.R3[(size_t)k * BAND + b]);
-        if (r4) v -= q4 * (t.w4[k] * c1[k] * t.R4[(size_t)k * BAND + b]);
-        row[j - i + 8] += v;
-      }
-    }
-    if (bc_lo == 0) {
-      if (i < BAND) row[0 - i + 8] += (t.bs0[i] + (i == 0 ? t.alphaD : 0.0)) * c1[0];
-    } else if (i == 0) {
-      for (int b = HALF; b < BAND; ++b) row[b - HALF + 8] += c1[0] * t.D[b];
-    }
-    if (bc_hi == 0) {
-      if (i >= n - BAND) row[(n - 1) - i + 8] += (t.bsN[i - (n - BAND)] + (i == n - 1 ? t.alphaD : 0.0)) * c1[n - 1];
-    } else if (i == n - 1) {
-      for (int b = 0; b <= HALF; ++b) row[b - HALF + 8] -= c1[n - 1] * t.D[(size_t)(n - 1) * BAND + b];
-    }
-  }
-}
-
 template <typename T>
 int LevelStore<T>::init(const LevelHost& h, cudaStream_t s) {
   Ny = h.Ny;
@@ -308,8 +268,8 @@ int LevelStore<T>::init(const LevelHost& h, cudaStream_t s) {
         }
       if (all) {
         std::vector<double> Cy17, Cz17, CzT17((size_t)17 * Nz);
-        compose_full(h.ty, h.bc[2], h.bc[0], cy1, m3y1, Cy17);
-        compose_full(h.tz, h.bc[1], h.bc[3], cz1, m3z1, Cz17);
+        compose_line(h.ty, h.bc[2], h.bc[0], cy1, m3y1, Cy17);
+        compose_line(h.tz, h.bc[1], h.bc[3], cz1, m3z1, Cz17);
         for (int iz = 0; iz < Nz; ++iz)
           for (int o = 0; o < 17; ++o) CzT17[(size_t)o * Nz + iz] = Cz17[(size_t)iz * 17 + o];
         SCY_TRY(upload<T>(comp17[0], Cy17, s));

@@ -40,6 +40,9 @@ def test_host_tables_match_assembled_A(order, grid, compat, bcs, shape):
     a = op.A @ x
     b = S.host_apply(d, x)
     assert np.abs(a - b).max() <= 1e-13 * np.abs(a).max()
+    # the per-node cross-stencil form of the batched ensemble: the same operator
+    c = S.host_apply(d, x, form="cross")
+    assert np.abs(a - c).max() <= 1e-13 * np.abs(a).max()
 
 
 def test_host_apply_rejects_small_order4_grid():
