@@ -198,6 +198,38 @@ def run_batched(args, dist, rank, world, local):
         v_ref, v_b = q.field("slipVel"), b.instance(0).field("slipVel")
         out["v_rel_err_vs_fp64_single"] = float(np.max(np.abs(v_b - v_ref) / np.abs(v_ref)))
         q.close()
+    # roofline of the batch's main kernels: a separate pass with the round's
+    # launches issued directly and CUDA events around each launch
+    b.set_graphs(False)
+    b.profile(True)
+    b.run(min(args.steps, 10))
+    torch.cuda.synchronize()
+    b.profile(False)
+    peak = _peaks().get("hbm_gbs")
+    peak_src = "measured"
+    if peak is None:
+        peak, peak_src = 6650.0, "fallback"
+    kern = {}
+    for nm, desc in (("ysolve", "b_ysolve_kernel (banded Cholesky sweeps along y of the preconditioner)"),
+                     ("matvec", "b_cross_kernel<1> (CG operator application, p update fused)"),
+                     ("residual", "b_cross_kernel<0> (initial residual of each stage solve)")):
+        pm, pl, pb = b.profile_collect(nm)
+        if pl:
+            us = pm / pl * 1e3
+            ach = (pb / pl) / (us / 1e6) / 1e9
+            kern[nm] = {"kernel": desc, "launch_us": us, "algorithmic_bytes_per_launch": pb / pl,
+                        "achieved": ach, "frac": ach / peak, "total_ms": pm, "launches": pl}
+    b.profile_clear()
+    b.set_graphs(True)
+    if kern:
+        top = max(kern, key=lambda k: kern[k]["total_ms"])
+        t = kern[top]
+        out["roofline"] = {"kernel": t["kernel"], "bound": "hbm", "achieved": t["achieved"], "peak": peak,
+                           "unit": "GB/s", "frac": t["frac"], "peak_source": peak_src, "traffic": None,
+                           "launch_us": t["launch_us"], "algorithmic_bytes_per_launch": t["algorithmic_bytes_per_launch"],
+                           "kernels": kern,
+                           "note": "CUDA events on the launching stream in a pass with the round's launches issued "
+                                   "directly; the dominant kernel is the one with the largest total time"}
     # end to end through the C ABI: every step the states go host -> device and
     # psi, slip and slip velocity device -> host (pinned buffers)
     pin = lambda n: torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
@@ -241,6 +273,53 @@ def run_batched(args, dist, rank, world, local):
     return out
 
 
+C3_WORKLOAD = ("pl_ensemble_c3: %d power-law viscoelastic instances (dislocation creep A=1e-4 MPa^-n/s, n=3, "
+               "Q=135 kJ/mol, geotherm gradient U(15,30) K/km per instance, a-b perturbed by a Gaussian random "
+               "field of std 0.002 and correlation length 2 km), grid sizes 101^2/201^2/301^2 in thirds, RK43")
+
+
+def run_ensemble_c3(args, dist, rank, world, local):
+    """The power-law ensemble of mixed grid sizes as one batch (one operator
+    group per size, the groups on concurrent streams inside each round's
+    graph).  A step is one scy_batch_run(1)."""
+    import torch
+    from scycle_b200.batch import Batch
+    from scycle_b200.configs import pl_ensemble_c3
+    work = tempfile.mkdtemp(prefix="scy_c3_")
+    paths = pl_ensemble_c3(work, n_inst=args.c3, seed=rank)
+    t0 = time.perf_counter()
+    b = Batch(paths, solve_rtol=args.rtol, precision=args.batch_precision)
+    setup_s = time.perf_counter() - t0
+    b.run(args.warmup)
+    torch.cuda.synchronize()
+
+    def totals():
+        st = [b.instance(i).integrate_steps(0) for i in range(b.n)]
+        return sum(x.d_dt_evals for x in st), sum(x.t for x in st)
+
+    steps = max(1, args.steps // 4)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, s0 = totals()
+    st0 = b.run(0)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(steps):
+        st1 = b.run(1)
+    ev1.record()
+    torch.cuda.synchronize()
+    ms = _max_over_ranks(dist, ev0.elapsed_time(ev1))
+    e1, s1 = totals()
+    out = {"workload": C3_WORKLOAD % args.c3, "instances": b.n * world, "groups": st1.groups, "steps": steps,
+           "value": _sum_over_ranks(dist, e1 - e0) / (ms / 1e3), "unit": "stage-solves/s",
+           "ms_per_step": ms / steps, "sim_years_per_hour": _sum_over_ranks(dist, (s1 - s0) / YEAR) / (ms / 3.6e6),
+           "setup_s": setup_s, "cg_its": st1.cg_its, "rounds": st1.rounds - st0.rounds,
+           "redo_rounds": st1.redo_rounds - st0.redo_rounds, "precision": args.batch_precision}
+    b.close()
+    return out
+
+
 def run_ours(args, dist, rank, world, local):
     import torch
     torch.cuda.set_device(local)
@@ -249,6 +328,11 @@ def run_ours(args, dist, rank, world, local):
     from scycle_b200 import _lib as S
     from scycle_b200.qd import QD
     L = S.lib()
+    if args.c3_only:
+        r = run_ensemble_c3(args, dist, rank, world, local)
+        if rank == 0:
+            print(json.dumps(r))
+        return
     if args.batch_only:
         if rank == 0:
             print(json.dumps(run_batched(args, dist, rank, world, local)))
@@ -375,9 +459,10 @@ def run_ours(args, dist, rank, world, local):
               "cg_iterations_per_solve": solve_its, "gpu_launches": int(launches), "e2e": e2e,
               "solver": "FP64 PCG, %s preconditioner (%s), rtol %g, residual read back every %d iterations" % (
                   args.precond, "fp32" if prec == "mixed" else "fp64", args.rtol, args.check_every),
-              "l2": "flushed between steps (256 MB write)", "clocks": clk}
+              "l2": "flushed between steps (256 MB write)", "clocks": clk, "roofline": roofline}
     q.close()
     batched = run_batched(args, dist, rank, world, local) if args.batch > 0 else None
+    ensemble_c3 = run_ensemble_c3(args, dist, rank, world, local) if args.c3 > 0 else None
     head = batched if batched else single
     config = {"workload": (BATCH_WORKLOAD % args.batch) if batched else WORKLOAD, "Ny": args.n, "Nz": args.n,
               "integrator": "RK32", "parallelism": "replicas x%d" % world}
@@ -395,11 +480,12 @@ def run_ours(args, dist, rank, world, local):
            "dtype": "f64 (%s preconditioner)" % ((args.batch_precision if batched else prec)),
            "data": "synthetic (seeded; reference .in format)", "config": config,
            "sim_years_per_hour": head["sim_years_per_hour"], "sim_years_timed": head["sim_years_timed"],
-           "stage_solves": head["stage_solves"], "e2e": head["e2e"], "roofline": roofline, "cpu_baseline": cpu,
+           "stage_solves": head["stage_solves"], "e2e": head["e2e"],
+           "roofline": (batched.get("roofline") or roofline) if batched else roofline, "cpu_baseline": cpu,
            "gpu_launches": head["gpu_launches"], "clocks": head["clocks"],
            "batched": batched, "fp64_single": single,
            "batched_vs_fp64_single_sim_years": (batched["sim_years_per_hour"] / syph) if batched else None,
-           "response_mode": resp, "cycle": cycle}
+           "response_mode": resp, "cycle": cycle, "ensemble_c3": ensemble_c3}
     if rank == 0:
         print(json.dumps(out))
 
@@ -581,6 +667,8 @@ def main():
     ap.add_argument("--batch", type=int, default=32, help="instances per GPU of the batched ensemble (0: none)")
     ap.add_argument("--batch-precision", default="fp64", choices=["fp64", "mixed", "tf32"])
     ap.add_argument("--batch-only", action="store_true", help="measure the batched ensemble alone")
+    ap.add_argument("--c3", type=int, default=128, help="instances of the power-law ensemble (0: skip)")
+    ap.add_argument("--c3-only", action="store_true", help="measure the power-law ensemble alone")
     ap.add_argument("--cycle-n", type=int, default=801)
     ap.add_argument("--cycle-mode", default="response", choices=["response", "solve"])
     ap.add_argument("--profile-stencil", type=int, default=0,

@@ -551,6 +551,21 @@ scy_status scy_batch_set_states(scy_batch* b, const double* host);
  * STRENGTH) of every instance into one host array, Nz values per instance
  * in the caller's instance order. */
 scy_status scy_batch_get_fault_field(scy_batch* b, int field, double* host);
+/* 1: each round is one CUDA graph launch; 0: its launches issued directly. */
+scy_status scy_batch_set_graphs(scy_batch* b, int on);
+/* Per-launch timing of the batch's main kernels while on (takes effect in
+ * rounds launched directly, see scy_batch_set_graphs): CUDA events on the
+ * launching stream around each launch, for measurement passes. */
+scy_status scy_batch_profile(scy_batch* b, int on);
+enum { SCY_BATCH_KERNEL_YSOLVE = 0, SCY_BATCH_KERNEL_RESIDUAL = 1, SCY_BATCH_KERNEL_MATVEC = 2 };
+/* Sums the timed launches of one kernel (SCY_BATCH_KERNEL_*): milliseconds,
+ * launch count and algorithmic bytes (the banded sweeps: factor once plus
+ * read and write of the transform twice; the operator kernels: coefficient
+ * planes once plus the per-node operands and results of the active
+ * instances). */
+scy_status scy_batch_profile_collect(scy_batch* b, int kernel, double* ms, long long* launches, double* bytes);
+/* Drops the recorded launches. */
+scy_status scy_batch_profile_clear(scy_batch* b);
 
 #ifdef __cplusplus
 }

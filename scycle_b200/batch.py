@@ -75,6 +75,23 @@ class Batch:
         S.check(S.lib().scy_batch_get_fault_field(self.h, X.FIELDS[name], S.as_dptr(out)))
         return out
 
+    def set_graphs(self, on):
+        S.check(S.lib().scy_batch_set_graphs(self.h, 1 if on else 0))
+
+    def profile(self, on):
+        S.check(S.lib().scy_batch_profile(self.h, 1 if on else 0))
+
+    def profile_collect(self, kernel):
+        """(milliseconds, launches, algorithmic bytes) of the timed launches of
+        "ysolve", "residual" or "matvec"."""
+        ms, nl, by = C.c_double(), C.c_longlong(), C.c_double()
+        k = {"ysolve": 0, "residual": 1, "matvec": 2}[kernel]
+        S.check(S.lib().scy_batch_profile_collect(self.h, k, C.byref(ms), C.byref(nl), C.byref(by)))
+        return ms.value, nl.value, by.value
+
+    def profile_clear(self):
+        S.check(S.lib().scy_batch_profile_clear(self.h))
+
     def close(self):
         h = getattr(self, "h", None)
         if h:

@@ -175,3 +175,32 @@ def slip_var_401(workdir, seed=0, **kw):
                 stretch_beta=2.0, dc_lognormal=True, name="slip_var_401", guess_ss=1)
     args.update(kw)
     return make_qd_problem(workdir, **args)
+
+
+def pl_ensemble_c3(workdir, n_inst=128, seed=0, sizes=(101, 201, 301), Lz=30.0, sigma_ab=0.002, corr_km=2.0,
+                   grad_range=(15.0, 30.0), **kw):
+    """Ensemble of power-law viscoelastic instances with dislocation creep
+    (A = 1e-4 MPa^-n/s, n = 3, Q = 135 kJ/mol): grid sizes split in thirds
+    over ``sizes`` (43/43/42 of 128 for 101^2/201^2/301^2), a linear
+    geotherm with gradient ~ U(grad_range) K/km per instance, and a - b
+    perturbed by a seeded Gaussian random field on the fault (std
+    ``sigma_ab``, squared-exponential correlation length ``corr_km``),
+    written as inputDir/b.  Returns the .in paths, grouped by size."""
+    rng = np.random.default_rng(seed)
+    counts = [n_inst // len(sizes) + (1 if i < n_inst % len(sizes) else 0) for i in range(len(sizes))]
+    paths = []
+    i = 0
+    for n, cnt in zip(sizes, counts):
+        z = np.arange(n) / (n - 1.0) * Lz
+        d = z[:, None] - z[None, :]
+        Lc = np.linalg.cholesky(sigma_ab ** 2 * np.exp(-0.5 * (d / corr_km) ** 2) + 1e-12 * np.eye(n))
+        b0 = np.interp(z, [0.0, 12.0, 17.0, Lz], [0.015, 0.015, 0.005, 0.005])
+        for _ in range(cnt):
+            grad = rng.uniform(*grad_range)
+            path = make_pl_problem(os.path.join(workdir, "c3_%03d" % i), Ny=n, Nz=n, Lz=Lz, seed=seed * 1000 + i,
+                                   grad=grad, name="pl", **kw)
+            # a - b + delta: b - delta on the fault
+            write_petsc_vec(path[:-len(".in")] + "_in_b", b0 - Lc @ rng.standard_normal(n))
+            paths.append(path)
+            i += 1
+    return paths

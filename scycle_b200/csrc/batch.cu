@@ -295,14 +295,13 @@ __global__ void b_scale_kernel(T* __restrict__ x, const T* __restrict__ s, long 
 // back substitution), in place.  t is the Nz x Ny*K column-major matrix of
 // the transform, so consecutive threads (consecutive j) touch consecutive
 // addresses; the last eight values of the sweep stay in registers.
-template <typename T, int R>
+template <typename T, int R, int RB>
 __global__ void __launch_bounds__(128) b_ysolve_kernel(const T* __restrict__ Lb, T* __restrict__ t, int Ny, int Nz,
                                                        int K) {
   // A thread sweeps the systems of one z mode j for R instances at once:
   // every factor coefficient is loaded once for the R sweeps, and the rows
   // are taken RB at a time (their loads issued together, so one memory
   // latency covers RB steps of the R sweeps).
-  constexpr int RB = 4;
   const int KR = (K + R - 1) / R;
   const long g = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (g >= (long)Nz * KR) return;
@@ -520,6 +519,10 @@ BatchGroup::~BatchGroup() {
 }
 
 BatchContext::~BatchContext() {
+  for (auto& r : precs) {
+    cudaEventDestroy(r.a);
+    cudaEventDestroy(r.b);
+  }
   for (auto& kv : graph_of_its) cudaGraphExecDestroy(kv.second);
   graph_of_its.clear();
   groups.clear();
@@ -760,6 +763,51 @@ int BatchContext::setup_group(int base, int K) {
   return SCY_OK;
 }
 
+int BatchContext::active_in(const BatchGroup& g, const int* mask) const {
+  const int* h = reinterpret_cast<const int*>(static_cast<const double*>(ctl_host) + 2 * n);
+  if (mask == d_acc(g)) h += n;
+  else if (mask == d_run(g)) h += 2 * n;
+  int c = 0;
+  for (int k = 0; k < g.K; ++k) c += h[g.base + k] ? 1 : 0;
+  return c;
+}
+
+int BatchContext::prof_begin(cudaStream_t s, cudaEvent_t* a) {
+  *a = nullptr;
+  if (!prof || graphs) return SCY_OK;
+  SCY_CUDA_TRY(cudaEventCreate(a));
+  SCY_CUDA_TRY(cudaEventRecord(*a, s));
+  return SCY_OK;
+}
+
+int BatchContext::prof_end(cudaStream_t s, cudaEvent_t a, int tag, double bytes) {
+  if (!a) return SCY_OK;
+  ProfRec r{a, nullptr, tag, bytes};
+  SCY_CUDA_TRY(cudaEventCreate(&r.b));
+  SCY_CUDA_TRY(cudaEventRecord(r.b, s));
+  precs.push_back(r);
+  return SCY_OK;
+}
+
+int BatchContext::prof_collect(int tag, double* ms, long long* launches, double* bytes) {
+  double tms = 0.0, tb = 0.0;
+  long long nl = 0;
+  for (auto& r : precs) {
+    if (r.tag == tag) {
+      SCY_CUDA_TRY(cudaEventSynchronize(r.b));
+      float m = 0.0f;
+      SCY_CUDA_TRY(cudaEventElapsedTime(&m, r.a, r.b));
+      tms += m;
+      tb += r.bytes;
+      ++nl;
+    }
+  }
+  *ms = tms;
+  *launches = nl;
+  *bytes = tb;
+  return SCY_OK;
+}
+
 // z = K_sep^-1 r for every instance of the group (instance k's r at k*N):
 // Z = Vz [ (Vz^T R Vy) ./ (lz + ly) ] Vy^T with R the Nz x Ny column-major
 // view of an instance; the outer products act on all instances at once
@@ -772,8 +820,9 @@ int BatchContext::fd_apply(BatchGroup& g) {
   dim3 sg(node_blocks(N), 1, K);
   if (F.ybanded && !fd_dense) {
     // Z = Vz [ per z mode: (Ky + lz_j My)^-1 along y ] (Vz^T R)
-    // instances per thread in the banded sweeps (register budget: 4 in FP32, 2 in FP64)
-    const int R = precision != SCY_PREC_FP64 ? 4 : 2;
+    // instances per thread and rows per load round in the banded sweeps
+    // (register budget: 2 x 8 in FP32, 1 x 8 in FP64)
+    const int R = precision != SCY_PREC_FP64 ? 2 : 1;
     const int nb = (int)(((long)Nz * ((K + R - 1) / R) + 127) / 128);
     if (precision != SCY_PREC_FP64) {
       SCY_BLAS_TRY(cublasSetMathMode(g.blas, precision == SCY_PREC_TF32 ? CUBLAS_TF32_TENSOR_OP_MATH
@@ -782,8 +831,11 @@ int BatchContext::fd_apply(BatchGroup& g) {
       const float* vz = F.Vz32.as<float>();
       SCY_BLAS_TRY(cublasSgemm(g.blas, CUBLAS_OP_T, CUBLAS_OP_N, Nz, Ny * K, Nz, &one, vz, Nz, g.w.r32, Nz, &zero,
                                g.w.t1f, Nz));
-      b_ysolve_kernel<float, 4><<<nb, 128, 0, g.stream>>>(F.Lb32.as<float>(), g.w.t1f, Ny, Nz, K);
+      cudaEvent_t pa;
+      SCY_TRY(prof_begin(g.stream, &pa));
+      b_ysolve_kernel<float, 2, 8><<<nb, 128, 0, g.stream>>>(F.Lb32.as<float>(), g.w.t1f, Ny, Nz, K);
       SCY_LAUNCH_CHECK();
+      SCY_TRY(prof_end(g.stream, pa, PROF_YSOLVE, 4.0 * (9.0 * Ny * Nz + 4.0 * N * K)));
       SCY_BLAS_TRY(cublasSgemm(g.blas, CUBLAS_OP_N, CUBLAS_OP_N, Nz, Ny * K, Nz, &one, vz, Nz, g.w.t1f, Nz, &zero,
                                g.w.z32, Nz));
     } else {
@@ -792,8 +844,11 @@ int BatchContext::fd_apply(BatchGroup& g) {
       const double* vz = F.Vz.as<double>();
       SCY_BLAS_TRY(cublasDgemm(g.blas, CUBLAS_OP_T, CUBLAS_OP_N, Nz, Ny * K, Nz, &one, vz, Nz, g.w.r, Nz, &zero,
                                g.w.t1, Nz));
-      b_ysolve_kernel<double, 2><<<nb, 128, 0, g.stream>>>(F.Lb.as<double>(), g.w.t1, Ny, Nz, K);
+      cudaEvent_t pa;
+      SCY_TRY(prof_begin(g.stream, &pa));
+      b_ysolve_kernel<double, 1, 8><<<nb, 128, 0, g.stream>>>(F.Lb.as<double>(), g.w.t1, Ny, Nz, K);
       SCY_LAUNCH_CHECK();
+      SCY_TRY(prof_end(g.stream, pa, PROF_YSOLVE, 8.0 * (9.0 * Ny * Nz + 4.0 * N * K)));
       SCY_BLAS_TRY(cublasDgemm(g.blas, CUBLAS_OP_N, CUBLAS_OP_N, Nz, Ny * K, Nz, &one, vz, Nz, g.w.t1, Nz, &zero,
                                g.w.z, Nz));
     }
@@ -844,25 +899,33 @@ int BatchContext::solve(BatchGroup& g, const int* mask, int its_now) {
   const BatchInst* tab = g.tab.as<BatchInst>();
   const double* C = g.planes.as<double>();
   const int ntiles = (int)(tg.x * tg.y);
+  // algorithmic bytes: the coefficient planes once, per node and active
+  // instance the operand, rhs and result (residual) or z, p_old, p and q
+  const double nact = (double)active_in(g, mask);
+  cudaEvent_t pa;
+  SCY_TRY(prof_begin(g.stream, &pa));
   b_cross_kernel<0, double><<<tg, 256, 0, g.stream>>>(C, g.Ny, g.Nz, tab, mask, g.w, nullptr, 0, 0, mixed, g.kpb);
   SCY_LAUNCH_CHECK();
+  SCY_TRY(prof_end(g.stream, pa, PROF_RESIDUAL, 33.0 * 8 * g.N + nact * g.N * (24.0 + (mixed ? 4 : 0))));
   b_partials_kernel<<<g.K, 256, 0, g.stream>>>(mask, g.w, ntiles, 5);
   SCY_LAUNCH_CHECK();
   int pi = 0;
   for (int it = 1; it <= its_now; ++it) {
     SCY_TRY(fd_apply(g));
-    if (mixed) {
+    if (mixed)
       b_dot_rz_kernel<float><<<ng, TB, 0, g.stream>>>(mask, g.w, g.w.z32);
-      SCY_LAUNCH_CHECK();
+    else
+      b_dot_rz_kernel<double><<<ng, TB, 0, g.stream>>>(mask, g.w, g.w.z);
+    SCY_LAUNCH_CHECK();
+    SCY_TRY(prof_begin(g.stream, &pa));
+    if (mixed)
       b_cross_kernel<1, float><<<tg, 256, 0, g.stream>>>(C, g.Ny, g.Nz, tab, mask, g.w, g.w.z32, it == 1 ? 1 : 0,
                                                           pi, mixed, g.kpb);
-    } else {
-      b_dot_rz_kernel<double><<<ng, TB, 0, g.stream>>>(mask, g.w, g.w.z);
-      SCY_LAUNCH_CHECK();
+    else
       b_cross_kernel<1, double><<<tg, 256, 0, g.stream>>>(C, g.Ny, g.Nz, tab, mask, g.w, g.w.z, it == 1 ? 1 : 0,
                                                            pi, mixed, g.kpb);
-    }
     SCY_LAUNCH_CHECK();
+    SCY_TRY(prof_end(g.stream, pa, PROF_MATVEC, 33.0 * 8 * g.N + nact * g.N * (mixed ? 28.0 : 32.0)));
     b_partials_kernel<<<g.K, 256, 0, g.stream>>>(mask, g.w, ntiles, 4);
     SCY_LAUNCH_CHECK();
     b_update_kernel<<<ng, TB, 0, g.stream>>>(tab, mask, g.w, pi, mixed);
@@ -1306,6 +1369,34 @@ scy_status scy_batch_get_fault_field(scy_batch* b, int field, double* host) {
     off += c.Nz;
   }
   SCY_CUDA_TRY(cudaStreamSynchronize(B.stream));
+  return SCY_OK;
+}
+
+scy_status scy_batch_set_graphs(scy_batch* b, int on) {
+  if (!b) return SCY_ERR_ARG;
+  b->ctx.graphs = on ? 1 : 0;
+  return SCY_OK;
+}
+
+scy_status scy_batch_profile(scy_batch* b, int on) {
+  if (!b) return SCY_ERR_ARG;
+  b->ctx.prof = on ? 1 : 0;
+  return SCY_OK;
+}
+
+scy_status scy_batch_profile_collect(scy_batch* b, int kernel, double* ms, long long* launches, double* bytes) {
+  if (!b || !ms || !launches || !bytes || kernel < 0 || kernel > 2) return SCY_ERR_ARG;
+  SCY_TRY(b->ctx.prof_collect(kernel, ms, launches, bytes));
+  return SCY_OK;
+}
+
+scy_status scy_batch_profile_clear(scy_batch* b) {
+  if (!b) return SCY_ERR_ARG;
+  for (auto& r : b->ctx.precs) {
+    cudaEventDestroy(r.a);
+    cudaEventDestroy(r.b);
+  }
+  b->ctx.precs.clear();
   return SCY_OK;
 }
 

@@ -53,6 +53,9 @@ struct BatchWork {
   unsigned* status;    // K
 };
 
+// tags of the timed kernels (scy_batch_profile_collect)
+enum { PROF_YSOLVE = 0, PROF_RESIDUAL = 1, PROF_MATVEC = 2 };
+
 struct BatchGroup {
   int K = 0, base = 0;  // instances base .. base + K - 1 of the batch
   int Ny = 0, Nz = 0;
@@ -100,6 +103,19 @@ struct BatchContext {
   };
   std::vector<Ctl> hc;
   long rounds = 0, redo_rounds = 0, graph_launches = 0, inst_steps = 0, stage_solves = 0;
+  // optional per-launch timing of the main kernels (rounds launched directly
+  // while on): CUDA events on the launching stream around each launch
+  struct ProfRec {
+    cudaEvent_t a, b;
+    int tag;
+    double bytes;  // algorithmic bytes of the launch
+  };
+  int prof = 0;
+  std::vector<ProfRec> precs;
+  int active_in(const BatchGroup& g, const int* mask) const;  // instances of g the mask selects this round
+  int prof_begin(cudaStream_t s, cudaEvent_t* a);
+  int prof_end(cudaStream_t s, cudaEvent_t a, int tag, double bytes);
+  int prof_collect(int tag, double* ms, long long* launches, double* bytes);
 
   ~BatchContext();
   int create(int n, const char* const* paths, const scy_solve_opts* solve, const scy_batch_opts* o);

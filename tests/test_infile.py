@@ -76,3 +76,25 @@ def test_loader_rejects_truncated_binary(tmp_path):
     open(psi, "wb").write(data[:-8])
     with pytest.raises(S.ScyError):
         inspect_in(p)
+
+
+def test_pl_ensemble_files_load(tmp_path):
+    """The power-law ensemble writes one loadable input per instance: sizes
+    in thirds, b perturbed around the depth profile by about 0.002, and a
+    geotherm gradient per instance."""
+    from scycle_b200.configs import pl_ensemble_c3
+    from scycle_b200.qd import inspect_in
+    paths = pl_ensemble_c3(str(tmp_path), n_inst=6, sizes=(33, 41))
+    assert len(paths) == 6
+    sizes, dev, grads = [], [], set()
+    for p in paths:
+        info = inspect_in(p, fields=("b",))
+        sizes.append(info["grid"]["Ny"])
+        z = np.arange(info["grid"]["Nz"]) / (info["grid"]["Nz"] - 1.0) * 30.0
+        dev.append(info["b"] - np.interp(z, [0, 12, 17, 30], [0.015, 0.015, 0.005, 0.005]))
+        txt = open(p).read()
+        assert "bulkDeformationType = powerLaw" in txt
+        grads.add([l for l in txt.splitlines() if l.startswith("TVals")][0])
+    assert sizes == [33, 33, 33, 41, 41, 41]
+    assert 0.0005 < np.std(np.concatenate(dev)) < 0.005
+    assert len(grads) == 6
