@@ -85,6 +85,40 @@ __global__ void b_rhs_kernel(LevelDev<double> L, const BatchInst* __restrict__ t
   grid_reduce_finish(s, w.partials + (long)k * w.PB, w.counters + 4 * k, w.sc + 16 * k + 0, sh);
 }
 
+// Linear-elastic rhs: setRhs is nonzero only within BAND nodes of the
+// boundary (SAT columns of the Dirichlet sides, boundary values of the
+// Neumann sides), and the interior of every instance's rhs was written with
+// zeros by its first (single-instance) d_dt, so only that frame is
+// rewritten.  Frame index f < 2 * BAND * Nz: rows 0..BAND-1 and Ny-BAND..Ny-1;
+// after that, columns 0..BAND-1 and Nz-BAND..Nz-1 of the rows in between.
+__global__ void b_rhs_frame_kernel(LevelDev<double> L, const BatchInst* __restrict__ tab,
+                                   const int* __restrict__ mask, BatchWork w, int nframe) {
+  __shared__ double sh[32];
+  const int k = blockIdx.z;
+  if (!mask[k]) return;
+  const BatchInst& I = tab[k];
+  const int Ny = L.Ny, Nz = L.Nz;
+  double acc = 0.0;
+  for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < nframe; f += gridDim.x * blockDim.x) {
+    int iy, iz;
+    if (f < 2 * BAND * Nz) {
+      const int r = f / Nz;
+      iz = f - r * Nz;
+      iy = r < BAND ? r : Ny - 2 * BAND + r;
+    } else {
+      const int e = f - 2 * BAND * Nz, r = e / (2 * BAND), c = e - r * (2 * BAND);
+      iy = BAND + r;
+      iz = c < BAND ? c : Nz - 2 * BAND + c;
+    }
+    const long node = (long)iy * Nz + iz;
+    const double v = set_rhs_node(L, I.bcL, I.bcR, I.bcT, I.bcB, node);
+    I.rhs[node] = v;
+    acc += v * v;
+  }
+  double s = block_sum(acc, sh);
+  grid_reduce_finish(s, w.partials + (long)k * w.PB, w.counters + 4 * k, w.sc + 16 * k + 0, sh);
+}
+
 // rz = r.z -> sc[2] (the previous value moves to sc[3])
 template <typename Tz>
 __global__ void b_dot_rz_kernel(const int* __restrict__ mask, BatchWork w, const Tz* __restrict__ z) {
@@ -136,10 +170,9 @@ __global__ void __launch_bounds__(256) b_cross_kernel(const double* __restrict__
                                                       BatchWork w, const Tz* __restrict__ zv, int first, int pi,
                                                       int mixed, int kpb) {
   constexpr int NY = (XTY + 2 * XH) * XTZ, NZ = XTY * (XTZ + 2 * XH);
-  constexpr int PY = (NY + 255) / 256, PZ = (NZ + 255) / 256;  // staged values per thread
-  __shared__ double xy[NY];
-  __shared__ double xz[NZ];
-  __shared__ double red[32];
+  constexpr int NV = (NY + NZ + 255) / 256;  // staged values per thread
+  __shared__ double xs[NY + NZ];             // y arm rows, then z arm rows
+  __shared__ double red[8];
   const long N = (long)Ny * Nz;
   const int tid = threadIdx.x, ty = tid / XTZ, tz = tid % XTZ;
   const int y0 = blockIdx.y * XTY, z0 = blockIdx.x * XTZ;
@@ -150,37 +183,46 @@ __global__ void __launch_bounds__(256) b_cross_kernel(const double* __restrict__
   double c[33];
 #pragma unroll
   for (int o = 0; o < 33; ++o) c[o] = valid ? C[(long)o * N + node] : 0.0;
+  // the staged positions do not depend on the instance: their node offsets
+  // (-1 outside the grid) are worked out once
+  int src[NV];
+#pragma unroll
+  for (int a = 0; a < NV; ++a) {
+    const int i = tid + 256 * a;
+    int jy = -1, jz = -1;
+    if (i < NY) {
+      jy = y0 - XH + i / XTZ;
+      jz = z0 + i % XTZ;
+    } else if (i < NY + NZ) {
+      const int e = i - NY;
+      jy = y0 + e / (XTZ + 2 * XH);
+      jz = z0 - XH + e % (XTZ + 2 * XH);
+    }
+    src[a] = (jy >= 0 && jy < Ny && jz >= 0 && jz < Nz) ? jy * Nz + jz : -1;
+  }
   const int kb = blockIdx.z * kpb, ke = min(w.K, kb + kpb);
-  // the operand of instance k at the staged positions, into registers
-  double vy[PY], vz[PZ];
+  double v[NV];
+  double rhs_n = 0.0;  // MODE 0: the next instance's rhs at this node
+  bool zero_n = false;  // MODE 0: the next instance's rhs is zero
   auto fetch = [&](int k) {
     const long off = (long)k * N;
-    const double* xsrc = tab[k].u;
-    const Tz* zsrc = zv + off;
-    const double* pold = (pi ? w.p1 : w.p0) + off;
-    double beta = 0.0;
-    if (MODE == 1 && !first) {
-      const double ro = w.sc[16 * k + 3];
-      beta = ro != 0.0 ? w.sc[16 * k + 2] / ro : 0.0;
-    }
-    auto ld = [&](long n) -> double {
-      if (MODE == 0) return xsrc[n];
-      const double zz = (double)zsrc[n];
-      return first ? zz : zz + beta * pold[n];
-    };
+    if (MODE == 0) {
+      const double* x = tab[k].u;
 #pragma unroll
-    for (int a = 0; a < PY; ++a) {
-      const int i = tid + 256 * a;
-      const int r = i / XTZ, cc = i % XTZ;
-      const int jy = y0 - XH + r, jz = z0 + cc;
-      vy[a] = (i < NY && jy >= 0 && jy < Ny && jz < Nz) ? ld((long)jy * Nz + jz) : 0.0;
-    }
+      for (int a = 0; a < NV; ++a) v[a] = src[a] >= 0 ? x[src[a]] : 0.0;
+      rhs_n = (valid && w.sc[16 * k] != 0.0) ? tab[k].rhs[node] : 0.0;
+      zero_n = w.sc[16 * k] == 0.0;
+    } else {
+      const Tz* zz = zv + off;
+      const double* pold = (pi ? w.p1 : w.p0) + off;
+      double beta = 0.0;
+      if (!first) {
+        const double ro = w.sc[16 * k + 3];
+        beta = ro != 0.0 ? w.sc[16 * k + 2] / ro : 0.0;
+      }
 #pragma unroll
-    for (int a = 0; a < PZ; ++a) {
-      const int i = tid + 256 * a;
-      const int r = i / (XTZ + 2 * XH), cc = i % (XTZ + 2 * XH);
-      const int jy = y0 + r, jz = z0 - XH + cc;
-      vz[a] = (i < NZ && jy < Ny && jz >= 0 && jz < Nz) ? ld((long)jy * Nz + jz) : 0.0;
+      for (int a = 0; a < NV; ++a)
+        v[a] = src[a] >= 0 ? (first ? (double)zz[src[a]] : (double)zz[src[a]] + beta * pold[src[a]]) : 0.0;
     }
   };
   auto next_active = [&](int k) {
@@ -191,31 +233,31 @@ __global__ void __launch_bounds__(256) b_cross_kernel(const double* __restrict__
   if (k < ke) fetch(k);
   while (k < ke) {
 #pragma unroll
-    for (int a = 0; a < PY; ++a)
-      if (tid + 256 * a < NY) xy[tid + 256 * a] = vy[a];
-#pragma unroll
-    for (int a = 0; a < PZ; ++a)
-      if (tid + 256 * a < NZ) xz[tid + 256 * a] = vz[a];
+    for (int a = 0; a < NV; ++a)
+      if (tid + 256 * a < NY + NZ) xs[tid + 256 * a] = v[a];
+    const double rhs_k = rhs_n;
+    const bool zero_k = zero_n;
     __syncthreads();
     const int kn = next_active(k + 1);
     if (kn < ke) fetch(kn);  // in flight while this instance is computed
     const long off = (long)k * N;
     double contrib = 0.0;
     if (valid) {
-      const double* ay = xy + ty * XTZ + tz;             // row iy - 8
-      const double* az = xz + ty * (XTZ + 2 * XH) + tz;  // column iz - 8
-      double Ax = 0.0;
+      const double* ay = xs + ty * XTZ + tz;                   // row iy - 8
+      const double* az = xs + NY + ty * (XTZ + 2 * XH) + tz;   // column iz - 8
+      double Ay = 0.0, Az = 0.0;
 #pragma unroll
-      for (int o = 0; o < 17; ++o) Ax += c[o] * ay[o * XTZ];
+      for (int o = 0; o < 17; ++o) Ay += c[o] * ay[o * XTZ];
 #pragma unroll
-      for (int o = 0; o < 8; ++o) Ax += c[17 + o] * az[o];
+      for (int o = 0; o < 8; ++o) Az += c[17 + o] * az[o];
 #pragma unroll
-      for (int o = 9; o < 17; ++o) Ax += c[16 + o] * az[o];
+      for (int o = 9; o < 17; ++o) Az += c[16 + o] * az[o];
+      const double Ax = Ay + Az;
       if (MODE == 0) {
-        const double v = w.sc[16 * k] == 0.0 ? 0.0 : -1.0 * tab[k].rhs[node] + Ax;
-        w.r[off + node] = v;
-        if (mixed) w.r32[off + node] = (float)v;
-        contrib = v * v;
+        const double vv = zero_k ? 0.0 : -1.0 * rhs_k + Ax;
+        w.r[off + node] = vv;
+        if (mixed) w.r32[off + node] = (float)vv;
+        contrib = vv * vv;
       } else {
         const double p = ay[XH * XTZ];
         const double qv = -Ax;
@@ -224,9 +266,16 @@ __global__ void __launch_bounds__(256) b_cross_kernel(const double* __restrict__
         contrib = p * qv;
       }
     }
-    // block partial of this instance; b_partials_kernel adds the tiles up
-    const double tot = block_sum(contrib, red);
-    if (tid == 0) w.partials[(long)k * w.PB + tile] = tot;
+    // block partial of this instance (warp sums, then warp 0 adds the 8 in
+    // order); b_partials_kernel adds the tiles up
+    contrib = warp_sum(contrib);
+    if ((tid & 31) == 0) red[tid >> 5] = contrib;
+    __syncthreads();
+    if (tid < 32) {
+      double t = tid < 8 ? red[tid] : 0.0;
+      t = warp_sum(t);
+      if (tid == 0) w.partials[(long)k * w.PB + tile] = t;
+    }
     k = kn;
   }
 }
@@ -943,7 +992,13 @@ int BatchContext::d_dt(BatchGroup& g, const int* mask, double c, int in_slot, in
   const dim3 ng(node_blocks(g.N), 1, g.K);
   b_bc_kernel<<<fg, 64, 0, g.stream>>>(tab, mask, d_t(), d_dt_(), g.base, c, in_slot);
   SCY_LAUNCH_CHECK();
-  b_rhs_kernel<<<ng, TB, 0, g.stream>>>(g.L, tab, mask, in_slot, g.w);
+  if (!pl && g.Ny > 2 * BAND && g.Nz > 2 * BAND) {
+    const int nframe = 2 * BAND * g.Nz + (g.Ny - 2 * BAND) * 2 * BAND;
+    const dim3 rg((nframe + TB - 1) / TB < 64 ? (nframe + TB - 1) / TB : 64, 1, g.K);
+    b_rhs_frame_kernel<<<rg, TB, 0, g.stream>>>(g.L, tab, mask, g.w, nframe);
+  } else {
+    b_rhs_kernel<<<ng, TB, 0, g.stream>>>(g.L, tab, mask, in_slot, g.w);
+  }
   SCY_LAUNCH_CHECK();
   SCY_TRY(solve(g, mask, its_now));
   if (pl) {
