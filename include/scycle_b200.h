@@ -567,6 +567,37 @@ scy_status scy_batch_profile_collect(scy_batch* b, int kernel, double* ms, long 
 /* Drops the recorded launches. */
 scy_status scy_batch_profile_clear(scy_batch* b);
 
+/* ---------------------------------------------------------------------------
+ * Discrete adjoint of the linear-elastic quasi-dynamic RK32 integration.
+ * No counterpart in the reference (it has no adjoint); the forward map is
+ * RK32::integrate (odeSolver.cpp:505-627) over a fixed sequence of accepted
+ * step sizes with StrikeSlip_LinearElastic_qd::d_dt (solve mode).  The misfit
+ * is J = sum_n w_surf |surfDisp_n - target_surf_n|^2 + w_vel |V_n - target_vel_n|^2
+ * over the accepted states n = 1..M; the gradient is with respect to a, b
+ * and Dc at every fault node (the initial state is held fixed).  States are
+ * checkpointed every `checkpoint_every` steps and each segment recomputed
+ * before its reverse sweep; one reverse stage costs one elliptic solve. */
+typedef struct scy_adj scy_adj;
+/* On a driver that has been begun with RK32 (its current state and time are
+ * the initial state and time of every forward run). */
+scy_status scy_adj_create(scy_qd* q, int checkpoint_every, scy_adj** out);
+scy_status scy_adj_destroy(scy_adj* a);
+/* The accepted step sizes (e.g. the accepted entries of scy_qd_get_attempts). */
+scy_status scy_adj_set_steps(scy_adj* a, const double* dts, long n);
+/* Targets (host, n x Ny surface displacement and n x Nz slip velocity,
+ * state-major) and the misfit weights. */
+scy_status scy_adj_set_targets(scy_adj* a, const double* target_surf, const double* target_vel, double w_surf,
+                               double w_vel);
+/* Replaces the fault's a, b and / or Dc (host, Nz each; NULL keeps a field). */
+scy_status scy_adj_set_fault_params(scy_adj* a, const double* fa, const double* fb, const double* fDc);
+/* Runs the forward map from the initial state; J = the misfit (0 without targets). */
+scy_status scy_adj_forward(scy_adj* a, double* J);
+/* Surface displacement and slip velocity of the accepted states of the last
+ * forward run (host, n x Ny and n x Nz). */
+scy_status scy_adj_observations(scy_adj* a, double* surf, double* vel);
+/* Forward run, then the reverse sweep: J and dJ/da, dJ/db, dJ/dDc (host, Nz each). */
+scy_status scy_adj_gradient(scy_adj* a, double* J, double* grad_a, double* grad_b, double* grad_Dc);
+
 #ifdef __cplusplus
 }
 #endif
