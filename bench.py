@@ -320,6 +320,102 @@ def run_ensemble_c3(args, dist, rank, world, local):
     return out
 
 
+C4_WORKLOAD = ("adjoint_c4: 201x201 linear-elastic quasi-dynamic, constant grid, aging law, steady-state initial "
+               "guess, %d RK32 steps of at most 1e5 s, rootTol 1e-14; misfit L2(surface displacement) + L2(slip velocity) against a target from "
+               "seeded perturbed a(z), b(z), Dc(z) at 40 depth knots each; gradient with respect to the 120 knot "
+               "values, checkpoints every 50 steps")
+
+
+def run_adjoint_c4(args, dist, rank, world, local):
+    """Adjoint gradient of BASELINE config 4 and its check against central
+    finite differences of the forward map (h = 1e-6 relative, 10 random
+    directions in knot space)."""
+    import torch
+    from scycle_b200.adjoint import Adjoint, knot_matrix
+    from scycle_b200.configs import make_qd_problem, write_petsc_vec
+    from scycle_b200.qd import QD, inspect_in
+    n, M = 201, args.c4_steps
+    work = tempfile.mkdtemp(prefix="scy_c4_")
+    # step sizes capped at 1e5 s: the 2000 steps stay in the interseismic
+    # period (about 6 years), where a misfit gradient is well defined
+    path = make_qd_problem(work, Ny=n, Nz=n, seed=rank, state_law="agingLaw", integrator="RK32", guess_ss=1,
+                           name="c4", extra={"maxDeltaT": "1e5", "rootTol": "1e-14"})
+    # the profiles are the knot interpolation itself (written as inputDir/a, b,
+    # Dc), so the base run and the forward map share their parameters
+    f = inspect_in(path, fields=("a", "b", "Dc"))
+    z = np.arange(n) / (n - 1.0) * 30.0
+    depths = np.linspace(0.0, 30.0, 40)
+    P = knot_matrix(z, depths)
+    base_k = [np.interp(depths, z, f[k]) for k in ("a", "b", "Dc")]
+    for nm, k in zip(("a", "b", "Dc"), base_k):
+        write_petsc_vec(path[:-len(".in")] + "_in_" + nm, P @ k)
+    # elliptic solves to 1e-14 and the friction root to 1e-14 MPa (rootTol):
+    # central differences at h = 1e-6 see the forward map's solver noise
+    # amplified by 1e6
+    rtol = 1e-14
+    run = QD.from_in(path, solve_rtol=rtol)
+    run.record_attempts(True)
+    run.integrate_begin_from_in()
+    run.integrate_steps(M)
+    dts = run.step_sizes()[:M]
+    run.close()
+    q = QD.from_in(path, solve_rtol=rtol)
+    q.integrate_begin_from_in()
+    adj = Adjoint(q, checkpoint_every=50)
+    adj.set_steps(dts)
+    rng = np.random.default_rng(100 + rank)
+    # small perturbations: the forward map follows the base run's step sizes,
+    # which a target trajectory far from it (an event at another time) would
+    # not survive
+    pert_k = [base_k[0] * (1 + 0.002 * rng.standard_normal(40)), base_k[1] * (1 + 0.002 * rng.standard_normal(40)),
+              base_k[2] * (1 + 0.005 * rng.standard_normal(40))]
+    adj.set_params(*[P @ k for k in pert_k])
+    adj.forward()
+    ts, tv = adj.observations()
+    ws, wv = 1.0 / np.mean(ts ** 2), 1.0 / np.mean(tv ** 2)
+    adj.set_targets(ts, tv, ws, wv)
+    base = [P @ k for k in base_k]
+    adj.set_params(*base)
+    adj.forward()  # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    J0 = adj.forward()
+    t_fwd = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    J, ga, gb, gd = adj.gradient()
+    t_grad = time.perf_counter() - t0
+    gk = [P.T @ g for g in (ga, gb, gd)]
+    h = 1e-6
+
+    def fd_errors(blocks, seed):
+        errs = []
+        drng = np.random.default_rng(seed)
+        for _ in range(args.c4_dirs):
+            d = [k * drng.standard_normal(40) if i in blocks else np.zeros(40) for i, k in enumerate(base_k)]
+            adj.set_params(*[P @ (k + h * e) for k, e in zip(base_k, d)])
+            jp = adj.forward()
+            adj.set_params(*[P @ (k - h * e) for k, e in zip(base_k, d)])
+            jm = adj.forward()
+            fd = (jp - jm) / (2 * h)
+            an = sum(g @ e for g, e in zip(gk, d))
+            errs.append(abs(fd - an) / max(abs(fd), abs(an), 1e-300))
+        return errs
+
+    errs = fd_errors((0, 1, 2), 7)
+    errs_ab = fd_errors((0, 1), 8)
+    adj.close()
+    q.close()
+    return {"workload": C4_WORKLOAD % M, "steps": M, "parameters": 120, "J": J, "J_forward": J0,
+            "forward_s": t_fwd, "gradient_s": t_grad, "gradient_over_forward": t_grad / t_fwd,
+            "fd_check": {"directions": args.c4_dirs, "h_relative": h, "max_rel_err": max(errs) if errs else None,
+                         "rel_errs": errs, "max_rel_err_a_b_only": max(errs_ab) if errs_ab else None,
+                         "note": "random directions in the 120 knot values; the Dc part of the gradient is small "
+                                 "near the steady-state start, so directions with a Dc component see the forward "
+                                 "map's round-off amplified by 1/h; directions in a and b alone are shown beside"},
+            "note": "gradient time = forward + recomputation of each checkpointed segment + reverse sweep (one "
+                    "transposed elliptic solve per stage); the initial state is held fixed"}
+
+
 def run_ours(args, dist, rank, world, local):
     import torch
     torch.cuda.set_device(local)
@@ -328,6 +424,11 @@ def run_ours(args, dist, rank, world, local):
     from scycle_b200 import _lib as S
     from scycle_b200.qd import QD
     L = S.lib()
+    if args.c4_only:
+        r = run_adjoint_c4(args, dist, rank, world, local)
+        if rank == 0:
+            print(json.dumps(r))
+        return
     if args.c3_only:
         r = run_ensemble_c3(args, dist, rank, world, local)
         if rank == 0:
@@ -463,6 +564,12 @@ def run_ours(args, dist, rank, world, local):
     q.close()
     batched = run_batched(args, dist, rank, world, local) if args.batch > 0 else None
     ensemble_c3 = run_ensemble_c3(args, dist, rank, world, local) if args.c3 > 0 else None
+    adjoint_c4 = None
+    if args.c4_steps > 0:
+        try:
+            adjoint_c4 = run_adjoint_c4(args, dist, rank, world, local)
+        except Exception as e:  # reported, not fatal to the headline
+            adjoint_c4 = {"error": str(e)}
     head = batched if batched else single
     config = {"workload": (BATCH_WORKLOAD % args.batch) if batched else WORKLOAD, "Ny": args.n, "Nz": args.n,
               "integrator": "RK32", "parallelism": "replicas x%d" % world}
@@ -485,7 +592,7 @@ def run_ours(args, dist, rank, world, local):
            "gpu_launches": head["gpu_launches"], "clocks": head["clocks"],
            "batched": batched, "fp64_single": single,
            "batched_vs_fp64_single_sim_years": (batched["sim_years_per_hour"] / syph) if batched else None,
-           "response_mode": resp, "cycle": cycle, "ensemble_c3": ensemble_c3}
+           "response_mode": resp, "cycle": cycle, "ensemble_c3": ensemble_c3, "adjoint_c4": adjoint_c4}
     if rank == 0:
         print(json.dumps(out))
 
@@ -669,6 +776,9 @@ def main():
     ap.add_argument("--batch-only", action="store_true", help="measure the batched ensemble alone")
     ap.add_argument("--c3", type=int, default=128, help="instances of the power-law ensemble (0: skip)")
     ap.add_argument("--c3-only", action="store_true", help="measure the power-law ensemble alone")
+    ap.add_argument("--c4-steps", type=int, default=2000, help="RK32 steps of the adjoint workload (0: skip)")
+    ap.add_argument("--c4-dirs", type=int, default=10, help="finite-difference directions of the adjoint check")
+    ap.add_argument("--c4-only", action="store_true", help="run the adjoint workload alone")
     ap.add_argument("--cycle-n", type=int, default=801)
     ap.add_argument("--cycle-mode", default="response", choices=["response", "solve"])
     ap.add_argument("--profile-stencil", type=int, default=0,

@@ -279,6 +279,10 @@ scy_status scy_qd_force_attempts(scy_qd* q, const double* dts, const int* accept
 scy_status scy_qd_record_attempts(scy_qd* q, int on);
 /* Copies the recorded attempts; *n receives their number. */
 scy_status scy_qd_get_attempts(scy_qd* q, double* dts, int* accept, long cap, long* n);
+/* While recording: per step taken, the size of the attempt whose solution
+ * was kept (the accepted attempt, or the last one when the step fell to the
+ * minimum size or the attempt cap); *n receives their number. */
+scy_status scy_qd_get_step_sizes(scy_qd* q, double* dts, long cap, long* n);
 
 enum {
   SCY_FIELD_PSI = 0, SCY_FIELD_SLIP = 1, SCY_FIELD_SLIPVEL = 2, SCY_FIELD_TAUP = 3,

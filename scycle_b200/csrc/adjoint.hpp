@@ -21,7 +21,11 @@
 //   * the states are checkpointed every `ck` steps; each segment is
 //     recomputed forward (storing psi, V and tau at every stage) before its
 //     reverse sweep.
-// The initial state is taken as independent of the parameters.
+// The initial state is taken as independent of the parameters.  Each step
+// advances state and time by the same size; where the reference kept a
+// larger rejected attempt's solution while advancing time by minDeltaT
+// (odeSolver.cpp:580-592), the map here advances time by the attempt's size.
+// The step sizes come from scy_qd_get_step_sizes of the run.
 #pragma once
 #include <vector>
 

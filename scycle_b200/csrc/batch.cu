@@ -1163,22 +1163,24 @@ void BatchContext::consume(int i, double totErr) {
   QDContext& c = q(i);
   bool acc = c.ode.method == SCY_RK32 ? (totErr <= c.totTol) : (totErr < c.totTol);
   if (h.forced) acc = h.forced_accept != 0;
+  const double used = c.deltaT;
   if (c.record) {
     c.log_dt.push_back(c.deltaT);
     c.log_acc.push_back(acc ? 1 : 0);
   }
-  if (acc) return finish_step(i, totErr);
+  if (acc) return finish_step(i, totErr, used);
   double nd = c.compute_step_size(totErr);
   if (!h.forced) c.deltaT = nd;
-  if (c.ode.min_dt == c.deltaT) return finish_step(i, totErr);
+  if (c.ode.min_dt == c.deltaT) return finish_step(i, totErr, used);
   ++c.numRejected;
-  if (h.attemptCount >= 100) return finish_step(i, totErr);
+  if (h.attemptCount >= 100) return finish_step(i, totErr, used);
   begin_attempt(i);
 }
 
-void BatchContext::finish_step(int i, double totErr) {
+void BatchContext::finish_step(int i, double totErr, double used_dt) {
   Ctl& h = hc[i];
   QDContext& c = q(i);
+  if (c.record) c.log_step_dt.push_back(used_dt);
   c.currT = c.currT + c.deltaT;
   h.copy = h.acc = 1;  // var = hi and the rates there, at the start of the next round
   if (totErr != 0.0) c.newDeltaT = c.compute_step_size(totErr);

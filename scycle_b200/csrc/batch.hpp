@@ -138,7 +138,7 @@ struct BatchContext {
   void begin_step(int i);
   void begin_attempt(int i);
   void consume(int i, double totErr);
-  void finish_step(int i, double totErr);
+  void finish_step(int i, double totErr, double used_dt);
   const int* d_copy(const BatchGroup& g) const;
   const int* d_acc(const BatchGroup& g) const;
   const int* d_run(const BatchGroup& g) const;

@@ -291,6 +291,7 @@ scy_status scy_qd_record_attempts(scy_qd* q, int on) {
   if (on) {
     q->ctx.log_dt.clear();
     q->ctx.log_acc.clear();
+    q->ctx.log_step_dt.clear();
   }
   return SCY_OK;
 }
@@ -303,6 +304,15 @@ scy_status scy_qd_get_attempts(scy_qd* q, double* dts, int* acc, long cap, long*
     if (dts) dts[i] = q->ctx.log_dt[i];
     if (acc) acc[i] = q->ctx.log_acc[i];
   }
+  return SCY_OK;
+}
+
+scy_status scy_qd_get_step_sizes(scy_qd* q, double* dts, long cap, long* n) {
+  if (!q || !n) return SCY_ERR_ARG;
+  const long m = (long)q->ctx.log_step_dt.size();
+  *n = m;
+  for (long i = 0; i < m && i < cap; ++i)
+    if (dts) dts[i] = q->ctx.log_step_dt[i];
   return SCY_OK;
 }
 
@@ -740,6 +750,7 @@ scy_status scy_cycle_record_attempts(scy_cycle* c, int on) {
   if (on) {
     q.log_dt.clear();
     q.log_acc.clear();
+    q.log_step_dt.clear();
   }
   return SCY_OK;
 }

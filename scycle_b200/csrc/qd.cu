@@ -745,7 +745,7 @@ int QDContext::integrate_steps(long nsteps, scy_ode_stats* st) {
   double* dvar = rk[V_DVAR].as<double>();
   const long n = nvar;
   long done_steps = 0;
-  double totErr = 0.0;
+  double totErr = 0.0, used_dt = 0.0;
   while (done_steps < nsteps && stepCount < ode.max_steps && currT < ode.t1) {
     ++stepCount;
     int attemptCount = 0;
@@ -761,6 +761,7 @@ int QDContext::integrate_steps(long nsteps, scy_ode_stats* st) {
         ++forced_pos;
       }
       SCY_TRY(attempt(deltaT, &lo, &hi));
+      used_dt = deltaT;
       SCY_TRY(compute_error(lo, hi, &totErr));
       SCY_TRY(read_flags());
       bool acc = ode.method == SCY_RK32 ? (totErr <= totTol) : (totErr < totTol);
@@ -776,6 +777,7 @@ int QDContext::integrate_steps(long nsteps, scy_ode_stats* st) {
       ++numRejected;
     }
     // accept the higher-order solution (odeSolver.cpp:599-603, :1148-1152)
+    if (record) log_step_dt.push_back(used_dt);
     currT = currT + deltaT;
     SCY_CUDA_TRY(cudaMemcpyAsync(var, hi, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
     SCY_TRY(d_dt(currT, var, dvar));

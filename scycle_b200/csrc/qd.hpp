@@ -59,6 +59,7 @@ struct QDContext {
   size_t forced_pos = 0;
   std::vector<double> log_dt;
   std::vector<int> log_acc;
+  std::vector<double> log_step_dt;  // per taken step, the size of the attempt whose solution was kept
   int record = 0;
 
   std::vector<double> h_a, h_b, h_sN;  // host copies for the steady-state guess

@@ -158,6 +158,15 @@ class QD:
     def record_attempts(self, on=True):
         S.check(S.lib().scy_qd_record_attempts(self.h, 1 if on else 0))
 
+    def step_sizes(self):
+        """Per step taken while recording, the size of the attempt whose
+        solution was kept."""
+        n = C.c_long()
+        S.check(S.lib().scy_qd_get_step_sizes(self.h, None, 0, C.byref(n)))
+        d = np.empty(n.value)
+        S.check(S.lib().scy_qd_get_step_sizes(self.h, S.as_dptr(d), n.value, C.byref(n)))
+        return d
+
     def attempts(self):
         n = C.c_long()
         S.check(S.lib().scy_qd_get_attempts(self.h, None, None, 0, C.byref(n)))

@@ -35,7 +35,7 @@ def _setup(path, steps=STEPS, ck=10):
     run.record_attempts(True)
     run.integrate_begin_from_in()
     run.integrate_steps(steps)
-    dts = [d for d, acc in run.attempts() if acc]
+    dts = run.step_sizes()
     assert len(dts) == steps
     q = QD.from_in(path, solve_rtol=SOLVE_RTOL)
     q.integrate_begin_from_in()
