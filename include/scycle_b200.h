@@ -306,6 +306,20 @@ scy_status scy_qd_get_problem(scy_qd* q, int* Ny, int* Nz, scy_ode_opts* ode);
  * initiateIntegrand (with the steady-state guess when the file asks for it,
  * strikeSlip_linearElastic_qd.cpp:377-413) and the first d_dt. */
 scy_status scy_qd_integrate_begin_from_in(scy_qd* q);
+/* Output at the reference's strides (timeMonitor with writeStep1D/2D of the
+ * driver, LinearElastic and Fault, strikeSlip_linearElastic_qd.cpp:417-495,
+ * linearElastic.cpp:623-686, fault.cpp:512-557): PETSc-binary Vec records
+ * appended to files named output_dir + field (surfDisp, momBal_bcR/T/L/B,
+ * momBal_bcRShift, slip, slipVel, tauP, tauQSP, strength, psi, sNEff; with
+ * stride2D momBal_u, momBal_sxy) and med_time1D/2D.txt, med_dt1D/2D.txt, at
+ * step 0 (before the first rates) and every stride-th accepted step.  The
+ * copies are queued on the driver's stream and written by a worker thread.
+ * stride1D = stride2D = 0 or output_dir = NULL: no output.  append = 1
+ * continues existing files.  scy_qd_integrate_begin_from_in turns it on from
+ * the file's outputDir / stride1D / stride2D (linear-elastic driver). */
+scy_status scy_qd_set_output(scy_qd* q, const char* output_dir, int stride1D, int stride2D, int append);
+/* Waits until every queued output step is in its files. */
+scy_status scy_qd_flush_output(scy_qd* q);
 /* Host-only inspection of an input file (no GPU needed): the derived array
  * `name` ("y", "z", "mu", "rho", "cs", "a", "b", "sN", "Dc", "psi",
  * "locked", "prestress", "eta", "bcL", "bcRShift") is copied to out (cap

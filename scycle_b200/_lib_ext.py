@@ -49,6 +49,8 @@ def declare(L):
     L.scy_qd_record_attempts.argtypes = [vp, C.c_int]
     L.scy_qd_get_attempts.argtypes = [vp, dptr, C.POINTER(C.c_int), C.c_long, C.POINTER(C.c_long)]
     L.scy_qd_get_step_sizes.argtypes = [vp, dptr, C.c_long, C.POINTER(C.c_long)]
+    L.scy_qd_set_output.argtypes = [vp, C.c_char_p, C.c_int, C.c_int, C.c_int]
+    L.scy_qd_flush_output.argtypes = [vp]
     L.scy_qd_get_field.argtypes = [vp, C.c_int, dptr]
     L.scy_qd_create_from_in.argtypes = [C.c_char_p, C.POINTER(S.SolveOpts), C.POINTER(vp)]
     L.scy_qd_get_problem.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(OdeOpts)]

@@ -674,7 +674,10 @@ int BatchContext::create(int n_inst, const char* const* paths, const scy_solve_o
     for (size_t k = 1; k < m.size(); ++k) q(base + (int)k).sbp.fd = q(base).sbp.fd;
     base += (int)m.size();
   }
-  // begin every instance (initial state and first rates on its own solver)
+  // begin every instance (initial state and first rates on its own solver);
+  // the batch writes no stride output (fields come through scy_qd_get_field
+  // and scy_batch_get_fault_field)
+  for (int s = 0; s < n; ++s) inst[s]->prob->stride1D = inst[s]->prob->stride2D = 0;
   for (int s = 0; s < n; ++s) {
     int rc = scy_qd_integrate_begin_from_in(inst[s]);
     if (rc != SCY_OK) {

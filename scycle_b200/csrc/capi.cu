@@ -456,7 +456,30 @@ scy_status scy_qd_integrate_begin_from_in(scy_qd* q) {
   SCY_CUDA_TRY(cudaMemcpyAsync(c.rk[0].p, var0.data(), var0.size() * sizeof(double), cudaMemcpyHostToDevice,
                                c.sbp.stream));
   SCY_CUDA_TRY(cudaStreamSynchronize(c.sbp.stream));
+  // the file's output settings (stride1D / stride2D under outputDir), as the
+  // reference's timeMonitor writes them
+  if (!P.pl && !c.out && (P.stride1D > 0 || P.stride2D > 0))
+    SCY_TRY(scy_qd_set_output(q, P.outputDir.c_str(), P.stride1D, P.stride2D, 0));
   return c.integrate_begin(P.ode);
+}
+
+scy_status scy_qd_set_output(scy_qd* q, const char* output_dir, int stride1D, int stride2D, int append) {
+  if (!q) return SCY_ERR_ARG;
+  scy::QDContext& c = q->ctx;
+  if (c.out) SCY_TRY(c.out->flush());
+  c.out.reset();
+  if (!output_dir || (stride1D <= 0 && stride2D <= 0)) return SCY_OK;
+  std::unique_ptr<scy::OutputWriter> w(new (std::nothrow) scy::OutputWriter());
+  if (!w) return SCY_ERR_NOMEM;
+  const double tmax = q->prob ? q->prob->ode.t1 : c.ode.t1;
+  SCY_TRY(w->open(output_dir, stride1D, stride2D, tmax, append ? 1 : 0, c));
+  c.out = std::move(w);
+  return SCY_OK;
+}
+
+scy_status scy_qd_flush_output(scy_qd* q) {
+  if (!q) return SCY_ERR_ARG;
+  return q->ctx.out ? q->ctx.out->flush() : SCY_OK;
 }
 
 scy_status scy_qd_set_mode(scy_qd* q, int mode) {

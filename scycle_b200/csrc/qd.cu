@@ -703,6 +703,9 @@ int QDContext::integrate_begin(const scy_ode_opts& o) {
   errA[0] = errA[1] = 0.0;
   if (deltaT == 0) deltaT = (o.t1 - o.t0) / (double)o.max_steps;
   ode_ready = 1;
+  // the driver's timeMonitor(initTime, initDeltaT, 0) before integrating
+  // (strikeSlip_linearElastic_qd.cpp:733-735)
+  if (out) SCY_TRY(out->on_step(*this, stepCount, currT, o.init_dt));
   // first evaluation of the rates (odeSolver.cpp:545)
   SCY_TRY(d_dt(currT, rk[V_VAR].as<double>(), rk[V_DVAR].as<double>()));
   return read_flags();
@@ -783,6 +786,7 @@ int QDContext::integrate_steps(long nsteps, scy_ode_stats* st) {
     SCY_TRY(d_dt(currT, var, dvar));
     SCY_TRY(read_flags());
     if (totErr != 0.0) newDeltaT = compute_step_size(totErr);
+    if (out) SCY_TRY(out->on_step(*this, stepCount, currT, deltaT));
     errA[1] = errA[0];
     errA[0] = totErr;
     last_dt = deltaT;

@@ -2,10 +2,12 @@
 // StrikeSlip_LinearElastic_qd and the adaptive RK32 / RK43 integrators.
 #pragma once
 #include <functional>
+#include <memory>
 #include <vector>
 
 #include "fault_dev.cuh"
 #include "sbp_solver.hpp"
+#include "writer.hpp"
 
 namespace scy {
 
@@ -60,6 +62,8 @@ struct QDContext {
   std::vector<double> log_dt;
   std::vector<int> log_acc;
   std::vector<double> log_step_dt;  // per taken step, the size of the attempt whose solution was kept
+  // timeMonitor's output at the reference's strides (writer.cu); null: none
+  std::unique_ptr<OutputWriter> out;
   int record = 0;
 
   std::vector<double> h_a, h_b, h_sN;  // host copies for the steady-state guess

@@ -158,6 +158,14 @@ class QD:
     def record_attempts(self, on=True):
         S.check(S.lib().scy_qd_record_attempts(self.h, 1 if on else 0))
 
+    def set_output(self, output_dir, stride1D=1, stride2D=0, append=False):
+        """PETSc-binary output at the reference's strides (None: off)."""
+        d = None if output_dir is None else str(output_dir).encode()
+        S.check(S.lib().scy_qd_set_output(self.h, d, int(stride1D), int(stride2D), 1 if append else 0))
+
+    def flush_output(self):
+        S.check(S.lib().scy_qd_flush_output(self.h))
+
     def step_sizes(self):
         """Per step taken while recording, the size of the attempt whose
         solution was kept."""
