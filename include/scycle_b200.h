@@ -266,7 +266,8 @@ typedef struct scy_ode_stats {
   double t, dt, new_dt;
   long step_count, rejected, d_dt_evals, solve_its, solves;
   double errA[2];       /* errA[0] newest accepted error */
-  int done;             /* 1: reached t1 or max_steps */
+  int done;             /* 1: reached t1 or max_steps; 2: stopped after writing a checkpoint
+                           (enableCheckpointing, as the reference's run ends there) */
 } scy_ode_stats;
 
 /* OdeSolver setInitialConds + the first d_dt.  var0 = [psi | slip] host. */
@@ -304,7 +305,12 @@ scy_status scy_qd_create_from_in(const char* path, const scy_solve_opts* solve, 
 scy_status scy_qd_get_problem(scy_qd* q, int* Ny, int* Nz, scy_ode_opts* ode);
 /* integrate()'s set-up for a driver made by scy_qd_create_from_in:
  * initiateIntegrand (with the steady-state guess when the file asks for it,
- * strikeSlip_linearElastic_qd.cpp:377-413) and the first d_dt. */
+ * strikeSlip_linearElastic_qd.cpp:377-413) and the first d_dt.  With
+ * enableCheckpointing > 0 and a checkpoint in outputDir (ckptNumber > 0) the
+ * run restarts from its chkpt_* files (time, step size, step count, error
+ * history, state, slip velocity, stresses, boundary data) and appends to the
+ * output files; checkpoints are written at step 0, every `interval` steps
+ * and at the end, after which scy_qd_integrate_steps returns with done = 2. */
 scy_status scy_qd_integrate_begin_from_in(scy_qd* q);
 /* Output at the reference's strides (timeMonitor with writeStep1D/2D of the
  * driver, LinearElastic and Fault, strikeSlip_linearElastic_qd.cpp:417-495,

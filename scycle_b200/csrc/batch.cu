@@ -677,7 +677,13 @@ int BatchContext::create(int n_inst, const char* const* paths, const scy_solve_o
   // begin every instance (initial state and first rates on its own solver);
   // the batch writes no stride output (fields come through scy_qd_get_field
   // and scy_batch_get_fault_field)
-  for (int s = 0; s < n; ++s) inst[s]->prob->stride1D = inst[s]->prob->stride2D = 0;
+  for (int s = 0; s < n; ++s) {
+    inst[s]->prob->stride1D = inst[s]->prob->stride2D = 0;
+    if (inst[s]->prob->ckpt) {
+      set_error("instance %d: checkpointing (enableCheckpointing) is not available in a batch", user_of[s]);
+      return SCY_ERR_ARG;
+    }
+  }
   for (int s = 0; s < n; ++s) {
     int rc = scy_qd_integrate_begin_from_in(inst[s]);
     if (rc != SCY_OK) {

@@ -447,6 +447,10 @@ scy_status scy_qd_integrate_begin_from_in(scy_qd* q) {
     if (!P.slip_file.empty()) slip = P.slip_file;
     std::copy(P.gVxy0.begin(), P.gVxy0.end(), var0.begin() + c.key_off[SCY_KEY_GVXY]);
     std::copy(P.gVxz0.begin(), P.gVxz0.end(), var0.begin() + c.key_off[SCY_KEY_GVXZ]);
+  } else if (P.ckpt_number > 0) {
+    slip = P.slip_file;  // a restart: the checkpoint's state
+    if (!P.slipVel0.empty())
+      SCY_CUDA_TRY(cudaMemcpy(c.slipVel.p, P.slipVel0.data(), Nz * sizeof(double), cudaMemcpyHostToDevice));
   } else {
     for (int i = 0; i < Nz; ++i) slip[i] = P.bcL0[i] * P.desc.fault_type_scale;
     if (P.guess_ss) SCY_TRY(c.steady_state_guess(psi, P.stateVals_given, slip));
@@ -459,8 +463,22 @@ scy_status scy_qd_integrate_begin_from_in(scy_qd* q) {
   // the file's output settings (stride1D / stride2D under outputDir), as the
   // reference's timeMonitor writes them
   if (!P.pl && !c.out && (P.stride1D > 0 || P.stride2D > 0))
-    SCY_TRY(scy_qd_set_output(q, P.outputDir.c_str(), P.stride1D, P.stride2D, 0));
-  return c.integrate_begin(P.ode);
+    SCY_TRY(scy_qd_set_output(q, P.outputDir.c_str(), P.stride1D, P.stride2D, P.ckpt_number > 0 ? 1 : 0));
+  if (!P.pl && P.ckpt > 0) {
+    c.ckpt = P.ckpt;
+    c.ckpt_interval = P.ckpt_interval;
+    c.ckpt_number = P.ckpt_number;
+    c.ckpt_dir = P.outputDir;
+  }
+  SCY_TRY(c.integrate_begin(P.ode));
+  if (P.ckpt_number > 0) {
+    // the restarted integrator continues the step count and the error history
+    // (strikeSlip_linearElastic_qd.cpp:734-738)
+    c.stepCount = P.step0;
+    c.errA[0] = P.errA[0];
+    c.errA[1] = P.errA[1];
+  }
+  return SCY_OK;
 }
 
 scy_status scy_qd_set_output(scy_qd* q, const char* output_dir, int stride1D, int stride2D, int append) {

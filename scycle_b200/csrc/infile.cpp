@@ -162,6 +162,16 @@ static int parse_bc(const std::string& t) {
   throw std::runtime_error("unknown boundary condition type '" + t + "'");
 }
 
+// First number of a PETSc ASCII value file (loadValueFromCheckpoint,
+// genFuncs.cpp:889-935); `fallback` when the file is absent.
+static double read_ascii_value(const std::string& path, double fallback) {
+  if (!file_exists(path)) return fallback;
+  std::ifstream f(path);
+  double v = fallback;
+  if (!(f >> v)) throw std::runtime_error("cannot read a value from " + path);
+  return v;
+}
+
 void load_qd_problem(const std::string& path, QDProblem& P, int cycle) {
   const std::vector<InEntry> E = parse_in_file(path);
   // ---- Domain (domain.cpp:8-16, :133-196, :233-262)
@@ -185,7 +195,10 @@ void load_qd_problem(const std::string& path, QDProblem& P, int cycle) {
     else if (e.var == "momentumBalanceType") momBal = e.rhs;
     else if (e.var == "bCoordTrans") bCoordTrans = c_atof(e.rhs);
     else if (e.var == "vL") vL_dom = c_atof(e.rhs);
+    else if (e.var == "enableCheckpointing") P.ckpt = c_atoi(e.rhs);
+    else if (e.var == "interval") P.ckpt_interval = (long)c_atof(e.rhs);
   }
+  if (P.ckpt < 0 || P.ckpt_interval < 0) throw std::runtime_error("invalid enableCheckpointing / interval");
   if (bCoordTrans > 0.0) gridType = "variableGridSpacing";
   P.pl = (!cycle && bulk == "powerLaw") ? 1 : 0;
   if (bulk != "linearElastic" && !P.pl)
@@ -386,6 +399,29 @@ void load_qd_problem(const std::string& path, QDProblem& P, int cycle) {
   P.bcRShift.assign(Nz, 0.0);
   read_petsc_vec(P.inputDir + "momBal_bcL", Nz, P.bcL0);
   read_petsc_vec(P.inputDir + "momBal_bcR", Nz, P.bcRShift);
+  // a restart: the driver's, the material's and the fault's checkpoint files
+  // (StrikeSlip_LinearElastic_qd ctor :33-39, LinearElastic::loadCheckpoint
+  // :396-410, Fault::loadCheckpoint fault.cpp:144-166); the rate-and-state
+  // parameters come from this file as for the first run
+  if (P.ckpt > 0 && !cycle && !P.pl) {
+    P.ckpt_number = (int)read_ascii_value(P.outputDir + "ckptNumber", 0.0);
+    if (P.ckpt_number > 0) {
+      initTime = read_ascii_value(P.outputDir + "chkpt_currT", initTime);
+      initDeltaT = read_ascii_value(P.outputDir + "chkpt_deltaT", initDeltaT);
+      P.step0 = (long)read_ascii_value(P.outputDir + "chkpt_stepCount", 0.0);
+      P.errA[1] = read_ascii_value(P.outputDir + "chkpt_prevErr", 0.0);
+      P.errA[0] = read_ascii_value(P.outputDir + "chkpt_currErr", 0.0);
+      P.guess_ss = 0;
+      const std::string c = P.outputDir + "chkpt_";
+      read_petsc_vec(c + "psi", Nz, P.psi);
+      if (!read_petsc_vec(c + "slip", Nz, P.slip_file)) throw std::runtime_error("checkpoint without chkpt_slip");
+      if (!read_petsc_vec(c + "slipVel", Nz, P.slipVel0)) P.slipVel0.clear();
+      read_petsc_vec(c + "sNEff", Nz, P.sN);
+      read_petsc_vec(c + "prestress", Nz, P.prestress);
+      read_petsc_vec(c + "momBal_bcRShift", Nz, P.bcRShift);
+      read_petsc_vec(c + "momBal_bcL", Nz, P.bcL0);
+    }
+  }
   // descriptor
   scy_qd_desc& d = P.desc;
   d.grid.order = order;

@@ -54,6 +54,14 @@ struct QDProblem {
   int cycle = 0;
   scy_cycle_desc cdesc{};
   std::vector<double> slip_file;  // inputDir/slip, empty if absent
+  // checkpointing (Domain enableCheckpointing / interval, domain.cpp:17-28,
+  // :187-188); a restart (ckptNumber > 0 in outputDir) starts from the
+  // chkpt_* files written by the previous run
+  int ckpt = 0, ckpt_number = 0;
+  long ckpt_interval = 10000;
+  long step0 = 0;
+  double errA[2] = {0.0, 0.0};
+  std::vector<double> slipVel0;  // chkpt_slipVel (first guess of the root finder), empty if none
 };
 
 // Builds the problem like Domain + LinearElastic + Fault_qd +

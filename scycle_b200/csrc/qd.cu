@@ -12,6 +12,7 @@
 
 #include "common.cuh"
 #include "fault_node.cuh"
+#include "infile.hpp"
 #include "qd.hpp"
 
 namespace scy {
@@ -705,7 +706,8 @@ int QDContext::integrate_begin(const scy_ode_opts& o) {
   ode_ready = 1;
   // the driver's timeMonitor(initTime, initDeltaT, 0) before integrating
   // (strikeSlip_linearElastic_qd.cpp:733-735)
-  if (out) SCY_TRY(out->on_step(*this, stepCount, currT, o.init_dt));
+  if (out) SCY_TRY(out->on_step(*this, 0, currT, o.init_dt));
+  if (ckpt > 0) SCY_TRY(write_checkpoint());  // stepCount 0: 0 % interval == 0
   // first evaluation of the rates (odeSolver.cpp:545)
   SCY_TRY(d_dt(currT, rk[V_VAR].as<double>(), rk[V_DVAR].as<double>()));
   return read_flags();
@@ -747,6 +749,7 @@ int QDContext::integrate_steps(long nsteps, scy_ode_stats* st) {
   double* var = rk[V_VAR].as<double>();
   double* dvar = rk[V_DVAR].as<double>();
   const long n = nvar;
+  ckpt_stopped = 0;
   long done_steps = 0;
   double totErr = 0.0, used_dt = 0.0;
   while (done_steps < nsteps && stepCount < ode.max_steps && currT < ode.t1) {
@@ -786,11 +789,19 @@ int QDContext::integrate_steps(long nsteps, scy_ode_stats* st) {
     SCY_TRY(d_dt(currT, var, dvar));
     SCY_TRY(read_flags());
     if (totErr != 0.0) newDeltaT = compute_step_size(totErr);
-    if (out) SCY_TRY(out->on_step(*this, stepCount, currT, deltaT));
     errA[1] = errA[0];
     errA[0] = totErr;
     last_dt = deltaT;
     ++done_steps;
+    // timeMonitor (odeSolver.cpp:608): output, then a checkpoint that ends the run
+    if (out) SCY_TRY(out->on_step(*this, stepCount, currT, deltaT));
+    if (ckpt > 0 && ((ckpt_interval > 0 && stepCount % ckpt_interval == 0) || stepCount >= ode.max_steps ||
+                     currT >= ode.t1)) {
+      SCY_TRY(write_checkpoint());
+      ckpt_stopped = 1;
+      deltaT = newDeltaT;  // as a run restarted from the checkpoint would take it
+      break;
+    }
     if (monitor) {
       int stop = 0;
       SCY_TRY(monitor(&stop));
@@ -812,7 +823,76 @@ int QDContext::integrate_steps(long nsteps, scy_ode_stats* st) {
     st->solves = n_solves;
     st->errA[0] = errA[0];
     st->errA[1] = errA[1];
-    st->done = (stepCount >= ode.max_steps || currT >= ode.t1) ? 1 : 0;
+    st->done = ckpt_stopped ? 2 : (stepCount >= ode.max_steps || currT >= ode.t1) ? 1 : 0;
+  }
+  return SCY_OK;
+}
+
+// StrikeSlip_LinearElastic_qd::writeCheckpoint (:527-556), LinearElastic::
+// writeCheckpoint (linearElastic.cpp:689-702) and Fault::writeCheckpoint
+// (fault.cpp:561-578): the step's scalars as ASCII, the fields as PETSc
+// binary Vecs, all under ckpt_dir.
+int QDContext::write_checkpoint() {
+  cudaStream_t s = sbp.stream;
+  if (out) SCY_TRY(out->flush());
+  auto get = [&](const void* src, size_t n, std::vector<double>& h) -> int {
+    h.resize(n);
+    SCY_CUDA_TRY(cudaMemcpyAsync(h.data(), src, n * 8, cudaMemcpyDeviceToHost, s));
+    return SCY_OK;
+  };
+  std::vector<double> slip, vel, psi, sn, tau, tq, pre, bR, bS, bT, bL, bB;
+  const double* var = rk[V_VAR].as<double>();
+  SCY_TRY(get(var + fp.slip_off, Nz, slip));
+  SCY_TRY(get(slipVel.p, Nz, vel));
+  SCY_TRY(get(var + fp.psi_off, Nz, psi));
+  SCY_TRY(get(fsN.p, Nz, sn));
+  SCY_TRY(get(tauP.p, Nz, tau));
+  SCY_TRY(get(tauQSP.p, Nz, tq));
+  SCY_TRY(get(fprestress.p, Nz, pre));
+  SCY_TRY(get(bcR.p, Nz, bR));
+  SCY_TRY(get(bcRShift.p, Nz, bS));
+  SCY_TRY(get(bcT.p, Ny, bT));
+  SCY_TRY(get(bcL.p, Nz, bL));
+  SCY_TRY(get(bcB.p, Ny, bB));
+  SCY_CUDA_TRY(cudaStreamSynchronize(s));
+  ++ckpt_number;
+  auto ascii = [&](const char* name, const char* fmt, double v, bool integer) -> int {
+    FILE* f = fopen((ckpt_dir + name).c_str(), "w");
+    if (!f) {
+      set_error("cannot write %s%s", ckpt_dir.c_str(), name);
+      return SCY_ERR_IO;
+    }
+    if (integer)
+      fprintf(f, fmt, (long)v);
+    else
+      fprintf(f, fmt, v);
+    fclose(f);
+    return SCY_OK;
+  };
+  SCY_TRY(ascii("ckptNumber", "%ld\n", ckpt_number, true));
+  SCY_TRY(ascii("chkpt_currT", "%.15e\n", currT, false));
+  SCY_TRY(ascii("chkpt_stepCount", "%ld\n", (double)stepCount, true));
+  SCY_TRY(ascii("chkpt_prevErr", "%.15e\n", errA[1], false));
+  SCY_TRY(ascii("chkpt_currErr", "%.15e\n", errA[0], false));
+  SCY_TRY(ascii("chkpt_deltaT", "%.15e\n", newDeltaT, false));
+  try {
+    const std::string c = ckpt_dir + "chkpt_";
+    write_petsc_vec(c + "momBal_bcR", bR.data(), Nz, 0);
+    write_petsc_vec(c + "momBal_bcRShift", bS.data(), Nz, 0);
+    write_petsc_vec(c + "momBal_bcT", bT.data(), Ny, 0);
+    write_petsc_vec(c + "momBal_bcL", bL.data(), Nz, 0);
+    write_petsc_vec(c + "momBal_bcB", bB.data(), Ny, 0);
+    write_petsc_vec(c + "slip", slip.data(), Nz, 0);
+    write_petsc_vec(c + "slipVel", vel.data(), Nz, 0);
+    write_petsc_vec(c + "psi", psi.data(), Nz, 0);
+    write_petsc_vec(c + "sNEff", sn.data(), Nz, 0);
+    write_petsc_vec(c + "sN", sn.data(), Nz, 0);
+    write_petsc_vec(c + "tau", tau.data(), Nz, 0);
+    write_petsc_vec(c + "tauQS", tq.data(), Nz, 0);
+    write_petsc_vec(c + "prestress", pre.data(), Nz, 0);
+  } catch (const std::exception& e) {
+    set_error("%s", e.what());
+    return SCY_ERR_IO;
   }
   return SCY_OK;
 }

@@ -3,6 +3,7 @@
 #pragma once
 #include <functional>
 #include <memory>
+#include <string>
 #include <vector>
 
 #include "fault_dev.cuh"
@@ -64,6 +65,14 @@ struct QDContext {
   std::vector<double> log_step_dt;  // per taken step, the size of the attempt whose solution was kept
   // timeMonitor's output at the reference's strides (writer.cu); null: none
   std::unique_ptr<OutputWriter> out;
+  // checkpointing (timeMonitor :448-455 with writeCheckpoint of the driver,
+  // LinearElastic and Fault): every ckpt_interval steps and at the end, the
+  // chkpt_* files under ckpt_dir, after which integrate_steps returns with
+  // done = 2 (the reference stops the run there)
+  int ckpt = 0, ckpt_number = 0, ckpt_stopped = 0;
+  long ckpt_interval = 10000;
+  std::string ckpt_dir;
+  int write_checkpoint();
   int record = 0;
 
   std::vector<double> h_a, h_b, h_sN;  // host copies for the steady-state guess
