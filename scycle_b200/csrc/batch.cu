@@ -24,6 +24,7 @@
 #include "common.cuh"
 #include "fault_node.cuh"
 #include "powerlaw_dev.cuh"
+#include "tma.cuh"
 
 namespace scy {
 
@@ -347,10 +348,12 @@ __global__ void b_scale_kernel(T* __restrict__ x, const T* __restrict__ s, long 
 template <typename T, int R, int RB>
 __global__ void __launch_bounds__(128) b_ysolve_kernel(const T* __restrict__ Lb, T* __restrict__ t, int Ny, int Nz,
                                                        int K) {
-  // A thread sweeps the systems of one z mode j for R instances at once:
-  // every factor coefficient is loaded once for the R sweeps, and the rows
-  // are taken RB at a time (their loads issued together, so one memory
-  // latency covers RB steps of the R sweeps).
+  // A thread sweeps the systems of one z mode j for R instances at once
+  // (every factor coefficient loaded once for the R sweeps), rows taken RB
+  // at a time (their loads issued together).  Both sweeps run column by
+  // column: as soon as a value is known, its column of the factor is added
+  // into the partial sums of the next eight rows (acc), so a row waits only
+  // for one multiply-add on the previous row's value.
   const int KR = (K + R - 1) / R;
   const long g = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (g >= (long)Nz * KR) return;
@@ -359,20 +362,20 @@ __global__ void __launch_bounds__(128) b_ysolve_kernel(const T* __restrict__ Lb,
   T* col = t + (long)k0 * NN + j;
   const int nr = min(R, K - k0);
   const T* L = Lb + j;
-  T w[R][8];
+  T acc[R][8];
 #pragma unroll
   for (int q = 0; q < R; ++q)
 #pragma unroll
-    for (int m = 0; m < 8; ++m) w[q][m] = T(0);
-  // forward: y(i) = (b(i) - sum_m L(i, i-m) y(i-m)) / L(i, i); w[q][m-1] = y(i-m)
+    for (int m = 0; m < 8; ++m) acc[q][m] = T(0);
+  // forward, L y = b: y(i) = (b(i) - acc(i)) / L(i, i), then acc(i+m) += L(i+m, i) y(i)
   for (int i0 = 0; i0 < Ny; i0 += RB) {
     T cf[RB][9], bv[RB][R];
 #pragma unroll
     for (int r = 0; r < RB; ++r) {
-      const int i = i0 + r;
-      const T* row = L + (long)i * 9 * Nz;  // rows up to Ny + 7 exist (zero padded)
+      const int i = i0 + r;  // rows up to Ny + RB + 7 are read: the table has Ny + 8 rows, see below
+      cf[r][0] = i < Ny ? L[(long)i * 9 * Nz] : T(0);
 #pragma unroll
-      for (int m = 0; m < 9; ++m) cf[r][m] = row[(long)m * Nz];
+      for (int m = 1; m <= 8; ++m) cf[r][m] = i < Ny ? L[((long)(i + m) * 9 + m) * Nz] : T(0);
 #pragma unroll
       for (int q = 0; q < R; ++q) bv[r][q] = (i < Ny && q < nr) ? col[q * NN + (long)i * Nz] : T(0);
     }
@@ -382,14 +385,11 @@ __global__ void __launch_bounds__(128) b_ysolve_kernel(const T* __restrict__ Lb,
       if (i < Ny) {
 #pragma unroll
         for (int q = 0; q < R; ++q) {
-          T s = bv[r][q];
-#pragma unroll
-          for (int m = 8; m >= 1; --m) s -= cf[r][m] * w[q][m - 1];
-          const T y = s * cf[r][0];
+          const T y = (bv[r][q] - acc[q][0]) * cf[r][0];
           if (q < nr) col[q * NN + (long)i * Nz] = y;
 #pragma unroll
-          for (int m = 7; m >= 1; --m) w[q][m] = w[q][m - 1];
-          w[q][0] = y;
+          for (int m = 0; m < 7; ++m) acc[q][m] = acc[q][m + 1] + cf[r][m + 1] * y;
+          acc[q][7] = cf[r][8] * y;
         }
       }
     }
@@ -397,17 +397,16 @@ __global__ void __launch_bounds__(128) b_ysolve_kernel(const T* __restrict__ Lb,
 #pragma unroll
   for (int q = 0; q < R; ++q)
 #pragma unroll
-    for (int m = 0; m < 8; ++m) w[q][m] = T(0);
-  // back: x(i) = (y(i) - sum_m L(i+m, i) x(i+m)) / L(i, i); w[q][m-1] = x(i+m)
+    for (int m = 0; m < 8; ++m) acc[q][m] = T(0);
+  // back, L^T x = y: x(i) = (y(i) - acc(i)) / L(i, i), then acc(i-m) += L(i, i-m) x(i)
   for (int i0 = Ny - 1; i0 >= 0; i0 -= RB) {
     T cf[RB][9], bv[RB][R];
 #pragma unroll
     for (int r = 0; r < RB; ++r) {
       const int i = i0 - r;
       const bool in = i >= 0;
-      cf[r][0] = in ? L[(long)i * 9 * Nz] : T(0);
 #pragma unroll
-      for (int m = 1; m <= 8; ++m) cf[r][m] = in ? L[((long)(i + m) * 9 + m) * Nz] : T(0);
+      for (int m = 0; m <= 8; ++m) cf[r][m] = in ? L[((long)i * 9 + m) * Nz] : T(0);
 #pragma unroll
       for (int q = 0; q < R; ++q) bv[r][q] = (in && q < nr) ? col[q * NN + (long)i * Nz] : T(0);
     }
@@ -417,19 +416,131 @@ __global__ void __launch_bounds__(128) b_ysolve_kernel(const T* __restrict__ Lb,
       if (i >= 0) {
 #pragma unroll
         for (int q = 0; q < R; ++q) {
-          T s = bv[r][q];
-#pragma unroll
-          for (int m = 8; m >= 1; --m) s -= cf[r][m] * w[q][m - 1];
-          const T x = s * cf[r][0];
+          const T x = (bv[r][q] - acc[q][0]) * cf[r][0];
           if (q < nr) col[q * NN + (long)i * Nz] = x;
 #pragma unroll
-          for (int m = 7; m >= 1; --m) w[q][m] = w[q][m - 1];
-          w[q][0] = x;
+          for (int m = 0; m < 7; ++m) acc[q][m] = acc[q][m + 1] + cf[r][m + 1] * x;
+          acc[q][7] = cf[r][8] * x;
         }
       }
     }
   }
 }
+
+// The banded sweeps fed by the tensor memory accelerator: a block of YS_W
+// warps owns 32 consecutive z modes of YS_W instances (one instance per
+// warp), so each chunk of the factor (16 rows x 9 table rows x 32 columns)
+// arrives once for YS_W sweeps; the chunks of the transform (16 rows x 32
+// columns, one per warp) come with it.  Two stages in shared memory: a chunk
+// is swept while the next lands.  Column-oriented as b_ysolve_kernel.  A
+// wait that runs out sets status bit 4 of the block's instances (their solve
+// is then repeated) and the block stops.
+constexpr int YS_R = 16, YS_C = 32, YS_S = 2, YS_W = 8;
+
+template <typename T>
+__global__ void __launch_bounds__(32 * YS_W) b_ysolve_tma_kernel(const __grid_constant__ CUtensorMap mLcol,
+                                                                 const __grid_constant__ CUtensorMap mLrow,
+                                                                 const __grid_constant__ CUtensorMap mT,
+                                                                 T* __restrict__ t, int Ny, int Nz, int Nzp, int K,
+                                                                 unsigned* __restrict__ status) {
+  extern __shared__ __align__(128) unsigned char ys_smem[];
+  constexpr int CT = YS_R * 9 * YS_C, DT = YS_R * YS_C;  // elements per tile
+  T* coef = reinterpret_cast<T*>(ys_smem);                // [YS_S][CT]
+  T* dat = coef + YS_S * CT;                              // [YS_S][YS_W][DT]
+  uint64_t* bar = reinterpret_cast<uint64_t*>(dat + YS_S * YS_W * DT);
+  const int lane = threadIdx.x & 31, wv = threadIdx.x >> 5;
+  const int j0 = blockIdx.x * YS_C, j = j0 + lane;
+  const int kb = blockIdx.y * YS_W, nw = min(YS_W, K - kb), k = kb + wv;
+  const bool active = wv < nw, valid = active && j < Nz;
+  T* colp = t + (long)k * Ny * Nzp + j;
+  const uint32_t bytes = (uint32_t)((CT + nw * DT) * sizeof(T));
+  const int nch = (Ny + YS_R - 1) / YS_R;
+  constexpr int kPolls = 1 << 18;
+  const bool leader = threadIdx.x == 0;
+  if (leader) {
+    for (int st = 0; st < YS_S; ++st) mbar_init(&bar[st], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  // chunk g of the 2 * nch chunks (forward 0..nch-1, back nch..2nch-1) into stage g % YS_S
+  auto issue = [&](int g) {
+    const int st = g % YS_S;
+    mbar_expect_tx(&bar[st], bytes);
+    const bool fwd = g < nch;
+    const int lo = fwd ? g * YS_R : Ny - 1 - (g - nch) * YS_R - (YS_R - 1);  // first row (may be < 0)
+    tma_load_2d(coef + st * CT, fwd ? &mLcol : &mLrow, &bar[st], j0, lo * 9);
+    for (int q = 0; q < nw; ++q) tma_load_2d(dat + (st * YS_W + q) * DT, &mT, &bar[st], j0, (kb + q) * Ny + lo);
+  };
+  if (leader)
+    for (int q = 0; q < YS_S && q < nch; ++q) issue(q);
+  bool ok = true;
+  T acc[8];
+#pragma unroll
+  for (int m = 0; m < 8; ++m) acc[m] = T(0);
+  int g = 0;
+  for (; g < 2 * nch; ++g) {
+    if (g == nch) {
+      // the back sweep reads the forward result through the TMA: order the
+      // stores first, then start its chunks
+      fence_proxy_async_global();
+      __syncthreads();
+      if (leader)
+        for (int q = nch; q < nch + YS_S && q < 2 * nch; ++q) issue(q);
+#pragma unroll
+      for (int m = 0; m < 8; ++m) acc[m] = T(0);
+    }
+    const int st = g % YS_S;
+    ok = mbar_wait(&bar[st], (g / YS_S) & 1, kPolls);
+    if (__syncthreads_or(!ok)) {
+      ok = false;
+      break;
+    }
+    const T* cf = coef + st * CT + lane;
+    const T* dv = dat + (st * YS_W + wv) * DT + lane;
+    if (active) {
+      if (g < nch) {
+        const int i0 = g * YS_R;
+#pragma unroll 4
+        for (int r = 0; r < YS_R; ++r) {
+          const int i = i0 + r;
+          if (i >= Ny) break;
+          const T* c = cf + r * 9 * YS_C;
+          const T y = (dv[r * YS_C] - acc[0]) * c[0];
+          if (valid) colp[(long)i * Nzp] = y;
+#pragma unroll
+          for (int m = 0; m < 7; ++m) acc[m] = acc[m + 1] + c[(m + 1) * YS_C] * y;
+          acc[7] = c[8 * YS_C] * y;
+        }
+      } else {
+        const int lo = Ny - 1 - (g - nch) * YS_R - (YS_R - 1);
+#pragma unroll 4
+        for (int r = YS_R - 1; r >= 0; --r) {
+          const int i = lo + r;
+          if (i < 0) break;
+          const T* c = cf + r * 9 * YS_C;
+          const T x = (dv[r * YS_C] - acc[0]) * c[0];
+          if (valid) colp[(long)i * Nzp] = x;
+#pragma unroll
+          for (int m = 0; m < 7; ++m) acc[m] = acc[m + 1] + c[(m + 1) * YS_C] * x;
+          acc[7] = c[8 * YS_C] * x;
+        }
+      }
+    }
+    __syncthreads();  // every warp is done with stage st
+    const int nx = g + YS_S;
+    if (leader && nx < 2 * nch && nx != nch && nx != nch + 1) issue(nx);
+  }
+  if (!ok) {
+    if (leader) {
+      for (int q = 0; q < nw; ++q) atomicOr(status + kb + q, 4u);
+      // let the loads already issued land before the block's shared memory goes
+      for (int q = g; q < g + YS_S && q < 2 * nch; ++q) mbar_wait(&bar[q % YS_S], (q / YS_S) & 1, kPolls);
+    }
+    __syncthreads();
+  }
+}
+
+int ys_smem_bytes(int esize) { return YS_S * (YS_R * 9 * YS_C + YS_W * YS_R * YS_C) * esize + YS_S * 8; }
 
 // Fault_qd::d_dt with tauQS = mu Dy u on the fault row (linear elastic) or
 // the material's sxy there (power law)
@@ -561,6 +672,37 @@ __global__ void b_status_kernel(const BatchInst* __restrict__ tab, BatchWork w, 
 }  // namespace
 
 // ---------------------------------------------------------------------------
+int tma_map_2d(CUtensorMap* map, const void* base, CUtensorMapDataType type, int esize, long cols, long rows,
+               long stride_bytes, int box_cols, int box_rows) {
+  typedef CUresult (*EncodeFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                               const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                               CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+  static EncodeFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess || !p ||
+        q != cudaDriverEntryPointSuccess) {
+      set_error("cuTensorMapEncodeTiled is not available");
+      return SCY_ERR_CUDA;
+    }
+    fn = reinterpret_cast<EncodeFn>(p);
+  }
+  (void)esize;
+  const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)stride_bytes};
+  const cuuint32_t box[2] = {(cuuint32_t)box_cols, (cuuint32_t)box_rows};
+  const cuuint32_t es[2] = {1, 1};
+  const CUresult r = fn(map, type, 2, const_cast<void*>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                        CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_error("cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return SCY_ERR_CUDA;
+  }
+  return SCY_OK;
+}
+
 BatchGroup::~BatchGroup() {
   if (blas) cublasDestroy(blas);
   if (join) cudaEventDestroy(join);
@@ -808,6 +950,27 @@ int BatchContext::setup_group(int base, int K) {
       I.inv_cap = c.inv_visc_cap;
     }
   }
+  if (g.fd->ybanded) {
+    // the z transform with rows padded to Nzp values (TMA strides are
+    // multiples of 16 bytes), and the tile maps of the TMA-fed sweeps
+    const int Nzp = g.fd->Nzp;
+    const long rowsT = (long)g.K * g.Ny;
+    SCY_TRY(g.t1p.alloc((size_t)rowsT * Nzp * 8));
+    SCY_TRY(g.t1pf.alloc((size_t)rowsT * Nzp * 4));
+    SCY_CUDA_TRY(cudaMemset(g.t1p.p, 0, (size_t)rowsT * Nzp * 8));
+    SCY_CUDA_TRY(cudaMemset(g.t1pf.p, 0, (size_t)rowsT * Nzp * 4));
+    const CUtensorMapDataType d64 = CU_TENSOR_MAP_DATA_TYPE_FLOAT64, d32 = CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    SCY_TRY(tma_map_2d(&g.mLcol, g.fd->Lcol.p, d64, 8, g.Nz, (long)g.Ny * 9, (long)Nzp * 8, YS_C, YS_R * 9));
+    SCY_TRY(tma_map_2d(&g.mLrow, g.fd->Lrow.p, d64, 8, g.Nz, (long)(g.Ny + 8) * 9, (long)Nzp * 8, YS_C, YS_R * 9));
+    SCY_TRY(tma_map_2d(&g.mT, g.t1p.p, d64, 8, g.Nz, rowsT, (long)Nzp * 8, YS_C, YS_R));
+    SCY_TRY(tma_map_2d(&g.mLcol32, g.fd->Lcol32.p, d32, 4, g.Nz, (long)g.Ny * 9, (long)Nzp * 4, YS_C, YS_R * 9));
+    SCY_TRY(tma_map_2d(&g.mLrow32, g.fd->Lrow32.p, d32, 4, g.Nz, (long)(g.Ny + 8) * 9, (long)Nzp * 4, YS_C, YS_R * 9));
+    SCY_TRY(tma_map_2d(&g.mT32, g.t1pf.p, d32, 4, g.Nz, rowsT, (long)Nzp * 4, YS_C, YS_R));
+    SCY_CUDA_TRY(cudaFuncSetAttribute(b_ysolve_tma_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      ys_smem_bytes(8)));
+    SCY_CUDA_TRY(cudaFuncSetAttribute(b_ysolve_tma_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      ys_smem_bytes(4)));
+  }
   SCY_TRY(g.tab.alloc(sizeof(BatchInst) * g.K));
   SCY_CUDA_TRY(cudaMemcpy(g.tab.p, tab.data(), sizeof(BatchInst) * g.K, cudaMemcpyHostToDevice));
   SCY_CUDA_TRY(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
@@ -878,36 +1041,37 @@ int BatchContext::fd_apply(BatchGroup& g) {
   dim3 sg(node_blocks(N), 1, K);
   if (F.ybanded && !fd_dense) {
     // Z = Vz [ per z mode: (Ky + lz_j My)^-1 along y ] (Vz^T R)
-    // instances per thread and rows per load round in the banded sweeps
-    // (register budget: 2 x 8 in FP32, 1 x 8 in FP64)
-    const int R = precision != SCY_PREC_FP64 ? 2 : 1;
-    const int nb = (int)(((long)Nz * ((K + R - 1) / R) + 127) / 128);
     if (precision != SCY_PREC_FP64) {
       SCY_BLAS_TRY(cublasSetMathMode(g.blas, precision == SCY_PREC_TF32 ? CUBLAS_TF32_TENSOR_OP_MATH
                                                                        : CUBLAS_DEFAULT_MATH));
       const float one = 1.0f, zero = 0.0f;
       const float* vz = F.Vz32.as<float>();
+      float* t1 = g.t1pf.as<float>();
       SCY_BLAS_TRY(cublasSgemm(g.blas, CUBLAS_OP_T, CUBLAS_OP_N, Nz, Ny * K, Nz, &one, vz, Nz, g.w.r32, Nz, &zero,
-                               g.w.t1f, Nz));
+                               t1, F.Nzp));
       cudaEvent_t pa;
       SCY_TRY(prof_begin(g.stream, &pa));
-      b_ysolve_kernel<float, 2, 8><<<nb, 128, 0, g.stream>>>(F.Lb32.as<float>(), g.w.t1f, Ny, Nz, K);
+      b_ysolve_tma_kernel<float><<<dim3((Nz + YS_C - 1) / YS_C, (K + YS_W - 1) / YS_W), 32 * YS_W, ys_smem_bytes(4),
+                                   g.stream>>>(g.mLcol32, g.mLrow32, g.mT32, t1, Ny, Nz, F.Nzp, K, g.w.status);
       SCY_LAUNCH_CHECK();
       SCY_TRY(prof_end(g.stream, pa, PROF_YSOLVE, 4.0 * (9.0 * Ny * Nz + 4.0 * N * K)));
-      SCY_BLAS_TRY(cublasSgemm(g.blas, CUBLAS_OP_N, CUBLAS_OP_N, Nz, Ny * K, Nz, &one, vz, Nz, g.w.t1f, Nz, &zero,
+      SCY_BLAS_TRY(cublasSgemm(g.blas, CUBLAS_OP_N, CUBLAS_OP_N, Nz, Ny * K, Nz, &one, vz, Nz, t1, F.Nzp, &zero,
                                g.w.z32, Nz));
     } else {
       SCY_BLAS_TRY(cublasSetMathMode(g.blas, CUBLAS_DEFAULT_MATH));
       const double one = 1.0, zero = 0.0;
       const double* vz = F.Vz.as<double>();
-      SCY_BLAS_TRY(cublasDgemm(g.blas, CUBLAS_OP_T, CUBLAS_OP_N, Nz, Ny * K, Nz, &one, vz, Nz, g.w.r, Nz, &zero,
-                               g.w.t1, Nz));
+      double* t1 = g.t1p.as<double>();
+      SCY_BLAS_TRY(cublasDgemm(g.blas, CUBLAS_OP_T, CUBLAS_OP_N, Nz, Ny * K, Nz, &one, vz, Nz, g.w.r, Nz, &zero, t1,
+                               F.Nzp));
       cudaEvent_t pa;
       SCY_TRY(prof_begin(g.stream, &pa));
-      b_ysolve_kernel<double, 1, 8><<<nb, 128, 0, g.stream>>>(F.Lb.as<double>(), g.w.t1, Ny, Nz, K);
+      b_ysolve_tma_kernel<double><<<dim3((Nz + YS_C - 1) / YS_C, (K + YS_W - 1) / YS_W), 32 * YS_W,
+                                    ys_smem_bytes(8), g.stream>>>(g.mLcol, g.mLrow, g.mT, t1, Ny, Nz, F.Nzp, K,
+                                                                  g.w.status);
       SCY_LAUNCH_CHECK();
       SCY_TRY(prof_end(g.stream, pa, PROF_YSOLVE, 8.0 * (9.0 * Ny * Nz + 4.0 * N * K)));
-      SCY_BLAS_TRY(cublasDgemm(g.blas, CUBLAS_OP_N, CUBLAS_OP_N, Nz, Ny * K, Nz, &one, vz, Nz, g.w.t1, Nz, &zero,
+      SCY_BLAS_TRY(cublasDgemm(g.blas, CUBLAS_OP_N, CUBLAS_OP_N, Nz, Ny * K, Nz, &one, vz, Nz, t1, F.Nzp, &zero,
                                g.w.z, Nz));
     }
     count_launch();

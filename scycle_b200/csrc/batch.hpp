@@ -9,6 +9,7 @@
 // reads that instance's pointers from a device table.
 #pragma once
 #include <cublas_v2.h>
+#include <cuda.h>
 
 #include <map>
 #include <memory>
@@ -63,6 +64,8 @@ struct BatchGroup {
   LevelDev<double> L{};
   std::shared_ptr<FDPrecond> fd;
   DevBuf tab;     // BatchInst[K]
+  DevBuf t1p, t1pf;  // the z transform, rows padded to the factor tables' Nzp (FP64, FP32)
+  CUtensorMap mLcol, mLrow, mT, mLcol32, mLrow32, mT32;  // tile maps of the TMA-fed banded sweeps
   DevBuf planes;  // the operator's 33 cross-stencil coefficient planes (build_cross_planes)
   int kpb = 1;    // instances per block of the operator kernels
   DevBuf vec[7], vecf[4], sc, partials, counters, status;

@@ -231,6 +231,21 @@ int FDPrecond::build(const LevelHost& L, cudaStream_t s) {
       if (spd) {
         SCY_TRY(upload_as<double>(Lb, Lbh, s));
         SCY_TRY(upload_as<float>(Lb32, Lbh, s));
+        // padded row and column forms for the TMA-fed sweeps
+        Nzp = (Nz + 3) / 4 * 4;
+        std::vector<double> Lr((size_t)(Ny + bw) * 9 * Nzp, 0.0), Lc((size_t)Ny * 9 * Nzp, 0.0);
+        for (int i = 0; i < Ny + bw; ++i)
+          for (int k = 0; k < 9; ++k)
+            for (int j = 0; j < Nz; ++j) Lr[((size_t)i * 9 + k) * Nzp + j] = Lbh[((size_t)i * 9 + k) * Nz + j];
+        for (int i = 0; i < Ny; ++i)
+          for (int j = 0; j < Nz; ++j) {
+            Lc[((size_t)i * 9) * Nzp + j] = Lbh[((size_t)i * 9) * Nz + j];
+            for (int m = 1; m <= bw; ++m) Lc[((size_t)i * 9 + m) * Nzp + j] = Lbh[((size_t)(i + m) * 9 + m) * Nz + j];
+          }
+        SCY_TRY(upload_as<double>(Lrow, Lr, s));
+        SCY_TRY(upload_as<double>(Lcol, Lc, s));
+        SCY_TRY(upload_as<float>(Lrow32, Lr, s));
+        SCY_TRY(upload_as<float>(Lcol32, Lc, s));
         ybanded = 1;
       }
     }

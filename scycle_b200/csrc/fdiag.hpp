@@ -32,6 +32,12 @@ struct FDPrecond {
   // for k = 0, with 8 zero rows after the last (Ny + 8 rows in all).
   int ybanded = 0;
   DevBuf Lb, Lb32;
+  // The same factors for the TMA-fed sweeps, rows padded to Nzp (a multiple
+  // of 4) values: row form [(i * 9 + m) * Nzp + j] = L_j(i, i - m) (Ny + 8
+  // rows), column form [(i * 9 + m) * Nzp + j] = L_j(i + m, i) (Ny rows);
+  // slot m = 0 holds 1 / L_j(i, i) in both.
+  int Nzp = 0;
+  DevBuf Lrow, Lcol, Lrow32, Lcol32;
   ~FDPrecond();
   int build(const LevelHost& L, cudaStream_t s);
   // z = K_sep^-1 r (FP64)
