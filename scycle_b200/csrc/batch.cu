@@ -427,15 +427,21 @@ __global__ void __launch_bounds__(128) b_ysolve_kernel(const T* __restrict__ Lb,
   }
 }
 
-// The banded sweeps fed by the tensor memory accelerator: a block of YS_W
-// warps owns 32 consecutive z modes of YS_W instances (one instance per
-// warp), so each chunk of the factor (16 rows x 9 table rows x 32 columns)
-// arrives once for YS_W sweeps; the chunks of the transform (16 rows x 32
-// columns, one per warp) come with it.  Two stages in shared memory: a chunk
-// is swept while the next lands.  Column-oriented as b_ysolve_kernel.  A
-// wait that runs out sets status bit 4 of the block's instances (their solve
-// is then repeated) and the block stops.
-constexpr int YS_R = 16, YS_C = 32, YS_S = 2, YS_W = 8;
+// The banded sweeps fed by the tensor memory accelerator.  A block owns
+// YS_C = 16 consecutive z modes of YS_B = 8 instances: lane c + 16 h of warp
+// w carries the chains of mode j0 + c for the YS_I = 2 instances
+// (2 w + h) * 2 + s, so one read of a factor value from shared memory serves
+// two chains, and lanes c and c + 16 read the same value (a broadcast).  Per
+// chunk of YS_R = 16 rows one 2D copy brings the factor (16 rows x 9 table
+// rows x 16 modes) and one 3D copy the transform of all eight instances
+// (16 modes x 16 rows x 8 instances); YS_S = 3 stages, so two chunks are in
+// flight while one is swept.  Every chunk is swept over all 16 rows: rows
+// outside 0..Ny-1 arrive as zeros (factor and data), give zero and only
+// shift the accumulators, and are not stored.  A wait that runs out sets
+// status bit 4 of the block's instances (their solve is then repeated) and
+// the block stops.
+constexpr int YS_R = 16, YS_C = 16, YS_I = 2, YS_W = 2, YS_S = 3;
+constexpr int YS_B = YS_W * (32 / YS_C) * YS_I;  // instances per block
 
 template <typename T>
 __global__ void __launch_bounds__(32 * YS_W) b_ysolve_tma_kernel(const __grid_constant__ CUtensorMap mLcol,
@@ -444,16 +450,23 @@ __global__ void __launch_bounds__(32 * YS_W) b_ysolve_tma_kernel(const __grid_co
                                                                  T* __restrict__ t, int Ny, int Nz, int Nzp, int K,
                                                                  unsigned* __restrict__ status) {
   extern __shared__ __align__(128) unsigned char ys_smem[];
-  constexpr int CT = YS_R * 9 * YS_C, DT = YS_R * YS_C;  // elements per tile
-  T* coef = reinterpret_cast<T*>(ys_smem);                // [YS_S][CT]
-  T* dat = coef + YS_S * CT;                              // [YS_S][YS_W][DT]
-  uint64_t* bar = reinterpret_cast<uint64_t*>(dat + YS_S * YS_W * DT);
-  const int lane = threadIdx.x & 31, wv = threadIdx.x >> 5;
-  const int j0 = blockIdx.x * YS_C, j = j0 + lane;
-  const int kb = blockIdx.y * YS_W, nw = min(YS_W, K - kb), k = kb + wv;
-  const bool active = wv < nw, valid = active && j < Nz;
-  T* colp = t + (long)k * Ny * Nzp + j;
-  const uint32_t bytes = (uint32_t)((CT + nw * DT) * sizeof(T));
+  constexpr int CT = YS_R * 9 * YS_C, DT = YS_B * YS_R * YS_C;  // elements per tile
+  T* coef = reinterpret_cast<T*>(ys_smem);                      // [YS_S][YS_R][9][YS_C]
+  T* dat = coef + YS_S * CT;                                    // [YS_S][YS_B][YS_R][YS_C]
+  uint64_t* bar = reinterpret_cast<uint64_t*>(dat + YS_S * DT);
+  const int lane = threadIdx.x & 31, c = lane % YS_C, h = lane / YS_C, wv = threadIdx.x >> 5;
+  const int j0 = blockIdx.x * YS_C, j = j0 + c, kb = blockIdx.y * YS_B;
+  int kk[YS_I];
+  bool valid[YS_I];
+  T* colp[YS_I];
+#pragma unroll
+  for (int s = 0; s < YS_I; ++s) {
+    kk[s] = (wv * (32 / YS_C) + h) * YS_I + s;
+    const int k = kb + kk[s];
+    valid[s] = j < Nz && k < K;
+    colp[s] = t + (long)min(k, K - 1) * Ny * Nzp + j;
+  }
+  constexpr uint32_t bytes = (uint32_t)((CT + DT) * sizeof(T));
   const int nch = (Ny + YS_R - 1) / YS_R;
   constexpr int kPolls = 1 << 18;
   const bool leader = threadIdx.x == 0;
@@ -462,21 +475,24 @@ __global__ void __launch_bounds__(32 * YS_W) b_ysolve_tma_kernel(const __grid_co
     fence_mbar_init();
   }
   __syncthreads();
-  // chunk g of the 2 * nch chunks (forward 0..nch-1, back nch..2nch-1) into stage g % YS_S
+  // chunk g of the 2 * nch chunks (forward 0..nch-1 from row 0, back
+  // nch..2nch-1 from row Ny-1) into stage g % YS_S
   auto issue = [&](int g) {
     const int st = g % YS_S;
     mbar_expect_tx(&bar[st], bytes);
     const bool fwd = g < nch;
-    const int lo = fwd ? g * YS_R : Ny - 1 - (g - nch) * YS_R - (YS_R - 1);  // first row (may be < 0)
+    const int lo = fwd ? g * YS_R : Ny - (g - nch + 1) * YS_R;  // first row (may be < 0)
     tma_load_2d(coef + st * CT, fwd ? &mLcol : &mLrow, &bar[st], j0, lo * 9);
-    for (int q = 0; q < nw; ++q) tma_load_2d(dat + (st * YS_W + q) * DT, &mT, &bar[st], j0, (kb + q) * Ny + lo);
+    tma_load_3d(dat + st * DT, &mT, &bar[st], j0, lo, kb);
   };
   if (leader)
     for (int q = 0; q < YS_S && q < nch; ++q) issue(q);
   bool ok = true;
-  T acc[8];
+  T acc[YS_I][8];
 #pragma unroll
-  for (int m = 0; m < 8; ++m) acc[m] = T(0);
+  for (int s = 0; s < YS_I; ++s)
+#pragma unroll
+    for (int m = 0; m < 8; ++m) acc[s][m] = T(0);
   int g = 0;
   for (; g < 2 * nch; ++g) {
     if (g == nch) {
@@ -487,7 +503,9 @@ __global__ void __launch_bounds__(32 * YS_W) b_ysolve_tma_kernel(const __grid_co
       if (leader)
         for (int q = nch; q < nch + YS_S && q < 2 * nch; ++q) issue(q);
 #pragma unroll
-      for (int m = 0; m < 8; ++m) acc[m] = T(0);
+      for (int s = 0; s < YS_I; ++s)
+#pragma unroll
+        for (int m = 0; m < 8; ++m) acc[s][m] = T(0);
     }
     const int st = g % YS_S;
     ok = mbar_wait(&bar[st], (g / YS_S) & 1, kPolls);
@@ -495,44 +513,35 @@ __global__ void __launch_bounds__(32 * YS_W) b_ysolve_tma_kernel(const __grid_co
       ok = false;
       break;
     }
-    const T* cf = coef + st * CT + lane;
-    const T* dv = dat + (st * YS_W + wv) * DT + lane;
-    if (active) {
-      if (g < nch) {
-        const int i0 = g * YS_R;
-#pragma unroll 4
-        for (int r = 0; r < YS_R; ++r) {
-          const int i = i0 + r;
-          if (i >= Ny) break;
-          const T* c = cf + r * 9 * YS_C;
-          const T y = (dv[r * YS_C] - acc[0]) * c[0];
-          if (valid) colp[(long)i * Nzp] = y;
+    const T* cf = coef + st * CT + c;
+    const T* dv = dat + st * DT + c;
+    const bool fwd = g < nch;
+    const int lo = fwd ? g * YS_R : Ny - (g - nch + 1) * YS_R;
 #pragma unroll
-          for (int m = 0; m < 7; ++m) acc[m] = acc[m + 1] + c[(m + 1) * YS_C] * y;
-          acc[7] = c[8 * YS_C] * y;
-        }
-      } else {
-        const int lo = Ny - 1 - (g - nch) * YS_R - (YS_R - 1);
-#pragma unroll 4
-        for (int r = YS_R - 1; r >= 0; --r) {
-          const int i = lo + r;
-          if (i < 0) break;
-          const T* c = cf + r * 9 * YS_C;
-          const T x = (dv[r * YS_C] - acc[0]) * c[0];
-          if (valid) colp[(long)i * Nzp] = x;
+    for (int q = 0; q < YS_R; ++q) {
+      const int r = fwd ? q : YS_R - 1 - q;
+      const int i = lo + r;
+      const bool in = i >= 0 && i < Ny;
+      const T* cr = cf + r * 9 * YS_C;
+      T cm[9];
 #pragma unroll
-          for (int m = 0; m < 7; ++m) acc[m] = acc[m + 1] + c[(m + 1) * YS_C] * x;
-          acc[7] = c[8 * YS_C] * x;
-        }
+      for (int m = 0; m < 9; ++m) cm[m] = cr[m * YS_C];
+#pragma unroll
+      for (int s = 0; s < YS_I; ++s) {
+        const T y = (dv[(kk[s] * YS_R + r) * YS_C] - acc[s][0]) * cm[0];
+        if (valid[s] && in) colp[s][(long)i * Nzp] = y;
+#pragma unroll
+        for (int m = 0; m < 7; ++m) acc[s][m] = acc[s][m + 1] + cm[m + 1] * y;
+        acc[s][7] = cm[8] * y;
       }
     }
     __syncthreads();  // every warp is done with stage st
     const int nx = g + YS_S;
-    if (leader && nx < 2 * nch && nx != nch && nx != nch + 1) issue(nx);
+    if (leader && (nx < nch || (nx >= nch + YS_S && nx < 2 * nch))) issue(nx);
   }
   if (!ok) {
     if (leader) {
-      for (int q = 0; q < nw; ++q) atomicOr(status + kb + q, 4u);
+      for (int q = 0; q < YS_B && kb + q < K; ++q) atomicOr(status + kb + q, 4u);
       // let the loads already issued land before the block's shared memory goes
       for (int q = g; q < g + YS_S && q < 2 * nch; ++q) mbar_wait(&bar[q % YS_S], (q / YS_S) & 1, kPolls);
     }
@@ -540,7 +549,7 @@ __global__ void __launch_bounds__(32 * YS_W) b_ysolve_tma_kernel(const __grid_co
   }
 }
 
-int ys_smem_bytes(int esize) { return YS_S * (YS_R * 9 * YS_C + YS_W * YS_R * YS_C) * esize + YS_S * 8; }
+int ys_smem_bytes(int esize) { return YS_S * (YS_R * 9 * YS_C + YS_B * YS_R * YS_C) * esize + YS_S * 8; }
 
 // Fault_qd::d_dt with tauQS = mu Dy u on the fault row (linear elastic) or
 // the material's sxy there (power law)
@@ -672,12 +681,16 @@ __global__ void b_status_kernel(const BatchInst* __restrict__ tab, BatchWork w, 
 }  // namespace
 
 // ---------------------------------------------------------------------------
-int tma_map_2d(CUtensorMap* map, const void* base, CUtensorMapDataType type, int esize, long cols, long rows,
-               long stride_bytes, int box_cols, int box_rows) {
-  typedef CUresult (*EncodeFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
-                               const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
-                               CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-  static EncodeFn fn = nullptr;
+namespace {
+typedef CUresult (*TmaEncodeFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// a tile map of `rank` dimensions (dims[0] innermost; strides in bytes of
+// dimensions 1..rank-1) without swizzle, reads outside the array give zeros
+int tma_encode(CUtensorMap* map, const void* base, CUtensorMapDataType type, int rank, const cuuint64_t* dims,
+               const cuuint64_t* strides, const cuuint32_t* box) {
+  static TmaEncodeFn fn = nullptr;
   if (!fn) {
     void* p = nullptr;
     cudaDriverEntryPointQueryResult q;
@@ -686,21 +699,35 @@ int tma_map_2d(CUtensorMap* map, const void* base, CUtensorMapDataType type, int
       set_error("cuTensorMapEncodeTiled is not available");
       return SCY_ERR_CUDA;
     }
-    fn = reinterpret_cast<EncodeFn>(p);
+    fn = reinterpret_cast<TmaEncodeFn>(p);
   }
-  (void)esize;
-  const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
-  const cuuint64_t strides[1] = {(cuuint64_t)stride_bytes};
-  const cuuint32_t box[2] = {(cuuint32_t)box_cols, (cuuint32_t)box_rows};
-  const cuuint32_t es[2] = {1, 1};
-  const CUresult r = fn(map, type, 2, const_cast<void*>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                        CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+  const cuuint32_t es[3] = {1, 1, 1};
+  const CUresult r = fn(map, type, (cuuint32_t)rank, const_cast<void*>(base), dims, strides, box, es,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) {
     set_error("cuTensorMapEncodeTiled failed (%d)", (int)r);
     return SCY_ERR_CUDA;
   }
   return SCY_OK;
+}
+}  // namespace
+
+int tma_map_2d(CUtensorMap* map, const void* base, CUtensorMapDataType type, int esize, long cols, long rows,
+               long stride_bytes, int box_cols, int box_rows) {
+  (void)esize;
+  const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)stride_bytes};
+  const cuuint32_t box[2] = {(cuuint32_t)box_cols, (cuuint32_t)box_rows};
+  return tma_encode(map, base, type, 2, dims, strides, box);
+}
+
+int tma_map_3d(CUtensorMap* map, const void* base, CUtensorMapDataType type, long d0, long d1, long d2,
+               long stride1_bytes, long stride2_bytes, int box0, int box1, int box2) {
+  const cuuint64_t dims[3] = {(cuuint64_t)d0, (cuuint64_t)d1, (cuuint64_t)d2};
+  const cuuint64_t strides[2] = {(cuuint64_t)stride1_bytes, (cuuint64_t)stride2_bytes};
+  const cuuint32_t box[3] = {(cuuint32_t)box0, (cuuint32_t)box1, (cuuint32_t)box2};
+  return tma_encode(map, base, type, 3, dims, strides, box);
 }
 
 BatchGroup::~BatchGroup() {
@@ -962,10 +989,11 @@ int BatchContext::setup_group(int base, int K) {
     const CUtensorMapDataType d64 = CU_TENSOR_MAP_DATA_TYPE_FLOAT64, d32 = CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
     SCY_TRY(tma_map_2d(&g.mLcol, g.fd->Lcol.p, d64, 8, g.Nz, (long)g.Ny * 9, (long)Nzp * 8, YS_C, YS_R * 9));
     SCY_TRY(tma_map_2d(&g.mLrow, g.fd->Lrow.p, d64, 8, g.Nz, (long)(g.Ny + 8) * 9, (long)Nzp * 8, YS_C, YS_R * 9));
-    SCY_TRY(tma_map_2d(&g.mT, g.t1p.p, d64, 8, g.Nz, rowsT, (long)Nzp * 8, YS_C, YS_R));
+    SCY_TRY(tma_map_3d(&g.mT, g.t1p.p, d64, g.Nz, g.Ny, g.K, (long)Nzp * 8, (long)g.Ny * Nzp * 8, YS_C, YS_R, YS_B));
     SCY_TRY(tma_map_2d(&g.mLcol32, g.fd->Lcol32.p, d32, 4, g.Nz, (long)g.Ny * 9, (long)Nzp * 4, YS_C, YS_R * 9));
     SCY_TRY(tma_map_2d(&g.mLrow32, g.fd->Lrow32.p, d32, 4, g.Nz, (long)(g.Ny + 8) * 9, (long)Nzp * 4, YS_C, YS_R * 9));
-    SCY_TRY(tma_map_2d(&g.mT32, g.t1pf.p, d32, 4, g.Nz, rowsT, (long)Nzp * 4, YS_C, YS_R));
+    SCY_TRY(tma_map_3d(&g.mT32, g.t1pf.p, d32, g.Nz, g.Ny, g.K, (long)Nzp * 4, (long)g.Ny * Nzp * 4, YS_C, YS_R,
+                       YS_B));
     SCY_CUDA_TRY(cudaFuncSetAttribute(b_ysolve_tma_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       ys_smem_bytes(8)));
     SCY_CUDA_TRY(cudaFuncSetAttribute(b_ysolve_tma_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1051,7 +1079,7 @@ int BatchContext::fd_apply(BatchGroup& g) {
                                t1, F.Nzp));
       cudaEvent_t pa;
       SCY_TRY(prof_begin(g.stream, &pa));
-      b_ysolve_tma_kernel<float><<<dim3((Nz + YS_C - 1) / YS_C, (K + YS_W - 1) / YS_W), 32 * YS_W, ys_smem_bytes(4),
+      b_ysolve_tma_kernel<float><<<dim3((Nz + YS_C - 1) / YS_C, (K + YS_B - 1) / YS_B), 32 * YS_W, ys_smem_bytes(4),
                                    g.stream>>>(g.mLcol32, g.mLrow32, g.mT32, t1, Ny, Nz, F.Nzp, K, g.w.status);
       SCY_LAUNCH_CHECK();
       SCY_TRY(prof_end(g.stream, pa, PROF_YSOLVE, 4.0 * (9.0 * Ny * Nz + 4.0 * N * K)));
@@ -1066,7 +1094,7 @@ int BatchContext::fd_apply(BatchGroup& g) {
                                F.Nzp));
       cudaEvent_t pa;
       SCY_TRY(prof_begin(g.stream, &pa));
-      b_ysolve_tma_kernel<double><<<dim3((Nz + YS_C - 1) / YS_C, (K + YS_W - 1) / YS_W), 32 * YS_W,
+      b_ysolve_tma_kernel<double><<<dim3((Nz + YS_C - 1) / YS_C, (K + YS_B - 1) / YS_B), 32 * YS_W,
                                     ys_smem_bytes(8), g.stream>>>(g.mLcol, g.mLrow, g.mT, t1, Ny, Nz, F.Nzp, K,
                                                                   g.w.status);
       SCY_LAUNCH_CHECK();

@@ -18,6 +18,11 @@ namespace scy {
 int tma_map_2d(CUtensorMap* map, const void* base, CUtensorMapDataType type, int esize, long cols, long rows,
                long stride_bytes, int box_cols, int box_rows);
 
+// 3D map over d0 x d1 x d2 elements (d0 innermost, strides of dimensions 1
+// and 2 in bytes, multiples of 16) with a box of box0 x box1 x box2
+int tma_map_3d(CUtensorMap* map, const void* base, CUtensorMapDataType type, long d0, long d1, long d2,
+               long stride1_bytes, long stride2_bytes, int box0, int box1, int box2);
+
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
@@ -53,6 +58,15 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, u
       "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
           smem_u32(dst)),
       "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// box at element coordinates (x, y, z) of a 3D map into dst, completion on bar
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y, int z) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(smem_u32(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
       : "memory");
 }
 
