@@ -157,23 +157,50 @@ __global__ void b_dot_rz_kernel(const int* __restrict__ mask, BatchWork w, const
 
 // A applied in its per-node cross form (33 coefficient planes shared by
 // the group, see build_cross_planes): a block owns one 8 x 32 tile of
-// nodes, keeps its nodes' coefficients in registers and applies them to
-// kpb instances in turn, staging each instance's operand (tile plus an
-// 8-node halo in y and in z) in shared memory.
+// nodes, keeps its nodes' coefficients in registers and applies them to its
+// (up to XKPB) instances in turn.  Each instance's operand (the tile plus an
+// 8-node halo in y and in z) is staged in shared memory by asynchronous
+// copies (cp.async, zero-filled outside the grid) in an XS-stage ring, so
+// the copies of the next two instances are in flight while one is computed.
 //   MODE 0: r = -rhs + A u (0 where rhs = 0), r.r -> sc[5]
 //   MODE 1: p = z + beta p_old (beta = rz / rz_old; p = z on the first
 //           iteration), q = -A p, p stored, p.q -> sc[4]
-constexpr int XTY = 8, XTZ = 32, XH = 8;
+constexpr int XTY = 8, XTZ = 32, XH = 8, XS = 3, XKPB = 8;
+constexpr int XNY = (XTY + 2 * XH) * XTZ, XNZ = XTY * (XTZ + 2 * XH), XNS = XNY + XNZ;
+
+__device__ __forceinline__ void cp_async4(void* dst, const void* src, int src_bytes) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(src_bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src, int src_bytes) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(src_bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// dynamic shared memory of b_cross_kernel: MODE 0 stages the operand and
+// the rhs of the tile; MODE 1 stages z (zsize bytes a value) and p_old and
+// forms p in one more buffer
+constexpr int xs_smem_bytes(int mode, int zsize) {
+  return mode == 0 ? XS * (XNS + 256) * 8 : (XS * XNS * zsize + 15) / 16 * 16 + XS * XNS * 8 + XNS * 8;
+}
 
 template <int MODE, typename Tz>
 __global__ void __launch_bounds__(256) b_cross_kernel(const double* __restrict__ C, int Ny, int Nz,
                                                       const BatchInst* __restrict__ tab, const int* __restrict__ mask,
                                                       BatchWork w, const Tz* __restrict__ zv, int first, int pi,
                                                       int mixed, int kpb) {
-  constexpr int NY = (XTY + 2 * XH) * XTZ, NZ = XTY * (XTZ + 2 * XH);
-  constexpr int NV = (NY + NZ + 255) / 256;  // staged values per thread
-  __shared__ double xs[NY + NZ];             // y arm rows, then z arm rows
+  constexpr int NV = (XNS + 255) / 256;  // staged values per thread
+  extern __shared__ __align__(16) unsigned char xsm[];
   __shared__ double red[8];
+  __shared__ int act[XKPB];                // the block's active instances
+  __shared__ double sck[XKPB];             // MODE 0: |rhs|^2 (0: rhs = 0); MODE 1: beta
+  __shared__ const double* srck[XKPB][2];  // MODE 0: u, rhs
+  __shared__ int nact;
   const long N = (long)Ny * Nz;
   const int tid = threadIdx.x, ty = tid / XTZ, tz = tid % XTZ;
   const int y0 = blockIdx.y * XTY, z0 = blockIdx.x * XTZ;
@@ -181,6 +208,28 @@ __global__ void __launch_bounds__(256) b_cross_kernel(const double* __restrict__
   const bool valid = iy < Ny && iz < Nz;
   const long node = (long)iy * Nz + iz;
   const int tile = blockIdx.x + gridDim.x * blockIdx.y;
+  const int kb = blockIdx.z * kpb, ke = min(w.K, kb + kpb);
+  if (tid == 0) {
+    int n = 0;
+    for (int k = kb; k < ke; ++k) {
+      if (!mask[k]) continue;
+      act[n] = k;
+      if (MODE == 0) {
+        sck[n] = w.sc[16 * k];
+        srck[n][0] = tab[k].u;
+        srck[n][1] = tab[k].rhs;
+      } else {
+        double beta = 0.0;
+        if (!first) {
+          const double ro = w.sc[16 * k + 3];
+          beta = ro != 0.0 ? w.sc[16 * k + 2] / ro : 0.0;
+        }
+        sck[n] = beta;
+      }
+      ++n;
+    }
+    nact = n;
+  }
   double c[33];
 #pragma unroll
   for (int o = 0; o < 33; ++o) c[o] = valid ? C[(long)o * N + node] : 0.0;
@@ -191,61 +240,90 @@ __global__ void __launch_bounds__(256) b_cross_kernel(const double* __restrict__
   for (int a = 0; a < NV; ++a) {
     const int i = tid + 256 * a;
     int jy = -1, jz = -1;
-    if (i < NY) {
+    if (i < XNY) {
       jy = y0 - XH + i / XTZ;
       jz = z0 + i % XTZ;
-    } else if (i < NY + NZ) {
-      const int e = i - NY;
+    } else if (i < XNS) {
+      const int e = i - XNY;
       jy = y0 + e / (XTZ + 2 * XH);
       jz = z0 - XH + e % (XTZ + 2 * XH);
     }
     src[a] = (jy >= 0 && jy < Ny && jz >= 0 && jz < Nz) ? jy * Nz + jz : -1;
   }
-  const int kb = blockIdx.z * kpb, ke = min(w.K, kb + kpb);
-  double v[NV];
-  double rhs_n = 0.0;  // MODE 0: the next instance's rhs at this node
-  bool zero_n = false;  // MODE 0: the next instance's rhs is zero
-  auto fetch = [&](int k) {
-    const long off = (long)k * N;
-    if (MODE == 0) {
-      const double* x = tab[k].u;
+  __syncthreads();
+  const int na = nact;
+  double* us = reinterpret_cast<double*>(xsm);  // MODE 0: [XS][XNS] operand, then [XS][256] rhs
+  double* rs = us + XS * XNS;
+  Tz* zs = reinterpret_cast<Tz*>(xsm);  // MODE 1: [XS][XNS] z, [XS][XNS] p_old, [XNS] p
+  double* ps = reinterpret_cast<double*>(xsm + (XS * XNS * sizeof(Tz) + 15) / 16 * 16);
+  double* xd = ps + XS * XNS;
+  // copies of the q-th active instance into stage q % XS (one commit group
+  // per call, empty past the last instance)
+  auto issue = [&](int q) {
+    if (q < na) {
+      const int st = q % XS;
+      if (MODE == 0) {
+        const double* x = srck[q][0];
 #pragma unroll
-      for (int a = 0; a < NV; ++a) v[a] = src[a] >= 0 ? x[src[a]] : 0.0;
-      rhs_n = (valid && w.sc[16 * k] != 0.0) ? tab[k].rhs[node] : 0.0;
-      zero_n = w.sc[16 * k] == 0.0;
-    } else {
-      const Tz* zz = zv + off;
-      const double* pold = (pi ? w.p1 : w.p0) + off;
-      double beta = 0.0;
-      if (!first) {
-        const double ro = w.sc[16 * k + 3];
-        beta = ro != 0.0 ? w.sc[16 * k + 2] / ro : 0.0;
+        for (int a = 0; a < NV; ++a) {
+          const int i = tid + 256 * a;
+          if (i < XNS) cp_async8(us + st * XNS + i, src[a] >= 0 ? x + src[a] : x, src[a] >= 0 ? 8 : 0);
+        }
+        const double* rh = srck[q][1];
+        const bool rv = valid && sck[q] != 0.0;
+        cp_async8(rs + st * 256 + tid, rv ? rh + node : rh, rv ? 8 : 0);
+      } else {
+        const long off = (long)act[q] * N;
+        const Tz* zz = zv + off;
+        const double* pold = (pi ? w.p1 : w.p0) + off;
+#pragma unroll
+        for (int a = 0; a < NV; ++a) {
+          const int i = tid + 256 * a;
+          if (i >= XNS) continue;
+          const bool in = src[a] >= 0;
+          if (sizeof(Tz) == 4)
+            cp_async4(zs + st * XNS + i, in ? zz + src[a] : zz, in ? 4 : 0);
+          else
+            cp_async8(zs + st * XNS + i, in ? zz + src[a] : zz, in ? 8 : 0);
+          if (!first) cp_async8(ps + st * XNS + i, in ? pold + src[a] : pold, in ? 8 : 0);
+        }
       }
-#pragma unroll
-      for (int a = 0; a < NV; ++a)
-        v[a] = src[a] >= 0 ? (first ? (double)zz[src[a]] : (double)zz[src[a]] + beta * pold[src[a]]) : 0.0;
     }
+    cp_async_commit();
   };
-  auto next_active = [&](int k) {
-    while (k < ke && !mask[k]) ++k;
-    return k;
-  };
-  int k = next_active(kb);
-  if (k < ke) fetch(k);
-  while (k < ke) {
 #pragma unroll
-    for (int a = 0; a < NV; ++a)
-      if (tid + 256 * a < NY + NZ) xs[tid + 256 * a] = v[a];
-    const double rhs_k = rhs_n;
-    const bool zero_k = zero_n;
-    __syncthreads();
-    const int kn = next_active(k + 1);
-    if (kn < ke) fetch(kn);  // in flight while this instance is computed
+  for (int q = 0; q < XS - 1; ++q) issue(q);
+  for (int q = 0; q < na; ++q) {
+    const int st = q % XS, k = act[q];
+    cp_async_wait<XS - 2>();  // this instance's group has landed (the next may not have)
+    __syncthreads();          // ... for every thread, and stage (q - 1) % XS is free
+    issue(q + XS - 1);
+    const double* X = us + st * XNS;
+    if (MODE == 1) {
+      bool direct = false;  // p = z in FP64: read the staged z as it is
+      if constexpr (sizeof(Tz) == 8) {
+        if (first) {
+          X = reinterpret_cast<const double*>(zs + st * XNS);
+          direct = true;
+        }
+      }
+      if (!direct) {
+        const double beta = sck[q];
+#pragma unroll
+        for (int a = 0; a < NV; ++a) {
+          const int i = tid + 256 * a;
+          if (i < XNS)
+            xd[i] = first ? (double)zs[st * XNS + i] : (double)zs[st * XNS + i] + beta * ps[st * XNS + i];
+        }
+        __syncthreads();
+        X = xd;
+      }
+    }
     const long off = (long)k * N;
     double contrib = 0.0;
     if (valid) {
-      const double* ay = xs + ty * XTZ + tz;                   // row iy - 8
-      const double* az = xs + NY + ty * (XTZ + 2 * XH) + tz;   // column iz - 8
+      const double* ay = X + ty * XTZ + tz;                   // row iy - 8
+      const double* az = X + XNY + ty * (XTZ + 2 * XH) + tz;  // column iz - 8
       double Ay = 0.0, Az = 0.0;
 #pragma unroll
       for (int o = 0; o < 17; ++o) Ay += c[o] * ay[o * XTZ];
@@ -255,7 +333,7 @@ __global__ void __launch_bounds__(256) b_cross_kernel(const double* __restrict__
       for (int o = 9; o < 17; ++o) Az += c[16 + o] * az[o];
       const double Ax = Ay + Az;
       if (MODE == 0) {
-        const double vv = zero_k ? 0.0 : -1.0 * rhs_k + Ax;
+        const double vv = sck[q] == 0.0 ? 0.0 : -1.0 * rs[st * 256 + tid] + Ax;
         w.r[off + node] = vv;
         if (mixed) w.r32[off + node] = (float)vv;
         contrib = vv * vv;
@@ -277,8 +355,8 @@ __global__ void __launch_bounds__(256) b_cross_kernel(const double* __restrict__
       t = warp_sum(t);
       if (tid == 0) w.partials[(long)k * w.PB + tile] = t;
     }
-    k = kn;
   }
+  cp_async_wait<0>();
 }
 
 // sc[16 k + slot] = sum of the instance's first n partials, in tile order
@@ -340,129 +418,65 @@ __global__ void b_scale_kernel(T* __restrict__ x, const T* __restrict__ s, long 
     x[off + i] *= s[i];
 }
 
-// After the z transform: for every z mode j and instance k, the banded
-// solve (Ky + lz_j My) x = t along y with the Cholesky factor (forward and
-// back substitution), in place.  t is the Nz x Ny*K column-major matrix of
-// the transform, so consecutive threads (consecutive j) touch consecutive
-// addresses; the last eight values of the sweep stay in registers.
-template <typename T, int R, int RB>
-__global__ void __launch_bounds__(128) b_ysolve_kernel(const T* __restrict__ Lb, T* __restrict__ t, int Ny, int Nz,
-                                                       int K) {
-  // A thread sweeps the systems of one z mode j for R instances at once
-  // (every factor coefficient loaded once for the R sweeps), rows taken RB
-  // at a time (their loads issued together).  Both sweeps run column by
-  // column: as soon as a value is known, its column of the factor is added
-  // into the partial sums of the next eight rows (acc), so a row waits only
-  // for one multiply-add on the previous row's value.
-  const int KR = (K + R - 1) / R;
-  const long g = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (g >= (long)Nz * KR) return;
-  const int j = (int)(g % Nz), k0 = (int)(g / Nz) * R;
-  const long NN = (long)Ny * Nz;
-  T* col = t + (long)k0 * NN + j;
-  const int nr = min(R, K - k0);
-  const T* L = Lb + j;
-  T acc[R][8];
-#pragma unroll
-  for (int q = 0; q < R; ++q)
-#pragma unroll
-    for (int m = 0; m < 8; ++m) acc[q][m] = T(0);
-  // forward, L y = b: y(i) = (b(i) - acc(i)) / L(i, i), then acc(i+m) += L(i+m, i) y(i)
-  for (int i0 = 0; i0 < Ny; i0 += RB) {
-    T cf[RB][9], bv[RB][R];
-#pragma unroll
-    for (int r = 0; r < RB; ++r) {
-      const int i = i0 + r;  // rows up to Ny + RB + 7 are read: the table has Ny + 8 rows, see below
-      cf[r][0] = i < Ny ? L[(long)i * 9 * Nz] : T(0);
-#pragma unroll
-      for (int m = 1; m <= 8; ++m) cf[r][m] = i < Ny ? L[((long)(i + m) * 9 + m) * Nz] : T(0);
-#pragma unroll
-      for (int q = 0; q < R; ++q) bv[r][q] = (i < Ny && q < nr) ? col[q * NN + (long)i * Nz] : T(0);
-    }
-#pragma unroll
-    for (int r = 0; r < RB; ++r) {
-      const int i = i0 + r;
-      if (i < Ny) {
-#pragma unroll
-        for (int q = 0; q < R; ++q) {
-          const T y = (bv[r][q] - acc[q][0]) * cf[r][0];
-          if (q < nr) col[q * NN + (long)i * Nz] = y;
-#pragma unroll
-          for (int m = 0; m < 7; ++m) acc[q][m] = acc[q][m + 1] + cf[r][m + 1] * y;
-          acc[q][7] = cf[r][8] * y;
-        }
-      }
-    }
-  }
-#pragma unroll
-  for (int q = 0; q < R; ++q)
-#pragma unroll
-    for (int m = 0; m < 8; ++m) acc[q][m] = T(0);
-  // back, L^T x = y: x(i) = (y(i) - acc(i)) / L(i, i), then acc(i-m) += L(i, i-m) x(i)
-  for (int i0 = Ny - 1; i0 >= 0; i0 -= RB) {
-    T cf[RB][9], bv[RB][R];
-#pragma unroll
-    for (int r = 0; r < RB; ++r) {
-      const int i = i0 - r;
-      const bool in = i >= 0;
-#pragma unroll
-      for (int m = 0; m <= 8; ++m) cf[r][m] = in ? L[((long)i * 9 + m) * Nz] : T(0);
-#pragma unroll
-      for (int q = 0; q < R; ++q) bv[r][q] = (in && q < nr) ? col[q * NN + (long)i * Nz] : T(0);
-    }
-#pragma unroll
-    for (int r = 0; r < RB; ++r) {
-      const int i = i0 - r;
-      if (i >= 0) {
-#pragma unroll
-        for (int q = 0; q < R; ++q) {
-          const T x = (bv[r][q] - acc[q][0]) * cf[r][0];
-          if (q < nr) col[q * NN + (long)i * Nz] = x;
-#pragma unroll
-          for (int m = 0; m < 7; ++m) acc[q][m] = acc[q][m + 1] + cf[r][m + 1] * x;
-          acc[q][7] = cf[r][8] * x;
-        }
-      }
-    }
-  }
+template <typename T>
+__device__ __forceinline__ T fma_t(T a, T b, T c);
+template <>
+__device__ __forceinline__ double fma_t<double>(double a, double b, double c) {
+  return fma(a, b, c);
+}
+template <>
+__device__ __forceinline__ float fma_t<float>(float a, float b, float c) {
+  return fmaf(a, b, c);
 }
 
-// The banded sweeps fed by the tensor memory accelerator.  A block owns
-// YS_C = 16 consecutive z modes of YS_B = 8 instances: lane c + 16 h of warp
-// w carries the chains of mode j0 + c for the YS_I = 2 instances
-// (2 w + h) * 2 + s, so one read of a factor value from shared memory serves
-// two chains, and lanes c and c + 16 read the same value (a broadcast).  Per
-// chunk of YS_R = 16 rows one 2D copy brings the factor (16 rows x 9 table
-// rows x 16 modes) and one 3D copy the transform of all eight instances
-// (16 modes x 16 rows x 8 instances); YS_S = 3 stages, so two chunks are in
-// flight while one is swept.  Every chunk is swept over all 16 rows: rows
-// outside 0..Ny-1 arrive as zeros (factor and data), give zero and only
-// shift the accumulators, and are not stored.  A wait that runs out sets
-// status bit 4 of the block's instances (their solve is then repeated) and
-// the block stops.
-constexpr int YS_R = 16, YS_C = 16, YS_I = 2, YS_W = 2, YS_S = 3;
-constexpr int YS_B = YS_W * (32 / YS_C) * YS_I;  // instances per block
+// After the z transform: for every z mode j and instance k, the banded
+// solve (Ky + lz_j My) x = t along y with the Cholesky factor L (forward
+// L y = t, back L^T x = y), in place in t (rows of Nzp values, instance k
+// at rows k Ny ..).  The factor tables hold, per row i and mode j, nine
+// values in the order the row is processed: [0] 1 / L_ii, [1] the coupling
+// to the row processed just before, already divided by L_ii (forward
+// L(i, i-1) / L_ii, back L(i+1, i) / L_ii), [2..8] the contributions of
+// row i to the rows 2..8 further on (forward L(i+m, i), back L(i, i-m)).
+// With the coupling folded in, a row costs one dependent FMA on the chain:
+//   x_i = (t_i - b_i) / L_ii - c1_i x_prev
+// where b_i collects the contributions of the rows before x_prev.
+//
+// Tensor-memory-accelerator feed: a block owns YS_C = 16 consecutive z
+// modes of B = 2 W I instances: lane c + 16 h of warp w carries the chains
+// of mode j0 + c for the I instances (2 w + h) I + s, so one read of a
+// factor value from shared memory serves I chains, and lanes c and c + 16
+// read the same value (a broadcast).  Per chunk of YS_R = 16 rows one 2D
+// copy brings the factor (16 rows x 9 table rows x 16 modes) and one 3D copy
+// the transform of the block's instances (16 modes x 16 rows x B); YS_S = 3
+// stages, so two chunks are in flight while one is swept.  Every chunk is
+// swept over all 16 rows: rows outside 0..Ny-1 arrive as zeros (factor and
+// data), give zero and only shift the accumulators, and are not stored.  A
+// wait that runs out sets status bit 4 of the block's instances (their solve
+// is then repeated) and the block stops.
+constexpr int YS_R = 16, YS_C = 16, YS_S = 3;
+constexpr int YS_I = 2, YS_W = 2;          // chains per lane, warps per block
+constexpr int YS_B = 2 * YS_W * YS_I;      // instances per block
 
-template <typename T>
-__global__ void __launch_bounds__(32 * YS_W) b_ysolve_tma_kernel(const __grid_constant__ CUtensorMap mLcol,
-                                                                 const __grid_constant__ CUtensorMap mLrow,
-                                                                 const __grid_constant__ CUtensorMap mT,
-                                                                 T* __restrict__ t, int Ny, int Nz, int Nzp, int K,
-                                                                 unsigned* __restrict__ status) {
+template <typename T, int I, int W>
+__global__ void __launch_bounds__(32 * W) b_ysolve_tma_kernel(const __grid_constant__ CUtensorMap mLcol,
+                                                              const __grid_constant__ CUtensorMap mLrow,
+                                                              const __grid_constant__ CUtensorMap mT,
+                                                              T* __restrict__ t, int Ny, int Nz, int Nzp, int K,
+                                                              unsigned* __restrict__ status) {
+  constexpr int B = 2 * W * I;
   extern __shared__ __align__(128) unsigned char ys_smem[];
-  constexpr int CT = YS_R * 9 * YS_C, DT = YS_B * YS_R * YS_C;  // elements per tile
-  T* coef = reinterpret_cast<T*>(ys_smem);                      // [YS_S][YS_R][9][YS_C]
-  T* dat = coef + YS_S * CT;                                    // [YS_S][YS_B][YS_R][YS_C]
+  constexpr int CT = YS_R * 9 * YS_C, DT = B * YS_R * YS_C;  // elements per tile
+  T* coef = reinterpret_cast<T*>(ys_smem);                   // [YS_S][YS_R][9][YS_C]
+  T* dat = coef + YS_S * CT;                                 // [YS_S][B][YS_R][YS_C]
   uint64_t* bar = reinterpret_cast<uint64_t*>(dat + YS_S * DT);
   const int lane = threadIdx.x & 31, c = lane % YS_C, h = lane / YS_C, wv = threadIdx.x >> 5;
-  const int j0 = blockIdx.x * YS_C, j = j0 + c, kb = blockIdx.y * YS_B;
-  int kk[YS_I];
-  bool valid[YS_I];
-  T* colp[YS_I];
+  const int j0 = blockIdx.x * YS_C, j = j0 + c, kb = blockIdx.y * B;
+  const int kk0 = (wv * 2 + h) * I;  // the lane's first instance in the block
+  bool valid[I];
+  T* colp[I];
 #pragma unroll
-  for (int s = 0; s < YS_I; ++s) {
-    kk[s] = (wv * (32 / YS_C) + h) * YS_I + s;
-    const int k = kb + kk[s];
+  for (int s = 0; s < I; ++s) {
+    const int k = kb + kk0 + s;
     valid[s] = j < Nz && k < K;
     colp[s] = t + (long)min(k, K - 1) * Ny * Nzp + j;
   }
@@ -488,11 +502,36 @@ __global__ void __launch_bounds__(32 * YS_W) b_ysolve_tma_kernel(const __grid_co
   if (leader)
     for (int q = 0; q < YS_S && q < nch; ++q) issue(q);
   bool ok = true;
-  T acc[YS_I][8];
+  // per chain: the previous row's value, the contributions b to the current
+  // row, and a[m] the contributions to the rows m + 1 .. 7 further on
+  T xp[I], b[I], a[I][7];
+  auto reset = [&]() {
 #pragma unroll
-  for (int s = 0; s < YS_I; ++s)
+    for (int s = 0; s < I; ++s) {
+      xp[s] = b[s] = T(0);
 #pragma unroll
-    for (int m = 0; m < 8; ++m) acc[s][m] = T(0);
+      for (int m = 0; m < 7; ++m) a[s][m] = T(0);
+    }
+  };
+  reset();
+  // one row r of the chunk in stage st; stored at colp[s] + off when in range
+  auto row = [&](const T* cf, const T* dv, int r, long off, bool in) {
+    const T* cr = cf + r * 9 * YS_C;
+    T cm[9];
+#pragma unroll
+    for (int m = 0; m < 9; ++m) cm[m] = cr[m * YS_C];
+#pragma unroll
+    for (int s = 0; s < I; ++s) {
+      const T tt = (dv[((kk0 + s) * YS_R + r) * YS_C] - b[s]) * cm[0];
+      const T x = fma_t<T>(-cm[1], xp[s], tt);
+      if (valid[s] && in) colp[s][off] = x;
+      b[s] = a[s][0];
+#pragma unroll
+      for (int m = 0; m < 6; ++m) a[s][m] = fma_t<T>(cm[m + 2], x, a[s][m + 1]);
+      a[s][6] = cm[8] * x;
+      xp[s] = x;
+    }
+  };
   int g = 0;
   for (; g < 2 * nch; ++g) {
     if (g == nch) {
@@ -502,10 +541,7 @@ __global__ void __launch_bounds__(32 * YS_W) b_ysolve_tma_kernel(const __grid_co
       __syncthreads();
       if (leader)
         for (int q = nch; q < nch + YS_S && q < 2 * nch; ++q) issue(q);
-#pragma unroll
-      for (int s = 0; s < YS_I; ++s)
-#pragma unroll
-        for (int m = 0; m < 8; ++m) acc[s][m] = T(0);
+      reset();
     }
     const int st = g % YS_S;
     ok = mbar_wait(&bar[st], (g / YS_S) & 1, kPolls);
@@ -515,24 +551,21 @@ __global__ void __launch_bounds__(32 * YS_W) b_ysolve_tma_kernel(const __grid_co
     }
     const T* cf = coef + st * CT + c;
     const T* dv = dat + st * DT + c;
-    const bool fwd = g < nch;
-    const int lo = fwd ? g * YS_R : Ny - (g - nch + 1) * YS_R;
+    if (g < nch) {
+      const int i0 = g * YS_R;
+      long off = (long)i0 * Nzp;
 #pragma unroll
-    for (int q = 0; q < YS_R; ++q) {
-      const int r = fwd ? q : YS_R - 1 - q;
-      const int i = lo + r;
-      const bool in = i >= 0 && i < Ny;
-      const T* cr = cf + r * 9 * YS_C;
-      T cm[9];
+      for (int r = 0; r < YS_R; ++r) {
+        row(cf, dv, r, off, i0 + r < Ny);
+        off += Nzp;
+      }
+    } else {
+      const int lo = Ny - (g - nch + 1) * YS_R;
+      long off = (long)(lo + YS_R - 1) * Nzp;
 #pragma unroll
-      for (int m = 0; m < 9; ++m) cm[m] = cr[m * YS_C];
-#pragma unroll
-      for (int s = 0; s < YS_I; ++s) {
-        const T y = (dv[(kk[s] * YS_R + r) * YS_C] - acc[s][0]) * cm[0];
-        if (valid[s] && in) colp[s][(long)i * Nzp] = y;
-#pragma unroll
-        for (int m = 0; m < 7; ++m) acc[s][m] = acc[s][m + 1] + cm[m + 1] * y;
-        acc[s][7] = cm[8] * y;
+      for (int r = YS_R - 1; r >= 0; --r) {
+        row(cf, dv, r, off, lo + r >= 0);
+        off -= Nzp;
       }
     }
     __syncthreads();  // every warp is done with stage st
@@ -541,7 +574,7 @@ __global__ void __launch_bounds__(32 * YS_W) b_ysolve_tma_kernel(const __grid_co
   }
   if (!ok) {
     if (leader) {
-      for (int q = 0; q < YS_B && kb + q < K; ++q) atomicOr(status + kb + q, 4u);
+      for (int q = 0; q < B && kb + q < K; ++q) atomicOr(status + kb + q, 4u);
       // let the loads already issued land before the block's shared memory goes
       for (int q = g; q < g + YS_S && q < 2 * nch; ++q) mbar_wait(&bar[q % YS_S], (q / YS_S) & 1, kPolls);
     }
@@ -906,7 +939,13 @@ int BatchContext::setup_group(int base, int K) {
   g.w.PB = std::max(tiles, node_blocks(g.N));
   // instances per block of the operator kernels: enough blocks for about
   // four per SM, at most eight instances each
-  g.kpb = (int)std::max(1L, std::min(8L, (long)g.K * tiles / (148L * 4)));
+  g.kpb = (int)std::max(1L, std::min((long)XKPB, (long)g.K * tiles / (148L * 4)));
+  SCY_CUDA_TRY(cudaFuncSetAttribute(b_cross_kernel<0, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    xs_smem_bytes(0, 8)));
+  SCY_CUDA_TRY(cudaFuncSetAttribute(b_cross_kernel<1, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    xs_smem_bytes(1, 8)));
+  SCY_CUDA_TRY(cudaFuncSetAttribute(b_cross_kernel<1, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    xs_smem_bytes(1, 4)));
   {
     std::vector<double> planes;
     build_cross_planes(q0.sbp.hosts[0], planes);
@@ -994,9 +1033,9 @@ int BatchContext::setup_group(int base, int K) {
     SCY_TRY(tma_map_2d(&g.mLrow32, g.fd->Lrow32.p, d32, 4, g.Nz, (long)(g.Ny + 8) * 9, (long)Nzp * 4, YS_C, YS_R * 9));
     SCY_TRY(tma_map_3d(&g.mT32, g.t1pf.p, d32, g.Nz, g.Ny, g.K, (long)Nzp * 4, (long)g.Ny * Nzp * 4, YS_C, YS_R,
                        YS_B));
-    SCY_CUDA_TRY(cudaFuncSetAttribute(b_ysolve_tma_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    SCY_CUDA_TRY(cudaFuncSetAttribute(b_ysolve_tma_kernel<double, YS_I, YS_W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       ys_smem_bytes(8)));
-    SCY_CUDA_TRY(cudaFuncSetAttribute(b_ysolve_tma_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    SCY_CUDA_TRY(cudaFuncSetAttribute(b_ysolve_tma_kernel<float, YS_I, YS_W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       ys_smem_bytes(4)));
   }
   SCY_TRY(g.tab.alloc(sizeof(BatchInst) * g.K));
@@ -1079,7 +1118,7 @@ int BatchContext::fd_apply(BatchGroup& g) {
                                t1, F.Nzp));
       cudaEvent_t pa;
       SCY_TRY(prof_begin(g.stream, &pa));
-      b_ysolve_tma_kernel<float><<<dim3((Nz + YS_C - 1) / YS_C, (K + YS_B - 1) / YS_B), 32 * YS_W, ys_smem_bytes(4),
+      b_ysolve_tma_kernel<float, YS_I, YS_W><<<dim3((Nz + YS_C - 1) / YS_C, (K + YS_B - 1) / YS_B), 32 * YS_W, ys_smem_bytes(4),
                                    g.stream>>>(g.mLcol32, g.mLrow32, g.mT32, t1, Ny, Nz, F.Nzp, K, g.w.status);
       SCY_LAUNCH_CHECK();
       SCY_TRY(prof_end(g.stream, pa, PROF_YSOLVE, 4.0 * (9.0 * Ny * Nz + 4.0 * N * K)));
@@ -1094,7 +1133,7 @@ int BatchContext::fd_apply(BatchGroup& g) {
                                F.Nzp));
       cudaEvent_t pa;
       SCY_TRY(prof_begin(g.stream, &pa));
-      b_ysolve_tma_kernel<double><<<dim3((Nz + YS_C - 1) / YS_C, (K + YS_B - 1) / YS_B), 32 * YS_W,
+      b_ysolve_tma_kernel<double, YS_I, YS_W><<<dim3((Nz + YS_C - 1) / YS_C, (K + YS_B - 1) / YS_B), 32 * YS_W,
                                     ys_smem_bytes(8), g.stream>>>(g.mLcol, g.mLrow, g.mT, t1, Ny, Nz, F.Nzp, K,
                                                                   g.w.status);
       SCY_LAUNCH_CHECK();
@@ -1154,7 +1193,7 @@ int BatchContext::solve(BatchGroup& g, const int* mask, int its_now) {
   const double nact = (double)active_in(g, mask);
   cudaEvent_t pa;
   SCY_TRY(prof_begin(g.stream, &pa));
-  b_cross_kernel<0, double><<<tg, 256, 0, g.stream>>>(C, g.Ny, g.Nz, tab, mask, g.w, nullptr, 0, 0, mixed, g.kpb);
+  b_cross_kernel<0, double><<<tg, 256, xs_smem_bytes(0, 8), g.stream>>>(C, g.Ny, g.Nz, tab, mask, g.w, nullptr, 0, 0, mixed, g.kpb);
   SCY_LAUNCH_CHECK();
   SCY_TRY(prof_end(g.stream, pa, PROF_RESIDUAL, 33.0 * 8 * g.N + nact * g.N * (24.0 + (mixed ? 4 : 0))));
   b_partials_kernel<<<g.K, 256, 0, g.stream>>>(mask, g.w, ntiles, 5);
@@ -1169,10 +1208,10 @@ int BatchContext::solve(BatchGroup& g, const int* mask, int its_now) {
     SCY_LAUNCH_CHECK();
     SCY_TRY(prof_begin(g.stream, &pa));
     if (mixed)
-      b_cross_kernel<1, float><<<tg, 256, 0, g.stream>>>(C, g.Ny, g.Nz, tab, mask, g.w, g.w.z32, it == 1 ? 1 : 0,
+      b_cross_kernel<1, float><<<tg, 256, xs_smem_bytes(1, 4), g.stream>>>(C, g.Ny, g.Nz, tab, mask, g.w, g.w.z32, it == 1 ? 1 : 0,
                                                           pi, mixed, g.kpb);
     else
-      b_cross_kernel<1, double><<<tg, 256, 0, g.stream>>>(C, g.Ny, g.Nz, tab, mask, g.w, g.w.z, it == 1 ? 1 : 0,
+      b_cross_kernel<1, double><<<tg, 256, xs_smem_bytes(1, 8), g.stream>>>(C, g.Ny, g.Nz, tab, mask, g.w, g.w.z, it == 1 ? 1 : 0,
                                                            pi, mixed, g.kpb);
     SCY_LAUNCH_CHECK();
     SCY_TRY(prof_end(g.stream, pa, PROF_MATVEC, 33.0 * 8 * g.N + nact * g.N * (mixed ? 28.0 : 32.0)));

@@ -229,18 +229,25 @@ int FDPrecond::build(const LevelHost& L, cudaStream_t s) {
           }
       }
       if (spd) {
-        SCY_TRY(upload_as<double>(Lb, Lbh, s));
-        SCY_TRY(upload_as<float>(Lb32, Lbh, s));
         // padded row and column forms for the TMA-fed sweeps
         Nzp = (Nz + 3) / 4 * 4;
         std::vector<double> Lr((size_t)(Ny + bw) * 9 * Nzp, 0.0), Lc((size_t)Ny * 9 * Nzp, 0.0);
+        // slot 1 holds the coupling to the row processed just before,
+        // divided by L_ii: L(i+1, i) / L_ii going up (row form), L(i, i-1) /
+        // L_ii going down (column form)
         for (int i = 0; i < Ny + bw; ++i)
           for (int k = 0; k < 9; ++k)
-            for (int j = 0; j < Nz; ++j) Lr[((size_t)i * 9 + k) * Nzp + j] = Lbh[((size_t)i * 9 + k) * Nz + j];
+            for (int j = 0; j < Nz; ++j) {
+              double v = Lbh[((size_t)i * 9 + k) * Nz + j];
+              if (k == 1)
+                v = i + 1 < Ny + bw ? Lbh[((size_t)(i + 1) * 9 + 1) * Nz + j] * Lbh[((size_t)i * 9) * Nz + j] : 0.0;
+              Lr[((size_t)i * 9 + k) * Nzp + j] = v;
+            }
         for (int i = 0; i < Ny; ++i)
           for (int j = 0; j < Nz; ++j) {
             Lc[((size_t)i * 9) * Nzp + j] = Lbh[((size_t)i * 9) * Nz + j];
-            for (int m = 1; m <= bw; ++m) Lc[((size_t)i * 9 + m) * Nzp + j] = Lbh[((size_t)(i + m) * 9 + m) * Nz + j];
+            Lc[((size_t)i * 9 + 1) * Nzp + j] = Lbh[((size_t)i * 9 + 1) * Nz + j] * Lbh[((size_t)i * 9) * Nz + j];
+            for (int m = 2; m <= bw; ++m) Lc[((size_t)i * 9 + m) * Nzp + j] = Lbh[((size_t)(i + m) * 9 + m) * Nz + j];
           }
         SCY_TRY(upload_as<double>(Lrow, Lr, s));
         SCY_TRY(upload_as<double>(Lcol, Lc, s));

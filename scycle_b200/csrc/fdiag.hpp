@@ -27,15 +27,15 @@ struct FDPrecond {
   // Banded form of the y part (ybanded = 1 when the symmetric part of the y
   // line operator has half-bandwidth <= 8): after the z transform the
   // operator splits into one banded SPD system per z mode j,
-  // Ky + lz_j My, solved with its Cholesky factor L_j.  Layout
-  // [(iy * 9 + k) * Nz + j] = L_j(iy, iy - k) for k = 1..8 and 1 / L_j(iy, iy)
-  // for k = 0, with 8 zero rows after the last (Ny + 8 rows in all).
+  // Ky + lz_j My, solved with its Cholesky factor L_j.  The factors are
+  // kept for the TMA-fed sweeps, rows padded to Nzp (a multiple of 4)
+  // values: row form [(i * 9 + m) * Nzp + j] = L_j(i, i - m) (Ny + 8
+  // rows), column form [(i * 9 + m) * Nzp + j] = L_j(i + m, i) (Ny rows)
+  // for m = 2..8; slot m = 0 holds 1 / L_j(i, i) in both, slot 1 the
+  // coupling to the row a sweep processes just before row i over L_j(i, i):
+  // L_j(i + 1, i) / L_j(i, i) in the row form (back sweep, rows going up),
+  // L_j(i, i - 1) / L_j(i, i) in the column form (forward sweep).
   int ybanded = 0;
-  DevBuf Lb, Lb32;
-  // The same factors for the TMA-fed sweeps, rows padded to Nzp (a multiple
-  // of 4) values: row form [(i * 9 + m) * Nzp + j] = L_j(i, i - m) (Ny + 8
-  // rows), column form [(i * 9 + m) * Nzp + j] = L_j(i + m, i) (Ny rows);
-  // slot m = 0 holds 1 / L_j(i, i) in both.
   int Nzp = 0;
   DevBuf Lrow, Lcol, Lrow32, Lcol32;
   ~FDPrecond();
