@@ -230,9 +230,24 @@ __global__ void __launch_bounds__(256) b_cross_kernel(const double* __restrict__
     }
     nact = n;
   }
-  double c[33];
+  // y arm: c[0..16] for rows iy-8..iy+8.  z arm: read as 16-byte pairs
+  // from the even column at or below iz-8 (nine pairs, columns
+  // (iz & ~1) - 8 .. + 17), so its coefficients are held shifted by the
+  // lane's parity e: c[17 + o] multiplies column (iz & ~1) - 8 + o, zero at
+  // the centre and outside the arm
+  const int e = tz & 1;
+  double c[35];
 #pragma unroll
-  for (int o = 0; o < 33; ++o) c[o] = valid ? C[(long)o * N + node] : 0.0;
+  for (int o = 0; o < 17; ++o) c[o] = valid ? C[(long)o * N + node] : 0.0;
+  {
+    double cz[18];  // by z offset + 8, with the centre 0 and cz[17] = 0
+#pragma unroll
+    for (int o = 0; o < 18; ++o)
+      cz[o] = (valid && o != 8 && o < 17) ? C[(long)(o < 8 ? 17 + o : 16 + o) * N + node] : 0.0;
+    c[17] = e ? 0.0 : cz[0];
+#pragma unroll
+    for (int o = 1; o < 18; ++o) c[17 + o] = e ? cz[o - 1] : cz[o];
+  }
   // the staged positions do not depend on the instance: their node offsets
   // (-1 outside the grid) are worked out once
   int src[NV];
@@ -323,14 +338,16 @@ __global__ void __launch_bounds__(256) b_cross_kernel(const double* __restrict__
     double contrib = 0.0;
     if (valid) {
       const double* ay = X + ty * XTZ + tz;                   // row iy - 8
-      const double* az = X + XNY + ty * (XTZ + 2 * XH) + tz;  // column iz - 8
+      const double2* az = reinterpret_cast<const double2*>(X + XNY + ty * (XTZ + 2 * XH) + (tz - e));
       double Ay = 0.0, Az = 0.0;
 #pragma unroll
       for (int o = 0; o < 17; ++o) Ay += c[o] * ay[o * XTZ];
 #pragma unroll
-      for (int o = 0; o < 8; ++o) Az += c[17 + o] * az[o];
-#pragma unroll
-      for (int o = 9; o < 17; ++o) Az += c[16 + o] * az[o];
+      for (int m = 0; m < 9; ++m) {
+        const double2 v = az[m];
+        Az += c[17 + 2 * m] * v.x;
+        Az += c[18 + 2 * m] * v.y;
+      }
       const double Ax = Ay + Az;
       if (MODE == 0) {
         const double vv = sck[q] == 0.0 ? 0.0 : -1.0 * rs[st * 256 + tid] + Ax;
