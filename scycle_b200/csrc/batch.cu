@@ -196,7 +196,7 @@ __global__ void __launch_bounds__(256) b_cross_kernel(const double* __restrict__
                                                       int mixed, int kpb) {
   constexpr int NV = (XNS + 255) / 256;  // staged values per thread
   extern __shared__ __align__(16) unsigned char xsm[];
-  __shared__ double red[8];
+  __shared__ double red[XKPB][8];  // warp sums by instance
   __shared__ int act[XKPB];                // the block's active instances
   __shared__ double sck[XKPB];             // MODE 0: |rhs|^2 (0: rhs = 0); MODE 1: beta
   __shared__ const double* srck[XKPB][2];  // MODE 0: u, rhs
@@ -362,18 +362,21 @@ __global__ void __launch_bounds__(256) b_cross_kernel(const double* __restrict__
         contrib = p * qv;
       }
     }
-    // block partial of this instance (warp sums, then warp 0 adds the 8 in
-    // order); b_partials_kernel adds the tiles up
+    // warp sums of this instance; the block partials are formed at the end
     contrib = warp_sum(contrib);
-    if ((tid & 31) == 0) red[tid >> 5] = contrib;
-    __syncthreads();
-    if (tid < 32) {
-      double t = tid < 8 ? red[tid] : 0.0;
-      t = warp_sum(t);
-      if (tid == 0) w.partials[(long)k * w.PB + tile] = t;
-    }
+    if ((tid & 31) == 0) red[q][tid >> 5] = contrib;
   }
   cp_async_wait<0>();
+  // block partial of every instance (warp 0 adds the 8 warp sums in order);
+  // b_partials_kernel adds the tiles up
+  __syncthreads();
+  if (tid < 32) {
+    for (int q = 0; q < na; ++q) {
+      double t = tid < 8 ? red[q][tid] : 0.0;
+      t = warp_sum(t);
+      if (tid == 0) w.partials[(long)act[q] * w.PB + tile] = t;
+    }
+  }
 }
 
 // sc[16 k + slot] = sum of the instance's first n partials, in tile order
