@@ -249,8 +249,10 @@ __global__ void __launch_bounds__(256) b_cross_kernel(const double* __restrict__
     for (int o = 1; o < 18; ++o) c[17 + o] = e ? cz[o - 1] : cz[o];
   }
   // the staged positions do not depend on the instance: their node offsets
-  // (-1 outside the grid) are worked out once
+  // (0 outside the grid, where bit a of inb is clear and nothing is read)
+  // are worked out once
   int src[NV];
+  unsigned inb = 0;
 #pragma unroll
   for (int a = 0; a < NV; ++a) {
     const int i = tid + 256 * a;
@@ -263,7 +265,9 @@ __global__ void __launch_bounds__(256) b_cross_kernel(const double* __restrict__
       jy = y0 + e / (XTZ + 2 * XH);
       jz = z0 - XH + e % (XTZ + 2 * XH);
     }
-    src[a] = (jy >= 0 && jy < Ny && jz >= 0 && jz < Nz) ? jy * Nz + jz : -1;
+    const bool in = jy >= 0 && jy < Ny && jz >= 0 && jz < Nz;
+    src[a] = in ? jy * Nz + jz : 0;
+    inb |= (in ? 1u : 0u) << a;
   }
   __syncthreads();
   const int na = nact;
@@ -279,11 +283,10 @@ __global__ void __launch_bounds__(256) b_cross_kernel(const double* __restrict__
       const int st = q % XS;
       if (MODE == 0) {
         const double* x = srck[q][0];
+        double* d = us + st * XNS + tid;
 #pragma unroll
-        for (int a = 0; a < NV; ++a) {
-          const int i = tid + 256 * a;
-          if (i < XNS) cp_async8(us + st * XNS + i, src[a] >= 0 ? x + src[a] : x, src[a] >= 0 ? 8 : 0);
-        }
+        for (int a = 0; a < NV; ++a)
+          if (tid + 256 * a < XNS) cp_async8(d + 256 * a, x + src[a], (inb >> a & 1u) * 8);
         const double* rh = srck[q][1];
         const bool rv = valid && sck[q] != 0.0;
         cp_async8(rs + st * 256 + tid, rv ? rh + node : rh, rv ? 8 : 0);
@@ -295,12 +298,12 @@ __global__ void __launch_bounds__(256) b_cross_kernel(const double* __restrict__
         for (int a = 0; a < NV; ++a) {
           const int i = tid + 256 * a;
           if (i >= XNS) continue;
-          const bool in = src[a] >= 0;
+          const unsigned in = inb >> a & 1u;
           if (sizeof(Tz) == 4)
-            cp_async4(zs + st * XNS + i, in ? zz + src[a] : zz, in ? 4 : 0);
+            cp_async4(zs + st * XNS + i, zz + src[a], in * 4);
           else
-            cp_async8(zs + st * XNS + i, in ? zz + src[a] : zz, in ? 8 : 0);
-          if (!first) cp_async8(ps + st * XNS + i, in ? pold + src[a] : pold, in ? 8 : 0);
+            cp_async8(zs + st * XNS + i, zz + src[a], in * 8);
+          if (!first) cp_async8(ps + st * XNS + i, pold + src[a], in * 8);
         }
       }
     }
@@ -339,16 +342,20 @@ __global__ void __launch_bounds__(256) b_cross_kernel(const double* __restrict__
     if (valid) {
       const double* ay = X + ty * XTZ + tz;                   // row iy - 8
       const double2* az = reinterpret_cast<const double2*>(X + XNY + ty * (XTZ + 2 * XH) + (tz - e));
-      double Ay = 0.0, Az = 0.0;
+      // four partial sums (even / odd offsets of each arm), so the FMA
+      // chains are short
+      double Ay0 = 0.0, Ay1 = 0.0, Az0 = 0.0, Az1 = 0.0;
 #pragma unroll
-      for (int o = 0; o < 17; ++o) Ay += c[o] * ay[o * XTZ];
+      for (int o = 0; o < 17; o += 2) Ay0 += c[o] * ay[o * XTZ];
+#pragma unroll
+      for (int o = 1; o < 17; o += 2) Ay1 += c[o] * ay[o * XTZ];
 #pragma unroll
       for (int m = 0; m < 9; ++m) {
         const double2 v = az[m];
-        Az += c[17 + 2 * m] * v.x;
-        Az += c[18 + 2 * m] * v.y;
+        Az0 += c[17 + 2 * m] * v.x;
+        Az1 += c[18 + 2 * m] * v.y;
       }
-      const double Ax = Ay + Az;
+      const double Ax = (Ay0 + Ay1) + (Az0 + Az1);
       if (MODE == 0) {
         const double vv = sck[q] == 0.0 ? 0.0 : -1.0 * rs[st * 256 + tid] + Ax;
         w.r[off + node] = vv;
