@@ -164,7 +164,8 @@ __global__ void b_dot_rz_kernel(const int* __restrict__ mask, BatchWork w, const
 // the copies of the next two instances are in flight while one is computed.
 //   MODE 0: r = -rhs + A u (0 where rhs = 0), r.r -> sc[5]
 //   MODE 1: p = z + beta p_old (beta = rz / rz_old; p = z on the first
-//           iteration), q = -A p, p stored, p.q -> sc[4]
+//           iteration), q = -A p, p stored (unless store_p = 0), p.q ->
+//           partials; on the first iteration also r.z -> partials2
 constexpr int XTY = 8, XTZ = 32, XH = 8, XS = 3, XKPB = 8;
 constexpr int XNY = (XTY + 2 * XH) * XTZ, XNZ = XTY * (XTZ + 2 * XH), XNS = XNY + XNZ;
 
@@ -183,20 +184,21 @@ __device__ __forceinline__ void cp_async_wait() {
 }
 
 // dynamic shared memory of b_cross_kernel: MODE 0 stages the operand and
-// the rhs of the tile; MODE 1 stages z (zsize bytes a value) and p_old and
-// forms p in one more buffer
+// the rhs of the tile; MODE 1 stages z (zsize bytes a value), p_old and the
+// tile's r, and forms p in one more buffer
 constexpr int xs_smem_bytes(int mode, int zsize) {
-  return mode == 0 ? XS * (XNS + 256) * 8 : (XS * XNS * zsize + 15) / 16 * 16 + XS * XNS * 8 + XNS * 8;
+  return mode == 0 ? XS * (XNS + 256) * 8 : (XS * XNS * zsize + 15) / 16 * 16 + XS * XNS * 8 + XNS * 8 + XS * 256 * 8;
 }
 
 template <int MODE, typename Tz>
 __global__ void __launch_bounds__(256) b_cross_kernel(const double* __restrict__ C, int Ny, int Nz,
                                                       const BatchInst* __restrict__ tab, const int* __restrict__ mask,
                                                       BatchWork w, const Tz* __restrict__ zv, int first, int pi,
-                                                      int mixed, int kpb) {
+                                                      int mixed, int kpb, int store_p = 1) {
   constexpr int NV = (XNS + 255) / 256;  // staged values per thread
   extern __shared__ __align__(16) unsigned char xsm[];
   __shared__ double red[XKPB][8];  // warp sums by instance
+  __shared__ double red2[MODE == 1 ? XKPB : 1][8];
   __shared__ int act[XKPB];                // the block's active instances
   __shared__ double sck[XKPB];             // MODE 0: |rhs|^2 (0: rhs = 0); MODE 1: beta
   __shared__ const double* srck[XKPB][2];  // MODE 0: u, rhs
@@ -276,6 +278,7 @@ __global__ void __launch_bounds__(256) b_cross_kernel(const double* __restrict__
   Tz* zs = reinterpret_cast<Tz*>(xsm);  // MODE 1: [XS][XNS] z, [XS][XNS] p_old, [XNS] p
   double* ps = reinterpret_cast<double*>(xsm + (XS * XNS * sizeof(Tz) + 15) / 16 * 16);
   double* xd = ps + XS * XNS;
+  double* rr = xd + XNS;  // MODE 1: [XS][256] r of the tile (first iteration)
   // copies of the q-th active instance into stage q % XS (one commit group
   // per call, empty past the last instance)
   auto issue = [&](int q) {
@@ -305,6 +308,7 @@ __global__ void __launch_bounds__(256) b_cross_kernel(const double* __restrict__
             cp_async8(zs + st * XNS + i, zz + src[a], in * 8);
           if (!first) cp_async8(ps + st * XNS + i, pold + src[a], in * 8);
         }
+        if (first) cp_async8(rr + st * 256 + tid, w.r + off + (valid ? node : 0), valid ? 8 : 0);
       }
     }
     cp_async_commit();
@@ -338,7 +342,7 @@ __global__ void __launch_bounds__(256) b_cross_kernel(const double* __restrict__
       }
     }
     const long off = (long)k * N;
-    double contrib = 0.0;
+    double contrib = 0.0, rz = 0.0;
     if (valid) {
       const double* ay = X + ty * XTZ + tz;                   // row iy - 8
       const double2* az = reinterpret_cast<const double2*>(X + XNY + ty * (XTZ + 2 * XH) + (tz - e));
@@ -364,14 +368,19 @@ __global__ void __launch_bounds__(256) b_cross_kernel(const double* __restrict__
       } else {
         const double p = ay[XH * XTZ];
         const double qv = -Ax;
-        (pi ? w.p0 : w.p1)[off + node] = p;
+        if (store_p) (pi ? w.p0 : w.p1)[off + node] = p;
         w.q[off + node] = qv;
         contrib = p * qv;
+        if (first) rz = rr[st * 256 + tid] * p;
       }
     }
     // warp sums of this instance; the block partials are formed at the end
     contrib = warp_sum(contrib);
     if ((tid & 31) == 0) red[q][tid >> 5] = contrib;
+    if (MODE == 1 && first) {
+      rz = warp_sum(rz);
+      if ((tid & 31) == 0) red2[q][tid >> 5] = rz;
+    }
   }
   cp_async_wait<0>();
   // block partial of every instance (warp 0 adds the 8 warp sums in order);
@@ -382,25 +391,32 @@ __global__ void __launch_bounds__(256) b_cross_kernel(const double* __restrict__
       double t = tid < 8 ? red[q][tid] : 0.0;
       t = warp_sum(t);
       if (tid == 0) w.partials[(long)act[q] * w.PB + tile] = t;
+      if (MODE == 1 && first) {
+        t = tid < 8 ? red2[q][tid] : 0.0;
+        t = warp_sum(t);
+        if (tid == 0) w.partials2[(long)act[q] * w.PB + tile] = t;
+      }
     }
   }
 }
 
-// sc[16 k + slot] = sum of the instance's first n partials, in tile order
-__global__ void b_partials_kernel(const int* __restrict__ mask, BatchWork w, int n, int slot) {
+// sc[16 k + slot] = sum of the instance's first n partials (of w.partials,
+// or of w.partials2 when second is set), in tile order
+__global__ void b_partials_kernel(const int* __restrict__ mask, BatchWork w, int n, int slot, int second = 0) {
   __shared__ double sh[32];
   const int k = blockIdx.x;
   if (!mask[k]) return;
-  const double* p = w.partials + (long)k * w.PB;
+  const double* p = (second ? w.partials2 : w.partials) + (long)k * w.PB;
   double acc = 0.0;
   for (int i = threadIdx.x; i < n; i += blockDim.x) acc += p[i];
   acc = block_sum(acc, sh);
   if (threadIdx.x == 0) w.sc[16 * k + slot] = acc;
 }
 
-// u += alpha p ; r -= alpha q ; r.r -> sc[1]   (alpha = rz / pq)
+// u += alpha p ; r -= alpha q ; r.r -> sc[1]   (alpha = rz / pq).  pz: p
+// was not stored and is z (the first iteration); last: r is only summed
 __global__ void b_update_kernel(const BatchInst* __restrict__ tab, const int* __restrict__ mask, BatchWork w, int pi,
-                                int mixed) {
+                                int mixed, int pz, int last) {
   __shared__ double sh[32];
   const int k = blockIdx.z;
   if (!mask[k]) return;
@@ -416,11 +432,14 @@ __global__ void b_update_kernel(const BatchInst* __restrict__ tab, const int* __
     if (zero) {
       x[i] = 0.0;
     } else {
-      x[i] += alpha * p[i];
+      const double pv = !pz ? p[i] : mixed ? (double)w.z32[off + i] : w.z[off + i];
+      x[i] += alpha * pv;
     }
     double rv = w.r[off + i] - alpha * w.q[off + i];
-    w.r[off + i] = rv;
-    if (mixed) w.r32[off + i] = (float)rv;
+    if (!last) {
+      w.r[off + i] = rv;
+      if (mixed) w.r32[off + i] = (float)rv;
+    }
     acc += rv * rv;
   }
   double t = block_sum(acc, sh);
@@ -981,7 +1000,7 @@ int BatchContext::setup_group(int base, int K) {
   }
   SCY_TRY(g.sc.alloc((size_t)g.K * 16 * 8));
   SCY_CUDA_TRY(cudaMemset(g.sc.p, 0, (size_t)g.K * 16 * 8));
-  SCY_TRY(g.partials.alloc((size_t)g.K * g.w.PB * 8));
+  SCY_TRY(g.partials.alloc((size_t)g.K * g.w.PB * 8 * 2));
   SCY_TRY(g.counters.alloc((size_t)g.K * 4 * 4));
   SCY_CUDA_TRY(cudaMemset(g.counters.p, 0, (size_t)g.K * 16));
   SCY_TRY(g.status.alloc((size_t)g.K * 4));
@@ -1001,6 +1020,7 @@ int BatchContext::setup_group(int base, int K) {
   g.w.t2f = g.vecf[3].as<float>();
   g.w.sc = g.sc.as<double>();
   g.w.partials = g.partials.as<double>();
+  g.w.partials2 = g.w.partials + (long)g.K * g.w.PB;
   g.w.counters = g.counters.as<unsigned>();
   g.w.status = g.status.as<unsigned>();
   std::vector<BatchInst> tab(g.K);
@@ -1227,24 +1247,35 @@ int BatchContext::solve(BatchGroup& g, const int* mask, int its_now) {
   SCY_LAUNCH_CHECK();
   int pi = 0;
   for (int it = 1; it <= its_now; ++it) {
+    // the first iteration has p = z: r.z comes with the operator kernel, p
+    // is stored only for a later iteration, and the update reads z for it
+    const int first = it == 1, last = it == its_now, store_p = !(first && last);
     SCY_TRY(fd_apply(g));
-    if (mixed)
-      b_dot_rz_kernel<float><<<ng, TB, 0, g.stream>>>(mask, g.w, g.w.z32);
-    else
-      b_dot_rz_kernel<double><<<ng, TB, 0, g.stream>>>(mask, g.w, g.w.z);
-    SCY_LAUNCH_CHECK();
+    if (!first) {
+      if (mixed)
+        b_dot_rz_kernel<float><<<ng, TB, 0, g.stream>>>(mask, g.w, g.w.z32);
+      else
+        b_dot_rz_kernel<double><<<ng, TB, 0, g.stream>>>(mask, g.w, g.w.z);
+      SCY_LAUNCH_CHECK();
+    }
     SCY_TRY(prof_begin(g.stream, &pa));
     if (mixed)
-      b_cross_kernel<1, float><<<tg, 256, xs_smem_bytes(1, 4), g.stream>>>(C, g.Ny, g.Nz, tab, mask, g.w, g.w.z32, it == 1 ? 1 : 0,
-                                                          pi, mixed, g.kpb);
+      b_cross_kernel<1, float><<<tg, 256, xs_smem_bytes(1, 4), g.stream>>>(C, g.Ny, g.Nz, tab, mask, g.w, g.w.z32, first,
+                                                                           pi, mixed, g.kpb, store_p);
     else
-      b_cross_kernel<1, double><<<tg, 256, xs_smem_bytes(1, 8), g.stream>>>(C, g.Ny, g.Nz, tab, mask, g.w, g.w.z, it == 1 ? 1 : 0,
-                                                           pi, mixed, g.kpb);
+      b_cross_kernel<1, double><<<tg, 256, xs_smem_bytes(1, 8), g.stream>>>(C, g.Ny, g.Nz, tab, mask, g.w, g.w.z, first,
+                                                                            pi, mixed, g.kpb, store_p);
     SCY_LAUNCH_CHECK();
-    SCY_TRY(prof_end(g.stream, pa, PROF_MATVEC, 33.0 * 8 * g.N + nact * g.N * (mixed ? 28.0 : 32.0)));
+    // z, q, p when stored, and r (first iteration) or p_old (later ones)
+    SCY_TRY(prof_end(g.stream, pa, PROF_MATVEC,
+                     33.0 * 8 * g.N + nact * g.N * ((mixed ? 4.0 : 8.0) + 8.0 + (store_p ? 8.0 : 0.0) + 8.0)));
     b_partials_kernel<<<g.K, 256, 0, g.stream>>>(mask, g.w, ntiles, 4);
     SCY_LAUNCH_CHECK();
-    b_update_kernel<<<ng, TB, 0, g.stream>>>(tab, mask, g.w, pi, mixed);
+    if (first) {
+      b_partials_kernel<<<g.K, 256, 0, g.stream>>>(mask, g.w, ntiles, 2, 1);
+      SCY_LAUNCH_CHECK();
+    }
+    b_update_kernel<<<ng, TB, 0, g.stream>>>(tab, mask, g.w, pi, mixed, store_p ? 0 : 1, last);
     SCY_LAUNCH_CHECK();
     pi ^= 1;
   }

@@ -50,6 +50,7 @@ struct BatchWork {
   float *r32, *z32, *t1f, *t2f;
   double* sc;          // K * 16: [0] |rhs|^2, [1] r.r, [2] rz, [3] rz old, [4] p.q, [5] |r0|^2
   double* partials;    // K * PB
+  double* partials2;   // K * PB (r.z of the first CG iteration)
   unsigned* counters;  // K * 4
   unsigned* status;    // K
 };
