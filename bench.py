@@ -210,7 +210,7 @@ def run_batched(args, dist, rank, world, local):
     if peak is None:
         peak, peak_src = 6650.0, "fallback"
     kern = {}
-    for nm, desc in (("ysolve", "b_ysolve_kernel (banded Cholesky sweeps along y of the preconditioner)"),
+    for nm, desc in (("ysolve", "b_ysolve_tma_kernel (banded Cholesky sweeps along y of the preconditioner)"),
                      ("matvec", "b_cross_kernel<1> (CG operator application, p update fused)"),
                      ("residual", "b_cross_kernel<0> (initial residual of each stage solve)")):
         pm, pl, pb = b.profile_collect(nm)
