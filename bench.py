@@ -209,6 +209,12 @@ def run_batched(args, dist, rank, world, local):
     peak_src = "measured"
     if peak is None:
         peak, peak_src = 6650.0, "fallback"
+    # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of
+    # one ncu capture of these kernels at 32 instances of the 401 x 401
+    # workload (profiles/batched_ensemble_kernels_401x401.md); other sizes
+    # report none
+    traffic = {"ysolve": 65362176.0, "matvec": 178643456.0, "residual": 187187968.0} \
+        if (args.batch == 32 and args.n == 401) else {}
     kern = {}
     for nm, desc in (("ysolve", "b_ysolve_tma_kernel (banded Cholesky sweeps along y of the preconditioner)"),
                      ("matvec", "b_cross_kernel<1> (CG operator application, p update fused)"),
@@ -218,14 +224,15 @@ def run_batched(args, dist, rank, world, local):
             us = pm / pl * 1e3
             ach = (pb / pl) / (us / 1e6) / 1e9
             kern[nm] = {"kernel": desc, "launch_us": us, "algorithmic_bytes_per_launch": pb / pl,
-                        "achieved": ach, "frac": ach / peak, "total_ms": pm, "launches": pl}
+                        "achieved": ach, "frac": ach / peak, "total_ms": pm, "launches": pl,
+                        "traffic": traffic.get(nm)}
     b.profile_clear()
     b.set_graphs(True)
     if kern:
         top = max(kern, key=lambda k: kern[k]["total_ms"])
         t = kern[top]
         out["roofline"] = {"kernel": t["kernel"], "bound": "hbm", "achieved": t["achieved"], "peak": peak,
-                           "unit": "GB/s", "frac": t["frac"], "peak_source": peak_src, "traffic": None,
+                           "unit": "GB/s", "frac": t["frac"], "peak_source": peak_src, "traffic": t["traffic"],
                            "launch_us": t["launch_us"], "algorithmic_bytes_per_launch": t["algorithmic_bytes_per_launch"],
                            "kernels": kern,
                            "note": "CUDA events on the launching stream in a pass with the round's launches issued "
