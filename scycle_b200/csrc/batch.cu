@@ -628,6 +628,18 @@ __global__ void __launch_bounds__(32 * W) b_ysolve_tma_kernel(const __grid_const
   }
 }
 
+// the caller's array <-> the instances' vectors, one segment per instance
+// (blockIdx.y): scatter into the instances, or gather from them
+__global__ void b_io_kernel(const IoSeg* __restrict__ seg, double* __restrict__ stage, int gather) {
+  const IoSeg g = seg[blockIdx.y];
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < g.n; i += (long)gridDim.x * blockDim.x) {
+    if (gather)
+      stage[g.off + i] = g.p[i];
+    else
+      g.p[i] = stage[g.off + i];
+  }
+}
+
 int ys_smem_bytes(int esize) { return YS_S * (YS_R * 9 * YS_C + YS_B * YS_R * YS_C) * esize + YS_S * 8; }
 
 // Fault_qd::d_dt with tauQS = mu Dy u on the fault row (linear elastic) or
@@ -955,6 +967,53 @@ int BatchContext::create(int n_inst, const char* const* paths, const scy_solve_o
   SCY_CUDA_TRY(cudaMemset(err.p, 0, (size_t)n * 16 * sizeof(double)));
   SCY_CUDA_TRY(cudaMallocHost((void**)&err_host, (size_t)n * 16 * sizeof(double)));
   hc.assign(n, Ctl());
+  // segment tables of the state and fault-field transfers, in the caller's
+  // numbering
+  {
+    std::vector<IoSeg> segs((size_t)(1 + kIoFields) * n, IoSeg{nullptr, 0, 0});
+    long os = 0, of = 0;
+    for (int i = 0; i < n; ++i) {
+      QDContext& c = q(slot_of[i]);
+      segs[i] = IoSeg{c.rk[V_VAR].as<double>(), c.nvar, os};
+      os += c.nvar;
+      double* var = c.rk[V_VAR].as<double>();
+      double* dvar = c.rk[V_DVAR].as<double>();
+      double* src[kIoFields] = {var + c.key_off[SCY_KEY_PSI], var + c.key_off[SCY_KEY_SLIP], c.slipVel.as<double>(),
+                                c.tauP.as<double>(), c.tauQSP.as<double>(), c.strength.as<double>(), nullptr,
+                                nullptr, nullptr, dvar + c.key_off[SCY_KEY_PSI], dvar + c.key_off[SCY_KEY_SLIP]};
+      for (int f = 0; f < kIoFields; ++f) segs[(size_t)(1 + f) * n + i] = IoSeg{src[f], src[f] ? c.Nz : 0, of};
+      of += c.Nz;
+      io_maxn = std::max(io_maxn, std::max(c.nvar, (long)c.Nz));
+    }
+    io_states = os;
+    io_fault = of;
+    SCY_TRY(io.alloc((size_t)std::max(os, of) * sizeof(double)));
+    SCY_TRY(io_seg.alloc(segs.size() * sizeof(IoSeg)));
+    SCY_CUDA_TRY(cudaMemcpy(io_seg.p, segs.data(), segs.size() * sizeof(IoSeg), cudaMemcpyHostToDevice));
+  }
+  return SCY_OK;
+}
+
+int BatchContext::set_states(const double* host) {
+  SCY_CUDA_TRY(cudaMemcpyAsync(io.p, host, (size_t)io_states * sizeof(double), cudaMemcpyHostToDevice, stream));
+  const dim3 gr((unsigned)std::min((io_maxn + 255) / 256, 64L), (unsigned)n);
+  b_io_kernel<<<gr, 256, 0, stream>>>(io_seg.as<IoSeg>(), io.as<double>(), 0);
+  SCY_LAUNCH_CHECK();
+  SCY_CUDA_TRY(cudaStreamSynchronize(stream));
+  return SCY_OK;
+}
+
+int BatchContext::get_fault_field(int field, double* host) {
+  if (field < 0 || field >= kIoFields || field == SCY_FIELD_U || field == SCY_FIELD_SURFDISP ||
+      field == SCY_FIELD_SXY) {
+    set_error("scy_batch_get_fault_field: field %d is not a fault field", field);
+    return SCY_ERR_ARG;
+  }
+  const dim3 gr((unsigned)std::min((io_maxn + 255) / 256, 64L), (unsigned)n);
+  b_io_kernel<<<gr, 256, 0, stream>>>(io_seg.as<IoSeg>() + (size_t)(1 + field) * n, io.as<double>(), 1);
+  SCY_LAUNCH_CHECK();
+  SCY_CUDA_TRY(cudaMemcpyAsync(host, io.p, (size_t)io_fault * sizeof(double), cudaMemcpyDeviceToHost, stream));
+  SCY_CUDA_TRY(cudaStreamSynchronize(stream));
   return SCY_OK;
 }
 
@@ -1688,43 +1747,12 @@ scy_status scy_batch_state_size(scy_batch* b, long* total) {
 
 scy_status scy_batch_set_states(scy_batch* b, const double* host) {
   if (!b || !host) return SCY_ERR_ARG;
-  scy::BatchContext& B = b->ctx;
-  long off = 0;
-  for (int i = 0; i < B.n; ++i) {
-    scy::QDContext& c = B.inst[B.slot_of[i]]->ctx;
-    SCY_CUDA_TRY(cudaMemcpyAsync(c.rk[scy::V_VAR].p, host + off, (size_t)c.nvar * sizeof(double),
-                                 cudaMemcpyHostToDevice, B.stream));
-    off += c.nvar;
-  }
-  SCY_CUDA_TRY(cudaStreamSynchronize(B.stream));
-  return SCY_OK;
+  return b->ctx.set_states(host);
 }
 
 scy_status scy_batch_get_fault_field(scy_batch* b, int field, double* host) {
   if (!b || !host) return SCY_ERR_ARG;
-  scy::BatchContext& B = b->ctx;
-  long off = 0;
-  for (int i = 0; i < B.n; ++i) {
-    scy::QDContext& c = B.inst[B.slot_of[i]]->ctx;
-    const double* src = nullptr;
-    switch (field) {
-      case SCY_FIELD_PSI: src = c.rk[scy::V_VAR].as<double>() + c.key_off[SCY_KEY_PSI]; break;
-      case SCY_FIELD_SLIP: src = c.rk[scy::V_VAR].as<double>() + c.key_off[SCY_KEY_SLIP]; break;
-      case SCY_FIELD_DPSI: src = c.rk[scy::V_DVAR].as<double>() + c.key_off[SCY_KEY_PSI]; break;
-      case SCY_FIELD_DSLIP: src = c.rk[scy::V_DVAR].as<double>() + c.key_off[SCY_KEY_SLIP]; break;
-      case SCY_FIELD_SLIPVEL: src = c.slipVel.as<double>(); break;
-      case SCY_FIELD_TAUP: src = c.tauP.as<double>(); break;
-      case SCY_FIELD_TAUQSP: src = c.tauQSP.as<double>(); break;
-      case SCY_FIELD_STRENGTH: src = c.strength.as<double>(); break;
-      default:
-        scy::set_error("scy_batch_get_fault_field: field %d is not a fault field", field);
-        return SCY_ERR_ARG;
-    }
-    SCY_CUDA_TRY(cudaMemcpyAsync(host + off, src, (size_t)c.Nz * sizeof(double), cudaMemcpyDeviceToHost, B.stream));
-    off += c.Nz;
-  }
-  SCY_CUDA_TRY(cudaStreamSynchronize(B.stream));
-  return SCY_OK;
+  return b->ctx.get_fault_field(field, host);
 }
 
 scy_status scy_batch_set_graphs(scy_batch* b, int on) {

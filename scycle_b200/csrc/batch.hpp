@@ -78,6 +78,15 @@ struct BatchGroup {
   ~BatchGroup();
 };
 
+// One instance's slice of the host array of scy_batch_set_states or
+// scy_batch_get_fault_field: n values of device vector p, at offset off of
+// the array.
+struct IoSeg {
+  double* p;
+  long n, off;
+};
+constexpr int kIoFields = 11;  // SCY_FIELD_PSI .. SCY_FIELD_DSLIP
+
 struct BatchContext {
   std::vector<scy_qd*> inst;  // owned, in slot order (group by group)
   std::vector<int> group_of;  // by the caller's numbering
@@ -106,6 +115,14 @@ struct BatchContext {
     long done_steps = 0, target = 0;
   };
   std::vector<Ctl> hc;
+  // the states and fault fields move between the caller's array and the
+  // instances as one transfer through a staging buffer, scattered or
+  // gathered by a kernel (IoSeg tables: the states, then one per field)
+  DevBuf io, io_seg;
+  long io_states = 0, io_fault = 0;
+  long io_maxn = 0;
+  int set_states(const double* host);
+  int get_fault_field(int field, double* host);
   long rounds = 0, redo_rounds = 0, graph_launches = 0, inst_steps = 0, stage_solves = 0;
   // optional per-launch timing of the main kernels (rounds launched directly
   // while on): CUDA events on the launching stream around each launch
