@@ -156,7 +156,7 @@ __global__ void b_dot_rz_kernel(const int* __restrict__ mask, BatchWork w, const
 }
 
 // A applied in its per-node cross form (33 coefficient planes shared by
-// the group, see build_cross_planes): a block owns one 8 x 32 tile of
+// the group, see build_cross_planes): a block owns one XTY x 32 tile of
 // nodes, keeps its nodes' coefficients in registers and applies them to its
 // (up to XKPB) instances in turn.  Each instance's operand (the tile plus an
 // 8-node halo in y and in z) is staged in shared memory by asynchronous
@@ -167,6 +167,7 @@ __global__ void b_dot_rz_kernel(const int* __restrict__ mask, BatchWork w, const
 //           iteration), q = -A p, p stored (unless store_p = 0), p.q ->
 //           partials; on the first iteration also r.z -> partials2
 constexpr int XTY = 8, XTZ = 32, XH = 8, XS = 3, XKPB = 8;
+constexpr int XT = XTY * XTZ, XW = XT / 32;  // threads and warps of a block
 constexpr int XNY = (XTY + 2 * XH) * XTZ, XNZ = XTY * (XTZ + 2 * XH), XNS = XNY + XNZ;
 
 __device__ __forceinline__ void cp_async4(void* dst, const void* src, int src_bytes) {
@@ -187,18 +188,18 @@ __device__ __forceinline__ void cp_async_wait() {
 // the rhs of the tile; MODE 1 stages z (zsize bytes a value), p_old and the
 // tile's r, and forms p in one more buffer
 constexpr int xs_smem_bytes(int mode, int zsize) {
-  return mode == 0 ? XS * (XNS + 256) * 8 : (XS * XNS * zsize + 15) / 16 * 16 + XS * XNS * 8 + XNS * 8 + XS * 256 * 8;
+  return mode == 0 ? XS * (XNS + XT) * 8 : (XS * XNS * zsize + 15) / 16 * 16 + XS * XNS * 8 + XNS * 8 + XS * XT * 8;
 }
 
 template <int MODE, typename Tz>
-__global__ void __launch_bounds__(256) b_cross_kernel(const double* __restrict__ C, int Ny, int Nz,
+__global__ void __launch_bounds__(XT) b_cross_kernel(const double* __restrict__ C, int Ny, int Nz,
                                                       const BatchInst* __restrict__ tab, const int* __restrict__ mask,
                                                       BatchWork w, const Tz* __restrict__ zv, int first, int pi,
                                                       int mixed, int kpb, int store_p = 1) {
-  constexpr int NV = (XNS + 255) / 256;  // staged values per thread
+  constexpr int NV = (XNS + XT - 1) / XT;  // staged values per thread
   extern __shared__ __align__(16) unsigned char xsm[];
-  __shared__ double red[XKPB][8];  // warp sums by instance
-  __shared__ double red2[MODE == 1 ? XKPB : 1][8];
+  __shared__ double red[XKPB][XW];  // warp sums by instance
+  __shared__ double red2[MODE == 1 ? XKPB : 1][XW];
   __shared__ int act[XKPB];                // the block's active instances
   __shared__ double sck[XKPB];             // MODE 0: |rhs|^2 (0: rhs = 0); MODE 1: beta
   __shared__ const double* srck[XKPB][2];  // MODE 0: u, rhs
@@ -257,7 +258,7 @@ __global__ void __launch_bounds__(256) b_cross_kernel(const double* __restrict__
   unsigned inb = 0;
 #pragma unroll
   for (int a = 0; a < NV; ++a) {
-    const int i = tid + 256 * a;
+    const int i = tid + XT * a;
     int jy = -1, jz = -1;
     if (i < XNY) {
       jy = y0 - XH + i / XTZ;
@@ -273,12 +274,12 @@ __global__ void __launch_bounds__(256) b_cross_kernel(const double* __restrict__
   }
   __syncthreads();
   const int na = nact;
-  double* us = reinterpret_cast<double*>(xsm);  // MODE 0: [XS][XNS] operand, then [XS][256] rhs
+  double* us = reinterpret_cast<double*>(xsm);  // MODE 0: [XS][XNS] operand, then [XS][XT] rhs
   double* rs = us + XS * XNS;
   Tz* zs = reinterpret_cast<Tz*>(xsm);  // MODE 1: [XS][XNS] z, [XS][XNS] p_old, [XNS] p
   double* ps = reinterpret_cast<double*>(xsm + (XS * XNS * sizeof(Tz) + 15) / 16 * 16);
   double* xd = ps + XS * XNS;
-  double* rr = xd + XNS;  // MODE 1: [XS][256] r of the tile (first iteration)
+  double* rr = xd + XNS;  // MODE 1: [XS][XT] r of the tile (first iteration)
   // copies of the q-th active instance into stage q % XS (one commit group
   // per call, empty past the last instance)
   auto issue = [&](int q) {
@@ -289,17 +290,17 @@ __global__ void __launch_bounds__(256) b_cross_kernel(const double* __restrict__
         double* d = us + st * XNS + tid;
 #pragma unroll
         for (int a = 0; a < NV; ++a)
-          if (tid + 256 * a < XNS) cp_async8(d + 256 * a, x + src[a], (inb >> a & 1u) * 8);
+          if (tid + XT * a < XNS) cp_async8(d + XT * a, x + src[a], (inb >> a & 1u) * 8);
         const double* rh = srck[q][1];
         const bool rv = valid && sck[q] != 0.0;
-        cp_async8(rs + st * 256 + tid, rv ? rh + node : rh, rv ? 8 : 0);
+        cp_async8(rs + st * XT + tid, rv ? rh + node : rh, rv ? 8 : 0);
       } else {
         const long off = (long)act[q] * N;
         const Tz* zz = zv + off;
         const double* pold = (pi ? w.p1 : w.p0) + off;
 #pragma unroll
         for (int a = 0; a < NV; ++a) {
-          const int i = tid + 256 * a;
+          const int i = tid + XT * a;
           if (i >= XNS) continue;
           const unsigned in = inb >> a & 1u;
           if (sizeof(Tz) == 4)
@@ -308,7 +309,7 @@ __global__ void __launch_bounds__(256) b_cross_kernel(const double* __restrict__
             cp_async8(zs + st * XNS + i, zz + src[a], in * 8);
           if (!first) cp_async8(ps + st * XNS + i, pold + src[a], in * 8);
         }
-        if (first) cp_async8(rr + st * 256 + tid, w.r + off + (valid ? node : 0), valid ? 8 : 0);
+        if (first) cp_async8(rr + st * XT + tid, w.r + off + (valid ? node : 0), valid ? 8 : 0);
       }
     }
     cp_async_commit();
@@ -333,7 +334,7 @@ __global__ void __launch_bounds__(256) b_cross_kernel(const double* __restrict__
         const double beta = sck[q];
 #pragma unroll
         for (int a = 0; a < NV; ++a) {
-          const int i = tid + 256 * a;
+          const int i = tid + XT * a;
           if (i < XNS)
             xd[i] = first ? (double)zs[st * XNS + i] : (double)zs[st * XNS + i] + beta * ps[st * XNS + i];
         }
@@ -361,7 +362,7 @@ __global__ void __launch_bounds__(256) b_cross_kernel(const double* __restrict__
       }
       const double Ax = (Ay0 + Ay1) + (Az0 + Az1);
       if (MODE == 0) {
-        const double vv = sck[q] == 0.0 ? 0.0 : -1.0 * rs[st * 256 + tid] + Ax;
+        const double vv = sck[q] == 0.0 ? 0.0 : -1.0 * rs[st * XT + tid] + Ax;
         w.r[off + node] = vv;
         if (mixed) w.r32[off + node] = (float)vv;
         contrib = vv * vv;
@@ -371,7 +372,7 @@ __global__ void __launch_bounds__(256) b_cross_kernel(const double* __restrict__
         if (store_p) (pi ? w.p0 : w.p1)[off + node] = p;
         w.q[off + node] = qv;
         contrib = p * qv;
-        if (first) rz = rr[st * 256 + tid] * p;
+        if (first) rz = rr[st * XT + tid] * p;
       }
     }
     // warp sums of this instance; the block partials are formed at the end
@@ -383,16 +384,16 @@ __global__ void __launch_bounds__(256) b_cross_kernel(const double* __restrict__
     }
   }
   cp_async_wait<0>();
-  // block partial of every instance (warp 0 adds the 8 warp sums in order);
+  // block partial of every instance (warp 0 adds the XW warp sums in order);
   // b_partials_kernel adds the tiles up
   __syncthreads();
   if (tid < 32) {
     for (int q = 0; q < na; ++q) {
-      double t = tid < 8 ? red[q][tid] : 0.0;
+      double t = tid < XW ? red[q][tid] : 0.0;
       t = warp_sum(t);
       if (tid == 0) w.partials[(long)act[q] * w.PB + tile] = t;
       if (MODE == 1 && first) {
-        t = tid < 8 ? red2[q][tid] : 0.0;
+        t = tid < XW ? red2[q][tid] : 0.0;
         t = warp_sum(t);
         if (tid == 0) w.partials2[(long)act[q] * w.PB + tile] = t;
       }
@@ -1299,7 +1300,7 @@ int BatchContext::solve(BatchGroup& g, const int* mask, int its_now) {
   const double nact = (double)active_in(g, mask);
   cudaEvent_t pa;
   SCY_TRY(prof_begin(g.stream, &pa));
-  b_cross_kernel<0, double><<<tg, 256, xs_smem_bytes(0, 8), g.stream>>>(C, g.Ny, g.Nz, tab, mask, g.w, nullptr, 0, 0, mixed, g.kpb);
+  b_cross_kernel<0, double><<<tg, XT, xs_smem_bytes(0, 8), g.stream>>>(C, g.Ny, g.Nz, tab, mask, g.w, nullptr, 0, 0, mixed, g.kpb);
   SCY_LAUNCH_CHECK();
   SCY_TRY(prof_end(g.stream, pa, PROF_RESIDUAL, 33.0 * 8 * g.N + nact * g.N * (24.0 + (mixed ? 4 : 0))));
   b_partials_kernel<<<g.K, 256, 0, g.stream>>>(mask, g.w, ntiles, 5);
@@ -1319,10 +1320,10 @@ int BatchContext::solve(BatchGroup& g, const int* mask, int its_now) {
     }
     SCY_TRY(prof_begin(g.stream, &pa));
     if (mixed)
-      b_cross_kernel<1, float><<<tg, 256, xs_smem_bytes(1, 4), g.stream>>>(C, g.Ny, g.Nz, tab, mask, g.w, g.w.z32, first,
+      b_cross_kernel<1, float><<<tg, XT, xs_smem_bytes(1, 4), g.stream>>>(C, g.Ny, g.Nz, tab, mask, g.w, g.w.z32, first,
                                                                            pi, mixed, g.kpb, store_p);
     else
-      b_cross_kernel<1, double><<<tg, 256, xs_smem_bytes(1, 8), g.stream>>>(C, g.Ny, g.Nz, tab, mask, g.w, g.w.z, first,
+      b_cross_kernel<1, double><<<tg, XT, xs_smem_bytes(1, 8), g.stream>>>(C, g.Ny, g.Nz, tab, mask, g.w, g.w.z, first,
                                                                             pi, mixed, g.kpb, store_p);
     SCY_LAUNCH_CHECK();
     // z, q, p when stored, and r (first iteration) or p_old (later ones)
