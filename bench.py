@@ -247,13 +247,14 @@ def run_batched(args, dist, rank, world, local):
     b.fault_field("psi", hs["psi"])
     b.fault_field("slip", hs["slip"])
 
+    # positions of every instance's psi and slip in the state array
+    # (instance i: psi then slip, Nz values each)
+    pos_psi = np.concatenate([2 * offs[i] + np.arange(offs[i + 1] - offs[i]) for i in range(K)])
+    pos_slip = pos_psi + np.repeat(np.diff(offs), np.diff(offs))
+
     def pack():
-        o = 0
-        for i in range(K):
-            nz = offs[i + 1] - offs[i]
-            hs["state"][o:o + nz] = hs["psi"][offs[i]:offs[i + 1]]
-            hs["state"][o + nz:o + 2 * nz] = hs["slip"][offs[i]:offs[i + 1]]
-            o += 2 * nz
+        hs["state"][pos_psi] = hs["psi"]
+        hs["state"][pos_slip] = hs["slip"]
 
     pack()
     torch.cuda.synchronize()
