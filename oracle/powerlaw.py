@@ -14,9 +14,16 @@ checkInput :200-256, initiateIntegrand :305-350, integrate :561-631, d_dt
 integrator.  The integrated variables are, in the std::map's key order,
 gVxy, gVxz (viscous strains, Ny*Nz each), psi and slip (Nz each).
 
-Not restated: the steady-state iteration of guessSteadyStateICs (solveSS
-:922-1108), diffusion creep, pseudoplasticity, linear Maxwell viscosity,
-thermal / hydraulic / grain-size coupling.
+The steady-state initial guess of guessSteadyStateICs = 1 (initiateIntegrand
+:320-324 -> solveSS :922-955, guessTauSS :888-918, solveSSViscoelasticProblem
+:1018-1107, setSSBCs :1295-1342; PowerLaw::guessSteadyStateEffVisc
+:1999-2037, initializeSSMatrices / setSSRHS :2040-2096, updateSSa / updateSSb
+:2099-2195; DislocationCreep::guessInvEffVisc :399-433) is restated in
+PowerLawQD.solve_ss.
+
+Not restated: diffusion creep, pseudoplasticity, linear Maxwell viscosity,
+thermal / hydraulic / grain-size coupling, and the repeated steady-state
+cycles of integrateSS (:827-885, a separate driver mode).
 """
 import numpy as np
 import scipy.sparse as sp
@@ -25,7 +32,9 @@ import scipy.sparse.linalg as spla
 from .infile import atof, atoi, load_vector_double, load_vector_string, parse_lines, set_vec
 from .ode import AdaptiveRK
 from .problem import _load_vec_file, build_qd_problem, driver_settings
+from .fault import compute_vel_qd
 from .qd import QDLinearElastic
+from .sbp2d import SbpOps
 
 
 def pl_settings(text):
@@ -83,6 +92,17 @@ def build_pl_problem(text, input_dir=None):
     if s["initDeltaT"] < s["minDeltaT"] or s["initDeltaT"] < 1e-14:
         s["initDeltaT"] = s["minDeltaT"]
     P["slip_file"] = _load_vec_file(d["inputDir"], "slip", P["Nz"])
+    # steady-state iteration settings (strikeSlip_powerLaw_qd.cpp:27-29,
+    # :157-163) and its optional input files
+    ss = dict(fss_EffVisc=0.2, gss_t=1e-10, atolSS_effVisc=1e-3, maxSSIts_effVisc=50)
+    for var, rhs, full in parse_lines(text):
+        if var in ("fss_EffVisc", "gss_t", "atolSS_effVisc"):
+            ss[var] = atof(rhs)
+        elif var == "maxSSIts_effVisc":
+            ss[var] = atoi(rhs)
+    ss["effVisc_file"] = _load_vec_file(d["inputDir"], "effVisc", N)
+    ss["tauSS_file"] = _load_vec_file(d["inputDir"], "tauSS", P["Nz"])
+    P["ss"] = ss
     return P
 
 
@@ -179,10 +199,104 @@ class PowerLawQD(QDLinearElastic):
         return False
 
     def initiate_integrand(self):
-        """StrikeSlip_PowerLaw_qd::initiateIntegrand (:305-350) without the
-        steady-state iteration: slip = 2 bcL (or inputDir/slip), the viscous
-        strains of the material, psi of the fault."""
+        """StrikeSlip_PowerLaw_qd::initiateIntegrand (:305-350): slip = 2 bcL
+        (or inputDir/slip), with guessSteadyStateICs = 1 the steady-state
+        iteration first, then the viscous strains of the material and psi of
+        the fault."""
         slip = self.bcL * 2.0
         if self.P.get("slip_file") is not None:
             slip = self.P["slip_file"].copy()
+        if self.P["driver"]["guessSteadyStateICs"] == 1:
+            slip = self.solve_ss()
         return {"gVxy": self.gVxy.copy(), "gVxz": self.gVxz.copy(), "psi": self.fault.psi.copy(), "slip": slip}
+
+    def solve_ss(self):
+        """solveSS(0) (strikeSlip_powerLaw_qd.cpp:922-955) with
+        solveSSViscoelasticProblem (:1018-1107) and setSSBCs (:1295-1342).
+        Sets psi, slipVel, tauP of the fault, the material's effVisc, sxy,
+        sxz, sdev, viscous strains and u, bcRShift / bcR; returns the slip.
+        self.ss_its / self.ss_err keep the iteration count and last change."""
+        f, ss = self.fault, self.P["ss"]
+        N, Nz = self.N, self.Nz
+        # Fault::guessSS (fault.cpp:633-672)
+        f.slipVel = np.full(Nz, self.vL)
+        if not self.P["fault"]["stateVals"]:
+            f.psi = f.f0 - f.b * np.log(abs(self.vL) / f.v0)
+        f.tauP = f.sN * f.a * np.arcsinh(0.5 * self.vL * np.exp(f.psi / f.a) / f.v0)
+        # PowerLaw::guessSteadyStateEffVisc (powerLaw.cpp:1999-2037) with
+        # DislocationCreep::guessInvEffVisc (:399-433)
+        dg = ss["gss_t"]
+        temp = self.A * np.exp(-self.Bq / self.T)
+        inv_disl = dg / np.power(dg / temp, 1.0 / self.nexp)
+        eff = 1.0 / (np.full(N, 1.0 / self.cap) + inv_disl)
+        if ss["effVisc_file"] is not None:
+            eff = ss["effVisc_file"].copy()
+        # guessTauSS (:888-918): tauSS = min(tauRS, gss_t * effVisc on the fault)
+        if ss["tauSS_file"] is not None:
+            f.tauP = ss["tauSS_file"].copy()
+        else:
+            f.tauP = np.minimum(f.tauP, eff[:Nz] * dg)
+        f.tauQSP = f.tauP.copy()
+        # Fault_qd::computeVel (fault.cpp:812-858)
+        V, its, conv = compute_vel_qd(f.slipVel, f.tauQSP, f.eta, f.sN, f.psi, f.a, f.locked, f.v0, f.vL,
+                                      f.root_tol, f.max_its)
+        if not conv:
+            raise FloatingPointError("rootFinder BracketedNewton did not converge")
+        f.slipVel = V
+        # solveSSViscoelasticProblem: bcL = tauSS (traction), bcR = vL / 2
+        bcL = f.tauP.copy()
+        bcR = np.full(Nz, self.vL / 2.0)
+        d = self.P["domain"]
+        grid = d["gridSpacingType"]
+        err, it = 1e10, 0
+        v = np.zeros(N)
+        sxy = np.zeros(N)
+        sxz = np.zeros(N)
+        while it < ss["maxSSIts_effVisc"] and err >= ss["atolSS_effVisc"]:
+            old = eff.copy()
+            # initializeSSMatrices / setSSRHS (powerLaw.cpp:2040-2096): the
+            # operator with mu = effVisc, R Dirichlet, T / L / B Neumann
+            sbp = SbpOps(d["order"], self.Ny, self.Nz, d["Ly"], d["Lz"], eff, grid=grid,
+                         y=self.P["y"] if grid != "constantGridSpacing" and self.Ny > 1 else None,
+                         z=self.P["z"] if grid != "constantGridSpacing" and self.Nz > 1 else None,
+                         compat=d["sbpCompatibilityType"],
+                         bcs=("Dirichlet", "Neumann", "Neumann", "Neumann"))
+            rhs = sbp.set_rhs(bcL, bcR, self.bcT, self.bcB)
+            # updateSSa (:2099-2137)
+            v = spla.splu(sbp.A.tocsc()).solve(rhs)
+            gxy_t = sbp.Dy_Iz @ v
+            gxz_t = sbp.Iy_Dz @ v
+            sxy = eff * gxy_t
+            sxz = eff * gxz_t
+            sdev = np.sqrt(np.abs(sxy * sxy + sxz * sxz))
+            inv = 1e3 * self.A * np.power(sdev, self.nexp - 1.0) * np.exp(-self.Bq / self.T)
+            new = 1.0 / (np.full(N, 1.0 / self.cap) + 1.0 * inv)
+            # MyVecLog10AXPBY (genFuncs.cpp:339-365)
+            fss = ss["fss_EffVisc"]
+            eff = np.power(10.0, (1.0 - fss) * np.log10(old) + fss * np.log10(new))
+            # computeNormDiff_L2_scaleL2 (genFuncs.cpp:221-238)
+            err = np.linalg.norm(eff - old) / np.linalg.norm(old)
+            it += 1
+        self.ss_its, self.ss_err = it, err
+        self.effVisc = eff
+        self.sxy, self.sxz = sxy, sxz
+        self.sdev = np.sqrt(np.abs(sxy * sxy + sxz * sxz))
+        # updateSSb (:2140-2195) at initTime
+        t0 = self.P["driver"]["initTime"]
+        u = v * t0
+        mn = u.min()
+        if mn < 0:
+            u = u + abs(mn)
+        self.gVxy = (sbp.Dy_Iz @ v) * t0 - sxy / self.mu if it else self.gVxy
+        self.gVxz = (sbp.Iy_Dz @ v) * t0 - sxz / self.mu if it else self.gVxz
+        # setSSBCs: non-negative u, bcRShift = u at y = Ly, slip = u at y = 0
+        mn = u.min()
+        if mn < 0:
+            u = u + abs(mn)
+        self.u = u
+        self.bcRShift = u[-Nz:].copy()
+        self.bcR = self.bcRShift.copy()
+        slip = u[:Nz].copy()
+        if self.P["driver"]["bcLType"] == "symmFault":
+            slip = slip * 2.0
+        return slip

@@ -447,6 +447,10 @@ scy_status scy_qd_integrate_begin_from_in(scy_qd* q) {
     if (!P.slip_file.empty()) slip = P.slip_file;
     std::copy(P.gVxy0.begin(), P.gVxy0.end(), var0.begin() + c.key_off[SCY_KEY_GVXY]);
     std::copy(P.gVxz0.begin(), P.gVxz0.end(), var0.begin() + c.key_off[SCY_KEY_GVXZ]);
+    // guessSteadyStateICs = 1: the steady-state iteration first (:320-324)
+    if (P.guess_ss)
+      SCY_TRY(c.pl_steady_state(P, psi, slip, var0.data() + c.key_off[SCY_KEY_GVXY],
+                                var0.data() + c.key_off[SCY_KEY_GVXZ], &c.ss_its, &c.ss_err));
   } else if (P.ckpt_number > 0) {
     slip = P.slip_file;  // a restart: the checkpoint's state
     if (!P.slipVel0.empty())

@@ -469,6 +469,7 @@ void load_qd_problem(const std::string& path, QDProblem& P, int cycle) {
   o.max_dt = maxDeltaT;
   o.init_dt = initDeltaT;
   o.t0 = initTime;
+  P.init_time = initTime;
   o.t1 = maxTime;
   o.max_steps = maxStepCount;
   if (timeIntInds.size() > (P.pl ? 4u : 2u)) throw std::runtime_error("timeIntInds names more fields than are integrated");
@@ -505,7 +506,18 @@ void load_qd_problem(const std::string& path, QDProblem& P, int cycle) {
     }
     if (wDisl != "yes" || wDiff != "no" || wPlast != "no" || wLM != "no")
       throw std::runtime_error("the power-law path covers dislocation creep only (wDislCreep = yes, the others no)");
-    if (guess) throw std::runtime_error("the power-law steady-state iteration (guessSteadyStateICs = 1) is outside this path");
+    // the steady-state iteration's settings (strikeSlip_powerLaw_qd.cpp:27-29,
+    // :157-163) and optional input fields (powerLaw.cpp:2021, strikeSlip_powerLaw_qd.cpp:898)
+    for (const auto& e : E) {
+      if (e.var == "fss_EffVisc") P.ss_fss = c_atof(e.rhs);
+      else if (e.var == "gss_t") P.ss_gss_t = c_atof(e.rhs);
+      else if (e.var == "atolSS_effVisc") P.ss_atol = c_atof(e.rhs);
+      else if (e.var == "maxSSIts_effVisc") P.ss_max_its = c_atoi(e.rhs);
+    }
+    if (guess) {
+      if (!read_petsc_vec(P.inputDir + "effVisc", N, P.ss_effvisc)) P.ss_effvisc.clear();
+      if (!read_petsc_vec(P.inputDir + "tauSS", Nz, P.ss_tau)) P.ss_tau.clear();
+    }
     if (AV.size() < 2 || BV.size() < 2 || nV.size() < 2 || AV.size() != AD.size() || BV.size() != BD.size() ||
         nV.size() != nD.size())
       throw std::runtime_error("disl_A/B/n values and depths need at least two matching entries");

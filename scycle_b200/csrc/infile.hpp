@@ -50,6 +50,13 @@ struct QDProblem {
   int pl = 0;
   scy_pl_desc pdesc{};
   std::vector<double> plA, plB, pln, plT, gVxy0, gVxz0;
+  // the steady-state iteration of guessSteadyStateICs = 1
+  // (strikeSlip_powerLaw_qd.cpp:27-29, :157-163) and its optional
+  // inputDir/effVisc and inputDir/tauSS (empty if absent)
+  double ss_fss = 0.2, ss_gss_t = 1e-10, ss_atol = 1e-3;
+  int ss_max_its = 50;
+  std::vector<double> ss_effvisc, ss_tau;
+  double init_time = 0.0;
   // strikeSlip_linearElastic_qd_fd only (cycle = 1)
   int cycle = 0;
   scy_cycle_desc cdesc{};

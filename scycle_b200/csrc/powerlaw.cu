@@ -12,11 +12,13 @@
 // matrix-free: yq zr H = wy * wz, zr Hz = wy and yq Hy = wz in terms of the
 // operator's outer weights (wy = Hz zr, wz = Hy yq; zr = yq = 1 on the
 // constant grid), Dy = qy Dq and Dz = rz Dr.
+#include <algorithm>
 #include <cmath>
 
 #include "common.cuh"
 #include "fault_node.cuh"
 #include "qd.hpp"
+#include "infile.hpp"
 #include "powerlaw_dev.cuh"
 #include "sbp_dev.cuh"
 
@@ -92,6 +94,131 @@ int pl_d_dt(QDContext& q, double t, const double* var, double* f) {
                                     q.tauP.as<double>(), q.strength.as<double>(), q.flags.as<unsigned>(),
                                     q.fault_its.as<unsigned long long>());
   SCY_LAUNCH_CHECK();
+  return SCY_OK;
+}
+
+// ---------------------------------------------------------------------------
+// The steady-state initial guess of guessSteadyStateICs = 1:
+// StrikeSlip_PowerLaw_qd::solveSS(0) (strikeSlip_powerLaw_qd.cpp:922-955)
+// with Fault::guessSS (fault.cpp:633-672), PowerLaw::guessSteadyStateEffVisc
+// (powerLaw.cpp:1999-2037; DislocationCreep::guessInvEffVisc :399-433),
+// guessTauSS (:888-918), solveSSViscoelasticProblem (:1018-1107; setSSRHS,
+// updateSSa and updateSSb, powerLaw.cpp:2040-2195) and setSSBCs
+// (:1295-1342).  Every iteration builds the SBP operator with mu = effVisc
+// and the boundary types R Dirichlet, T / L / B Neumann, solves for the
+// steady velocity v on the GPU and applies Dy and Dz there; the per-node
+// viscosity update (stresses, dislocation-creep viscosity, log10 damping)
+// is host arithmetic on the read-back strain rates.  The fault's slip
+// velocity is seeded with vL (guessSS); the root find the reference runs
+// after guessTauSS only moves the first root find's starting point.
+int QDContext::pl_steady_state(const QDProblem& P, std::vector<double>& psi, std::vector<double>& slip,
+                               double* gVxy, double* gVxz, int* its_out, double* err_out) {
+  cudaStream_t s = sbp.stream;
+  const double dg = P.ss_gss_t, cap = P.pdesc.visc_cap;
+  // Fault::guessSS
+  std::vector<double> tau(Nz), vel(Nz, vL);
+  for (int i = 0; i < Nz; ++i) {
+    if (!P.stateVals_given) psi[i] = f0 - h_b[i] * std::log(std::fabs(vL) / v0);
+    tau[i] = h_sN[i] * h_a[i] * std::asinh(0.5 * vL * std::exp(psi[i] / h_a[i]) / v0);
+  }
+  // guessSteadyStateEffVisc: 1 / effVisc = 1 / cap + dg / (dg / (A e^(-B/T)))^(1/n)
+  std::vector<double> eff((size_t)N);
+  for (long k = 0; k < N; ++k) {
+    const double temp = P.plA[k] * std::exp(-P.plB[k] / P.plT[k]);
+    const double sk = std::pow(dg / temp, 1.0 / P.pln[k]);
+    eff[k] = 1.0 / (1.0 / cap + dg / sk);
+  }
+  if (!P.ss_effvisc.empty()) eff = P.ss_effvisc;
+  // guessTauSS: tauSS = min(tauRS, dg * effVisc on the fault)
+  if (!P.ss_tau.empty())
+    tau = P.ss_tau;
+  else
+    for (int i = 0; i < Nz; ++i) tau[i] = std::min(tau[i], eff[i] * dg);
+  SCY_CUDA_TRY(cudaMemcpyAsync(slipVel.p, vel.data(), Nz * 8, cudaMemcpyHostToDevice, s));
+  // solveSSViscoelasticProblem: bcL = tauSS (traction), bcR = vL / 2
+  DevBuf dbcL, dbcR, dzero, drhs, dv, dgxy, dgxz;
+  SCY_TRY(dbcL.alloc(Nz * 8));
+  SCY_TRY(dbcR.alloc(Nz * 8));
+  SCY_TRY(dzero.alloc((size_t)std::max(Ny, Nz) * 8));
+  SCY_TRY(drhs.alloc(N * 8));
+  SCY_TRY(dv.alloc(N * 8));
+  SCY_TRY(dgxy.alloc(N * 8));
+  SCY_TRY(dgxz.alloc(N * 8));
+  const std::vector<double> half(Nz, vL / 2.0);
+  SCY_CUDA_TRY(cudaMemcpyAsync(dbcL.p, tau.data(), Nz * 8, cudaMemcpyHostToDevice, s));
+  SCY_CUDA_TRY(cudaMemcpyAsync(dbcR.p, half.data(), Nz * 8, cudaMemcpyHostToDevice, s));
+  SCY_CUDA_TRY(cudaMemsetAsync(dzero.p, 0, (size_t)std::max(Ny, Nz) * 8, s));
+  SCY_CUDA_TRY(cudaStreamSynchronize(s));
+  scy_grid_desc g = P.desc.grid;
+  g.bcR = SCY_BC_DIRICHLET;
+  g.bcT = SCY_BC_NEUMANN;
+  g.bcL = SCY_BC_NEUMANN;
+  g.bcB = SCY_BC_NEUMANN;
+  scy_solve_opts o = solve_opts;
+  o.nonzero_guess = 0;
+  o.max_its = std::max(o.max_its, 2000);
+  std::vector<double> gxy((size_t)N), gxz((size_t)N), v((size_t)N), sxy_h((size_t)N), sxz_h((size_t)N);
+  int it = 0;
+  double err = 1e10;
+  while (it < P.ss_max_its && err >= P.ss_atol) {
+    g.mu = eff.data();
+    SbpContext eta;  // initializeSSMatrices: the operator of this iteration's viscosity
+    SCY_TRY(eta.create(g));
+    SCY_CUDA_TRY(cudaDeviceSynchronize());
+    eta.stream = s;
+    SCY_TRY(eta.set_rhs(dbcL.as<double>(), dbcR.as<double>(), dzero.as<double>(), dzero.as<double>(),
+                        drhs.as<double>()));
+    scy_solve_stats st{};
+    SCY_TRY(eta.solve(drhs.as<double>(), dv.as<double>(), o, st));
+    SCY_TRY(eta.apply(SCY_OP_DY, dv.as<double>(), dgxy.as<double>()));
+    SCY_TRY(eta.apply(SCY_OP_DZ, dv.as<double>(), dgxz.as<double>()));
+    SCY_CUDA_TRY(cudaMemcpyAsync(gxy.data(), dgxy.p, N * 8, cudaMemcpyDeviceToHost, s));
+    SCY_CUDA_TRY(cudaMemcpyAsync(gxz.data(), dgxz.p, N * 8, cudaMemcpyDeviceToHost, s));
+    SCY_CUDA_TRY(cudaMemcpyAsync(v.data(), dv.p, N * 8, cudaMemcpyDeviceToHost, s));
+    SCY_CUDA_TRY(cudaStreamSynchronize(s));
+    // updateSSa: stresses, deviatoric stress, the new viscosity; then the
+    // damped update log10(eff) = (1 - f) log10(old) + f log10(new)
+    // (MyVecLog10AXPBY, genFuncs.cpp:339-365) and the change
+    // |eff - old| / |old| (computeNormDiff_L2_scaleL2, genFuncs.cpp:221-238)
+    double dn = 0.0, on = 0.0;
+    for (long k = 0; k < N; ++k) {
+      const double old = eff[k];
+      sxy_h[k] = old * gxy[k];
+      sxz_h[k] = old * gxz[k];
+      const double sdev = std::sqrt(std::fabs(sxy_h[k] * sxy_h[k] + sxz_h[k] * sxz_h[k]));
+      const double inv = 1e3 * P.plA[k] * std::pow(sdev, P.pln[k] - 1.0) * std::exp(-P.plB[k] / P.plT[k]);
+      const double nw = 1.0 / (1.0 / cap + 1.0 * inv);
+      const double damped = std::pow(10.0, (1.0 - P.ss_fss) * std::log10(old) + P.ss_fss * std::log10(nw));
+      dn += (damped - old) * (damped - old);
+      on += old * old;
+      eff[k] = damped;
+    }
+    err = std::sqrt(dn) / std::sqrt(on);
+    ++it;
+  }
+  // updateSSb at initTime: u = v t0 (made non-negative), viscous strains
+  // gV = gV_t t0 - s / mu; setSSBCs: bcRShift = bcR = u at y = Ly, slip =
+  // u at y = 0 (times 2 for a symmetric fault)
+  const double t0 = P.init_time;
+  std::vector<double> hu((size_t)N);
+  for (long k = 0; k < N; ++k) hu[k] = v[k] * t0;
+  double mn = *std::min_element(hu.begin(), hu.end());
+  if (mn < 0)
+    for (auto& x : hu) x += std::fabs(mn);
+  if (it > 0)
+    for (long k = 0; k < N; ++k) {
+      gVxy[k] = gxy[k] * t0 - sxy_h[k] / P.mu[k];
+      gVxz[k] = gxz[k] * t0 - sxz_h[k] / P.mu[k];
+    }
+  std::vector<double> shift(hu.end() - Nz, hu.end());
+  slip.assign(hu.begin(), hu.begin() + Nz);
+  for (auto& x : slip) x *= fts;
+  SCY_CUDA_TRY(cudaMemcpyAsync(u.p, hu.data(), N * 8, cudaMemcpyHostToDevice, s));
+  SCY_CUDA_TRY(cudaMemcpyAsync(bcRShift.p, shift.data(), Nz * 8, cudaMemcpyHostToDevice, s));
+  SCY_CUDA_TRY(cudaMemcpyAsync(bcR.p, shift.data(), Nz * 8, cudaMemcpyHostToDevice, s));
+  SCY_CUDA_TRY(cudaStreamSynchronize(s));
+  if (its_out) *its_out = it;
+  if (err_out) *err_out = err;
   return SCY_OK;
 }
 

@@ -32,6 +32,8 @@ constexpr double a61 = 647845179188. / 3216320057751., a62 = 73281519250. / 8382
                  a63 = 552539513391. / 3454668386233., a64 = 3354512671639. / 8306763924573., a65 = 4040. / 17871.;
 }  // namespace rk43
 
+struct QDProblem;
+
 struct QDContext {
   SbpContext sbp;
   int Ny = 0, Nz = 0;
@@ -100,6 +102,13 @@ struct QDContext {
   // StrikeSlip_LinearElastic_qd::solveSS + solveSSb + Fault::guessSS: fills
   // psi (unless keep_psi) and slip, updates bcL, bcRShift, slipVel, u.
   int steady_state_guess(std::vector<double>& psi, int keep_psi, std::vector<double>& slip);
+  // the power-law driver's steady-state initial guess (solveSS); fills psi,
+  // slip and the viscous strains gVxy, gVxz (N each), sets bcRShift / bcR;
+  // *its and *err report the effective-viscosity iteration
+  int ss_its = 0;        // effective-viscosity iterations of the last pl_steady_state
+  double ss_err = 0.0;   // and its last relative change
+  int pl_steady_state(const QDProblem& P, std::vector<double>& psi, std::vector<double>& slip,
+                      double* gVxy, double* gVxz, int* its, double* err);
   // computeMinTimeStep (strikeSlip_linearElastic_qd.cpp:262-322)
   double compute_min_dt(const std::vector<double>& cs, double Ly, double Lz) const;
   // f = d_dt(t, var) with var = [psi | slip] and f = [dpsi | dslip] (device, 2*Nz each)
