@@ -1,0 +1,169 @@
+"""Heat equation: settings, fields and the initial steady-state geotherm
+(oracle; test infrastructure only).
+
+Restates HeatEquation (source/heatEquation.cpp): loadSettings :138-216,
+checkInput :369-407, setFields :316-366, loadFieldsFromFiles :217-259 and
+computeInitialSteadyStateTemp :525-683, on the oracle SBP operator with the
+"z" Laplace type (sbpOps_m_constGrid.cpp:621-690, :886-905).  The initial
+temperature solves k T'' = -Qrad column by column in the lithosphere (the
+first Nz_lab nodes of every column, down to Lz_lab = TDepths[1]) with
+Dirichlet values from the linear extrapolation of TVals[0..1] at z = 0 and
+z = Lz_lab, then follows the mantle adiabat of the last two TVals below the
+lithosphere when four TVals are given.
+
+Differences from the reference, both where it is undefined: he_Lrad has no
+default there (an uninitialised member); here a missing he_Lrad with a
+nonzero he_A0Vals is an error and with zero he_A0Vals gives Qrad = 0.
+
+Not restated yet: the transient backward-Euler step, shear heating (the
+frictional Green's function and the viscous source), the IMEX integrators
+and flash heating.
+"""
+import numpy as np
+import scipy.sparse.linalg as spla
+
+from .infile import atof, atoi, load_vector_double, parse_lines, set_vec
+from .problem import _load_vec_file
+from .sbp2d import SbpOps
+
+
+def heat_settings(text, Nz):
+    """HeatEquation::loadSettings + the constructor defaults (:7-23) and
+    checkInput (:369-407)."""
+    h = dict(heatEquationType="transient", withViscShearHeating="yes", withFrictionalHeating="yes",
+             withRadioHeatGeneration="yes", linSolver_heateq="CG", kspTol_heateq=1e-11, Nz_lab=Nz,
+             rhoVals=[], rhoDepths=[], kVals=[], kDepths=[], cVals=[], cDepths=[], TVals=[], TDepths=[],
+             wVals=[], wDepths=[], he_A0Vals=[], he_A0Depths=[], he_Lrad=None)
+    lists = ("rhoVals", "rhoDepths", "kVals", "kDepths", "cVals", "cDepths", "TVals", "TDepths",
+             "wVals", "wDepths", "he_A0Vals", "he_A0Depths")
+    for var, rhs, full in parse_lines(text):
+        if var in lists:
+            h[var] = h[var] + load_vector_double(full)
+        elif var in ("heatEquationType", "withViscShearHeating", "withFrictionalHeating",
+                     "withRadioHeatGeneration", "linSolver_heateq"):
+            h[var] = rhs
+        elif var == "kspTol_heateq":
+            h[var] = atof(rhs)
+        elif var == "Nz_lab":
+            h[var] = atoi(rhs)
+        elif var == "he_Lrad":
+            h[var] = atof(rhs)
+    if h["heatEquationType"] not in ("transient", "steadyState"):
+        raise ValueError("heatEquationType must be transient or steadyState")
+    for a, b in (("kVals", "kDepths"), ("rhoVals", "rhoDepths"), ("cVals", "cDepths"),
+                 ("TVals", "TDepths"), ("wVals", "wDepths")):
+        if len(h[a]) != len(h[b]):
+            raise ValueError("%s and %s differ in length" % (a, b))
+    if not 2 <= len(h["TVals"]) <= 4:
+        raise ValueError("TVals needs 2 to 4 entries")
+    if h["Nz_lab"] > Nz:
+        raise ValueError("Nz_lab must not exceed Nz")
+    h["Lz_lab"] = h["TDepths"][1]
+    if h["withRadioHeatGeneration"] == "yes":
+        if len(h["he_A0Vals"]) != len(h["he_A0Depths"]):
+            raise ValueError("he_A0Vals and he_A0Depths differ in length")
+        if not h["he_A0Vals"]:
+            h["he_A0Vals"], h["he_A0Depths"] = [0.0], [0.0]
+    return h
+
+
+class HeatEquation:
+    """The fields of HeatEquation and its initial steady-state temperature."""
+
+    def __init__(self, P, text):
+        d = P["domain"]
+        self.P = P
+        self.Ny, self.Nz = P["Ny"], P["Nz"]
+        self.N = self.Ny * self.Nz
+        h = heat_settings(text, self.Nz)
+        self.h = h
+        if h["Lz_lab"] > d["Lz"]:
+            raise ValueError("the LAB depth TDepths[1] must not exceed Lz")
+        z = P["z"]
+        # setFields (:316-366)
+        self.k = set_vec(z, h["kVals"], h["kDepths"])
+        self.rho = set_vec(z, h["rhoVals"], h["rhoDepths"])
+        self.c = set_vec(z, h["cVals"], h["cDepths"])
+        self.Tamb = set_vec(z, h["TVals"], h["TDepths"])
+        self.T = self.Tamb.copy()
+        self.dT = np.zeros(self.N)
+        if h["withRadioHeatGeneration"] == "yes":
+            A0 = set_vec(z, h["he_A0Vals"], h["he_A0Depths"])
+            if h["he_Lrad"] is None:
+                if np.any(A0 != 0):
+                    raise ValueError("he_Lrad is needed with a nonzero he_A0Vals")
+                self.Qrad = np.zeros(self.N)
+            else:
+                self.Qrad = A0 * np.exp(-z / h["he_Lrad"])
+        else:
+            self.Qrad = np.zeros(self.N)
+        # loadFieldsFromFiles (:217-259)
+        inp = d["inputDir"]
+        for nm, attr in (("rho", "rho"), ("k", "k"), ("h", "Qrad"), ("c", "c")):
+            v = _load_vec_file(inp, nm, self.N)
+            if v is not None:
+                setattr(self, attr, v)
+        Tamb = _load_vec_file(inp, "Tamb", self.N)
+        T = _load_vec_file(inp, "T", self.N)
+        dT = _load_vec_file(inp, "dT", self.N)
+        self.load_ics = Tamb is not None
+        if Tamb is not None:
+            self.Tamb = Tamb
+        if T is not None:
+            self.T = T
+        elif Tamb is not None:
+            self.T = Tamb.copy()
+        if dT is not None:
+            self.dT = dT
+        elif Tamb is not None:
+            self.dT = self.T - self.Tamb
+        if not self.load_ics:
+            self.initial_steady_state_temp()
+
+    def lith_index(self):
+        """bodyFull2bodyLith (constructScatters :409-458): the nodes with
+        iz < Nz_lab, column by column."""
+        Nzl = self.h["Nz_lab"]
+        iy, iz = np.meshgrid(np.arange(self.Ny), np.arange(Nzl), indexing="ij")
+        return (iy * self.Nz + iz).ravel()
+
+    def initial_steady_state_temp(self):
+        """computeInitialSteadyStateTemp (:525-683)."""
+        h, d = self.h, self.P["domain"]
+        TV, TD = h["TVals"], h["TDepths"]
+        if self.Nz == 1:
+            self.Tamb = np.full(self.N, TV[0])
+            self.T = self.Tamb.copy()
+            self.dT = np.zeros(self.N)
+            return
+        slope = (TV[1] - TV[0]) / (TD[1] - TD[0])
+        bcT = np.full(self.Ny, slope * (0.0 - TD[0]) + TV[0])
+        bcB = np.full(self.Ny, slope * (h["Lz_lab"] - TD[0]) + TV[0])
+        idx = self.lith_index()
+        Nzl = h["Nz_lab"]
+        grid = d["gridSpacingType"]
+        var = grid == "variableGridSpacing"
+        # SbpOps(order, Ny, Nz_lab, Ly, Lz, k) with the full Ly, Lz (the
+        # constant grid then spaces Nz_lab points over Lz, as the reference
+        # does), Dirichlet on every side, Laplace type "z"
+        sbp = SbpOps(d["order"], self.Ny, Nzl, d["Ly"], d["Lz"], self.k[idx], grid=grid,
+                     y=self.P["y"][idx] if var and self.Ny > 1 else None,
+                     z=self.P["z"][idx] if var and Nzl > 1 else None,
+                     compat=d["sbpCompatibilityType"], bcs=("Dirichlet",) * 4, laplace="z")
+        rhs = sbp.set_rhs(np.zeros(Nzl), np.zeros(Nzl), bcT, bcB)
+        if h["withRadioHeatGeneration"] == "yes":
+            Q = self.Qrad[idx]
+            if var:
+                Q = sbp.yq @ (sbp.zr @ Q)  # J = yq zr
+            rhs = rhs - sbp.H @ Q
+        Tl = spla.splu(sbp.A.tocsc()).solve(rhs)
+        self.Tamb = self.Tamb.copy()
+        self.Tamb[idx] = Tl
+        # the mantle adiabat below the lithosphere
+        if Nzl < self.Nz and h["Lz_lab"] < d["Lz"] and len(TV) > 3:
+            a = (TV[-1] - TV[-2]) / (TD[-1] - TD[-2])
+            z = self.P["z"]
+            below = z >= h["Lz_lab"]
+            self.Tamb[below] = a * (z[below] - TD[-2]) + TV[-2]
+        self.dT = np.zeros(self.N)
+        self.T = self.Tamb.copy()

@@ -63,7 +63,7 @@ class SbpOps:
 
     def __init__(self, order, Ny, Nz, Ly, Lz, mu, grid="constantGridSpacing",
                  y=None, z=None, compat="fullyCompatible",
-                 bcs=("Dirichlet", "Neumann", "Dirichlet", "Neumann"), multByH=1):
+                 bcs=("Dirichlet", "Neumann", "Dirichlet", "Neumann"), multByH=1, laplace="yz"):
         assert order in (2, 4)
         self.order, self.Ny, self.Nz = order, Ny, Nz
         self.N = Ny * Nz
@@ -71,6 +71,10 @@ class SbpOps:
         self.grid = grid
         self.compat = compat
         self.multByH = multByH
+        # setLaplaceType (constGrid.cpp:159-164): "yz", "y" or "z" selects the
+        # parts of D2, the SAT terms in A and the sides setRhs uses (:621-690, :886-905)
+        assert laplace in ("yz", "y", "z")
+        self.laplace = laplace
         self.mu_vec = np.asarray(mu, dtype=np.float64).copy()
         assert self.mu_vec.size == self.N
         if grid == "constantGridSpacing":
@@ -144,7 +148,12 @@ class SbpOps:
         BSy_Iz = kr(o1y["BS"], Iz); Iy_BSz = kr(Iy, o1z["BS"])
         self.muxBySy_IzT = (BSy_Iz.T @ self.muqy).tocsr()
         self.Iy_muxBzSzT = (Iy_BSz.T @ self.murz).tocsr()
-        self.D2 = (self._dyymu() + self._dzzmu()).tocsr()
+        if self.laplace == "yz":
+            self.D2 = (self._dyymu() + self._dzzmu()).tocsr()
+        elif self.laplace == "y":
+            self.D2 = self._dyymu().tocsr()
+        else:
+            self.D2 = self._dzzmu().tocsr()
         self._build_bc()
 
     # ------------------------------------------------------------------
@@ -243,7 +252,11 @@ class SbpOps:
                 self.rhs_side[s] = self._bc_neumann_rhs(L, Hinv, Bfact, e)
             else:
                 raise ValueError(typ)
-        self.A = (self.D2 + self.A_side["L"] + self.A_side["R"] + self.A_side["T"] + self.A_side["B"]).tocsr()
+        used = {"yz": "LRTB", "y": "LR", "z": "TB"}[self.laplace]
+        self.A = self.D2.copy()
+        for side in used:
+            self.A = self.A + self.A_side[side]
+        self.A = self.A.tocsr()
 
     # ------------------------------------------------------------------
     def change_bc_types(self, bcR, bcT, bcL, bcB):
@@ -253,8 +266,12 @@ class SbpOps:
 
     def set_rhs(self, bcL, bcR, bcT, bcB):
         """setRhs (constGrid.cpp:877-914)."""
-        return (self.rhs_side["L"] @ bcL + self.rhs_side["R"] @ bcR
-                + self.rhs_side["T"] @ bcT + self.rhs_side["B"] @ bcB)
+        out = np.zeros(self.N)
+        used = {"yz": "LRTB", "y": "LR", "z": "TB"}[self.laplace]
+        for side, v in (("L", bcL), ("R", bcR), ("T", bcT), ("B", bcB)):
+            if side in used:
+                out = out + self.rhs_side[side] @ v
+        return out
 
     def Dy(self, u):
         return self.Dy_Iz @ u

@@ -1,0 +1,97 @@
+"""The heat-equation oracle's initial steady-state geotherm (CPU).
+
+HeatEquation::computeInitialSteadyStateTemp solves k T'' = -Qrad in the
+lithosphere with Dirichlet temperatures at z = 0 and at the LAB; the SBP-SAT
+operator with the "z" Laplace type reproduces linear profiles exactly and
+quadratic ones (constant heat production) to the boundary closure's order,
+and below the LAB the temperature follows the mantle adiabat of the last
+two TVals.
+"""
+import numpy as np
+import pytest
+
+from oracle.heat import HeatEquation, heat_settings
+from oracle.problem import build_qd_problem
+from scycle_b200.configs import make_qd_problem
+
+
+def _problem(tmp_path, n=25, grid="constantGridSpacing", extra=None, name="he"):
+    kw = dict(Ny=n, Nz=n, grid=grid, name=name, extra=extra or {})
+    if grid == "variableGridSpacing":
+        kw["stretch_beta"] = 1.5
+    path = make_qd_problem(str(tmp_path), **kw)
+    text = open(path).read()
+    return build_qd_problem(text), text
+
+
+LINEAR = {"kVals": "[2 2]", "kDepths": "[0 30]", "TVals": "[283 733]", "TDepths": "[0 30]",
+          "withRadioHeatGeneration": "no", "rhoVals": "[3 3]", "rhoDepths": "[0 30]",
+          "cVals": "[900 900]", "cDepths": "[0 30]"}
+
+
+def test_linear_geotherm_is_exact(tmp_path):
+    P, text = _problem(tmp_path, extra=LINEAR)
+    he = HeatEquation(P, text)
+    exact = 283.0 + 450.0 * P["z"] / 30.0
+    assert np.max(np.abs(he.T - exact)) <= 1e-9 * 733.0
+    assert np.array_equal(he.T, he.Tamb) and not np.any(he.dT)
+
+
+def test_linear_geotherm_stretched_grid_converges(tmp_path):
+    """On a stretched grid the SBP remainder term acts on a profile that is
+    linear in z but not in the logical coordinate: the error falls at least
+    like h^2."""
+    errs = []
+    for n in (21, 41, 81):
+        P, text = _problem(tmp_path / str(n), n=n, grid="variableGridSpacing", extra=LINEAR)
+        he = HeatEquation(P, text)
+        errs.append(np.max(np.abs(he.T - (283.0 + 450.0 * P["z"] / 30.0))))
+    assert errs[0] / errs[1] >= 3.5 and errs[1] / errs[2] >= 3.5
+    assert errs[-1] <= 1e-3 * 733.0
+
+
+def test_heat_production_converges(tmp_path):
+    """k T'' = -A0 with T(0) = T0, T(L) = TL: T = T0 + (TL - T0) z / L +
+    A0 z (L - z) / (2 k); the error falls at least like h^2."""
+    errs = []
+    for n in (21, 41, 81):
+        extra = {"kVals": "[2 2]", "kDepths": "[0 30]", "TVals": "[283 733]", "TDepths": "[0 30]",
+                 "withRadioHeatGeneration": "yes", "he_A0Vals": "[0.5 0.5]", "he_A0Depths": "[0 30]",
+                 "he_Lrad": "1e30", "rhoVals": "[3 3]", "rhoDepths": "[0 30]", "cVals": "[900 900]",
+                 "cDepths": "[0 30]"}
+        P, text = _problem(tmp_path / str(n), n=n, extra=extra)
+        he = HeatEquation(P, text)
+        z = P["z"]
+        exact = 283.0 + 450.0 * z / 30.0 + 0.5 * z * (30.0 - z) / (2.0 * 2.0)
+        errs.append(np.max(np.abs(he.T - exact)))
+    assert errs[-1] <= 1e-6 * 733.0
+    assert errs[0] / errs[1] >= 3.5 or errs[1] <= 1e-10 * 733.0
+    assert errs[1] / errs[2] >= 3.5 or errs[2] <= 1e-10 * 733.0
+
+
+def test_mantle_adiabat_below_the_lab(tmp_path):
+    """Four TVals: linear conduction down to the LAB (TDepths[1] = 20 km,
+    the first 21 of 31 nodes of every column), the adiabat of TVals[2..3]
+    below it."""
+    n, nz_lab, lab = 31, 21, 20.0
+    extra = {"kVals": "[2 2]", "kDepths": "[0 30]", "rhoVals": "[3 3]", "rhoDepths": "[0 30]",
+             "cVals": "[900 900]", "cDepths": "[0 30]", "withRadioHeatGeneration": "no",
+             "Nz_lab": str(nz_lab), "TVals": "[283 1200 1200.5 1250]",
+             "TDepths": "[0 %r %r 30]" % (lab, lab + 1e-3)}
+    P, text = _problem(tmp_path / "lab", n=n, extra=extra)
+    he = HeatEquation(P, text)
+    z = P["z"]
+    above = (np.arange(P["N"]) % n < nz_lab) & (z < lab)  # the LAB node itself takes the adiabat (z >= Lz_lab)
+    lin = 283.0 + (1200.0 - 283.0) * z / lab
+    assert np.max(np.abs(he.T[above] - lin[above])) <= 1e-9 * 1250.0
+    below = z >= lab
+    adiabat = (1250.0 - 1200.5) / (30.0 - lab - 1e-3) * (z - lab - 1e-3) + 1200.5
+    assert np.allclose(he.T[below], adiabat[below], rtol=0, atol=1e-9 * 1250.0)
+
+
+def test_heat_settings_checks():
+    text = "TVals = [283]\nTDepths = [0]\n"
+    with pytest.raises(ValueError):
+        heat_settings(text, 10)
+    h = heat_settings("TVals = [1 2]\nTDepths = [0 5]\nNz_lab = 7\n", 10)
+    assert h["Lz_lab"] == 5 and h["Nz_lab"] == 7 and h["he_A0Vals"] == [0.0]
