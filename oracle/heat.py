@@ -15,11 +15,23 @@ Differences from the reference, both where it is undefined: he_Lrad has no
 default there (an uninitialised member); here a missing he_Lrad with a
 nonzero he_A0Vals is an error and with zero he_A0Vals gives Qrad = 0.
 
-Not restated yet: the transient backward-Euler step, shear heating (the
-frictional Green's function and the viscous source), the IMEX integrators
-and flash heating.
+The transient problem (setUpTransientProblem :1627-1711) and its
+backward-Euler step (be_transient :1146-1240) are restated with the shear
+heating sources (constructMapV :460-523, computeViscousShearHeating
+:1509-1540, computeFrictionalShearHeating :1543-1576): a shear zone of zero
+width puts the frictional heat tau*V/2 into the fault boundary as a flux,
+a finite width spreads it into the body with the Gaussian Gw.  As in the
+reference, the body source J*Q enters the step only on the variable grid
+(on the constant grid be_transient multiplies H by a fresh, zero vector),
+and the boundary data enter the step as + dt (rho c)^-1 setRhs, the sign of
+the source term: the steady problem solves A T = setRhs, so a zero-width
+shear zone's flux bcL = -tau V / 2 lowers the temperature at the fault in
+the step as written.  Both are kept.
+
+Not restated yet: the IMEX integrators and the coupled drivers.
 """
 import numpy as np
+import scipy.sparse as sp
 import scipy.sparse.linalg as spla
 
 from .infile import atof, atoi, load_vector_double, parse_lines, set_vec
@@ -119,6 +131,17 @@ class HeatEquation:
             self.dT = self.T - self.Tamb
         if not self.load_ics:
             self.initial_steady_state_temp()
+        # constructMapV (:460-523): shear-zone width w (m -> km) and the
+        # Gaussian Gw = exp(-y^2 / (2 w^2)) / sqrt(2 pi) / w
+        self.w = np.zeros(self.N)
+        self.Gw = np.zeros(self.N)
+        if h["wVals"]:
+            self.w = set_vec(z, h["wVals"], h["wDepths"]) * 1e-3
+            y = P["y"]
+            self.Gw = np.exp(-y * y / (2.0 * self.w * self.w)) / np.sqrt(2.0 * np.pi) / self.w
+        self.wMax = float(np.max(self.w))
+        if h["heatEquationType"] == "transient":
+            self.setup_transient()
 
     def lith_index(self):
         """bodyFull2bodyLith (constructScatters :409-458): the nodes with
@@ -167,3 +190,55 @@ class HeatEquation:
             self.Tamb[below] = a * (z[below] - TD[-2]) + TV[-2]
         self.dT = np.zeros(self.N)
         self.T = self.Tamb.copy()
+
+    def setup_transient(self):
+        """setUpTransientProblem (:1627-1711): the operator of k with R, T and
+        B Dirichlet and L Neumann (zero data), I = (J) H, rcInv = 1/(rho c)
+        and D2ath = rcInv A."""
+        d = self.P["domain"]
+        grid = d["gridSpacingType"]
+        var = grid == "variableGridSpacing"
+        self.sbp = SbpOps(d["order"], self.Ny, self.Nz, d["Ly"], d["Lz"], self.k, grid=grid,
+                          y=self.P["y"] if var and self.Ny > 1 else None,
+                          z=self.P["z"] if var and self.Nz > 1 else None,
+                          compat=d["sbpCompatibilityType"],
+                          bcs=("Dirichlet", "Dirichlet", "Neumann", "Dirichlet"))
+        s = self.sbp
+        self.I = ((s.yq @ s.zr) @ s.H).tocsr() if var else s.H.copy()
+        self.rcInv = sp.diags(1.0 / (self.rho * self.c))
+        self.D2ath = (self.rcInv @ s.A).tocsr()
+
+    def frictional_heating(self, tau, slipVel):
+        """computeFrictionalShearHeating (:1543-1576): returns (bcL, Qfric)."""
+        q = tau * slipVel
+        if self.wMax == 0:
+            return -0.5 * q, np.zeros(self.N)
+        Qfric = np.tile(q, self.Ny) * self.Gw  # MapV: node i takes fault value i % Nz
+        return np.zeros(self.Nz), Qfric
+
+    def be_transient(self, slipVel, tau, Tn, dt, sdev=None, dgxy=None, dgxz=None):
+        """be_transient (:1146-1240): one backward-Euler step from Tn over dt;
+        returns T and keeps T, dT."""
+        h = self.h
+        s = self.sbp
+        var = self.P["domain"]["gridSpacingType"] == "variableGridSpacing"
+        bcL = np.zeros(self.Nz)
+        Q = np.zeros(self.N)
+        if h["withFrictionalHeating"] == "yes":
+            bcL, Qfric = self.frictional_heating(tau, slipVel)
+            Q = Q + Qfric
+        if h["withViscShearHeating"] == "yes" and sdev is not None and dgxy is not None and dgxz is not None:
+            Q = Q + sdev * np.sqrt(np.abs(dgxy * dgxy + dgxz * dgxz))
+        temp = s.set_rhs(bcL, np.zeros(self.Nz), np.zeros(self.Ny), np.zeros(self.Ny))
+        if var:
+            temp = temp + s.H @ ((s.yq @ s.zr) @ Q)
+        rhs = dt * (self.rcInv @ temp)
+        dTn = Tn - self.Tamb
+        Hd = s.H @ dTn
+        if var:
+            Hd = (s.yq @ s.zr) @ Hd
+        rhs = rhs + Hd
+        B = (self.I - dt * self.D2ath).tocsc()
+        self.dT = spla.spsolve(B, rhs)
+        self.T = self.Tamb + self.dT
+        return self.T.copy()

@@ -95,3 +95,62 @@ def test_heat_settings_checks():
         heat_settings(text, 10)
     h = heat_settings("TVals = [1 2]\nTDepths = [0 5]\nNz_lab = 7\n", 10)
     assert h["Lz_lab"] == 5 and h["Nz_lab"] == 7 and h["he_A0Vals"] == [0.0]
+
+
+def _transient_problem(tmp_path, n, grid="constantGridSpacing", extra=None):
+    e = dict(LINEAR)
+    e.update({"withFrictionalHeating": "no", "withViscShearHeating": "no"})
+    e.update(extra or {})
+    return _problem(tmp_path, n=n, grid=grid, extra=e)
+
+
+@pytest.mark.parametrize("grid", ["constantGridSpacing", "variableGridSpacing"])
+def test_backward_euler_decays_an_eigenmode(tmp_path, grid):
+    """dT = sin(pi z / Lz) cos(pi y / (2 Ly)) meets the transient problem's
+    boundary types (Neumann at the fault, Dirichlet elsewhere); one
+    backward-Euler step divides it by 1 + dt kappa lambda."""
+    n = 41
+    P, text = _transient_problem(tmp_path, n, grid)
+    he = HeatEquation(P, text)
+    y, z = P["y"], P["z"]
+    mode = np.sin(np.pi * z / 30.0) * np.cos(np.pi * y / 60.0)
+    kappa = 2.0 / (3.0 * 900.0)
+    lam = np.pi ** 2 * (1.0 / 900.0 + 1.0 / 3600.0)
+    dt = 1.0 / (kappa * lam)
+    T = he.be_transient(np.zeros(P["Nz"]), np.zeros(P["Nz"]), he.Tamb + mode, dt)
+    dT = T - he.Tamb
+    assert np.max(np.abs(dT - mode / 2.0)) <= 2e-3
+
+
+def test_zero_width_shear_zone_flux_sign(tmp_path):
+    """A shear zone of zero width: bcL = -tau V / 2 as the fault boundary's
+    Neumann data.  be_transient adds setRhs with the sign of the source
+    term, the opposite of the steady problem's A T = setRhs, so the step
+    changes the temperature next to the fault by -tau V in sign (a cooling
+    the restatement keeps); the change is linear in tau V and largest at
+    the fault."""
+    P, text = _transient_problem(tmp_path, 31, extra={"withFrictionalHeating": "yes"})
+    he = HeatEquation(P, text)
+    Nz = P["Nz"]
+    he.be_transient(np.full(Nz, 1e-9), np.full(Nz, 30.0), he.Tamb.copy(), 1e9)
+    d1 = he.dT.reshape(P["Ny"], Nz).copy()
+    he.be_transient(np.full(Nz, 2e-9), np.full(Nz, 30.0), he.Tamb.copy(), 1e9)
+    d2 = he.dT.reshape(P["Ny"], Nz).copy()
+    assert np.all(d1[0, 1:-1] < 0) and np.all(np.abs(d1[0, 1:-1]) > np.abs(d1[5, 1:-1]))
+    assert np.allclose(d2, 2.0 * d1, rtol=1e-10, atol=0)
+
+
+def test_finite_shear_zone_source_only_on_the_variable_grid(tmp_path):
+    """With wVals the frictional heat is a body source tau V Gw; the
+    reference's be_transient adds it through J (variable grid) and adds
+    nothing on the constant grid."""
+    e = {"withFrictionalHeating": "yes", "wVals": "[2000 2000]", "wDepths": "[0 30]"}
+    for grid, warms in (("constantGridSpacing", False), ("variableGridSpacing", True)):
+        P, text = _transient_problem(tmp_path / grid, 31, grid, extra=e)
+        he = HeatEquation(P, text)
+        Nz = P["Nz"]
+        T = he.be_transient(np.full(Nz, 1e-9), np.full(Nz, 30.0), he.Tamb.copy(), 1e9)
+        if warms:
+            assert np.max(T - he.Tamb) > 0
+        else:
+            assert np.max(np.abs(T - he.Tamb)) == 0
