@@ -146,6 +146,24 @@ def slip_law_psi(psi, V, a, b, f0, v0, Dc):
     return np.where(V == 0, 0.0, d)
 
 
+def flash_heating_vw(T, rho, c, k, D, Tw, tau_c):
+    """flashHeating_Vw (fault.cpp:2162-2168): weakening velocity."""
+    rc = rho * c
+    ath = k / rc
+    return (np.pi * ath / D) * np.power(rc * (Tw - T) / tau_c, 2.0)
+
+
+def flash_heating_psi(psi, V, Vw, fw, Dc, a, b, f0, v0):
+    """flashHeating_psi (fault.cpp:2171-2196): the regularised steady-state
+    friction fLV, weakened to fw + (fLV - fw) Vw / |V| above Vw."""
+    absV = np.abs(V)
+    fLV = (a - b) * np.arcsinh(absV / v0 / 2.0 * np.exp(f0 / (a - b)))
+    with np.errstate(divide="ignore", invalid="ignore"):
+        fss = np.where(absV > Vw, fw + (fLV - fw) * (Vw / absV), fLV)
+    f = a * np.arcsinh((absV / 2.0 / v0) * np.exp(psi / a))
+    return -absV / Dc * (f - fss)
+
+
 class FaultQD:
     """Fault_qd state (fault.hpp:138-160) with the fields d_dt touches."""
 
@@ -189,6 +207,12 @@ class FaultQD:
             dpsi = slip_law_psi(self.psi, V, self.a, self.b, self.f0, self.v0, self.Dc)
         elif self.state_law == "constantState":
             dpsi = np.zeros_like(V)
+        elif self.state_law == "flashHeating":
+            # flashHeating_psi_Vec (fault.cpp:2199-2243) with the fault's
+            # temperature, density and the heat equation's c, k
+            fh = self.flash
+            self.Vw = flash_heating_vw(fh["T"], fh["rho"], fh["c"], fh["k"], fh["D"], fh["Tw"], fh["tau_c"])
+            dpsi = flash_heating_psi(self.psi, V, self.Vw, fh["fw"], self.Dc, self.a, self.b, self.f0, self.v0)
         else:
             raise ValueError(self.state_law)
         self.tauP = self.tauQSP - self.eta * V

@@ -28,7 +28,15 @@ the source term: the steady problem solves A T = setRhs, so a zero-width
 shear zone's flux bcL = -tau V / 2 lowers the temperature at the fault in
 the step as written.  Both are kept.
 
-Not restated yet: the IMEX integrators and the coupled drivers.
+QDThermal restates StrikeSlip_LinearElastic_qd with thermalCoupling =
+uncoupled or coupled and the RK32_WBE integrator (constructor :45-52,
+initiateIntegrand :395-404, the IMEX d_dt :800-870): after every accepted
+step the heat equation takes one backward-Euler step with the new slip
+velocity and shear stress, and in coupled mode the fault's temperature is
+the heat equation's of the step before, set at the start of that d_dt;
+flash heating (stateLaw = flashHeating, fault.cpp:2162-2243) reads it.
+
+Not restated yet: RK43_WBE, be_steadyState, the power-law thermal driver.
 """
 import numpy as np
 import scipy.sparse as sp
@@ -36,6 +44,7 @@ import scipy.sparse.linalg as spla
 
 from .infile import atof, atoi, load_vector_double, parse_lines, set_vec
 from .problem import _load_vec_file
+from .qd import QDLinearElastic
 from .sbp2d import SbpOps
 
 
@@ -242,3 +251,47 @@ class HeatEquation:
         self.dT = spla.spsolve(B, rhs)
         self.T = self.Tamb + self.dT
         return self.T.copy()
+
+
+class QDThermal(QDLinearElastic):
+    """StrikeSlip_LinearElastic_qd with the heat equation (thermalCoupling
+    uncoupled / coupled) integrated by RK32_WBE."""
+
+    def __init__(self, P, text, keep_history=True):
+        super().__init__(P, keep_history)
+        s = P["driver"]
+        if s["thermalCoupling"] not in ("uncoupled", "coupled"):
+            raise ValueError("thermalCoupling must be uncoupled or coupled")
+        if s["timeIntegrator"] != "RK32_WBE":
+            raise ValueError("the thermal driver integrates with RK32_WBE")
+        self.he = HeatEquation(P, text)
+        if self.he.h["heatEquationType"] != "transient":
+            raise ValueError("only the transient heat equation is restated")
+        self.coupled = s["thermalCoupling"] == "coupled"
+        self.flash = s["stateLaw"] == "flashHeating"
+        Nz = self.Nz
+        if self.flash:
+            fs = P["fault"]
+            zf = P["z"][:Nz]
+            # setThermalFields (fault.cpp:316-345): T = Tamb, k and c on the
+            # fault, Vw = Vw_const until the first d_dt
+            self.fault.flash = dict(T=self.he.Tamb[:Nz].copy(), rho=np.asarray(P["rho_f"], float),
+                                    c=self.he.c[:Nz].copy(), k=self.he.k[:Nz].copy(),
+                                    Tw=set_vec(zf, fs["TwVals"], fs["TwDepths"]), D=fs["D"],
+                                    tau_c=fs["tau_c"], fw=fs["fw"])
+            self.fault.Vw = np.full(Nz, fs["Vw"])
+
+    def initiate_integrand(self):
+        var = super().initiate_integrand()
+        if self.flash:  # _fault->updateTemperature(_he->_T)
+            self.fault.flash["T"] = self.he.T[:self.Nz].copy()
+        return var
+
+    def imex_before(self, t, dt):
+        """updateTemperature(varImo) at the start of the IMEX d_dt (coupled)."""
+        if self.coupled and self.flash:
+            self.fault.flash["T"] = self.he.T[:self.Nz].copy()
+
+    def imex_after(self, t, dt, dvar):
+        """HeatEquation::be with the new slip velocity and tauP."""
+        self.he.be_transient(dvar["slip"], self.fault.tauP.copy(), self.he.T.copy(), dt)

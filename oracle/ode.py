@@ -38,9 +38,13 @@ class AdaptiveRK:
     """RK32 (method="RK32") or RK43 (method="RK43") with P / PID control."""
 
     def __init__(self, method, max_num_steps, final_t, delta_t, control_type="PID"):
-        assert method in ("RK32", "RK43")
-        self.method = method
-        self.ord = 3.0 if method == "RK32" else 4.0
+        assert method in ("RK32", "RK43", "RK32_WBE")
+        # RK32_WBE (odeSolverImex.cpp:352-470): the RK32 stages, error and
+        # step size with a strict acceptance test, and after each accepted
+        # step the implicit (backward-Euler) update through the driver
+        self.imex = method == "RK32_WBE"
+        self.method = "RK32" if self.imex else method
+        self.ord = 3.0 if self.method == "RK32" else 4.0
         self.maxNumSteps = max_num_steps
         self.initT = 0.0; self.currT = 0.0; self.finalT = final_t
         self.deltaT = delta_t; self.newDeltaT = delta_t
@@ -159,7 +163,7 @@ class AdaptiveRK:
                     self.deltaT = forced[0]
                 lo, hi = self._attempt(ev, keys, dvar)
                 totErr = self.compute_error(lo, hi)
-                if self.method == "RK32":
+                if self.method == "RK32" and not self.imex:
                     acc = totErr <= self.totTol
                 else:
                     acc = totErr < self.totTol
@@ -178,7 +182,11 @@ class AdaptiveRK:
             # accept the higher-order solution (odeSolver.cpp:599-603 / :1148-1152)
             self.currT = self.currT + self.deltaT
             self.var = {k: hi[k].copy() for k in keys}
+            if self.imex:
+                obj.imex_before(self.currT, self.deltaT)
             dvar = ev(self.currT, self.var)
+            if self.imex:
+                obj.imex_after(self.currT, self.deltaT, dvar)
             if totErr != 0.0:
                 self.newDeltaT = self.compute_step_size(totErr)
             self.errA = [totErr, self.errA[0]]

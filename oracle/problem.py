@@ -59,7 +59,7 @@ def domain_settings(text):
 def fault_settings(text):
     """Fault::loadSettings + defaults (fault.cpp:8-16, :35-109)."""
     f = dict(stateLaw="agingLaw", f0=0.6, v0=1e-6, sN_cap=1e14, sN_floor=0.0, rootTol=1e-12,
-             maxNumIts=10000)
+             maxNumIts=10000, fw=0.64, Vw=0.12, D=5.0, tau_c=3.0)
     vecs = {"DcVals", "DcDepths", "sNVals", "sNDepths", "aVals", "aDepths", "bVals", "bDepths",
             "cohesionVals", "cohesionDepths", "muVals", "muDepths", "rhoVals", "rhoDepths",
             "stateVals", "stateDepths", "lockedVals", "lockedDepths", "TwVals", "TwDepths"}
@@ -73,6 +73,7 @@ def fault_settings(text):
         elif var == "rootTol": f["rootTol"] = atof(rhs)
         elif var == "f0": f["f0"] = atof(rhs)
         elif var == "v0": f["v0"] = atof(rhs)
+        elif var in ("fw", "Vw", "D", "tau_c"): f[var] = atof(rhs)  # flash heating (fault.cpp:89-97)
     return f
 
 

@@ -154,3 +154,66 @@ def test_finite_shear_zone_source_only_on_the_variable_grid(tmp_path):
             assert np.max(T - he.Tamb) > 0
         else:
             assert np.max(np.abs(T - he.Tamb)) == 0
+
+
+def test_flash_heating_law():
+    """flashHeating_psi: below Vw the steady state is the regularised
+    velocity-weakening friction fLV, above it fw + (fLV - fw) Vw / |V|."""
+    from oracle.fault import flash_heating_psi, flash_heating_vw
+    a, b, f0, v0, Dc, fw = 0.01, 0.015, 0.6, 1e-6, 0.01, 0.2
+    psi = np.array([0.6, 0.7])
+    V = np.array([1e-3, 1.0])
+    Vw = np.array([0.1, 0.1])
+    d = flash_heating_psi(psi, V, Vw, fw, Dc, a, b, f0, v0)
+    fLV = (a - b) * np.arcsinh(V / v0 / 2.0 * np.exp(f0 / (a - b)))
+    f = a * np.arcsinh(V / 2.0 / v0 * np.exp(psi / a))
+    fss = np.array([fLV[0], fw + (fLV[1] - fw) * 0.1 / 1.0])
+    assert np.allclose(d, -V / Dc * (f - fss), rtol=1e-14, atol=0)
+    vw = flash_heating_vw(300.0, 3.0, 900.0, 2.0, 5.0, 900.0, 3.0)
+    assert vw == pytest.approx(np.pi * (2.0 / 2700.0) / 5.0 * (2700.0 * 600.0 / 3.0) ** 2, rel=1e-14)
+
+
+THERMAL = dict(LINEAR, thermalCoupling="uncoupled", timeIntegrator="RK32_WBE", heatEquationType="transient",
+               withFrictionalHeating="no", withViscShearHeating="no")
+
+
+def test_uncoupled_thermal_run_keeps_the_mechanical_path(tmp_path):
+    """Uncoupled and without heat sources, RK32_WBE takes the RK32 path of
+    the purely mechanical driver (the strict acceptance test aside) and the
+    temperature stays at the geotherm."""
+    from oracle.heat import QDThermal
+    from oracle.qd import QDLinearElastic
+    P, text = _problem(tmp_path / "th", n=21, extra=dict(THERMAL, maxDeltaT="1e7"))
+    th = QDThermal(P, text)
+    th.integrate(max_steps=25)
+    Pm, _ = _problem(tmp_path / "me", n=21, extra=dict(THERMAL, maxDeltaT="1e7", timeIntegrator="RK32"))
+    me = QDLinearElastic(Pm)
+    me.integrate(max_steps=25)
+    assert len(th.history) == len(me.history)
+    for a, b in zip(th.history, me.history):
+        assert a["t"] == b["t"]
+        assert np.array_equal(a["slip"], b["slip"]) and np.array_equal(a["psi"], b["psi"])
+    assert np.array_equal(th.he.T, th.he.Tamb) and not np.any(th.he.dT)
+
+
+def test_coupled_flash_heating_run(tmp_path):
+    """Coupled, frictional heating through the fault boundary and the flash
+    heating state law: the run advances, the temperature changes, and the
+    fault reads the heat equation's temperature of the step before."""
+    from oracle.heat import QDThermal
+    extra = dict(THERMAL, thermalCoupling="coupled", withFrictionalHeating="yes", stateLaw="flashHeating",
+                 TwVals="[1000 1000]", TwDepths="[0 30]", maxDeltaT="1e7")
+    P, text = _problem(tmp_path, n=21, extra=extra)
+    th = QDThermal(P, text)
+    seen = []
+    orig = th.imex_after
+
+    def after(t, dt, dvar):
+        seen.append(th.he.T[:P["Nz"]].copy())
+        orig(t, dt, dvar)
+    th.imex_after = after
+    th.integrate(max_steps=15)
+    assert len(th.history) == 16
+    assert np.max(np.abs(th.he.dT)) > 0
+    assert np.array_equal(th.fault.flash["T"], seen[-1])
+    assert np.all(np.isfinite(th.fault.Vw)) and np.all(th.fault.Vw > 0)
