@@ -29,14 +29,14 @@ shear zone's flux bcL = -tau V / 2 lowers the temperature at the fault in
 the step as written.  Both are kept.
 
 QDThermal restates StrikeSlip_LinearElastic_qd with thermalCoupling =
-uncoupled or coupled and the RK32_WBE integrator (constructor :45-52,
+uncoupled or coupled and the RK32_WBE / RK43_WBE integrators (constructor :45-52,
 initiateIntegrand :395-404, the IMEX d_dt :800-870): after every accepted
 step the heat equation takes one backward-Euler step with the new slip
 velocity and shear stress, and in coupled mode the fault's temperature is
 the heat equation's of the step before, set at the start of that d_dt;
 flash heating (stateLaw = flashHeating, fault.cpp:2162-2243) reads it.
 
-Not restated yet: RK43_WBE, be_steadyState, the power-law thermal driver.
+Not restated yet: be_steadyState and the power-law thermal driver.
 """
 import numpy as np
 import scipy.sparse as sp
@@ -255,15 +255,15 @@ class HeatEquation:
 
 class QDThermal(QDLinearElastic):
     """StrikeSlip_LinearElastic_qd with the heat equation (thermalCoupling
-    uncoupled / coupled) integrated by RK32_WBE."""
+    uncoupled / coupled) integrated by RK32_WBE or RK43_WBE."""
 
     def __init__(self, P, text, keep_history=True):
         super().__init__(P, keep_history)
         s = P["driver"]
         if s["thermalCoupling"] not in ("uncoupled", "coupled"):
             raise ValueError("thermalCoupling must be uncoupled or coupled")
-        if s["timeIntegrator"] != "RK32_WBE":
-            raise ValueError("the thermal driver integrates with RK32_WBE")
+        if s["timeIntegrator"] not in ("RK32_WBE", "RK43_WBE"):
+            raise ValueError("the thermal driver integrates with RK32_WBE or RK43_WBE")
         self.he = HeatEquation(P, text)
         if self.he.h["heatEquationType"] != "transient":
             raise ValueError("only the transient heat equation is restated")

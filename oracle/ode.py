@@ -38,12 +38,13 @@ class AdaptiveRK:
     """RK32 (method="RK32") or RK43 (method="RK43") with P / PID control."""
 
     def __init__(self, method, max_num_steps, final_t, delta_t, control_type="PID"):
-        assert method in ("RK32", "RK43", "RK32_WBE")
-        # RK32_WBE (odeSolverImex.cpp:352-470): the RK32 stages, error and
-        # step size with a strict acceptance test, and after each accepted
-        # step the implicit (backward-Euler) update through the driver
-        self.imex = method == "RK32_WBE"
-        self.method = "RK32" if self.imex else method
+        assert method in ("RK32", "RK43", "RK32_WBE", "RK43_WBE")
+        # RK32_WBE / RK43_WBE (odeSolverImex.cpp:352-470, :837-): the RK32 /
+        # RK43 stages and step size with a strict acceptance test, the plain
+        # L2 ratio for L2_relative errors, and after each accepted step the
+        # implicit (backward-Euler) update through the driver
+        self.imex = method.endswith("_WBE")
+        self.method = method[:4]
         self.ord = 3.0 if self.method == "RK32" else 4.0
         self.maxNumSteps = max_num_steps
         self.initT = 0.0; self.currT = 0.0; self.finalT = final_t
@@ -119,7 +120,7 @@ class AdaptiveRK:
                 err = math.sqrt(float(np.dot(d, d)))
                 tot += err / (math.sqrt(d.size) * self.scale[i])
             else:
-                if self.method == "RK32":
+                if self.method == "RK32" or self.imex:
                     s = math.sqrt(float(np.dot(hi[key], hi[key])))
                     err = math.sqrt(float(np.dot(d, d)))
                     tot += err / (s * self.scale[i])

@@ -217,3 +217,18 @@ def test_coupled_flash_heating_run(tmp_path):
     assert np.max(np.abs(th.he.dT)) > 0
     assert np.array_equal(th.fault.flash["T"], seen[-1])
     assert np.all(np.isfinite(th.fault.Vw)) and np.all(th.fault.Vw > 0)
+
+
+def test_uncoupled_rk43_wbe_matches_rk43_decisions(tmp_path):
+    """RK43_WBE without heat sources follows RK43 (L2_absolute errors, the
+    same strict acceptance) step for step."""
+    from oracle.heat import QDThermal
+    from oracle.qd import QDLinearElastic
+    P, text = _problem(tmp_path / "th", n=21, extra=dict(THERMAL, maxDeltaT="1e7", timeIntegrator="RK43_WBE"))
+    th = QDThermal(P, text)
+    th.integrate(max_steps=20)
+    Pm, _ = _problem(tmp_path / "me", n=21, extra=dict(THERMAL, maxDeltaT="1e7", timeIntegrator="RK43"))
+    me = QDLinearElastic(Pm)
+    me.integrate(max_steps=20)
+    assert [h["t"] for h in th.history] == [h["t"] for h in me.history]
+    assert np.array_equal(th.history[-1]["slip"], me.history[-1]["slip"])
