@@ -36,7 +36,10 @@ velocity and shear stress, and in coupled mode the fault's temperature is
 the heat equation's of the step before, set at the start of that d_dt;
 flash heating (stateLaw = flashHeating, fault.cpp:2162-2243) reads it.
 
-Not restated yet: be_steadyState and the power-law thermal driver.
+be_steadyState (:1242-1318, setUpSteadyStateProblem :1577-1625) is the
+heatEquationType = steadyState step: A dT = setRhs - H J Q on both grids.
+
+Not restated yet: the power-law thermal driver.
 """
 import numpy as np
 import scipy.sparse as sp
@@ -151,6 +154,8 @@ class HeatEquation:
         self.wMax = float(np.max(self.w))
         if h["heatEquationType"] == "transient":
             self.setup_transient()
+        else:
+            self.setup_steady_state()
 
     def lith_index(self):
         """bodyFull2bodyLith (constructScatters :409-458): the nodes with
@@ -217,6 +222,44 @@ class HeatEquation:
         self.rcInv = sp.diags(1.0 / (self.rho * self.c))
         self.D2ath = (self.rcInv @ s.A).tocsr()
 
+    def setup_steady_state(self):
+        """setUpSteadyStateProblem (:1577-1625): the operator of k with R, T
+        and B Dirichlet and L Neumann."""
+        d = self.P["domain"]
+        grid = d["gridSpacingType"]
+        var = grid == "variableGridSpacing"
+        self.sbp = SbpOps(d["order"], self.Ny, self.Nz, d["Ly"], d["Lz"], self.k, grid=grid,
+                          y=self.P["y"] if var and self.Ny > 1 else None,
+                          z=self.P["z"] if var and self.Nz > 1 else None,
+                          compat=d["sbpCompatibilityType"],
+                          bcs=("Dirichlet", "Dirichlet", "Neumann", "Dirichlet"))
+        self.lu_ss = spla.splu(self.sbp.A.tocsc())
+
+    def be_steady_state(self, slipVel, tau, Tn, dt, sdev=None, dgxy=None, dgxz=None):
+        """be_steadyState (:1242-1318): A dT = setRhs - H J (Qfric + Qvisc)
+        on both grids; returns T and keeps T, dT."""
+        h = self.h
+        s = self.sbp
+        var = self.P["domain"]["gridSpacingType"] == "variableGridSpacing"
+        bcL = np.zeros(self.Nz)
+        Q = np.zeros(self.N)
+        if h["withFrictionalHeating"] == "yes":
+            bcL, Qfric = self.frictional_heating(tau, slipVel)
+            Q = Q - Qfric
+        if h["withViscShearHeating"] == "yes" and sdev is not None and dgxy is not None and dgxz is not None:
+            Q = Q - sdev * np.sqrt(np.abs(dgxy * dgxy + dgxz * dgxz))
+        rhs = s.set_rhs(bcL, np.zeros(self.Nz), np.zeros(self.Ny), np.zeros(self.Ny))
+        rhs = rhs + (s.H @ ((s.yq @ s.zr) @ Q) if var else s.H @ Q)
+        self.dT = self.lu_ss.solve(rhs)
+        self.T = self.Tamb + self.dT
+        return self.T.copy()
+
+    def be(self, slipVel, tau, Tn, dt, sdev=None, dgxy=None, dgxz=None):
+        """HeatEquation::be (:1108-1143): the transient or steady step."""
+        if self.h["heatEquationType"] == "transient":
+            return self.be_transient(slipVel, tau, Tn, dt, sdev, dgxy, dgxz)
+        return self.be_steady_state(slipVel, tau, Tn, dt, sdev, dgxy, dgxz)
+
     def frictional_heating(self, tau, slipVel):
         """computeFrictionalShearHeating (:1543-1576): returns (bcL, Qfric)."""
         q = tau * slipVel
@@ -265,8 +308,6 @@ class QDThermal(QDLinearElastic):
         if s["timeIntegrator"] not in ("RK32_WBE", "RK43_WBE"):
             raise ValueError("the thermal driver integrates with RK32_WBE or RK43_WBE")
         self.he = HeatEquation(P, text)
-        if self.he.h["heatEquationType"] != "transient":
-            raise ValueError("only the transient heat equation is restated")
         self.coupled = s["thermalCoupling"] == "coupled"
         self.flash = s["stateLaw"] == "flashHeating"
         Nz = self.Nz
@@ -294,4 +335,4 @@ class QDThermal(QDLinearElastic):
 
     def imex_after(self, t, dt, dvar):
         """HeatEquation::be with the new slip velocity and tauP."""
-        self.he.be_transient(dvar["slip"], self.fault.tauP.copy(), self.he.T.copy(), dt)
+        self.he.be(dvar["slip"], self.fault.tauP.copy(), self.he.T.copy(), dt)

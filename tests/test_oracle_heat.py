@@ -232,3 +232,18 @@ def test_uncoupled_rk43_wbe_matches_rk43_decisions(tmp_path):
     me.integrate(max_steps=20)
     assert [h["t"] for h in th.history] == [h["t"] for h in me.history]
     assert np.array_equal(th.history[-1]["slip"], me.history[-1]["slip"])
+
+
+def test_steady_state_step_heats_the_fault(tmp_path):
+    """heatEquationType = steadyState: A dT = setRhs - H J Q with the
+    steady problem's own sign convention, so the zero-width shear zone's
+    flux warms the fault; the result does not depend on dt or Tn."""
+    P, text = _transient_problem(tmp_path, 31, extra={"withFrictionalHeating": "yes",
+                                                      "heatEquationType": "steadyState"})
+    he = HeatEquation(P, text)
+    Nz = P["Nz"]
+    T1 = he.be(np.full(Nz, 1e-9), np.full(Nz, 30.0), he.Tamb.copy(), 1e9)
+    d1 = he.dT.reshape(P["Ny"], Nz).copy()
+    T2 = he.be(np.full(Nz, 1e-9), np.full(Nz, 30.0), he.Tamb + 1.0, 5.0)
+    assert np.all(d1[0, 1:-1] > 0) and np.all(d1[0, 1:-1] > d1[5, 1:-1])
+    assert np.array_equal(T1, T2)
