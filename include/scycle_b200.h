@@ -305,7 +305,10 @@ scy_status scy_qd_create_from_in(const char* path, const scy_solve_opts* solve, 
 scy_status scy_qd_get_problem(scy_qd* q, int* Ny, int* Nz, scy_ode_opts* ode);
 /* integrate()'s set-up for a driver made by scy_qd_create_from_in:
  * initiateIntegrand (with the steady-state guess when the file asks for it,
- * strikeSlip_linearElastic_qd.cpp:377-413) and the first d_dt.  With
+ * strikeSlip_linearElastic_qd.cpp:377-413; for the power-law driver the
+ * effective-viscosity iteration of solveSS, strikeSlip_powerLaw_qd.cpp:922-955
+ * and :1018-1107, each iteration a GPU solve with mu = effVisc) and the
+ * first d_dt.  With
  * enableCheckpointing > 0 and a checkpoint in outputDir (ckptNumber > 0) the
  * run restarts from its chkpt_* files (time, step size, step count, error
  * history, state, slip velocity, stresses, boundary data) and appends to the
