@@ -39,13 +39,18 @@ flash heating (stateLaw = flashHeating, fault.cpp:2162-2243) reads it.
 be_steadyState (:1242-1318, setUpSteadyStateProblem :1577-1625) is the
 heatEquationType = steadyState step: A dT = setRhs - H J Q on both grids.
 
-Not restated yet: the power-law thermal driver.
+PLThermal restates StrikeSlip_PowerLaw_qd with the heat equation
+(constructor :43-52, initiateIntegrand :329-333, the IMEX d_dt :692-781):
+coupled, the material's temperature (the viscosity's exp(-B/T)) starts at
+the heat equation's geotherm and, like the fault's, is the previous step's
+at every IMEX d_dt; the heat step adds the viscous shear heating sdev |dgV|.
 """
 import numpy as np
 import scipy.sparse as sp
 import scipy.sparse.linalg as spla
 
 from .infile import atof, atoi, load_vector_double, parse_lines, set_vec
+from .powerlaw import PowerLawQD
 from .problem import _load_vec_file
 from .qd import QDLinearElastic
 from .sbp2d import SbpOps
@@ -336,3 +341,46 @@ class QDThermal(QDLinearElastic):
     def imex_after(self, t, dt, dvar):
         """HeatEquation::be with the new slip velocity and tauP."""
         self.he.be(dvar["slip"], self.fault.tauP.copy(), self.he.T.copy(), dt)
+
+
+class PLThermal(PowerLawQD):
+    """StrikeSlip_PowerLaw_qd with the heat equation (thermalCoupling
+    uncoupled / coupled) integrated by RK32_WBE or RK43_WBE."""
+
+    def __init__(self, P, text, keep_history=True):
+        super().__init__(P, keep_history)
+        s = P["driver"]
+        if s["thermalCoupling"] not in ("uncoupled", "coupled"):
+            raise ValueError("thermalCoupling must be uncoupled or coupled")
+        if s["timeIntegrator"] not in ("RK32_WBE", "RK43_WBE"):
+            raise ValueError("the thermal driver integrates with RK32_WBE or RK43_WBE")
+        self.he = HeatEquation(P, text)
+        self.coupled = s["thermalCoupling"] == "coupled"
+        if self.coupled:  # VecCopy(_he->_T, _material->_T)
+            self.T = self.he.T.copy()
+        self.flash = s["stateLaw"] == "flashHeating"
+        Nz = self.Nz
+        if self.flash:
+            fs = P["fault"]
+            zf = P["z"][:Nz]
+            self.fault.flash = dict(T=self.he.T[:Nz].copy(), rho=np.asarray(P["rho_f"], float),
+                                    c=self.he.c[:Nz].copy(), k=self.he.k[:Nz].copy(),
+                                    Tw=set_vec(zf, fs["TwVals"], fs["TwDepths"]), D=fs["D"],
+                                    tau_c=fs["tau_c"], fw=fs["fw"])
+            self.fault.Vw = np.full(Nz, fs["Vw"])
+
+    def initiate_integrand(self):
+        var = super().initiate_integrand()
+        if self.flash:
+            self.fault.flash["T"] = self.he.T[:self.Nz].copy()
+        return var
+
+    def imex_before(self, t, dt):
+        if self.coupled:
+            if self.flash:
+                self.fault.flash["T"] = self.he.T[:self.Nz].copy()
+            self.T = self.he.T.copy()
+
+    def imex_after(self, t, dt, dvar):
+        self.he.be(dvar["slip"], self.fault.tauP.copy(), self.he.T.copy(), dt, sdev=self.sdev.copy(),
+                   dgxy=dvar["gVxy"], dgxz=dvar["gVxz"])

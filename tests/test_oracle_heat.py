@@ -247,3 +247,57 @@ def test_steady_state_step_heats_the_fault(tmp_path):
     T2 = he.be(np.full(Nz, 1e-9), np.full(Nz, 30.0), he.Tamb + 1.0, 5.0)
     assert np.all(d1[0, 1:-1] > 0) and np.all(d1[0, 1:-1] > d1[5, 1:-1])
     assert np.array_equal(T1, T2)
+
+
+def _pl_thermal_problem(tmp_path, extra):
+    from scycle_b200.configs import make_pl_problem
+    e = {"kVals": "[2 2]", "kDepths": "[0 30]", "rhoVals": "[3 3]", "rhoDepths": "[0 30]",
+         "cVals": "[900 900]", "cDepths": "[0 30]", "withRadioHeatGeneration": "no",
+         "maxEffVisc": "1e12", "maxDeltaT": "1e7"}
+    e.update(extra)
+    path = make_pl_problem(str(tmp_path), Ny=21, Nz=21, extra=e)
+    text = open(path).read()
+    from oracle.powerlaw import build_pl_problem
+    return build_pl_problem(text), text
+
+
+def test_uncoupled_power_law_thermal_keeps_the_mechanical_path(tmp_path):
+    """The power-law driver, uncoupled and without heat sources: RK43_WBE
+    takes the RK43 path (the explicit rates do not see the temperature) and
+    the temperature stays at the geotherm."""
+    from oracle.heat import PLThermal
+    from oracle.powerlaw import PowerLawQD
+    extra = {"thermalCoupling": "uncoupled", "timeIntegrator": "RK43_WBE", "withFrictionalHeating": "no",
+             "withViscShearHeating": "no"}
+    P, text = _pl_thermal_problem(tmp_path / "th", extra)
+    th = PLThermal(P, text)
+    th.integrate(max_steps=10)
+    Pm, _ = _pl_thermal_problem(tmp_path / "me", dict(extra, timeIntegrator="RK43"))
+    me = PowerLawQD(Pm)
+    me.integrate(max_steps=10)
+    assert [h["t"] for h in th.history] == [h["t"] for h in me.history]
+    assert np.array_equal(th.history[-1]["gVxy"], me.history[-1]["gVxy"])
+    assert not np.any(th.he.dT)
+
+
+def test_coupled_power_law_thermal_run(tmp_path):
+    """Coupled with viscous and frictional heating: the material's
+    temperature starts at the heat equation's geotherm and follows it one
+    step behind."""
+    from oracle.heat import PLThermal
+    extra = {"thermalCoupling": "coupled", "timeIntegrator": "RK32_WBE", "withFrictionalHeating": "yes",
+             "withViscShearHeating": "yes"}
+    P, text = _pl_thermal_problem(tmp_path, extra)
+    th = PLThermal(P, text)
+    T0 = th.T.copy()
+    assert np.array_equal(T0, th.he.T)
+    seen = []
+    orig = th.imex_after
+
+    def after(t, dt, dvar):
+        seen.append(th.he.T.copy())
+        orig(t, dt, dvar)
+    th.imex_after = after
+    th.integrate(max_steps=8)
+    assert np.max(np.abs(th.he.dT)) > 0
+    assert np.array_equal(th.T, seen[-1])
