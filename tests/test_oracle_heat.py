@@ -301,3 +301,18 @@ def test_coupled_power_law_thermal_run(tmp_path):
     th.integrate(max_steps=8)
     assert np.max(np.abs(th.he.dT)) > 0
     assert np.array_equal(th.T, seen[-1])
+
+
+def test_power_law_thermal_with_steady_state_guess(tmp_path):
+    """The shape of the reference's thermal example (power law, the
+    steady-state initial guess, coupled heat equation, RK43_WBE): the
+    steady-state iteration sees the heat equation's geotherm as the
+    material temperature, and the coupled run advances."""
+    from oracle.heat import PLThermal
+    extra = {"thermalCoupling": "coupled", "timeIntegrator": "RK43_WBE", "withFrictionalHeating": "yes",
+             "withViscShearHeating": "yes", "guessSteadyStateICs": "1"}
+    P, text = _pl_thermal_problem(tmp_path, extra)
+    th = PLThermal(P, text)
+    th.integrate(max_steps=5)
+    assert 1 < th.ss_its < P["ss"]["maxSSIts_effVisc"]
+    assert len(th.history) == 6 and np.all(np.isfinite(th.history[-1]["slipVel"]))
