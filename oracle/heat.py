@@ -260,10 +260,21 @@ class HeatEquation:
         return self.T.copy()
 
     def be(self, slipVel, tau, Tn, dt, sdev=None, dgxy=None, dgxz=None):
-        """HeatEquation::be (:1108-1143): the transient or steady step."""
+        """HeatEquation::be (:1108-1143): the transient or steady step, then
+        the heat flux."""
         if self.h["heatEquationType"] == "transient":
-            return self.be_transient(slipVel, tau, Tn, dt, sdev, dgxy, dgxz)
-        return self.be_steady_state(slipVel, tau, Tn, dt, sdev, dgxy, dgxz)
+            T = self.be_transient(slipVel, tau, Tn, dt, sdev, dgxy, dgxz)
+        else:
+            T = self.be_steady_state(slipVel, tau, Tn, dt, sdev, dgxy, dgxz)
+        self.compute_heat_flux()
+        return T
+
+    def compute_heat_flux(self):
+        """computeHeatFlux (:1713-1733): kTz = 1e9 k Dz T over the body and
+        its values at the surface z = 0 (body2T: node iz = 0 of each column)."""
+        self.kTz = self.sbp.muxDz(self.T) * 1e9
+        self.kTz_z0 = self.kTz[::self.Nz].copy()
+        return self.kTz_z0
 
     def frictional_heating(self, tau, slipVel):
         """computeFrictionalShearHeating (:1543-1576): returns (bcL, Qfric)."""

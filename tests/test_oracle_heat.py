@@ -316,3 +316,12 @@ def test_power_law_thermal_with_steady_state_guess(tmp_path):
     th.integrate(max_steps=5)
     assert 1 < th.ss_its < P["ss"]["maxSSIts_effVisc"]
     assert len(th.history) == 6 and np.all(np.isfinite(th.history[-1]["slipVel"]))
+
+
+def test_surface_heat_flux_of_a_linear_geotherm(tmp_path):
+    """computeHeatFlux: 1e9 k dT/dz, exact for the linear geotherm."""
+    P, text = _transient_problem(tmp_path, 21)
+    he = HeatEquation(P, text)
+    Nz = P["Nz"]
+    he.be(np.zeros(Nz), np.zeros(Nz), he.Tamb.copy(), 1.0)
+    assert np.allclose(he.kTz_z0, 1e9 * 2.0 * 450.0 / 30.0, rtol=1e-10, atol=0)
