@@ -164,7 +164,11 @@ scy_status scy_sbp_solve(scy_sbp* s, const double* rhs, double* u,
  * stats mean what they mean for scy_sbp_solve (opts->precision is ignored:
  * FP64).  All calls share the array: calls that overlap on the GPU race.
  * The first call on each device looks up the array's address with that
- * device current. */
+ * device current; with lazy module loading (the CUDA default) that first
+ * call also loads the library's module on the device, which is when the
+ * array's memory is reserved, so make it before another allocator reserves
+ * the device.  A zero rhs with atol = 0 returns u = 0, as scy_sbp_solve
+ * does. */
 scy_status scy_sbp_solve_noalloc(scy_sbp* s, const double* rhs, double* u,
                                  const scy_solve_opts* opts, scy_solve_stats* stats);
 

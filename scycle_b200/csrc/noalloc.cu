@@ -19,8 +19,12 @@
 //   clears what must start at zero itself, and calls that overlap on the GPU
 //   (different streams, threads or contexts at the same time) race on it.
 // * the address of the array is looked up once per device, on the first call
-//   made with that device current (cudaGetSymbolAddress); make that first
-//   call outside any code that forbids runtime set-up calls.
+//   made with that device current (cudaGetSymbolAddress).  With lazy module
+//   loading (CUDA_MODULE_LOADING=LAZY, the default) that first call is also
+//   when the module is loaded on the device and the array's memory is
+//   reserved, so it may itself need about 2.6 MB of free device memory:
+//   make the first call on each device before another allocator reserves
+//   the device, and outside any code that forbids runtime set-up calls.
 #include <cmath>
 #include <mutex>
 
@@ -154,6 +158,14 @@ int SbpContext::solve_noalloc(const double* rhs, double* u, const scy_solve_opts
   st.iterations = 0;
   st.converged = 0;
   const double tol = std::max(o.rtol * st.bnorm, o.atol);
+  if (h2[0] == 0.0 && tol == 0.0) {
+    // zero right-hand side: the solution is zero (as in scy_sbp_solve; a
+    // warm start would otherwise never reach ||r|| <= 0)
+    SCY_CUDA_TRY(cudaMemsetAsync(u, 0, n * sizeof(double), s));
+    st.rnorm = 0.0;
+    st.converged = 1;
+    return SCY_OK;
+  }
   if (st.rnorm0 <= tol) {
     st.converged = 1;
     return SCY_OK;
@@ -194,7 +206,9 @@ int SbpContext::solve_noalloc(const double* rhs, double* u, const scy_solve_opts
     set_error("non-finite residual in the elliptic solve");
     return SCY_ERR_NONFINITE;
   }
-  st.converged = st.rnorm <= tol * 1.0000001 ? 1 : st.converged;
+  // the recursive residual may have met the target while the true one
+  // does not: the true residual decides
+  st.converged = st.rnorm <= tol * 1.0000001 + 1e-300 ? 1 : 0;
   if (!st.converged) {
     set_error("elliptic solve stopped at ||r|| = %g after %d iterations (target %g)", st.rnorm, st.iterations, tol);
     return SCY_ERR_CG_NOCONV;

@@ -1,7 +1,7 @@
 """Generates tests/golden/reference_examples.json from the reference tree.
 
-Run in a container that has the reference checked out (path as first
-argument, default /root/reference).  The fixture holds facts derived from
+Run where the reference tree is checked out, with its path as the first
+argument or in the environment variable SCYCLE_REFERENCE.  The fixture holds facts derived from
 the reference's shipped inputs -- the key/value settings of the
 linear-elastic quasi-dynamic example examples/ex2.in as its own parser
 reads them, and summary values of the PETSc-binary vector examples/ex3_z --
@@ -54,4 +54,7 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SCYCLE_REFERENCE")
+    if not ref:
+        sys.exit("usage: make_golden.py <reference tree>  (or set SCYCLE_REFERENCE)")
+    main(ref)
