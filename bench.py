@@ -131,7 +131,60 @@ def make_workload(workdir, n=401, seed=0):
     return slip_var_401(workdir, seed=seed, Ny=n, Nz=n, years=1.0e4)
 
 
+def _fixture(name):
+    path = os.path.join(HERE, "tests", "golden", "parity_%s.npz" % name)
+    return np.load(path) if os.path.exists(path) else None
+
+
+def _field_errors(view, fx, k):
+    rel = lambda a, b, fl: float(np.max(np.abs(a - b) / np.maximum(np.abs(b), fl)))
+    return {"slip": rel(view.field("slip"), fx["slip"][k], 1e-12),
+            "slipVel": rel(view.field("slipVel"), fx["slipVel"][k], 1e-300),
+            "psi": rel(view.field("psi"), fx["psi"][k], 1e-300),
+            "tauP": rel(view.field("tauP"), fx["tauP"][k], 1e-9),
+            "surfDisp": float(np.max(np.abs(view.field("surfDisp") - fx["surfDisp"][k]))
+                              / max(np.max(np.abs(fx["surfDisp"][k])), 1e-300))}
+
+
+def oracle_errors(name, make, rtol, batch_precision=None):
+    """Error of the device path against the FP64 oracle: the driver (or a
+    one-instance batch when ``batch_precision`` is given) forced onto the
+    oracle's attempt sequence of the committed fixture
+    tests/golden/parity_<name>.npz, fields compared after every recorded
+    step; the maximum relative error per field."""
+    fx = _fixture(name)
+    if fx is None:
+        return None
+    work = tempfile.mkdtemp(prefix="scy_err_")
+    att = list(zip(fx["attempt_dt"].tolist(), fx["attempt_acc"].astype(bool).tolist()))
+    worst = {}
+    if batch_precision is None:
+        from scycle_b200.qd import QD
+        q = QD.from_in(make(work), solve_rtol=rtol)
+        q.force_attempts(att)
+        q.integrate_begin_from_in()
+        step = lambda n: q.integrate_steps(n)
+        view, closer = q, q.close
+    else:
+        from scycle_b200.batch import Batch
+        b = Batch([make(work)], solve_rtol=rtol, precision=batch_precision)
+        view = b.instance(0)
+        view.force_attempts(att)
+        step = lambda n: b.run(n)
+        closer = b.close
+    done = 0
+    for k, st in enumerate(fx["snap_steps"].tolist()):
+        step(st - done)
+        done = st
+        for f, e in _field_errors(view, fx, k).items():
+            worst[f] = max(worst.get(f, 0.0), e)
+    closer()
+    return {"steps": int(done), "solve_rtol": rtol, "max_rel_err": worst,
+            "fixture": "tests/golden/parity_%s.npz (oracle run free, device forced onto its attempts)" % name}
+
+
 # ---------------------------------------------------------------------------
+ZT_DESC = "z transforms of the preconditioner (cuBLAS DGEMM, two per apply)"
 BATCH_WORKLOAD = ("slip_var_401 ensemble: %d instances per GPU of the 401x401 stretched-grid slip-law workload "
                   "(seeds differ: lognormal Dc and initial state), every instance with its own RK32 step control")
 
@@ -198,6 +251,13 @@ def run_batched(args, dist, rank, world, local):
         v_ref, v_b = q.field("slipVel"), b.instance(0).field("slipVel")
         out["v_rel_err_vs_fp64_single"] = float(np.max(np.abs(v_b - v_ref) / np.abs(v_ref)))
         q.close()
+        # against the FP64 oracle: instance 0's workload (seed 0) forced onto
+        # the oracle's first 100 attempts, through the same batched kernels
+        if args.n == 401:
+            e = oracle_errors("c1", lambda w: make_workload(w, n=401, seed=0), args.rtol,
+                              batch_precision=args.batch_precision)
+            out["oracle_error"] = e
+            out["v_rel_err_vs_fp64_oracle"] = e["max_rel_err"]["slipVel"] if e else None
     # roofline of the batch's main kernels: a separate pass with the round's
     # launches issued directly and CUDA events around each launch
     b.set_graphs(False)
@@ -218,7 +278,8 @@ def run_batched(args, dist, rank, world, local):
     kern = {}
     for nm, desc in (("ysolve", "b_ysolve_tma_kernel (banded Cholesky sweeps along y of the preconditioner)"),
                      ("matvec", "b_cross_kernel<1> (CG operator application, p update fused)"),
-                     ("residual", "b_cross_kernel<0> (initial residual of each stage solve)")):
+                     ("residual", "b_cross_kernel<0> (initial residual of each stage solve)"),
+                     ("ztransform", ZT_DESC)):
         pm, pl, pb = b.profile_collect(nm)
         if pl:
             us = pm / pl * 1e3
@@ -229,6 +290,9 @@ def run_batched(args, dist, rank, world, local):
     b.profile_clear()
     b.set_graphs(True)
     if kern:
+        tot = sum(k["total_ms"] for k in kern.values())
+        for k in kern.values():
+            k["share_of_timed_kernels"] = k["total_ms"] / tot if tot else None
         top = max(kern, key=lambda k: kern[k]["total_ms"])
         t = kern[top]
         out["roofline"] = {"kernel": t["kernel"], "bound": "hbm", "achieved": t["achieved"], "peak": peak,
@@ -278,6 +342,40 @@ def run_batched(args, dist, rank, world, local):
                   "h2d_bytes_per_step": nst * 8, "d2h_bytes_per_step": 3 * nz_tot * 8,
                   "wall_s": time.perf_counter() - t_w}
     b.close()
+    return out
+
+
+C0_WORKLOAD = ("aging_const_101: linear-elastic quasi-dynamic, 101x101 SBP order 4 on a constant grid over 30x30 km, "
+               "aging law, psi = 0.6 + N(0, 1e-4), RK32 atol 1e-7, the whole 200 simulated years")
+
+
+def run_c0(args):
+    """The CPU-runnable configuration end to end: the whole 200-year run on
+    the device (plain FP64 driver), its error against the oracle on the
+    oracle's own attempt sequence, and the oracle's run of the same 200
+    years timed on one host core."""
+    import torch
+    from scycle_b200.configs import aging_const_101
+    from scycle_b200.qd import QD
+    work = tempfile.mkdtemp(prefix="scy_c0_")
+    q = QD.from_in(aging_const_101(work, seed=0), solve_rtol=args.rtol)
+    q.integrate_begin_from_in()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    st = q.integrate_steps(10 ** 8)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    q.close()
+    out = {"workload": C0_WORKLOAD, "steps": st.step_count, "stage_solves": st.d_dt_evals, "wall_s": wall,
+           "sim_years": st.t / YEAR, "sim_years_per_hour": (st.t / YEAR) / (wall / 3600.0),
+           "stage_solves_per_s": st.d_dt_evals / wall,
+           "oracle_error": oracle_errors("c0", lambda w: aging_const_101(w, seed=0), args.rtol)}
+    if not args.no_cpu_baseline:
+        r = oracle_on_all_cores("c0", 10 ** 8, max_workers=1)
+        out["cpu_oracle_one_core"] = {"wall_s": r["timed_s_max"], "stage_solves": r["stage_solves"],
+                                      "sim_years_per_hour": r["sim_years_per_hour"], "cpu_model": r["cpu_model"],
+                                      "kind": "port", "note": "the whole 200-year run, one single-threaded instance"}
+        out["gpu_over_cpu_sim_years"] = out["sim_years_per_hour"] / r["sim_years_per_hour"]
     return out
 
 
@@ -564,9 +662,10 @@ def run_ours(args, dist, rank, world, local):
     cycle = None
     if not args.no_cycle:
         cycle = run_cycle(args)
+    c0 = None if (args.no_c0 or rank != 0) else run_c0(args)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(path, args)
+        cpu = cpu_baseline(args)
     single = {"value": value, "unit": "stage-solves/s", "ms_per_step": ms_max / args.steps,
               "sim_years_per_hour": syph, "sim_years_timed": total_sim_years, "stage_solves": total_evals,
               "cg_iterations_per_solve": solve_its, "gpu_launches": int(launches), "e2e": e2e,
@@ -574,6 +673,8 @@ def run_ours(args, dist, rank, world, local):
                   args.precond, "fp32" if prec == "mixed" else "fp64", args.rtol, args.check_every),
               "l2": "flushed between steps (256 MB write)", "clocks": clk, "roofline": roofline}
     q.close()
+    if rank == 0 and args.n == 401:
+        single["oracle_error"] = oracle_errors("c1", lambda w: make_workload(w, n=401, seed=0), args.rtol)
     batched = run_batched(args, dist, rank, world, local) if args.batch > 0 else None
     ensemble_c3 = run_ensemble_c3(args, dist, rank, world, local) if args.c3 > 0 else None
     adjoint_c4 = None
@@ -604,7 +705,8 @@ def run_ours(args, dist, rank, world, local):
            "gpu_launches": head["gpu_launches"], "clocks": head["clocks"],
            "batched": batched, "fp64_single": single,
            "batched_vs_fp64_single_sim_years": (batched["sim_years_per_hour"] / syph) if batched else None,
-           "response_mode": resp, "cycle": cycle, "ensemble_c3": ensemble_c3, "adjoint_c4": adjoint_c4}
+           "response_mode": resp, "cycle": cycle, "ensemble_c3": ensemble_c3, "adjoint_c4": adjoint_c4,
+           "config0": c0, "v_rel_err_vs_fp64_oracle": (batched or {}).get("v_rel_err_vs_fp64_oracle")}
     if rank == 0:
         print(json.dumps(out))
 
@@ -721,49 +823,140 @@ def run_stencil_only(args):
                       "algorithmic_GBps": algo / (ms / 1e3) / 1e9, "frac_of_measured_hbm": algo / (ms / 1e3) / 1e9 / peak}))
 
 
-def cpu_baseline(path, args, max_evals=None):
-    """The oracle (SciPy SuperLU direct solve + restated fault / RK32) on the
-    host cores, on a bounded sample of the same workload."""
+# ---------------------------------------------------------------------------
+# CPU baseline: the oracle (SciPy SuperLU direct solve + the restated fault
+# and RK32) on the host's own cores.  One single-threaded oracle instance per
+# core (the GPU side is an ensemble too), each with its own seed; the
+# factorisations and the steady-state initial guess happen before a barrier,
+# the timed steps after it.
+
+
+def _host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def _cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return None
+
+
+def _avail_bytes():
+    try:
+        for line in open("/proc/meminfo"):
+            if line.startswith("MemAvailable:"):
+                return int(line.split()[1]) * 1024
+    except Exception:
+        pass
+    return None
+
+
+_POOL_BARRIER = None
+
+
+def _pool_init(barrier):
+    global _POOL_BARRIER
+    _POOL_BARRIER = barrier
+
+
+def _oracle_worker(job):
+    """One oracle instance: set-up, wait at the barrier, time ``steps`` RK32
+    steps.  Returns (stage-solves, seconds, simulated seconds, set-up s)."""
+    import tempfile as _tf
     from oracle.problem import build_qd_problem
     from oracle.qd import QDLinearElastic
+    kind, seed, n, steps = job
     t0 = time.perf_counter()
+    work = _tf.mkdtemp(prefix="scy_cpu_")
+    if kind == "c1":
+        path = make_workload(work, n=n, seed=seed)
+    else:
+        from scycle_b200.configs import aging_const_101
+        path = aging_const_101(work, seed=seed)
     P = build_qd_problem(open(path).read())
     ora = QDLinearElastic(P, keep_history=False)
+    var0 = ora.initiate_integrand()
     setup = time.perf_counter() - t0
-    steps = args.cpu_steps
+    if _POOL_BARRIER is not None:
+        _POOL_BARRIER.wait()
     t1 = time.perf_counter()
-    rk = ora.integrate(max_steps=steps)
+    rk = ora.integrate(max_steps=steps, var0=var0)
     el = time.perf_counter() - t1
-    evals = rk.stage_evals
-    return {"value": evals / el, "unit": "stage-solves/s", "cores": 1, "kind": "port",
-            "sample": "%d RK32 steps (%d stage-solves) of the same workload after a %.1f s SuperLU factorisation; "
-                      "SuperLU and the restated root finder are single-threaded" % (steps, evals, setup),
-            "sim_years_per_hour": (rk.currT - P["driver"]["initTime"]) / YEAR / (el / 3600.0)}
+    return rk.stage_evals, el, rk.currT - P["driver"]["initTime"], setup
+
+
+def oracle_on_all_cores(kind, steps, n=401, max_workers=None):
+    """Runs one oracle instance per usable core (capped by host memory: a
+    401^2 instance holds about 4 GB at its peak) and returns the aggregate
+    stage-solves/s over the timed steps."""
+    import multiprocessing as mp
+    cores = _host_cores()
+    per = 5e9 if kind == "c1" else 0.5e9
+    avail = _avail_bytes()
+    workers = cores if avail is None else max(1, min(cores, int(avail // per)))
+    if max_workers:
+        workers = min(workers, max_workers)
+    saved = {k: os.environ.get(k) for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS")}
+    for k in saved:
+        os.environ[k] = "1"
+    try:
+        ctx = mp.get_context("spawn")  # the parent may already hold a CUDA context
+        barrier = ctx.Barrier(workers)
+        with ctx.Pool(workers, initializer=_pool_init, initargs=(barrier,)) as pool:
+            res = pool.map(_oracle_worker, [(kind, s, n, steps) for s in range(workers)])
+    finally:
+        for k, v in saved.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+    evals = sum(r[0] for r in res)
+    value = sum(r[0] / r[1] for r in res)
+    return {"value": value, "unit": "stage-solves/s", "cores": workers, "host_cores": cores,
+            "cpu_model": _cpu_model(), "workers": workers, "steps_per_worker": steps, "stage_solves": evals,
+            "timed_s_max": max(r[1] for r in res), "setup_s_max": max(r[3] for r in res),
+            "sim_years_per_hour": sum((r[2] / YEAR) / (r[1] / 3600.0) for r in res)}
+
+
+def cpu_baseline(args):
+    """The oracle on a bounded sample of the headline workload, on all host
+    cores (one single-threaded instance per core)."""
+    r = oracle_on_all_cores("c1", args.cpu_steps, n=args.n)
+    r.update({"kind": "port",
+              "sample": "%d RK32 steps of the 401x401 workload on each of %d single-threaded oracle instances "
+                        "(one per core, seeds 0..%d), summed stage-solves/s; SuperLU factorisations and the "
+                        "steady-state initial guess before the timed steps" % (args.cpu_steps, r["workers"],
+                                                                              r["workers"] - 1)})
+    return r
 
 
 def run_reference(args, dist, rank, world, local):
+    """The reference arm: the oracle port of the reference's CPU path on all
+    host cores, each core running its own instance of the headline workload
+    for ``--steps`` RK32 steps (rank 0 only)."""
     if rank != 0:
         return
-    work = tempfile.mkdtemp(prefix="scy_ref_")
-    path = make_workload(work, n=args.n, seed=0)
-    from oracle.problem import build_qd_problem
-    from oracle.qd import QDLinearElastic
-    P = build_qd_problem(open(path).read())
-    ora = QDLinearElastic(P, keep_history=False)
-    k = min(args.steps, args.cpu_steps)
-    w = min(args.warmup, 1)
-    t0 = time.perf_counter()
-    rk = ora.integrate(max_steps=w + k)
-    el = time.perf_counter() - t0
-    evals = rk.stage_evals
-    value = evals / el
+    k = max(1, min(args.steps, args.cpu_steps_ref))
+    r = oracle_on_all_cores("c1", k, n=args.n)
+    value = r["value"]
+    cpu = dict(r)
+    cpu.update({"kind": "port",
+                "sample": "%d RK32 steps on each of %d single-threaded oracle instances (one per core), "
+                          "factorisations and steady-state guess excluded" % (k, r["workers"])})
     out = {"impl": "reference", "metric": METRIC, "value": value, "unit": "stage-solves/s", "n_gpus": 1,
-           "steps": k, "warmup": w, "ms_per_step": el * 1e3 / (w + k), "higher_is_better": True,
+           "steps": k, "warmup": 0, "ms_per_step": r["timed_s_max"] * 1e3 / k, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded; reference .in format)",
-           "config": {"workload": WORKLOAD, "Ny": args.n, "Nz": args.n, "integrator": "RK32",
-                      "solver": "SciPy SuperLU direct (stands in for the reference's MUMPS Cholesky)"},
-           "cpu_baseline": {"value": value, "unit": "stage-solves/s", "cores": 1, "kind": "port",
-                            "sample": "%d RK32 steps (%d stage-solves, factorisation excluded)" % (w + k, evals)},
+           "config": {"workload": BATCH_WORKLOAD % r["workers"], "Ny": args.n, "Nz": args.n, "integrator": "RK32",
+                      "solver": "SciPy SuperLU direct (stands in for the reference's MUMPS Cholesky)",
+                      "parallelism": "one instance per host core"},
+           "cpu_baseline": cpu,
            "e2e": {"value": value, "unit": "stage-solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
 
@@ -779,10 +972,12 @@ def main():
     ap.add_argument("--rtol", type=float, default=1e-12)
     ap.add_argument("--check-every", type=int, default=1)
     ap.add_argument("--precond", default="auto", choices=["auto", "mg", "fd"])
-    ap.add_argument("--cpu-steps", type=int, default=4)
+    ap.add_argument("--cpu-steps", type=int, default=10, help="RK32 steps per core of the CPU baseline")
+    ap.add_argument("--cpu-steps-ref", type=int, default=20, help="cap on the reference arm's steps per core")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-response", action="store_true")
     ap.add_argument("--no-cycle", action="store_true", help="skip the 801x801 quasi-dynamic / fully dynamic cycles")
+    ap.add_argument("--no-c0", action="store_true", help="skip the 200-year 101x101 run (config 0)")
     ap.add_argument("--batch", type=int, default=32, help="instances per GPU of the batched ensemble (0: none)")
     ap.add_argument("--batch-precision", default="fp64", choices=["fp64", "mixed", "tf32"])
     ap.add_argument("--batch-only", action="store_true", help="measure the batched ensemble alone")

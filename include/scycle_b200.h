@@ -588,12 +588,14 @@ scy_status scy_batch_set_graphs(scy_batch* b, int on);
  * rounds launched directly, see scy_batch_set_graphs): CUDA events on the
  * launching stream around each launch, for measurement passes. */
 scy_status scy_batch_profile(scy_batch* b, int on);
-enum { SCY_BATCH_KERNEL_YSOLVE = 0, SCY_BATCH_KERNEL_RESIDUAL = 1, SCY_BATCH_KERNEL_MATVEC = 2 };
+enum { SCY_BATCH_KERNEL_YSOLVE = 0, SCY_BATCH_KERNEL_RESIDUAL = 1, SCY_BATCH_KERNEL_MATVEC = 2,
+       SCY_BATCH_KERNEL_ZTRANSFORM = 3 };
 /* Sums the timed launches of one kernel (SCY_BATCH_KERNEL_*): milliseconds,
  * launch count and algorithmic bytes (the banded sweeps: factor once plus
  * read and write of the transform twice; the operator kernels: coefficient
  * planes once plus the per-node operands and results of the active
- * instances). */
+ * instances; a z transform of the FP64 preconditioner: its operand and
+ * result for every instance plus the eigenvector matrix once). */
 scy_status scy_batch_profile_collect(scy_batch* b, int kernel, double* ms, long long* launches, double* bytes);
 /* Drops the recorded launches. */
 scy_status scy_batch_profile_clear(scy_batch* b);

@@ -120,9 +120,12 @@ class QDLinearElastic:
         self.sbp.change_bc_types(bc["R"], bc["T"], bc["L"], bc["B"])
         return uL * self.fts
 
-    def integrate(self, max_steps=None, replay=None, record=None):
+    def integrate(self, max_steps=None, replay=None, record=None, var0=None):
+        """integrate (strikeSlip_linearElastic_qd.cpp:666-751).  ``var0``: a
+        state from an earlier ``initiate_integrand()`` call (the initial
+        guess is then not repeated, so a timing can leave it out)."""
         s = self.P["driver"]
-        var = self.initiate_integrand()
+        var = self.initiate_integrand() if var0 is None else {k: v.copy() for k, v in var0.items()}
         rk = AdaptiveRK(s["timeIntegrator"], s["maxStepCount"] if max_steps is None else max_steps,
                         s["maxTime"], s["initDeltaT"], s["timeControlType"])
         rk.set_tolerance(s["timeStepTol"])

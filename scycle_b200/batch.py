@@ -83,9 +83,9 @@ class Batch:
 
     def profile_collect(self, kernel):
         """(milliseconds, launches, algorithmic bytes) of the timed launches of
-        "ysolve", "residual" or "matvec"."""
+        "ysolve", "residual", "matvec" or "ztransform"."""
         ms, nl, by = C.c_double(), C.c_longlong(), C.c_double()
-        k = {"ysolve": 0, "residual": 1, "matvec": 2}[kernel]
+        k = {"ysolve": 0, "residual": 1, "matvec": 2, "ztransform": 3}[kernel]
         S.check(S.lib().scy_batch_profile_collect(self.h, k, C.byref(ms), C.byref(nl), C.byref(by)))
         return ms.value, nl.value, by.value
 

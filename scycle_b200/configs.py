@@ -204,3 +204,27 @@ def pl_ensemble_c3(workdir, n_inst=128, seed=0, sizes=(101, 201, 301), Lz=30.0, 
             paths.append(path)
             i += 1
     return paths
+
+
+C4_DEPTHS = np.linspace(0.0, 30.0, 40)
+
+
+def adjoint_c4(workdir, seed=0, n=201, name="c4"):
+    """201x201 constant-grid aging-law run of the adjoint workload: steady-
+    state initial guess, RK32 steps of at most 1e4 s (the 2000 steps stay
+    early in the interseismic period), rootTol 1e-14.  a, b and Dc are
+    written as inputDir fields equal to their piecewise-linear interpolation
+    from 40 depth knots (the same map the gradient is taken through).
+    Returns (path, knot matrix P, [a, b, Dc] knot values)."""
+    from .adjoint import knot_matrix
+    path = make_qd_problem(workdir, Ny=n, Nz=n, seed=seed, state_law="agingLaw", integrator="RK32", guess_ss=1,
+                           name=name, extra={"maxDeltaT": "1e4", "rootTol": "1e-14"})
+    z = np.arange(n) / (n - 1.0) * 30.0
+    prof = {"a": np.interp(z, [0.0, 30.0], [0.010, 0.010]),
+            "b": np.interp(z, [0.0, 12.0, 17.0, 30.0], [0.015, 0.015, 0.005, 0.005]),
+            "Dc": np.full(n, 0.008)}
+    P = knot_matrix(z, C4_DEPTHS)
+    base_k = [np.interp(C4_DEPTHS, z, prof[k]) for k in ("a", "b", "Dc")]
+    for nm, k in zip(("a", "b", "Dc"), base_k):
+        write_petsc_vec(path[:-len(".in")] + "_in_" + nm, P @ k)
+    return path, P, base_k

@@ -1236,17 +1236,24 @@ int BatchContext::fd_apply(BatchGroup& g) {
       const double one = 1.0, zero = 0.0;
       const double* vz = F.Vz.as<double>();
       double* t1 = g.t1p.as<double>();
+      // algorithmic bytes of one z transform: operand and result of every
+      // instance, Vz once
+      const double ztb = 8.0 * ((double)Nz * Ny * K + (double)F.Nzp * Ny * K + (double)Nz * Nz);
+      cudaEvent_t pa;
+      SCY_TRY(prof_begin(g.stream, &pa));
       SCY_BLAS_TRY(cublasDgemm(g.blas, CUBLAS_OP_T, CUBLAS_OP_N, Nz, Ny * K, Nz, &one, vz, Nz, g.w.r, Nz, &zero, t1,
                                F.Nzp));
-      cudaEvent_t pa;
+      SCY_TRY(prof_end(g.stream, pa, PROF_ZTRANSFORM, ztb));
       SCY_TRY(prof_begin(g.stream, &pa));
       b_ysolve_tma_kernel<double, YS_I, YS_W><<<dim3((Nz + YS_C - 1) / YS_C, (K + YS_B - 1) / YS_B), 32 * YS_W,
                                     ys_smem_bytes(8), g.stream>>>(g.mLcol, g.mLrow, g.mT, t1, Ny, Nz, F.Nzp, K,
                                                                   g.w.status);
       SCY_LAUNCH_CHECK();
       SCY_TRY(prof_end(g.stream, pa, PROF_YSOLVE, 8.0 * (9.0 * Ny * Nz + 4.0 * N * K)));
+      SCY_TRY(prof_begin(g.stream, &pa));
       SCY_BLAS_TRY(cublasDgemm(g.blas, CUBLAS_OP_N, CUBLAS_OP_N, Nz, Ny * K, Nz, &one, vz, Nz, t1, F.Nzp, &zero,
                                g.w.z, Nz));
+      SCY_TRY(prof_end(g.stream, pa, PROF_ZTRANSFORM, ztb));
     }
     count_launch();
     count_launch();
@@ -1769,7 +1776,7 @@ scy_status scy_batch_profile(scy_batch* b, int on) {
 }
 
 scy_status scy_batch_profile_collect(scy_batch* b, int kernel, double* ms, long long* launches, double* bytes) {
-  if (!b || !ms || !launches || !bytes || kernel < 0 || kernel > 2) return SCY_ERR_ARG;
+  if (!b || !ms || !launches || !bytes || kernel < 0 || kernel > 3) return SCY_ERR_ARG;
   SCY_TRY(b->ctx.prof_collect(kernel, ms, launches, bytes));
   return SCY_OK;
 }

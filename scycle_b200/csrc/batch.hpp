@@ -56,7 +56,7 @@ struct BatchWork {
 };
 
 // tags of the timed kernels (scy_batch_profile_collect)
-enum { PROF_YSOLVE = 0, PROF_RESIDUAL = 1, PROF_MATVEC = 2 };
+enum { PROF_YSOLVE = 0, PROF_RESIDUAL = 1, PROF_MATVEC = 2, PROF_ZTRANSFORM = 3 };
 
 struct BatchGroup {
   int K = 0, base = 0;  // instances base .. base + K - 1 of the batch

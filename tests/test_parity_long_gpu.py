@@ -1,0 +1,111 @@
+"""Long-horizon parity on the benchmark configurations against oracle fixtures (GPU).
+
+The fixtures tests/golden/parity_{c0,c1,c4}.npz come from the oracle
+(tests/golden/make_parity_fixtures.py: the CPU restatement of
+StrikeSlip_LinearElastic_qd with a SuperLU direct solve) run free on the
+seeded inputs:
+
+* c0: 101x101 constant grid, aging law, RK32 -- the whole 200-year run
+  (805 accepted steps);
+* c1: 401x401 tanh-stretched grid, slip law, lognormal per-node Dc,
+  steady-state start -- the first 100 RK32 steps (the benchmark's instance 0);
+* c4: 201x201 constant grid, aging law, steady-state start, 2000 RK32 steps
+  of at most 1e4 s (the adjoint workload's forward run).
+
+The device driver is forced onto the oracle's attempt sequence (step sizes
+and accept decisions) and slip, slip velocity, state, shear stress and
+surface displacement are compared after the recorded steps, to 1e-9
+relative.  The batched ensemble runs the c1 instance the same way.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from scycle_b200 import configs
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REL = 1e-9
+SOLVE_RTOL = 1e-14
+
+BUILD = {
+    "c0": lambda w: configs.aging_const_101(w, seed=0),
+    "c1": lambda w: configs.slip_var_401(w, seed=0, Ny=401, Nz=401, years=1.0e4),
+    "c4": lambda w: configs.adjoint_c4(w, seed=0)[0],
+}
+
+
+def _fixture(name):
+    return np.load(os.path.join(HERE, "golden", "parity_%s.npz" % name))
+
+
+def _rel(a, b, floor):
+    a, b = np.asarray(a), np.asarray(b)
+    return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), floor)))
+
+
+def _nrel(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def _check(view, fx, k):
+    """Fields of a device driver (QD view) against snapshot k of a fixture."""
+    errs = {"slip": _rel(view.field("slip"), fx["slip"][k], 1e-12),
+            "slipVel": _rel(view.field("slipVel"), fx["slipVel"][k], 1e-300),
+            "psi": _rel(view.field("psi"), fx["psi"][k], 1e-300),
+            "tauP": _rel(view.field("tauP"), fx["tauP"][k], 1e-9),
+            "tauQSP": _rel(view.field("tauQSP"), fx["tauQSP"][k], 1e-9),
+            "surfDisp": _nrel(view.field("surfDisp"), fx["surfDisp"][k])}
+    return errs
+
+
+def _attempts(fx):
+    return list(zip(fx["attempt_dt"].tolist(), fx["attempt_acc"].astype(bool).tolist()))
+
+
+@pytest.mark.parametrize("name", ["c0", "c1", "c4"])
+def test_forced_oracle_sequence_matches_oracle(tmp_path, name):
+    from scycle_b200.qd import QD
+    fx = _fixture(name)
+    dev = QD.from_in(BUILD[name](str(tmp_path)), solve_rtol=SOLVE_RTOL)
+    dev.force_attempts(_attempts(fx))
+    dev.integrate_begin_from_in()
+    done = 0
+    worst = {}
+    for k, step in enumerate(fx["snap_steps"].tolist()):
+        st = dev.integrate_steps(step - done)
+        done = step
+        assert st.step_count == step
+        assert abs(st.t - fx["snap_t"][k]) <= 1e-12 * abs(fx["snap_t"][k])
+        for f, e in _check(dev, fx, k).items():
+            worst[f] = max(worst.get(f, 0.0), e)
+    dev.close()
+    for f, e in worst.items():
+        assert e <= REL, (name, f, e)
+
+
+def test_batched_c1_instance_matches_oracle(tmp_path):
+    """The batched ensemble (here a group of two instances of the c1
+    workload, the first forced onto the oracle's attempts) reproduces the
+    oracle's first 100 steps."""
+    from scycle_b200.batch import Batch
+    fx = _fixture("c1")
+    p0 = BUILD["c1"](str(tmp_path / "i0"))
+    p1 = configs.slip_var_401(str(tmp_path / "i1"), seed=1, Ny=401, Nz=401, years=1.0e4)
+    b = Batch([p0, p1], solve_rtol=SOLVE_RTOL)
+    v = b.instance(0)
+    v.force_attempts(_attempts(fx))
+    done = 0
+    worst = {}
+    for k, step in enumerate(fx["snap_steps"].tolist()):
+        b.run(step - done)
+        done = step
+        assert v.integrate_steps(0).step_count == step
+        for f, e in _check(v, fx, k).items():
+            worst[f] = max(worst.get(f, 0.0), e)
+    b.close()
+    for f, e in worst.items():
+        assert e <= REL, ("batch c1", f, e)
