@@ -172,6 +172,18 @@ scy_status scy_sbp_solve(scy_sbp* s, const double* rhs, double* u,
 scy_status scy_sbp_solve_noalloc(scy_sbp* s, const double* rhs, double* u,
                                  const scy_solve_opts* opts, scy_solve_stats* stats);
 
+/* FP64-accurate dense product on the integer tensor cores: D[r][c] =
+ * sum_k X[r][k] W[c][k] for r < rows, c < cols, with each row of X and W
+ * written as S = 3..7 signed 8-bit digit planes scaled by a power of two,
+ * the S(S+1)/2 digit products accumulated exactly in 32-bit integers
+ * (tcgen05.mma kind::i8) and combined in FP64; relative error per row about
+ * 100^-S.  X and D are device arrays (row strides ldx, ldd), W a host array
+ * (row stride ldw), K <= 1024.  No counterpart in the reference: it is the
+ * z transform of the fast-diagonalisation preconditioner that stands in for
+ * the reference's direct solve, exported so it can be checked on its own. */
+scy_status scy_ozaki_matmul(const double* X, long ldx, int rows, int K, const double* W, long ldw, int cols, int S,
+                            double* D, long ldd);
+
 /* Grid facts for callers (levels of the multigrid hierarchy, sizes). */
 scy_status scy_sbp_info(scy_sbp* s, int* Ny, int* Nz, int* n_levels);
 

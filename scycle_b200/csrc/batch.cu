@@ -781,7 +781,8 @@ typedef CUresult (*TmaEncodeFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, v
 // a tile map of `rank` dimensions (dims[0] innermost; strides in bytes of
 // dimensions 1..rank-1) without swizzle, reads outside the array give zeros
 int tma_encode(CUtensorMap* map, const void* base, CUtensorMapDataType type, int rank, const cuuint64_t* dims,
-               const cuuint64_t* strides, const cuuint32_t* box) {
+               const cuuint64_t* strides, const cuuint32_t* box,
+               CUtensorMapSwizzle swizzle = CU_TENSOR_MAP_SWIZZLE_NONE) {
   static TmaEncodeFn fn = nullptr;
   if (!fn) {
     void* p = nullptr;
@@ -795,7 +796,7 @@ int tma_encode(CUtensorMap* map, const void* base, CUtensorMapDataType type, int
   }
   const cuuint32_t es[3] = {1, 1, 1};
   const CUresult r = fn(map, type, (cuuint32_t)rank, const_cast<void*>(base), dims, strides, box, es,
-                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) {
     set_error("cuTensorMapEncodeTiled failed (%d)", (int)r);
@@ -820,6 +821,14 @@ int tma_map_3d(CUtensorMap* map, const void* base, CUtensorMapDataType type, lon
   const cuuint64_t strides[2] = {(cuuint64_t)stride1_bytes, (cuuint64_t)stride2_bytes};
   const cuuint32_t box[3] = {(cuuint32_t)box0, (cuuint32_t)box1, (cuuint32_t)box2};
   return tma_encode(map, base, type, 3, dims, strides, box);
+}
+
+int tma_map_3d_sw64(CUtensorMap* map, const void* base, CUtensorMapDataType type, long d0, long d1, long d2,
+                    long stride1_bytes, long stride2_bytes, int box0, int box1, int box2) {
+  const cuuint64_t dims[3] = {(cuuint64_t)d0, (cuuint64_t)d1, (cuuint64_t)d2};
+  const cuuint64_t strides[2] = {(cuuint64_t)stride1_bytes, (cuuint64_t)stride2_bytes};
+  const cuuint32_t box[3] = {(cuuint32_t)box0, (cuuint32_t)box1, (cuuint32_t)box2};
+  return tma_encode(map, base, type, 3, dims, strides, box, CU_TENSOR_MAP_SWIZZLE_64B);
 }
 
 BatchGroup::~BatchGroup() {

@@ -1,0 +1,387 @@
+// FP64-accurate products on the integer tensor cores (see ozaki.hpp).
+//
+// ozk_gemm_kernel<S, T>: one CTA of 128 threads per output tile of 128 rows
+// x CN columns.  Thread 0 of warp 0 streams 64-byte K slices of the S digit
+// planes of both operands into a ring of shared-memory stages by TMA
+// (cp.async.bulk.tensor, 64-byte swizzle, completion on an mbarrier per
+// stage); thread 0 of warp 1 issues, per stage and per 32-byte K step, the
+// S(S+1)/2 digit products (tcgen05.mma.cta_group::1.kind::i8, both operands
+// K-major in shared memory, signed 8-bit, 32-bit integer accumulators) into
+// S accumulators of 128 x CN in tensor memory, one per digit-weight group,
+// and frees each stage with tcgen05.commit on its "empty" mbarrier.  After
+// the last stage all four warps read their 32 rows of the accumulators
+// (tcgen05.ld 32x32b), combine the groups in FP64 with their powers of two,
+// apply the row and column exponents and store the tile.
+//
+// Every mbarrier wait is bounded (2^20 polls).  A wait that runs out marks
+// the tile's rows in the caller's status words; the producer then waits
+// (bounded) for the copies it issued that nobody consumed, the epilogue
+// waits (bounded) for the issued products, and tensor memory is freed
+// before the CTA exits.  TMA loads read this GPU's own memory only and use
+// no cluster multicast.
+#include <cmath>
+#include <vector>
+
+#include "ozaki.hpp"
+#include "tma.cuh"
+
+namespace scy {
+namespace {
+
+constexpr int OZK_BM = 128;  // rows per tile (tensor-memory lanes)
+constexpr int OZK_BK = 64;   // bytes of K per stage (one 64-byte swizzle row)
+constexpr int OZK_POLLS = 1 << 20;
+constexpr int OZK_SMEM_BUDGET = 220 * 1024;
+
+__host__ __device__ constexpr int ozk_cn(int S) { return S <= 3 ? 144 : S == 4 ? 112 : S == 5 ? 96 : 64; }
+__host__ __device__ constexpr int ozk_stage_bytes(int S) { return S * OZK_BM * OZK_BK + S * ozk_cn(S) * OZK_BK; }
+__host__ __device__ constexpr int ozk_stages(int S) {
+  return OZK_SMEM_BUDGET / ozk_stage_bytes(S) > 4 ? 4 : OZK_SMEM_BUDGET / ozk_stage_bytes(S);
+}
+__host__ __device__ constexpr int ozk_smem_bytes(int S) { return ozk_stages(S) * ozk_stage_bytes(S) + 1024; }
+
+// shared-memory matrix descriptor (tcgen05 format): K-major operand whose
+// rows are 64 bytes with 64-byte swizzling, 8-row groups 512 bytes apart
+__device__ __forceinline__ uint64_t umma_desc_sw64(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);  // start address, 16-byte units
+  d |= (uint64_t)1u << 16;                  // leading byte offset (unused by swizzled K-major layouts)
+  d |= (uint64_t)(512u >> 4) << 32;         // stride byte offset: next 8-row group
+  d |= (uint64_t)1u << 46;                  // descriptor version of sm_100
+  d |= (uint64_t)4u << 61;                  // layout: 64-byte swizzle
+  return d;
+}
+
+// instruction descriptor: signed 8-bit A and B, K-major, 32-bit integer
+// accumulator, M = 128, N = n
+__host__ __device__ constexpr uint32_t umma_idesc_s8(int n) {
+  return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(OZK_BM >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_s8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                        uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15}, [%16];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+        "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+      : "r"(taddr));
+}
+
+template <int S, typename T>
+__global__ void __launch_bounds__(128, 1)
+    ozk_gemm_kernel(const __grid_constant__ CUtensorMap mx, const __grid_constant__ CUtensorMap mw,
+                    const int* __restrict__ ex, const int* __restrict__ ew, T* __restrict__ D, long ldd, int rows,
+                    int cout, int nkb, unsigned* __restrict__ status, int rows_per_status, unsigned bit) {
+  constexpr int CN = ozk_cn(S);
+  constexpr int XB = S * OZK_BM * OZK_BK;
+  constexpr int WB = S * CN * OZK_BK;
+  constexpr int ST = ozk_stages(S);
+  static_assert(S * CN <= 512, "accumulators exceed tensor memory");
+  static_assert(CN % 16 == 0 && CN >= 16 && CN <= 256, "invalid MMA N");
+  extern __shared__ __align__(1024) unsigned char ozk_smem_raw[];
+  __shared__ __align__(8) uint64_t full[ST], empty[ST], done;
+  __shared__ uint32_t tmem_slot;
+  __shared__ int consumed, failed;
+  // tiles on a 1024-byte boundary (the swizzle pattern repeats every 512 B)
+  unsigned char* smem = ozk_smem_raw + ((1024u - (smem_u32(ozk_smem_raw) & 1023u)) & 1023u);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int m0 = blockIdx.x * OZK_BM, c0 = blockIdx.y * CN;
+
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < ST; ++i) {
+      mbar_init(&full[i], 1);
+      mbar_init(&empty[i], 1);
+    }
+    mbar_init(&done, 1);
+    fence_mbar_init();
+    consumed = 0;
+    failed = 0;
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(smem_u32(&tmem_slot))
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_slot;
+
+  int issued = 0;
+  if (warp == 0 && lane == 0) {
+    // producer
+    for (int kb = 0; kb < nkb; ++kb) {
+      const int st = kb % ST;
+      if (kb >= ST && !mbar_wait(&empty[st], ((kb / ST) - 1) & 1, OZK_POLLS)) {
+        failed = 1;
+        break;
+      }
+      unsigned char* sx = smem + st * (XB + WB);
+      mbar_expect_tx(&full[st], XB + WB);
+      tma_load_3d(sx, &mx, &full[st], kb * OZK_BK, m0, 0);
+      tma_load_3d(sx + XB, &mw, &full[st], kb * OZK_BK, c0, 0);
+      ++issued;
+    }
+  } else if (warp == 1 && lane == 0) {
+    // MMA issuer
+    constexpr uint32_t idesc = umma_idesc_s8(CN);
+    int kb = 0;
+    for (; kb < nkb; ++kb) {
+      const int st = kb % ST;
+      if (!mbar_wait(&full[st], (kb / ST) & 1, OZK_POLLS)) {
+        failed = 1;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t xa = smem_u32(smem + st * (XB + WB));
+      const uint32_t wa = xa + XB;
+#pragma unroll
+      for (int ks = 0; ks < 2; ++ks)
+#pragma unroll
+        for (int g = 0; g < S; ++g)
+#pragma unroll
+          for (int i = 1; i <= g + 1; ++i) {
+            const int j = g + 2 - i;
+            const uint64_t ad = umma_desc_sw64(xa + (i - 1) * OZK_BM * OZK_BK + ks * 32);
+            const uint64_t bd = umma_desc_sw64(wa + (j - 1) * CN * OZK_BK + ks * 32);
+            umma_s8(tmem + g * CN, ad, bd, idesc, (kb > 0 || ks > 0 || i > 1) ? 1u : 0u);
+          }
+      umma_commit(&empty[st]);
+    }
+    consumed = kb;
+    umma_commit(&done);  // arrives once every product issued above has completed
+  }
+  __syncthreads();
+  if (warp == 0 && lane == 0) {
+    // copies issued but never consumed (only after a wait ran out)
+    for (int kb = consumed; kb < issued; ++kb) mbar_wait(&full[kb % ST], (kb / ST) & 1, OZK_POLLS);
+  }
+  // one verdict for the whole block: the warp-collective tensor-memory
+  // loads below run in every warp or in none
+  const bool ok = __syncthreads_and(mbar_wait(&done, 0, OZK_POLLS) ? 1 : 0) && !failed;
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (!ok) {
+    if (threadIdx.x == 0 && status) {
+      const int r1 = min(m0 + OZK_BM, rows) - 1;
+      for (int q = m0 / rows_per_status; q <= r1 / rows_per_status; ++q) atomicOr(status + q, bit);
+    }
+  } else {
+    // epilogue: warp w owns tensor-memory lanes 32 w .. 32 w + 31 (rows)
+    const int row = m0 + warp * 32 + lane;
+    const int er = row < rows ? ex[row] : 0;
+    const uint32_t tl = tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll 1
+    for (int cc = 0; cc < CN; cc += 16) {
+      uint32_t v[S][16];
+#pragma unroll
+      for (int g = 0; g < S; ++g) tmem_ld16(tl + g * CN + cc, v[g]);
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      double acc[16];
+#pragma unroll
+      for (int q = 0; q < 16; ++q) acc[q] = 0.0;
+#pragma unroll
+      for (int g = S - 1; g >= 0; --g) {
+        // smallest weights first
+        const double wgt = ldexp(1.0, -7 * (g + 2));
+#pragma unroll
+        for (int q = 0; q < 16; ++q) acc[q] += (double)(int)v[g][q] * wgt;
+      }
+      if (row < rows) {
+        T* drow = D + (long)row * ldd;
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          const int c = c0 + cc + q;
+          if (c < cout) drow[c] = (T)ldexp(acc[q], er + ew[c]);
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 1) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem) : "memory");
+}
+
+// digits of one row per warp; four consecutive K positions per lane and
+// plane are written as one 32-bit word
+__global__ void ozk_split_kernel(const double* __restrict__ X, long ldx, int rows, int K, int Kp, int S,
+                                 int8_t* __restrict__ dig, long plane, int* __restrict__ expo) {
+  const int row = (int)((blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (row >= rows) return;
+  const double* x = X + (long)row * ldx;
+  double m = 0.0;
+  for (int k = lane; k < K; k += 32) m = fmax(m, fabs(x[k]));
+  m = warp_max(m);
+  const int e = m > 0.0 ? ilogb(m) + 2 : 0;
+  if (lane == 0) expo[row] = e;
+  for (int k0 = lane * 4; k0 < Kp; k0 += 128) {
+    double t[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) t[q] = (k0 + q < K) ? ldexp(x[k0 + q], 7 - e) : 0.0;
+    for (int i = 0; i < S; ++i) {
+      uint32_t w = 0;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const double d = rint(t[q]);
+        t[q] = (t[q] - d) * 128.0;
+        w |= ((uint32_t)(int)d & 0xFFu) << (8 * q);
+      }
+      *reinterpret_cast<uint32_t*>(dig + i * plane + (long)row * Kp + k0) = w;
+    }
+  }
+}
+
+template <int S, typename T>
+int launch_gemm(const OzkOperand& x, const OzkOperand& w, T* D, long ldd, int cout, cudaStream_t s, unsigned* status,
+                int rows_per_status, unsigned bit) {
+  constexpr int CN = ozk_cn(S);
+  // the shared-memory limit is a per-device function attribute
+  static unsigned long long attr_set = 0;
+  int dev = 0;
+  SCY_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64 || !(attr_set >> dev & 1ull)) {
+    SCY_CUDA_TRY(cudaFuncSetAttribute(ozk_gemm_kernel<S, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      ozk_smem_bytes(S)));
+    if (dev >= 0 && dev < 64) attr_set |= 1ull << dev;
+  }
+  const dim3 grid((x.rows + OZK_BM - 1) / OZK_BM, (cout + CN - 1) / CN);
+  ozk_gemm_kernel<S, T><<<grid, 128, ozk_smem_bytes(S), s>>>(x.map, w.map, x.expo.as<int>(), w.expo.as<int>(), D,
+                                                             ldd, x.rows, cout, x.Kp / OZK_BK, status,
+                                                             rows_per_status, bit);
+  SCY_LAUNCH_CHECK();
+  return SCY_OK;
+}
+
+template <typename T>
+int gemm_any(const OzkOperand& x, const OzkOperand& w, T* D, long ldd, int cout, cudaStream_t s, unsigned* status,
+             int rps, unsigned bit) {
+  if (x.S != w.S || x.Kp != w.Kp || x.K != w.K || cout > w.rows || cout < 1 || x.rows < 1 ||
+      w.box_rows != ozk_cn(w.S) || x.box_rows != OZK_BM || rps < 1) {
+    set_error("ozk_gemm: operands do not match (S %d/%d, K %d/%d, cout %d, W rows %d)", x.S, w.S, x.K, w.K, cout,
+              w.rows);
+    return SCY_ERR_ARG;
+  }
+  switch (x.S) {
+    case 3: return launch_gemm<3, T>(x, w, D, ldd, cout, s, status, rps, bit);
+    case 4: return launch_gemm<4, T>(x, w, D, ldd, cout, s, status, rps, bit);
+    case 5: return launch_gemm<5, T>(x, w, D, ldd, cout, s, status, rps, bit);
+    case 6: return launch_gemm<6, T>(x, w, D, ldd, cout, s, status, rps, bit);
+    case 7: return launch_gemm<7, T>(x, w, D, ldd, cout, s, status, rps, bit);
+    default: break;
+  }
+  set_error("ozk_gemm: %d digit planes (3 to 7 are built)", x.S);
+  return SCY_ERR_ARG;
+}
+
+}  // namespace
+
+int ozk_cols_per_tile(int S) { return ozk_cn(S); }
+
+int OzkOperand::alloc(int S_, int rows_, int K_, int box_rows_) {
+  if (S_ < 3 || S_ > 7 || rows_ < 1 || K_ < 1 || K_ > 1024 || box_rows_ < 8 || box_rows_ > 256) {
+    set_error("OzkOperand: invalid shape (S %d, rows %d, K %d, box rows %d)", S_, rows_, K_, box_rows_);
+    return SCY_ERR_ARG;
+  }
+  S = S_;
+  rows = rows_;
+  K = K_;
+  Kp = (K + OZK_BK - 1) / OZK_BK * OZK_BK;
+  box_rows = box_rows_;
+  plane = (long)rows * Kp;
+  SCY_TRY(dig.alloc((size_t)S * plane));
+  SCY_TRY(expo.alloc((size_t)rows * sizeof(int)));
+  // zero once: the K padding of every row stays zero
+  SCY_CUDA_TRY(cudaMemset(dig.p, 0, (size_t)S * plane));
+  SCY_CUDA_TRY(cudaMemset(expo.p, 0, (size_t)rows * sizeof(int)));
+  if (tma_map_3d_sw64(&map, dig.p, CU_TENSOR_MAP_DATA_TYPE_UINT8, Kp, rows, S, Kp, plane, OZK_BK, box_rows, S) !=
+      SCY_OK)
+    return SCY_ERR_CUDA;
+  return SCY_OK;
+}
+
+int ozk_split(OzkOperand& o, const double* X, long ldx, cudaStream_t s) {
+  const int threads = 256;
+  const int blocks = (int)(((long)o.rows * 32 + threads - 1) / threads);
+  ozk_split_kernel<<<blocks, threads, 0, s>>>(X, ldx, o.rows, o.K, o.Kp, o.S, o.dig.as<int8_t>(), o.plane,
+                                              o.expo.as<int>());
+  SCY_LAUNCH_CHECK();
+  return SCY_OK;
+}
+
+int ozk_set_host(OzkOperand& o, const double* W, long ldw, cudaStream_t s) {
+  std::vector<int8_t> dig((size_t)o.S * o.plane, 0);
+  std::vector<int> ex(o.rows, 0);
+  for (int r = 0; r < o.rows; ++r) {
+    const double* x = W + (long)r * ldw;
+    double m = 0.0;
+    for (int k = 0; k < o.K; ++k) m = std::fmax(m, std::fabs(x[k]));
+    const int e = m > 0.0 ? std::ilogb(m) + 2 : 0;
+    ex[r] = e;
+    for (int k = 0; k < o.K; ++k) {
+      double t = std::ldexp(x[k], 7 - e);
+      for (int i = 0; i < o.S; ++i) {
+        const double d = std::nearbyint(t);
+        t = (t - d) * 128.0;
+        dig[(size_t)i * o.plane + (size_t)r * o.Kp + k] = (int8_t)(int)d;
+      }
+    }
+  }
+  SCY_CUDA_TRY(cudaMemcpyAsync(o.dig.p, dig.data(), dig.size(), cudaMemcpyHostToDevice, s));
+  SCY_CUDA_TRY(cudaMemcpyAsync(o.expo.p, ex.data(), ex.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+  SCY_CUDA_TRY(cudaStreamSynchronize(s));
+  return SCY_OK;
+}
+
+int ozk_gemm(const OzkOperand& x, const OzkOperand& w, double* D, long ldd, int cout, cudaStream_t s,
+             unsigned* status, int rows_per_status, unsigned bit) {
+  return gemm_any<double>(x, w, D, ldd, cout, s, status, rows_per_status, bit);
+}
+
+int ozk_gemm(const OzkOperand& x, const OzkOperand& w, float* D, long ldd, int cout, cudaStream_t s,
+             unsigned* status, int rows_per_status, unsigned bit) {
+  return gemm_any<float>(x, w, D, ldd, cout, s, status, rows_per_status, bit);
+}
+
+}  // namespace scy
+
+// ---------------------------------------------------------------------------
+// C ABI: the product on its own (set-up and digit planes allocated per call)
+extern "C" scy_status scy_ozaki_matmul(const double* X, long ldx, int rows, int K, const double* W, long ldw,
+                                       int cols, int S, double* D, long ldd) {
+  using namespace scy;
+  if (!X || !W || !D || rows < 1 || cols < 1 || K < 1 || ldx < K || ldw < K || ldd < cols) {
+    set_error("scy_ozaki_matmul: invalid arguments");
+    return SCY_ERR_ARG;
+  }
+  OzkOperand x, w;
+  SCY_TRY(x.alloc(S, rows, K, 128));
+  SCY_TRY(w.alloc(S, cols, K, ozk_cols_per_tile(S)));
+  cudaStream_t s = 0;
+  SCY_TRY(ozk_set_host(w, W, ldw, s));
+  SCY_TRY(ozk_split(x, X, ldx, s));
+  DevBuf status;
+  SCY_TRY(status.alloc(sizeof(unsigned)));
+  SCY_CUDA_TRY(cudaMemsetAsync(status.p, 0, sizeof(unsigned), s));
+  SCY_TRY(ozk_gemm(x, w, D, ldd, cols, s, status.as<unsigned>(), 1 << 30, 1u));
+  unsigned st = 0;
+  SCY_CUDA_TRY(cudaMemcpyAsync(&st, status.p, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+  SCY_CUDA_TRY(cudaStreamSynchronize(s));
+  if (st) {
+    set_error("scy_ozaki_matmul: a pipeline wait in the product kernel ran out");
+    return SCY_ERR_CUDA;
+  }
+  return SCY_OK;
+}

@@ -23,6 +23,13 @@ int tma_map_2d(CUtensorMap* map, const void* base, CUtensorMapDataType type, int
 int tma_map_3d(CUtensorMap* map, const void* base, CUtensorMapDataType type, long d0, long d1, long d2,
                long stride1_bytes, long stride2_bytes, int box0, int box1, int box2);
 
+// the same with 64-byte swizzling of the box's rows in shared memory (box0
+// elements of the innermost dimension must span exactly 64 bytes; the
+// destination must be 512-byte aligned): the K-major canonical layout
+// tcgen05.mma reads through a SWIZZLE_64B shared-memory descriptor
+int tma_map_3d_sw64(CUtensorMap* map, const void* base, CUtensorMapDataType type, long d0, long d1, long d2,
+                    long stride1_bytes, long stride2_bytes, int box0, int box1, int box2);
+
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }

@@ -1,0 +1,90 @@
+"""Integer-tensor-core products of FP64 matrices (scy_ozaki_matmul) on the GPU.
+
+The product splits every row of X and W into S signed 8-bit digit planes
+scaled by a power of two, multiplies the planes exactly on the tensor cores
+(tcgen05.mma kind::i8, 32-bit accumulators) and combines the digit-weight
+groups in FP64.  ``emulate`` restates that arithmetic in numpy: with exact
+integer products and the same combination order the device must agree with
+it to the last bit (up to one rounding of the final FP64 sums); against the
+plain FP64 product the error per row is about 100^-S.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from scycle_b200 import _lib as S
+
+pytestmark = pytest.mark.gpu
+
+
+def digits(X, s):
+    m = np.abs(X).max(axis=1)
+    _, p = np.frexp(m)  # m = f 2^p, f in [1/2, 1): ilogb(m) = p - 1
+    e = np.where(m > 0, p.astype(np.int64) + 1, 0)
+    t = np.ldexp(X, (7 - e)[:, None])
+    D = []
+    for _ in range(s):
+        d = np.rint(t)
+        D.append(d.astype(np.int64))
+        t = (t - d) * 128.0
+    return D, e
+
+
+def emulate(X, W, s):
+    dx, ex = digits(X, s)
+    dw, ew = digits(W, s)
+    acc = np.zeros((X.shape[0], W.shape[0]))
+    for g in range(s - 1, -1, -1):
+        P = np.zeros(acc.shape, dtype=np.int64)
+        for i in range(1, g + 2):
+            P += dx[i - 1] @ dw[g + 1 - i].T
+        assert np.abs(P).max() < 2 ** 31
+        acc += P.astype(np.float64) * 2.0 ** (-7 * (g + 2))
+    return np.ldexp(acc, ex[:, None] + ew[None, :])
+
+
+BOUND = {3: 1e-4, 4: 1e-6, 5: 1e-8, 6: 1e-10, 7: 1e-12}
+
+
+def _matmul(X, W, s, ldx=None, ldd=None):
+    import torch
+    rows, K = X.shape[0], W.shape[1]
+    cols = W.shape[0]
+    ldx = ldx or X.shape[1]
+    ldd = ldd or cols
+    Xd = torch.from_numpy(np.ascontiguousarray(X)).cuda()
+    Dd = torch.zeros((rows, ldd), dtype=torch.float64, device="cuda")
+    S.check(S.lib().scy_ozaki_matmul(C.c_void_p(Xd.data_ptr()), ldx, rows, K, S.as_dptr(np.ascontiguousarray(W)), K,
+                                     cols, s, C.c_void_p(Dd.data_ptr()), ldd))
+    return Dd.cpu().numpy()
+
+
+@pytest.mark.parametrize("s", [3, 4, 5, 6, 7])
+@pytest.mark.parametrize("rows,K,cols", [(300, 401, 401), (1000, 129, 200)])
+def test_ozaki_matmul_matches_emulation_and_fp64(s, rows, K, cols):
+    rng = np.random.default_rng(s * 100 + K)
+    X = rng.standard_normal((rows, K)) * np.exp(3 * rng.standard_normal((rows, 1)))
+    X[:, : K // 8] *= 1e-5
+    X[7] = 0.0  # an all-zero row
+    Q, _ = np.linalg.qr(rng.standard_normal((K, K)))
+    W = np.ascontiguousarray(np.vstack([Q, Q])[:cols])
+    D = _matmul(X, W, s)
+    E = emulate(X, W, s)
+    assert np.all(np.isfinite(D))
+    assert np.all(D[7] == 0.0)
+    np.testing.assert_allclose(D, E, rtol=1e-15, atol=1e-300)
+    exact = X @ W.T
+    rel = np.linalg.norm(D - exact, axis=1) / np.maximum(np.linalg.norm(exact, axis=1), 1e-300)
+    assert rel.max() <= BOUND[s], rel.max()
+
+
+def test_ozaki_matmul_strided_rows():
+    """Row strides larger than K (the padded layouts the preconditioner uses)."""
+    rng = np.random.default_rng(5)
+    rows, K, cols, ldx, ldd = 257, 401, 401, 404, 404
+    Xfull = rng.standard_normal((rows, ldx))
+    W = rng.standard_normal((cols, K))
+    D = _matmul(Xfull, W, 7, ldx=ldx, ldd=ldd)
+    np.testing.assert_allclose(D[:, :cols], emulate(Xfull[:, :K], W, 7), rtol=1e-15, atol=1e-300)
+    assert np.all(D[:, cols:] == 0.0)
