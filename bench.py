@@ -184,7 +184,9 @@ def oracle_errors(name, make, rtol, batch_precision=None):
 
 
 # ---------------------------------------------------------------------------
-ZT_DESC = "z transforms of the preconditioner (cuBLAS DGEMM, two per apply)"
+ZT_DESC = ("ozk_gemm_kernel (z transforms of the preconditioner on the integer tensor cores: tcgen05 kind::i8 "
+           "digit-plane products, TMA-fed, tensor-memory accumulators; two per apply)")
+ZS_DESC = "ozk_split_kernel (digit planes of the z-transform operand, two per apply)"
 BATCH_WORKLOAD = ("slip_var_401 ensemble: %d instances per GPU of the 401x401 stretched-grid slip-law workload "
                   "(seeds differ: lognormal Dc and initial state), every instance with its own RK32 step control")
 
@@ -202,7 +204,7 @@ def run_batched(args, dist, rank, world, local):
     work = tempfile.mkdtemp(prefix="scy_batch_")
     paths = [make_workload(os.path.join(work, "i%d" % s), n=args.n, seed=rank * K + s) for s in range(K)]
     t0 = time.perf_counter()
-    b = Batch(paths, solve_rtol=args.rtol, precision=args.batch_precision)
+    b = Batch(paths, solve_rtol=args.rtol, precision=args.batch_precision, transform_planes=args.transform_planes)
     setup_s = time.perf_counter() - t0
     for i in range(K):
         b.instance(i).record_attempts(True)
@@ -279,14 +281,31 @@ def run_batched(args, dist, rank, world, local):
     for nm, desc in (("ysolve", "b_ysolve_tma_kernel (banded Cholesky sweeps along y of the preconditioner)"),
                      ("matvec", "b_cross_kernel<1> (CG operator application, p update fused)"),
                      ("residual", "b_cross_kernel<0> (initial residual of each stage solve)"),
-                     ("ztransform", ZT_DESC)):
+                     ("ztransform", ZT_DESC), ("zsplit", ZS_DESC)):
         pm, pl, pb = b.profile_collect(nm)
         if pl:
             us = pm / pl * 1e3
             ach = (pb / pl) / (us / 1e6) / 1e9
-            kern[nm] = {"kernel": desc, "launch_us": us, "algorithmic_bytes_per_launch": pb / pl,
-                        "achieved": ach, "frac": ach / peak, "total_ms": pm, "launches": pl,
-                        "traffic": traffic.get(nm)}
+            kern[nm] = {"kernel": desc, "bound": "hbm", "unit": "GB/s", "peak": peak, "launch_us": us,
+                        "algorithmic_bytes_per_launch": pb / pl, "achieved": ach, "frac": ach / peak,
+                        "total_ms": pm, "launches": pl, "traffic": traffic.get(nm)}
+    if "ztransform" in kern:
+        # tensor-bound: algorithmic 8-bit integer operations of the digit
+        # products (2 per multiply-add, S(S+1)/2 products of rows x Nz x Nz)
+        # against the int8 dense rate, taken as twice the measured bf16 GEMM
+        # rate (the nominal B200 ratio)
+        S = args.transform_planes or (7 if args.batch_precision == "fp64" else 4 if args.batch_precision == "mixed"
+                                      else 3)
+        ops = 2.0 * S * (S + 1) / 2 * (args.n * K) * args.n * args.n
+        bf16 = _peaks().get("bf16_tflops")
+        tpeak, tsrc = (2.0 * bf16, "2 x measured bf16") if bf16 else (2.0 * 1590.0, "2 x fallback bf16 1590")
+        k = kern["ztransform"]
+        hbm_frac = k["frac"]
+        k.update({"bound": "tensor", "unit": "TOP/s (int8)", "achieved": ops / (k["launch_us"] * 1e-6) / 1e12,
+                  "peak": tpeak, "peak_source": tsrc, "planes": S, "int8_ops_per_launch": ops,
+                  "fp64_equivalent_TFLOPs": 2.0 * (args.n * K) * args.n * args.n / (k["launch_us"] * 1e-6) / 1e12,
+                  "hbm_frac_of_algorithmic_bytes": hbm_frac})
+        k["frac"] = k["achieved"] / tpeak
     b.profile_clear()
     b.set_graphs(True)
     if kern:
@@ -295,8 +314,9 @@ def run_batched(args, dist, rank, world, local):
             k["share_of_timed_kernels"] = k["total_ms"] / tot if tot else None
         top = max(kern, key=lambda k: kern[k]["total_ms"])
         t = kern[top]
-        out["roofline"] = {"kernel": t["kernel"], "bound": "hbm", "achieved": t["achieved"], "peak": peak,
-                           "unit": "GB/s", "frac": t["frac"], "peak_source": peak_src, "traffic": t["traffic"],
+        out["roofline"] = {"kernel": t["kernel"], "bound": t["bound"], "achieved": t["achieved"], "peak": t["peak"],
+                           "unit": t["unit"], "frac": t["frac"], "peak_source": t.get("peak_source", peak_src),
+                           "traffic": t["traffic"],
                            "launch_us": t["launch_us"], "algorithmic_bytes_per_launch": t["algorithmic_bytes_per_launch"],
                            "kernels": kern,
                            "note": "CUDA events on the launching stream in a pass with the round's launches issued "
@@ -688,8 +708,9 @@ def run_ours(args, dist, rank, world, local):
               "integrator": "RK32", "parallelism": "replicas x%d" % world}
     if batched:
         config.update({"instances_per_gpu": args.batch,
-                       "solver": "FP64 CG preconditioned by fast diagonalisation (%s GEMMs over the ensemble), "
-                                 "device-verified rtol %g" % (args.batch_precision, args.rtol),
+                       "solver": "FP64 CG preconditioned by fast diagonalisation (%s preconditioner; z transforms "
+                                 "on the integer tensor cores, banded sweeps along y), device-verified rtol %g"
+                                 % (args.batch_precision, args.rtol),
                        "l2": "not flushed: the ensemble's working set (about 20 MB per instance) exceeds the "
                              "126 MB L2"})
     else:
@@ -980,6 +1001,8 @@ def main():
     ap.add_argument("--no-c0", action="store_true", help="skip the 200-year 101x101 run (config 0)")
     ap.add_argument("--batch", type=int, default=32, help="instances per GPU of the batched ensemble (0: none)")
     ap.add_argument("--batch-precision", default="fp64", choices=["fp64", "mixed", "tf32"])
+    ap.add_argument("--transform-planes", type=int, default=0,
+                    help="digit planes of the tensor-core z transforms (0: by precision)")
     ap.add_argument("--batch-only", action="store_true", help="measure the batched ensemble alone")
     ap.add_argument("--c3", type=int, default=128, help="instances of the power-law ensemble (0: skip)")
     ap.add_argument("--c3-only", action="store_true", help="measure the power-law ensemble alone")

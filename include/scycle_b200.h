@@ -543,16 +543,20 @@ scy_status scy_in_cycle_info(const char* path, scy_cycle_desc* cd, double* dt_fd
  * elastic or power law) and integrator. */
 typedef struct scy_batch scy_batch;
 typedef struct scy_batch_opts {
-  int precision;  /* preconditioner of the FP64 CG: SCY_PREC_FP64 (FP64 GEMMs), SCY_PREC_MIXED (FP32
-                     GEMMs), SCY_PREC_TF32 (FP32 data, GEMMs on the TF32 tensor cores) */
+  int precision;  /* preconditioner of the FP64 CG: SCY_PREC_FP64 (FP64 data, FP64-accurate z
+                     transforms), SCY_PREC_MIXED (FP32 data and sweeps, z transforms of FP32
+                     accuracy), SCY_PREC_TF32 (FP32 data, coarser z transforms) */
   int cg_its;     /* CG iterations per stage solve at the start (0: 1 for FP64, 2 otherwise); the
                      batch raises it after a missed tolerance and tries one fewer after a run of
                      rounds without one */
   int graphs;     /* 1: one CUDA graph launch per round (default); 0: the same launches issued directly */
   int concurrent; /* 1: groups on concurrent streams (default); 0: one stream */
   int exact_jacobian; /* root-finder derivative of every instance (see scy_qd_set_jacobian) */
-  int fd_dense;   /* 1: the preconditioner as four GEMMs (y and z transforms) even where the y part
-                     is banded; 0 (default): z transform GEMMs and banded Cholesky solves along y */
+  int fd_dense;   /* 1: the preconditioner as four cuBLAS GEMMs (y and z transforms) even where the
+                     y part is banded, a reference form for tests; 0 (default): z transforms on the
+                     integer tensor cores (see scy_ozaki_matmul) and banded Cholesky solves along y */
+  int transform_planes; /* digit planes of those z transforms, 3..7 (0: 7 with the FP64
+                           preconditioner, 4 with SCY_PREC_MIXED, 3 with SCY_PREC_TF32) */
 } scy_batch_opts;
 typedef struct scy_batch_stats {
   long rounds;          /* rounds of batched attempts so far */
@@ -601,13 +605,15 @@ scy_status scy_batch_set_graphs(scy_batch* b, int on);
  * launching stream around each launch, for measurement passes. */
 scy_status scy_batch_profile(scy_batch* b, int on);
 enum { SCY_BATCH_KERNEL_YSOLVE = 0, SCY_BATCH_KERNEL_RESIDUAL = 1, SCY_BATCH_KERNEL_MATVEC = 2,
-       SCY_BATCH_KERNEL_ZTRANSFORM = 3 };
+       SCY_BATCH_KERNEL_ZTRANSFORM = 3, SCY_BATCH_KERNEL_ZSPLIT = 4 };
 /* Sums the timed launches of one kernel (SCY_BATCH_KERNEL_*): milliseconds,
  * launch count and algorithmic bytes (the banded sweeps: factor once plus
  * read and write of the transform twice; the operator kernels: coefficient
  * planes once plus the per-node operands and results of the active
- * instances; a z transform of the FP64 preconditioner: its operand and
- * result for every instance plus the eigenvector matrix once). */
+ * instances; a z transform of the preconditioner on the tensor cores: the
+ * digit planes and exponents of the operand and of the weights read, the
+ * result written; the digit split: the operand read, its planes and
+ * exponents written). */
 scy_status scy_batch_profile_collect(scy_batch* b, int kernel, double* ms, long long* launches, double* bytes);
 /* Drops the recorded launches. */
 scy_status scy_batch_profile_clear(scy_batch* b);

@@ -115,7 +115,7 @@ def declare_cycle(L):
 
 class BatchOpts(C.Structure):
     _fields_ = [("precision", C.c_int), ("cg_its", C.c_int), ("graphs", C.c_int), ("concurrent", C.c_int),
-                ("exact_jacobian", C.c_int), ("fd_dense", C.c_int)]
+                ("exact_jacobian", C.c_int), ("fd_dense", C.c_int), ("transform_planes", C.c_int)]
 
 
 class BatchStats(C.Structure):

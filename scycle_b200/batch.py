@@ -24,12 +24,12 @@ class _InstanceView(QD):
 
 class Batch:
     def __init__(self, paths, solve_rtol=1e-12, solve_atol=0.0, precision="fp64", cg_its=0, graphs=True,
-                 concurrent=True, solve_max_its=300, exact_jacobian=True, fd_dense=False):
+                 concurrent=True, solve_max_its=300, exact_jacobian=True, fd_dense=False, transform_planes=0):
         self.paths = [str(p) for p in paths]
         arr = (C.c_char_p * len(self.paths))(*[p.encode() for p in self.paths])
         o = S.SolveOpts(solve_rtol, solve_atol, solve_max_its, 0, 1, 1, S.PRECOND["auto"])
         bo = X.BatchOpts(S.PREC[precision], int(cg_its), 1 if graphs else 0, 1 if concurrent else 0,
-                         1 if exact_jacobian else 0, 1 if fd_dense else 0)
+                         1 if exact_jacobian else 0, 1 if fd_dense else 0, int(transform_planes))
         h = C.c_void_p()
         S.check(S.lib().scy_batch_create_from_in(len(self.paths), arr, C.byref(o), C.byref(bo), C.byref(h)))
         self.h = h
@@ -83,9 +83,9 @@ class Batch:
 
     def profile_collect(self, kernel):
         """(milliseconds, launches, algorithmic bytes) of the timed launches of
-        "ysolve", "residual", "matvec" or "ztransform"."""
+        "ysolve", "residual", "matvec", "ztransform" or "zsplit"."""
         ms, nl, by = C.c_double(), C.c_longlong(), C.c_double()
-        k = {"ysolve": 0, "residual": 1, "matvec": 2, "ztransform": 3}[kernel]
+        k = {"ysolve": 0, "residual": 1, "matvec": 2, "ztransform": 3, "zsplit": 4}[kernel]
         S.check(S.lib().scy_batch_profile_collect(self.h, k, C.byref(ms), C.byref(nl), C.byref(by)))
         return ms.value, nl.value, by.value
 

@@ -886,6 +886,12 @@ int BatchContext::create(int n_inst, const char* const* paths, const scy_solve_o
     set_error("unknown batch precision %d", precision);
     return SCY_ERR_ARG;
   }
+  zt_planes = precision == SCY_PREC_FP64 ? 7 : precision == SCY_PREC_MIXED ? 4 : 3;
+  if (o && o->transform_planes) zt_planes = o->transform_planes;
+  if (zt_planes < 3 || zt_planes > 7) {
+    set_error("transform_planes must be 3..7 (got %d)", zt_planes);
+    return SCY_ERR_ARG;
+  }
   if (its <= 0) its = precision == SCY_PREC_FP64 ? 1 : 2;
   std::vector<scy_qd*> made(n, nullptr);
   for (int i = 0; i < n; ++i) {
@@ -1149,6 +1155,22 @@ int BatchContext::setup_group(int base, int K) {
     SCY_TRY(tma_map_2d(&g.mLrow32, g.fd->Lrow32.p, d32, 4, g.Nz, (long)(g.Ny + 8) * 9, (long)Nzp * 4, YS_C, YS_R * 9));
     SCY_TRY(tma_map_3d(&g.mT32, g.t1pf.p, d32, g.Nz, g.Ny, g.K, (long)Nzp * 4, (long)g.Ny * Nzp * 4, YS_C, YS_R,
                        YS_B));
+    // digit planes of the z transforms: the operand (K*Ny rows of Nz) and
+    // the weights, rows of Vz^T (forward) and of Vz (inverse); Vz is
+    // column-major, so its columns are the forward weights' rows
+    {
+      const int S = zt_planes, Nz = g.Nz;
+      SCY_TRY(g.zx.alloc(S, (int)rowsT, Nz, 128));
+      SCY_TRY(g.zw1.alloc(S, Nz, Nz, ozk_cols_per_tile(S)));
+      SCY_TRY(g.zw2.alloc(S, Nz, Nz, ozk_cols_per_tile(S)));
+      std::vector<double> vz((size_t)Nz * Nz), vzt((size_t)Nz * Nz);
+      SCY_CUDA_TRY(cudaMemcpy(vz.data(), g.fd->Vz.p, vz.size() * 8, cudaMemcpyDeviceToHost));
+      for (int k = 0; k < Nz; ++k)
+        for (int m = 0; m < Nz; ++m) vzt[(size_t)k * Nz + m] = vz[(size_t)m * Nz + k];
+      SCY_TRY(ozk_set_host(g.zw1, vz.data(), Nz, 0));
+      SCY_TRY(ozk_set_host(g.zw2, vzt.data(), Nz, 0));
+      SCY_TRY(ozk_prepare(S));
+    }
     SCY_CUDA_TRY(cudaFuncSetAttribute(b_ysolve_tma_kernel<double, YS_I, YS_W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       ys_smem_bytes(8)));
     SCY_CUDA_TRY(cudaFuncSetAttribute(b_ysolve_tma_kernel<float, YS_I, YS_W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1223,49 +1245,57 @@ int BatchContext::fd_apply(BatchGroup& g) {
   SCY_BLAS_TRY(cublasSetStream(g.blas, g.stream));
   dim3 sg(node_blocks(N), 1, K);
   if (F.ybanded && !fd_dense) {
-    // Z = Vz [ per z mode: (Ky + lz_j My)^-1 along y ] (Vz^T R)
+    // Z = Vz [ per z mode: (Ky + lz_j My)^-1 along y ] (Vz^T R): the z
+    // transforms on the integer tensor cores (digit planes of the operand,
+    // then the product), the banded sweeps in between; a pipeline wait that
+    // runs out marks the instances of its tile (status bit 4) for a repeat
+    const double rowsT = (double)Ny * K;
+    const int S = zt_planes;
+    const double split_b = rowsT * ((precision != SCY_PREC_FP64 ? 4.0 : 8.0) * Nz + S * (double)g.zx.Kp + 4.0);
+    const double gemm_b = rowsT * (S * (double)g.zx.Kp + 4.0) + 2.0 * S * Nz * (double)g.zx.Kp +
+                          rowsT * Nz * (precision != SCY_PREC_FP64 ? 4.0 : 8.0);
+    cudaEvent_t pa;
     if (precision != SCY_PREC_FP64) {
-      SCY_BLAS_TRY(cublasSetMathMode(g.blas, precision == SCY_PREC_TF32 ? CUBLAS_TF32_TENSOR_OP_MATH
-                                                                       : CUBLAS_DEFAULT_MATH));
-      const float one = 1.0f, zero = 0.0f;
-      const float* vz = F.Vz32.as<float>();
       float* t1 = g.t1pf.as<float>();
-      SCY_BLAS_TRY(cublasSgemm(g.blas, CUBLAS_OP_T, CUBLAS_OP_N, Nz, Ny * K, Nz, &one, vz, Nz, g.w.r32, Nz, &zero,
-                               t1, F.Nzp));
-      cudaEvent_t pa;
       SCY_TRY(prof_begin(g.stream, &pa));
-      b_ysolve_tma_kernel<float, YS_I, YS_W><<<dim3((Nz + YS_C - 1) / YS_C, (K + YS_B - 1) / YS_B), 32 * YS_W, ys_smem_bytes(4),
-                                   g.stream>>>(g.mLcol32, g.mLrow32, g.mT32, t1, Ny, Nz, F.Nzp, K, g.w.status);
+      SCY_TRY(ozk_split(g.zx, g.w.r, Nz, g.stream));
+      SCY_TRY(prof_end(g.stream, pa, PROF_ZSPLIT, split_b));
+      SCY_TRY(prof_begin(g.stream, &pa));
+      SCY_TRY(ozk_gemm(g.zx, g.zw1, t1, F.Nzp, Nz, g.stream, g.w.status, Ny, 4u));
+      SCY_TRY(prof_end(g.stream, pa, PROF_ZTRANSFORM, gemm_b));
+      SCY_TRY(prof_begin(g.stream, &pa));
+      b_ysolve_tma_kernel<float, YS_I, YS_W><<<dim3((Nz + YS_C - 1) / YS_C, (K + YS_B - 1) / YS_B), 32 * YS_W,
+                                               ys_smem_bytes(4), g.stream>>>(g.mLcol32, g.mLrow32, g.mT32, t1, Ny,
+                                                                             Nz, F.Nzp, K, g.w.status);
       SCY_LAUNCH_CHECK();
       SCY_TRY(prof_end(g.stream, pa, PROF_YSOLVE, 4.0 * (9.0 * Ny * Nz + 4.0 * N * K)));
-      SCY_BLAS_TRY(cublasSgemm(g.blas, CUBLAS_OP_N, CUBLAS_OP_N, Nz, Ny * K, Nz, &one, vz, Nz, t1, F.Nzp, &zero,
-                               g.w.z32, Nz));
-    } else {
-      SCY_BLAS_TRY(cublasSetMathMode(g.blas, CUBLAS_DEFAULT_MATH));
-      const double one = 1.0, zero = 0.0;
-      const double* vz = F.Vz.as<double>();
-      double* t1 = g.t1p.as<double>();
-      // algorithmic bytes of one z transform: operand and result of every
-      // instance, Vz once
-      const double ztb = 8.0 * ((double)Nz * Ny * K + (double)F.Nzp * Ny * K + (double)Nz * Nz);
-      cudaEvent_t pa;
       SCY_TRY(prof_begin(g.stream, &pa));
-      SCY_BLAS_TRY(cublasDgemm(g.blas, CUBLAS_OP_T, CUBLAS_OP_N, Nz, Ny * K, Nz, &one, vz, Nz, g.w.r, Nz, &zero, t1,
-                               F.Nzp));
-      SCY_TRY(prof_end(g.stream, pa, PROF_ZTRANSFORM, ztb));
+      SCY_TRY(ozk_split(g.zx, (const float*)t1, F.Nzp, g.stream));
+      SCY_TRY(prof_end(g.stream, pa, PROF_ZSPLIT, split_b));
+      SCY_TRY(prof_begin(g.stream, &pa));
+      SCY_TRY(ozk_gemm(g.zx, g.zw2, g.w.z32, Nz, Nz, g.stream, g.w.status, Ny, 4u));
+      SCY_TRY(prof_end(g.stream, pa, PROF_ZTRANSFORM, gemm_b));
+    } else {
+      double* t1 = g.t1p.as<double>();
+      SCY_TRY(prof_begin(g.stream, &pa));
+      SCY_TRY(ozk_split(g.zx, g.w.r, Nz, g.stream));
+      SCY_TRY(prof_end(g.stream, pa, PROF_ZSPLIT, split_b));
+      SCY_TRY(prof_begin(g.stream, &pa));
+      SCY_TRY(ozk_gemm(g.zx, g.zw1, t1, F.Nzp, Nz, g.stream, g.w.status, Ny, 4u));
+      SCY_TRY(prof_end(g.stream, pa, PROF_ZTRANSFORM, gemm_b));
       SCY_TRY(prof_begin(g.stream, &pa));
       b_ysolve_tma_kernel<double, YS_I, YS_W><<<dim3((Nz + YS_C - 1) / YS_C, (K + YS_B - 1) / YS_B), 32 * YS_W,
-                                    ys_smem_bytes(8), g.stream>>>(g.mLcol, g.mLrow, g.mT, t1, Ny, Nz, F.Nzp, K,
-                                                                  g.w.status);
+                                                ys_smem_bytes(8), g.stream>>>(g.mLcol, g.mLrow, g.mT, t1, Ny, Nz,
+                                                                              F.Nzp, K, g.w.status);
       SCY_LAUNCH_CHECK();
       SCY_TRY(prof_end(g.stream, pa, PROF_YSOLVE, 8.0 * (9.0 * Ny * Nz + 4.0 * N * K)));
       SCY_TRY(prof_begin(g.stream, &pa));
-      SCY_BLAS_TRY(cublasDgemm(g.blas, CUBLAS_OP_N, CUBLAS_OP_N, Nz, Ny * K, Nz, &one, vz, Nz, t1, F.Nzp, &zero,
-                               g.w.z, Nz));
-      SCY_TRY(prof_end(g.stream, pa, PROF_ZTRANSFORM, ztb));
+      SCY_TRY(ozk_split(g.zx, (const double*)t1, F.Nzp, g.stream));
+      SCY_TRY(prof_end(g.stream, pa, PROF_ZSPLIT, split_b));
+      SCY_TRY(prof_begin(g.stream, &pa));
+      SCY_TRY(ozk_gemm(g.zx, g.zw2, g.w.z, Nz, Nz, g.stream, g.w.status, Ny, 4u));
+      SCY_TRY(prof_end(g.stream, pa, PROF_ZTRANSFORM, gemm_b));
     }
-    count_launch();
-    count_launch();
     return SCY_OK;
   }
   if (precision != SCY_PREC_FP64) {
@@ -1785,7 +1815,7 @@ scy_status scy_batch_profile(scy_batch* b, int on) {
 }
 
 scy_status scy_batch_profile_collect(scy_batch* b, int kernel, double* ms, long long* launches, double* bytes) {
-  if (!b || !ms || !launches || !bytes || kernel < 0 || kernel > 3) return SCY_ERR_ARG;
+  if (!b || !ms || !launches || !bytes || kernel < 0 || kernel > 4) return SCY_ERR_ARG;
   SCY_TRY(b->ctx.prof_collect(kernel, ms, launches, bytes));
   return SCY_OK;
 }

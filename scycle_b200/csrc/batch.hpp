@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "fdiag.hpp"
+#include "ozaki.hpp"
 #include "qd.hpp"
 
 struct scy_qd;
@@ -56,7 +57,7 @@ struct BatchWork {
 };
 
 // tags of the timed kernels (scy_batch_profile_collect)
-enum { PROF_YSOLVE = 0, PROF_RESIDUAL = 1, PROF_MATVEC = 2, PROF_ZTRANSFORM = 3 };
+enum { PROF_YSOLVE = 0, PROF_RESIDUAL = 1, PROF_MATVEC = 2, PROF_ZTRANSFORM = 3, PROF_ZSPLIT = 4 };
 
 struct BatchGroup {
   int K = 0, base = 0;  // instances base .. base + K - 1 of the batch
@@ -74,6 +75,11 @@ struct BatchGroup {
   cudaStream_t stream = nullptr;
   cudaEvent_t join = nullptr;
   cublasHandle_t blas = nullptr;
+  // the z transforms of the banded preconditioner on the integer tensor
+  // cores: the digit planes of the operand (residual, then the swept
+  // transform; K*Ny rows of Nz values) and of the two weight matrices
+  // (rows of Vz^T for the forward transform, rows of Vz for the inverse)
+  OzkOperand zx, zw1, zw2;
   DevBuf blas_ws;
   ~BatchGroup();
 };
@@ -93,6 +99,7 @@ struct BatchContext {
   std::vector<int> slot_of, user_of;
   std::vector<std::unique_ptr<BatchGroup>> groups;
   int n = 0, pl = 0, method = 0, precision = 0, its = 1, graphs = 1, concurrent = 1, fd_dense = 0;
+  int zt_planes = 7;  // digit planes of the tensor-core z transforms
   double rtol = 1e-12, atol = 0.0;
   int max_its = 300;
   cudaStream_t stream = nullptr;

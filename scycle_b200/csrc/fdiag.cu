@@ -148,6 +148,46 @@ int upload_as(DevBuf& b, const std::vector<double>& v, cudaStream_t s) {
   SCY_CUDA_TRY(cudaStreamSynchronize(s));
   return SCY_OK;
 }
+// Banded Cholesky solves along y, one thread per z mode j, in place on the
+// padded transform T (row i of the body at T[i * Nzp], mode j at column j):
+// forward with the column form of the factor, back with the row form (the
+// table layouts of fdiag.hpp); the eight most recent solution values of the
+// chain stay in registers.
+template <typename T>
+__global__ void fd_ysweep_kernel(const T* __restrict__ Lcol, const T* __restrict__ Lrow, T* __restrict__ t,
+                                 int Ny, int Nz, int Nzp) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= Nz) return;
+  T w[9];  // w[m]: solution at row i - m (forward) or i + m (back)
+#pragma unroll
+  for (int m = 0; m < 9; ++m) w[m] = T(0);
+  for (int i = 0; i < Ny; ++i) {
+    T s = t[(long)i * Nzp + j];
+#pragma unroll
+    for (int m = 2; m <= 8; ++m)
+      if (i - m >= 0) s -= Lcol[((long)(i - m) * 9 + m) * Nzp + j] * w[m - 1];
+    const T* c = Lcol + (long)i * 9 * Nzp + j;
+    const T y = s * c[0] - c[Nzp] * w[0];
+#pragma unroll
+    for (int m = 8; m > 0; --m) w[m] = w[m - 1];
+    w[0] = y;
+    t[(long)i * Nzp + j] = y;
+  }
+#pragma unroll
+  for (int m = 0; m < 9; ++m) w[m] = T(0);
+  for (int i = Ny - 1; i >= 0; --i) {
+    T s = t[(long)i * Nzp + j];
+#pragma unroll
+    for (int m = 2; m <= 8; ++m) s -= Lrow[((long)(i + m) * 9 + m) * Nzp + j] * w[m - 1];
+    const T* c = Lrow + (long)i * 9 * Nzp + j;
+    const T x = s * c[0] - c[Nzp] * w[0];
+#pragma unroll
+    for (int m = 8; m > 0; --m) w[m] = w[m - 1];
+    w[0] = x;
+    t[(long)i * Nzp + j] = x;
+  }
+}
+
 }  // namespace
 
 FDPrecond::~FDPrecond() {
@@ -263,6 +303,26 @@ int FDPrecond::build(const LevelHost& L, cudaStream_t s) {
   SCY_TRY(upload_as<float>(Vy32, Vyh, s));
   SCY_TRY(upload_as<float>(Vz32, Vzh, s));
   SCY_TRY(upload_as<float>(inv_lam32, il, s));
+  if (ybanded) {
+    SCY_TRY(t1p.alloc((size_t)Ny * Nzp * 8));
+    SCY_TRY(t1pf.alloc((size_t)Ny * Nzp * 4));
+    SCY_CUDA_TRY(cudaMemset(t1p.p, 0, (size_t)Ny * Nzp * 8));
+    SCY_CUDA_TRY(cudaMemset(t1pf.p, 0, (size_t)Ny * Nzp * 4));
+    std::vector<double> vzt((size_t)Nz * Nz);
+    for (int k = 0; k < Nz; ++k)
+      for (int m = 0; m < Nz; ++m) vzt[(size_t)k * Nz + m] = Vzh[(size_t)m * Nz + k];
+    for (int S : {7, 4}) {
+      OzkOperand& x = S == 7 ? zx64 : zx32;
+      OzkOperand& w1 = S == 7 ? zw1_64 : zw1_32;
+      OzkOperand& w2 = S == 7 ? zw2_64 : zw2_32;
+      SCY_TRY(x.alloc(S, Ny, Nz, 128));
+      SCY_TRY(w1.alloc(S, Nz, Nz, ozk_cols_per_tile(S)));
+      SCY_TRY(w2.alloc(S, Nz, Nz, ozk_cols_per_tile(S)));
+      SCY_TRY(ozk_set_host(w1, Vzh.data(), Nz, s));  // rows of Vz^T: the columns of Vz
+      SCY_TRY(ozk_set_host(w2, vzt.data(), Nz, s));  // rows of Vz
+      SCY_TRY(ozk_prepare(S));
+    }
+  }
   SCY_TRY(t1.alloc(N * 8));
   SCY_TRY(t2.alloc(N * 8));
   SCY_TRY(t1f.alloc(N * 4));
@@ -274,6 +334,16 @@ int FDPrecond::build(const LevelHost& L, cudaStream_t s) {
 }
 
 int FDPrecond::apply(const double* r, double* z, cudaStream_t s) {
+  if (ybanded) {
+    double* t = t1p.as<double>();
+    SCY_TRY(ozk_split(zx64, r, Nz, s));
+    SCY_TRY(ozk_gemm(zx64, zw1_64, t, Nzp, Nz, s));
+    fd_ysweep_kernel<double><<<(Nz + 63) / 64, 64, 0, s>>>(Lcol.as<double>(), Lrow.as<double>(), t, Ny, Nz, Nzp);
+    SCY_LAUNCH_CHECK();
+    SCY_TRY(ozk_split(zx64, (const double*)t, Nzp, s));
+    SCY_TRY(ozk_gemm(zx64, zw2_64, z, Nz, Nz, s));
+    return SCY_OK;
+  }
   SCY_BLAS_TRY(cublasSetStream(blas, s));
   SCY_BLAS_TRY(cublasSetMathMode(blas, CUBLAS_DEFAULT_MATH));
   const double one = 1.0, zero = 0.0;
@@ -297,6 +367,16 @@ int FDPrecond::apply(const double* r, double* z, cudaStream_t s) {
 }
 
 int FDPrecond::apply32(const double* r, float* z, cudaStream_t s) {
+  if (ybanded) {
+    float* t = t1pf.as<float>();
+    SCY_TRY(ozk_split(zx32, r, Nz, s));
+    SCY_TRY(ozk_gemm(zx32, zw1_32, t, Nzp, Nz, s));
+    fd_ysweep_kernel<float><<<(Nz + 63) / 64, 64, 0, s>>>(Lcol32.as<float>(), Lrow32.as<float>(), t, Ny, Nz, Nzp);
+    SCY_LAUNCH_CHECK();
+    SCY_TRY(ozk_split(zx32, (const float*)t, Nzp, s));
+    SCY_TRY(ozk_gemm(zx32, zw2_32, z, Nz, Nz, s));
+    return SCY_OK;
+  }
   SCY_BLAS_TRY(cublasSetStream(blas, s));
   // full FP32 GEMMs: TF32 inputs (10-bit mantissa) cost CG two to three
   // times the iterations on these operators

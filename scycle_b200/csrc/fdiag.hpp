@@ -8,11 +8,15 @@
 // generalised eigendecompositions (-Ly) Vy = My Vy Ly_lambda (Vy^T My Vy = I)
 // and likewise for z,
 //     K_sep^-1 = (Vy (x) Vz) diag(1/(ly_i + lz_j)) (Vy^T (x) Vz^T),
-// applied to a body vector R (Ny x Nz, z fastest) as four dense GEMMs on
-// the tensor cores: Z = Vy [ (Vy^T R Vz) ./ (ly_i + lz_j) ] Vz^T.
+// applied to a body vector R (Ny x Nz, z fastest) either as four dense
+// GEMMs, Z = Vy [ (Vy^T R Vz) ./ (ly_i + lz_j) ] Vz^T (when the y operator
+// is not banded), or, in the banded form every order-2/4 SBP operator has,
+// as Z = Vz [ per z mode j: (Ky + lz_j My)^-1 along y ] Vz^T R with the two
+// z transforms on the integer tensor cores (ozaki.hpp).
 #pragma once
 #include <cublas_v2.h>
 
+#include "ozaki.hpp"
 #include "sbp_solver.hpp"
 
 namespace scy {
@@ -38,6 +42,12 @@ struct FDPrecond {
   int ybanded = 0;
   int Nzp = 0;
   DevBuf Lrow, Lcol, Lrow32, Lcol32;
+  // With the banded form, apply / apply32 run the z transforms on the
+  // integer tensor cores (digit planes: 7 for apply, 4 for apply32) and the
+  // sweeps in a kernel of one thread per z mode, into the padded transform
+  // t1p (Ny rows of Nzp values); no library GEMM.
+  OzkOperand zx64, zx32, zw1_64, zw2_64, zw1_32, zw2_32;
+  DevBuf t1p, t1pf;
   ~FDPrecond();
   int build(const LevelHost& L, cudaStream_t s);
   // z = K_sep^-1 r (FP64)

@@ -216,21 +216,22 @@ __global__ void __launch_bounds__(128, 1)
 
 // digits of one row per warp; four consecutive K positions per lane and
 // plane are written as one 32-bit word
-__global__ void ozk_split_kernel(const double* __restrict__ X, long ldx, int rows, int K, int Kp, int S,
+template <typename Tin>
+__global__ void ozk_split_kernel(const Tin* __restrict__ X, long ldx, int rows, int K, int Kp, int S,
                                  int8_t* __restrict__ dig, long plane, int* __restrict__ expo) {
   const int row = (int)((blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5);
   const int lane = threadIdx.x & 31;
   if (row >= rows) return;
-  const double* x = X + (long)row * ldx;
+  const Tin* x = X + (long)row * ldx;
   double m = 0.0;
-  for (int k = lane; k < K; k += 32) m = fmax(m, fabs(x[k]));
+  for (int k = lane; k < K; k += 32) m = fmax(m, fabs((double)x[k]));
   m = warp_max(m);
   const int e = m > 0.0 ? ilogb(m) + 2 : 0;
   if (lane == 0) expo[row] = e;
   for (int k0 = lane * 4; k0 < Kp; k0 += 128) {
     double t[4];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) t[q] = (k0 + q < K) ? ldexp(x[k0 + q], 7 - e) : 0.0;
+    for (int q = 0; q < 4; ++q) t[q] = (k0 + q < K) ? ldexp((double)x[k0 + q], 7 - e) : 0.0;
     for (int i = 0; i < S; ++i) {
       uint32_t w = 0;
 #pragma unroll
@@ -245,9 +246,7 @@ __global__ void ozk_split_kernel(const double* __restrict__ X, long ldx, int row
 }
 
 template <int S, typename T>
-int launch_gemm(const OzkOperand& x, const OzkOperand& w, T* D, long ldd, int cout, cudaStream_t s, unsigned* status,
-                int rows_per_status, unsigned bit) {
-  constexpr int CN = ozk_cn(S);
+int prepare_one() {
   // the shared-memory limit is a per-device function attribute
   static unsigned long long attr_set = 0;
   int dev = 0;
@@ -256,6 +255,23 @@ int launch_gemm(const OzkOperand& x, const OzkOperand& w, T* D, long ldd, int co
     SCY_CUDA_TRY(cudaFuncSetAttribute(ozk_gemm_kernel<S, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       ozk_smem_bytes(S)));
     if (dev >= 0 && dev < 64) attr_set |= 1ull << dev;
+  }
+  return SCY_OK;
+}
+
+template <int S>
+int prepare_s() {
+  const int rc = prepare_one<S, double>();
+  return rc != SCY_OK ? rc : prepare_one<S, float>();
+}
+
+template <int S, typename T>
+int launch_gemm(const OzkOperand& x, const OzkOperand& w, T* D, long ldd, int cout, cudaStream_t s, unsigned* status,
+                int rows_per_status, unsigned bit) {
+  constexpr int CN = ozk_cn(S);
+  {
+    const int rc = prepare_one<S, T>();
+    if (rc != SCY_OK) return rc;
   }
   const dim3 grid((x.rows + OZK_BM - 1) / OZK_BM, (cout + CN - 1) / CN);
   ozk_gemm_kernel<S, T><<<grid, 128, ozk_smem_bytes(S), s>>>(x.map, w.map, x.expo.as<int>(), w.expo.as<int>(), D,
@@ -290,6 +306,19 @@ int gemm_any(const OzkOperand& x, const OzkOperand& w, T* D, long ldd, int cout,
 
 int ozk_cols_per_tile(int S) { return ozk_cn(S); }
 
+int ozk_prepare(int S) {
+  switch (S) {
+    case 3: return prepare_s<3>();
+    case 4: return prepare_s<4>();
+    case 5: return prepare_s<5>();
+    case 6: return prepare_s<6>();
+    case 7: return prepare_s<7>();
+    default: break;
+  }
+  set_error("ozk_prepare: %d digit planes (3 to 7 are built)", S);
+  return SCY_ERR_ARG;
+}
+
 int OzkOperand::alloc(int S_, int rows_, int K_, int box_rows_) {
   if (S_ < 3 || S_ > 7 || rows_ < 1 || K_ < 1 || K_ > 1024 || box_rows_ < 8 || box_rows_ > 256) {
     set_error("OzkOperand: invalid shape (S %d, rows %d, K %d, box rows %d)", S_, rows_, K_, box_rows_);
@@ -312,14 +341,18 @@ int OzkOperand::alloc(int S_, int rows_, int K_, int box_rows_) {
   return SCY_OK;
 }
 
-int ozk_split(OzkOperand& o, const double* X, long ldx, cudaStream_t s) {
+template <typename Tin>
+static int split_any(OzkOperand& o, const Tin* X, long ldx, cudaStream_t s) {
   const int threads = 256;
   const int blocks = (int)(((long)o.rows * 32 + threads - 1) / threads);
-  ozk_split_kernel<<<blocks, threads, 0, s>>>(X, ldx, o.rows, o.K, o.Kp, o.S, o.dig.as<int8_t>(), o.plane,
-                                              o.expo.as<int>());
+  ozk_split_kernel<Tin><<<blocks, threads, 0, s>>>(X, ldx, o.rows, o.K, o.Kp, o.S, o.dig.as<int8_t>(), o.plane,
+                                                   o.expo.as<int>());
   SCY_LAUNCH_CHECK();
   return SCY_OK;
 }
+
+int ozk_split(OzkOperand& o, const double* X, long ldx, cudaStream_t s) { return split_any(o, X, ldx, s); }
+int ozk_split(OzkOperand& o, const float* X, long ldx, cudaStream_t s) { return split_any(o, X, ldx, s); }
 
 int ozk_set_host(OzkOperand& o, const double* W, long ldw, cudaStream_t s) {
   std::vector<int8_t> dig((size_t)o.S * o.plane, 0);

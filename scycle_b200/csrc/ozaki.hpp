@@ -48,8 +48,13 @@ struct OzkOperand {
 // tensor-memory columns)
 int ozk_cols_per_tile(int S);
 
+// sets the kernels' shared-memory limit for S planes on the current device
+// (done by the first product too; call it before capturing one in a graph)
+int ozk_prepare(int S);
+
 // digits of the rows of a device matrix X (rows x K, row stride ldx)
 int ozk_split(OzkOperand& o, const double* X, long ldx, cudaStream_t s);
+int ozk_split(OzkOperand& o, const float* X, long ldx, cudaStream_t s);
 // digits of the rows of a host matrix W (rows x K, row stride ldw); set-up
 int ozk_set_host(OzkOperand& o, const double* W, long ldw, cudaStream_t s);
 

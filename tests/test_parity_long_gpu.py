@@ -13,9 +13,11 @@ seeded inputs:
   of at most 1e4 s (the adjoint workload's forward run).
 
 The device driver is forced onto the oracle's attempt sequence (step sizes
-and accept decisions) and slip, slip velocity, state, shear stress and
-surface displacement are compared after the recorded steps, to 1e-9
-relative.  The batched ensemble runs the c1 instance the same way.
+and accept decisions), takes the reference's own Newton path in the
+friction root find (its Jacobian expression, fault.cpp:1051, as the oracle
+does), and slip, slip velocity, state, shear stress and surface
+displacement are compared after the recorded steps, to 1e-9 relative.  The
+batched ensemble runs the c1 instance the same way.
 """
 import os
 
@@ -70,7 +72,7 @@ def _attempts(fx):
 def test_forced_oracle_sequence_matches_oracle(tmp_path, name):
     from scycle_b200.qd import QD
     fx = _fixture(name)
-    dev = QD.from_in(BUILD[name](str(tmp_path)), solve_rtol=SOLVE_RTOL)
+    dev = QD.from_in(BUILD[name](str(tmp_path)), solve_rtol=SOLVE_RTOL, exact_jacobian=False)
     dev.force_attempts(_attempts(fx))
     dev.integrate_begin_from_in()
     done = 0
@@ -83,8 +85,7 @@ def test_forced_oracle_sequence_matches_oracle(tmp_path, name):
         for f, e in _check(dev, fx, k).items():
             worst[f] = max(worst.get(f, 0.0), e)
     dev.close()
-    for f, e in worst.items():
-        assert e <= REL, (name, f, e)
+    assert max(worst.values()) <= REL, (name, worst)
 
 
 def test_batched_c1_instance_matches_oracle(tmp_path):
@@ -95,7 +96,7 @@ def test_batched_c1_instance_matches_oracle(tmp_path):
     fx = _fixture("c1")
     p0 = BUILD["c1"](str(tmp_path / "i0"))
     p1 = configs.slip_var_401(str(tmp_path / "i1"), seed=1, Ny=401, Nz=401, years=1.0e4)
-    b = Batch([p0, p1], solve_rtol=SOLVE_RTOL)
+    b = Batch([p0, p1], solve_rtol=SOLVE_RTOL, exact_jacobian=False)
     v = b.instance(0)
     v.force_attempts(_attempts(fx))
     done = 0
@@ -107,5 +108,4 @@ def test_batched_c1_instance_matches_oracle(tmp_path):
         for f, e in _check(v, fx, k).items():
             worst[f] = max(worst.get(f, 0.0), e)
     b.close()
-    for f, e in worst.items():
-        assert e <= REL, ("batch c1", f, e)
+    assert max(worst.values()) <= REL, ("batch c1", worst)
