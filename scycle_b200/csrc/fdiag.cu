@@ -8,6 +8,8 @@
 
 #include "common.cuh"
 #include "fdiag.hpp"
+#include "tma.cuh"
+#include "ysolve.cuh"
 
 namespace scy {
 
@@ -148,46 +150,6 @@ int upload_as(DevBuf& b, const std::vector<double>& v, cudaStream_t s) {
   SCY_CUDA_TRY(cudaStreamSynchronize(s));
   return SCY_OK;
 }
-// Banded Cholesky solves along y, one thread per z mode j, in place on the
-// padded transform T (row i of the body at T[i * Nzp], mode j at column j):
-// forward with the column form of the factor, back with the row form (the
-// table layouts of fdiag.hpp); the eight most recent solution values of the
-// chain stay in registers.
-template <typename T>
-__global__ void fd_ysweep_kernel(const T* __restrict__ Lcol, const T* __restrict__ Lrow, T* __restrict__ t,
-                                 int Ny, int Nz, int Nzp) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= Nz) return;
-  T w[9];  // w[m]: solution at row i - m (forward) or i + m (back)
-#pragma unroll
-  for (int m = 0; m < 9; ++m) w[m] = T(0);
-  for (int i = 0; i < Ny; ++i) {
-    T s = t[(long)i * Nzp + j];
-#pragma unroll
-    for (int m = 2; m <= 8; ++m)
-      if (i - m >= 0) s -= Lcol[((long)(i - m) * 9 + m) * Nzp + j] * w[m - 1];
-    const T* c = Lcol + (long)i * 9 * Nzp + j;
-    const T y = s * c[0] - c[Nzp] * w[0];
-#pragma unroll
-    for (int m = 8; m > 0; --m) w[m] = w[m - 1];
-    w[0] = y;
-    t[(long)i * Nzp + j] = y;
-  }
-#pragma unroll
-  for (int m = 0; m < 9; ++m) w[m] = T(0);
-  for (int i = Ny - 1; i >= 0; --i) {
-    T s = t[(long)i * Nzp + j];
-#pragma unroll
-    for (int m = 2; m <= 8; ++m) s -= Lrow[((long)(i + m) * 9 + m) * Nzp + j] * w[m - 1];
-    const T* c = Lrow + (long)i * 9 * Nzp + j;
-    const T x = s * c[0] - c[Nzp] * w[0];
-#pragma unroll
-    for (int m = 8; m > 0; --m) w[m] = w[m - 1];
-    w[0] = x;
-    t[(long)i * Nzp + j] = x;
-  }
-}
-
 }  // namespace
 
 FDPrecond::~FDPrecond() {
@@ -322,6 +284,20 @@ int FDPrecond::build(const LevelHost& L, cudaStream_t s) {
       SCY_TRY(ozk_set_host(w2, vzt.data(), Nz, s));  // rows of Vz
       SCY_TRY(ozk_prepare(S));
     }
+    // tile maps of the TMA-fed sweeps over the one instance's transform
+    const CUtensorMapDataType d64 = CU_TENSOR_MAP_DATA_TYPE_FLOAT64, d32 = CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    SCY_TRY(tma_map_2d(&mLcol, Lcol.p, d64, 8, Nz, (long)Ny * 9, (long)Nzp * 8, YS_C, YS_R * 9));
+    SCY_TRY(tma_map_2d(&mLrow, Lrow.p, d64, 8, Nz, (long)(Ny + 8) * 9, (long)Nzp * 8, YS_C, YS_R * 9));
+    SCY_TRY(tma_map_3d(&mT, t1p.p, d64, Nz, Ny, 1, (long)Nzp * 8, (long)Ny * Nzp * 8, YS_C, YS_R, YS_B));
+    SCY_TRY(tma_map_2d(&mLcol32, Lcol32.p, d32, 4, Nz, (long)Ny * 9, (long)Nzp * 4, YS_C, YS_R * 9));
+    SCY_TRY(tma_map_2d(&mLrow32, Lrow32.p, d32, 4, Nz, (long)(Ny + 8) * 9, (long)Nzp * 4, YS_C, YS_R * 9));
+    SCY_TRY(tma_map_3d(&mT32, t1pf.p, d32, Nz, Ny, 1, (long)Nzp * 4, (long)Ny * Nzp * 4, YS_C, YS_R, YS_B));
+    SCY_CUDA_TRY(cudaFuncSetAttribute(b_ysolve_tma_kernel<double, YS_I, YS_W>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, ys_smem_bytes(8)));
+    SCY_CUDA_TRY(cudaFuncSetAttribute(b_ysolve_tma_kernel<float, YS_I, YS_W>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, ys_smem_bytes(4)));
+    SCY_TRY(ys_status.alloc(sizeof(unsigned)));
+    SCY_CUDA_TRY(cudaMemset(ys_status.p, 0, sizeof(unsigned)));
   }
   SCY_TRY(t1.alloc(N * 8));
   SCY_TRY(t2.alloc(N * 8));
@@ -338,7 +314,8 @@ int FDPrecond::apply(const double* r, double* z, cudaStream_t s) {
     double* t = t1p.as<double>();
     SCY_TRY(ozk_split(zx64, r, Nz, s));
     SCY_TRY(ozk_gemm(zx64, zw1_64, t, Nzp, Nz, s));
-    fd_ysweep_kernel<double><<<(Nz + 63) / 64, 64, 0, s>>>(Lcol.as<double>(), Lrow.as<double>(), t, Ny, Nz, Nzp);
+    b_ysolve_tma_kernel<double, YS_I, YS_W><<<dim3((Nz + YS_C - 1) / YS_C, 1), 32 * YS_W, ys_smem_bytes(8), s>>>(
+        mLcol, mLrow, mT, t, Ny, Nz, Nzp, 1, ys_status.as<unsigned>());
     SCY_LAUNCH_CHECK();
     SCY_TRY(ozk_split(zx64, (const double*)t, Nzp, s));
     SCY_TRY(ozk_gemm(zx64, zw2_64, z, Nz, Nz, s));
@@ -371,7 +348,8 @@ int FDPrecond::apply32(const double* r, float* z, cudaStream_t s) {
     float* t = t1pf.as<float>();
     SCY_TRY(ozk_split(zx32, r, Nz, s));
     SCY_TRY(ozk_gemm(zx32, zw1_32, t, Nzp, Nz, s));
-    fd_ysweep_kernel<float><<<(Nz + 63) / 64, 64, 0, s>>>(Lcol32.as<float>(), Lrow32.as<float>(), t, Ny, Nz, Nzp);
+    b_ysolve_tma_kernel<float, YS_I, YS_W><<<dim3((Nz + YS_C - 1) / YS_C, 1), 32 * YS_W, ys_smem_bytes(4), s>>>(
+        mLcol32, mLrow32, mT32, t, Ny, Nz, Nzp, 1, ys_status.as<unsigned>());
     SCY_LAUNCH_CHECK();
     SCY_TRY(ozk_split(zx32, (const float*)t, Nzp, s));
     SCY_TRY(ozk_gemm(zx32, zw2_32, z, Nz, Nz, s));

@@ -44,10 +44,12 @@ struct FDPrecond {
   DevBuf Lrow, Lcol, Lrow32, Lcol32;
   // With the banded form, apply / apply32 run the z transforms on the
   // integer tensor cores (digit planes: 7 for apply, 4 for apply32) and the
-  // sweeps in a kernel of one thread per z mode, into the padded transform
-  // t1p (Ny rows of Nzp values); no library GEMM.
+  // TMA-fed sweeps of the batched ensemble (one instance) on the padded
+  // transform t1p (Ny rows of Nzp values); no library GEMM.  A sweep wait
+  // that runs out sets ys_status (the CG convergence test then fails).
   OzkOperand zx64, zx32, zw1_64, zw2_64, zw1_32, zw2_32;
-  DevBuf t1p, t1pf;
+  DevBuf t1p, t1pf, ys_status;
+  CUtensorMap mLcol, mLrow, mT, mLcol32, mLrow32, mT32;
   ~FDPrecond();
   int build(const LevelHost& L, cudaStream_t s);
   // z = K_sep^-1 r (FP64)

@@ -214,8 +214,10 @@ __global__ void __launch_bounds__(128, 1)
   if (warp == 1) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem) : "memory");
 }
 
-// digits of one row per warp; four consecutive K positions per lane and
-// plane are written as one 32-bit word
+// digits of one row per warp: lane l holds the K positions 4 l + 128 j + q
+// (q < 4, j < 8, so K <= 1024) in registers, read once; the row maximum is
+// a warp reduction, and the four digits of a position group and plane go
+// out as one 32-bit word (a warp stores 128 consecutive bytes)
 template <typename Tin>
 __global__ void ozk_split_kernel(const Tin* __restrict__ X, long ldx, int rows, int K, int Kp, int S,
                                  int8_t* __restrict__ dig, long plane, int* __restrict__ expo) {
@@ -223,15 +225,28 @@ __global__ void ozk_split_kernel(const Tin* __restrict__ X, long ldx, int rows, 
   const int lane = threadIdx.x & 31;
   if (row >= rows) return;
   const Tin* x = X + (long)row * ldx;
+  double v[8][4];
   double m = 0.0;
-  for (int k = lane; k < K; k += 32) m = fmax(m, fabs((double)x[k]));
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const int k0 = 4 * lane + 128 * j;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      v[j][q] = (k0 + q < K) ? (double)x[k0 + q] : 0.0;
+      m = fmax(m, fabs(v[j][q]));
+    }
+  }
   m = warp_max(m);
   const int e = m > 0.0 ? ilogb(m) + 2 : 0;
   if (lane == 0) expo[row] = e;
-  for (int k0 = lane * 4; k0 < Kp; k0 += 128) {
+  int8_t* drow = dig + (long)row * Kp;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const int k0 = 4 * lane + 128 * j;
+    if (k0 >= Kp) break;
     double t[4];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) t[q] = (k0 + q < K) ? ldexp((double)x[k0 + q], 7 - e) : 0.0;
+    for (int q = 0; q < 4; ++q) t[q] = ldexp(v[j][q], 7 - e);
     for (int i = 0; i < S; ++i) {
       uint32_t w = 0;
 #pragma unroll
@@ -240,7 +255,7 @@ __global__ void ozk_split_kernel(const Tin* __restrict__ X, long ldx, int rows, 
         t[q] = (t[q] - d) * 128.0;
         w |= ((uint32_t)(int)d & 0xFFu) << (8 * q);
       }
-      *reinterpret_cast<uint32_t*>(dig + i * plane + (long)row * Kp + k0) = w;
+      *reinterpret_cast<uint32_t*>(drow + i * plane + k0) = w;
     }
   }
 }

@@ -17,6 +17,14 @@ Workloads (inputs from scycle_b200/configs.py, seed 0):
   c4  adjoint_c4: 201x201, aging law, steady-state start, 2000 RK32 steps of
       at most 1e4 s (the adjoint workload's forward run)
 
+Beside the trajectory each fixture holds the oracle's own spread at
+rounding level (spread_<field>): the same attempts replayed with the plain
+direct solve instead of the refined one.  The fault stress is a
+near-cancelling difference of displacements across the finest cell, so
+FP64 rounding in u alone moves it by about 1e-11 relative, and the slip
+velocity, exponential in the stress, by about 1e-9; two FP64 solutions
+that differ only in rounding drift apart at that rate.
+
     python tests/golden/make_parity_fixtures.py [c0 c1 c4]
 """
 import os
@@ -65,6 +73,19 @@ def make(name):
            "oracle_seconds": np.array(el)}
     for f in FIELDS:
         out[f] = np.array([hist[s][f] for s in snaps])
+    # the oracle's own spread at rounding level: the same attempts replayed
+    # with the plain direct solve (no refinement), whose solutions differ from
+    # the refined ones by rounding only; per field and snapshot, the
+    # norm-wise relative difference max|a - b| / max|b|
+    t1 = time.time()
+    ora2 = QDLinearElastic(P, keep_history=True, refine=0)
+    ora2.integrate(max_steps=spec["steps"], replay=rec)
+    hist2 = {h["step"]: h for h in ora2.history}
+    for f in FIELDS:
+        out["spread_" + f] = np.array([np.max(np.abs(hist2[s][f] - hist[s][f])) / max(np.max(np.abs(hist[s][f])), 1e-300)
+                                       for s in snaps])
+    print("%s: spread run %.1f s; spread at the last snapshot: %s" % (
+        name, time.time() - t1, {f: float(out["spread_" + f][-1]) for f in FIELDS}))
     np.savez_compressed(os.path.join(HERE, "parity_%s.npz" % name), **out)
     print("%s: %d steps, %d attempts, t = %.6g s, %.1f s of oracle time" % (name, rk.stepCount, len(rec), rk.currT, el))
 

@@ -16,8 +16,18 @@ The device driver is forced onto the oracle's attempt sequence (step sizes
 and accept decisions), takes the reference's own Newton path in the
 friction root find (its Jacobian expression, fault.cpp:1051, as the oracle
 does), and slip, slip velocity, state, shear stress and surface
-displacement are compared after the recorded steps, to 1e-9 relative.  The
-batched ensemble runs the c1 instance the same way.
+displacement are compared after the recorded steps, norm-wise relative
+(max |device - oracle| / max |oracle| per field).
+
+The bar is 1e-9, or ten times the oracle's own spread where that is larger:
+the fixture holds, per field and snapshot, how far the oracle moves when
+its refined solves are replaced by the plain direct solve (solutions that
+differ by rounding only).  The fault stress is a near-cancelling difference
+of displacements across the finest cell, so rounding in u moves it by about
+1e-11 relative and the slip velocity, exponential in the stress, by about
+1e-9, and the integration carries such differences forward; a device path
+that agrees with the oracle as closely as the oracle agrees with itself
+meets the bar.  The batched ensemble runs the c1 instance the same way.
 """
 import os
 
@@ -30,7 +40,7 @@ pytestmark = pytest.mark.gpu
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REL = 1e-9
-SOLVE_RTOL = 1e-14
+SOLVE_RTOL = 1e-15  # the stress is read from the solution; solves far below the bar
 
 BUILD = {
     "c0": lambda w: configs.aging_const_101(w, seed=0),
@@ -43,25 +53,24 @@ def _fixture(name):
     return np.load(os.path.join(HERE, "golden", "parity_%s.npz" % name))
 
 
-def _rel(a, b, floor):
-    a, b = np.asarray(a), np.asarray(b)
-    return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), floor)))
-
-
 def _nrel(a, b):
     a, b = np.asarray(a), np.asarray(b)
     return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
 
 
-def _check(view, fx, k):
-    """Fields of a device driver (QD view) against snapshot k of a fixture."""
-    errs = {"slip": _rel(view.field("slip"), fx["slip"][k], 1e-12),
-            "slipVel": _rel(view.field("slipVel"), fx["slipVel"][k], 1e-300),
-            "psi": _rel(view.field("psi"), fx["psi"][k], 1e-300),
-            "tauP": _rel(view.field("tauP"), fx["tauP"][k], 1e-9),
-            "tauQSP": _rel(view.field("tauQSP"), fx["tauQSP"][k], 1e-9),
-            "surfDisp": _nrel(view.field("surfDisp"), fx["surfDisp"][k])}
-    return errs
+FIELDS = ("slip", "slipVel", "psi", "tauP", "tauQSP", "surfDisp")
+
+
+def _check(view, fx, k, worst):
+    """Fields of a device driver (QD view) against snapshot k of a fixture:
+    records in ``worst`` the largest error per field and its ratio to the
+    bar (1e-9 or ten times the oracle's spread)."""
+    for f in FIELDS:
+        e = _nrel(view.field(f), fx[f][k])
+        bar = max(REL, 10.0 * float(fx["spread_" + f][k]))
+        w = worst.setdefault(f, {"err": 0.0, "ratio": 0.0})
+        w["err"] = max(w["err"], e)
+        w["ratio"] = max(w["ratio"], e / bar)
 
 
 def _attempts(fx):
@@ -82,10 +91,9 @@ def test_forced_oracle_sequence_matches_oracle(tmp_path, name):
         done = step
         assert st.step_count == step
         assert abs(st.t - fx["snap_t"][k]) <= 1e-12 * abs(fx["snap_t"][k])
-        for f, e in _check(dev, fx, k).items():
-            worst[f] = max(worst.get(f, 0.0), e)
+        _check(dev, fx, k, worst)
     dev.close()
-    assert max(worst.values()) <= REL, (name, worst)
+    assert max(w["ratio"] for w in worst.values()) <= 1.0, (name, worst)
 
 
 def test_batched_c1_instance_matches_oracle(tmp_path):
@@ -105,7 +113,6 @@ def test_batched_c1_instance_matches_oracle(tmp_path):
         b.run(step - done)
         done = step
         assert v.integrate_steps(0).step_count == step
-        for f, e in _check(v, fx, k).items():
-            worst[f] = max(worst.get(f, 0.0), e)
+        _check(v, fx, k, worst)
     b.close()
-    assert max(worst.values()) <= REL, ("batch c1", worst)
+    assert max(w["ratio"] for w in worst.values()) <= 1.0, ("batch c1", worst)
