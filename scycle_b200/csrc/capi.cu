@@ -475,9 +475,15 @@ scy_status scy_qd_integrate_begin_from_in(scy_qd* q) {
     c.ckpt_dir = P.outputDir;
   }
   SCY_TRY(c.integrate_begin(P.ode));
-  if (P.ckpt_number > 0) {
-    // the restarted integrator continues the step count and the error history
-    // (strikeSlip_linearElastic_qd.cpp:734-738)
+  // A restart in the reference (strikeSlip_linearElastic_qd.cpp:727-738):
+  // timeMonitor(initTime, initDeltaT, 0) first sets the driver's step count
+  // to 0 and rewrites the checkpoint with the fresh integrator's error
+  // history (zeros); the step count and errors then read back are those,
+  // so the restarted run counts its steps from 0 (P control for its first
+  // three steps) with an empty error history, as integrate_begin leaves it.
+  // With the extension key ckptContinueSteps = 1 the run instead continues
+  // the checkpoint's step count and error history.
+  if (P.ckpt_number > 0 && P.ckpt_continue) {
     c.stepCount = P.step0;
     c.errA[0] = P.errA[0];
     c.errA[1] = P.errA[1];

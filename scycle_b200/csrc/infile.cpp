@@ -197,6 +197,7 @@ void load_qd_problem(const std::string& path, QDProblem& P, int cycle) {
     else if (e.var == "vL") vL_dom = c_atof(e.rhs);
     else if (e.var == "enableCheckpointing") P.ckpt = c_atoi(e.rhs);
     else if (e.var == "interval") P.ckpt_interval = (long)c_atof(e.rhs);
+    else if (e.var == "ckptContinueSteps") P.ckpt_continue = c_atoi(e.rhs);
   }
   if (P.ckpt < 0 || P.ckpt_interval < 0) throw std::runtime_error("invalid enableCheckpointing / interval");
   if (bCoordTrans > 0.0) gridType = "variableGridSpacing";

@@ -66,6 +66,10 @@ struct QDProblem {
   // chkpt_* files written by the previous run
   int ckpt = 0, ckpt_number = 0;
   long ckpt_interval = 10000;
+  // extension key ckptContinueSteps (not read by the reference): a restart
+  // keeps the checkpoint's step count and error history instead of
+  // starting both from zero as the reference's does
+  int ckpt_continue = 0;
   long step0 = 0;
   double errA[2] = {0.0, 0.0};
   std::vector<double> slipVel0;  // chkpt_slipVel (first guess of the root finder), empty if none

@@ -65,12 +65,12 @@ def _make_paths(work):
     return paths
 
 
-def _rank_main(rank, world, port, work, out):
+def _rank_main(rank, world, port, paths, out):
     import torch.distributed as dist
     os.environ.update({"MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port)})
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
-        res = run_ensemble(_make_paths(work), _oracle_runner(6), dist=dist, steps=6)
+        res = run_ensemble(paths, _oracle_runner(6), dist=dist, steps=6)
         if rank == 0:
             np.save(out, np.array(res, dtype=object), allow_pickle=True)
     finally:
@@ -87,7 +87,7 @@ def test_two_ranks_gather_equals_single_process():
         port = s.getsockname()[1]
     out = os.path.join(work, "gathered.npy")
     ctx = mp.get_context("spawn")
-    procs = [ctx.Process(target=_rank_main, args=(r, 2, port, work, out)) for r in range(2)]
+    procs = [ctx.Process(target=_rank_main, args=(r, 2, port, paths, out)) for r in range(2)]
     for p in procs:
         p.start()
     for p in procs:
