@@ -297,7 +297,7 @@ def run_batched(args, dist, rank, world, local):
         # products (2 per multiply-add, S(S+1)/2 products of rows x Nz x Nz)
         # against the int8 dense rate, taken as twice the measured bf16 GEMM
         # rate (the nominal B200 ratio)
-        S = args.transform_planes or (7 if args.batch_precision == "fp64" else 4 if args.batch_precision == "mixed"
+        S = args.transform_planes or (5 if args.batch_precision == "fp64" else 4 if args.batch_precision == "mixed"
                                       else 3)
         ops = 2.0 * S * (S + 1) / 2 * (args.n * K) * args.n * args.n
         bf16 = _peaks().get("bf16_tflops")

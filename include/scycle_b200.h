@@ -555,8 +555,10 @@ typedef struct scy_batch_opts {
   int fd_dense;   /* 1: the preconditioner as four cuBLAS GEMMs (y and z transforms) even where the
                      y part is banded, a reference form for tests; 0 (default): z transforms on the
                      integer tensor cores (see scy_ozaki_matmul) and banded Cholesky solves along y */
-  int transform_planes; /* digit planes of those z transforms, 3..7 (0: 7 with the FP64
-                           preconditioner, 4 with SCY_PREC_MIXED, 3 with SCY_PREC_TF32) */
+  int transform_planes; /* digit planes of those z transforms, 3..7 (0: 5 with the FP64
+                           preconditioner, 4 with SCY_PREC_MIXED, 3 with SCY_PREC_TF32); the CG
+                           and its residuals stay FP64 whatever the planes, so they change the
+                           iteration count, not the converged solution */
 } scy_batch_opts;
 typedef struct scy_batch_stats {
   long rounds;          /* rounds of batched attempts so far */

@@ -722,7 +722,7 @@ int BatchContext::create(int n_inst, const char* const* paths, const scy_solve_o
     set_error("unknown batch precision %d", precision);
     return SCY_ERR_ARG;
   }
-  zt_planes = precision == SCY_PREC_FP64 ? 7 : precision == SCY_PREC_MIXED ? 4 : 3;
+  zt_planes = precision == SCY_PREC_FP64 ? 5 : precision == SCY_PREC_MIXED ? 4 : 3;
   if (o && o->transform_planes) zt_planes = o->transform_planes;
   if (zt_planes < 3 || zt_planes > 7) {
     set_error("transform_planes must be 3..7 (got %d)", zt_planes);

@@ -273,10 +273,10 @@ int FDPrecond::build(const LevelHost& L, cudaStream_t s) {
     std::vector<double> vzt((size_t)Nz * Nz);
     for (int k = 0; k < Nz; ++k)
       for (int m = 0; m < Nz; ++m) vzt[(size_t)k * Nz + m] = Vzh[(size_t)m * Nz + k];
-    for (int S : {7, 4}) {
-      OzkOperand& x = S == 7 ? zx64 : zx32;
-      OzkOperand& w1 = S == 7 ? zw1_64 : zw1_32;
-      OzkOperand& w2 = S == 7 ? zw2_64 : zw2_32;
+    for (int S : {kPlanes64, kPlanes32}) {
+      OzkOperand& x = S == kPlanes64 ? zx64 : zx32;
+      OzkOperand& w1 = S == kPlanes64 ? zw1_64 : zw1_32;
+      OzkOperand& w2 = S == kPlanes64 ? zw2_64 : zw2_32;
       SCY_TRY(x.alloc(S, Ny, Nz, 128));
       SCY_TRY(w1.alloc(S, Nz, Nz, ozk_cols_per_tile(S)));
       SCY_TRY(w2.alloc(S, Nz, Nz, ozk_cols_per_tile(S)));

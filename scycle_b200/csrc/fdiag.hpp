@@ -43,10 +43,11 @@ struct FDPrecond {
   int Nzp = 0;
   DevBuf Lrow, Lcol, Lrow32, Lcol32;
   // With the banded form, apply / apply32 run the z transforms on the
-  // integer tensor cores (digit planes: 7 for apply, 4 for apply32) and the
+  // integer tensor cores (digit planes: kPlanes64 for apply, kPlanes32 for apply32) and the
   // TMA-fed sweeps of the batched ensemble (one instance) on the padded
   // transform t1p (Ny rows of Nzp values); no library GEMM.  A sweep wait
   // that runs out sets ys_status (the CG convergence test then fails).
+  static constexpr int kPlanes64 = 5, kPlanes32 = 4;  // digit planes of apply / apply32
   OzkOperand zx64, zx32, zw1_64, zw2_64, zw1_32, zw2_32;
   DevBuf t1p, t1pf, ys_status;
   CUtensorMap mLcol, mLrow, mT, mLcol32, mLrow32, mT32;

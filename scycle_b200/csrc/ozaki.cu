@@ -52,6 +52,11 @@ __device__ __forceinline__ uint64_t umma_desc_sw64(uint32_t saddr) {
   return d;
 }
 
+// 2^e as a double (exact), by its bit pattern in the normal range
+__device__ __forceinline__ double pow2i(int e) {
+  return (e >= -1022 && e <= 1023) ? __longlong_as_double((long long)(e + 1023) << 52) : ldexp(1.0, e);
+}
+
 // instruction descriptor: signed 8-bit A and B, K-major, 32-bit integer
 // accumulator, M = 128, N = n
 __host__ __device__ constexpr uint32_t umma_idesc_s8(int n) {
@@ -92,6 +97,7 @@ __global__ void __launch_bounds__(128, 1)
   constexpr int ST = ozk_stages(S);
   static_assert(S * CN <= 512, "accumulators exceed tensor memory");
   static_assert(CN % 16 == 0 && CN >= 16 && CN <= 256, "invalid MMA N");
+  static_assert(8 * 256 + OZK_BM * (CN + 1) * (int)sizeof(T) <= ST * (XB + WB), "epilogue tile exceeds the stages");
   extern __shared__ __align__(1024) unsigned char ozk_smem_raw[];
   __shared__ __align__(8) uint64_t full[ST], empty[ST], done;
   __shared__ uint32_t tmem_slot;
@@ -179,9 +185,17 @@ __global__ void __launch_bounds__(128, 1)
       for (int q = m0 / rows_per_status; q <= r1 / rows_per_status; ++q) atomicOr(status + q, bit);
     }
   } else {
-    // epilogue: warp w owns tensor-memory lanes 32 w .. 32 w + 31 (rows)
-    const int row = m0 + warp * 32 + lane;
-    const int er = row < rows ? ex[row] : 0;
+    // epilogue: warp w owns tensor-memory lanes 32 w .. 32 w + 31 (rows).
+    // The tile goes through shared memory (the stage buffers are free once
+    // every product has completed) so that each warp stores whole row
+    // segments; the exponents become exact power-of-two factors.
+    constexpr int LDT = CN + 1;
+    double* sw = reinterpret_cast<double*>(smem);         // 2^ew of the tile's columns
+    T* tile = reinterpret_cast<T*>(smem + 8 * 256);       // 128 x LDT
+    for (int c = threadIdx.x; c < CN; c += 128) sw[c] = c0 + c < cout ? pow2i(ew[c0 + c]) : 0.0;
+    __syncthreads();
+    const int rl = warp * 32 + lane, row = m0 + rl;
+    const double xs = row < rows ? pow2i(ex[row]) : 0.0;
     const uint32_t tl = tmem + ((uint32_t)(warp * 32) << 16);
 #pragma unroll 1
     for (int cc = 0; cc < CN; cc += 16) {
@@ -195,18 +209,20 @@ __global__ void __launch_bounds__(128, 1)
 #pragma unroll
       for (int g = S - 1; g >= 0; --g) {
         // smallest weights first
-        const double wgt = ldexp(1.0, -7 * (g + 2));
+        const double wgt = pow2i(-7 * (g + 2));
 #pragma unroll
         for (int q = 0; q < 16; ++q) acc[q] += (double)(int)v[g][q] * wgt;
       }
-      if (row < rows) {
-        T* drow = D + (long)row * ldd;
 #pragma unroll
-        for (int q = 0; q < 16; ++q) {
-          const int c = c0 + cc + q;
-          if (c < cout) drow[c] = (T)ldexp(acc[q], er + ew[c]);
-        }
-      }
+      for (int q = 0; q < 16; ++q) tile[rl * LDT + cc + q] = (T)((acc[q] * xs) * sw[cc + q]);
+    }
+    __syncwarp();
+    const int ncol = min(CN, cout - c0);
+    for (int r = 0; r < 32; ++r) {
+      const int rr = warp * 32 + r;
+      if (m0 + rr >= rows) break;
+      T* drow = D + (long)(m0 + rr) * ldd + c0;
+      for (int c = lane; c < ncol; c += 32) drow[c] = tile[rr * LDT + c];
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
