@@ -212,7 +212,10 @@ scy_status scy_grid_host_apply_cross(const scy_grid_desc* desc, const double* in
  * (source/odeSolver.cpp:505-627, :973-1175) with P / PID step control
  * (:395-445, :846-898).
  * ---------------------------------------------------------------------- */
-enum { SCY_LAW_AGING = 0, SCY_LAW_SLIP = 1, SCY_LAW_CONSTANT = 2 };
+/* SCY_LAW_FLASH: flashHeating_psi (fault.cpp:2171-2196) with the weakening
+ * velocity of the fault temperature (flashHeating_Vw :2162-2168); drivers
+ * created from an input file with thermalCoupling set only. */
+enum { SCY_LAW_AGING = 0, SCY_LAW_SLIP = 1, SCY_LAW_CONSTANT = 2, SCY_LAW_FLASH = 3 };
 
 typedef struct scy_fault_desc {
   int Nz;

@@ -9,6 +9,7 @@
 #include "cycle.hpp"
 #include "cycle_host.hpp"
 #include "infile.hpp"
+#include "thermal.hpp"
 #include "qd.hpp"
 #include "sbp_solver.hpp"
 
@@ -566,6 +567,18 @@ scy_status scy_in_problem_field(const char* path, const char* name, double* out,
   else if (nm == "eta") v = &P.eta;
   else if (nm == "bcL") v = &P.bcL0;
   else if (nm == "bcRShift") v = &P.bcRShift;
+  else if (P.heat) {
+    // the heat equation's fields (thermalCoupling set)
+    const scy::HeatProblem& H = *P.heat;
+    if (nm == "Tamb") v = &H.Tamb;
+    else if (nm == "T") v = &H.T;
+    else if (nm == "heat_k") v = &H.k;
+    else if (nm == "heat_rho") v = &H.rho;
+    else if (nm == "heat_c") v = &H.c;
+    else if (nm == "Qrad") v = &H.Qrad;
+    else if (nm == "Gw") v = &H.Gw;
+    else if (nm == "Tw") v = &H.Tw;
+  }
   if (!v) {
     scy::set_error("unknown problem field '%s'", name);
     return SCY_ERR_ARG;

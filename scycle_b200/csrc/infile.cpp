@@ -2,6 +2,7 @@
 // interpolation and its PETSc-binary vectors, and assembly of a
 // linear-elastic quasi-dynamic problem from them.
 #include "infile.hpp"
+#include "thermal.hpp"
 
 #include <algorithm>
 #include <cmath>
@@ -373,13 +374,25 @@ void load_qd_problem(const std::string& path, QDProblem& P, int cycle) {
     else if (cycle && e.var == "momBal_bcB_fd") fdB = e.rhs;
     else if (cycle && e.var == "fd_ayIndexQuirk") ay_quirk = c_atoi(e.rhs);
   }
-  if (thermal != "no" || hydraulic != "no") throw std::runtime_error("thermal / hydraulic coupling is outside this path");
+  if (hydraulic != "no") throw std::runtime_error("hydraulic coupling is outside this path");
+  if (thermal != "no" && thermal != "uncoupled" && thermal != "coupled")
+    throw std::runtime_error("thermalCoupling must be no, uncoupled or coupled");
+  if (thermal != "no" && (cycle || P.pl))
+    throw std::runtime_error("thermal coupling is built for the linear-elastic quasi-dynamic driver");
   if (forcing != "no") throw std::runtime_error("forcingType '" + forcing + "' is outside this path");
-  if (stateLaw != "agingLaw" && stateLaw != "slipLaw" && stateLaw != "constantState")
+  if (stateLaw != "agingLaw" && stateLaw != "slipLaw" && stateLaw != "constantState" && stateLaw != "flashHeating")
     throw std::runtime_error("stateLaw '" + stateLaw + "' is outside this path");
+  if (stateLaw == "flashHeating" && thermal == "no")
+    throw std::runtime_error("stateLaw flashHeating reads the heat equation's temperature: set thermalCoupling");
   if (guess != 0 && guess != 1) throw std::runtime_error("guessSteadyStateICs must be 0 or 1");
+  // RK32_WBE / RK43_WBE (odeSolverImex.cpp): the RK32 / RK43 stages with a
+  // strict acceptance test, then one implicit heat step per accepted step
+  P.imex = (timeIntegrator == "RK32_WBE" || timeIntegrator == "RK43_WBE") ? 1 : 0;
+  if (P.imex) timeIntegrator = timeIntegrator.substr(0, 4);
+  if (P.imex && thermal == "no") throw std::runtime_error("RK32_WBE / RK43_WBE integrate the heat equation: set thermalCoupling");
+  if (thermal != "no" && !P.imex) throw std::runtime_error("thermalCoupling needs timeIntegrator RK32_WBE or RK43_WBE");
   if (timeIntegrator != "RK32" && timeIntegrator != "RK43")
-    throw std::runtime_error("timeIntegrator '" + timeIntegrator + "' is outside this path (RK32, RK43)");
+    throw std::runtime_error("timeIntegrator '" + timeIntegrator + "' is outside this path (RK32, RK43, RK32_WBE, RK43_WBE)");
   if (timeControlType != "P" && timeControlType != "PID") throw std::runtime_error("timeControlType must be P or PID");
   if (normType != "L2_absolute" && normType != "L2_relative") throw std::runtime_error("normType must be L2_absolute or L2_relative");
   // checkInput runs before computeMinTimeStep (strikeSlip_linearElastic_qd.cpp:218-220)
@@ -453,7 +466,13 @@ void load_qd_problem(const std::string& path, QDProblem& P, int cycle) {
   d.fault.vL = vL_dom;
   d.fault.root_tol = rootTol;
   d.fault.max_its = 10000;
-  d.fault.state_law = stateLaw == "agingLaw" ? SCY_LAW_AGING : stateLaw == "slipLaw" ? SCY_LAW_SLIP : SCY_LAW_CONSTANT;
+  d.fault.state_law = stateLaw == "agingLaw" ? SCY_LAW_AGING : stateLaw == "slipLaw" ? SCY_LAW_SLIP
+                      : stateLaw == "flashHeating" ? SCY_LAW_FLASH : SCY_LAW_CONSTANT;
+  // the heat equation (thermalCoupling uncoupled / coupled)
+  if (thermal != "no") {
+    P.heat = std::make_shared<HeatProblem>();
+    load_heat_problem(path, P, *P.heat);
+  }
   d.fault.exact_jacobian = 1;
   d.fault_type_scale = fts;
   d.bcL_from_slip = 1;

@@ -1,11 +1,14 @@
 // The reference's ``.in`` input format and PETSc-binary vectors, on the host.
 #pragma once
+#include <memory>
 #include <string>
 #include <vector>
 
 #include "../../include/scycle_b200.h"
 
 namespace scy {
+
+struct HeatProblem;
 
 struct InEntry {
   std::string var, rhs, full;  // key, value up to the first space, everything after " = "
@@ -73,6 +76,10 @@ struct QDProblem {
   long step0 = 0;
   double errA[2] = {0.0, 0.0};
   std::vector<double> slipVel0;  // chkpt_slipVel (first guess of the root finder), empty if none
+  // RK32_WBE / RK43_WBE (strict acceptance, a heat step after each accepted
+  // step) and the heat equation of thermalCoupling uncoupled / coupled
+  int imex = 0;
+  std::shared_ptr<HeatProblem> heat;
 };
 
 // Builds the problem like Domain + LinearElastic + Fault_qd +
