@@ -344,6 +344,17 @@ def run_batched(args, dist, rank, world, local):
         hs["state"][pos_slip] = hs["slip"]
 
     pack()
+
+    def e2e_step():
+        b.set_states(hs["state"])
+        b.run(1)
+        b.fault_field("psi", hs["psi"])
+        b.fault_field("slip", hs["slip"])
+        b.fault_field("slipVel", hs["vel"])
+        pack()
+
+    for _ in range(max(1, args.warmup // 2)):  # untimed: first uses of the transfer path
+        e2e_step()
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -351,12 +362,7 @@ def run_batched(args, dist, rank, world, local):
     t_w = time.perf_counter()
     ev0.record()
     for _ in range(args.steps):
-        b.set_states(hs["state"])
-        b.run(1)
-        b.fault_field("psi", hs["psi"])
-        b.fault_field("slip", hs["slip"])
-        b.fault_field("slipVel", hs["vel"])
-        pack()
+        e2e_step()
     ev1.record()
     torch.cuda.synchronize()
     e_ms = _max_over_ranks(dist, ev0.elapsed_time(ev1))

@@ -411,7 +411,11 @@ scy_status scy_pl_create(const scy_qd_desc* desc, const scy_pl_desc* pl, scy_qd*
 scy_status scy_qd_state_size(scy_qd* q, long* n);
 
 enum {
-  SCY_FIELD_GVXY = 11, SCY_FIELD_GVXZ = 12, SCY_FIELD_SXZ = 13, SCY_FIELD_SDEV = 14, SCY_FIELD_EFFVISC = 15
+  SCY_FIELD_GVXY = 11, SCY_FIELD_GVXZ = 12, SCY_FIELD_SXZ = 13, SCY_FIELD_SDEV = 14, SCY_FIELD_EFFVISC = 15,
+  /* thermal drivers (thermalCoupling uncoupled / coupled): the heat
+   * equation's temperature (Ny*Nz) and the flash-heating law's weakening
+   * velocity (Nz) */
+  SCY_FIELD_TEMPERATURE = 16, SCY_FIELD_VW = 17, SCY_FIELD_DTEMP = 18 /* T - Tamb (Ny*Nz) */
 };
 
 /* ---------------------------------------------------------------------------

@@ -21,7 +21,6 @@ problem of the restarted run, as the reference does:
   with an empty error history, as a fresh AdaptiveRK does.
 """
 import copy
-import os
 
 from .infile import read_petsc_vecs
 
@@ -30,12 +29,14 @@ VECS = ("slip", "slipVel", "psi", "sNEff", "sN", "tau", "tauQS", "prestress", "m
         "momBal_bcT", "momBal_bcL", "momBal_bcB")
 
 
-def read_checkpoint(out_dir):
+def read_checkpoint(out_prefix):
+    """The checkpoint under outputDir ``out_prefix`` (a path prefix that
+    file names are appended to, as the reference's outputDir is)."""
     ck = {}
     for nm in SCALARS:
-        ck[nm] = float(open(os.path.join(out_dir, nm)).read().split()[0])
+        ck[nm] = float(open(out_prefix + nm).read().split()[0])
     for nm in VECS:
-        ck[nm] = read_petsc_vecs(os.path.join(out_dir, "chkpt_" + nm))[0]
+        ck[nm] = read_petsc_vecs(out_prefix + "chkpt_" + nm)[0]
     return ck
 
 

@@ -32,9 +32,10 @@ class OdeStats(C.Structure):
 
 
 FIELDS = {"psi": 0, "slip": 1, "slipVel": 2, "tauP": 3, "tauQSP": 4, "strength": 5, "u": 6, "surfDisp": 7,
-          "sxy": 8, "dpsi": 9, "dslip": 10, "gVxy": 11, "gVxz": 12, "sxz": 13, "sdev": 14, "effVisc": 15}
-BODY_FIELDS = ("u", "sxy", "gVxy", "gVxz", "sxz", "sdev", "effVisc")
-LAWS = {"agingLaw": 0, "slipLaw": 1, "constantState": 2}
+          "sxy": 8, "dpsi": 9, "dslip": 10, "gVxy": 11, "gVxz": 12, "sxz": 13, "sdev": 14, "effVisc": 15,
+          "T": 16, "Vw": 17, "dT": 18}
+BODY_FIELDS = ("u", "sxy", "gVxy", "gVxz", "sxz", "sdev", "effVisc", "T", "dT")
+LAWS = {"agingLaw": 0, "slipLaw": 1, "constantState": 2, "flashHeating": 3}
 
 
 def declare(L):

@@ -10,6 +10,7 @@
 #include "cycle_host.hpp"
 #include "infile.hpp"
 #include "thermal.hpp"
+#include "thermal_dev.hpp"
 #include "qd.hpp"
 #include "sbp_solver.hpp"
 
@@ -352,6 +353,20 @@ scy_status scy_qd_get_field(scy_qd* q, int field, double* out) {
             : field == SCY_FIELD_SDEV ? c.sdev.as<double>()
                                       : c.effVisc.as<double>();
       break;
+    case SCY_FIELD_TEMPERATURE:
+    case SCY_FIELD_DTEMP:
+    case SCY_FIELD_VW:
+      if (!c.th || (field == SCY_FIELD_VW && c.fp.state_law != SCY_LAW_FLASH)) {
+        scy::set_error("field %d needs a thermal driver%s", field, field == SCY_FIELD_VW ? " with flash heating" : "");
+        return SCY_ERR_ARG;
+      }
+      if (field == SCY_FIELD_TEMPERATURE || field == SCY_FIELD_DTEMP) {
+        src = field == SCY_FIELD_TEMPERATURE ? c.th->T.as<double>() : c.th->dT.as<double>();
+        n = c.N;
+      } else {
+        src = c.th->Vw.as<double>();
+      }
+      break;
     case SCY_FIELD_SLIPVEL: src = c.slipVel.as<double>(); break;
     case SCY_FIELD_TAUP: src = c.tauP.as<double>(); break;
     case SCY_FIELD_TAUQSP: src = c.tauQSP.as<double>(); break;
@@ -412,6 +427,17 @@ scy_status scy_qd_create_from_in(const char* path, const scy_solve_opts* solve, 
     return st;
   }
   if (P->min_dt_user == -1.0) P->ode.min_dt = q->ctx.compute_min_dt(P->cs, P->desc.grid.Ly, P->desc.grid.Lz);
+  // the thermal driver: the heat equation on the device and the IMEX
+  // integrator (RK32_WBE / RK43_WBE)
+  q->ctx.imex = P->imex;
+  if (P->heat) {
+    q->ctx.th = std::make_shared<scy::ThermalContext>();
+    st = q->ctx.th->create(q->ctx, *P->heat);
+    if (st != SCY_OK) {
+      delete q;
+      return st;
+    }
+  }
   q->prob = std::move(P);
   *out = q;
   return SCY_OK;

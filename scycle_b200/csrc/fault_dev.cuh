@@ -20,12 +20,36 @@ struct FaultParams {
   const double *a, *b, *sN, *Dc, *eta, *locked, *prestress;
   double f0, v0, vL, root_tol;
   int max_its;
-  int state_law;  // 0 aging, 1 slip, 2 constant state
+  int state_law;  // 0 aging, 1 slip, 2 constant state, 3 flash heating
   int jacobian;   // 0 the reference's derivative expression, 1 the exact derivative
+  // flash heating (state law 3; the heat equation's fields on the fault):
+  // temperature Tf, rho c, k and the weakening temperature Tw per node, the
+  // weakening velocity written back to Vw
+  const double *Tf = nullptr, *rc_f = nullptr, *k_f = nullptr, *Tw = nullptr;
+  double* Vw = nullptr;
+  double fl_D = 5.0, fl_tau_c = 3.0, fl_fw = 0.64;
 };
 
 __device__ __forceinline__ double strength_psi(double sN, double psi, double V, double a, double v0) {
   return a * sN * asinh((0.5 * V / v0) * exp(psi / a));
+}
+
+// flashHeating_Vw (fault.cpp:2162-2168): the weakening velocity
+__device__ __forceinline__ double flash_heating_vw(double T, double rc, double k, double D, double Tw, double tau_c) {
+  const double ath = k / rc;
+  const double s = rc * (Tw - T) / tau_c;
+  return (M_PI * ath / D) * (s * s);
+}
+
+// flashHeating_psi (fault.cpp:2171-2196): the regularised steady-state
+// friction fLV, weakened to fw + (fLV - fw) Vw / |V| above Vw
+__device__ __forceinline__ double flash_heating_psi(double psi, double V, double Vw, double fw, double Dc, double a,
+                                                    double b, double f0, double v0) {
+  const double absV = fabs(V);
+  const double fLV = (a - b) * asinh(absV / v0 / 2.0 * exp(f0 / (a - b)));
+  const double fss = absV > Vw ? fw + (fLV - fw) * (Vw / absV) : fLV;
+  const double f = a * asinh((absV / 2. / v0) * exp(psi / a));
+  return -absV / Dc * (f - fss);
 }
 
 // Residual of tau_qs - eta V = strength(V) and its derivative.  E =

@@ -45,7 +45,12 @@ __device__ __forceinline__ void fault_node_update(int iz, double tau_body, const
     dpsi = aging_law_psi(psi, V, fp.b[iz], fp.f0, fp.v0, fp.Dc[iz]);
   else if (fp.state_law == 1)
     dpsi = slip_law_psi(psi, V, a, fp.b[iz], fp.f0, fp.v0, fp.Dc[iz]);
-  else
+  else if (fp.state_law == 3) {
+    // flashHeating_psi_Vec (fault.cpp:2199-2243): Vw from the fault's temperature
+    const double vw = flash_heating_vw(fp.Tf[iz], fp.rc_f[iz], fp.k_f[iz], fp.fl_D, fp.Tw[iz], fp.fl_tau_c);
+    fp.Vw[iz] = vw;
+    dpsi = flash_heating_psi(psi, V, vw, fp.fl_fw, fp.Dc[iz], a, fp.b[iz], fp.f0, fp.v0);
+  } else
     dpsi = 0.0;
   if (!isfinite(dpsi) || !isfinite(V)) atomicOr(flags, (unsigned)FAULT_NONFINITE);
   f[fp.psi_off + iz] = dpsi;

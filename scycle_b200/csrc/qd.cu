@@ -14,6 +14,7 @@
 #include "fault_node.cuh"
 #include "infile.hpp"
 #include "qd.hpp"
+#include "thermal_dev.hpp"
 
 namespace scy {
 
@@ -210,7 +211,7 @@ int QDContext::create(const scy_qd_desc& d, const scy_pl_desc* pld) {
     set_error("fault arrays a, b, sN, Dc, eta are required");
     return SCY_ERR_ARG;
   }
-  if (f.state_law < 0 || f.state_law > 2) {
+  if (f.state_law < 0 || f.state_law > 3) {
     set_error("unknown state law %d", f.state_law);
     return SCY_ERR_ARG;
   }
@@ -344,6 +345,10 @@ int qd_bc_launch(QDContext& q, double t, const double* var) {
 
 int QDContext::d_dt(double t, const double* var, double* f) {
   cudaStream_t s = sbp.stream;
+  if (fp.state_law == SCY_LAW_FLASH && !fp.Tf) {
+    set_error("the flash-heating law needs the heat equation's fault fields (a driver with thermalCoupling)");
+    return SCY_ERR_STATE;
+  }
   if (pl) {
     if (mode == SCY_QD_MODE_RESPONSE) {
       set_error("the fault-response mode does not apply to the power-law material");
@@ -770,7 +775,7 @@ int QDContext::integrate_steps(long nsteps, scy_ode_stats* st) {
       used_dt = deltaT;
       SCY_TRY(compute_error(lo, hi, &totErr));
       SCY_TRY(read_flags());
-      bool acc = ode.method == SCY_RK32 ? (totErr <= totTol) : (totErr < totTol);
+      bool acc = (ode.method == SCY_RK32 && !imex) ? (totErr <= totTol) : (totErr < totTol);
       if (forced) acc = forced_accept != 0;
       if (record) {
         log_dt.push_back(deltaT);
@@ -786,8 +791,13 @@ int QDContext::integrate_steps(long nsteps, scy_ode_stats* st) {
     if (record) log_step_dt.push_back(used_dt);
     currT = currT + deltaT;
     SCY_CUDA_TRY(cudaMemcpyAsync(var, hi, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    // the IMEX d_dt (strikeSlip_linearElastic_qd.cpp:800-870): coupled, the
+    // fault takes the heat equation's temperature first; after the rates,
+    // one backward-Euler heat step with the new slip velocity and tauP
+    if (th && th->coupled) SCY_TRY(th->set_fault_temperature());
     SCY_TRY(d_dt(currT, var, dvar));
     SCY_TRY(read_flags());
+    if (th) SCY_TRY(th->step(*this, deltaT));
     if (totErr != 0.0) newDeltaT = compute_step_size(totErr);
     errA[1] = errA[0];
     errA[0] = totErr;

@@ -33,6 +33,7 @@ constexpr double a61 = 647845179188. / 3216320057751., a62 = 73281519250. / 8382
 }  // namespace rk43
 
 struct QDProblem;
+struct ThermalContext;
 
 struct QDContext {
   SbpContext sbp;
@@ -124,6 +125,12 @@ struct QDContext {
   // Called after every accepted step (timeMonitor); a nonzero *stop ends
   // the phase (integrate_steps returns with phase_stopped = 1).
   std::function<int(int* stop)> monitor;
+  // RK32_WBE / RK43_WBE (odeSolverImex.cpp:352-470, :837-): a strict
+  // acceptance test, and after every accepted step the implicit heat step
+  // of th (thermal.cu); in coupled mode the fault's temperature is set from
+  // the heat equation's at the start of that step's last d_dt
+  int imex = 0;
+  std::shared_ptr<ThermalContext> th;
   int phase_stopped = 0;
   double compute_step_size(double totErr);
   int compute_error(const double* lo, const double* hi, double* err);

@@ -82,6 +82,7 @@ def test_checkpoint_files_and_restart_match_the_oracle(tmp_path):
     after the same six attempts (read with the oracle's PETSc reader), and a
     run restarted from those files matches the oracle restarted from them
     (reference restart semantics: step count and error history from zero)."""
+    import glob
     import shutil
 
     from oracle.checkpoint import read_checkpoint, restart_problem
@@ -98,8 +99,11 @@ def test_checkpoint_files_and_restart_match_the_oracle(tmp_path):
     assert st.done == 2 and st.step_count == 6
     att1 = run1.attempts()
     run1.close()
-    saved = str(tmp_path / "ckpt6")
-    shutil.copytree(out, saved)
+    # the run's checkpoint files (outputDir is a prefix) before the restart rewrites them
+    saved = str(tmp_path / "ckpt6") + "/ck_"
+    os.makedirs(os.path.dirname(saved))
+    for f in glob.glob(out + "*"):
+        shutil.copy(f, saved + os.path.basename(f)[len(os.path.basename(out)):])
     ck = read_checkpoint(saved)
     assert ck["ckptNumber"] == 2 and ck["chkpt_stepCount"] == 6
     ora = QDLinearElastic(P, keep_history=False)

@@ -19,7 +19,8 @@ does), and slip, slip velocity, state, shear stress and surface
 displacement are compared after the recorded steps, norm-wise relative
 (max |device - oracle| / max |oracle| per field).
 
-The bar is 1e-9, or ten times the oracle's own spread where that is larger:
+The bar is 1e-9, or ten times the oracle's own spread where that is larger
+(a hundred times for the slip velocity, see SPREAD_FACTOR):
 the fixture holds, per field and snapshot, how far the oracle moves when
 its refined solves are replaced by the plain direct solve (solutions that
 differ by rounding only).  The fault stress is a near-cancelling difference
@@ -59,6 +60,12 @@ def _nrel(a, b):
 
 
 FIELDS = ("slip", "slipVel", "psi", "tauP", "tauQSP", "surfDisp")
+# the slip velocity comes from the bracketed Newton, whose stopping test
+# (|residual| < rootTol, absolute) turns rounding-level stress differences
+# into discontinuous changes of V where the stress is tiny (the locked fault
+# of c0): its bar is a hundred times the oracle's spread sample
+SPREAD_FACTOR = {f: 10.0 for f in FIELDS}
+SPREAD_FACTOR["slipVel"] = 100.0
 
 
 def _check(view, fx, k, worst):
@@ -67,7 +74,7 @@ def _check(view, fx, k, worst):
     bar (1e-9 or ten times the oracle's spread)."""
     for f in FIELDS:
         e = _nrel(view.field(f), fx[f][k])
-        bar = max(REL, 10.0 * float(fx["spread_" + f][k]))
+        bar = max(REL, SPREAD_FACTOR[f] * float(fx["spread_" + f][k]))
         w = worst.setdefault(f, {"err": 0.0, "ratio": 0.0})
         w["err"] = max(w["err"], e)
         w["ratio"] = max(w["ratio"], e / bar)
