@@ -245,7 +245,7 @@ def run_batched(args, dist, rank, world, local):
            "sim_years_timed": sim_years, "stage_solves": evals, "instances": K * world, "setup_s": setup_s,
            "rounds": st1.rounds - st0.rounds, "redo_rounds": st1.redo_rounds - st0.redo_rounds,
            "cg_its": st1.cg_its, "groups": st1.groups, "gpu_launches": int(launches), "clocks": clk,
-           "precision": args.batch_precision}
+           "precision": args.batch_precision, "autotune": b.tuning(0)}
     # slip velocity against the plain FP64 single-instance path on instance 0's
     # own attempt sequence (the reported error of the batched form)
     if rank == 0:

@@ -626,6 +626,13 @@ enum { SCY_BATCH_KERNEL_YSOLVE = 0, SCY_BATCH_KERNEL_RESIDUAL = 1, SCY_BATCH_KER
 scy_status scy_batch_profile_collect(scy_batch* b, int kernel, double* ms, long long* launches, double* bytes);
 /* Drops the recorded launches. */
 scy_status scy_batch_profile_clear(scy_batch* b);
+/* The autotuner's choices for group g (no counterpart in the reference): at
+ * set-up every group times, on its own buffers, the CG operator kernel with
+ * 1, 2, 4 and 8 instances per block and the banded sweeps in three launch
+ * shapes (two chains per lane x two warps, one x four, four x one), and
+ * keeps the fastest.  kpb / sweep_variant get the choices, us (8 doubles,
+ * may be NULL) the timings in microseconds per launch (0 where not tried). */
+scy_status scy_batch_tuning(scy_batch* b, int g, int* kpb, int* sweep_variant, double* us);
 
 /* ---------------------------------------------------------------------------
  * Discrete adjoint of the linear-elastic quasi-dynamic RK32 integration.

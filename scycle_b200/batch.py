@@ -89,6 +89,17 @@ class Batch:
         S.check(S.lib().scy_batch_profile_collect(self.h, k, C.byref(ms), C.byref(nl), C.byref(by)))
         return ms.value, nl.value, by.value
 
+    def tuning(self, group=0):
+        """The autotuner's choices for a group: instances per block of the
+        operator kernels, the sweep launch shape and the timings (us)."""
+        kpb, var = C.c_int(), C.c_int()
+        us = (C.c_double * 8)()
+        S.check(S.lib().scy_batch_tuning(self.h, int(group), C.byref(kpb), C.byref(var), us))
+        return {"instances_per_block": kpb.value, "sweep_variant": ["2 chains x 2 warps", "1 chain x 4 warps",
+                                                                   "4 chains x 1 warp"][var.value],
+                "operator_us_by_kpb": {k: us[i] for i, k in enumerate((1, 2, 4, 8)) if us[i] > 0},
+                "sweep_us_by_variant": [us[4], us[5], us[6]]}
+
     def profile_clear(self):
         S.check(S.lib().scy_batch_profile_clear(self.h))
 

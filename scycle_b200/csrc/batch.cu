@@ -1007,9 +1007,17 @@ int BatchContext::setup_group(int base, int K) {
       SCY_TRY(ozk_set_host(g.zw2, vzt.data(), Nz, 0));
       SCY_TRY(ozk_prepare(S));
     }
-    SCY_CUDA_TRY(cudaFuncSetAttribute(b_ysolve_tma_kernel<double, YS_I, YS_W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    SCY_CUDA_TRY(cudaFuncSetAttribute(b_ysolve_tma_kernel<double, 2, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       ys_smem_bytes(8)));
-    SCY_CUDA_TRY(cudaFuncSetAttribute(b_ysolve_tma_kernel<float, YS_I, YS_W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    SCY_CUDA_TRY(cudaFuncSetAttribute(b_ysolve_tma_kernel<float, 2, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      ys_smem_bytes(4)));
+    SCY_CUDA_TRY(cudaFuncSetAttribute(b_ysolve_tma_kernel<double, 1, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      ys_smem_bytes(8)));
+    SCY_CUDA_TRY(cudaFuncSetAttribute(b_ysolve_tma_kernel<float, 1, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      ys_smem_bytes(4)));
+    SCY_CUDA_TRY(cudaFuncSetAttribute(b_ysolve_tma_kernel<double, 4, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      ys_smem_bytes(8)));
+    SCY_CUDA_TRY(cudaFuncSetAttribute(b_ysolve_tma_kernel<float, 4, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       ys_smem_bytes(4)));
   }
   SCY_TRY(g.tab.alloc(sizeof(BatchInst) * g.K));
@@ -1021,7 +1029,122 @@ int BatchContext::setup_group(int base, int K) {
   SCY_TRY(g.blas_ws.alloc(ws));
   SCY_BLAS_TRY(cublasSetWorkspace(g.blas, g.blas_ws.p, ws));
   SCY_BLAS_TRY(cublasSetMathMode(g.blas, CUBLAS_DEFAULT_MATH));
+  SCY_TRY(autotune(g));
   groups.push_back(std::move(G));
+  return SCY_OK;
+}
+
+// The banded sweeps in one of their launch shapes: variant 0 two chains per
+// lane and two warps per block, 1 one chain and four warps, 2 four chains
+// and one warp (a block serves eight instances in each)
+int BatchContext::launch_ysolve(BatchGroup& g, int variant) {
+  FDPrecond& F = *g.fd;
+  const int Ny = g.Ny, Nz = g.Nz, K = g.K;
+  const dim3 grid((Nz + YS_C - 1) / YS_C, (K + YS_B - 1) / YS_B);
+  const bool f32 = precision != SCY_PREC_FP64;
+  const int sm = ys_smem_bytes(f32 ? 4 : 8);
+#define SCY_YS_LAUNCH(I, W)                                                                                       \
+  do {                                                                                                              \
+    if (f32)                                                                                                        \
+      b_ysolve_tma_kernel<float, I, W><<<grid, 32 * W, sm, g.stream>>>(g.mLcol32, g.mLrow32, g.mT32,               \
+                                                                       g.t1pf.as<float>(), Ny, Nz, F.Nzp, K,        \
+                                                                       g.w.status);                                 \
+    else                                                                                                            \
+      b_ysolve_tma_kernel<double, I, W><<<grid, 32 * W, sm, g.stream>>>(g.mLcol, g.mLrow, g.mT, g.t1p.as<double>(), \
+                                                                        Ny, Nz, F.Nzp, K, g.w.status);              \
+  } while (0)
+  static_assert(2 * 2 * 2 == YS_B && 2 * 4 * 1 == YS_B && 2 * 1 * 4 == YS_B, "sweep variants serve YS_B instances");
+  if (variant == 1)
+    SCY_YS_LAUNCH(1, 4);
+  else if (variant == 2)
+    SCY_YS_LAUNCH(4, 1);
+  else
+    SCY_YS_LAUNCH(2, 2);
+#undef SCY_YS_LAUNCH
+  SCY_LAUNCH_CHECK();
+  return SCY_OK;
+}
+
+// Times, on the group's own buffers (their contents do not matter here),
+// the CG operator kernel with 1, 2, 4 and 8 instances per block and the
+// banded sweeps in their three launch shapes; keeps the fastest of each.
+// The sweep's status words are cleared afterwards.
+int BatchContext::autotune(BatchGroup& g) {
+  DevBuf ones;
+  SCY_TRY(ones.alloc((size_t)g.K * sizeof(int)));
+  std::vector<int> h(g.K, 1);
+  SCY_CUDA_TRY(cudaMemcpy(ones.p, h.data(), h.size() * sizeof(int), cudaMemcpyHostToDevice));
+  const int* mask = ones.as<int>();
+  cudaEvent_t e0, e1;
+  SCY_CUDA_TRY(cudaEventCreate(&e0));
+  SCY_CUDA_TRY(cudaEventCreate(&e1));
+  auto timed = [&](auto&& launch, double* us) -> int {
+    SCY_TRY(launch());  // warm-up
+    SCY_CUDA_TRY(cudaEventRecord(e0, g.stream));
+    for (int r = 0; r < 3; ++r) SCY_TRY(launch());
+    SCY_CUDA_TRY(cudaEventRecord(e1, g.stream));
+    SCY_CUDA_TRY(cudaEventSynchronize(e1));
+    float ms = 0.0f;
+    SCY_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+    *us = ms * 1e3 / 3.0;
+    return SCY_OK;
+  };
+  const BatchInst* tab = g.tab.as<BatchInst>();
+  const double* C = g.planes.as<double>();
+  const int mixed = precision != SCY_PREC_FP64 ? 1 : 0;
+  int best = g.kpb;
+  double best_us = 1e300;
+  const int cands[4] = {1, 2, 4, 8};
+  for (int c = 0; c < 4; ++c) {
+    const int kpb = cands[c];
+    if (kpb > XKPB || (kpb > 1 && kpb > g.K)) continue;
+    const dim3 tg((g.Nz + XTZ - 1) / XTZ, (g.Ny + XTY - 1) / XTY, (g.K + kpb - 1) / kpb);
+    double us = 0.0;
+    int rc = timed(
+        [&]() -> int {
+          if (mixed)
+            b_cross_kernel<1, float><<<tg, XT, xs_smem_bytes(1, 4), g.stream>>>(C, g.Ny, g.Nz, tab, mask, g.w, g.w.z32,
+                                                                                1, 0, mixed, kpb, 1);
+          else
+            b_cross_kernel<1, double><<<tg, XT, xs_smem_bytes(1, 8), g.stream>>>(C, g.Ny, g.Nz, tab, mask, g.w, g.w.z,
+                                                                                 1, 0, mixed, kpb, 1);
+          SCY_LAUNCH_CHECK();
+          return SCY_OK;
+        },
+        &us);
+    if (rc != SCY_OK) {
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      return rc;
+    }
+    g.tune_us[c] = us;
+    if (us < best_us) {
+      best_us = us;
+      best = kpb;
+    }
+  }
+  g.kpb = best;
+  if (g.fd->ybanded && !fd_dense) {
+    double best_ys = 1e300;
+    for (int v = 0; v < 3; ++v) {
+      double us = 0.0;
+      int rc = timed([&]() -> int { return launch_ysolve(g, v); }, &us);
+      if (rc != SCY_OK) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        return rc;
+      }
+      g.tune_us[4 + v] = us;
+      if (us < best_ys) {
+        best_ys = us;
+        g.ys_variant = v;
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  SCY_CUDA_TRY(cudaStreamSynchronize(g.stream));
+  SCY_CUDA_TRY(cudaMemset(g.status.p, 0, (size_t)g.K * 4));
   return SCY_OK;
 }
 
@@ -1100,10 +1223,7 @@ int BatchContext::fd_apply(BatchGroup& g) {
       SCY_TRY(ozk_gemm(g.zx, g.zw1, t1, F.Nzp, Nz, g.stream, g.w.status, Ny, 4u));
       SCY_TRY(prof_end(g.stream, pa, PROF_ZTRANSFORM, gemm_b));
       SCY_TRY(prof_begin(g.stream, &pa));
-      b_ysolve_tma_kernel<float, YS_I, YS_W><<<dim3((Nz + YS_C - 1) / YS_C, (K + YS_B - 1) / YS_B), 32 * YS_W,
-                                               ys_smem_bytes(4), g.stream>>>(g.mLcol32, g.mLrow32, g.mT32, t1, Ny,
-                                                                             Nz, F.Nzp, K, g.w.status);
-      SCY_LAUNCH_CHECK();
+      SCY_TRY(launch_ysolve(g, g.ys_variant));
       SCY_TRY(prof_end(g.stream, pa, PROF_YSOLVE, 4.0 * (9.0 * Ny * Nz + 4.0 * N * K)));
       SCY_TRY(prof_begin(g.stream, &pa));
       SCY_TRY(ozk_split(g.zx, (const float*)t1, F.Nzp, g.stream));
@@ -1120,10 +1240,7 @@ int BatchContext::fd_apply(BatchGroup& g) {
       SCY_TRY(ozk_gemm(g.zx, g.zw1, t1, F.Nzp, Nz, g.stream, g.w.status, Ny, 4u));
       SCY_TRY(prof_end(g.stream, pa, PROF_ZTRANSFORM, gemm_b));
       SCY_TRY(prof_begin(g.stream, &pa));
-      b_ysolve_tma_kernel<double, YS_I, YS_W><<<dim3((Nz + YS_C - 1) / YS_C, (K + YS_B - 1) / YS_B), 32 * YS_W,
-                                                ys_smem_bytes(8), g.stream>>>(g.mLcol, g.mLrow, g.mT, t1, Ny, Nz,
-                                                                              F.Nzp, K, g.w.status);
-      SCY_LAUNCH_CHECK();
+      SCY_TRY(launch_ysolve(g, g.ys_variant));
       SCY_TRY(prof_end(g.stream, pa, PROF_YSOLVE, 8.0 * (9.0 * Ny * Nz + 4.0 * N * K)));
       SCY_TRY(prof_begin(g.stream, &pa));
       SCY_TRY(ozk_split(g.zx, (const double*)t1, F.Nzp, g.stream));
@@ -1653,6 +1770,16 @@ scy_status scy_batch_profile(scy_batch* b, int on) {
 scy_status scy_batch_profile_collect(scy_batch* b, int kernel, double* ms, long long* launches, double* bytes) {
   if (!b || !ms || !launches || !bytes || kernel < 0 || kernel > 4) return SCY_ERR_ARG;
   SCY_TRY(b->ctx.prof_collect(kernel, ms, launches, bytes));
+  return SCY_OK;
+}
+
+scy_status scy_batch_tuning(scy_batch* b, int g, int* kpb, int* sweep_variant, double* us) {
+  if (!b || g < 0 || g >= (int)b->ctx.groups.size()) return SCY_ERR_ARG;
+  const scy::BatchGroup& G = *b->ctx.groups[g];
+  if (kpb) *kpb = G.kpb;
+  if (sweep_variant) *sweep_variant = G.ys_variant;
+  if (us)
+    for (int i = 0; i < 8; ++i) us[i] = G.tune_us[i];
   return SCY_OK;
 }
 

@@ -69,7 +69,9 @@ struct BatchGroup {
   DevBuf t1p, t1pf;  // the z transform, rows padded to the factor tables' Nzp (FP64, FP32)
   CUtensorMap mLcol, mLrow, mT, mLcol32, mLrow32, mT32;  // tile maps of the TMA-fed banded sweeps
   DevBuf planes;  // the operator's 33 cross-stencil coefficient planes (build_cross_planes)
-  int kpb = 1;    // instances per block of the operator kernels
+  int kpb = 1;    // instances per block of the operator kernels (autotuned at set-up)
+  int ys_variant = 0;  // chains per lane x warps per block of the banded sweeps (autotuned)
+  double tune_us[8] = {0};  // the autotuner's timings: kpb 1, 2, 4, 8, sweep variants 0, 1, 2
   DevBuf vec[7], vecf[4], sc, partials, counters, status;
   BatchWork w{};
   cudaStream_t stream = nullptr;
@@ -153,6 +155,10 @@ struct BatchContext {
  private:
   QDContext& q(int i) const;
   int setup_group(int base, int K);
+  // the autotuner: times the candidate launch shapes of the group's main
+  // kernels on its own buffers and keeps the fastest
+  int autotune(BatchGroup& g);
+  int launch_ysolve(BatchGroup& g, int variant);
   // phases: 1 = copy + rates at accepted states, 2 = an attempt (graphs keyed by its and phases)
   int enqueue_round(int its_now, int phases);
   int launch_round(int its_now, int phases);
