@@ -964,6 +964,27 @@ def oracle_on_all_cores(kind, steps, n=401, max_workers=None):
             "sim_years_per_hour": sum((r[2] / YEAR) / (r[1] / 3600.0) for r in res)}
 
 
+def run_ztransform_only(args):
+    """The tensor-core z transform alone at the batched ensemble's shape
+    (32 instances of 401 x 401: 12832 z-lines of 401 values times a 401 x 401
+    weight matrix) with the given number of digit planes, for profiling."""
+    import torch
+    from scycle_b200 import build
+    build.build(verbose=False)
+    from scycle_b200 import _lib as S
+    rows, K = 32 * 401, 401
+    x = torch.randn(rows, K, dtype=torch.float64, device="cuda")
+    w = np.ascontiguousarray(np.random.default_rng(0).standard_normal((K, K)))
+    d = torch.empty(rows, K, dtype=torch.float64, device="cuda")
+    L = S.lib()
+    for _ in range(args.profile_reps):
+        S.check(L.scy_ozaki_matmul(C.c_void_p(x.data_ptr()), K, rows, K, S.as_dptr(w), K, K, args.profile_ztransform,
+                                   C.c_void_p(d.data_ptr()), K))
+    torch.cuda.synchronize()
+    print(json.dumps({"ztransform_only": True, "rows": rows, "K": K, "planes": args.profile_ztransform,
+                      "reps": args.profile_reps}))
+
+
 def cpu_baseline(args):
     """The oracle on a bounded sample of the headline workload, on all host
     cores (one single-threaded instance per core)."""
@@ -1034,6 +1055,8 @@ def main():
     ap.add_argument("--profile-wave", type=int, default=0,
                     help="run the cycle workload on an n x n grid into a wave phase, time its two launches, exit")
     ap.add_argument("--profile-reps", type=int, default=20)
+    ap.add_argument("--profile-ztransform", type=int, default=0,
+                    help="run only the tensor-core z transform with this many digit planes (for ncu) and exit")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
@@ -1042,6 +1065,9 @@ def main():
         return
     if args.profile_wave:
         run_wave_only(args)
+        return
+    if args.profile_ztransform:
+        run_ztransform_only(args)
         return
     dist, rank, world, local = _dist()
     try:

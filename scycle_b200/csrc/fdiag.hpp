@@ -47,7 +47,7 @@ struct FDPrecond {
   // TMA-fed sweeps of the batched ensemble (one instance) on the padded
   // transform t1p (Ny rows of Nzp values); no library GEMM.  A sweep wait
   // that runs out sets ys_status (the CG convergence test then fails).
-  static constexpr int kPlanes64 = 5, kPlanes32 = 4;  // digit planes of apply / apply32
+  static constexpr int kPlanes64 = 7, kPlanes32 = 4;  // digit planes of apply (FP64-accurate) / apply32
   OzkOperand zx64, zx32, zw1_64, zw2_64, zw1_32, zw2_32;
   DevBuf t1p, t1pf, ys_status;
   CUtensorMap mLcol, mLrow, mT, mLcol32, mLrow32, mT32;
