@@ -109,8 +109,8 @@ def build_pl_problem(text, input_dir=None):
 class PowerLawQD(QDLinearElastic):
     """StrikeSlip_PowerLaw_qd with dislocation creep."""
 
-    def __init__(self, P, keep_history=True):
-        super().__init__(P, keep_history)
+    def __init__(self, P, keep_history=True, refine=0):
+        super().__init__(P, keep_history, refine)
         self.N = self.Ny * self.Nz
         self.min_dt = P["driver"]["minDeltaT"]
         self.mu = np.asarray(P["mu"], float)
@@ -263,7 +263,7 @@ class PowerLawQD(QDLinearElastic):
                          bcs=("Dirichlet", "Neumann", "Neumann", "Neumann"))
             rhs = sbp.set_rhs(bcL, bcR, self.bcT, self.bcB)
             # updateSSa (:2099-2137)
-            v = spla.splu(sbp.A.tocsc()).solve(rhs)
+            v = self._refined(sbp.A, spla.splu(sbp.A.tocsc()), rhs)
             gxy_t = sbp.Dy_Iz @ v
             gxz_t = sbp.Iy_Dz @ v
             sxy = eff * gxy_t
