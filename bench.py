@@ -986,10 +986,10 @@ def run_ztransform_only(args):
     L = S.lib()
     for _ in range(args.profile_reps):
         S.check(L.scy_ozaki_matmul(C.c_void_p(x.data_ptr()), K, rows, K, S.as_dptr(w), K, K, args.profile_ztransform,
-                                   C.c_void_p(d.data_ptr()), K))
+                                   C.c_void_p(d.data_ptr()), K, args.profile_ctas, args.profile_bf16))
     torch.cuda.synchronize()
     print(json.dumps({"ztransform_only": True, "rows": rows, "K": K, "planes": args.profile_ztransform,
-                      "reps": args.profile_reps}))
+                      "ctas_per_sm": args.profile_ctas, "bf16_digits": args.profile_bf16, "reps": args.profile_reps}))
 
 
 def cpu_baseline(args):
@@ -1063,6 +1063,10 @@ def main():
     ap.add_argument("--profile-wave", type=int, default=0,
                     help="run the cycle workload on an n x n grid into a wave phase, time its two launches, exit")
     ap.add_argument("--profile-reps", type=int, default=20)
+    ap.add_argument("--profile-bf16", type=int, default=0, choices=[0, 1],
+                    help="digits in bf16 (kind::f16) instead of 8-bit integers in --profile-ztransform")
+    ap.add_argument("--profile-ctas", type=int, default=1, choices=[1, 2],
+                    help="CTAs per SM of the z-transform product in --profile-ztransform (2: S <= 5)")
     ap.add_argument("--profile-ztransform", type=int, default=0,
                     help="run only the tensor-core z transform with this many digit planes (for ncu) and exit")
     args = ap.parse_args()

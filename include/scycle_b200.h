@@ -178,11 +178,16 @@ scy_status scy_sbp_solve_noalloc(scy_sbp* s, const double* rhs, double* u,
  * the S(S+1)/2 digit products accumulated exactly in 32-bit integers
  * (tcgen05.mma kind::i8) and combined in FP64; relative error per row about
  * 100^-S.  X and D are device arrays (row strides ldx, ldd), W a host array
- * (row stride ldw), K <= 1024.  No counterpart in the reference: it is the
- * z transform of the fast-diagonalisation preconditioner that stands in for
+ * (row stride ldw), K <= 1024.  ctas_per_sm: 1, or 2 for S <= 5 (narrower
+ * column tiles, one CTA's epilogue overlapping the other's products; the
+ * same result).  bf16_digits = 1 holds the same digits in bf16 and
+ * multiplies them with FP32 accumulation (tcgen05.mma kind::f16), exact and
+ * so bit-identical while S * 64 * 64 * K' < 2^24 (K' = K rounded up to 32;
+ * SCY_ERR_ARG beyond).  No counterpart in the reference: it is the z
+ * transform of the fast-diagonalisation preconditioner that stands in for
  * the reference's direct solve, exported so it can be checked on its own. */
 scy_status scy_ozaki_matmul(const double* X, long ldx, int rows, int K, const double* W, long ldw, int cols, int S,
-                            double* D, long ldd);
+                            double* D, long ldd, int ctas_per_sm, int bf16_digits);
 
 /* Grid facts for callers (levels of the multigrid hierarchy, sizes). */
 scy_status scy_sbp_info(scy_sbp* s, int* Ny, int* Nz, int* n_levels);
@@ -377,6 +382,20 @@ scy_status scy_qd_set_mode(scy_qd* q, int mode);
  * exact derivative (see scy_fault_desc.exact_jacobian).  Drivers made by
  * scy_qd_create_from_in start with the exact derivative. */
 scy_status scy_qd_set_jacobian(scy_qd* q, int exact);
+
+/* The power-law steady-state initial guess (guessSteadyStateICs = 1, run by
+ * scy_qd_integrate_begin_from_in; StrikeSlip_PowerLaw_qd::solveSS,
+ * strikeSlip_powerLaw_qd.cpp:922-955): effective-viscosity iterations, the
+ * last relative change of the viscosity (computeNormDiff_L2_scaleL2) and
+ * the conjugate-gradient iterations of all its elliptic solves.  Zeros when
+ * no guess was made.  Any pointer may be NULL. */
+scy_status scy_qd_steady_state_info(scy_qd* q, int* ss_its, double* ss_err, long* cg_its);
+/* Per effective-viscosity iteration of that guess, five doubles: defect-
+ * correction steps of its solve, relative residual ||rhs - A v|| / ||rhs||
+ * (double-double) before and after them, CG iterations, relative change of
+ * the viscosity.  *n gets the number of iterations; at most cap records are
+ * written to out (may be NULL). */
+scy_status scy_qd_steady_state_trace(scy_qd* q, double* out, long cap, long* n);
 
 /* Overwrites the integrated state [psi | slip] (host, 2*Nz) between steps.
  * recompute = 1 re-evaluates the rates from it (one d_dt); recompute = 0
@@ -628,11 +647,16 @@ scy_status scy_batch_profile_collect(scy_batch* b, int kernel, double* ms, long 
 scy_status scy_batch_profile_clear(scy_batch* b);
 /* The autotuner's choices for group g (no counterpart in the reference): at
  * set-up every group times, on its own buffers, the CG operator kernel with
- * 1, 2, 4 and 8 instances per block and the banded sweeps in three launch
- * shapes (two chains per lane x two warps, one x four, four x one), and
- * keeps the fastest.  kpb / sweep_variant get the choices, us (8 doubles,
- * may be NULL) the timings in microseconds per launch (0 where not tried). */
-scy_status scy_batch_tuning(scy_batch* b, int g, int* kpb, int* sweep_variant, double* us);
+ * 1, 2, 4 and 8 instances per block, the banded sweeps in three launch
+ * shapes (two chains per lane x two warps, one x four, four x one) and the
+ * z-transform product with one or two CTAs per SM and 8-bit or bf16 digits
+ * (identical results), and keeps the fastest.  kpb / sweep_variant /
+ * ztransform get the choices (ztransform bit 0: two CTAs per SM, bit 1:
+ * bf16 digits), us (12 doubles, may be NULL) the timings in microseconds per
+ * launch (kpb 1, 2, 4, 8; sweeps 0, 1, 2; unused; product with 8-bit
+ * digits, one and two CTAs per SM; with bf16 digits, one and two CTAs per
+ * SM; 0 where not tried). */
+scy_status scy_batch_tuning(scy_batch* b, int g, int* kpb, int* sweep_variant, int* ztransform, double* us);
 
 /* ---------------------------------------------------------------------------
  * Discrete adjoint of the linear-elastic quasi-dynamic RK32 integration.

@@ -249,6 +249,7 @@ class PowerLawQD(QDLinearElastic):
         d = self.P["domain"]
         grid = d["gridSpacingType"]
         err, it = 1e10, 0
+        trace = []  # the relative change of every iteration
         v = np.zeros(N)
         sxy = np.zeros(N)
         sxz = np.zeros(N)
@@ -276,8 +277,9 @@ class PowerLawQD(QDLinearElastic):
             eff = np.power(10.0, (1.0 - fss) * np.log10(old) + fss * np.log10(new))
             # computeNormDiff_L2_scaleL2 (genFuncs.cpp:221-238)
             err = np.linalg.norm(eff - old) / np.linalg.norm(old)
+            trace.append(err)
             it += 1
-        self.ss_its, self.ss_err = it, err
+        self.ss_its, self.ss_err, self.ss_trace = it, err, trace
         self.effVisc = eff
         self.sxy, self.sxz = sxy, sxz
         self.sdev = np.sqrt(np.abs(sxy * sxy + sxz * sxz))

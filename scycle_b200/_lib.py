@@ -72,7 +72,7 @@ def lib():
         L.scy_grid_host_apply.argtypes = [C.POINTER(GridDesc), dptr, dptr]
         L.scy_grid_host_apply_cross.argtypes = [C.POINTER(GridDesc), dptr, dptr]
         L.scy_ozaki_matmul.argtypes = [vp, C.c_long, C.c_int, C.c_int, dptr, C.c_long, C.c_int, C.c_int, vp,
-                                       C.c_long]
+                                       C.c_long, C.c_int, C.c_int]
         L.scy_launch_count.restype = C.c_longlong
         L.scy_profile_enable.argtypes = [C.c_int]
         L.scy_profile_collect.argtypes = [C.c_int, C.c_int, dptr, C.POINTER(C.c_longlong), dptr]

@@ -58,6 +58,8 @@ def declare(L):
     L.scy_qd_integrate_begin_from_in.argtypes = [vp]
     L.scy_qd_set_state.argtypes = [vp, dptr, C.c_int]
     L.scy_qd_set_jacobian.argtypes = [vp, C.c_int]
+    L.scy_qd_steady_state_info.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_long)]
+    L.scy_qd_steady_state_trace.argtypes = [vp, dptr, C.c_long, C.POINTER(C.c_long)]
     L.scy_qd_set_mode.argtypes = [vp, C.c_int]
     L.scy_pl_create.argtypes = [C.POINTER(QDDesc), vp, C.POINTER(vp)]
     L.scy_qd_state_size.argtypes = [vp, C.POINTER(C.c_long)]
@@ -126,7 +128,8 @@ class BatchStats(C.Structure):
 
 
 def declare_batch(L):
-    L.scy_batch_tuning.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double)]
+    L.scy_batch_tuning.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                   C.POINTER(C.c_double)]
     vp = C.c_void_p
     L.scy_batch_create_from_in.argtypes = [C.c_int, C.POINTER(C.c_char_p), C.POINTER(S.SolveOpts),
                                            C.POINTER(BatchOpts), C.POINTER(vp)]

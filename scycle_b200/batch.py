@@ -92,13 +92,17 @@ class Batch:
     def tuning(self, group=0):
         """The autotuner's choices for a group: instances per block of the
         operator kernels, the sweep launch shape and the timings (us)."""
-        kpb, var = C.c_int(), C.c_int()
-        us = (C.c_double * 8)()
-        S.check(S.lib().scy_batch_tuning(self.h, int(group), C.byref(kpb), C.byref(var), us))
+        kpb, var, zt = C.c_int(), C.c_int(), C.c_int()
+        us = (C.c_double * 12)()
+        S.check(S.lib().scy_batch_tuning(self.h, int(group), C.byref(kpb), C.byref(var), C.byref(zt), us))
         return {"instances_per_block": kpb.value, "sweep_variant": ["2 chains x 2 warps", "1 chain x 4 warps",
                                                                    "4 chains x 1 warp"][var.value],
+                "ztransform_ctas_per_sm": 2 if zt.value & 1 else 1,
+                "ztransform_digits": "bf16 (kind::f16)" if zt.value & 2 else "int8 (kind::i8)",
                 "operator_us_by_kpb": {k: us[i] for i, k in enumerate((1, 2, 4, 8)) if us[i] > 0},
-                "sweep_us_by_variant": [us[4], us[5], us[6]]}
+                "sweep_us_by_variant": [us[4], us[5], us[6]],
+                "ztransform_us_int8_by_ctas_per_sm": {1: us[8], 2: us[9]},
+                "ztransform_us_bf16_by_ctas_per_sm": {1: us[10], 2: us[11]}}
 
     def profile_clear(self):
         S.check(S.lib().scy_batch_profile_clear(self.h))

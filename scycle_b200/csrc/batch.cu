@@ -997,14 +997,21 @@ int BatchContext::setup_group(int base, int K) {
     {
       const int S = zt_planes, Nz = g.Nz;
       SCY_TRY(g.zx.alloc(S, (int)rowsT, Nz, 128));
-      SCY_TRY(g.zw1.alloc(S, Nz, Nz, ozk_cols_per_tile(S)));
-      SCY_TRY(g.zw2.alloc(S, Nz, Nz, ozk_cols_per_tile(S)));
+      SCY_TRY(g.zw1.alloc_weights(S, Nz, Nz));
+      SCY_TRY(g.zw2.alloc_weights(S, Nz, Nz));
       std::vector<double> vz((size_t)Nz * Nz), vzt((size_t)Nz * Nz);
       SCY_CUDA_TRY(cudaMemcpy(vz.data(), g.fd->Vz.p, vz.size() * 8, cudaMemcpyDeviceToHost));
       for (int k = 0; k < Nz; ++k)
         for (int m = 0; m < Nz; ++m) vzt[(size_t)k * Nz + m] = vz[(size_t)m * Nz + k];
       SCY_TRY(ozk_set_host(g.zw1, vz.data(), Nz, 0));
       SCY_TRY(ozk_set_host(g.zw2, vzt.data(), Nz, 0));
+      if (ozk_bf16_exact(S, Nz)) {
+        SCY_TRY(g.zx16.alloc(S, (int)rowsT, Nz, 128, 2));
+        SCY_TRY(g.zw1_16.alloc_weights(S, Nz, Nz, 2));
+        SCY_TRY(g.zw2_16.alloc_weights(S, Nz, Nz, 2));
+        SCY_TRY(ozk_set_host(g.zw1_16, vz.data(), Nz, 0));
+        SCY_TRY(ozk_set_host(g.zw2_16, vzt.data(), Nz, 0));
+      }
       SCY_TRY(ozk_prepare(S));
     }
     SCY_CUDA_TRY(cudaFuncSetAttribute(b_ysolve_tma_kernel<double, 2, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1140,6 +1147,47 @@ int BatchContext::autotune(BatchGroup& g) {
         g.ys_variant = v;
       }
     }
+    // the forward z-transform product in both shapes and both digit
+    // formats (identical results)
+    {
+      double zbest = 1e300;
+      for (int bf = 0; bf < 2; ++bf) {
+        if (bf && !g.zx16.dig.p) continue;
+        for (int pr = 0; pr < 2; ++pr) {
+          if (pr && ozk_cols_per_tile_pair(zt_planes) == 0) continue;
+          const OzkOperand& X = bf ? g.zx16 : g.zx;
+          const OzkOperand& W = bf ? g.zw1_16 : g.zw1;
+          double us = 0.0;
+          int rc = timed(
+              [&]() -> int {
+                if (precision != SCY_PREC_FP64)
+                  return ozk_gemm(X, W, g.t1pf.as<float>(), g.fd->Nzp, g.Nz, g.stream, nullptr, g.Ny, 4u, pr);
+                return ozk_gemm(X, W, g.t1p.as<double>(), g.fd->Nzp, g.Nz, g.stream, nullptr, g.Ny, 4u, pr);
+              },
+              &us);
+          if (rc != SCY_OK) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            return rc;
+          }
+          g.tune_us[8 + 2 * bf + pr] = us;
+          if (us < zbest) {
+            zbest = us;
+            g.zt_pair = pr;
+            g.zt_bf16 = bf;
+          }
+        }
+      }
+      if (g.zt_bf16) {
+        g.zx = std::move(g.zx16);
+        g.zw1 = std::move(g.zw1_16);
+        g.zw2 = std::move(g.zw2_16);
+      } else {
+        g.zx16 = OzkOperand();
+        g.zw1_16 = OzkOperand();
+        g.zw2_16 = OzkOperand();
+      }
+    }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -1220,7 +1268,7 @@ int BatchContext::fd_apply(BatchGroup& g) {
       SCY_TRY(ozk_split(g.zx, g.w.r, Nz, g.stream));
       SCY_TRY(prof_end(g.stream, pa, PROF_ZSPLIT, split_b));
       SCY_TRY(prof_begin(g.stream, &pa));
-      SCY_TRY(ozk_gemm(g.zx, g.zw1, t1, F.Nzp, Nz, g.stream, g.w.status, Ny, 4u));
+      SCY_TRY(ozk_gemm(g.zx, g.zw1, t1, F.Nzp, Nz, g.stream, g.w.status, Ny, 4u, g.zt_pair));
       SCY_TRY(prof_end(g.stream, pa, PROF_ZTRANSFORM, gemm_b));
       SCY_TRY(prof_begin(g.stream, &pa));
       SCY_TRY(launch_ysolve(g, g.ys_variant));
@@ -1229,7 +1277,7 @@ int BatchContext::fd_apply(BatchGroup& g) {
       SCY_TRY(ozk_split(g.zx, (const float*)t1, F.Nzp, g.stream));
       SCY_TRY(prof_end(g.stream, pa, PROF_ZSPLIT, split_b));
       SCY_TRY(prof_begin(g.stream, &pa));
-      SCY_TRY(ozk_gemm(g.zx, g.zw2, g.w.z32, Nz, Nz, g.stream, g.w.status, Ny, 4u));
+      SCY_TRY(ozk_gemm(g.zx, g.zw2, g.w.z32, Nz, Nz, g.stream, g.w.status, Ny, 4u, g.zt_pair));
       SCY_TRY(prof_end(g.stream, pa, PROF_ZTRANSFORM, gemm_b));
     } else {
       double* t1 = g.t1p.as<double>();
@@ -1237,7 +1285,7 @@ int BatchContext::fd_apply(BatchGroup& g) {
       SCY_TRY(ozk_split(g.zx, g.w.r, Nz, g.stream));
       SCY_TRY(prof_end(g.stream, pa, PROF_ZSPLIT, split_b));
       SCY_TRY(prof_begin(g.stream, &pa));
-      SCY_TRY(ozk_gemm(g.zx, g.zw1, t1, F.Nzp, Nz, g.stream, g.w.status, Ny, 4u));
+      SCY_TRY(ozk_gemm(g.zx, g.zw1, t1, F.Nzp, Nz, g.stream, g.w.status, Ny, 4u, g.zt_pair));
       SCY_TRY(prof_end(g.stream, pa, PROF_ZTRANSFORM, gemm_b));
       SCY_TRY(prof_begin(g.stream, &pa));
       SCY_TRY(launch_ysolve(g, g.ys_variant));
@@ -1246,7 +1294,7 @@ int BatchContext::fd_apply(BatchGroup& g) {
       SCY_TRY(ozk_split(g.zx, (const double*)t1, F.Nzp, g.stream));
       SCY_TRY(prof_end(g.stream, pa, PROF_ZSPLIT, split_b));
       SCY_TRY(prof_begin(g.stream, &pa));
-      SCY_TRY(ozk_gemm(g.zx, g.zw2, g.w.z, Nz, Nz, g.stream, g.w.status, Ny, 4u));
+      SCY_TRY(ozk_gemm(g.zx, g.zw2, g.w.z, Nz, Nz, g.stream, g.w.status, Ny, 4u, g.zt_pair));
       SCY_TRY(prof_end(g.stream, pa, PROF_ZTRANSFORM, gemm_b));
     }
     return SCY_OK;
@@ -1297,11 +1345,13 @@ int BatchContext::solve(BatchGroup& g, const int* mask, int its_now) {
   // algorithmic bytes: the coefficient planes once, per node and active
   // instance the operand, rhs and result (residual) or z, p_old, p and q
   const double nact = (double)active_in(g, mask);
+  const double coef_b = 33.0 * 8 * g.N;
   cudaEvent_t pa;
   SCY_TRY(prof_begin(g.stream, &pa));
-  b_cross_kernel<0, double><<<tg, XT, xs_smem_bytes(0, 8), g.stream>>>(C, g.Ny, g.Nz, tab, mask, g.w, nullptr, 0, 0, mixed, g.kpb);
+  b_cross_kernel<0, double><<<tg, XT, xs_smem_bytes(0, 8), g.stream>>>(C, g.Ny, g.Nz, tab, mask, g.w, nullptr, 0, 0,
+                                                                       mixed, g.kpb);
   SCY_LAUNCH_CHECK();
-  SCY_TRY(prof_end(g.stream, pa, PROF_RESIDUAL, 33.0 * 8 * g.N + nact * g.N * (24.0 + (mixed ? 4 : 0))));
+  SCY_TRY(prof_end(g.stream, pa, PROF_RESIDUAL, coef_b + nact * g.N * (24.0 + (mixed ? 4 : 0))));
   b_partials_kernel<<<g.K, 256, 0, g.stream>>>(mask, g.w, ntiles, 5);
   SCY_LAUNCH_CHECK();
   int pi = 0;
@@ -1327,7 +1377,7 @@ int BatchContext::solve(BatchGroup& g, const int* mask, int its_now) {
     SCY_LAUNCH_CHECK();
     // z, q, p when stored, and r (first iteration) or p_old (later ones)
     SCY_TRY(prof_end(g.stream, pa, PROF_MATVEC,
-                     33.0 * 8 * g.N + nact * g.N * ((mixed ? 4.0 : 8.0) + 8.0 + (store_p ? 8.0 : 0.0) + 8.0)));
+                     coef_b + nact * g.N * ((mixed ? 4.0 : 8.0) + 8.0 + (store_p ? 8.0 : 0.0) + 8.0)));
     b_partials_kernel<<<g.K, 256, 0, g.stream>>>(mask, g.w, ntiles, 4);
     SCY_LAUNCH_CHECK();
     if (first) {
@@ -1773,13 +1823,14 @@ scy_status scy_batch_profile_collect(scy_batch* b, int kernel, double* ms, long 
   return SCY_OK;
 }
 
-scy_status scy_batch_tuning(scy_batch* b, int g, int* kpb, int* sweep_variant, double* us) {
+scy_status scy_batch_tuning(scy_batch* b, int g, int* kpb, int* sweep_variant, int* ztransform, double* us) {
   if (!b || g < 0 || g >= (int)b->ctx.groups.size()) return SCY_ERR_ARG;
   const scy::BatchGroup& G = *b->ctx.groups[g];
   if (kpb) *kpb = G.kpb;
   if (sweep_variant) *sweep_variant = G.ys_variant;
+  if (ztransform) *ztransform = G.zt_pair | (G.zt_bf16 << 1);
   if (us)
-    for (int i = 0; i < 8; ++i) us[i] = G.tune_us[i];
+    for (int i = 0; i < 12; ++i) us[i] = G.tune_us[i];
   return SCY_OK;
 }
 

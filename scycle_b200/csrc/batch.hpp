@@ -71,7 +71,12 @@ struct BatchGroup {
   DevBuf planes;  // the operator's 33 cross-stencil coefficient planes (build_cross_planes)
   int kpb = 1;    // instances per block of the operator kernels (autotuned at set-up)
   int ys_variant = 0;  // chains per lane x warps per block of the banded sweeps (autotuned)
-  double tune_us[8] = {0};  // the autotuner's timings: kpb 1, 2, 4, 8, sweep variants 0, 1, 2
+  int zt_pair = 0;  // z-transform products in the two-CTAs-per-SM shape (autotuned)
+  int zt_bf16 = 0;  // z-transform digits in bf16 (kind::f16) instead of 8-bit integers (autotuned)
+  // the autotuner's timings: kpb 1, 2, 4, 8, sweep variants 0, 1, 2, -,
+  // z-transform product with 8-bit digits in the one- and two-CTAs-per-SM
+  // shapes, with bf16 digits in the two shapes
+  double tune_us[12] = {0};
   DevBuf vec[7], vecf[4], sc, partials, counters, status;
   BatchWork w{};
   cudaStream_t stream = nullptr;
@@ -82,6 +87,7 @@ struct BatchGroup {
   // transform; K*Ny rows of Nz values) and of the two weight matrices
   // (rows of Vz^T for the forward transform, rows of Vz for the inverse)
   OzkOperand zx, zw1, zw2;
+  OzkOperand zx16, zw1_16, zw2_16;  // the same digits in bf16 while the autotuner compares (then freed)
   DevBuf blas_ws;
   ~BatchGroup();
 };

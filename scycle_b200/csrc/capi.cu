@@ -553,6 +553,23 @@ scy_status scy_qd_set_jacobian(scy_qd* q, int exact) {
   return SCY_OK;
 }
 
+scy_status scy_qd_steady_state_info(scy_qd* q, int* ss_its, double* ss_err, long* cg_its) {
+  if (!q) return SCY_ERR_ARG;
+  if (ss_its) *ss_its = q->ctx.ss_its;
+  if (ss_err) *ss_err = q->ctx.ss_err;
+  if (cg_its) *cg_its = q->ctx.ss_cg_its;
+  return SCY_OK;
+}
+
+scy_status scy_qd_steady_state_trace(scy_qd* q, double* out, long cap, long* n) {
+  if (!q || !n) return SCY_ERR_ARG;
+  const std::vector<double>& t = q->ctx.ss_trace;
+  *n = (long)t.size() / 5;
+  if (out)
+    for (long i = 0; i < std::min<long>((long)t.size(), cap * 5); ++i) out[i] = t[i];
+  return SCY_OK;
+}
+
 scy_status scy_qd_set_state(scy_qd* q, const double* var, int recompute) {
   if (!q || !var) return SCY_ERR_ARG;
   scy::QDContext& c = q->ctx;

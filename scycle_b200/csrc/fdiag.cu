@@ -156,22 +156,74 @@ FDPrecond::~FDPrecond() {
   if (blas) cublasDestroy(blas);
 }
 
+namespace {
+// Product fit mu(y, z) ~ a(y) b(z) for a non-constant shear modulus (or
+// viscosity): log mu ~ alpha(iy) + beta(iz) by alternating midranges, which
+// drives down the largest log misfit (the spread of mu / (a b) bounds the
+// condition number of the preconditioned operator).  a = b = 1 for constant
+// or non-positive mu, so the averaged coefficients below are then the
+// plain means.
+void product_fit(const LevelHost& L, std::vector<double>& a, std::vector<double>& b) {
+  const int Ny = L.Ny, Nz = L.Nz;
+  a.assign(Ny, 1.0);
+  b.assign(Nz, 1.0);
+  bool varies = false;
+  for (size_t i = 0; i < L.mu.size(); ++i) {
+    if (!(L.mu[i] > 0)) return;
+    if (L.mu[i] != L.mu[0]) varies = true;
+  }
+  if (!varies) return;
+  std::vector<double> lg(L.mu.size()), al(Ny, 0.0), be(Nz, 0.0);
+  for (size_t i = 0; i < lg.size(); ++i) lg[i] = std::log(L.mu[i]);
+  for (int round = 0; round < 60; ++round) {
+    for (int iy = 0; iy < Ny; ++iy) {
+      double lo = INFINITY, hi = -INFINITY;
+      for (int iz = 0; iz < Nz; ++iz) {
+        const double v = lg[(size_t)iy * Nz + iz] - be[iz];
+        lo = std::min(lo, v);
+        hi = std::max(hi, v);
+      }
+      al[iy] = 0.5 * (lo + hi);
+    }
+    for (int iz = 0; iz < Nz; ++iz) {
+      double lo = INFINITY, hi = -INFINITY;
+      for (int iy = 0; iy < Ny; ++iy) {
+        const double v = lg[(size_t)iy * Nz + iz] - al[iy];
+        lo = std::min(lo, v);
+        hi = std::max(hi, v);
+      }
+      be[iz] = 0.5 * (lo + hi);
+    }
+  }
+  for (int iy = 0; iy < Ny; ++iy) a[iy] = std::exp(al[iy]);
+  for (int iz = 0; iz < Nz; ++iz) b[iz] = std::exp(be[iz]);
+}
+}  // namespace
+
 int FDPrecond::build(const LevelHost& L, cudaStream_t s) {
   Ny = L.Ny;
   Nz = L.Nz;
   const size_t N = (size_t)Ny * Nz;
-  // averaged 1D coefficients and weights
+  // Averaged 1D coefficients and weights of the separable operator
+  // Ly(cy1) x Mz + My x Lz(cz1).  Both directions' coefficients carry mu
+  // (cy = mu qy, cz = mu rz); with the product fit mu ~ a(y) b(z) the y
+  // operator takes cy / b and the z mass b, the z operator cz / a and the y
+  // mass a, which is exact when mu is a product and the metrics separate.
+  std::vector<double> fa, fb;
+  product_fit(L, fa, fb);
   std::vector<double> cy1(Ny, 0), m3y1(Ny, 0), My(Ny, 0), cz1(Nz, 0), m3z1(Nz, 0), Mz(Nz, 0);
   for (int iy = 0; iy < Ny; ++iy)
     for (int iz = 0; iz < Nz; ++iz) {
       size_t i = (size_t)iy * Nz + iz;
-      cy1[iy] += L.cy[i] / Nz;
-      m3y1[iy] += L.m3y[i] / Nz;
+      cy1[iy] += L.cy[i] / fb[iz] / Nz;
+      m3y1[iy] += L.m3y[i] / fb[iz] / Nz;
       My[iy] += L.wz[i] / Nz;
-      cz1[iz] += L.cz[i] / Ny;
-      m3z1[iz] += L.m3z[i] / Ny;
+      cz1[iz] += L.cz[i] / fa[iy] / Ny;
+      m3z1[iz] += L.m3z[i] / fa[iy] / Ny;
       Mz[iz] += L.wy[i] / Ny;
     }
+  for (int iy = 0; iy < Ny; ++iy) My[iy] *= fa[iy];
+  for (int iz = 0; iz < Nz; ++iz) Mz[iz] *= fb[iz];
   std::vector<double> Ly = dense_line_operator(L.ty, cy1, m3y1, L.bc[2], L.bc[0]);
   std::vector<double> Lz = dense_line_operator(L.tz, cz1, m3z1, L.bc[1], L.bc[3]);
   for (auto& v : Ly) v = -v;

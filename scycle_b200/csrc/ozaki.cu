@@ -13,6 +13,19 @@
 // (tcgen05.ld 32x32b), combine the groups in FP64 with their powers of two,
 // apply the row and column exponents and store the tile.
 //
+// Two digit formats: signed 8-bit digits multiplied by tcgen05.mma
+// kind::i8 into 32-bit integer accumulators, or the same digits held in
+// bf16 (every integer of magnitude <= 256 is exact there) multiplied by
+// kind::f16 into FP32 accumulators, exact while every partial sum stays
+// below 2^24 in magnitude (S * 64 * 64 * Kp < 2^24, checked on the host).
+// The products are bit-identical; which is faster depends on the tensor
+// pipe's integer and bf16 rates, so callers time both.
+//
+// Two shapes: one CTA per SM (all 512 tensor-memory columns, CN = 144 /
+// 112 / 96 / 64 columns for S = 3 / 4 / 5 / 6-7, up to four stages) and,
+// for S <= 5, two CTAs per SM (256 columns each, CN = 64 / 64 / 48, two
+// stages), where one CTA's epilogue overlaps the other's products.
+//
 // Every mbarrier wait is bounded (2^20 polls).  A wait that runs out marks
 // the tile's rows in the caller's status words; the producer then waits
 // (bounded) for the copies it issued that nobody consumed, the epilogue
@@ -20,6 +33,7 @@
 // before the CTA exits.  TMA loads read this GPU's own memory only and use
 // no cluster multicast.
 #include <cmath>
+#include <cstring>
 #include <vector>
 
 #include "ozaki.hpp"
@@ -33,12 +47,26 @@ constexpr int OZK_BK = 64;   // bytes of K per stage (one 64-byte swizzle row)
 constexpr int OZK_POLLS = 1 << 20;
 constexpr int OZK_SMEM_BUDGET = 220 * 1024;
 
-__host__ __device__ constexpr int ozk_cn(int S) { return S <= 3 ? 144 : S == 4 ? 112 : S == 5 ? 96 : 64; }
-__host__ __device__ constexpr int ozk_stage_bytes(int S) { return S * OZK_BM * OZK_BK + S * ozk_cn(S) * OZK_BK; }
-__host__ __device__ constexpr int ozk_stages(int S) {
-  return OZK_SMEM_BUDGET / ozk_stage_bytes(S) > 4 ? 4 : OZK_SMEM_BUDGET / ozk_stage_bytes(S);
+// PAIR = 0: one CTA per SM; PAIR = 1: two (S <= 5)
+__host__ __device__ constexpr int ozk_cn(int S, int pair = 0) {
+  return pair ? (S <= 4 ? 64 : 48) : (S <= 3 ? 144 : S == 4 ? 112 : S == 5 ? 96 : 64);
 }
-__host__ __device__ constexpr int ozk_smem_bytes(int S) { return ozk_stages(S) * ozk_stage_bytes(S) + 1024; }
+__host__ __device__ constexpr int ozk_tmem_cols(int pair) { return pair ? 256 : 512; }
+__host__ __device__ constexpr int ozk_stage_bytes(int S, int pair = 0) {
+  return S * OZK_BM * OZK_BK + S * ozk_cn(S, pair) * OZK_BK;
+}
+__host__ __device__ constexpr int ozk_stages(int S, int pair = 0) {
+  return pair ? 2 : OZK_SMEM_BUDGET / ozk_stage_bytes(S) > 4 ? 4 : OZK_SMEM_BUDGET / ozk_stage_bytes(S);
+}
+// the stage ring starts on a 1024-byte (one CTA per SM) or 512-byte (two)
+// boundary: the 64-byte swizzle repeats every 512 bytes
+__host__ __device__ constexpr int ozk_align(int pair) { return pair ? 512 : 1024; }
+__host__ __device__ constexpr int ozk_smem_bytes(int S, int pair = 0) {
+  return ozk_stages(S, pair) * ozk_stage_bytes(S, pair) + ozk_align(pair);
+}
+static_assert(2 * (ozk_smem_bytes(5, 1) + 1024 + 256) <= 228 * 1024, "two CTAs per SM do not fit");
+static_assert(2 * (ozk_smem_bytes(4, 1) + 1024 + 256) <= 228 * 1024, "two CTAs per SM do not fit");
+static_assert(2 * (ozk_smem_bytes(3, 1) + 1024 + 256) <= 228 * 1024, "two CTAs per SM do not fit");
 
 // shared-memory matrix descriptor (tcgen05 format): K-major operand whose
 // rows are 64 bytes with 64-byte swizzling, 8-row groups 512 bytes apart
@@ -63,11 +91,26 @@ __host__ __device__ constexpr uint32_t umma_idesc_s8(int n) {
   return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(OZK_BM >> 4) << 24);
 }
 
+// instruction descriptor: bf16 A and B, K-major, FP32 accumulator, M = 128,
+// N = n
+__host__ __device__ constexpr uint32_t umma_idesc_bf16(int n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(OZK_BM >> 4) << 24);
+}
+
 __device__ __forceinline__ void umma_s8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
                                         uint32_t accumulate) {
   asm volatile(
       "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
       " tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
       "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
       : "memory");
 }
@@ -86,24 +129,27 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
       : "r"(taddr));
 }
 
-template <int S, typename T>
-__global__ void __launch_bounds__(128, 1)
+template <int S, typename T, int PAIR, int BF>
+__global__ void __launch_bounds__(128, PAIR ? 2 : 1)
     ozk_gemm_kernel(const __grid_constant__ CUtensorMap mx, const __grid_constant__ CUtensorMap mw,
                     const int* __restrict__ ex, const int* __restrict__ ew, T* __restrict__ D, long ldd, int rows,
                     int cout, int nkb, unsigned* __restrict__ status, int rows_per_status, unsigned bit) {
-  constexpr int CN = ozk_cn(S);
+  constexpr int CN = ozk_cn(S, PAIR);
   constexpr int XB = S * OZK_BM * OZK_BK;
   constexpr int WB = S * CN * OZK_BK;
-  constexpr int ST = ozk_stages(S);
-  static_assert(S * CN <= 512, "accumulators exceed tensor memory");
+  constexpr int ST = ozk_stages(S, PAIR);
+  constexpr int TC = ozk_tmem_cols(PAIR);
+  constexpr unsigned AL = ozk_align(PAIR);
+  static_assert(S * CN <= TC, "accumulators exceed tensor memory");
+  static_assert(!PAIR || S <= 5, "two CTAs per SM only for S <= 5");
   static_assert(CN % 16 == 0 && CN >= 16 && CN <= 256, "invalid MMA N");
   static_assert(8 * 256 + OZK_BM * (CN + 1) * (int)sizeof(T) <= ST * (XB + WB), "epilogue tile exceeds the stages");
   extern __shared__ __align__(1024) unsigned char ozk_smem_raw[];
   __shared__ __align__(8) uint64_t full[ST], empty[ST], done;
   __shared__ uint32_t tmem_slot;
   __shared__ int consumed, failed;
-  // tiles on a 1024-byte boundary (the swizzle pattern repeats every 512 B)
-  unsigned char* smem = ozk_smem_raw + ((1024u - (smem_u32(ozk_smem_raw) & 1023u)) & 1023u);
+  // tiles on a 1024- or 512-byte boundary (the swizzle pattern repeats every 512 B)
+  unsigned char* smem = ozk_smem_raw + ((AL - (smem_u32(ozk_smem_raw) & (AL - 1))) & (AL - 1));
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m0 = blockIdx.x * OZK_BM, c0 = blockIdx.y * CN;
 
@@ -118,7 +164,8 @@ __global__ void __launch_bounds__(128, 1)
     failed = 0;
   }
   if (warp == 1) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(smem_u32(&tmem_slot))
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
+                 "n"(TC)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -137,13 +184,14 @@ __global__ void __launch_bounds__(128, 1)
       }
       unsigned char* sx = smem + st * (XB + WB);
       mbar_expect_tx(&full[st], XB + WB);
-      tma_load_3d(sx, &mx, &full[st], kb * OZK_BK, m0, 0);
-      tma_load_3d(sx + XB, &mw, &full[st], kb * OZK_BK, c0, 0);
+      // x coordinate in digits: 64 bytes of K per stage
+      tma_load_3d(sx, &mx, &full[st], kb * (OZK_BK / (BF ? 2 : 1)), m0, 0);
+      tma_load_3d(sx + XB, &mw, &full[st], kb * (OZK_BK / (BF ? 2 : 1)), c0, 0);
       ++issued;
     }
   } else if (warp == 1 && lane == 0) {
     // MMA issuer
-    constexpr uint32_t idesc = umma_idesc_s8(CN);
+    constexpr uint32_t idesc = BF ? umma_idesc_bf16(CN) : umma_idesc_s8(CN);
     int kb = 0;
     for (; kb < nkb; ++kb) {
       const int st = kb % ST;
@@ -163,7 +211,10 @@ __global__ void __launch_bounds__(128, 1)
             const int j = g + 2 - i;
             const uint64_t ad = umma_desc_sw64(xa + (i - 1) * OZK_BM * OZK_BK + ks * 32);
             const uint64_t bd = umma_desc_sw64(wa + (j - 1) * CN * OZK_BK + ks * 32);
-            umma_s8(tmem + g * CN, ad, bd, idesc, (kb > 0 || ks > 0 || i > 1) ? 1u : 0u);
+            if (BF)
+              umma_bf16(tmem + g * CN, ad, bd, idesc, (kb > 0 || ks > 0 || i > 1) ? 1u : 0u);
+            else
+              umma_s8(tmem + g * CN, ad, bd, idesc, (kb > 0 || ks > 0 || i > 1) ? 1u : 0u);
           }
       umma_commit(&empty[st]);
     }
@@ -211,7 +262,7 @@ __global__ void __launch_bounds__(128, 1)
         // smallest weights first
         const double wgt = pow2i(-7 * (g + 2));
 #pragma unroll
-        for (int q = 0; q < 16; ++q) acc[q] += (double)(int)v[g][q] * wgt;
+        for (int q = 0; q < 16; ++q) acc[q] += (BF ? (double)__uint_as_float(v[g][q]) : (double)(int)v[g][q]) * wgt;
       }
 #pragma unroll
       for (int q = 0; q < 16; ++q) tile[rl * LDT + cc + q] = (T)((acc[q] * xs) * sw[cc + q]);
@@ -227,16 +278,16 @@ __global__ void __launch_bounds__(128, 1)
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
-  if (warp == 1) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem) : "memory");
+  if (warp == 1) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "n"(TC) : "memory");
 }
 
 // digits of one row per warp: lane l holds the K positions 4 l + 128 j + q
 // (q < 4, j < 8, so K <= 1024) in registers, read once; the row maximum is
 // a warp reduction, and the four digits of a position group and plane go
 // out as one 32-bit word (a warp stores 128 consecutive bytes)
-template <typename Tin>
+template <typename Tin, int BF>
 __global__ void ozk_split_kernel(const Tin* __restrict__ X, long ldx, int rows, int K, int Kp, int S,
-                                 int8_t* __restrict__ dig, long plane, int* __restrict__ expo) {
+                                 unsigned char* __restrict__ dig, long plane, int* __restrict__ expo) {
   const int row = (int)((blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5);
   const int lane = threadIdx.x & 31;
   if (row >= rows) return;
@@ -255,7 +306,10 @@ __global__ void ozk_split_kernel(const Tin* __restrict__ X, long ldx, int rows, 
   m = warp_max(m);
   const int e = m > 0.0 ? ilogb(m) + 2 : 0;
   if (lane == 0) expo[row] = e;
-  int8_t* drow = dig + (long)row * Kp;
+  // digit element size: 1 byte, or 2 (bf16 bit pattern of the integer: the
+  // upper half of its FP32 pattern, exact for |d| <= 256)
+  constexpr int ES = BF ? 2 : 1;
+  unsigned char* drow = dig + (long)row * Kp * ES;
 #pragma unroll
   for (int j = 0; j < 8; ++j) {
     const int k0 = 4 * lane + 128 * j;
@@ -264,69 +318,109 @@ __global__ void ozk_split_kernel(const Tin* __restrict__ X, long ldx, int rows, 
 #pragma unroll
     for (int q = 0; q < 4; ++q) t[q] = ldexp(v[j][q], 7 - e);
     for (int i = 0; i < S; ++i) {
-      uint32_t w = 0;
+      uint32_t w = 0, w2 = 0;
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
         const double d = rint(t[q]);
         t[q] = (t[q] - d) * 128.0;
-        w |= ((uint32_t)(int)d & 0xFFu) << (8 * q);
+        if (BF) {
+          const uint32_t b = __float_as_uint((float)d) >> 16;
+          if (q < 2)
+            w |= b << (16 * q);
+          else
+            w2 |= b << (16 * (q - 2));
+        } else {
+          w |= ((uint32_t)(int)d & 0xFFu) << (8 * q);
+        }
       }
-      *reinterpret_cast<uint32_t*>(drow + i * plane + k0) = w;
+      if (BF)
+        *reinterpret_cast<uint2*>(drow + (i * plane + k0) * 2) = make_uint2(w, w2);
+      else
+        *reinterpret_cast<uint32_t*>(drow + i * plane + k0) = w;
     }
   }
 }
 
-template <int S, typename T>
+template <int S, typename T, int PAIR, int BF>
 int prepare_one() {
   // the shared-memory limit is a per-device function attribute
   static unsigned long long attr_set = 0;
   int dev = 0;
   SCY_CUDA_TRY(cudaGetDevice(&dev));
   if (dev < 0 || dev >= 64 || !(attr_set >> dev & 1ull)) {
-    SCY_CUDA_TRY(cudaFuncSetAttribute(ozk_gemm_kernel<S, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      ozk_smem_bytes(S)));
+    SCY_CUDA_TRY(cudaFuncSetAttribute(ozk_gemm_kernel<S, T, PAIR, BF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      ozk_smem_bytes(S, PAIR)));
     if (dev >= 0 && dev < 64) attr_set |= 1ull << dev;
   }
   return SCY_OK;
 }
 
-template <int S>
-int prepare_s() {
-  const int rc = prepare_one<S, double>();
-  return rc != SCY_OK ? rc : prepare_one<S, float>();
+template <int S, int BF>
+int prepare_sb() {
+  int rc = prepare_one<S, double, 0, BF>();
+  if (rc == SCY_OK) rc = prepare_one<S, float, 0, BF>();
+  if constexpr (S <= 5) {
+    if (rc == SCY_OK) rc = prepare_one<S, double, 1, BF>();
+    if (rc == SCY_OK) rc = prepare_one<S, float, 1, BF>();
+  }
+  return rc;
 }
 
-template <int S, typename T>
-int launch_gemm(const OzkOperand& x, const OzkOperand& w, T* D, long ldd, int cout, cudaStream_t s, unsigned* status,
-                int rows_per_status, unsigned bit) {
-  constexpr int CN = ozk_cn(S);
+template <int S>
+int prepare_s() {
+  const int rc = prepare_sb<S, 0>();
+  return rc != SCY_OK ? rc : prepare_sb<S, 1>();
+}
+
+template <int S, typename T, int PAIR, int BF>
+int launch_gemm(const OzkOperand& x, const CUtensorMap& wmap, const OzkOperand& w, T* D, long ldd, int cout,
+                cudaStream_t s, unsigned* status, int rows_per_status, unsigned bit) {
+  constexpr int CN = ozk_cn(S, PAIR);
   {
-    const int rc = prepare_one<S, T>();
+    const int rc = prepare_one<S, T, PAIR, BF>();
     if (rc != SCY_OK) return rc;
   }
   const dim3 grid((x.rows + OZK_BM - 1) / OZK_BM, (cout + CN - 1) / CN);
-  ozk_gemm_kernel<S, T><<<grid, 128, ozk_smem_bytes(S), s>>>(x.map, w.map, x.expo.as<int>(), w.expo.as<int>(), D,
-                                                             ldd, x.rows, cout, x.Kp / OZK_BK, status,
-                                                             rows_per_status, bit);
+  ozk_gemm_kernel<S, T, PAIR, BF><<<grid, 128, ozk_smem_bytes(S, PAIR), s>>>(
+      x.map, wmap, x.expo.as<int>(), w.expo.as<int>(), D, ldd, x.rows, cout, x.Kp * x.esz / OZK_BK, status,
+      rows_per_status, bit);
   SCY_LAUNCH_CHECK();
   return SCY_OK;
 }
 
+template <int S, typename T, int BF>
+int launch_variant_b(const OzkOperand& x, const OzkOperand& w, T* D, long ldd, int cout, cudaStream_t s,
+                     unsigned* status, int rps, unsigned bit, int pair) {
+  if constexpr (S <= 5) {
+    if (pair) return launch_gemm<S, T, 1, BF>(x, w.map_pair, w, D, ldd, cout, s, status, rps, bit);
+  }
+  return launch_gemm<S, T, 0, BF>(x, w.map, w, D, ldd, cout, s, status, rps, bit);
+}
+
+template <int S, typename T>
+int launch_variant(const OzkOperand& x, const OzkOperand& w, T* D, long ldd, int cout, cudaStream_t s,
+                   unsigned* status, int rps, unsigned bit, int pair) {
+  if (x.esz == 2) return launch_variant_b<S, T, 1>(x, w, D, ldd, cout, s, status, rps, bit, pair);
+  return launch_variant_b<S, T, 0>(x, w, D, ldd, cout, s, status, rps, bit, pair);
+}
+
 template <typename T>
 int gemm_any(const OzkOperand& x, const OzkOperand& w, T* D, long ldd, int cout, cudaStream_t s, unsigned* status,
-             int rps, unsigned bit) {
-  if (x.S != w.S || x.Kp != w.Kp || x.K != w.K || cout > w.rows || cout < 1 || x.rows < 1 ||
-      w.box_rows != ozk_cn(w.S) || x.box_rows != OZK_BM || rps < 1) {
-    set_error("ozk_gemm: operands do not match (S %d/%d, K %d/%d, cout %d, W rows %d)", x.S, w.S, x.K, w.K, cout,
-              w.rows);
+             int rps, unsigned bit, int pair) {
+  pair = pair ? 1 : 0;
+  if (x.S != w.S || x.Kp != w.Kp || x.K != w.K || x.esz != w.esz || cout > w.rows || cout < 1 || x.rows < 1 ||
+      w.box_rows != ozk_cn(w.S) || x.box_rows != OZK_BM || rps < 1 ||
+      (pair && (w.S > 5 || w.box_rows_pair != ozk_cn(w.S, 1)))) {
+    set_error("ozk_gemm: operands do not match (S %d/%d, K %d/%d, cout %d, W rows %d, two CTAs per SM %d)", x.S,
+              w.S, x.K, w.K, cout, w.rows, pair);
     return SCY_ERR_ARG;
   }
   switch (x.S) {
-    case 3: return launch_gemm<3, T>(x, w, D, ldd, cout, s, status, rps, bit);
-    case 4: return launch_gemm<4, T>(x, w, D, ldd, cout, s, status, rps, bit);
-    case 5: return launch_gemm<5, T>(x, w, D, ldd, cout, s, status, rps, bit);
-    case 6: return launch_gemm<6, T>(x, w, D, ldd, cout, s, status, rps, bit);
-    case 7: return launch_gemm<7, T>(x, w, D, ldd, cout, s, status, rps, bit);
+    case 3: return launch_variant<3, T>(x, w, D, ldd, cout, s, status, rps, bit, pair);
+    case 4: return launch_variant<4, T>(x, w, D, ldd, cout, s, status, rps, bit, pair);
+    case 5: return launch_variant<5, T>(x, w, D, ldd, cout, s, status, rps, bit, pair);
+    case 6: return launch_variant<6, T>(x, w, D, ldd, cout, s, status, rps, bit, 0);
+    case 7: return launch_variant<7, T>(x, w, D, ldd, cout, s, status, rps, bit, 0);
     default: break;
   }
   set_error("ozk_gemm: %d digit planes (3 to 7 are built)", x.S);
@@ -336,6 +430,7 @@ int gemm_any(const OzkOperand& x, const OzkOperand& w, T* D, long ldd, int cout,
 }  // namespace
 
 int ozk_cols_per_tile(int S) { return ozk_cn(S); }
+int ozk_cols_per_tile_pair(int S) { return S <= 5 ? ozk_cn(S, 1) : 0; }
 
 int ozk_prepare(int S) {
   switch (S) {
@@ -350,24 +445,43 @@ int ozk_prepare(int S) {
   return SCY_ERR_ARG;
 }
 
-int OzkOperand::alloc(int S_, int rows_, int K_, int box_rows_) {
-  if (S_ < 3 || S_ > 7 || rows_ < 1 || K_ < 1 || K_ > 1024 || box_rows_ < 8 || box_rows_ > 256) {
-    set_error("OzkOperand: invalid shape (S %d, rows %d, K %d, box rows %d)", S_, rows_, K_, box_rows_);
+int OzkOperand::alloc_weights(int S_, int rows_, int K_, int esz_) {
+  SCY_TRY(alloc(S_, rows_, K_, ozk_cols_per_tile(S_), esz_));
+  box_rows_pair = ozk_cols_per_tile_pair(S_);
+  if (box_rows_pair > 0 &&
+      tma_map_3d_sw64(&map_pair, dig.p, esz == 2 ? CU_TENSOR_MAP_DATA_TYPE_UINT16 : CU_TENSOR_MAP_DATA_TYPE_UINT8,
+                      Kp, rows, S, Kp * esz, plane * esz, OZK_BK / esz, box_rows_pair, S) != SCY_OK)
+    return SCY_ERR_CUDA;
+  return SCY_OK;
+}
+
+bool ozk_bf16_exact(int S, int K) {
+  const long Kp = (K + OZK_BK / 2 - 1) / (OZK_BK / 2) * (OZK_BK / 2);
+  return (long)S * 64 * 64 * Kp < (1L << 24);
+}
+
+int OzkOperand::alloc(int S_, int rows_, int K_, int box_rows_, int esz_) {
+  if (S_ < 3 || S_ > 7 || rows_ < 1 || K_ < 1 || K_ > 1024 || box_rows_ < 8 || box_rows_ > 256 ||
+      (esz_ != 1 && esz_ != 2) || (esz_ == 2 && !ozk_bf16_exact(S_, K_))) {
+    set_error("OzkOperand: invalid shape (S %d, rows %d, K %d, box rows %d, digit bytes %d)", S_, rows_, K_,
+              box_rows_, esz_);
     return SCY_ERR_ARG;
   }
   S = S_;
   rows = rows_;
   K = K_;
-  Kp = (K + OZK_BK - 1) / OZK_BK * OZK_BK;
+  esz = esz_;
+  const int kq = OZK_BK / esz;  // digits per 64-byte stage row
+  Kp = (K + kq - 1) / kq * kq;
   box_rows = box_rows_;
   plane = (long)rows * Kp;
-  SCY_TRY(dig.alloc((size_t)S * plane));
+  SCY_TRY(dig.alloc((size_t)S * plane * esz));
   SCY_TRY(expo.alloc((size_t)rows * sizeof(int)));
   // zero once: the K padding of every row stays zero
-  SCY_CUDA_TRY(cudaMemset(dig.p, 0, (size_t)S * plane));
+  SCY_CUDA_TRY(cudaMemset(dig.p, 0, (size_t)S * plane * esz));
   SCY_CUDA_TRY(cudaMemset(expo.p, 0, (size_t)rows * sizeof(int)));
-  if (tma_map_3d_sw64(&map, dig.p, CU_TENSOR_MAP_DATA_TYPE_UINT8, Kp, rows, S, Kp, plane, OZK_BK, box_rows, S) !=
-      SCY_OK)
+  if (tma_map_3d_sw64(&map, dig.p, esz == 2 ? CU_TENSOR_MAP_DATA_TYPE_UINT16 : CU_TENSOR_MAP_DATA_TYPE_UINT8, Kp,
+                      rows, S, Kp * esz, plane * esz, kq, box_rows, S) != SCY_OK)
     return SCY_ERR_CUDA;
   return SCY_OK;
 }
@@ -376,8 +490,12 @@ template <typename Tin>
 static int split_any(OzkOperand& o, const Tin* X, long ldx, cudaStream_t s) {
   const int threads = 256;
   const int blocks = (int)(((long)o.rows * 32 + threads - 1) / threads);
-  ozk_split_kernel<Tin><<<blocks, threads, 0, s>>>(X, ldx, o.rows, o.K, o.Kp, o.S, o.dig.as<int8_t>(), o.plane,
-                                                   o.expo.as<int>());
+  if (o.esz == 2)
+    ozk_split_kernel<Tin, 1><<<blocks, threads, 0, s>>>(X, ldx, o.rows, o.K, o.Kp, o.S, o.dig.as<unsigned char>(),
+                                                        o.plane, o.expo.as<int>());
+  else
+    ozk_split_kernel<Tin, 0><<<blocks, threads, 0, s>>>(X, ldx, o.rows, o.K, o.Kp, o.S, o.dig.as<unsigned char>(),
+                                                        o.plane, o.expo.as<int>());
   SCY_LAUNCH_CHECK();
   return SCY_OK;
 }
@@ -387,6 +505,7 @@ int ozk_split(OzkOperand& o, const float* X, long ldx, cudaStream_t s) { return 
 
 int ozk_set_host(OzkOperand& o, const double* W, long ldw, cudaStream_t s) {
   std::vector<int8_t> dig((size_t)o.S * o.plane, 0);
+  std::vector<uint16_t> dig2(o.esz == 2 ? (size_t)o.S * o.plane : 0, 0);
   std::vector<int> ex(o.rows, 0);
   for (int r = 0; r < o.rows; ++r) {
     const double* x = W + (long)r * ldw;
@@ -399,24 +518,36 @@ int ozk_set_host(OzkOperand& o, const double* W, long ldw, cudaStream_t s) {
       for (int i = 0; i < o.S; ++i) {
         const double d = std::nearbyint(t);
         t = (t - d) * 128.0;
-        dig[(size_t)i * o.plane + (size_t)r * o.Kp + k] = (int8_t)(int)d;
+        const size_t at = (size_t)i * o.plane + (size_t)r * o.Kp + k;
+        if (o.esz == 2) {
+          // bf16 pattern of the integer digit: the upper half of its FP32 pattern
+          const float f = (float)d;
+          uint32_t u;
+          std::memcpy(&u, &f, 4);
+          dig2[at] = (uint16_t)(u >> 16);
+        } else {
+          dig[at] = (int8_t)(int)d;
+        }
       }
     }
   }
-  SCY_CUDA_TRY(cudaMemcpyAsync(o.dig.p, dig.data(), dig.size(), cudaMemcpyHostToDevice, s));
+  if (o.esz == 2)
+    SCY_CUDA_TRY(cudaMemcpyAsync(o.dig.p, dig2.data(), dig2.size() * 2, cudaMemcpyHostToDevice, s));
+  else
+    SCY_CUDA_TRY(cudaMemcpyAsync(o.dig.p, dig.data(), dig.size(), cudaMemcpyHostToDevice, s));
   SCY_CUDA_TRY(cudaMemcpyAsync(o.expo.p, ex.data(), ex.size() * sizeof(int), cudaMemcpyHostToDevice, s));
   SCY_CUDA_TRY(cudaStreamSynchronize(s));
   return SCY_OK;
 }
 
 int ozk_gemm(const OzkOperand& x, const OzkOperand& w, double* D, long ldd, int cout, cudaStream_t s,
-             unsigned* status, int rows_per_status, unsigned bit) {
-  return gemm_any<double>(x, w, D, ldd, cout, s, status, rows_per_status, bit);
+             unsigned* status, int rows_per_status, unsigned bit, int pair) {
+  return gemm_any<double>(x, w, D, ldd, cout, s, status, rows_per_status, bit, pair);
 }
 
 int ozk_gemm(const OzkOperand& x, const OzkOperand& w, float* D, long ldd, int cout, cudaStream_t s,
-             unsigned* status, int rows_per_status, unsigned bit) {
-  return gemm_any<float>(x, w, D, ldd, cout, s, status, rows_per_status, bit);
+             unsigned* status, int rows_per_status, unsigned bit, int pair) {
+  return gemm_any<float>(x, w, D, ldd, cout, s, status, rows_per_status, bit, pair);
 }
 
 }  // namespace scy
@@ -424,22 +555,25 @@ int ozk_gemm(const OzkOperand& x, const OzkOperand& w, float* D, long ldd, int c
 // ---------------------------------------------------------------------------
 // C ABI: the product on its own (set-up and digit planes allocated per call)
 extern "C" scy_status scy_ozaki_matmul(const double* X, long ldx, int rows, int K, const double* W, long ldw,
-                                       int cols, int S, double* D, long ldd) {
+                                       int cols, int S, double* D, long ldd, int ctas_per_sm, int bf16_digits) {
   using namespace scy;
-  if (!X || !W || !D || rows < 1 || cols < 1 || K < 1 || ldx < K || ldw < K || ldd < cols) {
+  if (!X || !W || !D || rows < 1 || cols < 1 || K < 1 || ldx < K || ldw < K || ldd < cols ||
+      (ctas_per_sm != 1 && ctas_per_sm != 2) || (ctas_per_sm == 2 && S > 5) ||
+      (bf16_digits && !ozk_bf16_exact(S, K))) {
     set_error("scy_ozaki_matmul: invalid arguments");
     return SCY_ERR_ARG;
   }
+  const int esz = bf16_digits ? 2 : 1;
   OzkOperand x, w;
-  SCY_TRY(x.alloc(S, rows, K, 128));
-  SCY_TRY(w.alloc(S, cols, K, ozk_cols_per_tile(S)));
+  SCY_TRY(x.alloc(S, rows, K, 128, esz));
+  SCY_TRY(w.alloc_weights(S, cols, K, esz));
   cudaStream_t s = 0;
   SCY_TRY(ozk_set_host(w, W, ldw, s));
   SCY_TRY(ozk_split(x, X, ldx, s));
   DevBuf status;
   SCY_TRY(status.alloc(sizeof(unsigned)));
   SCY_CUDA_TRY(cudaMemsetAsync(status.p, 0, sizeof(unsigned), s));
-  SCY_TRY(ozk_gemm(x, w, D, ldd, cols, s, status.as<unsigned>(), 1 << 30, 1u));
+  SCY_TRY(ozk_gemm(x, w, D, ldd, cols, s, status.as<unsigned>(), 1 << 30, 1u, ctas_per_sm == 2 ? 1 : 0));
   unsigned st = 0;
   SCY_CUDA_TRY(cudaMemcpyAsync(&st, status.p, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
   SCY_CUDA_TRY(cudaStreamSynchronize(s));

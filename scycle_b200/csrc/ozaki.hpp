@@ -36,17 +36,27 @@ namespace scy {
 // layout the tensor cores read).
 struct OzkOperand {
   DevBuf dig, expo;
-  int S = 0, rows = 0, K = 0, Kp = 0, box_rows = 0;
-  long plane = 0;
-  CUtensorMap map;
+  int S = 0, rows = 0, K = 0, Kp = 0, box_rows = 0, box_rows_pair = 0;
+  int esz = 1;  // bytes of a digit: 1 (signed 8-bit) or 2 (bf16)
+  long plane = 0;  // digits of one plane (rows x Kp)
+  CUtensorMap map, map_pair;
   // box_rows: 128 for the row operand (X), the column tile width of S
-  // (ozk_cols_per_tile) for the weights (W)
-  int alloc(int S, int rows, int K, int box_rows);
+  // (ozk_cols_per_tile) for the weights (W); Kp = K rounded up to 64 bytes
+  // of digits
+  int alloc(int S, int rows, int K, int box_rows, int esz = 1);
+  // the weights' operand (W) with the maps of both product shapes
+  int alloc_weights(int S, int rows, int K, int esz = 1);
 };
 
-// column tile width of the product for S digit planes (S * width <= 512
-// tensor-memory columns)
+// bf16 digits give exact FP32 accumulation for S planes and K (every
+// partial sum below 2^24: S * 64 * 64 * Kp < 2^24)
+bool ozk_bf16_exact(int S, int K);
+
+// column tile width of the product for S digit planes: one CTA per SM
+// (S * width <= 512 tensor-memory columns) or, for S <= 5, two CTAs per SM
+// (S * width <= 256; 0 for S > 5)
 int ozk_cols_per_tile(int S);
+int ozk_cols_per_tile_pair(int S);
 
 // sets the kernels' shared-memory limit for S planes on the current device
 // (done by the first product too; call it before capturing one in a graph)
@@ -61,10 +71,11 @@ int ozk_set_host(OzkOperand& o, const double* W, long ldw, cudaStream_t s);
 // D[r, c] = sum_k X[r, k] W[c, k] for r < x.rows, c < cout (<= w.rows),
 // D of row stride ldd.  x.S == w.S.  A wait inside the kernel that runs out
 // (2^20 polls) sets `bit` in status[r / rows_per_status] for the rows of its
-// tile when status is given.
+// tile when status is given.  pair = 1 takes the two-CTAs-per-SM shape (S <=
+// 5, W made by alloc_weights); the two shapes give identical results.
 int ozk_gemm(const OzkOperand& x, const OzkOperand& w, double* D, long ldd, int cout, cudaStream_t s,
-             unsigned* status = nullptr, int rows_per_status = 1, unsigned bit = 4u);
+             unsigned* status = nullptr, int rows_per_status = 1, unsigned bit = 4u, int pair = 0);
 int ozk_gemm(const OzkOperand& x, const OzkOperand& w, float* D, long ldd, int cout, cudaStream_t s,
-             unsigned* status = nullptr, int rows_per_status = 1, unsigned bit = 4u);
+             unsigned* status = nullptr, int rows_per_status = 1, unsigned bit = 4u, int pair = 0);
 
 }  // namespace scy

@@ -97,6 +97,10 @@ int pl_d_dt(QDContext& q, double t, const double* var, double* f) {
   return SCY_OK;
 }
 
+__global__ void pl_axpy_kernel(double* __restrict__ x, const double* __restrict__ d, long n) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) x[i] += d[i];
+}
+
 // ---------------------------------------------------------------------------
 // The steady-state initial guess of guessSteadyStateICs = 1:
 // StrikeSlip_PowerLaw_qd::solveSS(0) (strikeSlip_powerLaw_qd.cpp:922-955)
@@ -154,9 +158,32 @@ int QDContext::pl_steady_state(const QDProblem& P, std::vector<double>& psi, std
   g.bcT = SCY_BC_NEUMANN;
   g.bcL = SCY_BC_NEUMANN;
   g.bcB = SCY_BC_NEUMANN;
+  // The viscosity spans many decades (up to the cap, 1e30 by default,
+  // powerLaw.cpp:757) and is far from separable; the stresses the update
+  // reads are products of that viscosity with small velocity gradients, so
+  // the velocity is needed to the accuracy of a direct solve.  Each solve
+  // is a defect correction: the residual in double-double arithmetic
+  // (SbpContext::residual_dd), a correction by preconditioned CG (multigrid
+  // unless the caller chose another preconditioner) to a relative 1e-6,
+  // repeated until the residual meets the solve tolerance or stops
+  // falling.  The first residual of each iteration is that of the previous
+  // iteration's velocity (a warm start).
+  const int kMaxRefine = 30;
   scy_solve_opts o = solve_opts;
+  o.verify = 1;
   o.nonzero_guess = 0;
-  o.max_its = std::max(o.max_its, 2000);
+  o.rtol = 1e-6;
+  o.atol = 0.0;
+  o.max_its = std::max(o.max_its, 4000);
+  ss_cg_its = 0;
+  ss_trace.clear();
+  DevBuf dres, dcor, dkeep, dzN;
+  SCY_TRY(dres.alloc(N * 8));
+  SCY_TRY(dcor.alloc(N * 8));
+  SCY_TRY(dkeep.alloc(N * 8));
+  SCY_TRY(dzN.alloc(N * 8));
+  SCY_CUDA_TRY(cudaMemsetAsync(dzN.p, 0, N * 8, s));
+  SCY_CUDA_TRY(cudaMemsetAsync(dv.p, 0, N * 8, s));
   std::vector<double> gxy((size_t)N), gxz((size_t)N), v((size_t)N), sxy_h((size_t)N), sxz_h((size_t)N);
   int it = 0;
   double err = 1e10;
@@ -168,8 +195,35 @@ int QDContext::pl_steady_state(const QDProblem& P, std::vector<double>& psi, std
     eta.stream = s;
     SCY_TRY(eta.set_rhs(dbcL.as<double>(), dbcR.as<double>(), dzero.as<double>(), dzero.as<double>(),
                         drhs.as<double>()));
-    scy_solve_stats st{};
-    SCY_TRY(eta.solve(drhs.as<double>(), dv.as<double>(), o, st));
+    double b2 = 0.0;
+    SCY_TRY(eta.residual_dd(drhs.as<double>(), dzN.as<double>(), dres.as<double>(), &b2));
+    const double tol = std::max(solve_opts.rtol * std::sqrt(b2), solve_opts.atol);
+    double prev = INFINITY, first_rn = -1.0, last_rn = -1.0;
+    long its_here = 0;
+    int steps = 0;
+    for (int m = 0; m <= kMaxRefine; ++m) {
+      double r2 = 0.0;
+      SCY_TRY(eta.residual_dd(drhs.as<double>(), dv.as<double>(), dres.as<double>(), &r2));
+      const double rn = std::sqrt(r2);
+      if (first_rn < 0) first_rn = rn;
+      if (rn > prev) {
+        // the last correction made it worse (rounding floor): keep the one before
+        SCY_CUDA_TRY(cudaMemcpyAsync(dv.p, dkeep.p, N * 8, cudaMemcpyDeviceToDevice, s));
+        break;
+      }
+      last_rn = rn;
+      if (rn <= tol || rn > 0.9 * prev || m == kMaxRefine) break;
+      prev = rn;
+      scy_solve_stats st{};
+      const int rc = eta.solve(dres.as<double>(), dcor.as<double>(), o, st);
+      ss_cg_its += st.iterations;
+      its_here += st.iterations;
+      ++steps;
+      if (rc != SCY_OK && rc != SCY_ERR_CG_NOCONV) return rc;
+      SCY_CUDA_TRY(cudaMemcpyAsync(dkeep.p, dv.p, N * 8, cudaMemcpyDeviceToDevice, s));
+      pl_axpy_kernel<<<grid_for(N), kBlock, 0, s>>>(dv.as<double>(), dcor.as<double>(), N);
+      SCY_LAUNCH_CHECK();
+    }
     SCY_TRY(eta.apply(SCY_OP_DY, dv.as<double>(), dgxy.as<double>()));
     SCY_TRY(eta.apply(SCY_OP_DZ, dv.as<double>(), dgxz.as<double>()));
     SCY_CUDA_TRY(cudaMemcpyAsync(gxy.data(), dgxy.p, N * 8, cudaMemcpyDeviceToHost, s));
@@ -194,6 +248,8 @@ int QDContext::pl_steady_state(const QDProblem& P, std::vector<double>& psi, std
       eff[k] = damped;
     }
     err = std::sqrt(dn) / std::sqrt(on);
+    const double bn = std::sqrt(b2) > 0 ? std::sqrt(b2) : 1.0;
+    ss_trace.insert(ss_trace.end(), {(double)steps, first_rn / bn, last_rn / bn, (double)its_here, err});
     ++it;
   }
   // updateSSb at initTime: u = v t0 (made non-negative), viscous strains

@@ -108,6 +108,10 @@ struct QDContext {
   // *its and *err report the effective-viscosity iteration
   int ss_its = 0;        // effective-viscosity iterations of the last pl_steady_state
   double ss_err = 0.0;   // and its last relative change
+  long ss_cg_its = 0;    // and the conjugate-gradient iterations of its solves
+  // per viscosity iteration: correction steps, relative residual before and
+  // after them, CG iterations, relative change of the viscosity
+  std::vector<double> ss_trace;
   int pl_steady_state(const QDProblem& P, std::vector<double>& psi, std::vector<double>& slip,
                       double* gVxy, double* gVxz, int* its, double* err);
   // computeMinTimeStep (strikeSlip_linearElastic_qd.cpp:262-322)

@@ -402,6 +402,47 @@ __global__ void dot_kernel(const Ta* __restrict__ a, const Tb* __restrict__ b, l
   grid_reduce_finish(t, partials, counter, out, sh);
 }
 
+// Error-free transformation of a sum (Knuth's TwoSum): a + b = s + e
+// exactly.  The _rn intrinsics keep the compiler from contracting or
+// reordering the operations.
+__device__ __forceinline__ void two_sum(double a, double b, double& s, double& e) {
+  s = __dadd_rn(a, b);
+  const double bb = __dsub_rn(s, a);
+  e = __dadd_rn(__dsub_rn(a, __dsub_rn(s, bb)), __dsub_rn(b, bb));
+}
+
+// r = rhs - A x over the cross form (C: 33 planes of N, offsets -8..8 along
+// y, then -8..-1 and 1..8 along z), with every product split exactly by an
+// FMA (c x = p + pe) and the sum carried as hi + lo: the rounding of A x
+// does not enter r.
+__global__ void residual_dd_kernel(const double* __restrict__ C, const double* __restrict__ x,
+                                   const double* __restrict__ rhs, double* __restrict__ r, int Ny, int Nz) {
+  const long N = (long)Ny * Nz;
+  for (long node = blockIdx.x * (long)blockDim.x + threadIdx.x; node < N; node += (long)gridDim.x * blockDim.x) {
+    const int iy = (int)(node / Nz), iz = (int)(node % Nz);
+    double hi = 0.0, lo = 0.0;
+    auto add = [&](double c, double v) {
+      const double p = __dmul_rn(c, v);
+      const double pe = fma(c, v, -p);
+      double s, e;
+      two_sum(hi, p, s, e);
+      hi = s;
+      lo = __dadd_rn(lo, __dadd_rn(e, pe));
+    };
+    for (int o = -8; o <= 8; ++o) {
+      const int jy = iy + o;
+      if (jy >= 0 && jy < Ny) add(C[(long)(o + 8) * N + node], x[(long)jy * Nz + iz]);
+    }
+    for (int o = -8; o <= 8; ++o) {
+      const int jz = iz + o;
+      if (o != 0 && jz >= 0 && jz < Nz) add(C[(long)(o < 0 ? 25 + o : 24 + o) * N + node], x[(long)iy * Nz + jz]);
+    }
+    double s, e;
+    two_sum(rhs[node], -hi, s, e);
+    r[node] = __dadd_rn(s, __dsub_rn(e, lo));
+  }
+}
+
 // x += alpha p ; r -= alpha q ; returns r.r   (alpha = rz/pq)
 __global__ void cg_update_kernel(double* __restrict__ x, double* __restrict__ r, const double* __restrict__ p,
                                  const double* __restrict__ q, const double* __restrict__ rz,
@@ -855,6 +896,7 @@ int SbpContext::rebuild() {
       }
     separable = sep ? 1 : 0;
   }
+  cross.release();
   fd.reset();
   fine.reset(new LevelStore<double>());
   SCY_TRY(fine->init(hosts[0], stream));
@@ -1028,6 +1070,34 @@ int SbpContext::solve(const double* rhs, double* u, const scy_solve_opts& o, scy
   SCY_TRY(ensure_mg(mg64));
   auto pc = [&](const double* r, double** zo) -> int { return mg64->vcycle(0, r, zo, stream); };
   return pcg<double>(pc, rhs, u, o, st);
+}
+
+int SbpContext::residual_dd(const double* rhs, const double* u, double* r, double* rnorm2_host) {
+  const LevelHost& h = hosts[0];
+  const long n = (long)h.Ny * h.Nz;
+  if (!cross.p) {
+    std::vector<double> planes;
+    build_cross_planes(h, planes);
+    SCY_TRY(cross.alloc(planes.size() * sizeof(double)));
+    SCY_CUDA_TRY(cudaMemcpyAsync(cross.p, planes.data(), planes.size() * sizeof(double), cudaMemcpyHostToDevice,
+                                 stream));
+    SCY_CUDA_TRY(cudaStreamSynchronize(stream));
+  }
+  residual_dd_kernel<<<grid_for(n, 256, 4096), 256, 0, stream>>>(cross.as<double>(), u, rhs, r, h.Ny, h.Nz);
+  SCY_LAUNCH_CHECK();
+  if (rnorm2_host) {
+    double* sc = scal.as<double>();
+    dot_kernel<double, double><<<red_blocks(n), 256, 0, stream>>>(r, r, n, red.partials.as<double>(),
+                                                                 red.counter.as<unsigned>(), sc + 6);
+    SCY_LAUNCH_CHECK();
+    SCY_CUDA_TRY(cudaMemcpyAsync(rnorm2_host, sc + 6, sizeof(double), cudaMemcpyDeviceToHost, stream));
+    SCY_CUDA_TRY(cudaStreamSynchronize(stream));
+    if (!std::isfinite(*rnorm2_host)) {
+      set_error("non-finite residual in the elliptic solve");
+      return SCY_ERR_NONFINITE;
+    }
+  }
+  return SCY_OK;
 }
 
 int SbpContext::change_bc(int R, int T, int Lb, int B) {

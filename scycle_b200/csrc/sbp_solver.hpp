@@ -125,6 +125,13 @@ struct SbpContext {
   int solve(const double* rhs, double* u, const scy_solve_opts& o, scy_solve_stats& st);
   int solve_noalloc(const double* rhs, double* u, const scy_solve_opts& o, scy_solve_stats& st);
   int change_bc(int R, int T, int L, int B);
+  // r = rhs - A u with A u summed in double-double arithmetic (error-free
+  // products and sums over the 33-point cross form) and rounded once, so r
+  // is the true residual to rounding even where ||A|| ||u|| >> ||rhs||;
+  // *rnorm2 (device or host pointer, may be NULL) gets ||r||^2 through the
+  // context's reducer.  For defect correction of ill-conditioned solves.
+  int residual_dd(const double* rhs, const double* u, double* r, double* rnorm2_host);
+  DevBuf cross;  // cross-form planes of the fine level (built on first use)
   template <typename T>
   int ensure_mg(std::unique_ptr<Multigrid<T>>& mg);
   int ensure_fd();

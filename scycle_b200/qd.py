@@ -39,6 +39,23 @@ class QD:
     def integrate_begin_from_in(self):
         S.check(S.lib().scy_qd_integrate_begin_from_in(self.h))
 
+    def steady_state_info(self):
+        """(effective-viscosity iterations, last relative change, CG
+        iterations) of the power-law steady-state guess."""
+        its, err, cg = C.c_int(), C.c_double(), C.c_long()
+        S.check(S.lib().scy_qd_steady_state_info(self.h, C.byref(its), C.byref(err), C.byref(cg)))
+        return its.value, err.value, cg.value
+
+    def steady_state_trace(self):
+        """Rows (correction steps, relative residual before, after, CG
+        iterations, viscosity change) per viscosity iteration of the
+        power-law steady-state guess."""
+        n = C.c_long()
+        S.check(S.lib().scy_qd_steady_state_trace(self.h, None, 0, C.byref(n)))
+        out = np.zeros(max(1, n.value) * 5)
+        S.check(S.lib().scy_qd_steady_state_trace(self.h, S.as_dptr(out), n.value, C.byref(n)))
+        return out[: n.value * 5].reshape(n.value, 5)
+
     def state_size(self):
         n = C.c_long()
         S.check(S.lib().scy_qd_state_size(self.h, C.byref(n)))

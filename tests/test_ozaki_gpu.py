@@ -47,7 +47,7 @@ def emulate(X, W, s):
 BOUND = {3: 1e-4, 4: 1e-6, 5: 1e-8, 6: 1e-10, 7: 1e-12}
 
 
-def _matmul(X, W, s, ldx=None, ldd=None):
+def _matmul(X, W, s, ldx=None, ldd=None, ctas=1, bf16=0):
     import torch
     rows, K = X.shape[0], W.shape[1]
     cols = W.shape[0]
@@ -56,7 +56,7 @@ def _matmul(X, W, s, ldx=None, ldd=None):
     Xd = torch.from_numpy(np.ascontiguousarray(X)).cuda()
     Dd = torch.zeros((rows, ldd), dtype=torch.float64, device="cuda")
     S.check(S.lib().scy_ozaki_matmul(C.c_void_p(Xd.data_ptr()), ldx, rows, K, S.as_dptr(np.ascontiguousarray(W)), K,
-                                     cols, s, C.c_void_p(Dd.data_ptr()), ldd))
+                                     cols, s, C.c_void_p(Dd.data_ptr()), ldd, ctas, bf16))
     return Dd.cpu().numpy()
 
 
@@ -88,3 +88,37 @@ def test_ozaki_matmul_strided_rows():
     D = _matmul(Xfull, W, 7, ldx=ldx, ldd=ldd)
     np.testing.assert_allclose(D[:, :cols], emulate(Xfull[:, :K], W, 7), rtol=1e-15, atol=1e-300)
     assert np.all(D[:, cols:] == 0.0)
+
+
+@pytest.mark.parametrize("s", [3, 4, 5])
+def test_ozaki_two_ctas_per_sm_shape_gives_the_same_product(s):
+    """The two-CTAs-per-SM shape (narrower column tiles, half the tensor
+    memory each) gives bit-for-bit the product of the one-CTA shape: the
+    digit products are exact integers and the epilogue combines them in the
+    same order."""
+    rng = np.random.default_rng(40 + s)
+    rows, K, cols = 700, 401, 401
+    X = rng.standard_normal((rows, K)) * np.exp(2 * rng.standard_normal((rows, 1)))
+    W = rng.standard_normal((cols, K))
+    D1 = _matmul(X, W, s, ctas=1)
+    D2 = _matmul(X, W, s, ctas=2)
+    assert np.array_equal(D1, D2)
+    np.testing.assert_allclose(D2, emulate(X, W, s), rtol=1e-15, atol=1e-300)
+
+
+@pytest.mark.parametrize("s", [3, 4, 5, 6, 7])
+@pytest.mark.parametrize("ctas", [1, 2])
+def test_ozaki_bf16_digits_give_the_same_product(s, ctas):
+    """The digits held in bf16 and multiplied with FP32 accumulation
+    (kind::f16) give bit-for-bit the integer product (kind::i8): every
+    partial sum stays below 2^24 at K = 401."""
+    if ctas == 2 and s > 5:
+        pytest.skip("two CTAs per SM only for S <= 5")
+    rng = np.random.default_rng(60 + s)
+    rows, K, cols = 600, 401, 401
+    X = rng.standard_normal((rows, K)) * np.exp(2 * rng.standard_normal((rows, 1)))
+    X[5] = 0.0
+    W = rng.standard_normal((cols, K))
+    D8 = _matmul(X, W, s, ctas=ctas, bf16=0)
+    D16 = _matmul(X, W, s, ctas=ctas, bf16=1)
+    assert np.array_equal(D8, D16)

@@ -140,3 +140,37 @@ def test_pl_steady_state_guess_matches_oracle(tmp_path, grid):
     d0 = ora.d_dt(P["driver"]["initTime"], {k: v.copy() for k, v in var.items()})
     assert _nrel(dev.field("slipVel"), d0["slip"]) <= 1e-8
     assert _nrel(dev.field("tauP"), ora.fault.tauP) <= 1e-8
+
+
+@pytest.mark.parametrize("grid", ["constantGridSpacing", "variableGridSpacing"])
+def test_pl_steady_state_guess_at_the_default_viscosity_cap(tmp_path, grid):
+    """guessSteadyStateICs = 1 at the reference's default cap maxEffVisc =
+    1e30 (powerLaw.cpp:757): the effective viscosity spans about fourteen
+    decades and is far from a product a(y) b(z), and the steady velocity is
+    ill-conditioned enough that the oracle's own answer moves between plain
+    and refined direct solves (its spread).  The device (multigrid-
+    preconditioned conjugate gradients, warm-started and restarted from a
+    fresh true residual until the residual stops falling) must land within
+    ten times that spread of the oracle, with the same number of viscosity
+    iterations give or take one (the stopping test compares a relative
+    change with 1e-3)."""
+    path = _problem(tmp_path, grid, n=25, nz=25, extra={"guessSteadyStateICs": "1", "maxEffVisc": "1e30"})
+    P = build_pl_problem(open(path).read())
+    runs = []
+    for refine in (0, 2):
+        o = PowerLawQD(P, keep_history=False, refine=refine)
+        var = o.initiate_integrand()
+        d0 = o.d_dt(P["driver"]["initTime"], {k: v.copy() for k, v in var.items()})
+        runs.append((o, dict(var, slipVel=d0["slip"], tauP=o.fault.tauP.copy())))
+    (ora, ref), (_, fine) = runs
+    assert ora.effVisc.max() / ora.effVisc.min() > 1e12
+    dev = _device(path)
+    dev.integrate_begin_from_in()
+    its, err, cg = dev.steady_state_info()
+    assert abs(its - ora.ss_its) <= 1, (its, ora.ss_its)
+    assert err < P["ss"]["atolSS_effVisc"]
+    assert cg > 0
+    for nm in ("gVxy", "gVxz", "psi", "slip", "slipVel", "tauP"):
+        spread = _nrel(fine[nm], ref[nm])
+        e = _nrel(dev.field(nm), ref[nm])
+        assert e <= max(1e-8, 10.0 * spread), (nm, e, spread)

@@ -119,6 +119,27 @@ def test_fast_diagonalisation_on_separable_stretched_grid(precision):
     assert _rel(u.cpu().numpy(), ref) <= 1e-10
 
 
+def test_fast_diagonalisation_of_a_product_shear_modulus():
+    """mu = a(y) b(z) (here b spans two decades, a a factor three): the
+    fast diagonalisation fits log mu as alpha(y) + beta(z) and weights the
+    two directions' operators and masses by the fitted factors, which makes
+    it exact for a product up to the mu3 column, so CG needs few
+    iterations where the plain averages of mu would not be close."""
+    import scipy.sparse.linalg as spla
+    from scycle_b200.sbp import SbpOps
+    Ny, Nz = 81, 73
+    yy = np.linspace(0.0, 1.0, Ny)[:, None]
+    zz = np.linspace(0.0, 1.0, Nz)[None, :]
+    mu = (32.04 * (1.0 + 2.0 * yy) * 10.0 ** (2.0 * zz ** 2)).ravel()
+    dev = SbpOps(4, Ny, Nz, 30.0, 24.0, mu)
+    ora = OracleSbp(4, Ny, Nz, 30.0, 24.0, mu)
+    rhs = ora.set_rhs(np.linspace(0, 1, Nz), np.full(Nz, 0.3), np.zeros(Ny), np.zeros(Ny))
+    ref = spla.spsolve(ora.A.tocsc(), rhs)
+    u, st = dev.solve(rhs, rtol=1e-12, max_its=200, precond="fd")
+    assert st.converged and st.iterations <= 40, st.iterations
+    assert _rel(u.cpu().numpy(), ref) <= 1e-9
+
+
 def test_change_bc_types_rebuilds_operator():
     dev, ora, rng = _case(4, "constantGridSpacing", 45, 37)
     dev.change_bc_types("Neumann", "Neumann", "Neumann", "Neumann")
