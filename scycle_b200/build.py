@@ -7,7 +7,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libscycle_b200.so")
 SOURCES = ["capi.cu", "sbp_solver.cu", "sbp_host.cpp", "qd.cu", "infile.cpp", "noalloc.cu", "fdiag.cu", "cycle.cu",
-           "cycle_host.cpp", "powerlaw.cu", "batch.cu", "adjoint.cu", "writer.cu", "ozaki.cu", "thermal_host.cpp", "thermal.cu"]
+           "cycle_host.cpp", "powerlaw.cu", "batch.cu", "adjoint.cu", "writer.cu", "ozaki.cu", "thermal_host.cpp", "thermal.cu",
+           "blockchol.cu"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC", "-Xcompiler", "-O3", "--expt-relaxed-constexpr"]
 

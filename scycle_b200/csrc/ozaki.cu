@@ -133,7 +133,7 @@ template <int S, typename T, int PAIR, int BF>
 __global__ void __launch_bounds__(128, PAIR ? 2 : 1)
     ozk_gemm_kernel(const __grid_constant__ CUtensorMap mx, const __grid_constant__ CUtensorMap mw,
                     const int* __restrict__ ex, const int* __restrict__ ew, T* __restrict__ D, long ldd, int rows,
-                    int cout, int nkb, unsigned* __restrict__ status, int rows_per_status, unsigned bit) {
+                    int cout, int nks, unsigned* __restrict__ status, int rows_per_status, unsigned bit) {
   constexpr int CN = ozk_cn(S, PAIR);
   constexpr int XB = S * OZK_BM * OZK_BK;
   constexpr int WB = S * CN * OZK_BK;
@@ -151,7 +151,11 @@ __global__ void __launch_bounds__(128, PAIR ? 2 : 1)
   // tiles on a 1024- or 512-byte boundary (the swizzle pattern repeats every 512 B)
   unsigned char* smem = ozk_smem_raw + ((AL - (smem_u32(ozk_smem_raw) & (AL - 1))) & (AL - 1));
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int m0 = blockIdx.x * OZK_BM, c0 = blockIdx.y * CN;
+  // column tiles vary fastest (the CTAs that run together share a row tile
+  // of X and spread over the tiles of W), and each CTA starts its K loop at
+  // its own stage (integer partial sums are exact in any order), so the
+  // CTAs reading one W tile at a time read different parts of it
+  const int c0 = blockIdx.x * CN, m0 = blockIdx.y * OZK_BM;
 
   if (threadIdx.x == 0) {
     for (int i = 0; i < ST; ++i) {
@@ -173,12 +177,18 @@ __global__ void __launch_bounds__(128, PAIR ? 2 : 1)
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_slot;
 
+  // K in 32-byte MMA steps (nks), two per 64-byte stage; the last stage may
+  // hold one.  N of the products: the tile's columns rounded up to 16 (the
+  // last column tile is narrower than CN)
+  const int nkb = (nks + 1) / 2;
+  const int rot = (int)((blockIdx.x * 7u + blockIdx.y) % (unsigned)nkb);
+  const int nmma = max(32, min(CN, (cout - c0 + 15) / 16 * 16));
   int issued = 0;
   if (warp == 0 && lane == 0) {
     // producer
-    for (int kb = 0; kb < nkb; ++kb) {
-      const int st = kb % ST;
-      if (kb >= ST && !mbar_wait(&empty[st], ((kb / ST) - 1) & 1, OZK_POLLS)) {
+    for (int q = 0; q < nkb; ++q) {
+      const int st = q % ST, kb = (q + rot) % nkb;
+      if (q >= ST && !mbar_wait(&empty[st], ((q / ST) - 1) & 1, OZK_POLLS)) {
         failed = 1;
         break;
       }
@@ -191,11 +201,11 @@ __global__ void __launch_bounds__(128, PAIR ? 2 : 1)
     }
   } else if (warp == 1 && lane == 0) {
     // MMA issuer
-    constexpr uint32_t idesc = BF ? umma_idesc_bf16(CN) : umma_idesc_s8(CN);
-    int kb = 0;
-    for (; kb < nkb; ++kb) {
-      const int st = kb % ST;
-      if (!mbar_wait(&full[st], (kb / ST) & 1, OZK_POLLS)) {
+    const uint32_t idesc = BF ? umma_idesc_bf16(nmma) : umma_idesc_s8(nmma);
+    int q = 0;
+    for (; q < nkb; ++q) {
+      const int st = q % ST, kb = (q + rot) % nkb;
+      if (!mbar_wait(&full[st], (q / ST) & 1, OZK_POLLS)) {
         failed = 1;
         break;
       }
@@ -203,7 +213,8 @@ __global__ void __launch_bounds__(128, PAIR ? 2 : 1)
       const uint32_t xa = smem_u32(smem + st * (XB + WB));
       const uint32_t wa = xa + XB;
 #pragma unroll
-      for (int ks = 0; ks < 2; ++ks)
+      for (int ks = 0; ks < 2; ++ks) {
+        if (2 * kb + ks >= nks) break;
 #pragma unroll
         for (int g = 0; g < S; ++g)
 #pragma unroll
@@ -212,19 +223,20 @@ __global__ void __launch_bounds__(128, PAIR ? 2 : 1)
             const uint64_t ad = umma_desc_sw64(xa + (i - 1) * OZK_BM * OZK_BK + ks * 32);
             const uint64_t bd = umma_desc_sw64(wa + (j - 1) * CN * OZK_BK + ks * 32);
             if (BF)
-              umma_bf16(tmem + g * CN, ad, bd, idesc, (kb > 0 || ks > 0 || i > 1) ? 1u : 0u);
+              umma_bf16(tmem + g * CN, ad, bd, idesc, (q > 0 || ks > 0 || i > 1) ? 1u : 0u);
             else
-              umma_s8(tmem + g * CN, ad, bd, idesc, (kb > 0 || ks > 0 || i > 1) ? 1u : 0u);
+              umma_s8(tmem + g * CN, ad, bd, idesc, (q > 0 || ks > 0 || i > 1) ? 1u : 0u);
           }
+      }
       umma_commit(&empty[st]);
     }
-    consumed = kb;
+    consumed = q;
     umma_commit(&done);  // arrives once every product issued above has completed
   }
   __syncthreads();
   if (warp == 0 && lane == 0) {
     // copies issued but never consumed (only after a wait ran out)
-    for (int kb = consumed; kb < issued; ++kb) mbar_wait(&full[kb % ST], (kb / ST) & 1, OZK_POLLS);
+    for (int q = consumed; q < issued; ++q) mbar_wait(&full[q % ST], (q / ST) & 1, OZK_POLLS);
   }
   // one verdict for the whole block: the warp-collective tensor-memory
   // loads below run in every warp or in none
@@ -249,7 +261,7 @@ __global__ void __launch_bounds__(128, PAIR ? 2 : 1)
     const double xs = row < rows ? pow2i(ex[row]) : 0.0;
     const uint32_t tl = tmem + ((uint32_t)(warp * 32) << 16);
 #pragma unroll 1
-    for (int cc = 0; cc < CN; cc += 16) {
+    for (int cc = 0; cc < nmma; cc += 16) {
       uint32_t v[S][16];
 #pragma unroll
       for (int g = 0; g < S; ++g) tmem_ld16(tl + g * CN + cc, v[g]);
@@ -281,62 +293,37 @@ __global__ void __launch_bounds__(128, PAIR ? 2 : 1)
   if (warp == 1) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "n"(TC) : "memory");
 }
 
-// digits of one row per warp: lane l holds the K positions 4 l + 128 j + q
-// (q < 4, j < 8, so K <= 1024) in registers, read once; the row maximum is
-// a warp reduction, and the four digits of a position group and plane go
-// out as one 32-bit word (a warp stores 128 consecutive bytes)
+// digits of one row per warp, in two coalesced passes over the row (the
+// second from L1): lane l takes the positions 32 t + l, so every load and
+// every digit store of the warp covers consecutive addresses.  The first
+// pass gives the row maximum (a warp reduction) and so the row's exponent;
+// the second writes the S digits of each position (one byte, or the two
+// bytes of the digit's bf16 pattern: the upper half of its FP32 pattern,
+// exact for |d| <= 256).  No per-lane arrays, so many rows are in flight
+// per SM.
 template <typename Tin, int BF>
-__global__ void ozk_split_kernel(const Tin* __restrict__ X, long ldx, int rows, int K, int Kp, int S,
-                                 unsigned char* __restrict__ dig, long plane, int* __restrict__ expo) {
+__global__ void __launch_bounds__(256) ozk_split_kernel(const Tin* __restrict__ X, long ldx, int rows, int K, int Kp,
+                                                        int S, unsigned char* __restrict__ dig, long plane,
+                                                        int* __restrict__ expo) {
   const int row = (int)((blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5);
   const int lane = threadIdx.x & 31;
   if (row >= rows) return;
   const Tin* x = X + (long)row * ldx;
-  double v[8][4];
   double m = 0.0;
-#pragma unroll
-  for (int j = 0; j < 8; ++j) {
-    const int k0 = 4 * lane + 128 * j;
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      v[j][q] = (k0 + q < K) ? (double)x[k0 + q] : 0.0;
-      m = fmax(m, fabs(v[j][q]));
-    }
-  }
+  for (int k = lane; k < K; k += 32) m = fmax(m, fabs((double)x[k]));
   m = warp_max(m);
   const int e = m > 0.0 ? ilogb(m) + 2 : 0;
   if (lane == 0) expo[row] = e;
-  // digit element size: 1 byte, or 2 (bf16 bit pattern of the integer: the
-  // upper half of its FP32 pattern, exact for |d| <= 256)
-  constexpr int ES = BF ? 2 : 1;
-  unsigned char* drow = dig + (long)row * Kp * ES;
-#pragma unroll
-  for (int j = 0; j < 8; ++j) {
-    const int k0 = 4 * lane + 128 * j;
-    if (k0 >= Kp) break;
-    double t[4];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) t[q] = ldexp(v[j][q], 7 - e);
+  for (int k = lane; k < Kp; k += 32) {
+    double t = k < K ? ldexp((double)x[k], 7 - e) : 0.0;
     for (int i = 0; i < S; ++i) {
-      uint32_t w = 0, w2 = 0;
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const double d = rint(t[q]);
-        t[q] = (t[q] - d) * 128.0;
-        if (BF) {
-          const uint32_t b = __float_as_uint((float)d) >> 16;
-          if (q < 2)
-            w |= b << (16 * q);
-          else
-            w2 |= b << (16 * (q - 2));
-        } else {
-          w |= ((uint32_t)(int)d & 0xFFu) << (8 * q);
-        }
-      }
+      const double d = rint(t);
+      t = (t - d) * 128.0;
+      const long at = (long)i * plane + (long)row * Kp + k;
       if (BF)
-        *reinterpret_cast<uint2*>(drow + (i * plane + k0) * 2) = make_uint2(w, w2);
+        reinterpret_cast<uint16_t*>(dig)[at] = (uint16_t)(__float_as_uint((float)d) >> 16);
       else
-        *reinterpret_cast<uint32_t*>(drow + i * plane + k0) = w;
+        reinterpret_cast<int8_t*>(dig)[at] = (int8_t)(int)d;
     }
   }
 }
@@ -380,9 +367,9 @@ int launch_gemm(const OzkOperand& x, const CUtensorMap& wmap, const OzkOperand& 
     const int rc = prepare_one<S, T, PAIR, BF>();
     if (rc != SCY_OK) return rc;
   }
-  const dim3 grid((x.rows + OZK_BM - 1) / OZK_BM, (cout + CN - 1) / CN);
+  const dim3 grid((cout + CN - 1) / CN, (x.rows + OZK_BM - 1) / OZK_BM);
   ozk_gemm_kernel<S, T, PAIR, BF><<<grid, 128, ozk_smem_bytes(S, PAIR), s>>>(
-      x.map, wmap, x.expo.as<int>(), w.expo.as<int>(), D, ldd, x.rows, cout, x.Kp * x.esz / OZK_BK, status,
+      x.map, wmap, x.expo.as<int>(), w.expo.as<int>(), D, ldd, x.rows, cout, x.Kp * x.esz / 32, status,
       rows_per_status, bit);
   SCY_LAUNCH_CHECK();
   return SCY_OK;
@@ -456,7 +443,7 @@ int OzkOperand::alloc_weights(int S_, int rows_, int K_, int esz_) {
 }
 
 bool ozk_bf16_exact(int S, int K) {
-  const long Kp = (K + OZK_BK / 2 - 1) / (OZK_BK / 2) * (OZK_BK / 2);
+  const long Kp = (K + 15) / 16 * 16;
   return (long)S * 64 * 64 * Kp < (1L << 24);
 }
 
@@ -471,8 +458,9 @@ int OzkOperand::alloc(int S_, int rows_, int K_, int box_rows_, int esz_) {
   rows = rows_;
   K = K_;
   esz = esz_;
-  const int kq = OZK_BK / esz;  // digits per 64-byte stage row
-  Kp = (K + kq - 1) / kq * kq;
+  const int kq = OZK_BK / esz;  // digits per 64-byte stage row (the TMA box; zero-filled past Kp)
+  const int ke = 32 / esz;      // digits per MMA K step
+  Kp = (K + ke - 1) / ke * ke;
   box_rows = box_rows_;
   plane = (long)rows * Kp;
   SCY_TRY(dig.alloc((size_t)S * plane * esz));

@@ -29,11 +29,12 @@
 
 namespace scy {
 
-// One operand in digit form: S planes of rows x Kp signed bytes (Kp = K
-// rounded up to 64; zero beyond K), a power-of-two exponent per row, and the
-// 3D TMA map (bytes of a row, rows, planes) with a box of 64 bytes x
-// box_rows rows x S planes and 64-byte swizzling (the K-major canonical
-// layout the tensor cores read).
+// One operand in digit form: S planes of rows x Kp digits (signed bytes,
+// or bf16; Kp = K rounded up to 32 bytes of digits, zero beyond K), a
+// power-of-two exponent per row, and the 3D TMA map (digits of a row, rows,
+// planes) with a box of 64 bytes x box_rows rows x S planes (zero-filled
+// past Kp) and 64-byte swizzling (the K-major canonical layout the tensor
+// cores read).
 struct OzkOperand {
   DevBuf dig, expo;
   int S = 0, rows = 0, K = 0, Kp = 0, box_rows = 0, box_rows_pair = 0;
@@ -41,15 +42,15 @@ struct OzkOperand {
   long plane = 0;  // digits of one plane (rows x Kp)
   CUtensorMap map, map_pair;
   // box_rows: 128 for the row operand (X), the column tile width of S
-  // (ozk_cols_per_tile) for the weights (W); Kp = K rounded up to 64 bytes
-  // of digits
+  // (ozk_cols_per_tile) for the weights (W); Kp = K rounded up to 32 bytes
+  // of digits (one MMA K step)
   int alloc(int S, int rows, int K, int box_rows, int esz = 1);
   // the weights' operand (W) with the maps of both product shapes
   int alloc_weights(int S, int rows, int K, int esz = 1);
 };
 
 // bf16 digits give exact FP32 accumulation for S planes and K (every
-// partial sum below 2^24: S * 64 * 64 * Kp < 2^24)
+// partial sum below 2^24: S * 64 * 64 * Kp < 2^24, Kp = K rounded up to 16)
 bool ozk_bf16_exact(int S, int K);
 
 // column tile width of the product for S digit planes: one CTA per SM

@@ -12,6 +12,7 @@
 // matrix-free: yq zr H = wy * wz, zr Hz = wy and yq Hy = wz in terms of the
 // operator's outer weights (wy = Hz zr, wz = Hy yq; zr = yq = 1 on the
 // constant grid), Dy = qy Dq and Dz = rz Dr.
+#include "blockchol.hpp"
 #include <algorithm>
 #include <cmath>
 
@@ -161,13 +162,16 @@ int QDContext::pl_steady_state(const QDProblem& P, std::vector<double>& psi, std
   // The viscosity spans many decades (up to the cap, 1e30 by default,
   // powerLaw.cpp:757) and is far from separable; the stresses the update
   // reads are products of that viscosity with small velocity gradients, so
-  // the velocity is needed to the accuracy of a direct solve.  Each solve
-  // is a defect correction: the residual in double-double arithmetic
-  // (SbpContext::residual_dd), a correction by preconditioned CG (multigrid
-  // unless the caller chose another preconditioner) to a relative 1e-6,
-  // repeated until the residual meets the solve tolerance or stops
-  // falling.  The first residual of each iteration is that of the previous
-  // iteration's velocity (a warm start).
+  // the velocity is needed to the accuracy of a direct solve, which is what
+  // the reference runs here (MUMPS Cholesky, powerLaw.cpp:2111-2116).  Each
+  // solve is a defect correction: the residual in double-double arithmetic
+  // (SbpContext::residual_dd) and a correction by the block Cholesky
+  // factorisation of this iteration's operator (BlockChol; by
+  // preconditioned CG to a relative 1e-6 when the caller chose a
+  // preconditioner or the factor would not fit in a third of the free
+  // device memory), repeated until the residual meets the solve tolerance
+  // or stops falling, and at least once.  The first residual of each
+  // iteration is that of the previous iteration's velocity (a warm start).
   const int kMaxRefine = 30;
   scy_solve_opts o = solve_opts;
   o.verify = 1;
@@ -185,6 +189,12 @@ int QDContext::pl_steady_state(const QDProblem& P, std::vector<double>& psi, std
   SCY_CUDA_TRY(cudaMemsetAsync(dzN.p, 0, N * 8, s));
   SCY_CUDA_TRY(cudaMemsetAsync(dv.p, 0, N * 8, s));
   std::vector<double> gxy((size_t)N), gxz((size_t)N), v((size_t)N), sxy_h((size_t)N), sxz_h((size_t)N);
+  bool direct = solve_opts.precond == SCY_PC_AUTO;
+  if (direct) {
+    size_t fr = 0, tot = 0;
+    SCY_CUDA_TRY(cudaMemGetInfo(&fr, &tot));
+    direct = BlockChol::bytes_for(Ny, Nz) < (double)fr / 3.0;
+  }
   int it = 0;
   double err = 1e10;
   while (it < P.ss_max_its && err >= P.ss_atol) {
@@ -195,6 +205,8 @@ int QDContext::pl_steady_state(const QDProblem& P, std::vector<double>& psi, std
     eta.stream = s;
     SCY_TRY(eta.set_rhs(dbcL.as<double>(), dbcR.as<double>(), dzero.as<double>(), dzero.as<double>(),
                         drhs.as<double>()));
+    BlockChol chol;
+    if (direct) SCY_TRY(chol.factor(eta.hosts[0], s));
     double b2 = 0.0;
     SCY_TRY(eta.residual_dd(drhs.as<double>(), dzN.as<double>(), dres.as<double>(), &b2));
     const double tol = std::max(solve_opts.rtol * std::sqrt(b2), solve_opts.atol);
@@ -212,14 +224,21 @@ int QDContext::pl_steady_state(const QDProblem& P, std::vector<double>& psi, std
         break;
       }
       last_rn = rn;
-      if (rn <= tol || rn > 0.9 * prev || m == kMaxRefine) break;
+      // at least one correction: with this contrast the relative residual
+      // barely sees the soft region, so a warm start that already meets the
+      // tolerance can still be far from this iteration's velocity there
+      if ((m > 0 && rn <= tol) || rn > 0.9 * prev || m == kMaxRefine) break;
       prev = rn;
-      scy_solve_stats st{};
-      const int rc = eta.solve(dres.as<double>(), dcor.as<double>(), o, st);
-      ss_cg_its += st.iterations;
-      its_here += st.iterations;
+      if (direct) {
+        SCY_TRY(chol.solve(dres.as<double>(), dcor.as<double>(), s));
+      } else {
+        scy_solve_stats st{};
+        const int rc = eta.solve(dres.as<double>(), dcor.as<double>(), o, st);
+        ss_cg_its += st.iterations;
+        its_here += st.iterations;
+        if (rc != SCY_OK && rc != SCY_ERR_CG_NOCONV) return rc;
+      }
       ++steps;
-      if (rc != SCY_OK && rc != SCY_ERR_CG_NOCONV) return rc;
       SCY_CUDA_TRY(cudaMemcpyAsync(dkeep.p, dv.p, N * 8, cudaMemcpyDeviceToDevice, s));
       pl_axpy_kernel<<<grid_for(N), kBlock, 0, s>>>(dv.as<double>(), dcor.as<double>(), N);
       SCY_LAUNCH_CHECK();
