@@ -280,10 +280,10 @@ def run_batched(args, dist, rank, world, local):
     if peak is None:
         peak, peak_src = 6650.0, "fallback"
     # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of
-    # one ncu capture of these kernels at 32 instances of the 401 x 401
-    # workload (profiles/batched_ensemble_kernels_401x401.md); other sizes
-    # report none
-    traffic = {"ysolve": 65362176.0, "matvec": 178643456.0, "residual": 187187968.0} \
+    # ncu captures of these kernels at 32 instances of the 401 x 401 workload
+    # (profiles/batched_ensemble_kernels_401x401.md,
+    # profiles/ozk_gemm_kernel_S5_12832x401x401.md); other sizes report none
+    traffic = {"ysolve": 65362176.0, "matvec": 178643456.0, "residual": 187187968.0, "ztransform": 28774656.0} \
         if (args.batch == 32 and args.n == 401) else {}
     kern = {}
     for nm, desc in (("ysolve", "b_ysolve_tma_kernel (banded Cholesky sweeps along y of the preconditioner)"),
@@ -470,7 +470,41 @@ def run_ensemble_c3(args, dist, rank, world, local):
            "setup_s": setup_s, "cg_its": st1.cg_its, "rounds": st1.rounds - st0.rounds,
            "redo_rounds": st1.redo_rounds - st0.redo_rounds, "precision": args.batch_precision}
     b.close()
+    if rank == 0 and not args.no_pl_ss:
+        out["steady_state_guess_1e30"] = run_pl_steady_state()
     return out
+
+
+def run_pl_steady_state():
+    """The power-law steady-state initial guess at the reference's default
+    viscosity cap (maxEffVisc = 1e30) for one instance of each grid size of
+    the power-law ensemble (geotherm 22.5 K/km, seed 0): the effective-
+    viscosity iteration with a direct solve of the non-separable viscosity
+    operator per iteration (block Cholesky with double-double defect
+    correction), timed end to end."""
+    import torch
+    from scycle_b200.configs import make_pl_problem
+    from scycle_b200.qd import QD
+    res = []
+    for n in (101, 201, 301):
+        work = tempfile.mkdtemp(prefix="scy_plss_")
+        path = make_pl_problem(work, Ny=n, Nz=n, grad=22.5, extra={"guessSteadyStateICs": "1", "maxDeltaT": "1e6"})
+        q = QD.from_in(path, solve_rtol=1e-12)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        q.integrate_begin_from_in()
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        its, err, _ = q.steady_state_info()
+        tr = q.steady_state_trace()
+        eff = q.field("effVisc")
+        res.append({"n": n, "wall_s": wall, "iterations": its, "last_change": err,
+                    "corrections": int(tr[:, 0].sum()), "max_rel_residual": float(tr[:, 2].max()),
+                    "effVisc_decades": float(np.log10(eff.max() / eff.min()))})
+        q.close()
+    return {"cases": res, "note": "set-up (once per run); the time-step operator of the power-law driver is "
+                                  "built on the shear modulus (powerLaw.cpp:1110-1113), the viscosity enters "
+                                  "through the viscous strain rates, so only this guess solves a viscosity operator"}
 
 
 C4_WORKLOAD = ("adjoint_c4: 201x201 linear-elastic quasi-dynamic, constant grid, aging law, steady-state initial "
@@ -1057,6 +1091,8 @@ def main():
     ap.add_argument("--c3", type=int, default=128, help="instances of the power-law ensemble (0: skip)")
     ap.add_argument("--c3-only", action="store_true", help="measure the power-law ensemble alone")
     ap.add_argument("--c3-steps", type=int, default=50, help="timed steps of the power-law ensemble")
+    ap.add_argument("--no-pl-ss", action="store_true",
+                    help="skip the power-law steady-state guess at the default viscosity cap")
     ap.add_argument("--c4-steps", type=int, default=2000, help="RK32 steps of the adjoint workload (0: skip)")
     ap.add_argument("--c4-dirs", type=int, default=10, help="finite-difference directions of the adjoint check")
     ap.add_argument("--c4-only", action="store_true", help="run the adjoint workload alone")

@@ -645,6 +645,14 @@ enum { SCY_BATCH_KERNEL_YSOLVE = 0, SCY_BATCH_KERNEL_RESIDUAL = 1, SCY_BATCH_KER
 scy_status scy_batch_profile_collect(scy_batch* b, int kernel, double* ms, long long* launches, double* bytes);
 /* Drops the recorded launches. */
 scy_status scy_batch_profile_clear(scy_batch* b);
+/* Test hook (no counterpart in the reference): limits the polls of the
+ * banded sweeps' data waits (default 2^18).  A wait that runs out marks its
+ * instances (status bit 4) and the round is repeated; after three repeats
+ * scy_batch_run returns SCY_ERR_TIMEOUT.  With polls = 1 the waits run out at
+ * once, exercising that path without a hang; the copies already issued are
+ * still awaited at the full limit before a block exits. */
+scy_status scy_batch_set_sweep_polls(scy_batch* b, int polls);
+
 /* The autotuner's choices for group g (no counterpart in the reference): at
  * set-up every group times, on its own buffers, the CG operator kernel with
  * 1, 2, 4 and 8 instances per block, the banded sweeps in three launch

@@ -141,6 +141,7 @@ def declare_batch(L):
     L.scy_batch_set_states.argtypes = [vp, dptr]
     L.scy_batch_get_fault_field.argtypes = [vp, C.c_int, dptr]
     L.scy_batch_set_graphs.argtypes = [vp, C.c_int]
+    L.scy_batch_set_sweep_polls.argtypes = [vp, C.c_int]
     L.scy_batch_profile.argtypes = [vp, C.c_int]
     L.scy_batch_profile_collect.argtypes = [vp, C.c_int, dptr, C.POINTER(C.c_longlong), dptr]
     L.scy_batch_profile_clear.argtypes = [vp]

@@ -1055,10 +1055,10 @@ int BatchContext::launch_ysolve(BatchGroup& g, int variant) {
     if (f32)                                                                                                        \
       b_ysolve_tma_kernel<float, I, W><<<grid, 32 * W, sm, g.stream>>>(g.mLcol32, g.mLrow32, g.mT32,               \
                                                                        g.t1pf.as<float>(), Ny, Nz, F.Nzp, K,        \
-                                                                       g.w.status);                                 \
+                                                                       g.w.status, sweep_polls);                    \
     else                                                                                                            \
       b_ysolve_tma_kernel<double, I, W><<<grid, 32 * W, sm, g.stream>>>(g.mLcol, g.mLrow, g.mT, g.t1p.as<double>(), \
-                                                                        Ny, Nz, F.Nzp, K, g.w.status);              \
+                                                                        Ny, Nz, F.Nzp, K, g.w.status, sweep_polls); \
   } while (0)
   static_assert(2 * 2 * 2 == YS_B && 2 * 4 * 1 == YS_B && 2 * 1 * 4 == YS_B, "sweep variants serve YS_B instances");
   if (variant == 1)
@@ -1673,6 +1673,12 @@ int BatchContext::run(long nsteps, scy_batch_stats* st) {
       SCY_TRY(check_fault_flags());
       const int redo_its = std::min(max_its, (attempt == 0 ? 2 : 8) * its_round);
       if (attempt == 2 || redo_its <= its_round) {
+        unsigned bits = 0;
+        for (int i = 0; i < n; ++i) bits |= (unsigned)err_host[16 * i + 15];
+        if (bits & 4u) {
+          set_error("batched stage solve: a bounded pipeline wait in a kernel ran out in three repeated rounds");
+          return SCY_ERR_TIMEOUT;
+        }
         set_error("batched stage solve missed its tolerance after %d CG iterations", redo_its);
         return SCY_ERR_CG_NOCONV;
       }
@@ -1803,6 +1809,16 @@ scy_status scy_batch_set_states(scy_batch* b, const double* host) {
 scy_status scy_batch_get_fault_field(scy_batch* b, int field, double* host) {
   if (!b || !host) return SCY_ERR_ARG;
   return b->ctx.get_fault_field(field, host);
+}
+
+scy_status scy_batch_set_sweep_polls(scy_batch* b, int polls) {
+  if (!b || polls < 1) return SCY_ERR_ARG;
+  b->ctx.sweep_polls = polls;
+  // captured rounds hold the old limit
+  SCY_CUDA_TRY(cudaStreamSynchronize(b->ctx.stream));
+  for (auto& kv : b->ctx.graph_of_its) cudaGraphExecDestroy(kv.second);
+  b->ctx.graph_of_its.clear();
+  return SCY_OK;
 }
 
 scy_status scy_batch_set_graphs(scy_batch* b, int on) {

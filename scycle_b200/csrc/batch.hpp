@@ -147,6 +147,7 @@ struct BatchContext {
     double bytes;  // algorithmic bytes of the launch
   };
   int prof = 0;
+  int sweep_polls = 1 << 18;  // polls of the banded sweeps' data waits (lowered only by a test hook)
   std::vector<ProfRec> precs;
   int active_in(const BatchGroup& g, const int* mask) const;  // instances of g the mask selects this round
   int prof_begin(cudaStream_t s, cudaEvent_t* a);

@@ -57,7 +57,8 @@ __global__ void __launch_bounds__(32 * W) b_ysolve_tma_kernel(const __grid_const
                                                               const __grid_constant__ CUtensorMap mLrow,
                                                               const __grid_constant__ CUtensorMap mT,
                                                               T* __restrict__ t, int Ny, int Nz, int Nzp, int K,
-                                                              unsigned* __restrict__ status) {
+                                                              unsigned* __restrict__ status,
+                                                              int first_polls = 1 << 18) {
   constexpr int B = 2 * W * I;
   extern __shared__ __align__(128) unsigned char ys_smem[];
   constexpr int CT = YS_R * 9 * YS_C, DT = B * YS_R * YS_C;  // elements per tile
@@ -139,7 +140,7 @@ __global__ void __launch_bounds__(32 * W) b_ysolve_tma_kernel(const __grid_const
       reset();
     }
     const int st = g % YS_S;
-    ok = mbar_wait(&bar[st], (g / YS_S) & 1, kPolls);
+    ok = mbar_wait(&bar[st], (g / YS_S) & 1, first_polls);
     if (__syncthreads_or(!ok)) {
       ok = false;
       break;

@@ -123,3 +123,39 @@ def test_batched_c1_instance_matches_oracle(tmp_path):
         _check(v, fx, k, worst)
     b.close()
     assert max(w["ratio"] for w in worst.values()) <= 1.0, ("batch c1", worst)
+
+
+def test_cycle_first_quasi_dynamic_phase_801():
+    """Config 2's first quasi-dynamic phase at 801x801 (qdfd_const_801, seed
+    0) into its first event: the device cycle driver in solve mode, forced
+    onto the oracle's attempts (tests/golden/make_cycle801_fixture.py), with
+    the reference's Newton path.  Nucleation amplifies rounding roughly like
+    the slip velocity grows, so the bar is 1e3 times the oracle's own
+    divergence from a 1e-13 perturbation of its initial slip (and 1e-9
+    while that is smaller), as in tests/test_cycle_gpu.py; the switch into
+    the wave equation must come at the oracle's step and time."""
+    import tempfile
+    from scycle_b200.cycle import Cycle
+    fx = _fixture("c2qd")
+    work = tempfile.mkdtemp(prefix="c2qd_")
+    path = configs.qdfd_const_801(work, seed=0, cycles=3, years=1000.0)
+    c = Cycle.from_in(path, solve_rtol=SOLVE_RTOL, solve_max_its=2000, exact_jacobian=False)
+    c.force_attempts(list(zip(fx["attempt_dt"].tolist(), fx["attempt_acc"].astype(bool).tolist())))
+    c.begin_from_in()
+    first = int(fx["switch_step"])
+    step = 0
+    worst = {}
+    for i, k in enumerate(fx["snap_steps"].tolist()):
+        st = c.run(k - step)
+        step = k
+        assert st.step_count == k
+        assert abs(st.t - fx["snap_t"][i]) <= 1e-12 * abs(fx["snap_t"][i])
+        for f in FIELDS:
+            e = float(np.linalg.norm(c.field(f) - fx[f][i]) / max(np.linalg.norm(fx[f][i]), 1e-300))
+            bar = max(REL, 1e3 * float(fx["sens_" + f][i]))
+            worst[f] = max(worst.get(f, 0.0), e / bar)
+            assert e <= bar, "step %d %s rel err %.3e > %.3e" % (k, f, e, bar)
+    sw = c.switches()
+    assert sw and sw[0]["step"] == first and sw[0]["to"] == "fd"
+    assert abs(sw[0]["t"] - float(fx["switch_t"])) <= 1e-12 * float(fx["switch_t"])
+    c.close()
