@@ -283,12 +283,16 @@ def run_batched(args, dist, rank, world, local):
     # ncu captures of these kernels at 32 instances of the 401 x 401 workload
     # (profiles/batched_ensemble_kernels_401x401.md,
     # profiles/ozk_gemm_kernel_S5_12832x401x401.md); other sizes report none
-    traffic = {"ysolve": 65362176.0, "matvec": 178643456.0, "residual": 187187968.0, "ztransform": 28774656.0} \
-        if (args.batch == 32 and args.n == 401) else {}
+    sep = b.tuning(0)["operator_form"] != "cross"
+    traffic = {"ysolve": 65362176.0, "ztransform": 28774656.0} if (args.batch == 32 and args.n == 401) else {}
+    if not sep and args.batch == 32 and args.n == 401:
+        traffic.update({"matvec": 178643456.0, "residual": 187187968.0})
+    opk = "b_full_kernel<%d> (separable form: 1D coefficient tables, register window along y)" if sep else \
+        "b_cross_kernel<%d> (cross form: 33 coefficient planes)"
     kern = {}
     for nm, desc in (("ysolve", "b_ysolve_tma_kernel (banded Cholesky sweeps along y of the preconditioner)"),
-                     ("matvec", "b_cross_kernel<1> (CG operator application, p update fused)"),
-                     ("residual", "b_cross_kernel<0> (initial residual of each stage solve)"),
+                     ("matvec", (opk % 1) + ", CG operator application, p update fused"),
+                     ("residual", (opk % 0) + ", initial residual of each stage solve"),
                      ("ztransform", ZT_DESC), ("zsplit", ZS_DESC)):
         pm, pl, pb = b.profile_collect(nm)
         if pl:
@@ -875,6 +879,26 @@ def run_wave_only(args):
     c.close()
 
 
+def run_batch_only_profile(args):
+    """The batched ensemble (args.profile_batch instances of the n x n
+    workload) set up and advanced args.profile_reps steps with its launches
+    issued directly (no graph), for ncu captures of its kernels."""
+    import torch
+    from scycle_b200 import build
+    build.build(verbose=False)
+    from scycle_b200.batch import Batch
+    K = args.profile_batch
+    work = tempfile.mkdtemp(prefix="scy_pbatch_")
+    paths = [make_workload(os.path.join(work, "i%d" % s), n=args.n, seed=s) for s in range(K)]
+    b = Batch(paths, solve_rtol=args.rtol, precision=args.batch_precision, transform_planes=args.transform_planes)
+    b.set_graphs(False)
+    b.run(args.profile_reps)
+    torch.cuda.synchronize()
+    print(json.dumps({"batch_only_profile": True, "instances": K, "n": args.n, "steps": args.profile_reps,
+                      "autotune": b.tuning(0)}))
+    b.close()
+
+
 def run_stencil_only(args):
     """A x on an n x n grid (FP64, constant grid, Dirichlet/Neumann SATs): the
     operator kernel alone, sized past L2 when n >= 4097, for profiling."""
@@ -1103,6 +1127,9 @@ def main():
     ap.add_argument("--profile-wave", type=int, default=0,
                     help="run the cycle workload on an n x n grid into a wave phase, time its two launches, exit")
     ap.add_argument("--profile-reps", type=int, default=20)
+    ap.add_argument("--profile-batch", type=int, default=0,
+                    help="set up this many instances of the batched workload, advance --profile-reps steps with "
+                         "direct launches (for ncu) and exit")
     ap.add_argument("--profile-bf16", type=int, default=0, choices=[0, 1],
                     help="digits in bf16 (kind::f16) instead of 8-bit integers in --profile-ztransform")
     ap.add_argument("--profile-ctas", type=int, default=1, choices=[1, 2],
@@ -1120,6 +1147,9 @@ def main():
         return
     if args.profile_ztransform:
         run_ztransform_only(args)
+        return
+    if args.profile_batch:
+        run_batch_only_profile(args)
         return
     dist, rank, world, local = _dist()
     try:

@@ -203,6 +203,15 @@ scy_status scy_grid_host_apply(const scy_grid_desc* desc, const double* in, doub
  * operator and every row's z operator composed with that line's
  * coefficients and SAT terms).  Same arguments as scy_grid_host_apply. */
 scy_status scy_grid_host_apply_cross(const scy_grid_desc* desc, const double* in, double* out);
+/* Host reference of the operator in the full form the single-instance
+ * operator kernels and the batched ensemble apply when it exists: outer
+ * weights separable over every node, every column's y operator and every
+ * row's z operator composed into 17-point stencils, one table per class of
+ * lines (the lines equal to the middle column / row, plus at most eight
+ * exceptional lines per direction such as the grid's corner lines), 9-point
+ * on the interior box.  Same arguments as scy_grid_host_apply; SCY_ERR_ARG
+ * when the operator has no full form. */
+scy_status scy_grid_host_apply_full(const scy_grid_desc* desc, const double* in, double* out);
 
 /* ------------------------------------------------------------------------
  * Fault_qd + StrikeSlip_LinearElastic_qd (linear-elastic quasi-dynamic).
@@ -293,6 +302,18 @@ typedef struct scy_ode_stats {
   int done;             /* 1: reached t1 or max_steps; 2: stopped after writing a checkpoint
                            (enableCheckpointing, as the reference's run ends there) */
 } scy_ode_stats;
+
+/* Fault_qd::d_dt (fault.cpp:861-918) on its own: with tau_body the body's
+ * shear stress on the fault (device, Nz: the fault-row mu Dy u a driver
+ * takes from its solve, LinearElastic::computeStresses), every fault node's
+ * tauQS = tau_body + prestress, its slip velocity from the bracketed Newton
+ * root of the friction law (ComputeVel_qd, fault.cpp:954-1059, starting from
+ * the current slip velocity), the state rate of the driver's state law,
+ * tauP and strength.  var, dvar: device arrays laid out as for scy_qd_d_dt
+ * (scy_qd_state_size doubles; only the fault entries of dvar are written).
+ * The fault fields (SCY_FIELD_SLIPVEL, TAUP, TAUQSP, ...) are updated as
+ * the member vectors of Fault_qd are. */
+scy_status scy_qd_fault_d_dt(scy_qd* q, const double* var, const double* tau_body, double* dvar);
 
 /* OdeSolver setInitialConds + the first d_dt.  var0 = [psi | slip] host. */
 scy_status scy_qd_integrate_begin(scy_qd* q, const scy_ode_opts* opts, const double* var0_host);
@@ -645,26 +666,37 @@ enum { SCY_BATCH_KERNEL_YSOLVE = 0, SCY_BATCH_KERNEL_RESIDUAL = 1, SCY_BATCH_KER
 scy_status scy_batch_profile_collect(scy_batch* b, int kernel, double* ms, long long* launches, double* bytes);
 /* Drops the recorded launches. */
 scy_status scy_batch_profile_clear(scy_batch* b);
-/* Test hook (no counterpart in the reference): limits the polls of the
- * banded sweeps' data waits (default 2^18).  A wait that runs out marks its
+/* Test hook (no counterpart in the reference) for the banded sweeps'
+ * bounded data waits: polls bounds the waits (default 2^18; every poll is an
+ * mbarrier.try_wait, which itself waits a while), and drop_first_copy = 1
+ * withholds each block's first chunk copy, so that wait runs out as a copy
+ * that never arrives would make it.  A wait that runs out marks its
  * instances (status bit 4) and the round is repeated; after three repeats
- * scy_batch_run returns SCY_ERR_TIMEOUT.  With polls = 1 the waits run out at
- * once, exercising that path without a hang; the copies already issued are
- * still awaited at the full limit before a block exits. */
-scy_status scy_batch_set_sweep_polls(scy_batch* b, int polls);
+ * scy_batch_run returns SCY_ERR_TIMEOUT.  Nothing is left in flight: a
+ * block awaits the copies it did issue (at the full limit) before it exits.
+ * (polls, 0) with the default restores normal operation. */
+scy_status scy_batch_set_sweep_test(scy_batch* b, int polls, int drop_first_copy);
 
 /* The autotuner's choices for group g (no counterpart in the reference): at
- * set-up every group times, on its own buffers, the CG operator kernel with
- * 1, 2, 4 and 8 instances per block, the banded sweeps in three launch
- * shapes (two chains per lane x two warps, one x four, four x one) and the
- * z-transform product with one or two CTAs per SM and 8-bit or bf16 digits
- * (identical results), and keeps the fastest.  kpb / sweep_variant /
- * ztransform get the choices (ztransform bit 0: two CTAs per SM, bit 1:
- * bf16 digits), us (12 doubles, may be NULL) the timings in microseconds per
- * launch (kpb 1, 2, 4, 8; sweeps 0, 1, 2; unused; product with 8-bit
- * digits, one and two CTAs per SM; with bf16 digits, one and two CTAs per
- * SM; 0 where not tried). */
+ * set-up every group times, on its own buffers, the CG operator kernel in
+ * the cross form (33 coefficient planes) with 1, 2, 4 and 8 instances per
+ * block and, when the operator is separable over every node, in the
+ * separable form (1D coefficient tables) with 1, 2 and 4 rows per thread,
+ * the banded sweeps in six launch shapes (chains per lane x warps per block:
+ * 2 x 2, 1 x 4, 4 x 1 serving 8 instances per block, 1 x 2 and 2 x 1
+ * serving 4, 1 x 1 serving 2) and the z-transform product with one or two
+ * CTAs per SM and 8-bit or bf16 digits (identical results), and keeps the
+ * fastest.  kpb / sweep_variant / ztransform get the choices (kpb: the cross
+ * form's, see scy_batch_operator_form for the form in use; ztransform bit 0:
+ * two CTAs per SM, bit 1: bf16 digits), us (17 doubles, may be NULL) the
+ * timings in microseconds per launch (cross form at kpb 1, 2, 4, 8; sweep
+ * shapes 0-5; product with 8-bit digits, one and two CTAs per SM; with bf16
+ * digits, one and two CTAs per SM; separable form at 1, 2, 4 rows per
+ * thread; 0 where not tried). */
 scy_status scy_batch_tuning(scy_batch* b, int g, int* kpb, int* sweep_variant, int* ztransform, double* us);
+/* The operator kernels group g runs: *rows_per_thread = 0 for the cross
+ * form, else the separable form's rows per thread (1, 2 or 4). */
+scy_status scy_batch_operator_form(scy_batch* b, int g, int* rows_per_thread);
 
 /* ---------------------------------------------------------------------------
  * Discrete adjoint of the linear-elastic quasi-dynamic RK32 integration.

@@ -10,7 +10,10 @@
  *                        linearElastic.cpp:465-489);
  *   scycle_b200::QD      a whole quasi-dynamic driver from a .in file
  *                        (StrikeSlip_LinearElastic_qd or _PowerLaw_qd:
- *                        main.cpp:227-233 and integrate()).
+ *                        main.cpp:227-233 and integrate());
+ *   scycle_b200::Fault_qd  the interface of Fault_qd (fault.hpp:138-160)
+ *                        over a driver's fault: d_dt given the body's
+ *                        stress on the fault, the member vectors.
  *
  * Methods return the library's status (0 = success, as PetscErrorCode 0);
  * scycle_b200::last_error() gives the message.  Vectors are device
@@ -151,6 +154,28 @@ class QD {
  private:
   scy_qd* q_ = nullptr;
   int status_ = SCY_OK;
+};
+
+/* The interface of Fault_qd (fault.hpp:138-160) over a driver's fault:
+ * d_dt with the body's shear stress on the fault supplied by the caller
+ * (what StrikeSlip_LinearElastic_qd::d_dt passes after its solve), the
+ * member vectors read back through getField.  The fault's parameters are
+ * those of the driver's input file. */
+class Fault_qd {
+ public:
+  explicit Fault_qd(QD& qd) : q_(qd.handle()) {}
+  /* var, dvar: device, scy_qd_state_size doubles; tauBody: device, Nz */
+  int d_dt(const double* var, const double* tauBody, double* dvar) {
+    return q_ ? scy_qd_fault_d_dt(q_, var, tauBody, dvar) : SCY_ERR_STATE;
+  }
+  int slipVel(double* host) { return get(SCY_FIELD_SLIPVEL, host); }
+  int tauP(double* host) { return get(SCY_FIELD_TAUP, host); }
+  int tauQSP(double* host) { return get(SCY_FIELD_TAUQSP, host); }
+  int strength(double* host) { return get(SCY_FIELD_STRENGTH, host); }
+
+ private:
+  int get(int f, double* host) { return q_ ? scy_qd_get_field(q_, f, host) : SCY_ERR_STATE; }
+  scy_qd* q_;
 };
 
 }  // namespace scycle_b200

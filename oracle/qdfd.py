@@ -102,8 +102,8 @@ def penalty_ay(Ny, Nz, h11y, h11z, bcR, bcT, bcL, bcB, cs):
 
 
 class QDFDLinearElastic(QDLinearElastic):
-    def __init__(self, P, keep_history=True):
-        super().__init__(P, keep_history)
+    def __init__(self, P, keep_history=True, refine=0):
+        super().__init__(P, keep_history, refine)
         self.N = self.Ny * self.Nz
         self.fdset = P["fd"]
         d = P["domain"]

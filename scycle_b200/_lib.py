@@ -71,6 +71,7 @@ def lib():
         L.scy_sbp_info.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.scy_grid_host_apply.argtypes = [C.POINTER(GridDesc), dptr, dptr]
         L.scy_grid_host_apply_cross.argtypes = [C.POINTER(GridDesc), dptr, dptr]
+        L.scy_grid_host_apply_full.argtypes = [C.POINTER(GridDesc), dptr, dptr]
         L.scy_ozaki_matmul.argtypes = [vp, C.c_long, C.c_int, C.c_int, dptr, C.c_long, C.c_int, C.c_int, vp,
                                        C.c_long, C.c_int, C.c_int]
         L.scy_launch_count.restype = C.c_longlong
@@ -122,10 +123,12 @@ def grid_desc(order, Ny, Nz, Ly, Lz, mu, grid="constantGridSpacing", y=None, z=N
 
 
 def host_apply(desc, x, form="stages"):
-    """A x on the host: the two-stage form of the device stencil ("stages")
-    or the per-node cross-stencil form of the batched ensemble ("cross")."""
+    """A x on the host: the two-stage form of the device stencil ("stages"),
+    the per-node cross-stencil form of the batched ensemble ("cross") or the
+    full form with line classes ("full")."""
     x = np.ascontiguousarray(x, dtype=np.float64)
     out = np.zeros_like(x)
-    f = lib().scy_grid_host_apply if form == "stages" else lib().scy_grid_host_apply_cross
+    f = {"stages": lib().scy_grid_host_apply, "cross": lib().scy_grid_host_apply_cross,
+         "full": lib().scy_grid_host_apply_full}[form]
     check(f(C.byref(desc), as_dptr(x), as_dptr(out)))
     return out

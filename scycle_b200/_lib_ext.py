@@ -58,6 +58,7 @@ def declare(L):
     L.scy_qd_integrate_begin_from_in.argtypes = [vp]
     L.scy_qd_set_state.argtypes = [vp, dptr, C.c_int]
     L.scy_qd_set_jacobian.argtypes = [vp, C.c_int]
+    L.scy_qd_fault_d_dt.argtypes = [vp, vp, vp, vp]
     L.scy_qd_steady_state_info.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_long)]
     L.scy_qd_steady_state_trace.argtypes = [vp, dptr, C.c_long, C.POINTER(C.c_long)]
     L.scy_qd_set_mode.argtypes = [vp, C.c_int]
@@ -130,6 +131,7 @@ class BatchStats(C.Structure):
 def declare_batch(L):
     L.scy_batch_tuning.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
                                    C.POINTER(C.c_double)]
+    L.scy_batch_operator_form.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int)]
     vp = C.c_void_p
     L.scy_batch_create_from_in.argtypes = [C.c_int, C.POINTER(C.c_char_p), C.POINTER(S.SolveOpts),
                                            C.POINTER(BatchOpts), C.POINTER(vp)]
@@ -141,7 +143,7 @@ def declare_batch(L):
     L.scy_batch_set_states.argtypes = [vp, dptr]
     L.scy_batch_get_fault_field.argtypes = [vp, C.c_int, dptr]
     L.scy_batch_set_graphs.argtypes = [vp, C.c_int]
-    L.scy_batch_set_sweep_polls.argtypes = [vp, C.c_int]
+    L.scy_batch_set_sweep_test.argtypes = [vp, C.c_int, C.c_int]
     L.scy_batch_profile.argtypes = [vp, C.c_int]
     L.scy_batch_profile_collect.argtypes = [vp, C.c_int, dptr, C.POINTER(C.c_longlong), dptr]
     L.scy_batch_profile_clear.argtypes = [vp]

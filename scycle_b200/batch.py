@@ -90,19 +90,26 @@ class Batch:
         return ms.value, nl.value, by.value
 
     def tuning(self, group=0):
-        """The autotuner's choices for a group: instances per block of the
-        operator kernels, the sweep launch shape and the timings (us)."""
-        kpb, var, zt = C.c_int(), C.c_int(), C.c_int()
-        us = (C.c_double * 12)()
+        """The autotuner's choices for a group: the operator kernels' form
+        (cross form with instances per block, or separable form with rows
+        per thread), the sweep launch shape, the z-transform product's shape
+        and digits, and the timings (us)."""
+        kpb, var, zt, rpt = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        us = (C.c_double * 17)()
         S.check(S.lib().scy_batch_tuning(self.h, int(group), C.byref(kpb), C.byref(var), C.byref(zt), us))
-        return {"instances_per_block": kpb.value, "sweep_variant": ["2 chains x 2 warps", "1 chain x 4 warps",
-                                                                   "4 chains x 1 warp"][var.value],
+        S.check(S.lib().scy_batch_operator_form(self.h, int(group), C.byref(rpt)))
+        shapes = ["2 chains x 2 warps (8 instances)", "1 chain x 4 warps (8)", "4 chains x 1 warp (8)",
+                  "1 chain x 2 warps (4)", "2 chains x 1 warp (4)", "1 chain x 1 warp (2)"]
+        return {"operator_form": ("separable, %d rows per thread" % rpt.value) if rpt.value else "cross",
+                "instances_per_block": kpb.value, "sweep_variant": shapes[var.value],
                 "ztransform_ctas_per_sm": 2 if zt.value & 1 else 1,
                 "ztransform_digits": "bf16 (kind::f16)" if zt.value & 2 else "int8 (kind::i8)",
                 "operator_us_by_kpb": {k: us[i] for i, k in enumerate((1, 2, 4, 8)) if us[i] > 0},
-                "sweep_us_by_variant": [us[4], us[5], us[6]],
-                "ztransform_us_int8_by_ctas_per_sm": {1: us[8], 2: us[9]},
-                "ztransform_us_bf16_by_ctas_per_sm": {1: us[10], 2: us[11]}}
+                "sweep_us_by_variant": {shapes[v]: us[4 + v] for v in range(6) if us[4 + v] > 0},
+                "ztransform_us_int8_by_ctas_per_sm": {1: us[10], 2: us[11]},
+                "ztransform_us_bf16_by_ctas_per_sm": {1: us[12], 2: us[13]},
+                "operator_us_separable_by_rows_per_thread": {r: us[14 + i] for i, r in enumerate((1, 2, 4))
+                                                             if us[14 + i] > 0}}
 
     def profile_clear(self):
         S.check(S.lib().scy_batch_profile_clear(self.h))

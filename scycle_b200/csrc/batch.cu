@@ -402,6 +402,104 @@ __global__ void __launch_bounds__(XT) b_cross_kernel(const double* __restrict__ 
   }
 }
 
+// The same two products when the group's operator is separable over every
+// node (L.full: one 17-point stencil per row and per column from 1D tables
+// shared by the group, L1/L2-resident): one instance per block
+// (blockIdx.z), its 8*RPT x 32 tile staged once and applied by full_apply
+// (register window along y, 9-point interior), so per node only the
+// instance's own fields move.  The partial sums do not depend on RPT: a
+// warp sums each of its rows across its 32 columns, and every band of 8 rows
+// (a tile of the 8 x 32 layout, index blockIdx.x + gridDim.x * band) adds
+// its 8 row sums with one warp sum, as b_cross_kernel does per tile.
+template <int MODE, typename Tz, int RPT>
+__global__ void __launch_bounds__(256) b_full_kernel(LevelDev<double> L, const BatchInst* __restrict__ tab,
+                                                     const int* __restrict__ mask, BatchWork w,
+                                                     const Tz* __restrict__ zv, int first, int pi, int mixed,
+                                                     int store_p) {
+  __shared__ double xs[full_smem_values<RPT>()];
+  __shared__ double rs[2][8 * RPT];  // row sums
+  const int k = blockIdx.z;
+  if (!mask[k]) return;
+  const int tid = threadIdx.x, lane = tid & 31, r0 = (tid >> 5) * RPT;
+  const long off = (long)k * w.N;
+  const double* sc = w.sc + 16 * k;
+  double a1 = 0.0, a2 = 0.0;  // the current row's contributions
+  auto row = [&](int j) {
+    const double t1 = warp_sum(a1);
+    const double t2 = (MODE == 1 && first) ? warp_sum(a2) : 0.0;
+    if (lane == 0) {
+      rs[0][r0 + j] = t1;
+      rs[1][r0 + j] = t2;
+    }
+    a1 = a2 = 0.0;
+  };
+  if (MODE == 0) {
+    const double* u = tab[k].u;
+    const double* rhs = tab[k].rhs;
+    const bool zero = sc[0] == 0.0;
+    auto ld = [&](long node, int, int) { return u[node]; };
+    auto out = [&](long node, int, int, double Ax, double) {
+      const double v = zero ? 0.0 : -1.0 * rhs[node] + Ax;
+      w.r[off + node] = v;
+      if (mixed) w.r32[off + node] = (float)v;
+      a1 = v * v;
+    };
+    full_apply<double, RPT>(L, ld, out, row, xs);
+  } else {
+    double beta = 0.0;
+    if (!first) {
+      const double ro = sc[3];
+      beta = ro != 0.0 ? sc[2] / ro : 0.0;
+    }
+    const Tz* z = zv + off;
+    const double* pold = (pi ? w.p1 : w.p0) + off;
+    double* pnew = (pi ? w.p0 : w.p1) + off;
+    const double* r = w.r + off;
+    double* q = w.q + off;
+    auto ld = [&](long node, int, int) {
+      return first ? (double)z[node] : (double)z[node] + beta * pold[node];
+    };
+    auto out = [&](long node, int, int, double Ax, double p) {
+      const double qv = -Ax;
+      if (store_p) pnew[node] = p;
+      q[node] = qv;
+      a1 = p * qv;
+      if (first) a2 = r[node] * p;
+    };
+    full_apply<double, RPT>(L, ld, out, row, xs);
+  }
+  __syncthreads();
+  const int wv = tid >> 5, band = blockIdx.y * RPT + wv;
+  if (wv < RPT && band * 8 < L.Ny) {
+    const long slot = (long)k * w.PB + blockIdx.x + (long)gridDim.x * band;
+    double t = lane < 8 ? rs[0][wv * 8 + lane] : 0.0;
+    t = warp_sum(t);
+    if (lane == 0) w.partials[slot] = t;
+    if (MODE == 1 && first) {
+      t = lane < 8 ? rs[1][wv * 8 + lane] : 0.0;
+      t = warp_sum(t);
+      if (lane == 0) w.partials2[slot] = t;
+    }
+  }
+}
+
+// grid of b_full_kernel: column tiles, row tiles of 8*rpt, instances
+static dim3 full_grid(const BatchGroup& g, int rpt) {
+  return dim3((g.Nz + TZ - 1) / TZ, (g.Ny + 8 * rpt - 1) / (8 * rpt), g.K);
+}
+
+template <int MODE, typename Tz>
+static void launch_full(const BatchGroup& g, int rpt, const BatchInst* tab, const int* mask, const Tz* zv, int first,
+                        int pi, int mixed, int store_p) {
+  const dim3 grid = full_grid(g, rpt);
+  if (rpt == 4)
+    b_full_kernel<MODE, Tz, 4><<<grid, 256, 0, g.stream>>>(g.L, tab, mask, g.w, zv, first, pi, mixed, store_p);
+  else if (rpt == 2)
+    b_full_kernel<MODE, Tz, 2><<<grid, 256, 0, g.stream>>>(g.L, tab, mask, g.w, zv, first, pi, mixed, store_p);
+  else
+    b_full_kernel<MODE, Tz, 1><<<grid, 256, 0, g.stream>>>(g.L, tab, mask, g.w, zv, first, pi, mixed, store_p);
+}
+
 // sc[16 k + slot] = sum of the instance's first n partials (of w.partials,
 // or of w.partials2 when second is set), in tile order
 __global__ void b_partials_kernel(const int* __restrict__ mask, BatchWork w, int n, int slot, int second = 0) {
@@ -991,6 +1089,10 @@ int BatchContext::setup_group(int base, int K) {
     SCY_TRY(tma_map_2d(&g.mLrow32, g.fd->Lrow32.p, d32, 4, g.Nz, (long)(g.Ny + 8) * 9, (long)Nzp * 4, YS_C, YS_R * 9));
     SCY_TRY(tma_map_3d(&g.mT32, g.t1pf.p, d32, g.Nz, g.Ny, g.K, (long)Nzp * 4, (long)g.Ny * Nzp * 4, YS_C, YS_R,
                        YS_B));
+    SCY_TRY(tma_map_3d(&g.mT4, g.t1p.p, d64, g.Nz, g.Ny, g.K, (long)Nzp * 8, (long)g.Ny * Nzp * 8, YS_C, YS_R, 4));
+    SCY_TRY(tma_map_3d(&g.mT2, g.t1p.p, d64, g.Nz, g.Ny, g.K, (long)Nzp * 8, (long)g.Ny * Nzp * 8, YS_C, YS_R, 2));
+    SCY_TRY(tma_map_3d(&g.mT4_32, g.t1pf.p, d32, g.Nz, g.Ny, g.K, (long)Nzp * 4, (long)g.Ny * Nzp * 4, YS_C, YS_R, 4));
+    SCY_TRY(tma_map_3d(&g.mT2_32, g.t1pf.p, d32, g.Nz, g.Ny, g.K, (long)Nzp * 4, (long)g.Ny * Nzp * 4, YS_C, YS_R, 2));
     // digit planes of the z transforms: the operand (K*Ny rows of Nz) and
     // the weights, rows of Vz^T (forward) and of Vz (inverse); Vz is
     // column-major, so its columns are the forward weights' rows
@@ -1014,18 +1116,22 @@ int BatchContext::setup_group(int base, int K) {
       }
       SCY_TRY(ozk_prepare(S));
     }
-    SCY_CUDA_TRY(cudaFuncSetAttribute(b_ysolve_tma_kernel<double, 2, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      ys_smem_bytes(8)));
-    SCY_CUDA_TRY(cudaFuncSetAttribute(b_ysolve_tma_kernel<float, 2, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      ys_smem_bytes(4)));
-    SCY_CUDA_TRY(cudaFuncSetAttribute(b_ysolve_tma_kernel<double, 1, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      ys_smem_bytes(8)));
-    SCY_CUDA_TRY(cudaFuncSetAttribute(b_ysolve_tma_kernel<float, 1, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      ys_smem_bytes(4)));
-    SCY_CUDA_TRY(cudaFuncSetAttribute(b_ysolve_tma_kernel<double, 4, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      ys_smem_bytes(8)));
-    SCY_CUDA_TRY(cudaFuncSetAttribute(b_ysolve_tma_kernel<float, 4, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      ys_smem_bytes(4)));
+    // every launch shape of launch_ysolve gets the shared memory of the
+    // eight-instance layout (the smaller shapes use part of it)
+#define SCY_YS_ATTR(I, W)                                                                                    \
+  do {                                                                                                      \
+    SCY_CUDA_TRY(cudaFuncSetAttribute(b_ysolve_tma_kernel<double, I, W>,                                    \
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, ys_smem_bytes(8)));      \
+    SCY_CUDA_TRY(cudaFuncSetAttribute(b_ysolve_tma_kernel<float, I, W>,                                     \
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, ys_smem_bytes(4)));      \
+  } while (0)
+    SCY_YS_ATTR(2, 2);
+    SCY_YS_ATTR(1, 4);
+    SCY_YS_ATTR(4, 1);
+    SCY_YS_ATTR(1, 2);
+    SCY_YS_ATTR(2, 1);
+    SCY_YS_ATTR(1, 1);
+#undef SCY_YS_ATTR
   }
   SCY_TRY(g.tab.alloc(sizeof(BatchInst) * g.K));
   SCY_CUDA_TRY(cudaMemcpy(g.tab.p, tab.data(), sizeof(BatchInst) * g.K, cudaMemcpyHostToDevice));
@@ -1047,26 +1153,35 @@ int BatchContext::setup_group(int base, int K) {
 int BatchContext::launch_ysolve(BatchGroup& g, int variant) {
   FDPrecond& F = *g.fd;
   const int Ny = g.Ny, Nz = g.Nz, K = g.K;
-  const dim3 grid((Nz + YS_C - 1) / YS_C, (K + YS_B - 1) / YS_B);
   const bool f32 = precision != SCY_PREC_FP64;
   const int sm = ys_smem_bytes(f32 ? 4 : 8);
-#define SCY_YS_LAUNCH(I, W)                                                                                       \
+  // B = 2 I W instances per block: the transform map whose box holds B of them
+#define SCY_YS_LAUNCH(I, W, M64, M32)                                                                             \
   do {                                                                                                              \
+    constexpr int B = 2 * (I) * (W);                                                                                \
+    const dim3 grid((Nz + YS_C - 1) / YS_C, (K + B - 1) / B);                                                      \
     if (f32)                                                                                                        \
-      b_ysolve_tma_kernel<float, I, W><<<grid, 32 * W, sm, g.stream>>>(g.mLcol32, g.mLrow32, g.mT32,               \
+      b_ysolve_tma_kernel<float, I, W><<<grid, 32 * W, sm, g.stream>>>(g.mLcol32, g.mLrow32, M32,                  \
                                                                        g.t1pf.as<float>(), Ny, Nz, F.Nzp, K,        \
-                                                                       g.w.status, sweep_polls);                    \
+                                                                       g.w.status, sweep_polls, sweep_drop);        \
     else                                                                                                            \
-      b_ysolve_tma_kernel<double, I, W><<<grid, 32 * W, sm, g.stream>>>(g.mLcol, g.mLrow, g.mT, g.t1p.as<double>(), \
-                                                                        Ny, Nz, F.Nzp, K, g.w.status, sweep_polls); \
+      b_ysolve_tma_kernel<double, I, W><<<grid, 32 * W, sm, g.stream>>>(g.mLcol, g.mLrow, M64, g.t1p.as<double>(),  \
+                                                                        Ny, Nz, F.Nzp, K, g.w.status, sweep_polls,  \
+                                                                        sweep_drop);                                \
   } while (0)
-  static_assert(2 * 2 * 2 == YS_B && 2 * 4 * 1 == YS_B && 2 * 1 * 4 == YS_B, "sweep variants serve YS_B instances");
+  static_assert(2 * 2 * 2 == YS_B && 2 * 4 * 1 == YS_B && 2 * 1 * 4 == YS_B, "sweep variants 0-2 serve YS_B instances");
   if (variant == 1)
-    SCY_YS_LAUNCH(1, 4);
+    SCY_YS_LAUNCH(1, 4, g.mT, g.mT32);
   else if (variant == 2)
-    SCY_YS_LAUNCH(4, 1);
+    SCY_YS_LAUNCH(4, 1, g.mT, g.mT32);
+  else if (variant == 3)
+    SCY_YS_LAUNCH(1, 2, g.mT4, g.mT4_32);
+  else if (variant == 4)
+    SCY_YS_LAUNCH(2, 1, g.mT4, g.mT4_32);
+  else if (variant == 5)
+    SCY_YS_LAUNCH(1, 1, g.mT2, g.mT2_32);
   else
-    SCY_YS_LAUNCH(2, 2);
+    SCY_YS_LAUNCH(2, 2, g.mT, g.mT32);
 #undef SCY_YS_LAUNCH
   SCY_LAUNCH_CHECK();
   return SCY_OK;
@@ -1131,9 +1246,43 @@ int BatchContext::autotune(BatchGroup& g) {
     }
   }
   g.kpb = best;
+  // the separable form (when the operator is separable over every node) at
+  // 1, 2 and 4 rows per thread: used whenever it exists, so that a group's
+  // results do not depend on timings (its arithmetic differs from the cross
+  // form's by rounding; its rows per thread change nothing, see
+  // b_full_kernel); the cross form's timings stay for comparison
+  g.full_rpt = 0;
+  if (g.L.full) {
+    best_us = 1e300;
+    const int rpts[3] = {1, 2, 4};
+    for (int c = 0; c < 3; ++c) {
+      const int rpt = rpts[c];
+      double us = 0.0;
+      int rc = timed(
+          [&]() -> int {
+            if (mixed)
+              launch_full<1, float>(g, rpt, tab, mask, g.w.z32, 1, 0, mixed, 1);
+            else
+              launch_full<1, double>(g, rpt, tab, mask, g.w.z, 1, 0, mixed, 1);
+            SCY_LAUNCH_CHECK();
+            return SCY_OK;
+          },
+          &us);
+      if (rc != SCY_OK) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        return rc;
+      }
+      g.tune_us[14 + c] = us;
+      if (us < best_us) {
+        best_us = us;
+        g.full_rpt = rpt;
+      }
+    }
+  }
   if (g.fd->ybanded && !fd_dense) {
     double best_ys = 1e300;
-    for (int v = 0; v < 3; ++v) {
+    for (int v = 0; v < 6; ++v) {
       double us = 0.0;
       int rc = timed([&]() -> int { return launch_ysolve(g, v); }, &us);
       if (rc != SCY_OK) {
@@ -1170,7 +1319,7 @@ int BatchContext::autotune(BatchGroup& g) {
             cudaEventDestroy(e1);
             return rc;
           }
-          g.tune_us[8 + 2 * bf + pr] = us;
+          g.tune_us[10 + 2 * bf + pr] = us;
           if (us < zbest) {
             zbest = us;
             g.zt_pair = pr;
@@ -1337,19 +1486,25 @@ int BatchContext::fd_apply(BatchGroup& g) {
 
 int BatchContext::solve(BatchGroup& g, const int* mask, int its_now) {
   const int mixed = precision != SCY_PREC_FP64 ? 1 : 0;
-  const dim3 tg((g.Nz + XTZ - 1) / XTZ, (g.Ny + XTY - 1) / XTY, (g.K + g.kpb - 1) / g.kpb);
+  const int rpt = g.full_rpt;  // > 0: the separable form
+  const dim3 tg = rpt ? full_grid(g, rpt)
+                      : dim3((g.Nz + XTZ - 1) / XTZ, (g.Ny + XTY - 1) / XTY, (g.K + g.kpb - 1) / g.kpb);
   const dim3 ng(node_blocks(g.N), 1, g.K);
   const BatchInst* tab = g.tab.as<BatchInst>();
   const double* C = g.planes.as<double>();
-  const int ntiles = (int)(tg.x * tg.y);
-  // algorithmic bytes: the coefficient planes once, per node and active
-  // instance the operand, rhs and result (residual) or z, p_old, p and q
+  const int ntiles = (int)(((g.Nz + XTZ - 1) / XTZ) * ((g.Ny + XTY - 1) / XTY));  // partials of either form
+  // algorithmic bytes: the coefficient planes once (the cross form), per
+  // node and active instance the operand, rhs and result (residual) or z,
+  // p_old, p and q
   const double nact = (double)active_in(g, mask);
-  const double coef_b = 33.0 * 8 * g.N;
+  const double coef_b = rpt ? 0.0 : 33.0 * 8 * g.N;
   cudaEvent_t pa;
   SCY_TRY(prof_begin(g.stream, &pa));
-  b_cross_kernel<0, double><<<tg, XT, xs_smem_bytes(0, 8), g.stream>>>(C, g.Ny, g.Nz, tab, mask, g.w, nullptr, 0, 0,
-                                                                       mixed, g.kpb);
+  if (rpt)
+    launch_full<0, double>(g, rpt, tab, mask, (const double*)nullptr, 0, 0, mixed, 0);
+  else
+    b_cross_kernel<0, double><<<tg, XT, xs_smem_bytes(0, 8), g.stream>>>(C, g.Ny, g.Nz, tab, mask, g.w, nullptr, 0,
+                                                                         0, mixed, g.kpb);
   SCY_LAUNCH_CHECK();
   SCY_TRY(prof_end(g.stream, pa, PROF_RESIDUAL, coef_b + nact * g.N * (24.0 + (mixed ? 4 : 0))));
   b_partials_kernel<<<g.K, 256, 0, g.stream>>>(mask, g.w, ntiles, 5);
@@ -1368,7 +1523,11 @@ int BatchContext::solve(BatchGroup& g, const int* mask, int its_now) {
       SCY_LAUNCH_CHECK();
     }
     SCY_TRY(prof_begin(g.stream, &pa));
-    if (mixed)
+    if (rpt && mixed)
+      launch_full<1, float>(g, rpt, tab, mask, g.w.z32, first, pi, mixed, store_p);
+    else if (rpt)
+      launch_full<1, double>(g, rpt, tab, mask, g.w.z, first, pi, mixed, store_p);
+    else if (mixed)
       b_cross_kernel<1, float><<<tg, XT, xs_smem_bytes(1, 4), g.stream>>>(C, g.Ny, g.Nz, tab, mask, g.w, g.w.z32, first,
                                                                            pi, mixed, g.kpb, store_p);
     else
@@ -1811,9 +1970,10 @@ scy_status scy_batch_get_fault_field(scy_batch* b, int field, double* host) {
   return b->ctx.get_fault_field(field, host);
 }
 
-scy_status scy_batch_set_sweep_polls(scy_batch* b, int polls) {
+scy_status scy_batch_set_sweep_test(scy_batch* b, int polls, int drop_first_copy) {
   if (!b || polls < 1) return SCY_ERR_ARG;
   b->ctx.sweep_polls = polls;
+  b->ctx.sweep_drop = drop_first_copy ? 1 : 0;
   // captured rounds hold the old limit
   SCY_CUDA_TRY(cudaStreamSynchronize(b->ctx.stream));
   for (auto& kv : b->ctx.graph_of_its) cudaGraphExecDestroy(kv.second);
@@ -1846,7 +2006,13 @@ scy_status scy_batch_tuning(scy_batch* b, int g, int* kpb, int* sweep_variant, i
   if (sweep_variant) *sweep_variant = G.ys_variant;
   if (ztransform) *ztransform = G.zt_pair | (G.zt_bf16 << 1);
   if (us)
-    for (int i = 0; i < 12; ++i) us[i] = G.tune_us[i];
+    for (int i = 0; i < 17; ++i) us[i] = G.tune_us[i];
+  return SCY_OK;
+}
+
+scy_status scy_batch_operator_form(scy_batch* b, int g, int* rows_per_thread) {
+  if (!b || !rows_per_thread || g < 0 || g >= (int)b->ctx.groups.size()) return SCY_ERR_ARG;
+  *rows_per_thread = b->ctx.groups[g]->full_rpt;
   return SCY_OK;
 }
 

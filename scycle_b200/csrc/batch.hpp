@@ -68,15 +68,18 @@ struct BatchGroup {
   DevBuf tab;     // BatchInst[K]
   DevBuf t1p, t1pf;  // the z transform, rows padded to the factor tables' Nzp (FP64, FP32)
   CUtensorMap mLcol, mLrow, mT, mLcol32, mLrow32, mT32;  // tile maps of the TMA-fed banded sweeps
+  CUtensorMap mT4, mT2, mT4_32, mT2_32;                 // the transform for 4 and 2 instances per block
   DevBuf planes;  // the operator's 33 cross-stencil coefficient planes (build_cross_planes)
   int kpb = 1;    // instances per block of the operator kernels (autotuned at set-up)
   int ys_variant = 0;  // chains per lane x warps per block of the banded sweeps (autotuned)
   int zt_pair = 0;  // z-transform products in the two-CTAs-per-SM shape (autotuned)
   int zt_bf16 = 0;  // z-transform digits in bf16 (kind::f16) instead of 8-bit integers (autotuned)
-  // the autotuner's timings: kpb 1, 2, 4, 8, sweep variants 0, 1, 2, -,
+  int full_rpt = 0;  // > 0: the operator kernels in the separable form, rows per thread (autotuned)
+  // the autotuner's timings: kpb 1, 2, 4, 8; sweep variants 0..5;
   // z-transform product with 8-bit digits in the one- and two-CTAs-per-SM
-  // shapes, with bf16 digits in the two shapes
-  double tune_us[12] = {0};
+  // shapes, with bf16 digits in the two shapes; the separable form at 1, 2
+  // and 4 rows per thread
+  double tune_us[17] = {0};
   DevBuf vec[7], vecf[4], sc, partials, counters, status;
   BatchWork w{};
   cudaStream_t stream = nullptr;
@@ -148,6 +151,7 @@ struct BatchContext {
   };
   int prof = 0;
   int sweep_polls = 1 << 18;  // polls of the banded sweeps' data waits (lowered only by a test hook)
+  int sweep_drop = 0;         // test hook: the sweeps' first copy is withheld
   std::vector<ProfRec> precs;
   int active_in(const BatchGroup& g, const int* mask) const;  // instances of g the mask selects this round
   int prof_begin(cudaStream_t s, cudaEvent_t* a);

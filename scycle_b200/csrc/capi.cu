@@ -196,6 +196,35 @@ scy_status scy_grid_host_apply_cross(const scy_grid_desc* g, const double* in, d
   return SCY_OK;
 }
 
+scy_status scy_grid_host_apply_full(const scy_grid_desc* g, const double* in, double* out) {
+  if (!g || !in || !out || !g->mu) {
+    scy::set_error("scy_grid_host_apply_full: NULL argument");
+    return SCY_ERR_ARG;
+  }
+  try {
+    const size_t N = (size_t)g->Ny * g->Nz;
+    std::vector<double> y, z, mu(g->mu, g->mu + N);
+    if (g->grid_type == SCY_GRID_VAR) {
+      if (g->y) y.assign(g->y, g->y + N);
+      if (g->z) z.assign(g->z, g->z + N);
+    }
+    int bc[4] = {g->bcR, g->bcT, g->bcL, g->bcB};
+    scy::LevelHost L = scy::build_level(g->order, g->Ny, g->Nz, g->Ly, g->Lz, g->grid_type, g->compat, y, z, mu, bc);
+    scy::FullForm F;
+    if (!scy::build_full_form(L, F)) {
+      scy::set_error("scy_grid_host_apply_full: the operator has no full form (order 2, fewer than 17 points in a "
+                     "direction, non-separable weights or more than %d exceptional lines)",
+                     scy::kMaxLineClasses);
+      return SCY_ERR_ARG;
+    }
+    scy::apply_full_form(F, g->Ny, g->Nz, in, out);
+  } catch (const std::exception& e) {
+    scy::set_error("scy_grid_host_apply_full: %s", e.what());
+    return SCY_ERR_ARG;
+  }
+  return SCY_OK;
+}
+
 scy_status scy_qd_create(const scy_qd_desc* d, scy_qd** out) {
   if (!d || !out) {
     scy::set_error("scy_qd_create: NULL argument");
@@ -253,6 +282,15 @@ scy_status scy_qd_d_dt(scy_qd* q, double t, const double* var, double* dvar) {
     return SCY_ERR_ARG;
   }
   SCY_TRY(q->ctx.d_dt(t, var, dvar));
+  return q->ctx.read_flags();
+}
+
+scy_status scy_qd_fault_d_dt(scy_qd* q, const double* var, const double* tau_body, double* dvar) {
+  if (!q || !var || !tau_body || !dvar) {
+    scy::set_error("scy_qd_fault_d_dt: NULL argument");
+    return SCY_ERR_ARG;
+  }
+  SCY_TRY(q->ctx.fault_d_dt(var, tau_body, dvar));
   return q->ctx.read_flags();
 }
 

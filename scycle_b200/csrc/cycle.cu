@@ -67,10 +67,21 @@ struct EpiWave {
   }
 };
 
+// RPT = 0: the two-stage tile (stencil_tile); 1, 2, 4: the full-form tile
+// with that many rows per thread (full_tile).
+template <int RPT>
+__device__ __forceinline__ void wave_tile(const LevelDev<double>& L, const LoadPlain<double>& ld, const EpiWave& ep) {
+  if constexpr (RPT == 0)
+    stencil_tile<double, LoadPlain<double>, EpiWave>(L, ld, ep, nullptr, nullptr, nullptr);
+  else
+    full_tile<double, RPT, LoadPlain<double>, EpiWave>(L, ld, ep, nullptr, nullptr, nullptr);
+}
+
+template <int RPT>
 __global__ void __launch_bounds__(256) fd_wave_kernel(LevelDev<double> L, LoadPlain<double> ld, EpiWave ep,
                                                       const CycleDevState* st) {
   if (st->stop) return;
-  stencil_tile<double, LoadPlain<double>, EpiWave>(L, ld, ep, nullptr, nullptr, nullptr);
+  wave_tile<RPT>(L, ld, ep);
 }
 
 struct FDFaultArgs {
@@ -234,9 +245,10 @@ __global__ void __launch_bounds__(kFaultBlock) fd_fault_kernel(FDFaultArgs A) {
 }
 
 // One fully dynamic step in one launch: every tile applies the wave update;
-// the tiles of the fault row (blockIdx.y == 0, rows 0..7) then run the fault
-// update of their 32 columns from the rows they just computed, while the
-// rest of the grid is still stepping the body.
+// the tiles of the fault row (blockIdx.y == 0, rows 0 .. 7 or more) then run
+// the fault update of their 32 columns from the rows they just computed,
+// while the rest of the grid is still stepping the body.
+template <int RPT>
 __global__ void __launch_bounds__(256) fd_step_kernel(LevelDev<double> L, LoadPlain<double> ld, EpiWave ep,
                                                       FDFaultArgs A) {
   CycleDevState* st = A.st;
@@ -247,7 +259,7 @@ __global__ void __launch_bounds__(256) fd_step_kernel(LevelDev<double> L, LoadPl
   EpiWave e = ep;
   e.s_rows = fault_tile ? s_rows : nullptr;
   e.s_d2u = fault_tile ? s_d2u : nullptr;
-  stencil_tile<double, LoadPlain<double>, EpiWave>(L, ld, e, nullptr, nullptr, nullptr);
+  wave_tile<RPT>(L, ld, e);
   if (!fault_tile) return;
   __syncthreads();
   const int lane = threadIdx.x & 31;
@@ -630,13 +642,28 @@ int CycleContext::fd_launch_step(int r, cudaStream_t s, int part) {
   A.partials = reinterpret_cast<double*>(dstate.as<char>() + sizeof(CycleDevState));
   A.st = st;
   const LoadPlain<double> ld{u3[cur].as<double>()};
-  dim3 g((Nz + TZ - 1) / TZ, (Ny + TY - 1) / TY);
+  const dim3 g = apply_grid(L);
+  const int rpt = L.full ? L.rpt : 0;
   if (part & FD_FUSED) {
-    fd_step_kernel<<<g, 256, 0, s>>>(L, ld, ep, A);
+    if (rpt == 4)
+      fd_step_kernel<4><<<g, 256, 0, s>>>(L, ld, ep, A);
+    else if (rpt == 2)
+      fd_step_kernel<2><<<g, 256, 0, s>>>(L, ld, ep, A);
+    else if (rpt == 1)
+      fd_step_kernel<1><<<g, 256, 0, s>>>(L, ld, ep, A);
+    else
+      fd_step_kernel<0><<<g, 256, 0, s>>>(L, ld, ep, A);
     SCY_LAUNCH_CHECK();
   }
   if (part & FD_WAVE) {
-    fd_wave_kernel<<<g, 256, 0, s>>>(L, ld, ep, st);
+    if (rpt == 4)
+      fd_wave_kernel<4><<<g, 256, 0, s>>>(L, ld, ep, st);
+    else if (rpt == 2)
+      fd_wave_kernel<2><<<g, 256, 0, s>>>(L, ld, ep, st);
+    else if (rpt == 1)
+      fd_wave_kernel<1><<<g, 256, 0, s>>>(L, ld, ep, st);
+    else
+      fd_wave_kernel<0><<<g, 256, 0, s>>>(L, ld, ep, st);
     SCY_LAUNCH_CHECK();
   }
   if (part & FD_FAULT) {

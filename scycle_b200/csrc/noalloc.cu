@@ -113,12 +113,12 @@ __global__ void na_copy_scalar(double* dst, const double* src) { *dst = *src; }
 template <class Ld, class Ep>
 int na_stencil(const LevelDev<double>& L, Ld ld, Ep ep, double* partials, unsigned* counter, double* out,
                cudaStream_t s) {
-  dim3 g((L.Nz + TZ - 1) / TZ, (L.Ny + TY - 1) / TY);
+  const dim3 g = apply_grid(L);
   if ((long)g.x * g.y > kNoAllocPartials) {
     set_error("grid of %u tiles exceeds the no-alloc partial-sum slots", g.x * g.y);
     return SCY_ERR_ARG;
   }
-  stencil_kernel<double, Ld, Ep><<<g, 256, 0, s>>>(L, ld, ep, partials, counter, out);
+  launch_apply<double, Ld, Ep>(L, ld, ep, partials, counter, out, s);
   SCY_LAUNCH_CHECK();
   return SCY_OK;
 }

@@ -294,13 +294,13 @@ __global__ void __launch_bounds__(128, PAIR ? 2 : 1)
 }
 
 // digits of one row per warp, in two coalesced passes over the row (the
-// second from L1): lane l takes the positions 32 t + l, so every load and
-// every digit store of the warp covers consecutive addresses.  The first
-// pass gives the row maximum (a warp reduction) and so the row's exponent;
-// the second writes the S digits of each position (one byte, or the two
-// bytes of the digit's bf16 pattern: the upper half of its FP32 pattern,
-// exact for |d| <= 256).  No per-lane arrays, so many rows are in flight
-// per SM.
+// second from L1).  The first pass (lane l reads positions 32 t + l) gives
+// the row maximum (a warp reduction) and so the row's exponent; in the
+// second lane l takes the four consecutive positions 128 t + 4 l .. + 3 and
+// writes their S digits with one store per plane (four bytes, or the four
+// bf16 patterns of the digits: the upper halves of their FP32 patterns,
+// exact for |d| <= 256).  Kp is a multiple of 4, so every store is aligned
+// and inside the row.
 template <typename Tin, int BF>
 __global__ void __launch_bounds__(256) ozk_split_kernel(const Tin* __restrict__ X, long ldx, int rows, int K, int Kp,
                                                         int S, unsigned char* __restrict__ dig, long plane,
@@ -314,16 +314,31 @@ __global__ void __launch_bounds__(256) ozk_split_kernel(const Tin* __restrict__ 
   m = warp_max(m);
   const int e = m > 0.0 ? ilogb(m) + 2 : 0;
   if (lane == 0) expo[row] = e;
-  for (int k = lane; k < Kp; k += 32) {
-    double t = k < K ? ldexp((double)x[k], 7 - e) : 0.0;
+  for (int k0 = 4 * lane; k0 < Kp; k0 += 128) {
+    double t[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) t[u] = k0 + u < K ? ldexp((double)x[k0 + u], 7 - e) : 0.0;
+    const long at = (long)row * Kp + k0;
     for (int i = 0; i < S; ++i) {
-      const double d = rint(t);
-      t = (t - d) * 128.0;
-      const long at = (long)i * plane + (long)row * Kp + k;
+      uint32_t w0 = 0, w1 = 0;
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const double d = rint(t[u]);
+        t[u] = (t[u] - d) * 128.0;
+        if (BF) {
+          const uint32_t h = __float_as_uint((float)d) >> 16;
+          if (u < 2)
+            w0 |= h << (16 * u);
+          else
+            w1 |= h << (16 * (u - 2));
+        } else {
+          w0 |= (uint32_t)(uint8_t)(int8_t)(int)d << (8 * u);
+        }
+      }
       if (BF)
-        reinterpret_cast<uint16_t*>(dig)[at] = (uint16_t)(__float_as_uint((float)d) >> 16);
+        *reinterpret_cast<uint2*>(reinterpret_cast<uint16_t*>(dig) + (long)i * plane + at) = make_uint2(w0, w1);
       else
-        reinterpret_cast<int8_t*>(dig)[at] = (int8_t)(int)d;
+        *reinterpret_cast<uint32_t*>(dig + (long)i * plane + at) = w0;
     }
   }
 }

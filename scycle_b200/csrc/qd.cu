@@ -42,6 +42,28 @@ __global__ void qd_fault_kernel(LevelDev<double> L, const double* __restrict__ u
   fault_node_update(iz, sxy, fp, var, f, slipVel, tauQSP, tauP, strength, flags, its_total);
 }
 
+// Fault_qd::d_dt with the body's shear stress on the fault given by the
+// caller (the fault-row sxy a driver gets from its own solve and muxDy).
+__global__ void qd_fault_given_tau_kernel(const double* __restrict__ tau_body, FaultParams fp,
+                                          const double* __restrict__ var, double* __restrict__ f,
+                                          double* __restrict__ slipVel, double* __restrict__ tauQSP,
+                                          double* __restrict__ tauP, double* __restrict__ strength, unsigned* flags,
+                                          unsigned long long* its_total) {
+  int iz = blockIdx.x * blockDim.x + threadIdx.x;
+  if (iz >= fp.Nz) return;
+  fault_node_update(iz, tau_body[iz], fp, var, f, slipVel, tauQSP, tauP, strength, flags, its_total);
+}
+
+int QDContext::fault_d_dt(const double* var, const double* tau_body, double* f) {
+  const int tb = 64, gb = (Nz + tb - 1) / tb;
+  qd_fault_given_tau_kernel<<<gb, tb, 0, sbp.stream>>>(tau_body, fp, var, f, slipVel.as<double>(),
+                                                       tauQSP.as<double>(), tauP.as<double>(),
+                                                       strength.as<double>(), flags.as<unsigned>(),
+                                                       fault_its.as<unsigned long long>());
+  SCY_LAUNCH_CHECK();
+  return SCY_OK;
+}
+
 // Fault column stress of a body displacement, for building the response
 // matrices: out[iz * ld + col] = mu * Dy u at (0, iz); surf[iy * ld + col] = u(iy, 0).
 __global__ void qd_response_column_kernel(LevelDev<double> L, const double* __restrict__ u, double* __restrict__ out,

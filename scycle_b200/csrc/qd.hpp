@@ -118,6 +118,8 @@ struct QDContext {
   double compute_min_dt(const std::vector<double>& cs, double Ly, double Lz) const;
   // f = d_dt(t, var) with var = [psi | slip] and f = [dpsi | dslip] (device, 2*Nz each)
   int d_dt(double t, const double* var, double* f);
+  // the fault's rates alone, given the body's shear stress on the fault
+  int fault_d_dt(const double* var, const double* tau_body, double* f);
   int integrate_begin(const scy_ode_opts& o);
   // A fresh integrator object of a driver that restarts the RK per phase
   // (strikeSlip_linearElastic_qd_fd.cpp:1436-1508, :891-956): time range

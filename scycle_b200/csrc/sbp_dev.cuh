@@ -53,13 +53,27 @@ struct LevelDev {
   // one 9-point stencil per direction: sy(i) = sum_o Cy[i*9 + o+4] x(i+o, iz)
   // and sz at column iz = sum_o CzT[(o+4)*Nz + iz] x(iy, iz+o) (host-built).
   const T *Cy, *CzT;
-  // full = 1: the coefficient fields are separable over every node, so the
-  // whole operator (closures and SAT terms included) composes into one
-  // 17-point stencil per row and per column (offsets -8..8):
-  // (A x)(iy,iz) = wy1[iz] sum_o Cy17[iy*17 + o+8] x(iy+o, iz)
-  //              + wz1[iy] sum_o CzT17[(o+8)*Nz + iz] x(iy, iz+o)
+  // full = 1: the outer weights are separable over every node (wy = wy1[iz],
+  // wz = wz1[iy]) and the line coefficients (cy, m3y down a column; cz, m3z
+  // along a row) are those of the separable interior on all but a few
+  // lines, so the whole operator (closures and SAT terms included) composes
+  // into one 17-point stencil per row and per column (offsets -8..8), one
+  // table per line class (class 0: the separable lines; one class per
+  // exceptional line, e.g. the flattened-index m3 average at the grid's
+  // corners):
+  // (A x)(iy,iz) = wy1[iz] sum_o Cy17[(ycls[iz]*Ny + iy)*17 + o+8] x(iy+o, iz)
+  //              + wz1[iy] sum_o CzT17[(zcls[iy]*17 + o+8)*Nz + iz] x(iy, iz+o)
   int full;
   const T *Cy17, *CzT17;
+  const int *ycls, *zcls;  // Nz, Ny
+  // Full form only: rows [ylo, yhi] and columns [zlo, zhi] of class 0 whose
+  // class-0 stencils have no entry beyond offsets -4..4 (bitwise zeros
+  // there), so a tile inside both ranges needs a halo of 4; crow / ccol = 1
+  // when all those rows (columns) carry the same 9 entries, held in cyc /
+  // czc (a constant grid's interior).  rpt: output rows per thread of the
+  // full-form tile.
+  int ylo, yhi, zlo, zhi, crow, ccol, rpt;
+  T cyc[BAND], czc[BAND];
 };
 
 // -------------------------------------------------------------------------
@@ -202,34 +216,7 @@ __device__ __forceinline__ void stencil_tile(const LevelDev<T>& L, const Loader&
     xs_z[i] = v;
   }
   __syncthreads();
-  // Interior tiles (every stage-1 row in the interior band of both
-  // directions) use the constant interior stencil from the kernel parameters.
-  if (L.full) {
-    const int ty = tid / TZ, tz = tid % TZ;
-    const int iy = y0 + ty, iz = z0 + tz;
-    double contrib = 0.0;
-    if (iy < Ny && iz < Nz) {
-      const long node = (long)iy * Nz + iz;
-      const T* cy = L.Cy17 + (long)iy * 17;
-      const T* xy = xs_y + (ty + HX) * TZ + tz;
-      const T* xz = xs_z + ty * (TZ + 2 * HX) + tz + HX;
-      T sy = T(0), sz = T(0);
-#pragma unroll
-      for (int o = 0; o < 17; ++o) {
-        sy += cy[o] * xy[(o - 8) * TZ];
-        sz += L.CzT17[(long)o * Nz + iz] * xz[o - 8];
-      }
-      T Ax = L.wy1[iz] * sy + L.wz1[iy] * sz;
-      contrib = ep(node, iy, iz, Ax, xy[0]);
-    }
-    if constexpr (Epi::kReduce) {
-      if (partials != nullptr) {
-        double tot = block_sum(contrib, red);
-        grid_reduce_finish(tot, partials, counter, red_out, red);
-      }
-    }
-    return;
-  }
+  // (full-form levels take full_tile instead)
   const bool fast = L.y.fast && L.z.fast && y0 - HG >= 4 && y0 + TY + HG - 1 <= Ny - 6 && z0 - HG >= 4 &&
                     z0 + TZ + HG - 1 <= Nz - 6;
   if (fast && L.sep) {
@@ -425,6 +412,148 @@ __device__ __forceinline__ void stencil_tile(const LevelDev<T>& L, const Loader&
   }
 }
 
+// -------------------------------------------------------------------------
+// Full-form tile (L.full = 1: the whole operator is one 17-point stencil per
+// row and per column, see LevelDev).  A block of 256 threads owns 8*RPT rows x
+// 32 columns: warp w the rows w*RPT .. w*RPT+RPT-1, a lane one column.  The
+// tile and its halo are staged once in shared memory.  In an interior tile
+// (rows in [ylo, yhi], columns in [zlo, zhi]) a thread keeps its column's
+// RPT+8 values along y and its column's 9 z entries in registers, so an
+// output costs 9 + 9 multiply-adds and 8 shared-memory reads; the other tiles
+// use all 17 offsets (halo 8, zeros outside the grid).  Sums run over the
+// offsets in increasing order as in the 17-point form (the skipped entries
+// are zeros).
+
+// values of the shared array full_apply stages into
+template <int RPT>
+constexpr int full_smem_values() {
+  return (8 * RPT + 16) * (TZ + 16);
+}
+
+// Stages rows y0-H .. y0+TYB+H-1 of columns z0 .. z0+31 at (r, H + c) and
+// columns z0-H .. z0-1, z0+32 .. z0+31+H of rows y0 .. y0+TYB-1 at
+// (r + H, c) of xs (pitch 32 + 2H) through ld(node, iy, iz), zeros outside
+// the grid when CHECK (else every node is inside).  256 threads; a thread
+// issues all its loads before its stores, so they are in flight together.
+template <typename T, int TYB, int H, bool CHECK, class Loader>
+__device__ __forceinline__ void full_stage(const Loader& ld, T* xs, int y0, int z0, int Ny, int Nz) {
+  constexpr int W = TZ + 2 * H, NM = (TYB + 2 * H) * TZ, NT = NM + TYB * 2 * H, NV = (NT + 255) / 256;
+  const int tid = threadIdx.x;
+  T v[NV];
+  int at[NV];
+#pragma unroll
+  for (int a = 0; a < NV; ++a) {
+    const int i = tid + 256 * a;
+    int iy, iz, sx;
+    if (i < NM) {
+      const int r = i >> 5, c = i & 31;
+      iy = y0 - H + r;
+      iz = z0 + c;
+      sx = r * W + H + c;
+    } else {
+      const int j = i - NM, r = j / (2 * H), k = j % (2 * H), c = k < H ? k : TZ + k;
+      iy = y0 + r;
+      iz = z0 - H + c;
+      sx = (r + H) * W + c;
+    }
+    at[a] = i < NT ? sx : -1;
+    v[a] = T(0);
+    if (i < NT && (!CHECK || (iy >= 0 && iy < Ny && iz >= 0 && iz < Nz))) v[a] = ld((long)iy * Nz + iz, iy, iz);
+  }
+#pragma unroll
+  for (int a = 0; a < NV; ++a)
+    if (at[a] >= 0) xs[at[a]] = v[a];
+}
+
+// The tile of block (blockIdx.x, blockIdx.y): stages the operand through
+// ld(node, iy, iz) into xs and calls out(node, iy, iz, A x, x) once per
+// output node of the tile; after each of its RPT rows j every thread of the
+// block calls row(j) (warp-uniform, so a row's values can be summed across
+// the warp there).
+template <typename T, int RPT, class Loader, class Out, class Row>
+__device__ __forceinline__ void full_apply(const LevelDev<T>& L, const Loader& ld, Out& out, Row& row, T* xs) {
+  constexpr int TYB = 8 * RPT;
+  const int Ny = L.Ny, Nz = L.Nz;
+  const int y0 = blockIdx.y * TYB, z0 = blockIdx.x * TZ;
+  const int tid = threadIdx.x, lane = tid & 31, r0 = (tid >> 5) * RPT;
+  const bool inner = y0 >= L.ylo && y0 + TYB - 1 <= L.yhi && z0 >= L.zlo && z0 + TZ - 1 <= L.zhi;
+  if (inner) {
+    constexpr int H = HALF, W = TZ + 2 * H;
+    full_stage<T, TYB, H, false>(ld, xs, y0, z0, Ny, Nz);  // all inside the grid
+    __syncthreads();
+    const int iz = z0 + lane;
+    T win[RPT + 2 * H];
+#pragma unroll
+    for (int k = 0; k < RPT + 2 * H; ++k) win[k] = xs[(r0 + k) * W + H + lane];
+    T cz[BAND];
+#pragma unroll
+    for (int o = 0; o < BAND; ++o) cz[o] = L.ccol ? L.czc[o] : L.CzT17[(long)(o + 8 - HALF) * Nz + iz];
+    const T wyv = L.wy1[iz];
+#pragma unroll
+    for (int j = 0; j < RPT; ++j) {
+      const int iy = y0 + r0 + j;
+      const T* cy = L.Cy17 + (long)iy * 17 + (8 - HALF);
+      const T* xr = xs + (r0 + j + H) * W + lane;  // columns iz-4 .. iz+4
+      T sy = T(0), sz = T(0);
+#pragma unroll
+      for (int o = 0; o < BAND; ++o) {
+        sy += (L.crow ? L.cyc[o] : cy[o]) * win[j + o];
+        sz += cz[o] * (o == HALF ? win[j + HALF] : xr[o]);
+      }
+      const T Ax = wyv * sy + L.wz1[iy] * sz;
+      out((long)iy * Nz + iz, iy, iz, Ax, win[j + HALF]);
+      row(j);
+    }
+  } else {
+    constexpr int H = 8, W = TZ + 2 * H;
+    full_stage<T, TYB, H, true>(ld, xs, y0, z0, Ny, Nz);
+    __syncthreads();
+    const int iz = z0 + lane;
+#pragma unroll
+    for (int j = 0; j < RPT; ++j) {
+      const int iy = y0 + r0 + j;
+      if (iz < Nz && iy < Ny) {
+        const T* cy = L.Cy17 + ((long)L.ycls[iz] * Ny + iy) * 17;
+        const T* cz = L.CzT17 + (long)L.zcls[iy] * 17 * Nz + iz;
+        const T* xy = xs + (r0 + j) * W + H + lane;  // rows iy-8 .. iy+8, stride W
+        const T* xz = xs + (r0 + j + H) * W + lane;  // columns iz-8 .. iz+8
+        T sy = T(0), sz = T(0);
+#pragma unroll
+        for (int o = 0; o < 17; ++o) {
+          sy += cy[o] * xy[o * W];
+          sz += cz[(long)o * Nz] * xz[o];
+        }
+        const T Ax = L.wy1[iz] * sy + L.wz1[iy] * sz;
+        out((long)iy * Nz + iz, iy, iz, Ax, xy[H * W]);
+      }
+      row(j);
+    }
+  }
+}
+
+template <typename T, int RPT, class Loader, class Epi>
+__device__ __forceinline__ void full_tile(const LevelDev<T>& L, const Loader& ld, const Epi& ep, double* partials,
+                                          unsigned int* counter, double* red_out) {
+  __shared__ T xs[full_smem_values<RPT>()];
+  __shared__ double red[32];
+  double contrib = 0.0;
+  auto out = [&](long node, int iy, int iz, T Ax, T xv) { contrib += ep(node, iy, iz, Ax, xv); };
+  auto row = [](int) {};
+  full_apply<T, RPT>(L, ld, out, row, xs);
+  if constexpr (Epi::kReduce) {
+    if (partials != nullptr) {  // uniform across the grid
+      double tot = block_sum(contrib, red);
+      grid_reduce_finish(tot, partials, counter, red_out, red);
+    }
+  }
+}
+
+template <typename T, int RPT, class Loader, class Epi>
+__global__ void __launch_bounds__(256) full_kernel(LevelDev<T> L, Loader ld, Epi ep, double* partials,
+                                                   unsigned int* counter, double* red_out) {
+  full_tile<T, RPT, Loader, Epi>(L, ld, ep, partials, counter, red_out);
+}
+
 // rhs at one node from the boundary data (SbpOps::setRhs,
 // sbpOps_m_constGrid.cpp:877-914): the SAT columns of the Dirichlet
 // boundaries and the Neumann boundary values, times the outer weights.
@@ -478,6 +607,30 @@ template <typename T, class Loader, class Epi>
 __global__ void __launch_bounds__(256) stencil_kernel(LevelDev<T> L, Loader ld, Epi ep, double* partials,
                                                       unsigned int* counter, double* red_out) {
   stencil_tile<T, Loader, Epi>(L, ld, ep, partials, counter, red_out);
+}
+
+// Launch grid of an operator application: full-form tiles of 8*rpt x 32 when
+// L.full, else the 8 x 32 tiles of stencil_tile.
+template <typename T>
+inline dim3 apply_grid(const LevelDev<T>& L) {
+  const int ty = L.full ? 8 * L.rpt : TY;
+  return dim3((L.Nz + TZ - 1) / TZ, (L.Ny + ty - 1) / ty);
+}
+
+// One operator application with the loader / epilogue given (the kernel the
+// level's form calls for); 256 threads per block.
+template <typename T, class Loader, class Epi>
+inline void launch_apply(const LevelDev<T>& L, const Loader& ld, const Epi& ep, double* partials,
+                         unsigned int* counter, double* red_out, cudaStream_t s) {
+  const dim3 g = apply_grid(L);
+  if (!L.full)
+    stencil_kernel<T, Loader, Epi><<<g, 256, 0, s>>>(L, ld, ep, partials, counter, red_out);
+  else if (L.rpt == 4)
+    full_kernel<T, 4, Loader, Epi><<<g, 256, 0, s>>>(L, ld, ep, partials, counter, red_out);
+  else if (L.rpt == 2)
+    full_kernel<T, 2, Loader, Epi><<<g, 256, 0, s>>>(L, ld, ep, partials, counter, red_out);
+  else
+    full_kernel<T, 1, Loader, Epi><<<g, 256, 0, s>>>(L, ld, ep, partials, counter, red_out);
 }
 
 }  // namespace scy

@@ -4,6 +4,7 @@
 // SbpOps_m_constGrid / SbpOps_m_varGrid with multiplyByH = 1
 // (source/sbpOps_m_constGrid.cpp:606-701, 963-1315;
 //  source/sbpOps_m_varGrid.cpp:333-436, 1133-1504).
+#include <algorithm>
 #include "sbp_host.hpp"
 
 #include <cmath>
@@ -574,6 +575,111 @@ void apply_cross_planes(const std::vector<double>& C, int Ny, int Nz, const doub
         s += C[(size_t)(o < 0 ? 25 + o : 24 + o) * N + node] * x[(size_t)iy * Nz + jz];
       }
       out[node] = s;
+    }
+}
+
+bool build_full_form(const LevelHost& h, FullForm& f) {
+  const int Ny = h.Ny, Nz = h.Nz;
+  if (h.order != 4 || Ny < 17 || Nz < 17) return false;
+  const int iy_ref = Ny / 2, iz_ref = Nz / 2;
+  std::vector<double> cy1(Ny), m3y1(Ny), cz1(Nz), m3z1(Nz);
+  f.wy1.assign(Nz, 0.0);
+  f.wz1.assign(Ny, 0.0);
+  for (int iy = 0; iy < Ny; ++iy) {
+    const size_t i = (size_t)iy * Nz + iz_ref;
+    cy1[iy] = h.cy[i];
+    m3y1[iy] = h.m3y[i];
+    f.wz1[iy] = h.wz[i];
+  }
+  for (int iz = 0; iz < Nz; ++iz) {
+    const size_t i = (size_t)iy_ref * Nz + iz;
+    cz1[iz] = h.cz[i];
+    m3z1[iz] = h.m3z[i];
+    f.wy1[iz] = h.wy[i];
+  }
+  f.ycls.assign(Nz, 0);
+  f.zcls.assign(Ny, 0);
+  std::vector<int> yexc, zexc;
+  for (int iy = 0; iy < Ny; ++iy)
+    for (int iz = 0; iz < Nz; ++iz) {
+      const size_t i = (size_t)iy * Nz + iz;
+      if (h.wy[i] != f.wy1[iz] || h.wz[i] != f.wz1[iy]) return false;
+      if ((h.cy[i] != cy1[iy] || h.m3y[i] != m3y1[iy]) && !f.ycls[iz]) {
+        yexc.push_back(iz);
+        f.ycls[iz] = (int)yexc.size();
+      }
+      if ((h.cz[i] != cz1[iz] || h.m3z[i] != m3z1[iz]) && !f.zcls[iy]) {
+        zexc.push_back(iy);
+        f.zcls[iy] = (int)zexc.size();
+      }
+      if (yexc.size() > (size_t)kMaxLineClasses || zexc.size() > (size_t)kMaxLineClasses) return false;
+    }
+  const int ncy = 1 + (int)yexc.size(), ncz = 1 + (int)zexc.size();
+  f.Cy17.assign((size_t)ncy * Ny * 17, 0.0);
+  f.CzT17.assign((size_t)ncz * 17 * Nz, 0.0);
+  std::vector<double> L17, c1, m31;
+  for (int c = 0; c < ncy; ++c) {
+    c1 = cy1;
+    m31 = m3y1;
+    if (c > 0)
+      for (int iy = 0; iy < Ny; ++iy) {
+        c1[iy] = h.cy[(size_t)iy * Nz + yexc[c - 1]];
+        m31[iy] = h.m3y[(size_t)iy * Nz + yexc[c - 1]];
+      }
+    compose_line(h.ty, h.bc[2], h.bc[0], c1, m31, L17);
+    std::copy(L17.begin(), L17.end(), f.Cy17.begin() + (size_t)c * Ny * 17);
+  }
+  for (int c = 0; c < ncz; ++c) {
+    c1 = cz1;
+    m31 = m3z1;
+    if (c > 0) {
+      const size_t r = (size_t)zexc[c - 1] * Nz;
+      c1.assign(h.cz.begin() + r, h.cz.begin() + r + Nz);
+      m31.assign(h.m3z.begin() + r, h.m3z.begin() + r + Nz);
+    }
+    compose_line(h.tz, h.bc[1], h.bc[3], c1, m31, L17);
+    for (int iz = 0; iz < Nz; ++iz)
+      for (int o = 0; o < 17; ++o) f.CzT17[((size_t)c * 17 + o) * Nz + iz] = L17[(size_t)iz * 17 + o];
+  }
+  // the interior box: class-0 lines around the middle whose class-0
+  // stencils vanish beyond offsets -4..4 (cross: the other direction's
+  // classes, since an interior tile holds class-0 lines only)
+  auto range = [](int n, const std::vector<int>& cross, auto entry, int& lo, int& hi) {
+    auto nine = [&](int i) {
+      if (i < kHalf || i > n - 1 - kHalf || cross[i] != 0) return false;
+      for (int o = 0; o < 8 - kHalf; ++o)
+        if (entry(i, o) != 0.0 || entry(i, 16 - o) != 0.0) return false;
+      return true;
+    };
+    lo = 1;
+    hi = 0;
+    const int m = n / 2;
+    if (!nine(m)) return;
+    lo = hi = m;
+    while (nine(lo - 1)) --lo;
+    while (nine(hi + 1)) ++hi;
+  };
+  range(Ny, f.zcls, [&](int i, int o) { return f.Cy17[(size_t)i * 17 + o]; }, f.ylo, f.yhi);
+  range(Nz, f.ycls, [&](int i, int o) { return f.CzT17[(size_t)o * Nz + i]; }, f.zlo, f.zhi);
+  return true;
+}
+
+void apply_full_form(const FullForm& f, int Ny, int Nz, const double* x, double* out) {
+  for (int iy = 0; iy < Ny; ++iy)
+    for (int iz = 0; iz < Nz; ++iz) {
+      const bool inner = iy >= f.ylo && iy <= f.yhi && iz >= f.zlo && iz <= f.zhi;
+      const int lo = inner ? 8 - kHalf : 0, hi = inner ? 8 + kHalf : 16;
+      const double* cy = &f.Cy17[((size_t)f.ycls[iz] * Ny + iy) * 17];
+      const double* cz = &f.CzT17[(size_t)f.zcls[iy] * 17 * Nz + iz];
+      double sy = 0.0, sz = 0.0;
+      for (int o = lo; o <= hi; ++o) {
+        const int jy = iy + o - 8, jz = iz + o - 8;
+        const double xy = jy >= 0 && jy < Ny ? x[(size_t)jy * Nz + iz] : 0.0;
+        const double xz = jz >= 0 && jz < Nz ? x[(size_t)iy * Nz + jz] : 0.0;
+        sy += cy[o] * xy;
+        sz += cz[(size_t)o * Nz] * xz;
+      }
+      out[(size_t)iy * Nz + iz] = f.wy1[iz] * sy + f.wz1[iy] * sz;
     }
 }
 

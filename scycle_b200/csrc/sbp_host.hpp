@@ -94,6 +94,28 @@ void compose_line(const DirTables& t, int bc_lo, int bc_hi, const std::vector<do
 // (each column's y operator and each row's z operator composed with that
 // line's coefficients, times the outer weights wy and wz).
 void build_cross_planes(const LevelHost& h, std::vector<double>& C);
+
+// The full form of a level: the outer weights separable over every node
+// (wy = wy1[iz], wz = wz1[iy]) and the line coefficients (cy, m3y down a
+// column; cz, m3z along a row) equal to those of the middle column / row on
+// all but at most kMaxLineClasses exceptional lines per direction, so
+// (A x)(iy,iz) = wy1[iz] sum_o Cy17[(ycls[iz]*Ny + iy)*17 + o+8] x(iy+o, iz)
+//              + wz1[iy] sum_o CzT17[(zcls[iy]*17 + o+8)*Nz + iz] x(iy, iz+o)
+// (class 0: the middle line's composition; class c > 0: exceptional line c).
+// [ylo, yhi] x [zlo, zhi]: the class-0 rows / columns around the middle
+// whose class-0 stencils vanish beyond offsets -4..4 (empty when lo > hi).
+constexpr int kMaxLineClasses = 8;
+struct FullForm {
+  std::vector<double> Cy17, CzT17, wy1, wz1;
+  std::vector<int> ycls, zcls;
+  int ylo = 1, yhi = 0, zlo = 1, zhi = 0;
+};
+// false when the level has no full form (order 2, a direction shorter than
+// 17 points, non-separable weights or too many exceptional lines)
+bool build_full_form(const LevelHost& h, FullForm& f);
+// A x from the full form, 9-point on the interior box and 17-point elsewhere
+// (the device's arithmetic order)
+void apply_full_form(const FullForm& f, int Ny, int Nz, const double* x, double* out);
 // Host reference of the cross-plane form (for checking it against apply_A).
 void apply_cross_planes(const std::vector<double>& C, int Ny, int Nz, const double* x, double* out);
 

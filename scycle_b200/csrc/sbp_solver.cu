@@ -7,9 +7,11 @@
 // geometric-multigrid V-cycle (rediscretised SBP-SAT operators on coarsened
 // grids, Chebyshev-Jacobi smoothing, bilinear transfer, dense coarsest solve)
 // run in FP64 or FP32.
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstdarg>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <stdexcept>
@@ -255,28 +257,47 @@ int LevelStore<T>::init(const LevelHost& h, cudaStream_t s) {
       SCY_TRY(upload<T>(comp[1], CzT, s));
       dev.Cy = comp[0].template as<T>();
       dev.CzT = comp[1].template as<T>();
-      // separable over every node too?  then compose the whole operator
-      bool all = true;
-      for (int iy = 0; all && iy < Ny; ++iy)
-        for (int iz = 0; iz < Nz; ++iz) {
-          const size_t i = (size_t)iy * Nz + iz;
-          if (h.cy[i] != cy1[iy] || h.m3y[i] != m3y1[iy] || h.wz[i] != wz1[iy] || h.cz[i] != cz1[iz] ||
-              h.m3z[i] != m3z1[iz] || h.wy[i] != wy1[iz]) {
-            all = false;
-            break;
-          }
-        }
-      if (all) {
-        std::vector<double> Cy17, Cz17, CzT17((size_t)17 * Nz);
-        compose_line(h.ty, h.bc[2], h.bc[0], cy1, m3y1, Cy17);
-        compose_line(h.tz, h.bc[1], h.bc[3], cz1, m3z1, Cz17);
-        for (int iz = 0; iz < Nz; ++iz)
-          for (int o = 0; o < 17; ++o) CzT17[(size_t)o * Nz + iz] = Cz17[(size_t)iz * 17 + o];
-        SCY_TRY(upload<T>(comp17[0], Cy17, s));
-        SCY_TRY(upload<T>(comp17[1], CzT17, s));
+      // the full form (LevelDev::full, build_full_form)
+      FullForm F;
+      if (build_full_form(h, F)) {
+        SCY_TRY(upload<T>(comp17[0], F.Cy17, s));
+        SCY_TRY(upload<T>(comp17[1], F.CzT17, s));
+        SCY_TRY(upload_ints<T>(cls[0], F.ycls, s));
+        SCY_TRY(upload_ints<T>(cls[1], F.zcls, s));
         dev.Cy17 = comp17[0].template as<T>();
         dev.CzT17 = comp17[1].template as<T>();
+        dev.ycls = cls[0].template as<int>();
+        dev.zcls = cls[1].template as<int>();
         dev.full = 1;
+        dev.ylo = F.ylo;
+        dev.yhi = F.yhi;
+        dev.zlo = F.zlo;
+        dev.zhi = F.zhi;
+        // whether the interior box's rows (columns) all carry the same 9
+        // entries in the stored precision (a constant grid)
+        auto same9 = [](int lo, int hi, auto entry, int& same, T* c9) {
+          same = lo <= hi ? 1 : 0;
+          for (int i = lo; same && i <= hi; ++i)
+            for (int o = 0; o < BAND; ++o)
+              if ((T)entry(i, o) != (T)entry(lo, o)) same = 0;
+          for (int o = 0; o < BAND; ++o) c9[o] = same ? (T)entry(lo, o) : T(0);
+        };
+        same9(F.ylo, F.yhi, [&](int i, int o) { return F.Cy17[(size_t)i * 17 + 8 - HALF + o]; }, dev.crow, dev.cyc);
+        same9(F.zlo, F.zhi, [&](int i, int o) { return F.CzT17[(size_t)(8 - HALF + o) * Nz + i]; }, dev.ccol,
+              dev.czc);
+        // rows per thread: the tallest tile that still gives about six
+        // blocks per SM (SCY_FULL_RPT = 1, 2 or 4 overrides)
+        const long cols = (Nz + TZ - 1) / TZ;
+        dev.rpt = 1;
+        for (int r : {4, 2})
+          if (cols * ((Ny + 8 * r - 1) / (8 * r)) >= 6L * kNumSMs) {
+            dev.rpt = r;
+            break;
+          }
+        if (const char* e = getenv("SCY_FULL_RPT")) {
+          const int r = atoi(e);
+          if (r == 1 || r == 2 || r == 4) dev.rpt = r;
+        }
       }
       dev.cy1 = sep1[0].template as<T>();
       dev.m3y1 = sep1[1].template as<T>();
@@ -293,12 +314,9 @@ int LevelStore<T>::init(const LevelHost& h, cudaStream_t s) {
 template struct LevelStore<double>;
 template struct LevelStore<float>;
 
-static dim3 tile_grid(int Ny, int Nz) { return dim3((Nz + TZ - 1) / TZ, (Ny + TY - 1) / TY); }
-
 template <typename T, class Ld, class Ep>
 static int launch_stencil(const LevelDev<T>& L, Ld ld, Ep ep, Reducer* red, double* out, cudaStream_t s,
                           int level = 0) {
-  dim3 g = tile_grid(L.Ny, L.Nz);
   double* parts = red ? red->partials.template as<double>() : nullptr;
   unsigned* cnt = red ? red->counter.template as<unsigned>() : nullptr;
   ProfRec rec{};
@@ -307,7 +325,7 @@ static int launch_stencil(const LevelDev<T>& L, Ld ld, Ep ep, Reducer* red, doub
     cudaEventCreate(&rec.b);
     cudaEventRecord(rec.a, s);
   }
-  stencil_kernel<T, Ld, Ep><<<g, 256, 0, s>>>(L, ld, ep, parts, cnt, out);
+  launch_apply<T, Ld, Ep>(L, ld, ep, parts, cnt, out, s);
   SCY_LAUNCH_CHECK();
   if (g_prof) {
     cudaEventRecord(rec.b, s);

@@ -58,7 +58,8 @@ struct LevelStore {
   DevBuf fld[10];     // cy, cz, m3y, m3z, wy, wz, mu, qy, rz, dinv
   DevBuf sep1[6];     // cy1, m3y1, wz1 (Ny), cz1, m3z1, wy1 (Nz) when separable
   DevBuf comp[2];     // composed interior stencils Cy (Ny x 9) and CzT (9 x Nz)
-  DevBuf comp17[2];   // composed whole-operator stencils Cy17 (Ny x 17), CzT17 (17 x Nz)
+  DevBuf comp17[2];   // composed whole-operator stencils Cy17 (classes x Ny x 17), CzT17 (classes x 17 x Nz)
+  DevBuf cls[2];      // line classes of the full form: ycls (Nz), zcls (Ny)
   LevelDev<T> dev{};
   int init(const LevelHost& h, cudaStream_t s);
 };

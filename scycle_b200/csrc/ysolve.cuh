@@ -58,7 +58,7 @@ __global__ void __launch_bounds__(32 * W) b_ysolve_tma_kernel(const __grid_const
                                                               const __grid_constant__ CUtensorMap mT,
                                                               T* __restrict__ t, int Ny, int Nz, int Nzp, int K,
                                                               unsigned* __restrict__ status,
-                                                              int first_polls = 1 << 18) {
+                                                              int first_polls = 1 << 18, int drop_first = 0) {
   constexpr int B = 2 * W * I;
   extern __shared__ __align__(128) unsigned char ys_smem[];
   constexpr int CT = YS_R * 9 * YS_C, DT = B * YS_R * YS_C;  // elements per tile
@@ -87,7 +87,10 @@ __global__ void __launch_bounds__(32 * W) b_ysolve_tma_kernel(const __grid_const
   __syncthreads();
   // chunk g of the 2 * nch chunks (forward 0..nch-1 from row 0, back
   // nch..2nch-1 from row Ny-1) into stage g % YS_S
+  // drop_first (a test hook): the first chunk's copy is never issued, so
+  // its wait runs out (no copy of it is in flight to await afterwards)
   auto issue = [&](int g) {
+    if (drop_first && g == 0) return;
     const int st = g % YS_S;
     mbar_expect_tx(&bar[st], bytes);
     const bool fwd = g < nch;
@@ -172,7 +175,8 @@ __global__ void __launch_bounds__(32 * W) b_ysolve_tma_kernel(const __grid_const
     if (leader) {
       for (int q = 0; q < B && kb + q < K; ++q) atomicOr(status + kb + q, 4u);
       // let the loads already issued land before the block's shared memory goes
-      for (int q = g; q < g + YS_S && q < 2 * nch; ++q) mbar_wait(&bar[q % YS_S], (q / YS_S) & 1, kPolls);
+      for (int q = g; q < g + YS_S && q < 2 * nch; ++q)
+        if (!(drop_first && q == 0)) mbar_wait(&bar[q % YS_S], (q / YS_S) & 1, kPolls);
     }
     __syncthreads();
   }

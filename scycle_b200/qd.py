@@ -135,6 +135,19 @@ class QD:
         o = out.cpu().numpy()
         return {"psi": o[:self.Nz], "slip": o[self.Nz:]}
 
+    def fault_d_dt(self, psi, slip, tau_body):
+        """Fault_qd::d_dt alone, the body's shear stress on the fault given
+        (scy_qd_fault_d_dt); linear-elastic state layout [psi | slip]."""
+        import torch
+        var = torch.from_numpy(np.concatenate([psi, slip]).astype(np.float64)).cuda()
+        tau = torch.from_numpy(np.ascontiguousarray(tau_body, dtype=np.float64)).cuda()
+        out = torch.zeros_like(var)
+        torch.cuda.synchronize()
+        S.check(S.lib().scy_qd_fault_d_dt(self.h, C.c_void_p(var.data_ptr()), C.c_void_p(tau.data_ptr()),
+                                          C.c_void_p(out.data_ptr())))
+        o = out.cpu().numpy()
+        return {"psi": o[:self.Nz], "slip": o[self.Nz:]}
+
     def field(self, name):
         n = self.N if name in X.BODY_FIELDS else (self.Ny if name == "surfDisp" else self.Nz)
         out = np.empty(n)

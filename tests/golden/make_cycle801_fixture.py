@@ -13,16 +13,21 @@ size deltaT_fd that prepares it).  The GPU test forces the device cycle
 driver onto the same attempts and compares the fields at those steps and
 the switch step.
 
-Beside the trajectory the fixture holds the oracle's own sensitivity
-(sens_<field>): the same attempts replayed with the steady-state initial
-slip perturbed by 1e-13.  Nucleation amplifies such a perturbation roughly
-like the slip velocity grows, so near the switch two correct FP64
-implementations differ far above rounding; the test's bar is 1e3 times this
-sensitivity (and 1e-9 while that is smaller), as in tests/test_cycle_gpu.py.
+Beside the trajectory the fixture holds two measures of the oracle's own
+uncertainty.  sens_<field>: the same attempts replayed with the
+steady-state initial slip perturbed by 1e-13; nucleation amplifies such a
+perturbation roughly like the slip velocity grows, so near the switch two
+correct FP64 implementations differ far above rounding.  spread_<field>:
+the same attempts replayed with every direct solve refined once in
+extended precision; the fault stress is a near-cancelling difference of
+displacements across the finest cell (37.5 m here), so FP64 rounding in u
+moves the slip velocity by about 1e-8 relative at this size.  The test's
+bar is the largest of 1e-9, ten times the spread and 1e3 times the
+sensitivity (as in tests/test_cycle_gpu.py and tests/golden/parity_*.npz).
 
 SuperLU factorises the 641,601-unknown operator once (about a minute, 4 GB)
-and takes about half a second per solve; the phase and its replay take
-about an hour on one core.
+and takes about half a second per solve; the phase and its two replays take
+about fifty minutes on one core.
 
     python tests/golden/make_cycle801_fixture.py
 """
@@ -49,9 +54,9 @@ class _FirstPhase(QDFDLinearElastic):
         self.hard_stop = True
 
 
-def _run(path, replay=None, perturb=0.0):
+def _run(path, replay=None, perturb=0.0, refine=0):
     P = build_qdfd_problem(open(path).read())
-    m = _FirstPhase(P)
+    m = _FirstPhase(P, refine=refine)
     if perturb:
         orig = m.solve_ss
         m.solve_ss = lambda: orig() * (1.0 + perturb)
@@ -73,6 +78,9 @@ def main():
     t0 = time.time()
     _, _, h1 = _run(path, replay=rec, perturb=1e-13)
     print("perturbed replay: %.0f s" % (time.time() - t0), flush=True)
+    t0 = time.time()
+    _, _, h2 = _run(path, replay=rec, refine=1)
+    print("refined replay: %.0f s" % (time.time() - t0), flush=True)
     out = {"attempt_dt": np.array([d for d, _ in rec]), "attempt_acc": np.array([a for _, a in rec], dtype=np.int8),
            "snap_steps": np.array(snaps), "snap_t": np.array([hist[k]["t"] for k in snaps]),
            "switch_step": np.array(first), "switch_t": np.array(m.switches[0]["t"])}
@@ -80,6 +88,8 @@ def main():
         out[f] = np.array([hist[k][f] for k in snaps])
         out["sens_" + f] = np.array([np.linalg.norm(h1[k][f] - hist[k][f]) / max(np.linalg.norm(hist[k][f]), 1e-300)
                                      for k in snaps])
+        out["spread_" + f] = np.array([np.linalg.norm(h2[k][f] - hist[k][f]) / max(np.linalg.norm(hist[k][f]), 1e-300)
+                                       for k in snaps])
     dst = os.path.join(HERE, "parity_c2qd.npz")
     np.savez_compressed(dst, **out)
     print("wrote", dst, os.path.getsize(dst), "bytes")

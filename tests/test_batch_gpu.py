@@ -229,23 +229,24 @@ def test_batch_banded_preconditioner_matches_dense(tmp_path, precision):
 
 
 def test_batch_sweep_wait_timeout_is_reported_and_recoverable(tmp_path):
-    """The banded sweeps' data waits are bounded: with the limit lowered to
-    one poll (a test hook) every wait runs out, the blocks mark their
-    instances (status bit 4) and still await the copies they issued, the
-    batch repeats the round three times and then reports SCY_ERR_TIMEOUT
-    (no hang, no fault).  With the limit restored the same batch carries on
-    and gives what an undisturbed batch gives."""
+    """The banded sweeps' data waits are bounded: with a test hook
+    withholding each block's first chunk copy (a wait that nothing
+    completes) and the limit lowered to 64 polls, the waits run out, the
+    blocks mark their instances (status bit 4) and still await the copies
+    they did issue, the batch repeats the round three times and then reports
+    SCY_ERR_TIMEOUT (no hang, no fault).  With the hook cleared the same
+    batch carries on and gives what an undisturbed batch gives."""
     from scycle_b200 import _lib as S
     paths = _le_paths(tmp_path)
     b = _batch(paths)
     ref = _batch(paths)
     b.run(2)
     ref.run(3)
-    S.check(S.lib().scy_batch_set_sweep_polls(b.h, 1))
+    S.check(S.lib().scy_batch_set_sweep_test(b.h, 64, 1))
     with pytest.raises(S.ScyError) as ei:
         b.run(1)
     assert "pipeline wait" in str(ei.value)
-    S.check(S.lib().scy_batch_set_sweep_polls(b.h, 1 << 18))
+    S.check(S.lib().scy_batch_set_sweep_test(b.h, 1 << 18, 0))
     b.run(1)
     for i in range(len(paths)):
         for f in FIELDS:

@@ -64,6 +64,38 @@ def test_d_dt_matches_oracle(tmp_path, law, grid, prestress, exact):
         assert _nrel(dev.field("surfDisp"), ora.u[::P["Nz"]]) <= REL
 
 
+@pytest.mark.parametrize("law,exact", [("agingLaw", False), ("slipLaw", True)])
+def test_fault_d_dt_alone_matches_oracle(tmp_path, law, exact):
+    """Fault_qd::d_dt on its own (scy_qd_fault_d_dt): given the body's shear
+    stress on the fault, the slip velocity from the friction root, the state
+    rate, tauQS, tauP and strength as the oracle's FaultQD.d_dt gives them;
+    and with the stress the full d_dt computed, the full d_dt's fault rates."""
+    from scycle_b200.qd import QD
+    P = _problem(tmp_path, law=law, prestress=26.5)
+    ora = QDLinearElastic(P, keep_history=False)
+    dev = QD(P, solve_rtol=SOLVE_RTOL, exact_jacobian=exact)
+    rng = np.random.default_rng(11)
+    Nz = P["Nz"]
+    psi = P["psi"] + 1e-3 * rng.standard_normal(Nz)
+    slip = 0.05 * rng.random(Nz)
+    full = dev.d_dt(2.0e8, psi, slip)
+    tau_body = dev.field("sxy")[:Nz]
+    alone = dev.fault_d_dt(psi, slip, tau_body)
+    assert _rel(alone["slip"], full["slip"], 1e-30) <= 1e-12
+    assert _rel(alone["psi"], full["psi"], 1e-12) <= 1e-12
+    v_start = dev.field("slipVel")  # the root finds start from the current slip velocity
+    tau = tau_body + rng.normal(0.0, 0.05, Nz)  # any stress, not only a solve's
+    alone = dev.fault_d_dt(psi, slip, tau)
+    f = ora.fault
+    f.update_fields({"psi": psi, "slip": slip})
+    f.slipVel = v_start.copy()
+    V_ref, dpsi_ref = f.d_dt(tau)
+    assert _rel(alone["slip"], V_ref, 1e-30) <= REL
+    assert _rel(alone["psi"], dpsi_ref, 1e-12) <= REL
+    for nm, r in (("tauQSP", f.tauQSP), ("tauP", f.tauP), ("strength", f.strength)):
+        assert _rel(dev.field(nm), r, 1e-9) <= REL, nm
+
+
 @pytest.mark.parametrize("integrator,law,steps", [("RK32", "agingLaw", 60), ("RK43", "slipLaw", 30)])
 def test_integrate_replay_matches_oracle(tmp_path, integrator, law, steps):
     from scycle_b200.qd import QD
