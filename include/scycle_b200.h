@@ -688,15 +688,20 @@ scy_status scy_batch_set_sweep_test(scy_batch* b, int polls, int drop_first_copy
  * CTAs per SM and 8-bit or bf16 digits (identical results), and keeps the
  * fastest.  kpb / sweep_variant / ztransform get the choices (kpb: the cross
  * form's, see scy_batch_operator_form for the form in use; ztransform bit 0:
- * two CTAs per SM, bit 1: bf16 digits), us (17 doubles, may be NULL) the
+ * two CTAs per SM, bit 1: bf16 digits), us (20 doubles, may be NULL) the
  * timings in microseconds per launch (cross form at kpb 1, 2, 4, 8; sweep
  * shapes 0-5; product with 8-bit digits, one and two CTAs per SM; with bf16
  * digits, one and two CTAs per SM; separable form at 1, 2, 4 rows per
- * thread; 0 where not tried). */
+ * thread with the compiler's register count, then with registers fitted to
+ * four blocks per SM; 0 where not tried).  The separable form is used
+ * whenever the operator has it (its results do not depend on its launch
+ * shape; they differ from the cross form's by rounding). */
 scy_status scy_batch_tuning(scy_batch* b, int g, int* kpb, int* sweep_variant, int* ztransform, double* us);
 /* The operator kernels group g runs: *rows_per_thread = 0 for the cross
- * form, else the separable form's rows per thread (1, 2 or 4). */
-scy_status scy_batch_operator_form(scy_batch* b, int g, int* rows_per_thread);
+ * form, else the separable form's rows per thread (1, 2 or 4), and
+ * *min_blocks_per_sm (may be NULL) the blocks per SM its registers are
+ * fitted to (1: the compiler's choice; 0 for the cross form). */
+scy_status scy_batch_operator_form(scy_batch* b, int g, int* rows_per_thread, int* min_blocks_per_sm);
 
 /* ---------------------------------------------------------------------------
  * Discrete adjoint of the linear-elastic quasi-dynamic RK32 integration.

@@ -131,7 +131,7 @@ class BatchStats(C.Structure):
 def declare_batch(L):
     L.scy_batch_tuning.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
                                    C.POINTER(C.c_double)]
-    L.scy_batch_operator_form.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int)]
+    L.scy_batch_operator_form.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     vp = C.c_void_p
     L.scy_batch_create_from_in.argtypes = [C.c_int, C.POINTER(C.c_char_p), C.POINTER(S.SolveOpts),
                                            C.POINTER(BatchOpts), C.POINTER(vp)]

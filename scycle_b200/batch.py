@@ -94,13 +94,18 @@ class Batch:
         (cross form with instances per block, or separable form with rows
         per thread), the sweep launch shape, the z-transform product's shape
         and digits, and the timings (us)."""
-        kpb, var, zt, rpt = C.c_int(), C.c_int(), C.c_int(), C.c_int()
-        us = (C.c_double * 17)()
+        kpb, var, zt, rpt, minb = C.c_int(), C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        us = (C.c_double * 20)()
         S.check(S.lib().scy_batch_tuning(self.h, int(group), C.byref(kpb), C.byref(var), C.byref(zt), us))
-        S.check(S.lib().scy_batch_operator_form(self.h, int(group), C.byref(rpt)))
+        S.check(S.lib().scy_batch_operator_form(self.h, int(group), C.byref(rpt), C.byref(minb)))
         shapes = ["2 chains x 2 warps (8 instances)", "1 chain x 4 warps (8)", "4 chains x 1 warp (8)",
                   "1 chain x 2 warps (4)", "2 chains x 1 warp (4)", "1 chain x 1 warp (2)"]
-        return {"operator_form": ("separable, %d rows per thread" % rpt.value) if rpt.value else "cross",
+        form = "cross"
+        if rpt.value:
+            form = "separable, %d rows per thread, %s" % (
+                rpt.value, "registers fitted to %d blocks per SM" % minb.value if minb.value > 1
+                else "compiler's register count")
+        return {"operator_form": form,
                 "instances_per_block": kpb.value, "sweep_variant": shapes[var.value],
                 "ztransform_ctas_per_sm": 2 if zt.value & 1 else 1,
                 "ztransform_digits": "bf16 (kind::f16)" if zt.value & 2 else "int8 (kind::i8)",
@@ -109,7 +114,9 @@ class Batch:
                 "ztransform_us_int8_by_ctas_per_sm": {1: us[10], 2: us[11]},
                 "ztransform_us_bf16_by_ctas_per_sm": {1: us[12], 2: us[13]},
                 "operator_us_separable_by_rows_per_thread": {r: us[14 + i] for i, r in enumerate((1, 2, 4))
-                                                             if us[14 + i] > 0}}
+                                                             if us[14 + i] > 0},
+                "operator_us_separable_4_blocks_per_sm_by_rows_per_thread": {
+                    r: us[17 + i] for i, r in enumerate((1, 2, 4)) if us[17 + i] > 0}}
 
     def profile_clear(self):
         S.check(S.lib().scy_batch_profile_clear(self.h))

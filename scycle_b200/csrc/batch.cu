@@ -407,17 +407,17 @@ __global__ void __launch_bounds__(XT) b_cross_kernel(const double* __restrict__ 
 // shared by the group, L1/L2-resident): one instance per block
 // (blockIdx.z), its 8*RPT x 32 tile staged once and applied by full_apply
 // (register window along y, 9-point interior), so per node only the
-// instance's own fields move.  The partial sums do not depend on RPT: a
-// warp sums each of its rows across its 32 columns, and every band of 8 rows
-// (a tile of the 8 x 32 layout, index blockIdx.x + gridDim.x * band) adds
-// its 8 row sums with one warp sum, as b_cross_kernel does per tile.
-template <int MODE, typename Tz, int RPT>
-__global__ void __launch_bounds__(256) b_full_kernel(LevelDev<double> L, const BatchInst* __restrict__ tab,
+// instance's own fields move.  The partial sums do not depend on RPT: the
+// contributions go to shared memory by node, then for every band of 8 rows
+// (a tile of the 8 x 32 layout, index blockIdx.x + gridDim.x * band) each
+// column adds its 8 rows in order and one warp sum adds the 32 columns.
+template <int MODE, typename Tz, int RPT, int MINB>
+__global__ void __launch_bounds__(256, MINB) b_full_kernel(LevelDev<double> L, const BatchInst* __restrict__ tab,
                                                      const int* __restrict__ mask, BatchWork w,
                                                      const Tz* __restrict__ zv, int first, int pi, int mixed,
                                                      int store_p) {
   __shared__ double xs[full_smem_values<RPT>()];
-  __shared__ double rs[2][8 * RPT];  // row sums
+  __shared__ double cs[2][8 * RPT][TZ];  // contributions by node of the tile
   const int k = blockIdx.z;
   if (!mask[k]) return;
   const int tid = threadIdx.x, lane = tid & 31, r0 = (tid >> 5) * RPT;
@@ -425,12 +425,8 @@ __global__ void __launch_bounds__(256) b_full_kernel(LevelDev<double> L, const B
   const double* sc = w.sc + 16 * k;
   double a1 = 0.0, a2 = 0.0;  // the current row's contributions
   auto row = [&](int j) {
-    const double t1 = warp_sum(a1);
-    const double t2 = (MODE == 1 && first) ? warp_sum(a2) : 0.0;
-    if (lane == 0) {
-      rs[0][r0 + j] = t1;
-      rs[1][r0 + j] = t2;
-    }
+    cs[0][r0 + j][lane] = a1;
+    if (MODE == 1 && first) cs[1][r0 + j][lane] = a2;
     a1 = a2 = 0.0;
   };
   if (MODE == 0) {
@@ -438,13 +434,14 @@ __global__ void __launch_bounds__(256) b_full_kernel(LevelDev<double> L, const B
     const double* rhs = tab[k].rhs;
     const bool zero = sc[0] == 0.0;
     auto ld = [&](long node, int, int) { return u[node]; };
-    auto out = [&](long node, int, int, double Ax, double) {
-      const double v = zero ? 0.0 : -1.0 * rhs[node] + Ax;
+    auto pre = [&](long node, int, int) { return zero ? 0.0 : rhs[node]; };
+    auto out = [&](long node, int, int, double Ax, double, double b) {
+      const double v = zero ? 0.0 : -1.0 * b + Ax;
       w.r[off + node] = v;
       if (mixed) w.r32[off + node] = (float)v;
       a1 = v * v;
     };
-    full_apply<double, RPT>(L, ld, out, row, xs);
+    full_apply<double, RPT>(L, ld, pre, out, row, xs);
   } else {
     double beta = 0.0;
     if (!first) {
@@ -459,24 +456,29 @@ __global__ void __launch_bounds__(256) b_full_kernel(LevelDev<double> L, const B
     auto ld = [&](long node, int, int) {
       return first ? (double)z[node] : (double)z[node] + beta * pold[node];
     };
-    auto out = [&](long node, int, int, double Ax, double p) {
+    auto pre = [&](long node, int, int) { return first ? r[node] : 0.0; };
+    auto out = [&](long node, int, int, double Ax, double p, double rv) {
       const double qv = -Ax;
       if (store_p) pnew[node] = p;
       q[node] = qv;
       a1 = p * qv;
-      if (first) a2 = r[node] * p;
+      if (first) a2 = rv * p;
     };
-    full_apply<double, RPT>(L, ld, out, row, xs);
+    full_apply<double, RPT>(L, ld, pre, out, row, xs);
   }
   __syncthreads();
   const int wv = tid >> 5, band = blockIdx.y * RPT + wv;
   if (wv < RPT && band * 8 < L.Ny) {
     const long slot = (long)k * w.PB + blockIdx.x + (long)gridDim.x * band;
-    double t = lane < 8 ? rs[0][wv * 8 + lane] : 0.0;
+    double t = 0.0;
+#pragma unroll
+    for (int r = 0; r < 8; ++r) t += cs[0][wv * 8 + r][lane];
     t = warp_sum(t);
     if (lane == 0) w.partials[slot] = t;
     if (MODE == 1 && first) {
-      t = lane < 8 ? rs[1][wv * 8 + lane] : 0.0;
+      t = 0.0;
+#pragma unroll
+      for (int r = 0; r < 8; ++r) t += cs[1][wv * 8 + r][lane];
       t = warp_sum(t);
       if (lane == 0) w.partials2[slot] = t;
     }
@@ -488,16 +490,26 @@ static dim3 full_grid(const BatchGroup& g, int rpt) {
   return dim3((g.Nz + TZ - 1) / TZ, (g.Ny + 8 * rpt - 1) / (8 * rpt), g.K);
 }
 
+// the separable form's launch shapes: rows per thread x minimum blocks per
+// SM the compiler fits its registers to (1: its own choice)
+constexpr int kFullShapes = 6;
+constexpr int kFullRpt[kFullShapes] = {1, 2, 4, 1, 2, 4}, kFullMinb[kFullShapes] = {1, 1, 1, 4, 4, 4};
+
 template <int MODE, typename Tz>
-static void launch_full(const BatchGroup& g, int rpt, const BatchInst* tab, const int* mask, const Tz* zv, int first,
-                        int pi, int mixed, int store_p) {
-  const dim3 grid = full_grid(g, rpt);
-  if (rpt == 4)
-    b_full_kernel<MODE, Tz, 4><<<grid, 256, 0, g.stream>>>(g.L, tab, mask, g.w, zv, first, pi, mixed, store_p);
-  else if (rpt == 2)
-    b_full_kernel<MODE, Tz, 2><<<grid, 256, 0, g.stream>>>(g.L, tab, mask, g.w, zv, first, pi, mixed, store_p);
-  else
-    b_full_kernel<MODE, Tz, 1><<<grid, 256, 0, g.stream>>>(g.L, tab, mask, g.w, zv, first, pi, mixed, store_p);
+static void launch_full(const BatchGroup& g, int shape, const BatchInst* tab, const int* mask, const Tz* zv,
+                        int first, int pi, int mixed, int store_p) {
+  const dim3 grid = full_grid(g, kFullRpt[shape]);
+#define SCY_FULL_LAUNCH(R, M) \
+  b_full_kernel<MODE, Tz, R, M><<<grid, 256, 0, g.stream>>>(g.L, tab, mask, g.w, zv, first, pi, mixed, store_p)
+  switch (shape) {
+    case 0: SCY_FULL_LAUNCH(1, 1); break;
+    case 1: SCY_FULL_LAUNCH(2, 1); break;
+    case 2: SCY_FULL_LAUNCH(4, 1); break;
+    case 3: SCY_FULL_LAUNCH(1, 4); break;
+    case 4: SCY_FULL_LAUNCH(2, 4); break;
+    default: SCY_FULL_LAUNCH(4, 4); break;
+  }
+#undef SCY_FULL_LAUNCH
 }
 
 // sc[16 k + slot] = sum of the instance's first n partials (of w.partials,
@@ -1251,19 +1263,17 @@ int BatchContext::autotune(BatchGroup& g) {
   // results do not depend on timings (its arithmetic differs from the cross
   // form's by rounding; its rows per thread change nothing, see
   // b_full_kernel); the cross form's timings stay for comparison
-  g.full_rpt = 0;
+  g.full_shape = -1;
   if (g.L.full) {
     best_us = 1e300;
-    const int rpts[3] = {1, 2, 4};
-    for (int c = 0; c < 3; ++c) {
-      const int rpt = rpts[c];
+    for (int c = 0; c < kFullShapes; ++c) {
       double us = 0.0;
       int rc = timed(
           [&]() -> int {
             if (mixed)
-              launch_full<1, float>(g, rpt, tab, mask, g.w.z32, 1, 0, mixed, 1);
+              launch_full<1, float>(g, c, tab, mask, g.w.z32, 1, 0, mixed, 1);
             else
-              launch_full<1, double>(g, rpt, tab, mask, g.w.z, 1, 0, mixed, 1);
+              launch_full<1, double>(g, c, tab, mask, g.w.z, 1, 0, mixed, 1);
             SCY_LAUNCH_CHECK();
             return SCY_OK;
           },
@@ -1276,7 +1286,7 @@ int BatchContext::autotune(BatchGroup& g) {
       g.tune_us[14 + c] = us;
       if (us < best_us) {
         best_us = us;
-        g.full_rpt = rpt;
+        g.full_shape = c;
       }
     }
   }
@@ -1486,7 +1496,7 @@ int BatchContext::fd_apply(BatchGroup& g) {
 
 int BatchContext::solve(BatchGroup& g, const int* mask, int its_now) {
   const int mixed = precision != SCY_PREC_FP64 ? 1 : 0;
-  const int rpt = g.full_rpt;  // > 0: the separable form
+  const int shape = g.full_shape, rpt = shape >= 0 ? kFullRpt[shape] : 0;  // rpt > 0: the separable form
   const dim3 tg = rpt ? full_grid(g, rpt)
                       : dim3((g.Nz + XTZ - 1) / XTZ, (g.Ny + XTY - 1) / XTY, (g.K + g.kpb - 1) / g.kpb);
   const dim3 ng(node_blocks(g.N), 1, g.K);
@@ -1501,7 +1511,7 @@ int BatchContext::solve(BatchGroup& g, const int* mask, int its_now) {
   cudaEvent_t pa;
   SCY_TRY(prof_begin(g.stream, &pa));
   if (rpt)
-    launch_full<0, double>(g, rpt, tab, mask, (const double*)nullptr, 0, 0, mixed, 0);
+    launch_full<0, double>(g, shape, tab, mask, (const double*)nullptr, 0, 0, mixed, 0);
   else
     b_cross_kernel<0, double><<<tg, XT, xs_smem_bytes(0, 8), g.stream>>>(C, g.Ny, g.Nz, tab, mask, g.w, nullptr, 0,
                                                                          0, mixed, g.kpb);
@@ -1524,9 +1534,9 @@ int BatchContext::solve(BatchGroup& g, const int* mask, int its_now) {
     }
     SCY_TRY(prof_begin(g.stream, &pa));
     if (rpt && mixed)
-      launch_full<1, float>(g, rpt, tab, mask, g.w.z32, first, pi, mixed, store_p);
+      launch_full<1, float>(g, shape, tab, mask, g.w.z32, first, pi, mixed, store_p);
     else if (rpt)
-      launch_full<1, double>(g, rpt, tab, mask, g.w.z, first, pi, mixed, store_p);
+      launch_full<1, double>(g, shape, tab, mask, g.w.z, first, pi, mixed, store_p);
     else if (mixed)
       b_cross_kernel<1, float><<<tg, XT, xs_smem_bytes(1, 4), g.stream>>>(C, g.Ny, g.Nz, tab, mask, g.w, g.w.z32, first,
                                                                            pi, mixed, g.kpb, store_p);
@@ -2006,13 +2016,15 @@ scy_status scy_batch_tuning(scy_batch* b, int g, int* kpb, int* sweep_variant, i
   if (sweep_variant) *sweep_variant = G.ys_variant;
   if (ztransform) *ztransform = G.zt_pair | (G.zt_bf16 << 1);
   if (us)
-    for (int i = 0; i < 17; ++i) us[i] = G.tune_us[i];
+    for (int i = 0; i < 20; ++i) us[i] = G.tune_us[i];
   return SCY_OK;
 }
 
-scy_status scy_batch_operator_form(scy_batch* b, int g, int* rows_per_thread) {
+scy_status scy_batch_operator_form(scy_batch* b, int g, int* rows_per_thread, int* min_blocks_per_sm) {
   if (!b || !rows_per_thread || g < 0 || g >= (int)b->ctx.groups.size()) return SCY_ERR_ARG;
-  *rows_per_thread = b->ctx.groups[g]->full_rpt;
+  const int shape = b->ctx.groups[g]->full_shape;
+  *rows_per_thread = shape >= 0 ? scy::kFullRpt[shape] : 0;
+  if (min_blocks_per_sm) *min_blocks_per_sm = shape >= 0 ? scy::kFullMinb[shape] : 0;
   return SCY_OK;
 }
 

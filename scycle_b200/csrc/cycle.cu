@@ -47,15 +47,19 @@ struct EpiWave {
   double* s_d2u;
   static constexpr bool kReduce = false;
   __device__ __forceinline__ double operator()(long node, int iy, int iz, double Ax, double u) const {
+    return apply(node, iy, iz, Ax, u, uPrev[node]);
+  }
+  // the same with uPrev at the node given (loaded ahead by the caller)
+  __device__ __forceinline__ double apply(long node, int iy, int iz, double Ax, double u, double up) const {
     const bool edge = iy == 0 || iy == Ny - 1 || iz == 0 || iz == Nz - 1;
     const double a = edge ? ay[node] : 0.0;
     const double w = wcy ? wcy[iy] * wcz[iz] : wc[node];
     const double acc = w * Ax + 2. * u;
     double un;
     if (a == 0.0)
-      un = acc - uPrev[node];
+      un = acc - up;
     else
-      un = (acc + (dt * a - 1.0) * uPrev[node]) / (dt * a + 1.0);
+      un = (acc + (dt * a - 1.0) * up) / (dt * a + 1.0);
     uNext[node] = un;
     if (s_rows) {
       if (iy < 5) s_rows[iy * TZ + (iz & (TZ - 1))] = un;
@@ -71,10 +75,16 @@ struct EpiWave {
 // with that many rows per thread (full_tile).
 template <int RPT>
 __device__ __forceinline__ void wave_tile(const LevelDev<double>& L, const LoadPlain<double>& ld, const EpiWave& ep) {
-  if constexpr (RPT == 0)
+  if constexpr (RPT == 0) {
     stencil_tile<double, LoadPlain<double>, EpiWave>(L, ld, ep, nullptr, nullptr, nullptr);
-  else
-    full_tile<double, RPT, LoadPlain<double>, EpiWave>(L, ld, ep, nullptr, nullptr, nullptr);
+  } else {
+    __shared__ double xs[full_smem_values<RPT>()];
+    const double* __restrict__ up = ep.uPrev;
+    auto pre = [&](long node, int, int) { return up[node]; };
+    auto out = [&](long node, int iy, int iz, double Ax, double u, double upv) { ep.apply(node, iy, iz, Ax, u, upv); };
+    auto row = [](int) {};
+    full_apply<double, RPT>(L, ld, pre, out, row, xs);
+  }
 }
 
 template <int RPT>

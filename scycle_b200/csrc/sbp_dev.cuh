@@ -466,70 +466,115 @@ __device__ __forceinline__ void full_stage(const Loader& ld, T* xs, int y0, int 
 }
 
 // The tile of block (blockIdx.x, blockIdx.y): stages the operand through
-// ld(node, iy, iz) into xs and calls out(node, iy, iz, A x, x) once per
-// output node of the tile; after each of its RPT rows j every thread of the
-// block calls row(j) (warp-uniform, so a row's values can be summed across
-// the warp there).
-template <typename T, int RPT, class Loader, class Out, class Row>
-__device__ __forceinline__ void full_apply(const LevelDev<T>& L, const Loader& ld, Out& out, Row& row, T* xs) {
+// ld(node, iy, iz) into xs; then pre(node, iy, iz) is called for each of
+// the thread's output nodes (the epilogue's own loads, issued before the
+// operator is applied so their latency is hidden; default value where the
+// node is outside the grid), and out(node, iy, iz, A x, x, pre value) once
+// per output node of the tile; after each of its RPT rows j every thread of
+// the block calls row(j) (warp-uniform, so a row's values can be summed
+// across the warp there).  The interior path also stages the class-0 rows
+// of the tile's y stencils in shared memory (past the operand) when they
+// differ from row to row.
+template <typename T, int RPT, class Loader, class Pre, class Out, class Row>
+__device__ __forceinline__ void full_apply(const LevelDev<T>& L, const Loader& ld, const Pre& pre, Out& out, Row& row,
+                                           T* xs) {
   constexpr int TYB = 8 * RPT;
+  using P = decltype(pre(0L, 0, 0));
   const int Ny = L.Ny, Nz = L.Nz;
   const int y0 = blockIdx.y * TYB, z0 = blockIdx.x * TZ;
   const int tid = threadIdx.x, lane = tid & 31, r0 = (tid >> 5) * RPT;
+  const int iz = z0 + lane;
   const bool inner = y0 >= L.ylo && y0 + TYB - 1 <= L.yhi && z0 >= L.zlo && z0 + TZ - 1 <= L.zhi;
+  P pv[RPT];
   if (inner) {
     constexpr int H = HALF, W = TZ + 2 * H;
-    full_stage<T, TYB, H, false>(ld, xs, y0, z0, Ny, Nz);  // all inside the grid
-    __syncthreads();
-    const int iz = z0 + lane;
-    T win[RPT + 2 * H];
+    T* cys = xs + (TYB + 2 * H) * W;  // [TYB][BAND] (within the generic layout's size)
+    const bool rows_differ = !L.crow;
+    constexpr int NC = (TYB * BAND + 255) / 256;
+    T cyv[NC];
 #pragma unroll
-    for (int k = 0; k < RPT + 2 * H; ++k) win[k] = xs[(r0 + k) * W + H + lane];
+    for (int a = 0; a < NC; ++a) {
+      const int i = tid + 256 * a;
+      cyv[a] = (rows_differ && i < TYB * BAND) ? L.Cy17[(long)(y0 + i / BAND) * 17 + (8 - HALF) + i % BAND] : T(0);
+    }
+    full_stage<T, TYB, H, false>(ld, xs, y0, z0, Ny, Nz);  // all inside the grid
+#pragma unroll
+    for (int j = 0; j < RPT; ++j) {
+      const int iy = y0 + r0 + j;
+      pv[j] = pre((long)iy * Nz + iz, iy, iz);
+    }
+#pragma unroll
+    for (int a = 0; a < NC; ++a)
+      if (rows_differ && tid + 256 * a < TYB * BAND) cys[tid + 256 * a] = cyv[a];
     T cz[BAND];
 #pragma unroll
     for (int o = 0; o < BAND; ++o) cz[o] = L.ccol ? L.czc[o] : L.CzT17[(long)(o + 8 - HALF) * Nz + iz];
     const T wyv = L.wy1[iz];
+    __syncthreads();
+    T win[RPT + 2 * H];
+#pragma unroll
+    for (int k = 0; k < RPT + 2 * H; ++k) win[k] = xs[(r0 + k) * W + H + lane];
 #pragma unroll
     for (int j = 0; j < RPT; ++j) {
       const int iy = y0 + r0 + j;
-      const T* cy = L.Cy17 + (long)iy * 17 + (8 - HALF);
+      const T* cy = cys + (r0 + j) * BAND;
       const T* xr = xs + (r0 + j + H) * W + lane;  // columns iz-4 .. iz+4
       T sy = T(0), sz = T(0);
 #pragma unroll
       for (int o = 0; o < BAND; ++o) {
-        sy += (L.crow ? L.cyc[o] : cy[o]) * win[j + o];
+        sy += (rows_differ ? cy[o] : L.cyc[o]) * win[j + o];
         sz += cz[o] * (o == HALF ? win[j + HALF] : xr[o]);
       }
       const T Ax = wyv * sy + L.wz1[iy] * sz;
-      out((long)iy * Nz + iz, iy, iz, Ax, win[j + HALF]);
+      out((long)iy * Nz + iz, iy, iz, Ax, win[j + HALF], pv[j]);
       row(j);
     }
   } else {
     constexpr int H = 8, W = TZ + 2 * H;
     full_stage<T, TYB, H, true>(ld, xs, y0, z0, Ny, Nz);
+#pragma unroll
+    for (int j = 0; j < RPT; ++j) {
+      const int iy = y0 + r0 + j;
+      pv[j] = (iz < Nz && iy < Ny) ? pre((long)iy * Nz + iz, iy, iz) : P{};
+    }
     __syncthreads();
-    const int iz = z0 + lane;
 #pragma unroll
     for (int j = 0; j < RPT; ++j) {
       const int iy = y0 + r0 + j;
       if (iz < Nz && iy < Ny) {
-        const T* cy = L.Cy17 + ((long)L.ycls[iz] * Ny + iy) * 17;
-        const T* cz = L.CzT17 + (long)L.zcls[iy] * 17 * Nz + iz;
+        const int yc = L.ycls[iz], zc = L.zcls[iy];
+        const T* cy = L.Cy17 + ((long)yc * Ny + iy) * 17;
+        const T* cz = L.CzT17 + (long)zc * 17 * Nz + iz;
         const T* xy = xs + (r0 + j) * W + H + lane;  // rows iy-8 .. iy+8, stride W
         const T* xz = xs + (r0 + j + H) * W + lane;  // columns iz-8 .. iz+8
         T sy = T(0), sz = T(0);
+        // the 9 middle offsets where the line's stencil has no others
+        if (yc == 0 && iy >= L.ylo && iy <= L.yhi) {
 #pragma unroll
-        for (int o = 0; o < 17; ++o) {
-          sy += cy[o] * xy[o * W];
-          sz += cz[(long)o * Nz] * xz[o];
+          for (int o = 8 - HALF; o <= 8 + HALF; ++o) sy += cy[o] * xy[o * W];
+        } else {
+#pragma unroll
+          for (int o = 0; o < 17; ++o) sy += cy[o] * xy[o * W];
+        }
+        if (zc == 0 && iz >= L.zlo && iz <= L.zhi) {
+#pragma unroll
+          for (int o = 8 - HALF; o <= 8 + HALF; ++o) sz += cz[(long)o * Nz] * xz[o];
+        } else {
+#pragma unroll
+          for (int o = 0; o < 17; ++o) sz += cz[(long)o * Nz] * xz[o];
         }
         const T Ax = L.wy1[iz] * sy + L.wz1[iy] * sz;
-        out((long)iy * Nz + iz, iy, iz, Ax, xy[H * W]);
+        out((long)iy * Nz + iz, iy, iz, Ax, xy[H * W], pv[j]);
       }
       row(j);
     }
   }
 }
+
+// No epilogue loads to prefetch.
+struct NoPre {
+  __device__ __forceinline__ int operator()(long, int, int) const { return 0; }
+};
 
 template <typename T, int RPT, class Loader, class Epi>
 __device__ __forceinline__ void full_tile(const LevelDev<T>& L, const Loader& ld, const Epi& ep, double* partials,
@@ -537,9 +582,9 @@ __device__ __forceinline__ void full_tile(const LevelDev<T>& L, const Loader& ld
   __shared__ T xs[full_smem_values<RPT>()];
   __shared__ double red[32];
   double contrib = 0.0;
-  auto out = [&](long node, int iy, int iz, T Ax, T xv) { contrib += ep(node, iy, iz, Ax, xv); };
+  auto out = [&](long node, int iy, int iz, T Ax, T xv, int) { contrib += ep(node, iy, iz, Ax, xv); };
   auto row = [](int) {};
-  full_apply<T, RPT>(L, ld, out, row, xs);
+  full_apply<T, RPT>(L, ld, NoPre{}, out, row, xs);
   if constexpr (Epi::kReduce) {
     if (partials != nullptr) {  // uniform across the grid
       double tot = block_sum(contrib, red);

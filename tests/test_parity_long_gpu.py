@@ -134,7 +134,12 @@ def test_cycle_first_quasi_dynamic_phase_801():
     solves) and 1e3 times its divergence from a 1e-13 perturbation of its
     initial slip (nucleation amplifies rounding roughly like the slip
     velocity grows), as in tests/test_cycle_gpu.py; the switch into the
-    wave equation must come at the oracle's step and time."""
+    wave equation must come at the oracle's step and time.  The bar is
+    tight (1e-9 .. 3e-4) up to step 100; at the last steps before the
+    switch the slip velocity grows by orders of magnitude and the oracle's
+    own plain and refined runs differ by O(1) there (spread_slipVel ~ 1), so
+    those snapshots bound nothing and the switch step and time carry the
+    check."""
     import tempfile
     from scycle_b200.cycle import Cycle
     fx = _fixture("c2qd")
