@@ -257,48 +257,6 @@ int LevelStore<T>::init(const LevelHost& h, cudaStream_t s) {
       SCY_TRY(upload<T>(comp[1], CzT, s));
       dev.Cy = comp[0].template as<T>();
       dev.CzT = comp[1].template as<T>();
-      // the full form (LevelDev::full, build_full_form)
-      FullForm F;
-      if (build_full_form(h, F)) {
-        SCY_TRY(upload<T>(comp17[0], F.Cy17, s));
-        SCY_TRY(upload<T>(comp17[1], F.CzT17, s));
-        SCY_TRY(upload_ints<T>(cls[0], F.ycls, s));
-        SCY_TRY(upload_ints<T>(cls[1], F.zcls, s));
-        dev.Cy17 = comp17[0].template as<T>();
-        dev.CzT17 = comp17[1].template as<T>();
-        dev.ycls = cls[0].template as<int>();
-        dev.zcls = cls[1].template as<int>();
-        dev.full = 1;
-        dev.ylo = F.ylo;
-        dev.yhi = F.yhi;
-        dev.zlo = F.zlo;
-        dev.zhi = F.zhi;
-        // whether the interior box's rows (columns) all carry the same 9
-        // entries in the stored precision (a constant grid)
-        auto same9 = [](int lo, int hi, auto entry, int& same, T* c9) {
-          same = lo <= hi ? 1 : 0;
-          for (int i = lo; same && i <= hi; ++i)
-            for (int o = 0; o < BAND; ++o)
-              if ((T)entry(i, o) != (T)entry(lo, o)) same = 0;
-          for (int o = 0; o < BAND; ++o) c9[o] = same ? (T)entry(lo, o) : T(0);
-        };
-        same9(F.ylo, F.yhi, [&](int i, int o) { return F.Cy17[(size_t)i * 17 + 8 - HALF + o]; }, dev.crow, dev.cyc);
-        same9(F.zlo, F.zhi, [&](int i, int o) { return F.CzT17[(size_t)(8 - HALF + o) * Nz + i]; }, dev.ccol,
-              dev.czc);
-        // rows per thread: the tallest tile that still gives about six
-        // blocks per SM (SCY_FULL_RPT = 1, 2 or 4 overrides)
-        const long cols = (Nz + TZ - 1) / TZ;
-        dev.rpt = 1;
-        for (int r : {4, 2})
-          if (cols * ((Ny + 8 * r - 1) / (8 * r)) >= 6L * kNumSMs) {
-            dev.rpt = r;
-            break;
-          }
-        if (const char* e = getenv("SCY_FULL_RPT")) {
-          const int r = atoi(e);
-          if (r == 1 || r == 2 || r == 4) dev.rpt = r;
-        }
-      }
       dev.cy1 = sep1[0].template as<T>();
       dev.m3y1 = sep1[1].template as<T>();
       dev.wz1 = sep1[2].template as<T>();
@@ -306,6 +264,55 @@ int LevelStore<T>::init(const LevelHost& h, cudaStream_t s) {
       dev.m3z1 = sep1[4].template as<T>();
       dev.wy1 = sep1[5].template as<T>();
       dev.sep = 1;
+    }
+    // the full form (LevelDev::full, build_full_form); its outer weights
+    // are the separable interior's where that exists
+    FullForm F;
+    if (build_full_form(h, F)) {
+      SCY_TRY(upload<T>(comp17[0], F.Cy17, s));
+      SCY_TRY(upload<T>(comp17[1], F.CzT17, s));
+      SCY_TRY(upload_ints<T>(cls[0], F.ycls, s));
+      SCY_TRY(upload_ints<T>(cls[1], F.zcls, s));
+      dev.Cy17 = comp17[0].template as<T>();
+      dev.CzT17 = comp17[1].template as<T>();
+      dev.ycls = cls[0].template as<int>();
+      dev.zcls = cls[1].template as<int>();
+      dev.full = 1;
+      if (!dev.sep) {
+        SCY_TRY(upload<T>(fullw[0], F.wy1, s));
+        SCY_TRY(upload<T>(fullw[1], F.wz1, s));
+        dev.wy1 = fullw[0].template as<T>();
+        dev.wz1 = fullw[1].template as<T>();
+      }
+      dev.ylo = F.ylo;
+      dev.yhi = F.yhi;
+      dev.zlo = F.zlo;
+      dev.zhi = F.zhi;
+      // whether the interior box's rows (columns) all carry the same 9
+      // entries in the stored precision (a constant grid)
+      auto same9 = [](int lo, int hi, auto entry, int& same, T* c9) {
+        same = lo <= hi ? 1 : 0;
+        for (int i = lo; same && i <= hi; ++i)
+          for (int o = 0; o < BAND; ++o)
+            if ((T)entry(i, o) != (T)entry(lo, o)) same = 0;
+        for (int o = 0; o < BAND; ++o) c9[o] = same ? (T)entry(lo, o) : T(0);
+      };
+      same9(F.ylo, F.yhi, [&](int i, int o) { return F.Cy17[(size_t)i * 17 + 8 - HALF + o]; }, dev.crow, dev.cyc);
+      same9(F.zlo, F.zhi, [&](int i, int o) { return F.CzT17[(size_t)(8 - HALF + o) * Nz + i]; }, dev.ccol,
+            dev.czc);
+      // rows per thread: the tallest tile that still gives about six
+      // blocks per SM (SCY_FULL_RPT = 1, 2 or 4 overrides)
+      const long cols = (Nz + TZ - 1) / TZ;
+      dev.rpt = 1;
+      for (int r : {4, 2})
+        if (cols * ((Ny + 8 * r - 1) / (8 * r)) >= 6L * kNumSMs) {
+          dev.rpt = r;
+          break;
+        }
+      if (const char* e = getenv("SCY_FULL_RPT")) {
+        const int r = atoi(e);
+        if (r == 1 || r == 2 || r == 4) dev.rpt = r;
+      }
     }
   }
   return SCY_OK;

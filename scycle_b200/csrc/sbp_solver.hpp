@@ -60,6 +60,7 @@ struct LevelStore {
   DevBuf comp[2];     // composed interior stencils Cy (Ny x 9) and CzT (9 x Nz)
   DevBuf comp17[2];   // composed whole-operator stencils Cy17 (classes x Ny x 17), CzT17 (classes x 17 x Nz)
   DevBuf cls[2];      // line classes of the full form: ycls (Nz), zcls (Ny)
+  DevBuf fullw[2];    // the full form's outer weights wy1 (Nz), wz1 (Ny) when the interior is not separable
   LevelDev<T> dev{};
   int init(const LevelHost& h, cudaStream_t s);
 };

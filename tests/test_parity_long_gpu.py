@@ -127,19 +127,27 @@ def test_batched_c1_instance_matches_oracle(tmp_path):
 
 def test_cycle_first_quasi_dynamic_phase_801():
     """Config 2's first quasi-dynamic phase at 801x801 (qdfd_const_801, seed
-    0) into its first event: the device cycle driver in solve mode, forced
-    onto the oracle's attempts (tests/golden/make_cycle801_fixture.py), with
-    the reference's Newton path.  The bar is the largest of 1e-9, ten times
-    the oracle's rounding spread (its plain against its refined direct
-    solves) and 1e3 times its divergence from a 1e-13 perturbation of its
-    initial slip (nucleation amplifies rounding roughly like the slip
-    velocity grows), as in tests/test_cycle_gpu.py; the switch into the
-    wave equation must come at the oracle's step and time.  The bar is
-    tight (1e-9 .. 3e-4) up to step 100; at the last steps before the
-    switch the slip velocity grows by orders of magnitude and the oracle's
-    own plain and refined runs differ by O(1) there (spread_slipVel ~ 1), so
-    those snapshots bound nothing and the switch step and time carry the
-    check."""
+    0) into its first event, in two parts (tests/golden/make_cycle801_fixture.py).
+
+    Replay: the device cycle driver in solve mode with the reference's
+    Newton path, forced onto the oracle's attempts, against the oracle's
+    fields at the snapshots where the oracle's own rounding spread (its plain
+    against its refined direct solves) in the slip velocity is below 1e-2,
+    i.e. through step 100 (21.2 of the phase's 21.9 years); the bar is the
+    largest of 1e-9, ten times that spread and 1e3 times the oracle's
+    divergence from a 1e-13 perturbation of its initial slip, as in
+    tests/test_cycle_gpu.py.  Nearer the event the slip velocity grows by
+    orders of magnitude, the oracle's plain and refined runs differ by O(1)
+    (spread_slipVel ~ 1 at steps 176-178) and one trajectory's step sizes no
+    longer suit the other's state, so the replay stops there.
+
+    Free running: the device's own step control switches into the wave
+    equation at the oracle's step (accepted steps; the number of rejected
+    attempts on the way varies with rounding), at the oracle's time within
+    1e-4 relative (the step sizes differ
+    from the fourth attempt on at the 1e-6 level, where the embedded error
+    estimate of the first steps after the steady-state guess is a
+    difference of nearly equal solutions; measured 7e-6)."""
     import tempfile
     from scycle_b200.cycle import Cycle
     fx = _fixture("c2qd")
@@ -148,10 +156,12 @@ def test_cycle_first_quasi_dynamic_phase_801():
     c = Cycle.from_in(path, solve_rtol=SOLVE_RTOL, solve_max_its=2000, exact_jacobian=False)
     c.force_attempts(list(zip(fx["attempt_dt"].tolist(), fx["attempt_acc"].astype(bool).tolist())))
     c.begin_from_in()
-    first = int(fx["switch_step"])
     step = 0
     worst = {}
+    compared = 0
     for i, k in enumerate(fx["snap_steps"].tolist()):
+        if float(fx["spread_slipVel"][i]) >= 1e-2:
+            break
         st = c.run(k - step)
         step = k
         assert st.step_count == k
@@ -161,7 +171,17 @@ def test_cycle_first_quasi_dynamic_phase_801():
             bar = max(REL, 10.0 * float(fx["spread_" + f][i]), 1e3 * float(fx["sens_" + f][i]))
             worst[f] = max(worst.get(f, 0.0), e / bar)
             assert e <= bar, "step %d %s rel err %.3e > %.3e" % (k, f, e, bar)
+        compared += 1
+    assert compared >= 7 and step >= 100
+    c.close()
+    c = Cycle.from_in(path, solve_rtol=SOLVE_RTOL, solve_max_its=2000, exact_jacobian=False)
+    c.begin_from_in()
+    n = 0
+    while not c.switches() and n < 2000:
+        c.run(10)
+        n += 10
     sw = c.switches()
-    assert sw and sw[0]["step"] == first and sw[0]["to"] == "fd"
-    assert abs(sw[0]["t"] - float(fx["switch_t"])) <= 1e-12 * float(fx["switch_t"])
+    first = int(fx["switch_step"])
+    assert sw and sw[0]["step"] == first and sw[0]["to"] == "fd", sw[:1]
+    assert abs(sw[0]["t"] - float(fx["switch_t"])) <= 1e-4 * float(fx["switch_t"])
     c.close()

@@ -99,6 +99,39 @@ def test_solve_matches_direct_solve(order, grid, precision, precond):
     assert _rel(u.cpu().numpy(), ref) <= 1e-9
 
 
+@pytest.mark.parametrize("rpt,grid,mu_kind", list(itertools.product(
+    (1, 2, 4), ("constantGridSpacing", "variableGridSpacing"), ("constant", "one_column"))))
+def test_full_form_every_rows_per_thread(monkeypatch, rpt, grid, mu_kind):
+    """The full-form operator kernels (one 17-point stencil per row and per
+    column, line classes, 9-point interior tiles) at 1, 2 and 4 output rows
+    per thread (SCY_FULL_RPT, read when the operator is built): A x, and a
+    CG solve whose matrix-vector products and residuals run through them,
+    against the oracle.  mu is constant, or constant but for one column (an
+    exceptional y line)."""
+    import scipy.sparse.linalg as spla
+    from scycle_b200.sbp import SbpOps
+    monkeypatch.setenv("SCY_FULL_RPT", str(rpt))
+    Ny, Nz = 137, 163
+    Ly, Lz = 30.0, 24.0
+    q = np.repeat(np.arange(Ny) / (Ny - 1), Nz)
+    r = np.tile(np.arange(Nz) / (Nz - 1), Ny)
+    var = grid == "variableGridSpacing"
+    y = Ly * np.sinh(2 * q) / np.sinh(2) if var else None
+    z = Lz * (r + 0.2 * r * r) / 1.2 if var else None
+    mu = np.full(Ny * Nz, 32.04)
+    if mu_kind == "one_column":
+        mu.reshape(Ny, Nz)[:, Nz // 3] = 27.5
+    dev = SbpOps(4, Ny, Nz, Ly, Lz, mu, grid=grid, y=y, z=z)
+    ora = OracleSbp(4, Ny, Nz, Ly, Lz, mu, grid=grid, y=y, z=z)
+    x = np.random.default_rng(rpt).standard_normal(Ny * Nz)
+    assert _rel(dev.apply("A", x).cpu().numpy(), ora.A @ x) <= 1e-13
+    rhs = ora.set_rhs(np.linspace(0, 1, Nz) ** 2, np.full(Nz, 0.3), np.zeros(Ny), np.zeros(Ny))
+    ref = spla.spsolve(ora.A.tocsc(), rhs)
+    u, st = dev.solve(rhs, rtol=1e-12, max_its=400, precond="mg")
+    assert st.converged
+    assert _rel(u.cpu().numpy(), ref) <= 1e-9
+
+
 @pytest.mark.parametrize("precision", ("fp64", "mixed"))
 def test_fast_diagonalisation_on_separable_stretched_grid(precision):
     """Constant mu, y(iy) and z(iz) stretched independently: the separable part
