@@ -282,11 +282,13 @@ def run_batched(args, dist, rank, world, local):
     # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of
     # ncu captures of these kernels at 32 instances of the 401 x 401 workload
     # (profiles/batched_ensemble_kernels_401x401.md,
-    # profiles/ozk_gemm_kernel_S5_12832x401x401.md); other sizes report none
+    # profiles/ozk_gemm_kernel_S5_12832x401x401.md,
+    # profiles/b_full_kernel_32x401x401.md); other sizes report none
     sep = b.tuning(0)["operator_form"] != "cross"
     traffic = {"ysolve": 65362176.0, "ztransform": 28774656.0} if (args.batch == 32 and args.n == 401) else {}
-    if not sep and args.batch == 32 and args.n == 401:
-        traffic.update({"matvec": 178643456.0, "residual": 187187968.0})
+    if args.batch == 32 and args.n == 401:
+        traffic.update({"matvec": 99618816.0, "residual": 98234880.0} if sep else
+                       {"matvec": 178643456.0, "residual": 187187968.0})
     opk = "b_full_kernel<%d> (separable form: 1D coefficient tables, register window along y)" if sep else \
         "b_cross_kernel<%d> (cross form: 33 coefficient planes)"
     kern = {}

@@ -267,14 +267,28 @@ __global__ void __launch_bounds__(128, PAIR ? 2 : 1)
       for (int g = 0; g < S; ++g) tmem_ld16(tl + g * CN + cc, v[g]);
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
       double acc[16];
+      if constexpr (S <= 5) {
+        // sum_g P_g 2^(-7 (g+2)) as one 64-bit integer (|P_g| < 2^24, so
+        // the Horner sum stays below 2^52) times 2^(-7 (S+1)): exact, the
+        // same value as the FP64 sum below, with one conversion per output
 #pragma unroll
-      for (int q = 0; q < 16; ++q) acc[q] = 0.0;
+        for (int q = 0; q < 16; ++q) {
+          long long h = 0;
 #pragma unroll
-      for (int g = S - 1; g >= 0; --g) {
-        // smallest weights first
-        const double wgt = pow2i(-7 * (g + 2));
+          for (int g = 0; g < S; ++g) h = (h << 7) + (long long)(BF ? (int)__uint_as_float(v[g][q]) : (int)v[g][q]);
+          acc[q] = (double)h * pow2i(-7 * (S + 1));
+        }
+      } else {
 #pragma unroll
-        for (int q = 0; q < 16; ++q) acc[q] += (BF ? (double)__uint_as_float(v[g][q]) : (double)(int)v[g][q]) * wgt;
+        for (int q = 0; q < 16; ++q) acc[q] = 0.0;
+#pragma unroll
+        for (int g = S - 1; g >= 0; --g) {
+          // smallest weights first
+          const double wgt = pow2i(-7 * (g + 2));
+#pragma unroll
+          for (int q = 0; q < 16; ++q)
+            acc[q] += (BF ? (double)__uint_as_float(v[g][q]) : (double)(int)v[g][q]) * wgt;
+        }
       }
 #pragma unroll
       for (int q = 0; q < 16; ++q) tile[rl * LDT + cc + q] = (T)((acc[q] * xs) * sw[cc + q]);
