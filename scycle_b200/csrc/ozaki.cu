@@ -10,8 +10,9 @@
 // S accumulators of 128 x CN in tensor memory, one per digit-weight group,
 // and frees each stage with tcgen05.commit on its "empty" mbarrier.  After
 // the last stage all four warps read their 32 rows of the accumulators
-// (tcgen05.ld 32x32b), combine the groups in FP64 with their powers of two,
-// apply the row and column exponents and store the tile.
+// (tcgen05.ld 32x32b), combine the groups with their powers of two, apply
+// the row and column exponents (loaded by warps 2 and 3 while the products
+// run) and store their row segments.
 //
 // Two digit formats: signed 8-bit digits multiplied by tcgen05.mma
 // kind::i8 into 32-bit integer accumulators, or the same digits held in
@@ -64,9 +65,14 @@ __host__ __device__ constexpr int ozk_align(int pair) { return pair ? 512 : 1024
 __host__ __device__ constexpr int ozk_smem_bytes(int S, int pair = 0) {
   return ozk_stages(S, pair) * ozk_stage_bytes(S, pair) + ozk_align(pair);
 }
-static_assert(2 * (ozk_smem_bytes(5, 1) + 1024 + 256) <= 228 * 1024, "two CTAs per SM do not fit");
-static_assert(2 * (ozk_smem_bytes(4, 1) + 1024 + 256) <= 228 * 1024, "two CTAs per SM do not fit");
-static_assert(2 * (ozk_smem_bytes(3, 1) + 1024 + 256) <= 228 * 1024, "two CTAs per SM do not fit");
+// per CTA beside the stages: the reserved kilobyte, the barriers and the
+// epilogue's exponent factors (CN + 128 doubles)
+static_assert(2 * (ozk_smem_bytes(5, 1) + 1024 + 256 + 8 * (ozk_cn(5, 1) + 128)) <= 228 * 1024,
+              "two CTAs per SM do not fit");
+static_assert(2 * (ozk_smem_bytes(4, 1) + 1024 + 256 + 8 * (ozk_cn(4, 1) + 128)) <= 228 * 1024,
+              "two CTAs per SM do not fit");
+static_assert(2 * (ozk_smem_bytes(3, 1) + 1024 + 256 + 8 * (ozk_cn(3, 1) + 128)) <= 228 * 1024,
+              "two CTAs per SM do not fit");
 
 // shared-memory matrix descriptor (tcgen05 format): K-major operand whose
 // rows are 64 bytes with 64-byte swizzling, 8-row groups 512 bytes apart
@@ -143,11 +149,11 @@ __global__ void __launch_bounds__(128, PAIR ? 2 : 1)
   static_assert(S * CN <= TC, "accumulators exceed tensor memory");
   static_assert(!PAIR || S <= 5, "two CTAs per SM only for S <= 5");
   static_assert(CN % 16 == 0 && CN >= 16 && CN <= 256, "invalid MMA N");
-  static_assert(8 * 256 + OZK_BM * (CN + 1) * (int)sizeof(T) <= ST * (XB + WB), "epilogue tile exceeds the stages");
   extern __shared__ __align__(1024) unsigned char ozk_smem_raw[];
   __shared__ __align__(8) uint64_t full[ST], empty[ST], done;
   __shared__ uint32_t tmem_slot;
   __shared__ int consumed, failed;
+  __shared__ double s_sw[CN], s_xs[OZK_BM];  // 2^ew of the tile's columns, 2^ex of its rows
   // tiles on a 1024- or 512-byte boundary (the swizzle pattern repeats every 512 B)
   unsigned char* smem = ozk_smem_raw + ((AL - (smem_u32(ozk_smem_raw) & (AL - 1))) & (AL - 1));
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -184,6 +190,15 @@ __global__ void __launch_bounds__(128, PAIR ? 2 : 1)
   const int rot = (int)((blockIdx.x * 7u + blockIdx.y) % (unsigned)nkb);
   const int nmma = max(32, min(CN, (cout - c0 + 15) / 16 * 16));
   int issued = 0;
+  if (warp >= 2) {
+    // the epilogue's exponent factors, loaded while the products run
+    for (int i = threadIdx.x - 64; i < CN + OZK_BM; i += 64) {
+      if (i < CN)
+        s_sw[i] = c0 + i < cout ? pow2i(ew[c0 + i]) : 0.0;
+      else
+        s_xs[i - CN] = m0 + (i - CN) < rows ? pow2i(ex[m0 + (i - CN)]) : 0.0;
+    }
+  }
   if (warp == 0 && lane == 0) {
     // producer
     for (int q = 0; q < nkb; ++q) {
@@ -248,17 +263,12 @@ __global__ void __launch_bounds__(128, PAIR ? 2 : 1)
       for (int q = m0 / rows_per_status; q <= r1 / rows_per_status; ++q) atomicOr(status + q, bit);
     }
   } else {
-    // epilogue: warp w owns tensor-memory lanes 32 w .. 32 w + 31 (rows).
-    // The tile goes through shared memory (the stage buffers are free once
-    // every product has completed) so that each warp stores whole row
-    // segments; the exponents become exact power-of-two factors.
-    constexpr int LDT = CN + 1;
-    double* sw = reinterpret_cast<double*>(smem);         // 2^ew of the tile's columns
-    T* tile = reinterpret_cast<T*>(smem + 8 * 256);       // 128 x LDT
-    for (int c = threadIdx.x; c < CN; c += 128) sw[c] = c0 + c < cout ? pow2i(ew[c0 + c]) : 0.0;
-    __syncthreads();
+    // epilogue: warp w owns tensor-memory lanes 32 w .. 32 w + 31 (rows);
+    // a thread combines its row's groups, 16 columns at a time, applies the
+    // exponent factors (exact powers of two, loaded during the products)
+    // and stores the 16 values of its row segment
     const int rl = warp * 32 + lane, row = m0 + rl;
-    const double xs = row < rows ? pow2i(ex[row]) : 0.0;
+    const double xs = s_xs[rl];
     const uint32_t tl = tmem + ((uint32_t)(warp * 32) << 16);
 #pragma unroll 1
     for (int cc = 0; cc < nmma; cc += 16) {
@@ -290,16 +300,12 @@ __global__ void __launch_bounds__(128, PAIR ? 2 : 1)
             acc[q] += (BF ? (double)__uint_as_float(v[g][q]) : (double)(int)v[g][q]) * wgt;
         }
       }
+      if (row < rows) {
+        T* drow = D + (long)row * ldd + c0 + cc;
 #pragma unroll
-      for (int q = 0; q < 16; ++q) tile[rl * LDT + cc + q] = (T)((acc[q] * xs) * sw[cc + q]);
-    }
-    __syncwarp();
-    const int ncol = min(CN, cout - c0);
-    for (int r = 0; r < 32; ++r) {
-      const int rr = warp * 32 + r;
-      if (m0 + rr >= rows) break;
-      T* drow = D + (long)(m0 + rr) * ldd + c0;
-      for (int c = lane; c < ncol; c += 32) drow[c] = tile[rr * LDT + c];
+        for (int q = 0; q < 16; ++q)
+          if (c0 + cc + q < cout) drow[q] = (T)((acc[q] * xs) * s_sw[cc + q]);
+      }
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -339,6 +345,61 @@ __global__ void __launch_bounds__(256) ozk_split_kernel(const Tin* __restrict__ 
       for (int u = 0; u < 4; ++u) {
         const double d = rint(t[u]);
         t[u] = (t[u] - d) * 128.0;
+        if (BF) {
+          const uint32_t h = __float_as_uint((float)d) >> 16;
+          if (u < 2)
+            w0 |= h << (16 * u);
+          else
+            w1 |= h << (16 * (u - 2));
+        } else {
+          w0 |= (uint32_t)(uint8_t)(int8_t)(int)d << (8 * u);
+        }
+      }
+      if (BF)
+        *reinterpret_cast<uint2*>(reinterpret_cast<uint16_t*>(dig) + (long)i * plane + at) = make_uint2(w0, w1);
+      else
+        *reinterpret_cast<uint32_t*>(dig + (long)i * plane + at) = w0;
+    }
+  }
+}
+
+// The same digits with the row held in registers (Kp <= 128 NC): lane l
+// loads positions 128 c + 4 l .. + 3 once, takes the row maximum from them
+// and writes the digits from them (one pass over the row in memory).
+template <typename Tin, int BF, int NC>
+__global__ void __launch_bounds__(256) ozk_split_reg_kernel(const Tin* __restrict__ X, long ldx, int rows, int K,
+                                                            int Kp, int S, unsigned char* __restrict__ dig,
+                                                            long plane, int* __restrict__ expo) {
+  const int row = (int)((blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (row >= rows) return;
+  const Tin* x = X + (long)row * ldx;
+  double t[NC][4];
+  double m = 0.0;
+#pragma unroll
+  for (int c = 0; c < NC; ++c)
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int k = 128 * c + 4 * lane + u;
+      t[c][u] = k < K ? (double)x[k] : 0.0;
+      m = fmax(m, fabs(t[c][u]));
+    }
+  m = warp_max(m);
+  const int e = m > 0.0 ? ilogb(m) + 2 : 0;
+  if (lane == 0) expo[row] = e;
+#pragma unroll
+  for (int c = 0; c < NC; ++c) {
+    const int k0 = 128 * c + 4 * lane;
+    if (k0 >= Kp) break;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) t[c][u] = ldexp(t[c][u], 7 - e);
+    const long at = (long)row * Kp + k0;
+    for (int i = 0; i < S; ++i) {
+      uint32_t w0 = 0, w1 = 0;
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const double d = rint(t[c][u]);
+        t[c][u] = (t[c][u] - d) * 128.0;
         if (BF) {
           const uint32_t h = __float_as_uint((float)d) >> 16;
           if (u < 2)
@@ -503,10 +564,32 @@ int OzkOperand::alloc(int S_, int rows_, int K_, int box_rows_, int esz_) {
   return SCY_OK;
 }
 
+template <typename Tin, int BF>
+static void launch_split_reg(OzkOperand& o, const Tin* X, long ldx, cudaStream_t s, int blocks) {
+  unsigned char* d = o.dig.as<unsigned char>();
+  int* ex = o.expo.as<int>();
+  if (o.Kp <= 128)
+    ozk_split_reg_kernel<Tin, BF, 1><<<blocks, 256, 0, s>>>(X, ldx, o.rows, o.K, o.Kp, o.S, d, o.plane, ex);
+  else if (o.Kp <= 256)
+    ozk_split_reg_kernel<Tin, BF, 2><<<blocks, 256, 0, s>>>(X, ldx, o.rows, o.K, o.Kp, o.S, d, o.plane, ex);
+  else if (o.Kp <= 512)
+    ozk_split_reg_kernel<Tin, BF, 4><<<blocks, 256, 0, s>>>(X, ldx, o.rows, o.K, o.Kp, o.S, d, o.plane, ex);
+  else
+    ozk_split_reg_kernel<Tin, BF, 8><<<blocks, 256, 0, s>>>(X, ldx, o.rows, o.K, o.Kp, o.S, d, o.plane, ex);
+}
+
 template <typename Tin>
 static int split_any(OzkOperand& o, const Tin* X, long ldx, cudaStream_t s) {
   const int threads = 256;
   const int blocks = (int)(((long)o.rows * 32 + threads - 1) / threads);
+  if (o.Kp <= 1024) {  // the row in registers
+    if (o.esz == 2)
+      launch_split_reg<Tin, 1>(o, X, ldx, s, blocks);
+    else
+      launch_split_reg<Tin, 0>(o, X, ldx, s, blocks);
+    SCY_LAUNCH_CHECK();
+    return SCY_OK;
+  }
   if (o.esz == 2)
     ozk_split_kernel<Tin, 1><<<blocks, threads, 0, s>>>(X, ldx, o.rows, o.K, o.Kp, o.S, o.dig.as<unsigned char>(),
                                                         o.plane, o.expo.as<int>());
