@@ -194,7 +194,7 @@ def oracle_errors(name, make, rtol=PARITY_RTOL, batch_precision=None):
 # ---------------------------------------------------------------------------
 ZT_DESC = ("ozk_gemm_kernel (z transforms of the preconditioner on the integer tensor cores: tcgen05 kind::i8 "
            "digit-plane products, TMA-fed, tensor-memory accumulators; two per apply)")
-ZS_DESC = "ozk_split_kernel (digit planes of the z-transform operand, two per apply)"
+ZS_DESC = "ozk_split_reg_kernel (digit planes of the z-transform operand, the row held in registers; two per apply)"
 BATCH_WORKLOAD = ("slip_var_401 ensemble: %d instances per GPU of the 401x401 stretched-grid slip-law workload "
                   "(seeds differ: lognormal Dc and initial state), every instance with its own RK32 step control")
 
