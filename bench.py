@@ -1134,8 +1134,9 @@ def main():
                          "direct launches (for ncu) and exit")
     ap.add_argument("--profile-bf16", type=int, default=0, choices=[0, 1],
                     help="digits in bf16 (kind::f16) instead of 8-bit integers in --profile-ztransform")
-    ap.add_argument("--profile-ctas", type=int, default=1, choices=[1, 2],
-                    help="CTAs per SM of the z-transform product in --profile-ztransform (2: S <= 5)")
+    ap.add_argument("--profile-ctas", type=int, default=1, choices=[0, 1, 2],
+                    help="shape of the z-transform product in --profile-ztransform: CTAs per SM (2: S <= 5), "
+                         "0 the persistent shape (S <= 5)")
     ap.add_argument("--profile-ztransform", type=int, default=0,
                     help="run only the tensor-core z transform with this many digit planes (for ncu) and exit")
     args = ap.parse_args()

@@ -178,9 +178,11 @@ scy_status scy_sbp_solve_noalloc(scy_sbp* s, const double* rhs, double* u,
  * the S(S+1)/2 digit products accumulated exactly in 32-bit integers
  * (tcgen05.mma kind::i8) and combined in FP64; relative error per row about
  * 100^-S.  X and D are device arrays (row strides ldx, ldd), W a host array
- * (row stride ldw), K <= 1024.  ctas_per_sm: 1, or 2 for S <= 5 (narrower
- * column tiles, one CTA's epilogue overlapping the other's products; the
- * same result).  bf16_digits = 1 holds the same digits in bf16 and
+ * (row stride ldw), K <= 1024.  ctas_per_sm: 1; 2 for S <= 5 (narrower
+ * column tiles, one CTA's epilogue overlapping the other's products); 0 for
+ * S <= 5, the persistent shape (one CTA per SM walking the narrower tiles
+ * with two accumulator sets in tensor memory, one tile's epilogue under the
+ * next tile's products); the same result in every shape.  bf16_digits = 1 holds the same digits in bf16 and
  * multiplies them with FP32 accumulation (tcgen05.mma kind::f16), exact and
  * so bit-identical while S * 64 * 64 * K' < 2^24 (K' = K rounded up to 32;
  * SCY_ERR_ARG beyond).  No counterpart in the reference: it is the z
@@ -684,16 +686,18 @@ scy_status scy_batch_set_sweep_test(scy_batch* b, int polls, int drop_first_copy
  * separable form (1D coefficient tables) with 1, 2 and 4 rows per thread,
  * the banded sweeps in six launch shapes (chains per lane x warps per block:
  * 2 x 2, 1 x 4, 4 x 1 serving 8 instances per block, 1 x 2 and 2 x 1
- * serving 4, 1 x 1 serving 2) and the z-transform product with one or two
- * CTAs per SM and 8-bit or bf16 digits (identical results), and keeps the
- * fastest.  kpb / sweep_variant / ztransform get the choices (kpb: the cross
- * form's, see scy_batch_operator_form for the form in use; ztransform bit 0:
- * two CTAs per SM, bit 1: bf16 digits), us (20 doubles, may be NULL) the
- * timings in microseconds per launch (cross form at kpb 1, 2, 4, 8; sweep
- * shapes 0-5; product with 8-bit digits, one and two CTAs per SM; with bf16
- * digits, one and two CTAs per SM; separable form at 1, 2, 4 rows per
- * thread with the compiler's register count, then with registers fitted to
- * four blocks per SM; 0 where not tried).  The separable form is used
+ * serving 4, 1 x 1 serving 2) and the z-transform product in three shapes
+ * (one CTA per tile, two CTAs per SM, persistent: one CTA per SM with two
+ * accumulator sets) with 8-bit or bf16 digits (identical results), and keeps
+ * the fastest.  kpb / sweep_variant / ztransform get the choices (kpb: the
+ * cross form's, see scy_batch_operator_form for the form in use; ztransform
+ * bit 0: two CTAs per SM, bit 1: bf16 digits, bit 2: persistent), us (22
+ * doubles, may be NULL) the timings in microseconds per launch (cross form
+ * at kpb 1, 2, 4, 8; sweep shapes 0-5; product with 8-bit digits, one and
+ * two CTAs per SM; with bf16 digits, one and two CTAs per SM; separable form
+ * at 1, 2, 4 rows per thread with the compiler's register count, then with
+ * registers fitted to four blocks per SM; persistent product with 8-bit and
+ * with bf16 digits; 0 where not tried).  The separable form is used
  * whenever the operator has it (its results do not depend on its launch
  * shape; they differ from the cross form's by rounding). */
 scy_status scy_batch_tuning(scy_batch* b, int g, int* kpb, int* sweep_variant, int* ztransform, double* us);

@@ -95,7 +95,7 @@ class Batch:
         per thread), the sweep launch shape, the z-transform product's shape
         and digits, and the timings (us)."""
         kpb, var, zt, rpt, minb = C.c_int(), C.c_int(), C.c_int(), C.c_int(), C.c_int()
-        us = (C.c_double * 20)()
+        us = (C.c_double * 22)()
         S.check(S.lib().scy_batch_tuning(self.h, int(group), C.byref(kpb), C.byref(var), C.byref(zt), us))
         S.check(S.lib().scy_batch_operator_form(self.h, int(group), C.byref(rpt), C.byref(minb)))
         shapes = ["2 chains x 2 warps (8 instances)", "1 chain x 4 warps (8)", "4 chains x 1 warp (8)",
@@ -107,12 +107,14 @@ class Batch:
                 else "compiler's register count")
         return {"operator_form": form,
                 "instances_per_block": kpb.value, "sweep_variant": shapes[var.value],
-                "ztransform_ctas_per_sm": 2 if zt.value & 1 else 1,
+                "ztransform_shape": "persistent (one CTA per SM, two accumulator sets)" if zt.value & 4 else
+                                    "two CTAs per SM" if zt.value & 1 else "one CTA per tile",
                 "ztransform_digits": "bf16 (kind::f16)" if zt.value & 2 else "int8 (kind::i8)",
                 "operator_us_by_kpb": {k: us[i] for i, k in enumerate((1, 2, 4, 8)) if us[i] > 0},
                 "sweep_us_by_variant": {shapes[v]: us[4 + v] for v in range(6) if us[4 + v] > 0},
                 "ztransform_us_int8_by_ctas_per_sm": {1: us[10], 2: us[11]},
                 "ztransform_us_bf16_by_ctas_per_sm": {1: us[12], 2: us[13]},
+                "ztransform_us_persistent": {"int8": us[20], "bf16": us[21]},
                 "operator_us_separable_by_rows_per_thread": {r: us[14 + i] for i, r in enumerate((1, 2, 4))
                                                              if us[14 + i] > 0},
                 "operator_us_separable_4_blocks_per_sm_by_rows_per_thread": {

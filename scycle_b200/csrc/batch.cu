@@ -1306,13 +1306,14 @@ int BatchContext::autotune(BatchGroup& g) {
         g.ys_variant = v;
       }
     }
-    // the forward z-transform product in both shapes and both digit
-    // formats (identical results)
+    // the forward z-transform product in its three shapes (one CTA per
+    // tile, two CTAs per SM, persistent) and both digit formats (identical
+    // results)
     {
       double zbest = 1e300;
       for (int bf = 0; bf < 2; ++bf) {
         if (bf && !g.zx16.dig.p) continue;
-        for (int pr = 0; pr < 2; ++pr) {
+        for (int pr = 0; pr < 3; ++pr) {
           if (pr && ozk_cols_per_tile_pair(zt_planes) == 0) continue;
           const OzkOperand& X = bf ? g.zx16 : g.zx;
           const OzkOperand& W = bf ? g.zw1_16 : g.zw1;
@@ -1329,7 +1330,7 @@ int BatchContext::autotune(BatchGroup& g) {
             cudaEventDestroy(e1);
             return rc;
           }
-          g.tune_us[10 + 2 * bf + pr] = us;
+          g.tune_us[pr == 2 ? 20 + bf : 10 + 2 * bf + pr] = us;
           if (us < zbest) {
             zbest = us;
             g.zt_pair = pr;
@@ -2014,9 +2015,9 @@ scy_status scy_batch_tuning(scy_batch* b, int g, int* kpb, int* sweep_variant, i
   const scy::BatchGroup& G = *b->ctx.groups[g];
   if (kpb) *kpb = G.kpb;
   if (sweep_variant) *sweep_variant = G.ys_variant;
-  if (ztransform) *ztransform = G.zt_pair | (G.zt_bf16 << 1);
+  if (ztransform) *ztransform = (G.zt_pair == 1 ? 1 : 0) | (G.zt_bf16 << 1) | (G.zt_pair == 2 ? 4 : 0);
   if (us)
-    for (int i = 0; i < 20; ++i) us[i] = G.tune_us[i];
+    for (int i = 0; i < 22; ++i) us[i] = G.tune_us[i];
   return SCY_OK;
 }
 

@@ -72,15 +72,16 @@ struct BatchGroup {
   DevBuf planes;  // the operator's 33 cross-stencil coefficient planes (build_cross_planes)
   int kpb = 1;    // instances per block of the operator kernels (autotuned at set-up)
   int ys_variant = 0;  // chains per lane x warps per block of the banded sweeps (autotuned)
-  int zt_pair = 0;  // z-transform products in the two-CTAs-per-SM shape (autotuned)
+  int zt_pair = 0;  // z-transform products: 0 one CTA per tile, 1 two CTAs per SM, 2 persistent (autotuned)
   int zt_bf16 = 0;  // z-transform digits in bf16 (kind::f16) instead of 8-bit integers (autotuned)
   int full_shape = -1;  // >= 0: the operator kernels in the separable form, in this launch shape (autotuned)
   // the autotuner's timings: kpb 1, 2, 4, 8; sweep variants 0..5;
   // z-transform product with 8-bit digits in the one- and two-CTAs-per-SM
   // shapes, with bf16 digits in the two shapes; the separable form at 1, 2
   // and 4 rows per thread, registers by the compiler's choice and then
-  // fitted to four blocks per SM
-  double tune_us[20] = {0};
+  // fitted to four blocks per SM; the persistent z-transform product with
+  // 8-bit and with bf16 digits
+  double tune_us[22] = {0};
   DevBuf vec[7], vecf[4], sc, partials, counters, status;
   BatchWork w{};
   cudaStream_t stream = nullptr;

@@ -22,10 +22,12 @@
 // The products are bit-identical; which is faster depends on the tensor
 // pipe's integer and bf16 rates, so callers time both.
 //
-// Two shapes: one CTA per SM (all 512 tensor-memory columns, CN = 144 /
-// 112 / 96 / 64 columns for S = 3 / 4 / 5 / 6-7, up to four stages) and,
-// for S <= 5, two CTAs per SM (256 columns each, CN = 64 / 64 / 48, two
-// stages), where one CTA's epilogue overlaps the other's products.
+// Three shapes: one CTA per SM per tile (all 512 tensor-memory columns, CN
+// = 144 / 112 / 96 / 64 columns for S = 3 / 4 / 5 / 6-7, up to four
+// stages); for S <= 5, two CTAs per SM (256 columns each, CN = 64 / 64 / 48,
+// two stages), where one CTA's epilogue overlaps the other's products; and
+// for S <= 5 the persistent ozk_gemm_pers_kernel (one CTA per SM walking the
+// tiles of width 64 / 64 / 48 with two accumulator sets).
 //
 // Every mbarrier wait is bounded (2^20 polls).  A wait that runs out marks
 // the tile's rows in the caller's status words; the producer then waits
@@ -33,6 +35,7 @@
 // waits (bounded) for the issued products, and tensor memory is freed
 // before the CTA exits.  TMA loads read this GPU's own memory only and use
 // no cluster multicast.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -65,6 +68,13 @@ __host__ __device__ constexpr int ozk_align(int pair) { return pair ? 512 : 1024
 __host__ __device__ constexpr int ozk_smem_bytes(int S, int pair = 0) {
   return ozk_stages(S, pair) * ozk_stage_bytes(S, pair) + ozk_align(pair);
 }
+// the persistent shape (S <= 5): the two-CTAs-per-SM tile width (S * CN <=
+// 256, so two accumulator sets fit the 512 tensor-memory columns) and as
+// many stages of that width as fit one CTA's shared memory (at most four)
+__host__ __device__ constexpr int ozk_pers_stages(int S) {
+  return (227 * 1024 - 2048) / ozk_stage_bytes(S, 1) > 4 ? 4 : (227 * 1024 - 2048) / ozk_stage_bytes(S, 1);
+}
+__host__ __device__ constexpr int ozk_pers_smem_bytes(int S) { return ozk_pers_stages(S) * ozk_stage_bytes(S, 1) + 1024; }
 // per CTA beside the stages: the reserved kilobyte, the barriers and the
 // epilogue's exponent factors (CN + 128 doubles)
 static_assert(2 * (ozk_smem_bytes(5, 1) + 1024 + 256 + 8 * (ozk_cn(5, 1) + 128)) <= 228 * 1024,
@@ -313,6 +323,201 @@ __global__ void __launch_bounds__(128, PAIR ? 2 : 1)
   if (warp == 1) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "n"(TC) : "memory");
 }
 
+// ozk_gemm_pers_kernel<S, T, BF> (S <= 5): the same product as a persistent
+// kernel.  One CTA of 256 threads per SM walks the output tiles of 128 rows
+// x CN columns (CN of the two-CTAs-per-SM shape, S * CN <= 256), tile t =
+// blockIdx.x + k * gridDim.x (column tiles fastest), with the accumulators
+// double-buffered in tensor memory (columns 0..255 for even, 256..511 for odd
+// tiles of the CTA), so the epilogue of one tile runs while the products of
+// the next are issued.  Thread 0 of warp 0 streams the K slices of all the
+// CTA's tiles through one stage ring; thread 0 of warp 1 issues the products
+// and marks a buffer's accumulators complete (accf, by tcgen05.commit);
+// warps 4..7 (tensor-memory lanes 32 (w - 4) ..) read, combine and store
+// them and mark the buffer free (acce, one arrival per warp).  Same digit
+// formats and the same results as ozk_gemm_kernel.  Every wait is bounded;
+// a role whose wait runs out stops, the others stop at their next bounded
+// wait or at the shared flag, issued copies and products are awaited
+// (bounded) before the tensor memory is freed, and the rows of every tile
+// of the CTA are marked in the caller's status words.
+template <int S, typename T, int BF>
+__global__ void __launch_bounds__(256, 1)
+    ozk_gemm_pers_kernel(const __grid_constant__ CUtensorMap mx, const __grid_constant__ CUtensorMap mw,
+                         const int* __restrict__ ex, const int* __restrict__ ew, T* __restrict__ D, long ldd,
+                         int rows, int cout, int nks, unsigned* __restrict__ status, int rows_per_status,
+                         unsigned bit) {
+  constexpr int CN = ozk_cn(S, 1);
+  constexpr int XB = S * OZK_BM * OZK_BK;
+  constexpr int WB = S * CN * OZK_BK;
+  constexpr int ST = ozk_pers_stages(S);
+  static_assert(S <= 5 && S * CN <= 256, "two accumulator sets must fit the tensor memory");
+  static_assert(CN % 16 == 0 && CN >= 32, "invalid MMA N");
+  extern __shared__ __align__(1024) unsigned char ozk_smem_raw[];
+  __shared__ __align__(8) uint64_t full[ST], empty[ST], accf[2], acce[2], done;
+  __shared__ uint32_t tmem_slot;
+  __shared__ volatile int failed;
+  __shared__ int issued_q, consumed_q;
+  unsigned char* smem = ozk_smem_raw + ((1024u - (smem_u32(ozk_smem_raw) & 1023u)) & 1023u);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int ntc = (cout + CN - 1) / CN, ntr = (rows + OZK_BM - 1) / OZK_BM, ntiles = ntc * ntr;
+  const int nkb = (nks + 1) / 2;
+
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < ST; ++i) {
+      mbar_init(&full[i], 1);
+      mbar_init(&empty[i], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&accf[b], 1);
+      mbar_init(&acce[b], 4);
+    }
+    mbar_init(&done, 1);
+    fence_mbar_init();
+    failed = 0;
+    issued_q = 0;
+    consumed_q = 0;
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(smem_u32(&tmem_slot))
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_slot;
+
+  if (warp == 0 && lane == 0) {
+    // producer
+    int q = 0;
+    for (int t = blockIdx.x; t < ntiles && !failed; t += gridDim.x) {
+      const int ct = t % ntc, rt = t / ntc, c0 = ct * CN, m0 = rt * OZK_BM;
+      const int rot = (int)((ct * 7u + rt) % (unsigned)nkb);
+      bool ok = true;
+      for (int k = 0; k < nkb; ++k) {
+        const int st = q % ST, kb = (k + rot) % nkb;
+        if (q >= ST && !mbar_wait(&empty[st], ((q / ST) - 1) & 1, OZK_POLLS)) {
+          failed = 1;
+          ok = false;
+          break;
+        }
+        unsigned char* sx = smem + st * (XB + WB);
+        mbar_expect_tx(&full[st], XB + WB);
+        tma_load_3d(sx, &mx, &full[st], kb * (OZK_BK / (BF ? 2 : 1)), m0, 0);
+        tma_load_3d(sx + XB, &mw, &full[st], kb * (OZK_BK / (BF ? 2 : 1)), c0, 0);
+        ++q;
+      }
+      if (!ok) break;
+    }
+    issued_q = q;
+  } else if (warp == 1 && lane == 0) {
+    // MMA issuer
+    int q = 0, i = 0;
+    for (int t = blockIdx.x; t < ntiles && !failed; t += gridDim.x, ++i) {
+      const int ct = t % ntc, rt = t / ntc, c0 = ct * CN;
+      const int rot = (int)((ct * 7u + rt) % (unsigned)nkb);
+      const int nmma = max(32, min(CN, (cout - c0 + 15) / 16 * 16));
+      const uint32_t idesc = BF ? umma_idesc_bf16(nmma) : umma_idesc_s8(nmma);
+      const int b = i & 1;
+      if (i >= 2 && !mbar_wait(&acce[b], ((i >> 1) - 1) & 1, OZK_POLLS)) {
+        failed = 1;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t tb = tmem + (uint32_t)(b * 256);
+      bool ok = true;
+      for (int k = 0; k < nkb; ++k) {
+        const int st = q % ST, kb = (k + rot) % nkb;
+        if (!mbar_wait(&full[st], (q / ST) & 1, OZK_POLLS)) {
+          failed = 1;
+          ok = false;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t xa = smem_u32(smem + st * (XB + WB));
+        const uint32_t wa = xa + XB;
+#pragma unroll
+        for (int ks = 0; ks < 2; ++ks) {
+          if (2 * kb + ks >= nks) break;
+#pragma unroll
+          for (int g = 0; g < S; ++g)
+#pragma unroll
+            for (int p = 1; p <= g + 1; ++p) {
+              const int j = g + 2 - p;
+              const uint64_t ad = umma_desc_sw64(xa + (p - 1) * OZK_BM * OZK_BK + ks * 32);
+              const uint64_t bd = umma_desc_sw64(wa + (j - 1) * CN * OZK_BK + ks * 32);
+              const uint32_t acc = (k > 0 || ks > 0 || p > 1) ? 1u : 0u;
+              if (BF)
+                umma_bf16(tb + g * CN, ad, bd, idesc, acc);
+              else
+                umma_s8(tb + g * CN, ad, bd, idesc, acc);
+            }
+        }
+        umma_commit(&empty[st]);
+        ++q;
+      }
+      if (!ok) break;
+      umma_commit(&accf[b]);  // arrives once the tile's products have completed
+    }
+    consumed_q = q;
+    umma_commit(&done);
+  } else if (warp >= 4) {
+    // epilogue
+    const int wq = warp - 4;
+    int i = 0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++i) {
+      const int ct = t % ntc, rt = t / ntc, c0 = ct * CN, m0 = rt * OZK_BM;
+      const int nmma = max(32, min(CN, (cout - c0 + 15) / 16 * 16));
+      const int b = i & 1;
+      const int row = m0 + wq * 32 + lane;
+      const double xs = row < rows ? pow2i(ex[row]) : 0.0;
+      const bool got = mbar_wait(&accf[b], (i >> 1) & 1, OZK_POLLS);
+      if (!__all_sync(0xffffffffu, got ? 1 : 0) || failed) {
+        failed = 1;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t tl = tmem + ((uint32_t)(wq * 32) << 16) + (uint32_t)(b * 256);
+#pragma unroll 1
+      for (int cc = 0; cc < nmma; cc += 16) {
+        uint32_t v[S][16];
+#pragma unroll
+        for (int g = 0; g < S; ++g) tmem_ld16(tl + g * CN + cc, v[g]);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (row < rows) {
+          T* drow = D + (long)row * ldd + c0 + cc;
+#pragma unroll
+          for (int q2 = 0; q2 < 16; ++q2) {
+            // the digit groups as one 64-bit integer (see ozk_gemm_kernel)
+            long long h = 0;
+#pragma unroll
+            for (int g = 0; g < S; ++g)
+              h = (h << 7) + (long long)(BF ? (int)__uint_as_float(v[g][q2]) : (int)v[g][q2]);
+            const int c = c0 + cc + q2;
+            if (c < cout) drow[q2] = (T)((((double)h * pow2i(-7 * (S + 1))) * xs) * pow2i(ew[c]));
+          }
+        }
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_expect_tx(&acce[b], 0);  // this warp's arrival: the buffer's lanes are read
+    }
+  }
+  __syncthreads();
+  if (warp == 0 && lane == 0) {
+    // copies issued but never consumed (only after a wait ran out)
+    for (int q = consumed_q; q < issued_q; ++q) mbar_wait(&full[q % ST], (q / ST) & 1, OZK_POLLS);
+  }
+  const bool okd = __syncthreads_and(mbar_wait(&done, 0, OZK_POLLS) ? 1 : 0) && !failed;
+  if (!okd && threadIdx.x == 0 && status) {
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+      const int m0 = (t / ntc) * OZK_BM, r1 = min(m0 + OZK_BM, rows) - 1;
+      for (int qq = m0 / rows_per_status; qq <= r1 / rows_per_status; ++qq) atomicOr(status + qq, bit);
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 1) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem) : "memory");
+}
+
 // digits of one row per warp, in two coalesced passes over the row (the
 // second from L1).  The first pass (lane l reads positions 32 t + l) gives
 // the row maximum (a warp reduction) and so the row's exponent; in the
@@ -432,6 +637,19 @@ int prepare_one() {
   return SCY_OK;
 }
 
+template <int S, typename T, int BF>
+int prepare_pers() {
+  static unsigned long long attr_set = 0;
+  int dev = 0;
+  SCY_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64 || !(attr_set >> dev & 1ull)) {
+    SCY_CUDA_TRY(cudaFuncSetAttribute(ozk_gemm_pers_kernel<S, T, BF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      ozk_pers_smem_bytes(S)));
+    if (dev >= 0 && dev < 64) attr_set |= 1ull << dev;
+  }
+  return SCY_OK;
+}
+
 template <int S, int BF>
 int prepare_sb() {
   int rc = prepare_one<S, double, 0, BF>();
@@ -439,8 +657,23 @@ int prepare_sb() {
   if constexpr (S <= 5) {
     if (rc == SCY_OK) rc = prepare_one<S, double, 1, BF>();
     if (rc == SCY_OK) rc = prepare_one<S, float, 1, BF>();
+    if (rc == SCY_OK) rc = prepare_pers<S, double, BF>();
+    if (rc == SCY_OK) rc = prepare_pers<S, float, BF>();
   }
   return rc;
+}
+
+// multiprocessors of the current device (cached per device)
+int sm_count() {
+  static int cached[64] = {0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return kNumSMs;
+  if (!cached[dev]) {
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n < 1) n = kNumSMs;
+    cached[dev] = n;
+  }
+  return cached[dev];
 }
 
 template <int S>
@@ -465,10 +698,26 @@ int launch_gemm(const OzkOperand& x, const CUtensorMap& wmap, const OzkOperand& 
   return SCY_OK;
 }
 
+// the persistent shape: one CTA per SM (at most one per tile)
+template <int S, typename T, int BF>
+int launch_pers(const OzkOperand& x, const OzkOperand& w, T* D, long ldd, int cout, cudaStream_t s,
+                unsigned* status, int rows_per_status, unsigned bit) {
+  constexpr int CN = ozk_cn(S, 1);
+  SCY_TRY((prepare_pers<S, T, BF>()));
+  const long ntiles = (long)((cout + CN - 1) / CN) * ((x.rows + OZK_BM - 1) / OZK_BM);
+  const int grid = (int)std::min<long>(ntiles, sm_count());
+  ozk_gemm_pers_kernel<S, T, BF><<<grid, 256, ozk_pers_smem_bytes(S), s>>>(
+      x.map, w.map_pair, x.expo.as<int>(), w.expo.as<int>(), D, ldd, x.rows, cout, x.Kp * x.esz / 32, status,
+      rows_per_status, bit);
+  SCY_LAUNCH_CHECK();
+  return SCY_OK;
+}
+
 template <int S, typename T, int BF>
 int launch_variant_b(const OzkOperand& x, const OzkOperand& w, T* D, long ldd, int cout, cudaStream_t s,
                      unsigned* status, int rps, unsigned bit, int pair) {
   if constexpr (S <= 5) {
+    if (pair == 2) return launch_pers<S, T, BF>(x, w, D, ldd, cout, s, status, rps, bit);
     if (pair) return launch_gemm<S, T, 1, BF>(x, w.map_pair, w, D, ldd, cout, s, status, rps, bit);
   }
   return launch_gemm<S, T, 0, BF>(x, w.map, w, D, ldd, cout, s, status, rps, bit);
@@ -484,11 +733,11 @@ int launch_variant(const OzkOperand& x, const OzkOperand& w, T* D, long ldd, int
 template <typename T>
 int gemm_any(const OzkOperand& x, const OzkOperand& w, T* D, long ldd, int cout, cudaStream_t s, unsigned* status,
              int rps, unsigned bit, int pair) {
-  pair = pair ? 1 : 0;
+  pair = pair == 2 ? 2 : pair ? 1 : 0;
   if (x.S != w.S || x.Kp != w.Kp || x.K != w.K || x.esz != w.esz || cout > w.rows || cout < 1 || x.rows < 1 ||
       w.box_rows != ozk_cn(w.S) || x.box_rows != OZK_BM || rps < 1 ||
       (pair && (w.S > 5 || w.box_rows_pair != ozk_cn(w.S, 1)))) {
-    set_error("ozk_gemm: operands do not match (S %d/%d, K %d/%d, cout %d, W rows %d, two CTAs per SM %d)", x.S,
+    set_error("ozk_gemm: operands do not match (S %d/%d, K %d/%d, cout %d, W rows %d, shape %d)", x.S,
               w.S, x.K, w.K, cout, w.rows, pair);
     return SCY_ERR_ARG;
   }
@@ -658,7 +907,7 @@ extern "C" scy_status scy_ozaki_matmul(const double* X, long ldx, int rows, int 
                                        int cols, int S, double* D, long ldd, int ctas_per_sm, int bf16_digits) {
   using namespace scy;
   if (!X || !W || !D || rows < 1 || cols < 1 || K < 1 || ldx < K || ldw < K || ldd < cols ||
-      (ctas_per_sm != 1 && ctas_per_sm != 2) || (ctas_per_sm == 2 && S > 5) ||
+      (ctas_per_sm < 0 || ctas_per_sm > 2) || (ctas_per_sm != 1 && S > 5) ||
       (bf16_digits && !ozk_bf16_exact(S, K))) {
     set_error("scy_ozaki_matmul: invalid arguments");
     return SCY_ERR_ARG;
@@ -673,7 +922,8 @@ extern "C" scy_status scy_ozaki_matmul(const double* X, long ldx, int rows, int 
   DevBuf status;
   SCY_TRY(status.alloc(sizeof(unsigned)));
   SCY_CUDA_TRY(cudaMemsetAsync(status.p, 0, sizeof(unsigned), s));
-  SCY_TRY(ozk_gemm(x, w, D, ldd, cols, s, status.as<unsigned>(), 1 << 30, 1u, ctas_per_sm == 2 ? 1 : 0));
+  SCY_TRY(ozk_gemm(x, w, D, ldd, cols, s, status.as<unsigned>(), 1 << 30, 1u,
+                   ctas_per_sm == 2 ? 1 : ctas_per_sm == 0 ? 2 : 0));
   unsigned st = 0;
   SCY_CUDA_TRY(cudaMemcpyAsync(&st, status.p, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
   SCY_CUDA_TRY(cudaStreamSynchronize(s));

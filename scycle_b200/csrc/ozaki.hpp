@@ -72,8 +72,9 @@ int ozk_set_host(OzkOperand& o, const double* W, long ldw, cudaStream_t s);
 // D[r, c] = sum_k X[r, k] W[c, k] for r < x.rows, c < cout (<= w.rows),
 // D of row stride ldd.  x.S == w.S.  A wait inside the kernel that runs out
 // (2^20 polls) sets `bit` in status[r / rows_per_status] for the rows of its
-// tile when status is given.  pair = 1 takes the two-CTAs-per-SM shape (S <=
-// 5, W made by alloc_weights); the two shapes give identical results.
+// tile when status is given.  pair = 1 takes the two-CTAs-per-SM shape, pair
+// = 2 the persistent shape with double-buffered accumulators (both S <= 5,
+// W made by alloc_weights); the shapes give identical results.
 int ozk_gemm(const OzkOperand& x, const OzkOperand& w, double* D, long ldd, int cout, cudaStream_t s,
              unsigned* status = nullptr, int rows_per_status = 1, unsigned bit = 4u, int pair = 0);
 int ozk_gemm(const OzkOperand& x, const OzkOperand& w, float* D, long ldd, int cout, cudaStream_t s,

@@ -106,6 +106,25 @@ def test_ozaki_two_ctas_per_sm_shape_gives_the_same_product(s):
     np.testing.assert_allclose(D2, emulate(X, W, s), rtol=1e-15, atol=1e-300)
 
 
+@pytest.mark.parametrize("s", [3, 4, 5])
+@pytest.mark.parametrize("rows,K,cols", [(700, 401, 401), (5000, 401, 401), (1500, 129, 200)])
+@pytest.mark.parametrize("bf16", [0, 1])
+def test_ozaki_persistent_shape_gives_the_same_product(s, rows, K, cols, bf16):
+    """The persistent shape (one CTA per SM walking the tiles, two
+    accumulator sets in tensor memory, one tile's epilogue under the next
+    tile's products) gives bit-for-bit the product of the one-CTA-per-tile
+    shape: with fewer tiles than SMs, with several tiles per CTA (5000 rows:
+    40 x 9 tiles), and with a narrow last column tile."""
+    rng = np.random.default_rng(80 + s + rows)
+    X = rng.standard_normal((rows, K)) * np.exp(2 * rng.standard_normal((rows, 1)))
+    X[3] = 0.0
+    W = rng.standard_normal((cols, K))
+    D1 = _matmul(X, W, s, ctas=1, bf16=bf16)
+    D0 = _matmul(X, W, s, ctas=0, bf16=bf16)
+    assert np.array_equal(D0, D1)
+    assert np.all(D0[3] == 0.0)
+
+
 @pytest.mark.parametrize("s", [3, 4, 5, 6, 7])
 @pytest.mark.parametrize("ctas", [1, 2])
 def test_ozaki_bf16_digits_give_the_same_product(s, ctas):
