@@ -7,8 +7,10 @@
 // stage); thread 0 of warp 1 issues, per stage and per 32-byte K step, the
 // S(S+1)/2 digit products (tcgen05.mma.cta_group::1.kind::i8, both operands
 // K-major in shared memory, signed 8-bit, 32-bit integer accumulators) into
-// S accumulators of 128 x CN in tensor memory, one per digit-weight group,
-// and frees each stage with tcgen05.commit on its "empty" mbarrier.  After
+// S accumulators of 128 x CN in tensor memory, one per digit-weight group
+// (the products of one X plane with a stack of W planes as one MMA of N up
+// to 256, see ozk_issue_kstep), and frees each stage with tcgen05.commit on
+// its "empty" mbarrier.  After
 // the last stage all four warps read their 32 rows of the accumulators
 // (tcgen05.ld 32x32b), combine the groups with their powers of two, apply
 // the row and column exponents (loaded by warps 2 and 3 while the products
@@ -145,6 +147,34 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
       : "r"(taddr));
 }
 
+// The digit products of one 32-byte K step: X plane p times the stack of W
+// planes 1 .. S+1-p.  Their products belong to the consecutive groups
+// p-1 .. S-1, whose accumulators are consecutive in tensor memory, and the
+// W planes are consecutive CN-row blocks of the stage, so one MMA of N =
+// planes x CN (at most 256) covers as many of them as fit: the A tile is read
+// once per MMA instead of once per product.  Integer (and the exact FP32)
+// sums are the same in any order.  first: the tile's first K step (the
+// products of X plane 1 start every group).
+template <int S, int CN, int BF>
+__device__ __forceinline__ void ozk_issue_kstep(uint32_t tacc, uint32_t xa, uint32_t wa, int ks, bool first) {
+  constexpr int PER = 256 / CN;  // W planes per MMA
+#pragma unroll
+  for (int p = 1; p <= S; ++p) {
+#pragma unroll
+    for (int j0 = 1; j0 <= S + 1 - p; j0 += PER) {
+      const int np = (S + 2 - p - j0) < PER ? (S + 2 - p - j0) : PER;
+      const uint64_t ad = umma_desc_sw64(xa + (p - 1) * OZK_BM * OZK_BK + ks * 32);
+      const uint64_t bd = umma_desc_sw64(wa + (j0 - 1) * CN * OZK_BK + ks * 32);
+      const uint32_t idesc = BF ? umma_idesc_bf16(np * CN) : umma_idesc_s8(np * CN);
+      const uint32_t acc = (first && p == 1) ? 0u : 1u;
+      if (BF)
+        umma_bf16(tacc + (p + j0 - 2) * CN, ad, bd, idesc, acc);
+      else
+        umma_s8(tacc + (p + j0 - 2) * CN, ad, bd, idesc, acc);
+    }
+  }
+}
+
 template <int S, typename T, int PAIR, int BF>
 __global__ void __launch_bounds__(128, PAIR ? 2 : 1)
     ozk_gemm_kernel(const __grid_constant__ CUtensorMap mx, const __grid_constant__ CUtensorMap mw,
@@ -226,7 +256,6 @@ __global__ void __launch_bounds__(128, PAIR ? 2 : 1)
     }
   } else if (warp == 1 && lane == 0) {
     // MMA issuer
-    const uint32_t idesc = BF ? umma_idesc_bf16(nmma) : umma_idesc_s8(nmma);
     int q = 0;
     for (; q < nkb; ++q) {
       const int st = q % ST, kb = (q + rot) % nkb;
@@ -240,18 +269,7 @@ __global__ void __launch_bounds__(128, PAIR ? 2 : 1)
 #pragma unroll
       for (int ks = 0; ks < 2; ++ks) {
         if (2 * kb + ks >= nks) break;
-#pragma unroll
-        for (int g = 0; g < S; ++g)
-#pragma unroll
-          for (int i = 1; i <= g + 1; ++i) {
-            const int j = g + 2 - i;
-            const uint64_t ad = umma_desc_sw64(xa + (i - 1) * OZK_BM * OZK_BK + ks * 32);
-            const uint64_t bd = umma_desc_sw64(wa + (j - 1) * CN * OZK_BK + ks * 32);
-            if (BF)
-              umma_bf16(tmem + g * CN, ad, bd, idesc, (q > 0 || ks > 0 || i > 1) ? 1u : 0u);
-            else
-              umma_s8(tmem + g * CN, ad, bd, idesc, (q > 0 || ks > 0 || i > 1) ? 1u : 0u);
-          }
+        ozk_issue_kstep<S, CN, BF>(tmem, xa, wa, ks, q == 0 && ks == 0);
       }
       umma_commit(&empty[st]);
     }
@@ -412,10 +430,8 @@ __global__ void __launch_bounds__(256, 1)
     // MMA issuer
     int q = 0, i = 0;
     for (int t = blockIdx.x; t < ntiles && !failed; t += gridDim.x, ++i) {
-      const int ct = t % ntc, rt = t / ntc, c0 = ct * CN;
+      const int ct = t % ntc, rt = t / ntc;
       const int rot = (int)((ct * 7u + rt) % (unsigned)nkb);
-      const int nmma = max(32, min(CN, (cout - c0 + 15) / 16 * 16));
-      const uint32_t idesc = BF ? umma_idesc_bf16(nmma) : umma_idesc_s8(nmma);
       const int b = i & 1;
       if (i >= 2 && !mbar_wait(&acce[b], ((i >> 1) - 1) & 1, OZK_POLLS)) {
         failed = 1;
@@ -437,19 +453,7 @@ __global__ void __launch_bounds__(256, 1)
 #pragma unroll
         for (int ks = 0; ks < 2; ++ks) {
           if (2 * kb + ks >= nks) break;
-#pragma unroll
-          for (int g = 0; g < S; ++g)
-#pragma unroll
-            for (int p = 1; p <= g + 1; ++p) {
-              const int j = g + 2 - p;
-              const uint64_t ad = umma_desc_sw64(xa + (p - 1) * OZK_BM * OZK_BK + ks * 32);
-              const uint64_t bd = umma_desc_sw64(wa + (j - 1) * CN * OZK_BK + ks * 32);
-              const uint32_t acc = (k > 0 || ks > 0 || p > 1) ? 1u : 0u;
-              if (BF)
-                umma_bf16(tb + g * CN, ad, bd, idesc, acc);
-              else
-                umma_s8(tb + g * CN, ad, bd, idesc, acc);
-            }
+          ozk_issue_kstep<S, CN, BF>(tb, xa, wa, ks, k == 0 && ks == 0);
         }
         umma_commit(&empty[st]);
         ++q;
