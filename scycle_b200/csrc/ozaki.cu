@@ -281,7 +281,7 @@ __global__ void __launch_bounds__(128, PAIR ? 2 : 1)
     // copies issued but never consumed (only after a wait ran out)
     for (int q = consumed; q < issued; ++q) mbar_wait(&full[q % ST], (q / ST) & 1, OZK_POLLS);
   }
-  // one verdict for the whole block: the warp-collective tensor-memory
+  // one decision for the whole block: the warp-collective tensor-memory
   // loads below run in every warp or in none
   const bool ok = __syncthreads_and(mbar_wait(&done, 0, OZK_POLLS) ? 1 : 0) && !failed;
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
