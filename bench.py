@@ -199,6 +199,12 @@ BATCH_WORKLOAD = ("slip_var_401 ensemble: %d instances per GPU of the 401x401 st
                   "(seeds differ: lognormal Dc and initial state), every instance with its own RK32 step control")
 
 
+def batch_config(args, world):
+    """The workload description shared by both arms of the headline line."""
+    return {"workload": BATCH_WORKLOAD % args.batch, "Ny": args.n, "Nz": args.n, "integrator": "RK32",
+            "instances_per_gpu": args.batch, "parallelism": "replicas x%d" % world}
+
+
 def run_batched(args, dist, rank, world, local):
     """The batched ensemble: args.batch instances of the workload per GPU
     advanced together (one CUDA graph launch per round of attempts).  A step
@@ -771,22 +777,20 @@ def run_ours(args, dist, rank, world, local):
         except Exception as e:  # reported, not fatal to the headline
             adjoint_c4 = {"error": str(e)}
     head = batched if batched else single
-    config = {"workload": (BATCH_WORKLOAD % args.batch) if batched else WORKLOAD, "Ny": args.n, "Nz": args.n,
-              "integrator": "RK32", "parallelism": "replicas x%d" % world}
     if batched:
-        config.update({"instances_per_gpu": args.batch,
-                       "solver": "FP64 CG preconditioned by fast diagonalisation (%s preconditioner; z transforms "
-                                 "on the integer tensor cores, banded sweeps along y), device-verified rtol %g"
-                                 % (args.batch_precision, args.rtol),
-                       "l2": "not flushed: the ensemble's working set (about 20 MB per instance) exceeds the "
-                             "126 MB L2"})
+        config = batch_config(args, world)
+        solver = ("FP64 CG preconditioned by fast diagonalisation (%s preconditioner; z transforms on the integer "
+                  "tensor cores, banded sweeps along y), device-verified rtol %g" % (args.batch_precision, args.rtol))
+        l2 = "not flushed: the ensemble's working set (about 20 MB per instance) exceeds the 126 MB L2"
     else:
-        config.update({"solver": single["solver"], "l2": single["l2"]})
+        config = {"workload": WORKLOAD, "Ny": args.n, "Nz": args.n, "integrator": "RK32",
+                  "parallelism": "replicas x%d" % world}
+        solver, l2 = single["solver"], single["l2"]
     out = {"metric": METRIC, "value": head["value"], "unit": "stage-solves/s", "n_gpus": world,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": head["ms_per_step"],
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
            "dtype": "f64 (%s preconditioner)" % ((args.batch_precision if batched else prec)),
-           "data": "synthetic (seeded; reference .in format)", "config": config,
+           "data": "synthetic (seeded; reference .in format)", "config": config, "solver": solver, "l2": l2,
            "sim_years_per_hour": head["sim_years_per_hour"], "sim_years_timed": head["sim_years_timed"],
            "stage_solves": head["stage_solves"], "e2e": head["e2e"],
            "roofline": (batched.get("roofline") or roofline) if batched else roofline, "cpu_baseline": cpu,
@@ -977,12 +981,15 @@ def _pool_init(barrier):
 
 
 def _oracle_worker(job):
-    """One oracle instance: set-up, wait at the barrier, time ``steps`` RK32
-    steps.  Returns (stage-solves, seconds, simulated seconds, set-up s)."""
+    """One oracle instance: set-up, wait at the barrier, run ``warm`` untimed
+    and then ``steps`` timed RK32 steps in one integration (the step control
+    carries on from the warm-up).  The timed window starts when the oracle's
+    time monitor reports step ``warm``.  Returns (timed stage-solves, timed
+    seconds, timed simulated seconds, set-up seconds)."""
     import tempfile as _tf
     from oracle.problem import build_qd_problem
     from oracle.qd import QDLinearElastic
-    kind, seed, n, steps = job
+    kind, seed, n, steps, warm = job
     t0 = time.perf_counter()
     work = _tf.mkdtemp(prefix="scy_cpu_")
     if kind == "c1":
@@ -994,18 +1001,37 @@ def _oracle_worker(job):
     ora = QDLinearElastic(P, keep_history=False)
     var0 = ora.initiate_integrand()
     setup = time.perf_counter() - t0
+    calls = [0]
+    mark = {}
+    d_dt, monitor = ora.d_dt, ora.time_monitor
+
+    def counted_d_dt(t, var):
+        calls[0] += 1
+        return d_dt(t, var)
+
+    def marked_monitor(t, dt, step):
+        if step == warm and not mark:
+            mark.update(t=time.perf_counter(), calls=calls[0], sim=t)
+        return monitor(t, dt, step)
+
+    ora.d_dt, ora.time_monitor = counted_d_dt, marked_monitor
     if _POOL_BARRIER is not None:
         _POOL_BARRIER.wait()
+    rk = ora.integrate(max_steps=warm + steps, var0=var0)
     t1 = time.perf_counter()
-    rk = ora.integrate(max_steps=steps, var0=var0)
-    el = time.perf_counter() - t1
-    return rk.stage_evals, el, rk.currT - P["driver"]["initTime"], setup
+    if not mark:  # the run ended inside the warm-up: nothing timed
+        return 0, 1e-30, 0.0, setup
+    return calls[0] - mark["calls"], t1 - mark["t"], rk.currT - mark["sim"], setup
 
 
-def oracle_on_all_cores(kind, steps, n=401, max_workers=None):
-    """Runs one oracle instance per usable core (capped by host memory: a
-    401^2 instance holds about 4 GB at its peak) and returns the aggregate
-    stage-solves/s over the timed steps."""
+def oracle_on_all_cores(kind, steps, n=401, max_workers=None, instances=None, warm=0):
+    """Runs oracle instances of the workload on the host cores, one single-
+    threaded instance per usable core at a time (capped by host memory: a
+    401^2 instance holds about 4 GB at its peak), and returns the aggregate
+    stage-solves/s over the timed steps.  ``instances``: how many instances
+    (seeds 0 .. instances-1) to run in all, in rounds of one per core (the
+    aggregate is the timed stage-solves of every round over the sum of the
+    rounds' slowest timed windows); default one per core."""
     import multiprocessing as mp
     cores = _host_cores()
     per = 5e9 if kind == "c1" else 0.5e9
@@ -1013,14 +1039,21 @@ def oracle_on_all_cores(kind, steps, n=401, max_workers=None):
     workers = cores if avail is None else max(1, min(cores, int(avail // per)))
     if max_workers:
         workers = min(workers, max_workers)
+    total = instances if instances else workers
     saved = {k: os.environ.get(k) for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS")}
     for k in saved:
         os.environ[k] = "1"
+    res, rounds, wall = [], 0, 0.0
     try:
         ctx = mp.get_context("spawn")  # the parent may already hold a CUDA context
-        barrier = ctx.Barrier(workers)
-        with ctx.Pool(workers, initializer=_pool_init, initargs=(barrier,)) as pool:
-            res = pool.map(_oracle_worker, [(kind, s, n, steps) for s in range(workers)])
+        for first in range(0, total, workers):
+            seeds = list(range(first, min(total, first + workers)))
+            barrier = ctx.Barrier(len(seeds))
+            with ctx.Pool(len(seeds), initializer=_pool_init, initargs=(barrier,)) as pool:
+                got = pool.map(_oracle_worker, [(kind, s, n, steps, warm) for s in seeds])
+            res += got
+            rounds += 1
+            wall += max(r[1] for r in got)
     finally:
         for k, v in saved.items():
             if v is None:
@@ -1028,11 +1061,13 @@ def oracle_on_all_cores(kind, steps, n=401, max_workers=None):
             else:
                 os.environ[k] = v
     evals = sum(r[0] for r in res)
-    value = sum(r[0] / r[1] for r in res)
+    value = evals / wall
     return {"value": value, "unit": "stage-solves/s", "cores": workers, "host_cores": cores,
-            "cpu_model": _cpu_model(), "workers": workers, "steps_per_worker": steps, "stage_solves": evals,
-            "timed_s_max": max(r[1] for r in res), "setup_s_max": max(r[3] for r in res),
-            "sim_years_per_hour": sum((r[2] / YEAR) / (r[1] / 3600.0) for r in res)}
+            "cpu_model": _cpu_model(), "workers": workers, "instances": total, "rounds": rounds,
+            "warmup_steps_per_instance": warm, "steps_per_worker": steps, "stage_solves": evals,
+            "timed_s_max": max(r[1] for r in res), "timed_s_sum_of_rounds": wall,
+            "setup_s_max": max(r[3] for r in res),
+            "sim_years_per_hour": sum(r[2] for r in res) / YEAR / (wall / 3600.0)}
 
 
 def run_ztransform_only(args):
@@ -1069,24 +1104,31 @@ def cpu_baseline(args):
 
 
 def run_reference(args, dist, rank, world, local):
-    """The reference arm: the oracle port of the reference's CPU path on all
-    host cores, each core running its own instance of the headline workload
-    for ``--steps`` RK32 steps (rank 0 only)."""
+    """The reference arm: the oracle port of the reference's CPU path timed on
+    the host cores over the headline ensemble (the same ``--batch`` instances
+    and seeds as one GPU's batch), each instance ``--warmup`` untimed and then
+    ``--steps`` timed RK32 steps (capped by ``--cpu-steps-ref``), one single-
+    threaded instance per core at a time (rank 0 only)."""
     if rank != 0:
         return
     k = max(1, min(args.steps, args.cpu_steps_ref))
-    r = oracle_on_all_cores("c1", k, n=args.n)
+    inst = args.batch if args.batch > 0 else 1
+    r = oracle_on_all_cores("c1", k, n=args.n, instances=inst, warm=args.warmup)
     value = r["value"]
     cpu = dict(r)
     cpu.update({"kind": "port",
-                "sample": "%d RK32 steps on each of %d single-threaded oracle instances (one per core), "
-                          "factorisations and steady-state guess excluded" % (k, r["workers"])})
-    out = {"impl": "reference", "metric": METRIC, "value": value, "unit": "stage-solves/s", "n_gpus": 1,
-           "steps": k, "warmup": 0, "ms_per_step": r["timed_s_max"] * 1e3 / k, "higher_is_better": True,
-           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded; reference .in format)",
-           "config": {"workload": BATCH_WORKLOAD % r["workers"], "Ny": args.n, "Nz": args.n, "integrator": "RK32",
-                      "solver": "SciPy SuperLU direct (stands in for the reference's MUMPS Cholesky)",
-                      "parallelism": "one instance per host core"},
+                "sample": "%d instances (seeds 0..%d) of the 401x401 workload, %d untimed and %d timed RK32 steps "
+                          "each, in %d round(s) of one single-threaded oracle instance per core on %d cores; "
+                          "SuperLU factorisations and the steady-state initial guess before the warm-up"
+                          % (inst, inst - 1, args.warmup, k, r["rounds"], r["workers"])})
+    config = batch_config(args, 1) if args.batch > 0 else {"workload": WORKLOAD, "Ny": args.n, "Nz": args.n,
+                                                            "integrator": "RK32", "parallelism": "replicas x1"}
+    out = {"impl": "reference", "metric": METRIC, "value": value, "unit": "stage-solves/s", "n_gpus": world,
+           "steps": k, "warmup": args.warmup, "ms_per_step": r["timed_s_sum_of_rounds"] * 1e3 / k,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic (seeded; reference .in format)", "config": config,
+           "solver": "SciPy SuperLU direct (stands in for the reference's MUMPS Cholesky), factorised once per "
+                     "instance", "host_parallelism": "one single-threaded instance per host core",
            "cpu_baseline": cpu,
            "e2e": {"value": value, "unit": "stage-solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
@@ -1104,7 +1146,7 @@ def main():
     ap.add_argument("--check-every", type=int, default=1)
     ap.add_argument("--precond", default="auto", choices=["auto", "mg", "fd"])
     ap.add_argument("--cpu-steps", type=int, default=10, help="RK32 steps per core of the CPU baseline")
-    ap.add_argument("--cpu-steps-ref", type=int, default=20, help="cap on the reference arm's steps per core")
+    ap.add_argument("--cpu-steps-ref", type=int, default=20, help="cap on the reference arm's timed steps per instance")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-response", action="store_true")
     ap.add_argument("--no-cycle", action="store_true", help="skip the 801x801 quasi-dynamic / fully dynamic cycles")
