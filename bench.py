@@ -1196,12 +1196,14 @@ def main():
     if args.profile_batch:
         run_batch_only_profile(args)
         return
+    if args.impl == "reference":
+        # rank 0 alone runs the CPU reference; with no process group the other
+        # ranks exit at once instead of waiting minutes at a collective
+        run_reference(args, None, int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), 0)
+        return
     dist, rank, world, local = _dist()
     try:
-        if args.impl == "reference":
-            run_reference(args, dist, rank, world, local)
-        else:
-            run_ours(args, dist, rank, world, local)
+        run_ours(args, dist, rank, world, local)
     finally:
         if dist is not None:
             dist.barrier()
