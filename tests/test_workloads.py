@@ -5,7 +5,8 @@ configurations (scycle_b200/configs.py), read back through the oracle's
 with a per-node lognormal Dc (mean 8 mm, sigma_ln 0.2); the power-law
 ensemble of three grid sizes with a linear geotherm of gradient U(15, 30)
 K/km and a - b perturbed by a Gaussian random field of std 0.002 and
-correlation length 2 km."""
+correlation length 2 km; the 201^2 adjoint workload with a, b and Dc given at
+40 depth knots each (120 parameters)."""
 import os
 import re
 
@@ -78,3 +79,17 @@ def test_pl_ensemble_sizes_geotherm_and_ab_field(tmp_path):
         c_far.append(np.mean(d[:-100] * d[100:]))
     assert np.mean(c_near) > 0.8 * d_all.var()
     assert abs(np.mean(c_far)) < 0.3 * d_all.var()
+
+
+def test_adjoint_c4_knots(tmp_path):
+    from scycle_b200.configs import C4_DEPTHS, adjoint_c4
+    path, K, knots = adjoint_c4(str(tmp_path))
+    P = _problem(path)
+    assert P["Ny"] == P["Nz"] == 201 and P["fault"]["stateLaw"] == "agingLaw"
+    assert K.shape == (201, 40) and len(C4_DEPTHS) == 40 and sum(len(k) for k in knots) == 120
+    # the piecewise-linear map from the 40 knots reproduces the fields it wrote,
+    # and every row of it is a partition of unity
+    np.testing.assert_allclose(K.sum(axis=1), 1.0, atol=1e-14)
+    for nm, k in zip(("a", "b", "Dc"), knots):
+        np.testing.assert_allclose(P[nm], K @ k, rtol=1e-14, atol=1e-16)
+    assert P["driver"]["timeIntegrator"] == "RK32"
